@@ -1,0 +1,210 @@
+"""Correlation job description.
+
+A job mirrors the tables that the reference reads from a DiFX ``.input`` file
+(mpifxcorr/src/configuration.cpp: FREQ TABLE :1982-2052, DATASTREAM TABLE
+:1433-1800, BASELINE TABLE :1059-1120, CONFIGURATIONS :1349-1430) for the one
+configuration this hot path correlates:
+
+* ``freqs``     -- the frequency table (sky frequency of the band edge, width,
+                   sideband, channel count);
+* ``stations``  -- one datastream per station: VDIF framing, bits per sample,
+                   recorded bands (frequency-table index and polarisation) in
+                   VDIF channel order, delay model;
+* ``baselines`` -- station pairs with, per frequency, the list of
+                   (band of station A, band of station B) polarisation products.
+
+The product library receives this as the plain C struct declared in
+include/fxb200.h (built by :func:`Job.to_native`).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Sequence, Tuple
+
+
+@dataclasses.dataclass
+class Freq:
+    freq_mhz: float          # sky frequency of the band edge (LO), MHz
+    bw_mhz: float            # bandwidth, MHz
+    nchan: int               # output channels (FFT length is 2*nchan)
+    sideband: str = "U"      # 'U' or 'L'
+    chans_to_avg: int = 1
+
+
+@dataclasses.dataclass
+class DelayPoly:
+    """Per-station delay polynomial in the ``.im`` convention
+    (mpifxcorr/src/model.cpp:229-299): delay(us) = sum_k c[k] * dt**k with dt
+    the seconds since ``start_sec`` (seconds after the job start), valid for
+    ``interval_s`` seconds.  A station may carry several consecutive polys."""
+    start_sec: float
+    interval_s: int
+    coeffs: Tuple[float, ...]
+
+
+@dataclasses.dataclass
+class Station:
+    name: str
+    bands: List[Tuple[int, str]]      # (freq index, pol) in VDIF channel order
+    nbits: int = 2
+    payload_bytes: int = 8000
+    header_bytes: int = 32
+    polys: List[DelayPoly] = dataclasses.field(default_factory=list)
+    clock_us: float = 0.0             # constant clock offset folded into the model
+
+    def recorded_freqs(self) -> List[int]:
+        seen: List[int] = []
+        for f, _ in self.bands:
+            if f not in seen:
+                seen.append(f)
+        return seen
+
+    @property
+    def nband(self) -> int:
+        return len(self.bands)
+
+
+@dataclasses.dataclass
+class Baseline:
+    ds1: int
+    ds2: int
+    # per frequency index: list of (band index in ds1, band index in ds2)
+    products: List[Tuple[int, List[Tuple[int, int]]]]
+
+
+@dataclasses.dataclass
+class Job:
+    freqs: List[Freq]
+    stations: List[Station]
+    baselines: List[Baseline]
+    subint_ns: int
+    start_mjd: int = 58000
+    start_sec: int = 0
+    fringe_rot_order: int = 1
+    num_buffered_ffts: int = 10
+    write_autocorrs: bool = True
+    duration_s: float = 1.0
+
+    # ---- derived quantities -------------------------------------------------
+    def station_bw(self, s: int) -> float:
+        return self.freqs[self.stations[s].bands[0][0]].bw_mhz
+
+    def station_nchan(self, s: int) -> int:
+        return self.freqs[self.stations[s].bands[0][0]].nchan
+
+    def fft_ns(self) -> float:
+        f = self.freqs[self.stations[0].bands[0][0]]
+        return 2 * f.nchan * 1e3 / (2 * f.bw_mhz)
+
+    def blocks_per_send(self) -> int:
+        n = self.subint_ns / self.fft_ns()
+        if abs(n - round(n)) > 1e-9:
+            raise ValueError("subint must hold a whole number of FFTs")
+        return int(round(n))
+
+    def samples_per_sec(self, s: int) -> int:
+        return int(round(2e6 * self.station_bw(s)))
+
+    def frame_samples(self, s: int) -> int:
+        st = self.stations[s]
+        return st.payload_bytes * 8 // (st.nbits * st.nband)
+
+    def frame_bytes(self, s: int) -> int:
+        st = self.stations[s]
+        return st.payload_bytes + st.header_bytes
+
+    def frames_per_sec(self, s: int) -> int:
+        return self.samples_per_sec(s) // self.frame_samples(s)
+
+    def mbps(self, s: int) -> int:
+        st = self.stations[s]
+        return int(round(self.samples_per_sec(s) * st.nbits * st.nband / 1e6))
+
+    def vdif_format(self, s: int) -> str:
+        st = self.stations[s]
+        return "VDIF_%d-%d-%d-%d" % (st.payload_bytes, self.mbps(s), st.nband, st.nbits)
+
+    def max_products(self) -> int:
+        return max(len(pp) for b in self.baselines for _, pp in b.products)
+
+    def used_freqs(self) -> List[int]:
+        used = set()
+        for b in self.baselines:
+            for f, _ in b.products:
+                used.add(f)
+        return sorted(used)
+
+    def station_mhz_per_sec(self) -> float:
+        """N_station x sum of recorded band widths (each polarisation counted),
+        i.e. the station.MHz processed per second of data."""
+        return sum(self.freqs[f].bw_mhz for st in self.stations for f, _ in st.bands)
+
+    def packed_bytes_per_sec(self) -> float:
+        tot = 0.0
+        for s in range(len(self.stations)):
+            tot += self.frames_per_sec(s) * self.frame_bytes(s)
+        return tot
+
+    def validate(self) -> None:
+        nfft = None
+        for s, st in enumerate(self.stations):
+            bws = {self.freqs[f].bw_mhz for f, _ in st.bands}
+            nch = {self.freqs[f].nchan for f, _ in st.bands}
+            if len(bws) != 1 or len(nch) != 1:
+                raise ValueError("all bands of one station share bandwidth and channel count")
+            if st.nbits not in (2, 8):
+                raise ValueError("2-bit and 8-bit VDIF are supported")
+            if (st.payload_bytes * 8) % (st.nbits * st.nband):
+                raise ValueError("payload must hold whole samples")
+            if self.samples_per_sec(s) % self.frame_samples(s):
+                raise ValueError("whole frames per second required")
+        for b in self.baselines:
+            for f, pp in b.products:
+                for b1, b2 in pp:
+                    if self.stations[b.ds1].bands[b1][0] != f or self.stations[b.ds2].bands[b2][0] != f:
+                        raise ValueError("product bands must record the baseline frequency")
+        self.blocks_per_send()
+
+
+def full_job(nstation: int, freqs: Sequence[Freq], pols: str = "RL", full_pol: bool = True,
+             subint_ns: int = 8_000_000, nbits: int = 2, **kw) -> Job:
+    """All stations record every frequency in every polarisation; every station
+    pair forms a baseline with parallel hands (and cross hands when full_pol).
+    Product order per frequency follows vex2difx: RR, RL, LR, LL."""
+    stations = []
+    for s in range(nstation):
+        bands = [(f, p) for f in range(len(freqs)) for p in pols]
+        stations.append(Station(name="S%02d" % s, bands=bands, nbits=nbits))
+    baselines = []
+    for a in range(nstation):
+        for b in range(a + 1, nstation):
+            prods = []
+            for f in range(len(freqs)):
+                idx = {p: i for i, (ff, p) in enumerate(stations[a].bands) if ff == f}
+                pp = []
+                for p1 in pols:
+                    for p2 in pols:
+                        if p1 == p2 or full_pol:
+                            pp.append((idx[p1], idx[p2]))
+                # vex2difx order: parallel hands first, then cross hands
+                par = [x for x in pp if stations[a].bands[x[0]][1] == stations[b].bands[x[1]][1]]
+                cross = [x for x in pp if x not in par]
+                if full_pol and len(pols) == 2:
+                    pp = [par[0], cross[0], cross[1], par[1]]
+                else:
+                    pp = par + cross
+                prods.append((f, pp))
+            baselines.append(Baseline(ds1=a, ds2=b, products=prods))
+    return Job(freqs=list(freqs), stations=stations, baselines=baselines, subint_ns=subint_ns, **kw)
+
+
+def ceil_div(a: int, b: int) -> int:
+    return -(-a // b)
+
+
+def gcd_list(v: Sequence[int]) -> int:
+    g = 0
+    for x in v:
+        g = math.gcd(g, x)
+    return g

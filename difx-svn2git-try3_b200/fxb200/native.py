@@ -1,0 +1,264 @@
+"""ctypes binding of the product library (libfxb200.so, C ABI in
+include/fxb200.h) and the struct builder for a job description.
+
+The library must exist: on import of :func:`lib` a missing or unloadable
+libfxb200.so raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .job import Job
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(PKG_DIR), "csrc", "libfxb200.so")
+
+FXB_STATUS = {
+    0: "FXB_OK", 1: "FXB_ERR_ARG", 2: "FXB_ERR_UNSUPPORTED", 3: "FXB_ERR_CUDA", 4: "FXB_ERR_NOMEM",
+    5: "FXB_ERR_STATE", 6: "FXB_ERR_TIMEOUT", 7: "FXB_ERR_BUSY", 8: "FXB_ERR_DATA",
+}
+XMAC_KIND = {"fp32": 0, "bf16": 1, "fp8": 2}
+
+
+class FxbFreq(ctypes.Structure):
+    _fields_ = [("freq_mhz", ctypes.c_double), ("bw_mhz", ctypes.c_double), ("nchan", ctypes.c_int32),
+                ("lower_sideband", ctypes.c_int32), ("chans_to_avg", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class FxbStation(ctypes.Structure):
+    _fields_ = [("nbits", ctypes.c_int32), ("payload_bytes", ctypes.c_int32), ("header_bytes", ctypes.c_int32),
+                ("nband", ctypes.c_int32), ("band_freq", ctypes.POINTER(ctypes.c_int32)),
+                ("band_pol", ctypes.c_char_p)]
+
+
+class FxbBaseline(ctypes.Structure):
+    _fields_ = [("ds1", ctypes.c_int32), ("ds2", ctypes.c_int32), ("nprod", ctypes.c_int32),
+                ("prod_freq", ctypes.POINTER(ctypes.c_int32)), ("prod_band1", ctypes.POINTER(ctypes.c_int32)),
+                ("prod_band2", ctypes.POINTER(ctypes.c_int32))]
+
+
+class FxbJobDesc(ctypes.Structure):
+    _fields_ = [("nfreq", ctypes.c_int32), ("freqs", ctypes.POINTER(FxbFreq)),
+                ("nstation", ctypes.c_int32), ("stations", ctypes.POINTER(FxbStation)),
+                ("nbaseline", ctypes.c_int32), ("baselines", ctypes.POINTER(FxbBaseline)),
+                ("subint_ns", ctypes.c_int64), ("fringe_rot_order", ctypes.c_int32),
+                ("write_autocorrs", ctypes.c_int32), ("xmac_kind", ctypes.c_int32),
+                ("max_subints_in_flight", ctypes.c_int32)]
+
+
+class DescHolder:
+    """Owns every ctypes array the descriptor points into."""
+
+    def __init__(self, job: Job, xmac: str = "fp32", inflight: int = 2):
+        job.validate()
+        self.keep = []
+        fr = (FxbFreq * len(job.freqs))()
+        for i, f in enumerate(job.freqs):
+            fr[i] = FxbFreq(f.freq_mhz, f.bw_mhz, f.nchan, 1 if f.sideband == "L" else 0, f.chans_to_avg, 0)
+        st = (FxbStation * len(job.stations))()
+        for i, s in enumerate(job.stations):
+            bf = (ctypes.c_int32 * s.nband)(*[b[0] for b in s.bands])
+            bp = ctypes.create_string_buffer("".join(b[1] for b in s.bands).encode(), s.nband + 1)
+            self.keep += [bf, bp]
+            st[i] = FxbStation(s.nbits, s.payload_bytes, s.header_bytes, s.nband,
+                               ctypes.cast(bf, ctypes.POINTER(ctypes.c_int32)), ctypes.cast(bp, ctypes.c_char_p))
+        bl = (FxbBaseline * len(job.baselines))()
+        for i, b in enumerate(job.baselines):
+            pf, p1, p2 = [], [], []
+            for f, pp in b.products:
+                for x1, x2 in pp:
+                    pf.append(f); p1.append(x1); p2.append(x2)
+            a = (ctypes.c_int32 * len(pf))(*pf)
+            c1 = (ctypes.c_int32 * len(pf))(*p1)
+            c2 = (ctypes.c_int32 * len(pf))(*p2)
+            self.keep += [a, c1, c2]
+            bl[i] = FxbBaseline(b.ds1, b.ds2, len(pf), ctypes.cast(a, ctypes.POINTER(ctypes.c_int32)),
+                                ctypes.cast(c1, ctypes.POINTER(ctypes.c_int32)),
+                                ctypes.cast(c2, ctypes.POINTER(ctypes.c_int32)))
+        self.keep += [fr, st, bl]
+        self.desc = FxbJobDesc(len(job.freqs), ctypes.cast(fr, ctypes.POINTER(FxbFreq)),
+                               len(job.stations), ctypes.cast(st, ctypes.POINTER(FxbStation)),
+                               len(job.baselines), ctypes.cast(bl, ctypes.POINTER(FxbBaseline)),
+                               job.subint_ns, job.fringe_rot_order, 1 if job.write_autocorrs else 0,
+                               XMAC_KIND[xmac], inflight)
+
+    def ptr(self):
+        return ctypes.byref(self.desc)
+
+
+def poly_arrays(job: Job, s: int) -> Tuple[int, int, float, int, np.ndarray]:
+    """(npoly, order, poly0_sec, interval_s, coeffs) of station s, padded to
+    a common order, in the form fxb_set_delay_poly takes."""
+    polys = job.stations[s].polys
+    order = max(len(p.coeffs) for p in polys) - 1
+    coeffs = np.zeros((len(polys), order + 1))
+    for i, p in enumerate(polys):
+        coeffs[i, :len(p.coeffs)] = p.coeffs
+        coeffs[i, 0] += job.stations[s].clock_us
+    return len(polys), order, polys[0].start_sec, polys[0].interval_s, np.ascontiguousarray(coeffs.reshape(-1))
+
+
+# ---------------------------------------------------------------- library
+_lib = None
+
+
+class FxbError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load libfxb200.so; raises when it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FxbError("libfxb200.so not built at %s: run __graft_entry__.build()" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    i32p, i64p, fp, dp = (ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64),
+                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double))
+    L.fxb_create.restype = vp
+    L.fxb_create.argtypes = [ctypes.POINTER(FxbJobDesc), i32p]
+    L.fxb_destroy.argtypes = [vp]
+    L.fxb_last_error.restype = ctypes.c_char_p
+    L.fxb_last_error.argtypes = [vp]
+    L.fxb_set_delay_poly.argtypes = [vp, i32, i32, i32, ctypes.c_double, i32, dp]
+    L.fxb_submit_subint.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p), i64p, i32p, i32p,
+                                    ctypes.POINTER(ctypes.c_void_p), i32, i32]
+    L.fxb_submit_subint_device.argtypes = L.fxb_submit_subint.argtypes
+    L.fxb_sync.argtypes = [vp]
+    L.fxb_core_result_length.argtypes = [vp, i64p]
+    L.fxb_layout.argtypes = [vp, i32p, ctypes.c_size_t]
+    L.fxb_read_results.argtypes = [vp, fp, ctypes.c_size_t]
+    L.fxb_reset.argtypes = [vp]
+    L.fxb_last_timing.argtypes = [vp, fp, fp, fp]
+    L.fxb_read_spectra.argtypes = [vp, i32, fp, ctypes.c_size_t, i32p, i32p]
+    L.fxb_read_fft_weights.argtypes = [vp, fp, ctypes.c_size_t]
+    L.fxb_vdif_unpack.argtypes = [ctypes.c_void_p, i64, i32, i32, i32, i32, i64, i32, fp, i32p]
+    for name in ("fxb_set_delay_poly", "fxb_submit_subint", "fxb_submit_subint_device", "fxb_sync",
+                 "fxb_core_result_length", "fxb_layout", "fxb_read_results", "fxb_reset", "fxb_last_timing",
+                 "fxb_read_spectra", "fxb_read_fft_weights", "fxb_vdif_unpack"):
+        getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def check(rc: int, ctx=None, what: str = "") -> None:
+    if rc != 0:
+        msg = ""
+        try:
+            m = lib().fxb_last_error(ctx)
+            msg = m.decode() if m else ""
+        except Exception:
+            pass
+        raise FxbError("%s failed: %s %s" % (what, FXB_STATUS.get(rc, rc), msg))
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class Correlator:
+    """Python view of one fxb_ctx (the product path)."""
+
+    def __init__(self, job: Job, xmac: str = "fp32", inflight: int = 2):
+        self.job = job
+        self.holder = DescHolder(job, xmac=xmac, inflight=inflight)
+        st = ctypes.c_int32(0)
+        self.ctx = lib().fxb_create(self.holder.ptr(), ctypes.byref(st))
+        if not self.ctx:
+            err = lib().fxb_last_error(None)
+            raise FxbError("fxb_create: %s %s" % (FXB_STATUS.get(st.value, st.value), err.decode() if err else ""))
+        n = ctypes.c_int64(0)
+        check(lib().fxb_core_result_length(self.ctx, ctypes.byref(n)), self.ctx, "core_result_length")
+        self.corelen = n.value
+        for s in range(len(job.stations)):
+            npoly, order, p0, interval, coeffs = poly_arrays(job, s)
+            check(lib().fxb_set_delay_poly(self.ctx, s, npoly, order, p0, interval,
+                                           coeffs.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                  self.ctx, "set_delay_poly")
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            lib().fxb_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def layout(self) -> np.ndarray:
+        nf, nb, ns = len(self.job.freqs), len(self.job.baselines), len(self.job.stations)
+        out = np.zeros(2 * nf * nb + 2 * ns, dtype=np.int32)
+        check(lib().fxb_layout(self.ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), out.size),
+              self.ctx, "layout")
+        return out
+
+    def _submit(self, fn, ptrs: Sequence[int], nbytes: Sequence[int], dsec, dns, validflags, sec, ns):
+        n = len(ptrs)
+        bufs = (ctypes.c_void_p * n)(*ptrs)
+        nb = (ctypes.c_int64 * n)(*nbytes)
+        ds = (ctypes.c_int32 * n)(*dsec)
+        dn = (ctypes.c_int32 * n)(*dns)
+        if validflags is None:
+            vf = None
+        else:
+            vf = (ctypes.c_void_p * n)(*[v.ctypes.data if v is not None else None for v in validflags])
+        check(fn(self.ctx, bufs, nb, ds, dn, vf, sec, ns), self.ctx, "submit_subint")
+
+    def submit(self, inputs: List[Tuple[np.ndarray, int, int]], sec: int, ns: int,
+               validflags: Optional[List[np.ndarray]] = None) -> None:
+        self._submit(lib().fxb_submit_subint, [b.ctypes.data for b, _, _ in inputs], [b.size for b, _, _ in inputs],
+                     [s for _, s, _ in inputs], [x for _, _, x in inputs], validflags, sec, ns)
+
+    def submit_device(self, ptrs: Sequence[int], nbytes: Sequence[int], dsec, dns, sec: int, ns: int,
+                      validflags=None) -> None:
+        self._submit(lib().fxb_submit_subint_device, ptrs, nbytes, dsec, dns, validflags, sec, ns)
+
+    def sync(self):
+        check(lib().fxb_sync(self.ctx), self.ctx, "sync")
+
+    def results(self) -> np.ndarray:
+        out = np.zeros(2 * self.corelen, dtype=np.float32)
+        check(lib().fxb_read_results(self.ctx, _fptr(out), out.size), self.ctx, "read_results")
+        return out
+
+    def reset(self):
+        check(lib().fxb_reset(self.ctx), self.ctx, "reset")
+
+    def timing(self):
+        a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        check(lib().fxb_last_timing(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), self.ctx, "timing")
+        return a.value, b.value, c.value
+
+    def spectra(self, freq: int) -> np.ndarray:
+        T = self.job.blocks_per_send()
+        nchan = self.job.freqs[freq].nchan
+        rows = sum(1 for st in self.job.stations for f, _ in st.bands if f == freq)
+        out = np.zeros(T * nchan * rows * 2, dtype=np.float32)
+        nt, nr = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().fxb_read_spectra(self.ctx, freq, _fptr(out), out.size, ctypes.byref(nt), ctypes.byref(nr)),
+              self.ctx, "read_spectra")
+        x = out.reshape(nt.value, nchan, nr.value, 2)
+        return x[..., 0] + 1j * x[..., 1]
+
+    def fft_weights(self) -> np.ndarray:
+        T = self.job.blocks_per_send()
+        out = np.zeros(len(self.job.stations) * T, dtype=np.float32)
+        check(lib().fxb_read_fft_weights(self.ctx, _fptr(out), out.size), self.ctx, "read_fft_weights")
+        return out.reshape(len(self.job.stations), T)
+
+
+def vdif_unpack(data: np.ndarray, payload: int, header: int, nchan: int, nbits: int,
+                offsetsamples: int, nsamp: int) -> Tuple[np.ndarray, int]:
+    out = np.zeros((nchan, nsamp), dtype=np.float32)
+    good = ctypes.c_int32(0)
+    check(lib().fxb_vdif_unpack(data.ctypes.data, data.size, payload, header, nchan, nbits, offsetsamples,
+                                nsamp, _fptr(out), ctypes.byref(good)), None, "vdif_unpack")
+    return out, good.value

@@ -1,0 +1,200 @@
+"""Seeded synthetic VLBI baseband: correlated sky + station noise, quantised
+and packed into VDIF frames.
+
+Signal model (the stand-in for recorded data; no dataset is used):
+
+* one common real Gaussian sky signal per (frequency, polarisation), unit
+  variance, shared by all stations, delayed per station by its delay model;
+* independent unit-variance Gaussian noise per (station, band);
+* station voltage = sqrt(rho) * delayed sky + sqrt(1 - rho) * noise;
+* quantised to 2 bits with thresholds +-0.98 sigma (codes 0..3 =
+  {x < -t, -t <= x < 0, 0 <= x < t, x >= t}, the order of the decoder table
+  {-HiMag, -1, +1, +HiMag}, libraries/mark5access/mark5access/format_vdif.c:78)
+  or to 8-bit offset binary b = clip(round(x * 10) + 128, 0, 255) (decoded as
+  (b - 128)/3.3, format_vdif.c:122);
+* packed LSB-first into single-thread VDIF frames (32-byte header, all bands
+  interleaved as VDIF channels, libraries/vdifio/src/vdifio.h:42-58).
+
+The delay is applied in the frequency domain per block of ``BLOCK`` samples
+(a phase ramp exp(-2 pi i (f_LO + f) tau) on the block's spectrum), so every
+block is reproducible from the seed alone and any window of frames can be
+generated independently of any other.
+"""
+from __future__ import annotations
+
+import hashlib
+from typing import Dict, Iterable, Optional, Sequence
+
+import numpy as np
+
+from .job import DelayPoly, Job
+
+BLOCK = 1 << 14
+THRESH = 0.98
+VDIF_HEADER = 32
+
+
+def _rng(*key) -> np.random.Generator:
+    h = hashlib.blake2b(repr(key).encode(), digest_size=16).digest()
+    return np.random.default_rng(np.frombuffer(h, dtype=np.uint64))
+
+
+def make_delay_polys(job: Job, seed: int, interval_s: int = 120, max_offset_us: float = 5.0,
+                     max_rate_us_s: float = 1.0, max_quad_us_s2: float = 1e-4) -> None:
+    """Seeded quadratic delay polynomial per station: offset U(+-5 us), rate
+    U(+-1 us/s), small quadratic term.  Stored in the .im convention."""
+    r = _rng("delay", seed)
+    for st in job.stations:
+        c0 = r.uniform(-max_offset_us, max_offset_us)
+        c1 = r.uniform(-max_rate_us_s, max_rate_us_s)
+        c2 = r.uniform(-max_quad_us_s2, max_quad_us_s2)
+        st.polys = [DelayPoly(start_sec=0.0, interval_s=interval_s, coeffs=(c0, c1, c2))]
+
+
+def station_delay_us(job: Job, s: int, t_sec) -> np.ndarray:
+    """Evaluate the station's delay polynomial (us) at job-relative time t."""
+    st = job.stations[s]
+    t = np.asarray(t_sec, dtype=np.float64)
+    out = np.zeros_like(t)
+    for p in st.polys:
+        dt = t - p.start_sec
+        sel = (dt >= 0) & (dt <= p.interval_s)
+        v = np.zeros_like(t)
+        for k, c in enumerate(p.coeffs):
+            v = v + c * dt ** k
+        out = np.where(sel, v, out)
+    return out + st.clock_us
+
+
+def _band_block(job: Job, s: int, band: int, blk: int, rho: float, seed: int) -> np.ndarray:
+    """Real voltage samples of one band of one station for one BLOCK."""
+    st = job.stations[s]
+    f, pol = st.bands[band]
+    fr = job.freqs[f]
+    fs = 2.0 * fr.bw_mhz                       # Ms/s
+    sky = _rng("sky", seed, f, pol, blk).standard_normal(BLOCK)
+    spec = np.fft.rfft(sky)
+    fb = np.arange(spec.size) * (fs / BLOCK)   # baseband frequency, MHz
+    tmid = (blk + 0.5) * BLOCK / (fs * 1e6)
+    tau = float(station_delay_us(job, s, tmid))
+    if fr.sideband == "U":
+        ph = -2.0 * np.pi * (fr.freq_mhz + fb) * tau
+    else:
+        ph = 2.0 * np.pi * (fr.freq_mhz - fb) * tau
+    skyd = np.fft.irfft(spec * np.exp(1j * ph), n=BLOCK)
+    noise = _rng("noise", seed, s, band, blk).standard_normal(BLOCK)
+    return np.sqrt(rho) * skyd + np.sqrt(1.0 - rho) * noise
+
+
+def band_samples(job: Job, s: int, band: int, n0: int, n: int, rho: float, seed: int) -> np.ndarray:
+    """Voltage samples [n0, n0+n) (job-relative sample index) of one band."""
+    b0, b1 = n0 // BLOCK, (n0 + n - 1) // BLOCK
+    parts = [_band_block(job, s, band, b, rho, seed) for b in range(b0, b1 + 1)]
+    x = np.concatenate(parts)
+    off = n0 - b0 * BLOCK
+    return x[off:off + n]
+
+
+def quantise(x: np.ndarray, nbits: int) -> np.ndarray:
+    if nbits == 2:
+        t = THRESH
+        return (np.where(x < -t, 0, np.where(x < 0.0, 1, np.where(x < t, 2, 3)))).astype(np.uint8)
+    if nbits == 8:
+        return np.clip(np.rint(x * 10.0) + 128, 0, 255).astype(np.uint8)
+    raise ValueError(nbits)
+
+
+def pack_payload(codes: np.ndarray, nbits: int) -> np.ndarray:
+    """codes [nchan][nsamp] -> VDIF payload bytes, fields LSB-first in
+    (time, channel) order."""
+    nchan, nsamp = codes.shape
+    fields = codes.T.reshape(-1)               # q = t*nchan + c
+    if nbits == 8:
+        return fields.astype(np.uint8)
+    per = 8 // nbits
+    f = fields.reshape(-1, per).astype(np.uint16)
+    out = np.zeros(f.shape[0], dtype=np.uint16)
+    for i in range(per):
+        out |= f[:, i] << (nbits * i)
+    return out.astype(np.uint8)
+
+
+def vdif_header(job: Job, s: int, frame_global: int, invalid: bool = False, station_id: int = 0) -> np.ndarray:
+    st = job.stations[s]
+    fps = job.frames_per_sec(s)
+    sec = frame_global // fps
+    fnum = frame_global % fps
+    w = np.zeros(8, dtype=np.uint32)
+    w[0] = (int(sec) & 0x3FFFFFFF) | ((1 << 31) if invalid else 0)
+    w[1] = (fnum & 0xFFFFFF)
+    log2ch = int(np.log2(st.nband)) if st.nband & (st.nband - 1) == 0 else 0
+    w[2] = (1 << 29) | (log2ch << 24) | ((job.frame_bytes(s) // 8) & 0xFFFFFF)
+    w[3] = ((st.nbits - 1) << 26) | (station_id & 0xFFFF)
+    return w.view(np.uint8)
+
+
+FILL_WORD = np.frombuffer(bytes.fromhex("4433221144332211")[::-1], dtype=np.uint8)  # 0x1122334411223344 little-endian
+
+
+def gen_station_frames(job: Job, s: int, frame0: int, nframes: int, rho: float, seed: int,
+                       invalid: Iterable[int] = (), fill: Iterable[int] = ()) -> np.ndarray:
+    """nframes VDIF frames of station s starting at job-relative frame index
+    frame0.  ``invalid`` / ``fill`` list job-relative frame indices to mark
+    with the header invalid bit / to overwrite with fill pattern."""
+    st = job.stations[s]
+    fsamp = job.frame_samples(s)
+    fb = job.frame_bytes(s)
+    inv = set(invalid)
+    fil = set(fill)
+    n0 = frame0 * fsamp
+    n = nframes * fsamp
+    codes = np.stack([quantise(band_samples(job, s, b, n0, n, rho, seed), st.nbits) for b in range(st.nband)])
+    out = np.empty(nframes * fb, dtype=np.uint8)
+    for k in range(nframes):
+        g = frame0 + k
+        payload = pack_payload(codes[:, k * fsamp:(k + 1) * fsamp], st.nbits)
+        out[k * fb:k * fb + VDIF_HEADER] = vdif_header(job, s, g, invalid=g in inv, station_id=s)
+        out[k * fb + VDIF_HEADER:(k + 1) * fb] = payload
+        if g in fil:
+            out[k * fb + VDIF_HEADER:(k + 1) * fb] = np.resize(FILL_WORD, st.payload_bytes)
+    return out
+
+
+def subint_window(job: Job, s: int, sec: int, ns: int, margin_us: float = 20.0):
+    """Frame range that a DataStream would deliver for the subintegration
+    starting at (sec, ns): from the frame holding (start - margin) to the frame
+    holding (end + margin).  Returns (frame0, nframes, datasec, datans)."""
+    fps = job.frames_per_sec(s)
+    t0 = sec + ns * 1e-9 - margin_us * 1e-6
+    t1 = sec + ns * 1e-9 + job.subint_ns * 1e-9 + margin_us * 1e-6
+    f0 = int(np.floor(t0 * fps))
+    f1 = int(np.floor(t1 * fps)) + 1
+    f0 = max(f0, 0)
+    dsec = f0 // fps
+    dns = int(round((f0 % fps) * 1e9 / fps))
+    return f0, f1 - f0, dsec, dns
+
+
+def subint_inputs(job: Job, sec: int, ns: int, rho: float, seed: int,
+                  invalid: Optional[Dict[int, Sequence[int]]] = None,
+                  fill: Optional[Dict[int, Sequence[int]]] = None):
+    """Per-station (bytes, datasec, datans) for one subintegration."""
+    out = []
+    for s in range(len(job.stations)):
+        f0, nf, dsec, dns = subint_window(job, s, sec, ns)
+        buf = gen_station_frames(job, s, f0, nf, rho, seed,
+                                 invalid=(invalid or {}).get(s, ()), fill=(fill or {}).get(s, ()))
+        out.append((buf, dsec, dns))
+    return out
+
+
+def valid_flags(job: Job, all_valid: bool = True, invalid_ffts: Sequence[int] = ()) -> np.ndarray:
+    """Valid-FFT bitfield as the DataStream control block carries it: 30 flags
+    per int32 (mpifxcorr/src/mpifxcorr.h:39, FLAGS_PER_INT)."""
+    bps = job.blocks_per_send()
+    n = (bps + 29) // 30
+    v = np.zeros(n, dtype=np.int32)
+    for i in range(bps):
+        if all_valid and i not in invalid_ffts:
+            v[i // 30] |= (1 << (i % 30))
+    return v

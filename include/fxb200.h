@@ -1,0 +1,185 @@
+/*
+ * fxb200 -- B200 (sm_100a) FX correlator hot path behind a plain C ABI.
+ *
+ * The library replaces, for one correlation configuration, the per-station
+ * F stage of DiFX's mpifxcorr (Mode::process, mpifxcorr/src/mode.cpp:649-1397,
+ * with Mk5Mode::unpack, mpifxcorr/src/mk5mode.cpp:104-177 and mark5access's
+ * VDIF decoders) and the per-baseline cross-multiply-accumulate of
+ * Core::processdata (mpifxcorr/src/core.cpp:877-972, weights :998-1045),
+ * writing the reference's core-result layout
+ * (Configuration::populateResultLengths, mpifxcorr/src/configuration.cpp:
+ * 2212-2440).  All compute runs on the GPU; there is no CPU fallback.
+ *
+ * Conventions: every call returns an fxb_status and never aborts the
+ * process.  Buffers passed in are borrowed for the duration of the call
+ * unless stated otherwise.  One context belongs to one host thread at a time.
+ */
+#ifndef FXB200_H
+#define FXB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+	FXB_OK = 0,
+	FXB_ERR_ARG = 1,          /* invalid argument or job description */
+	FXB_ERR_UNSUPPORTED = 2,  /* valid DiFX job outside what this build correlates */
+	FXB_ERR_CUDA = 3,         /* CUDA runtime error (message via fxb_last_error) */
+	FXB_ERR_NOMEM = 4,        /* device memory exhausted or over budget */
+	FXB_ERR_STATE = 5,        /* call out of order (e.g. no delay model yet) */
+	FXB_ERR_TIMEOUT = 6,      /* a bounded device wait expired */
+	FXB_ERR_BUSY = 7,         /* serving: no slot free, try again */
+	FXB_ERR_DATA = 8          /* subint data rejected (e.g. outside the delay model) */
+} fxb_status;
+
+/* Arithmetic of the cross-multiply stage. */
+typedef enum {
+	FXB_XMAC_FP32 = 0,        /* CUDA-core complex FP32 MAC (the plain FP32 form) */
+	FXB_XMAC_BF16 = 1,        /* BF16 spectra, tensor-core MAC, FP32 accumulate */
+	FXB_XMAC_FP8 = 2          /* FP8 e4m3 spectra with per-(channel, station) scale */
+} fxb_xmac_kind;
+
+/* One frequency-table entry (FREQ TABLE of the .input file,
+ * configuration.cpp:1982-2052). */
+typedef struct {
+	double freq_mhz;          /* sky frequency of the band edge (LO), MHz */
+	double bw_mhz;            /* bandwidth, MHz */
+	int32_t nchan;            /* channels; the FFT length is 2*nchan */
+	int32_t lower_sideband;   /* 0 = USB, 1 = LSB */
+	int32_t chans_to_avg;     /* output channel averaging (>= 1) */
+	int32_t reserved;
+} fxb_freq;
+
+/* One datastream: a single-thread VDIF stream whose channels are the
+ * recorded bands (DATASTREAM TABLE, configuration.cpp:1433-1800). */
+typedef struct {
+	int32_t nbits;            /* 2 or 8 */
+	int32_t payload_bytes;    /* VDIF payload bytes per frame */
+	int32_t header_bytes;     /* 32 (16 = legacy) */
+	int32_t nband;            /* recorded bands = VDIF channels */
+	const int32_t *band_freq; /* [nband] frequency-table index of each band */
+	const char *band_pol;     /* [nband] 'R'/'L'/'X'/'Y' */
+} fxb_station;
+
+/* One baseline (BASELINE TABLE, configuration.cpp:1059-1120): products are
+ * listed frequency by frequency, in .input order. */
+typedef struct {
+	int32_t ds1, ds2;         /* datastream indices, ds1 < ds2 */
+	int32_t nprod;
+	const int32_t *prod_freq; /* [nprod] frequency-table index */
+	const int32_t *prod_band1;/* [nprod] band index within ds1 */
+	const int32_t *prod_band2;/* [nprod] band index within ds2 */
+} fxb_baseline;
+
+typedef struct {
+	int32_t nfreq;
+	const fxb_freq *freqs;
+	int32_t nstation;
+	const fxb_station *stations;
+	int32_t nbaseline;
+	const fxb_baseline *baselines;
+	int64_t subint_ns;        /* SUBINT NANOSECONDS; a whole number of FFTs */
+	int32_t fringe_rot_order; /* FRINGE ROTN ORDER: 0, 1 or 2 */
+	int32_t write_autocorrs;  /* WRITE AUTOCORRS (also enables cross-pol autos) */
+	int32_t xmac_kind;        /* fxb_xmac_kind */
+	int32_t max_subints_in_flight; /* device staging depth, >= 1 */
+} fxb_job_desc;
+
+typedef struct fxb_ctx fxb_ctx;
+
+/* Build a correlation context on the current CUDA device: validates the job,
+ * computes the core-result layout and allocates device state.
+ * Replaces Configuration::getMode + Mode::Mode + Core's result buffers
+ * (configuration.cpp:954-1016, mode.cpp:43-462, core.cpp:33-197). */
+fxb_ctx *fxb_create(const fxb_job_desc *desc, fxb_status *status);
+void fxb_destroy(fxb_ctx *ctx);
+
+/* Text of the last error seen by this context (or by fxb_create when ctx is
+ * NULL).  Valid until the next call on the context. */
+const char *fxb_last_error(const fxb_ctx *ctx);
+
+/* Delay model of one station, in the .im convention read by
+ * Model (model.cpp:600-856): npoly consecutive polynomials, each of order
+ * `order` (<= 5) in seconds since its own start, the first starting at
+ * poly0_sec (seconds after the job start), each valid for interval_s seconds.
+ * coeffs holds npoly*(order+1) values in microseconds.  The per-subint
+ * quadratic interpolator is derived on the device in FP64 exactly as
+ * Model::calculateDelayInterpolator does (model.cpp:229-299). */
+fxb_status fxb_set_delay_poly(fxb_ctx *ctx, int32_t station, int32_t npoly, int32_t order,
+                              double poly0_sec, int32_t interval_s, const double *coeffs);
+
+/* Correlate one subintegration (Mode::setData/setValidFlags/setOffsets then
+ * Mode::process for every FFT, then the XMAC; mode.cpp:1525-1573, 649-1397,
+ * core.cpp:705-1045) and accumulate it on the device.
+ * bufs[s]/nbytes[s]: the station's VDIF frames (host memory) whose first
+ * sample is at datasec[s] s + datans[s] ns after the job start;
+ * validflags[s]: the valid-FFT bitfield (30 flags per int32, may be NULL for
+ * all valid); (sec, ns): subint start after the job start.  Returns once the
+ * inputs have been copied; the work completes asynchronously. */
+fxb_status fxb_submit_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes,
+                             const int32_t *datasec, const int32_t *datans,
+                             const int32_t *const *validflags, int32_t sec, int32_t ns);
+
+/* As fxb_submit_subint but with the station buffers already in device
+ * memory (pointers from cudaMalloc); they must stay valid until the next
+ * fxb_sync.  validflags stay in host memory. */
+fxb_status fxb_submit_subint_device(fxb_ctx *ctx, const uint8_t *const *dev_bufs, const int64_t *nbytes,
+                                    const int32_t *datasec, const int32_t *datans,
+                                    const int32_t *const *validflags, int32_t sec, int32_t ns);
+
+/* Wait for all submitted work. */
+fxb_status fxb_sync(fxb_ctx *ctx);
+
+/* Number of complex values in the core-result buffer
+ * (Configuration::getCoreResultLength). */
+fxb_status fxb_core_result_length(const fxb_ctx *ctx, int64_t *ncomplex);
+
+/* Offsets into the core result: for f in freqs, b in baselines the baseline
+ * offset (or -1), then the same for the baseline-weight offsets, then the
+ * autocorrelation offset and the autocorrelation-weight offset of every
+ * datastream (Configuration::getCoreResult*Offset).  out holds
+ * 2*nfreq*nbaseline + 2*nstation ints. */
+fxb_status fxb_layout(const fxb_ctx *ctx, int32_t *out, size_t nint);
+
+/* Copy the accumulated core result (2*ncomplex floats) to host memory, in
+ * the reference layout: cross-correlations, baseline weights,
+ * autocorrelations, autocorrelation weights.  Synchronises. */
+fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats);
+
+/* Zero the accumulators (Core::execute after each send, core.cpp:318-322). */
+fxb_status fxb_reset(fxb_ctx *ctx);
+
+/* Device time in ms of the last subint's kernels (F stage, XMAC, total),
+ * measured with CUDA events on the context's stream. */
+fxb_status fxb_last_timing(const fxb_ctx *ctx, float *fstage_ms, float *xmac_ms, float *total_ms);
+
+/* F-stage output of the last subint for one frequency: spectra[t][c][row]
+ * complex (FP32, converted from the XMAC operand type), rows = the
+ * (station, band) inputs recording that frequency in station order.
+ * Debug/parity access; synchronises. */
+fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloats,
+                            int32_t *nfft, int32_t *nrow);
+
+/* Per-FFT station weights of the last subint: weights[s][t] (the data
+ * weight of Mode::getDataWeight).  Synchronises. */
+fxb_status fxb_read_fft_weights(fxb_ctx *ctx, float *out, size_t nfloats);
+
+/* Decode VDIF payload samples on the GPU, the call Mk5Mode::unpack makes
+ * into mark5access (mark5_unpack_with_offset,
+ * libraries/mark5access/mark5access/mark5_stream_unpacker.c:129-147, with the
+ * decoders of format_vdif.c and the blanker of blanker_mark5.c:282-313).
+ * data: nbytes of back-to-back VDIF frames (host memory); out: [nchan][nsamp]
+ * floats (host memory); *good: good-sample count as mark5access returns it. */
+fxb_status fxb_vdif_unpack(const uint8_t *data, int64_t nbytes, int32_t payload_bytes, int32_t header_bytes,
+                           int32_t nchan, int32_t nbits, int64_t offsetsamples, int32_t nsamp,
+                           float *out, int32_t *good);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FXB200_H */

@@ -1,0 +1,380 @@
+/* Harness that drives the reference correlator's own compiled CPU hot path.
+ *
+ * Test infrastructure only (oracle): it links the reference's Configuration,
+ * Model, Mode/Mk5Mode and mark5access objects built by oracle/Makefile.ref
+ * and exposes a small C interface that the tests and the CPU baseline call
+ * through ctypes.  Nothing in the product library links this file.
+ *
+ * What comes from the reference unchanged: .input/.calc/.im parsing, the
+ * result layout (Configuration::populateResultLengths), the per-station
+ * F stage (Mode::process, Mk5Mode::unpack, mark5access VDIF decoding) and the
+ * delay interpolator (Model::calculateDelayInterpolator).
+ *
+ * What this file restates, because Core cannot be constructed without an MPI
+ * job: the per-thread loop of Core::processdata (mpifxcorr/src/core.cpp:
+ * 705-730 station set-up, 796-811 F-stage batches, 877-972 XMAC,
+ * 998-1045 baseline weights) and the result merge of
+ * Core::uvshiftAndAverageBaselineFreq (core.cpp:1774-1787, no-shift,
+ * no-averaging branch), Core::averageAndSendAutocorrs (core.cpp:1266-1363)
+ * and the baseline-weight copy (core.cpp:1068-1086).  Threads split the FFT
+ * blocks of a subintegration into contiguous ranges as Core::updateconfig
+ * does (core.cpp:2090-2095); each thread owns its own Mode objects.
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <thread>
+#include <mutex>
+#include "configuration.h"
+#include "mode.h"
+#include "mk5mode.h"
+#include "model.h"
+#include "mark5access.h"
+
+namespace {
+
+struct RefJob
+{
+	Configuration *config;
+	int numds, numbl, nfreq, blockspersend, nbuffered, corelen;
+	std::vector<std::vector<Mode *> > modes;   // [thread][datastream]
+};
+
+/* Per-thread accumulators in the core-result layout (complex index space). */
+struct ThreadAcc
+{
+	std::vector<cf32> results;
+};
+
+Mode *make_mode(Configuration *c, int ds)
+{
+	Mode *m = c->getMode(0, ds);
+	if(!m || !m->initialisedOK())
+		return 0;
+	return m;
+}
+
+void ensure_threads(RefJob *j, int nthreads)
+{
+	while((int)j->modes.size() < nthreads)
+	{
+		std::vector<Mode *> ms;
+		for(int d = 0; d < j->numds; d++)
+			ms.push_back(make_mode(j->config, d));
+		j->modes.push_back(ms);
+	}
+}
+
+/* One thread's share of Core::processdata for blocks [startblock, startblock+numblocks). */
+void process_range(RefJob *j, int t, int startblock, int numblocks,
+	const unsigned char *const *bufs, const int *nbytes, const int *dscan, const int *dsec, const int *dns,
+	const int *const *validflags, int scan, int sec, int ns, ThreadAcc *acc)
+{
+	Configuration *config = j->config;
+	std::vector<Mode *> &modes = j->modes[t];
+	const int nbuf = j->nbuffered;
+	f32 *fres = (f32 *)&acc->results[0];
+
+	for(int d = 0; d < j->numds; d++)
+	{
+		modes[d]->zeroAutocorrelations();
+		modes[d]->setValidFlags((s32 *)validflags[d]);
+		modes[d]->setData((u8 *)bufs[d], nbytes[d], dscan[d], dsec[d], dns[d]);
+		modes[d]->setOffsets(scan, sec, ns);
+		modes[d]->setDumpKurtosis(false);
+	}
+
+	int numfftloops = numblocks / nbuf + ((numblocks % nbuf) ? 1 : 0);
+	for(int fftloop = 0; fftloop < numfftloops; fftloop++)
+	{
+		for(int d = 0; d < j->numds; d++)
+			for(int sub = 0; sub < nbuf; sub++)
+			{
+				int i = fftloop * nbuf + sub + startblock;
+				if(i >= startblock + numblocks)
+					break;
+				modes[d]->process(i, sub);
+			}
+
+		/* XMAC (core.cpp:877-972): accumulate directly in core-result order;
+		 * each element receives the same sequence of products as the
+		 * reference's per-stride thread buffer. */
+		for(int f = 0; f < j->nfreq; f++)
+		{
+			if(!config->isFrequencyUsed(0, f))
+				continue;
+			int nchan = config->getFNumChannels(f);
+			for(int b = 0; b < j->numbl; b++)
+			{
+				int lf = config->getBLocalFreqIndex(0, b, f);
+				if(lf < 0)
+					continue;
+				const Mode *m1 = modes[config->getBOrderedDataStream1Index(0, b)];
+				const Mode *m2 = modes[config->getBOrderedDataStream2Index(0, b)];
+				int base = config->getCoreResultBaselineOffset(0, f, b);
+				for(int sub = 0; sub < nbuf; sub++)
+				{
+					int i = fftloop * nbuf + sub + startblock;
+					if(i >= startblock + numblocks)
+						break;
+					for(int p = 0; p < config->getBNumPolProducts(0, b, lf); p++)
+					{
+						const cf32 *v1 = m1->getFreqs(config->getBDataStream1BandIndex(0, b, lf, p), sub);
+						const cf32 *v2 = m2->getConjugatedFreqs(config->getBDataStream2BandIndex(0, b, lf, p), sub);
+						cf32 *a = &acc->results[base + p * nchan];
+						for(int l = 0; l < nchan; l++)
+						{
+							a[l].re += v1[l].re * v2[l].re - v1[l].im * v2[l].im;
+							a[l].im += v1[l].re * v2[l].im + v1[l].im * v2[l].re;
+						}
+					}
+				}
+			}
+		}
+
+		/* baseline weights (core.cpp:998-1045) */
+		for(int sub = 0; sub < nbuf; sub++)
+		{
+			int i = fftloop * nbuf + sub + startblock;
+			if(i >= startblock + numblocks)
+				break;
+			for(int f = 0; f < j->nfreq; f++)
+			{
+				if(!config->isFrequencyUsed(0, f))
+					continue;
+				for(int b = 0; b < j->numbl; b++)
+				{
+					int lf = config->getBLocalFreqIndex(0, b, f);
+					if(lf < 0)
+						continue;
+					const Mode *m1 = modes[config->getBOrderedDataStream1Index(0, b)];
+					const Mode *m2 = modes[config->getBOrderedDataStream2Index(0, b)];
+					int widx = config->getCoreResultBWeightOffset(0, f, b) * 2;
+					for(int p = 0; p < config->getBNumPolProducts(0, b, lf); p++)
+					{
+						int r1 = config->getBDataStream1RecordBandIndex(0, b, lf, p);
+						int r2 = config->getBDataStream2RecordBandIndex(0, b, lf, p);
+						if(r1 < 0 || r2 < 0)
+							continue;
+						fres[widx + p] += m1->getDataWeight(r1, sub) * m2->getDataWeight(r2, sub);
+					}
+				}
+			}
+		}
+	}
+
+	/* autocorrelations and their weights (core.cpp:1266-1363) */
+	bool writecross = modes[0]->writeCrossAutoCorrs() && config->getMaxProducts() > 2;
+	for(int d = 0; d < j->numds; d++)
+	{
+		modes[d]->averageFrequency();
+		int ridx = config->getCoreResultAutocorrOffset(0, d);
+		for(int pass = 0; pass < (writecross ? 2 : 1); pass++)
+			for(int k = 0; k < config->getDNumTotalBands(0, d); k++)
+			{
+				int fi = config->getDTotalFreqIndex(0, d, k);
+				if(!(config->isFrequencyUsed(0, fi) || config->isEquivalentFrequencyUsed(0, fi)))
+					continue;
+				int fc = config->getFNumChannels(fi) / config->getFChannelsToAverage(fi);
+				const cf32 *ac = modes[d]->getAutocorrelation(pass == 1, k);
+				for(int l = 0; l < fc; l++)
+				{
+					acc->results[ridx + l].re += ac[l].re;
+					acc->results[ridx + l].im += ac[l].im;
+				}
+				ridx += fc;
+			}
+		int widx = config->getCoreResultACWeightOffset(0, d) * 2;
+		int nrec = config->getDNumRecordedBands(0, d);
+		for(int pass = 0; pass < (writecross ? 2 : 1); pass++)
+			for(int k = 0; k < config->getDNumTotalBands(0, d); k++)
+			{
+				int fi = config->getDTotalFreqIndex(0, d, k);
+				if(!(config->isFrequencyUsed(0, fi) || config->isEquivalentFrequencyUsed(0, fi)))
+					continue;
+				if(k < nrec)
+					fres[widx] += modes[d]->getWeight(false, k);
+				widx++;
+			}
+	}
+}
+
+} // namespace
+
+extern "C" {
+
+/* Parse a .input file (with its .calc/.im) and build Mode objects for
+ * nthreads threads.  Returns 0 when the reference rejects the job. */
+void *dref_open(const char *inputfile, int nthreads)
+{
+	Configuration *c = new Configuration(inputfile, 0, 0.0);
+	if(!c->consistencyOK())
+	{
+		delete c;
+		return 0;
+	}
+	RefJob *j = new RefJob;
+	j->config = c;
+	j->numds = c->getNumDataStreams();
+	j->numbl = c->getNumBaselines();
+	j->nfreq = c->getFreqTableLength();
+	j->blockspersend = c->getBlocksPerSend(0);
+	j->nbuffered = c->getNumBufferedFFTs(0);
+	j->corelen = c->getCoreResultLength(0);
+	ensure_threads(j, nthreads < 1 ? 1 : nthreads);
+	for(size_t t = 0; t < j->modes.size(); t++)
+		for(int d = 0; d < j->numds; d++)
+			if(!j->modes[t][d])
+			{
+				delete c;
+				delete j;
+				return 0;
+			}
+	return j;
+}
+
+void dref_close(void *h)
+{
+	RefJob *j = (RefJob *)h;
+	if(!j) return;
+	for(size_t t = 0; t < j->modes.size(); t++)
+		for(size_t d = 0; d < j->modes[t].size(); d++)
+			delete j->modes[t][d];
+	delete j->config;
+	delete j;
+}
+
+/* info[0..5] = coreresultlength (complex), blockspersend, numdatastreams,
+ * numbaselines, numbufferedffts, maxproducts */
+void dref_info(void *h, int *info)
+{
+	RefJob *j = (RefJob *)h;
+	info[0] = j->corelen;
+	info[1] = j->blockspersend;
+	info[2] = j->numds;
+	info[3] = j->numbl;
+	info[4] = j->nbuffered;
+	info[5] = j->config->getMaxProducts();
+}
+
+/* Core-result offsets for layout parity: out[f*numbl + b] = baseline offset
+ * (or -1), then bweight offsets likewise, then per-datastream autocorr and
+ * acweight offsets.  out must hold 2*nfreq*numbl + 2*numds ints. */
+void dref_layout(void *h, int *out)
+{
+	RefJob *j = (RefJob *)h;
+	Configuration *c = j->config;
+	int k = 0;
+	for(int pass = 0; pass < 2; pass++)
+		for(int f = 0; f < j->nfreq; f++)
+			for(int b = 0; b < j->numbl; b++)
+			{
+				if(!c->isFrequencyUsed(0, f) || c->getBLocalFreqIndex(0, b, f) < 0)
+					out[k++] = -1;
+				else
+					out[k++] = pass == 0 ? c->getCoreResultBaselineOffset(0, f, b) : c->getCoreResultBWeightOffset(0, f, b);
+			}
+	for(int d = 0; d < j->numds; d++)
+		out[k++] = c->getCoreResultAutocorrOffset(0, d);
+	for(int d = 0; d < j->numds; d++)
+		out[k++] = c->getCoreResultACWeightOffset(0, d);
+}
+
+/* Correlate one subintegration and ADD it into coreresult (2*corelen floats).
+ * bufs/nbytes/dscan/dsec/dns/validflags are per datastream, as the
+ * DataStream control block would deliver them. */
+int dref_process_subint(void *h, int nthreads,
+	const unsigned char *const *bufs, const int *nbytes, const int *dscan, const int *dsec, const int *dns,
+	const int *const *validflags, int scan, int sec, int ns, float *coreresult)
+{
+	RefJob *j = (RefJob *)h;
+	if(nthreads < 1) nthreads = 1;
+	ensure_threads(j, nthreads);
+	std::vector<ThreadAcc> accs(nthreads);
+	std::vector<std::thread> th;
+	int bps = j->blockspersend;
+	for(int t = 0; t < nthreads; t++)
+	{
+		/* contiguous split as Core::updateconfig (core.cpp:2090-2095) */
+		int start = t * (bps / nthreads) + (t < bps % nthreads ? t : bps % nthreads);
+		int num = bps / nthreads + (t < bps % nthreads ? 1 : 0);
+		accs[t].results.assign(j->corelen, cf32{0.0f, 0.0f});
+		if(nthreads == 1)
+			process_range(j, 0, start, num, bufs, nbytes, dscan, dsec, dns, validflags, scan, sec, ns, &accs[0]);
+		else
+			th.emplace_back(process_range, j, t, start, num, bufs, nbytes, dscan, dsec, dns, validflags, scan, sec, ns, &accs[t]);
+	}
+	for(auto &x : th)
+		x.join();
+	for(int t = 0; t < nthreads; t++)
+	{
+		const float *src = (const float *)&accs[t].results[0];
+		for(int i = 0; i < 2 * j->corelen; i++)
+			coreresult[i] += src[i];
+	}
+	return 0;
+}
+
+/* Run Mode::process for one FFT of one datastream and return what the XMAC
+ * would read: spectra[band][nchan] complex (all recorded bands), the data
+ * weight, and the Mode's running autocorrelations after this FFT. */
+int dref_mode_fft(void *h, int ds, const unsigned char *buf, int nbytes, int dscan, int dsec, int dns,
+	const int *validflags, int scan, int sec, int ns, int fftindex, float *spectra, float *weight, float *autocorr)
+{
+	RefJob *j = (RefJob *)h;
+	Configuration *c = j->config;
+	Mode *m = j->modes[0][ds];
+	m->zeroAutocorrelations();
+	m->setValidFlags((s32 *)validflags);
+	m->setData((u8 *)buf, nbytes, dscan, dsec, dns);
+	m->setOffsets(scan, sec, ns);
+	m->process(fftindex, 0);
+	int nb = c->getDNumRecordedBands(0, ds);
+	int nchan = c->getFNumChannels(c->getDTotalFreqIndex(0, ds, 0));
+	for(int b = 0; b < nb; b++)
+	{
+		memcpy(spectra + (size_t)2 * b * nchan, m->getFreqs(b, 0), sizeof(float) * 2 * nchan);
+		if(autocorr)
+			memcpy(autocorr + (size_t)2 * b * nchan, m->getAutocorrelation(false, b), sizeof(float) * 2 * nchan);
+	}
+	*weight = m->getDataWeight(0, 0);
+	return nb;
+}
+
+/* Delay interpolator exactly as Mode::setOffsets obtains it (mode.cpp:1541-1549). */
+int dref_interpolator(void *h, int ds, int scan, int sec, int ns, double *coeffs)
+{
+	RefJob *j = (RefJob *)h;
+	Configuration *c = j->config;
+	Model *model = c->getModel();
+	int nchan = c->getFNumChannels(c->getDTotalFreqIndex(0, ds, 0));
+	double bw = c->getDRecordedBandwidth(0, ds, 0);
+	double sampletime = 1.0 / (2.0 * bw);
+	double timespan = j->blockspersend * 2 * nchan * sampletime / 1e6;
+	int srcindex = model->getNumPhaseCentres(scan) == 1 ? 1 : 0;
+	bool ok = model->calculateDelayInterpolator(scan, (double)sec + ns / 1e9, timespan, j->blockspersend,
+		c->getDModelFileIndex(0, ds), srcindex, 2, coeffs);
+	int intclockseconds = int(floor(c->getDClockCoeff(0, ds, 0) / 1000000.0 + 0.5));
+	coeffs[2] -= 1000000 * intclockseconds;
+	return ok ? 0 : -1;
+}
+
+/* Direct mark5access decode of nsamp samples per channel starting at
+ * offsetsamples, the call Mk5Mode::unpack makes (mk5mode.cpp:119).  out is
+ * [nchan][nsamp].  Returns mark5access's good-sample count. */
+int dref_unpack(const char *formatname, const unsigned char *data, int offsetsamples, int nsamp, float *out)
+{
+	struct mark5_stream *ms = new_mark5_stream(new_mark5_stream_unpacker(0), new_mark5_format_generic_from_string(formatname));
+	if(!ms)
+		return -1000000;
+	std::vector<float *> ptrs(ms->nchan);
+	for(int c = 0; c < ms->nchan; c++)
+		ptrs[c] = out + (size_t)c * nsamp;
+	int good = mark5_unpack_with_offset(ms, data, offsetsamples, &ptrs[0], nsamp);
+	delete_mark5_stream(ms);
+	return good;
+}
+
+} // extern "C"

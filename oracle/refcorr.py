@@ -1,0 +1,129 @@
+"""ctypes access to the reference correlator's own CPU hot path, compiled from
+the reference sources into oracle/_ref/libdifxref.so by oracle/Makefile.ref
+(harness: oracle/ref_harness.cpp).
+
+Oracle test infrastructure: used to pin the C restatement (oracle/fxoracle.c),
+to generate golden fixtures, and as the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libdifxref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, fp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
+        L.dref_open.restype = vp
+        L.dref_open.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        L.dref_close.argtypes = [vp]
+        L.dref_info.argtypes = [vp, ip]
+        L.dref_layout.argtypes = [vp, ip]
+        L.dref_process_subint.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ip, ip, ip, ip,
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, ctypes.c_int, fp]
+        L.dref_mode_fft.argtypes = [vp, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp, fp, fp]
+        L.dref_interpolator.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+        L.dref_unpack.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp]
+        _lib = L
+    return _lib
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _iarr(v: Sequence[int]):
+    return (ctypes.c_int * len(v))(*v)
+
+
+class RefCorrelator:
+    """The reference Configuration + Mode objects for one job (config 0)."""
+
+    def __init__(self, job, nthreads: int = 1, workdir: Optional[str] = None):
+        from difxinput import write_job_files
+        self._tmp = None
+        if workdir is None:
+            self._tmp = tempfile.TemporaryDirectory(prefix="fxref_")
+            workdir = self._tmp.name
+        self.job = job
+        self.input_path = write_job_files(job, workdir)
+        self.h = lib().dref_open(self.input_path.encode(), nthreads)
+        if not self.h:
+            raise RuntimeError("reference rejected the job (set ORACLE_REF_VERBOSE=1 for its alerts)")
+        info = (ctypes.c_int * 6)()
+        lib().dref_info(self.h, info)
+        self.corelen, self.blockspersend, self.numds, self.numbl, self.nbuffered, self.maxproducts = list(info)
+
+    def close(self):
+        if self.h:
+            lib().dref_close(self.h)
+            self.h = None
+        if self._tmp is not None:
+            self._tmp.cleanup()
+            self._tmp = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def layout(self) -> np.ndarray:
+        nf = len(self.job.freqs)
+        n = 2 * nf * self.numbl + 2 * self.numds
+        out = np.zeros(n, dtype=np.int32)
+        lib().dref_layout(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        return out
+
+    def process_subint(self, inputs: List[Tuple[np.ndarray, int, int]], validflags: List[np.ndarray],
+                       scan: int, sec: int, ns: int, coreresult: Optional[np.ndarray] = None,
+                       nthreads: int = 1) -> np.ndarray:
+        if coreresult is None:
+            coreresult = np.zeros(2 * self.corelen, dtype=np.float32)
+        n = len(inputs)
+        bufs = (ctypes.c_void_p * n)(*[b.ctypes.data for b, _, _ in inputs])
+        vflags = (ctypes.c_void_p * n)(*[v.ctypes.data for v in validflags])
+        lib().dref_process_subint(self.h, nthreads, bufs, _iarr([b.size for b, _, _ in inputs]),
+                                  _iarr([0] * n), _iarr([s for _, s, _ in inputs]), _iarr([x for _, _, x in inputs]),
+                                  vflags, scan, sec, ns, _fptr(coreresult))
+        return coreresult
+
+    def mode_fft(self, ds: int, buf: np.ndarray, dsec: int, dns: int, validflags: np.ndarray,
+                 sec: int, ns: int, fftindex: int):
+        st = self.job.stations[ds]
+        nchan = self.job.station_nchan(ds)
+        spec = np.zeros((st.nband, nchan, 2), dtype=np.float32)
+        ac = np.zeros((st.nband, nchan, 2), dtype=np.float32)
+        w = np.zeros(1, dtype=np.float32)
+        lib().dref_mode_fft(self.h, ds, buf.ctypes.data, buf.size, 0, dsec, dns, validflags.ctypes.data,
+                            0, sec, ns, fftindex, _fptr(spec), _fptr(w), _fptr(ac))
+        return spec[..., 0] + 1j * spec[..., 1], float(w[0]), ac[..., 0] + 1j * ac[..., 1]
+
+    def interpolator(self, ds: int, sec: int, ns: int) -> np.ndarray:
+        c = (ctypes.c_double * 3)()
+        rc = lib().dref_interpolator(self.h, ds, 0, sec, ns, c)
+        if rc != 0:
+            raise RuntimeError("no delay model for that time")
+        return np.array(list(c))
+
+
+def unpack(formatname: str, data: np.ndarray, offsetsamples: int, nsamp: int, nchan: int):
+    out = np.zeros((nchan, nsamp), dtype=np.float32)
+    good = lib().dref_unpack(formatname.encode(), data.ctypes.data, offsetsamples, nsamp, _fptr(out))
+    return out, good

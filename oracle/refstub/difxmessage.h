@@ -1,0 +1,22 @@
+/* Stand-in for the difxmessage UDP status library: alert levels and the one
+ * send call that the reference's Alert streams make. The oracle build routes
+ * alerts to stderr (level <= ERROR) or drops them. */
+#ifndef ORACLE_REFSTUB_DIFXMESSAGE_H
+#define ORACLE_REFSTUB_DIFXMESSAGE_H
+#define DIFX_ALERT_LEVEL_FATAL 0
+#define DIFX_ALERT_LEVEL_SEVERE 1
+#define DIFX_ALERT_LEVEL_ERROR 2
+#define DIFX_ALERT_LEVEL_WARNING 3
+#define DIFX_ALERT_LEVEL_INFO 4
+#define DIFX_ALERT_LEVEL_VERBOSE 5
+#define DIFX_ALERT_LEVEL_DEBUG 6
+#define DIFX_ALERT_LEVEL_DO_NOT_SEND 7
+#define DIFX_MESSAGE_PARAM_LENGTH 32
+#ifdef __cplusplus
+extern "C" {
+#endif
+int difxMessageSendDifxAlert(const char *alertMessage, int severity);
+#ifdef __cplusplus
+}
+#endif
+#endif
