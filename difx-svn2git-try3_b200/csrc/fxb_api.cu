@@ -1,0 +1,636 @@
+// C ABI of the FX path (include/fxb200.h): context life cycle, device memory,
+// the per-subint launch sequence and result readout.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fxb_internal.h"
+#include "fxb_kernels.h"
+
+namespace fxb {
+void upload_lut8(cudaStream_t stream);
+}
+
+using namespace fxb;
+
+struct Slot {
+	std::vector<uint8_t *> raw;        // device staging per station
+	std::vector<int64_t> rawcap;
+	DevSubintStation *d_sub = nullptr;
+	int32_t *d_vflags = nullptr;
+	DevSubintStation *h_sub = nullptr; // pinned
+	int32_t *h_vflags = nullptr;       // pinned
+	cudaEvent_t copied = nullptr, done = nullptr;
+	bool used = false;
+};
+
+struct fxb_ctx {
+	Job job;
+	std::string err;
+	int device = 0;
+	cudaStream_t stream = nullptr, copy_stream = nullptr;
+	int S = 0, T = 0, F = 0, nflagint = 0, maxband = 0, maxN = 0, maxfft = 0;
+	DevStation *d_st = nullptr;
+	std::vector<DevStation> h_st;
+	DevBand *d_bands = nullptr;
+	DevFreqPlan *d_plans = nullptr;
+	std::vector<DevFreqPlan> h_plans;
+	std::vector<void *> owned;          // misc device allocations
+	float2 *d_twiddle = nullptr;
+	FftParam *d_params = nullptr;
+	float2 *d_spec = nullptr;
+	float2 *d_acc = nullptr;
+	float *d_bwacc = nullptr, *d_acwacc = nullptr;
+	DevBWeight *d_bw = nullptr;
+	DevACWeight *d_acw = nullptr;
+	DevOutMap *d_om = nullptr;
+	int nbw = 0, nacw = 0, nom = 0;
+	float2 *d_core = nullptr;
+	uint8_t *d_valid = nullptr;
+	int64_t valid_stride = 0;
+	std::vector<Slot> slots;
+	int next_slot = 0;
+	cudaEvent_t ev_f0 = nullptr, ev_f1 = nullptr, ev_x1 = nullptr;
+	bool timed = false;
+	std::vector<bool> delay_set;
+};
+
+static std::mutex g_err_mutex;
+static std::string g_create_err;
+
+static fxb_status cuda_fail(fxb_ctx *ctx, cudaError_t e, const char *what)
+{
+	char buf[512];
+	snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+	if(ctx)
+		ctx->err = buf;
+	else
+	{
+		std::lock_guard<std::mutex> lk(g_err_mutex);
+		g_create_err = buf;
+	}
+	return e == cudaErrorMemoryAllocation ? FXB_ERR_NOMEM : FXB_ERR_CUDA;
+}
+
+#define CK(ctx, call)                                  \
+	do {                                               \
+		cudaError_t e_ = (call);                       \
+		if(e_ != cudaSuccess)                          \
+			return cuda_fail((ctx), e_, #call);        \
+	} while(0)
+
+template <typename T>
+static cudaError_t dalloc(fxb_ctx *ctx, T **p, size_t n)
+{
+	void *v = nullptr;
+	cudaError_t e = cudaMalloc(&v, std::max<size_t>(n, 1) * sizeof(T));
+	if(e == cudaSuccess)
+	{
+		ctx->owned.push_back(v);
+		*p = (T *)v;
+	}
+	return e;
+}
+
+static void free_ctx(fxb_ctx *ctx)
+{
+	if(!ctx)
+		return;
+	if(ctx->stream)
+		cudaStreamSynchronize(ctx->stream);
+	if(ctx->copy_stream)
+		cudaStreamSynchronize(ctx->copy_stream);
+	for(void *p : ctx->owned)
+		cudaFree(p);
+	if(ctx->d_valid)
+		cudaFree(ctx->d_valid);
+	for(auto &s : ctx->slots)
+	{
+		for(auto *p : s.raw)
+			if(p) cudaFree(p);
+		if(s.h_sub) cudaFreeHost(s.h_sub);
+		if(s.h_vflags) cudaFreeHost(s.h_vflags);
+		if(s.copied) cudaEventDestroy(s.copied);
+		if(s.done) cudaEventDestroy(s.done);
+	}
+	if(ctx->ev_f0) cudaEventDestroy(ctx->ev_f0);
+	if(ctx->ev_f1) cudaEventDestroy(ctx->ev_f1);
+	if(ctx->ev_x1) cudaEventDestroy(ctx->ev_x1);
+	if(ctx->stream) cudaStreamDestroy(ctx->stream);
+	if(ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+	delete ctx;
+}
+
+static fxb_status setup_device(fxb_ctx *ctx)
+{
+	Job &job = ctx->job;
+	CK(ctx, cudaGetDevice(&ctx->device));
+	CK(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+	CK(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+	CK(ctx, cudaEventCreate(&ctx->ev_f0));
+	CK(ctx, cudaEventCreate(&ctx->ev_f1));
+	CK(ctx, cudaEventCreate(&ctx->ev_x1));
+	ctx->S = (int)job.stations.size();
+	ctx->T = job.blockspersend;
+	ctx->F = (int)job.freqs.size();
+	ctx->nflagint = ctx->T / kFlagsPerInt + 1;
+	ctx->delay_set.assign(ctx->S, false);
+
+	// stations
+	ctx->h_st.resize(ctx->S);
+	ctx->maxband = 0;
+	ctx->maxN = 0;
+	for(int s = 0; s < ctx->S; s++)
+	{
+		const Job::Station &js = job.stations[s];
+		DevStation &d = ctx->h_st[s];
+		memset(&d, 0, sizeof(d));
+		const fxb_freq &f = job.freqs[js.band_freq[0]];
+		d.nbits = js.nbits;
+		d.payload = js.payload;
+		d.header = js.header;
+		d.nband = js.nband;
+		d.framebytes = js.payload + js.header;
+		d.framesamples = js.payload * 8 / (js.nbits * js.nband);
+		d.gran = 8 / (js.nband * js.nbits);
+		if(d.gran <= 0) d.gran = 1;
+		d.nchan = f.nchan;
+		d.fftchannels = 2 * f.nchan;
+		d.asl = calcstridelength((unsigned)f.nchan);
+		d.sticky = (js.nbits == 8 && (js.nband == 2 || js.nband == 4)) ? 1 : 0;
+		d.bpbn = (js.nband * 1 * js.nbits) / 8;
+		d.bpbd = 1;
+		if(d.bpbn == 0)
+		{
+			d.bpbn = 1;
+			d.bpbd = 8 / (js.nband * js.nbits);
+		}
+		d.bw = f.bw_mhz;
+		d.sampletime = 1.0 / (2.0 * f.bw_mhz);
+		ctx->maxband = std::max(ctx->maxband, js.nband);
+		ctx->maxN = std::max(ctx->maxN, d.fftchannels);
+	}
+	ctx->maxfft = ctx->maxN;
+	CK(ctx, dalloc(ctx, &ctx->d_st, ctx->S));
+	CK(ctx, cudaMemcpy(ctx->d_st, ctx->h_st.data(), sizeof(DevStation) * ctx->S, cudaMemcpyHostToDevice));
+
+	// bands
+	std::vector<DevBand> hb((size_t)ctx->S * ctx->maxband);
+	for(int s = 0; s < ctx->S; s++)
+		for(int b = 0; b < ctx->maxband; b++)
+		{
+			DevBand &d = hb[(size_t)s * ctx->maxband + b];
+			memset(&d, 0, sizeof(d));
+			d.row = -1;
+			if(b >= job.stations[s].nband) continue;
+			int f = job.stations[s].band_freq[b];
+			d.freq = f;
+			d.row = job.band_row[s][b];
+			d.lsb = job.freqs[f].lower_sideband;
+			d.lofreq = job.freqs[f].freq_mhz;
+		}
+	CK(ctx, dalloc(ctx, &ctx->d_bands, hb.size()));
+	CK(ctx, cudaMemcpy(ctx->d_bands, hb.data(), sizeof(DevBand) * hb.size(), cudaMemcpyHostToDevice));
+
+	// twiddles exp(-2 pi i k / maxN), computed in double
+	{
+		std::vector<float2> tw(ctx->maxN / 2);
+		for(int k = 0; k < ctx->maxN / 2; k++)
+		{
+			double ang = -2.0 * M_PI * (double)k / (double)ctx->maxN;
+			tw[k] = make_float2((float)cos(ang), (float)sin(ang));
+		}
+		CK(ctx, dalloc(ctx, &ctx->d_twiddle, tw.size()));
+		CK(ctx, cudaMemcpy(ctx->d_twiddle, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
+	}
+
+	// per-frequency plans
+	ctx->h_plans.assign(ctx->F, DevFreqPlan{});
+	for(int f = 0; f < ctx->F; f++)
+	{
+		const Job::FreqPlan &p = job.plan[f];
+		DevFreqPlan &d = ctx->h_plans[f];
+		memset(&d, 0, sizeof(d));
+		d.nrow = p.nrow;
+		d.nchan = p.nchan;
+		if(p.nrow == 0) continue;
+		d.ntr = (p.nrow + kTile - 1) / kTile;
+		d.npair = d.ntr * (d.ntr + 1) / 2;
+		d.spec_off = p.spec_off;
+		d.acc_off = p.acc_off;
+		int32_t *dA, *dB;
+		int16_t *pairs;
+		CK(ctx, dalloc(ctx, &dA, p.destA.size()));
+		CK(ctx, dalloc(ctx, &dB, p.destB.size()));
+		CK(ctx, cudaMemcpy(dA, p.destA.data(), sizeof(int32_t) * p.destA.size(), cudaMemcpyHostToDevice));
+		CK(ctx, cudaMemcpy(dB, p.destB.data(), sizeof(int32_t) * p.destB.size(), cudaMemcpyHostToDevice));
+		std::vector<int16_t> hp;
+		for(int i = 0; i < d.ntr; i++)
+			for(int j = i; j < d.ntr; j++)
+			{
+				hp.push_back((int16_t)i);
+				hp.push_back((int16_t)j);
+			}
+		CK(ctx, dalloc(ctx, &pairs, hp.size()));
+		CK(ctx, cudaMemcpy(pairs, hp.data(), sizeof(int16_t) * hp.size(), cudaMemcpyHostToDevice));
+		d.destA = dA;
+		d.destB = dB;
+		d.pairs = pairs;
+	}
+	CK(ctx, dalloc(ctx, &ctx->d_plans, ctx->F));
+	CK(ctx, cudaMemcpy(ctx->d_plans, ctx->h_plans.data(), sizeof(DevFreqPlan) * ctx->F, cudaMemcpyHostToDevice));
+
+	// big buffers
+	CK(ctx, dalloc(ctx, &ctx->d_params, (size_t)ctx->S * ctx->T));
+	CK(ctx, dalloc(ctx, &ctx->d_spec, (size_t)job.spec_total));
+	CK(ctx, dalloc(ctx, &ctx->d_acc, (size_t)job.acc_total));
+	CK(ctx, dalloc(ctx, &ctx->d_core, (size_t)job.corelen));
+	ctx->nbw = (int)job.bweights.size();
+	ctx->nacw = (int)job.acweights.size();
+	ctx->nom = (int)job.outmap.size();
+	CK(ctx, dalloc(ctx, &ctx->d_bwacc, ctx->nbw));
+	CK(ctx, dalloc(ctx, &ctx->d_acwacc, ctx->nacw));
+	{
+		std::vector<DevBWeight> hbw(ctx->nbw);
+		for(int i = 0; i < ctx->nbw; i++)
+			hbw[i] = DevBWeight{job.bweights[i].s1, job.bweights[i].s2, job.bweights[i].dst_float};
+		std::vector<DevACWeight> hacw(ctx->nacw);
+		for(int i = 0; i < ctx->nacw; i++)
+			hacw[i] = DevACWeight{job.acweights[i].s, 0, job.acweights[i].dst_float};
+		std::vector<DevOutMap> hom(ctx->nom);
+		for(int i = 0; i < ctx->nom; i++)
+			hom[i] = DevOutMap{job.outmap[i].acc, job.outmap[i].core, job.outmap[i].nchan, job.outmap[i].avg};
+		CK(ctx, dalloc(ctx, &ctx->d_bw, ctx->nbw));
+		CK(ctx, dalloc(ctx, &ctx->d_acw, ctx->nacw));
+		CK(ctx, dalloc(ctx, &ctx->d_om, ctx->nom));
+		if(ctx->nbw) CK(ctx, cudaMemcpy(ctx->d_bw, hbw.data(), sizeof(DevBWeight) * ctx->nbw, cudaMemcpyHostToDevice));
+		if(ctx->nacw) CK(ctx, cudaMemcpy(ctx->d_acw, hacw.data(), sizeof(DevACWeight) * ctx->nacw, cudaMemcpyHostToDevice));
+		if(ctx->nom) CK(ctx, cudaMemcpy(ctx->d_om, hom.data(), sizeof(DevOutMap) * ctx->nom, cudaMemcpyHostToDevice));
+	}
+
+	// staging slots
+	ctx->slots.resize(job.inflight);
+	for(auto &sl : ctx->slots)
+	{
+		sl.raw.assign(ctx->S, nullptr);
+		sl.rawcap.assign(ctx->S, 0);
+		CK(ctx, dalloc(ctx, &sl.d_sub, ctx->S));
+		CK(ctx, dalloc(ctx, &sl.d_vflags, (size_t)ctx->S * ctx->nflagint));
+		CK(ctx, cudaMallocHost(&sl.h_sub, sizeof(DevSubintStation) * ctx->S));
+		CK(ctx, cudaMallocHost(&sl.h_vflags, sizeof(int32_t) * ctx->S * ctx->nflagint));
+		CK(ctx, cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));
+		CK(ctx, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+	}
+	upload_lut8(ctx->stream);
+	CK(ctx, cudaMemsetAsync(ctx->d_acc, 0, sizeof(float2) * std::max<int64_t>(job.acc_total, 1), ctx->stream));
+	CK(ctx, cudaMemsetAsync(ctx->d_bwacc, 0, sizeof(float) * std::max(ctx->nbw, 1), ctx->stream));
+	CK(ctx, cudaMemsetAsync(ctx->d_acwacc, 0, sizeof(float) * std::max(ctx->nacw, 1), ctx->stream));
+	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	return FXB_OK;
+}
+
+extern "C" {
+
+fxb_ctx *fxb_create(const fxb_job_desc *desc, fxb_status *status)
+{
+	fxb_ctx *ctx = new fxb_ctx;
+	fxb_status st = FXB_OK;
+	std::string err;
+	if(!build_job(desc, ctx->job, err, st))
+	{
+		{
+			std::lock_guard<std::mutex> lk(g_err_mutex);
+			g_create_err = err;
+		}
+		delete ctx;
+		if(status) *status = st;
+		return nullptr;
+	}
+	st = setup_device(ctx);
+	if(st != FXB_OK)
+	{
+		{
+			std::lock_guard<std::mutex> lk(g_err_mutex);
+			g_create_err = ctx->err;
+		}
+		free_ctx(ctx);
+		if(status) *status = st;
+		return nullptr;
+	}
+	if(status) *status = FXB_OK;
+	return ctx;
+}
+
+void fxb_destroy(fxb_ctx *ctx) { free_ctx(ctx); }
+
+const char *fxb_last_error(const fxb_ctx *ctx)
+{
+	if(ctx)
+		return ctx->err.c_str();
+	std::lock_guard<std::mutex> lk(g_err_mutex);
+	return g_create_err.c_str();
+}
+
+fxb_status fxb_set_delay_poly(fxb_ctx *ctx, int32_t station, int32_t npoly, int32_t order, double poly0_sec,
+                              int32_t interval_s, const double *coeffs)
+{
+	if(!ctx) return FXB_ERR_ARG;
+	if(station < 0 || station >= ctx->S || npoly < 1 || npoly > kMaxPolys || order < 0 || order > kMaxPolyOrder ||
+	   interval_s <= 0 || !coeffs)
+	{
+		ctx->err = "bad delay polynomial";
+		return FXB_ERR_ARG;
+	}
+	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	DevStation &d = ctx->h_st[station];
+	d.npoly = npoly;
+	d.order = order;
+	d.interval = interval_s;
+	d.poly0 = poly0_sec;
+	memset(d.coeffs, 0, sizeof(d.coeffs));
+	memcpy(d.coeffs, coeffs, sizeof(double) * npoly * (order + 1));
+	CK(ctx, cudaMemcpy(ctx->d_st + station, &d, sizeof(DevStation), cudaMemcpyHostToDevice));
+	ctx->delay_set[station] = true;
+	return FXB_OK;
+}
+
+static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes, const int32_t *datasec,
+                         const int32_t *datans, const int32_t *const *validflags, int32_t sec, int32_t ns, bool device)
+{
+	if(!ctx || !bufs || !nbytes || !datasec || !datans)
+		return FXB_ERR_ARG;
+	for(int s = 0; s < ctx->S; s++)
+		if(!ctx->delay_set[s])
+		{
+			ctx->err = "delay model not set for every station";
+			return FXB_ERR_STATE;
+		}
+	const Job &job = ctx->job;
+	Slot &sl = ctx->slots[ctx->next_slot];
+	ctx->next_slot = (ctx->next_slot + 1) % (int)ctx->slots.size();
+	if(sl.used)
+		CK(ctx, cudaEventSynchronize(sl.done));
+	sl.used = true;
+
+	// frame-validity array sized for the largest buffer of this subint
+	int64_t need = 0;
+	for(int s = 0; s < ctx->S; s++)
+	{
+		if(nbytes[s] < 0 || (nbytes[s] > 0 && !bufs[s]))
+		{
+			ctx->err = "bad station buffer";
+			return FXB_ERR_ARG;
+		}
+		need = std::max<int64_t>(need, nbytes[s] / ctx->h_st[s].payload + 2);
+	}
+	if(need > ctx->valid_stride)
+	{
+		CK(ctx, cudaStreamSynchronize(ctx->stream));
+		if(ctx->d_valid)
+		{
+			cudaFree(ctx->d_valid);
+			ctx->d_valid = nullptr;
+		}
+		CK(ctx, cudaMalloc(&ctx->d_valid, (size_t)need * ctx->S));
+		ctx->valid_stride = need;
+	}
+
+	for(int s = 0; s < ctx->S; s++)
+	{
+		DevSubintStation &u = sl.h_sub[s];
+		memset(&u, 0, sizeof(u));
+		u.nbytes = nbytes[s];
+		u.datasec = datasec[s];
+		u.datans = datans[s];
+		if(device)
+			u.buf = bufs[s];
+		else
+		{
+			if(sl.rawcap[s] < nbytes[s])
+			{
+				if(sl.raw[s]) cudaFree(sl.raw[s]);
+				sl.raw[s] = nullptr;
+				int64_t cap = nbytes[s] + nbytes[s] / 8 + 4096;
+				CK(ctx, cudaMalloc(&sl.raw[s], cap));
+				sl.rawcap[s] = cap;
+			}
+			u.buf = sl.raw[s];
+			if(nbytes[s] > 0)
+				CK(ctx, cudaMemcpyAsync(sl.raw[s], bufs[s], nbytes[s], cudaMemcpyHostToDevice, ctx->copy_stream));
+		}
+		int32_t *vf = sl.h_vflags + (size_t)s * ctx->nflagint;
+		if(validflags && validflags[s])
+			memcpy(vf, validflags[s], sizeof(int32_t) * ((ctx->T + kFlagsPerInt - 1) / kFlagsPerInt));
+		else
+			for(int k = 0; k < ctx->nflagint; k++) vf[k] = 0x3FFFFFFF;
+	}
+	CK(ctx, cudaMemcpyAsync(sl.d_sub, sl.h_sub, sizeof(DevSubintStation) * ctx->S, cudaMemcpyHostToDevice, ctx->copy_stream));
+	CK(ctx, cudaMemcpyAsync(sl.d_vflags, sl.h_vflags, sizeof(int32_t) * ctx->S * ctx->nflagint, cudaMemcpyHostToDevice,
+	                        ctx->copy_stream));
+	CK(ctx, cudaEventRecord(sl.copied, ctx->copy_stream));
+	CK(ctx, cudaStreamWaitEvent(ctx->stream, sl.copied, 0));
+
+	cudaStream_t st = ctx->stream;
+	CK(ctx, cudaEventRecord(ctx->ev_f0, st));
+	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, sec, ns, st);
+	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->valid_stride, ctx->S, st);
+	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->valid_stride, ctx->S, ctx->T,
+	                  sec, ns, job.fringe_rot_order, ctx->d_params, st);
+	launch_fstage(ctx->d_st, sl.d_sub, ctx->d_bands, ctx->maxband, ctx->d_plans, ctx->d_valid, ctx->valid_stride,
+	              ctx->d_params, ctx->d_twiddle, ctx->maxN, ctx->S, ctx->T, job.fringe_rot_order, job.fractionallofreq,
+	              ctx->maxfft, ctx->d_spec, st);
+	CK(ctx, cudaEventRecord(ctx->ev_f1, st));
+	for(int f = 0; f < ctx->F; f++)
+		if(ctx->h_plans[f].nrow > 0)
+			launch_xmac_fp32(ctx->h_plans[f], ctx->d_plans + f, ctx->T, ctx->d_spec, ctx->d_acc, st);
+	launch_weights(ctx->d_bw, ctx->nbw, ctx->d_acw, ctx->nacw, ctx->d_params, ctx->T, ctx->d_bwacc, ctx->d_acwacc, st);
+	CK(ctx, cudaEventRecord(ctx->ev_x1, st));
+	CK(ctx, cudaGetLastError());
+	CK(ctx, cudaEventRecord(sl.done, st));
+	ctx->timed = true;
+	return FXB_OK;
+}
+
+fxb_status fxb_submit_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes, const int32_t *datasec,
+                             const int32_t *datans, const int32_t *const *validflags, int32_t sec, int32_t ns)
+{
+	return submit(ctx, bufs, nbytes, datasec, datans, validflags, sec, ns, false);
+}
+
+fxb_status fxb_submit_subint_device(fxb_ctx *ctx, const uint8_t *const *dev_bufs, const int64_t *nbytes,
+                                    const int32_t *datasec, const int32_t *datans, const int32_t *const *validflags,
+                                    int32_t sec, int32_t ns)
+{
+	return submit(ctx, dev_bufs, nbytes, datasec, datans, validflags, sec, ns, true);
+}
+
+fxb_status fxb_sync(fxb_ctx *ctx)
+{
+	if(!ctx) return FXB_ERR_ARG;
+	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	CK(ctx, cudaStreamSynchronize(ctx->copy_stream));
+	return FXB_OK;
+}
+
+fxb_status fxb_core_result_length(const fxb_ctx *ctx, int64_t *ncomplex)
+{
+	if(!ctx || !ncomplex) return FXB_ERR_ARG;
+	*ncomplex = ctx->job.corelen;
+	return FXB_OK;
+}
+
+fxb_status fxb_layout(const fxb_ctx *ctx, int32_t *out, size_t nint)
+{
+	if(!ctx || !out) return FXB_ERR_ARG;
+	const Job &j = ctx->job;
+	size_t need = 2 * j.bloff.size() + 2 * j.acoff.size();
+	if(nint < need) return FXB_ERR_ARG;
+	size_t k = 0;
+	for(auto v : j.bloff) out[k++] = (int32_t)v;
+	for(auto v : j.bwoff) out[k++] = (int32_t)v;
+	for(auto v : j.acoff) out[k++] = (int32_t)v;
+	for(auto v : j.acwoff) out[k++] = (int32_t)v;
+	return FXB_OK;
+}
+
+fxb_status fxb_job_layout(const fxb_job_desc *desc, int32_t *out, size_t nint, int64_t *ncomplex)
+{
+	Job job;
+	std::string err;
+	fxb_status st = FXB_OK;
+	if(!build_job(desc, job, err, st))
+	{
+		std::lock_guard<std::mutex> lk(g_err_mutex);
+		g_create_err = err;
+		return st;
+	}
+	size_t need = 2 * job.bloff.size() + 2 * job.acoff.size();
+	if(out)
+	{
+		if(nint < need) return FXB_ERR_ARG;
+		size_t k = 0;
+		for(auto v : job.bloff) out[k++] = (int32_t)v;
+		for(auto v : job.bwoff) out[k++] = (int32_t)v;
+		for(auto v : job.acoff) out[k++] = (int32_t)v;
+		for(auto v : job.acwoff) out[k++] = (int32_t)v;
+	}
+	if(ncomplex) *ncomplex = job.corelen;
+	return FXB_OK;
+}
+
+fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats)
+{
+	if(!ctx || !coreresult) return FXB_ERR_ARG;
+	if(nfloats < (size_t)(2 * ctx->job.corelen))
+	{
+		ctx->err = "result buffer too small";
+		return FXB_ERR_ARG;
+	}
+	launch_finalise(ctx->d_om, ctx->nom, 0, ctx->d_acc, ctx->d_bw, ctx->nbw, ctx->d_bwacc, ctx->d_acw, ctx->nacw,
+	                ctx->d_acwacc, ctx->d_core, ctx->job.corelen, ctx->stream);
+	CK(ctx, cudaGetLastError());
+	CK(ctx, cudaMemcpyAsync(coreresult, ctx->d_core, sizeof(float2) * ctx->job.corelen, cudaMemcpyDeviceToHost, ctx->stream));
+	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	return FXB_OK;
+}
+
+fxb_status fxb_reset(fxb_ctx *ctx)
+{
+	if(!ctx) return FXB_ERR_ARG;
+	CK(ctx, cudaMemsetAsync(ctx->d_acc, 0, sizeof(float2) * std::max<int64_t>(ctx->job.acc_total, 1), ctx->stream));
+	CK(ctx, cudaMemsetAsync(ctx->d_bwacc, 0, sizeof(float) * std::max(ctx->nbw, 1), ctx->stream));
+	CK(ctx, cudaMemsetAsync(ctx->d_acwacc, 0, sizeof(float) * std::max(ctx->nacw, 1), ctx->stream));
+	return FXB_OK;
+}
+
+fxb_status fxb_last_timing(const fxb_ctx *ctx, float *fstage_ms, float *xmac_ms, float *total_ms)
+{
+	if(!ctx || !ctx->timed) return FXB_ERR_STATE;
+	fxb_ctx *c = const_cast<fxb_ctx *>(ctx);
+	CK(c, cudaEventSynchronize(ctx->ev_x1));
+	float a = 0, b = 0;
+	CK(c, cudaEventElapsedTime(&a, ctx->ev_f0, ctx->ev_f1));
+	CK(c, cudaEventElapsedTime(&b, ctx->ev_f1, ctx->ev_x1));
+	if(fstage_ms) *fstage_ms = a;
+	if(xmac_ms) *xmac_ms = b;
+	if(total_ms) *total_ms = a + b;
+	return FXB_OK;
+}
+
+fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloats, int32_t *nfft, int32_t *nrow)
+{
+	if(!ctx || !out || freq < 0 || freq >= ctx->F) return FXB_ERR_ARG;
+	const DevFreqPlan &p = ctx->h_plans[freq];
+	size_t n = (size_t)ctx->T * p.nrow * p.nchan;
+	if(nfloats < 2 * n) return FXB_ERR_ARG;
+	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	if(n)
+		CK(ctx, cudaMemcpy(out, ctx->d_spec + p.spec_off, sizeof(float2) * n, cudaMemcpyDeviceToHost));
+	if(nfft) *nfft = ctx->T;
+	if(nrow) *nrow = p.nrow;
+	return FXB_OK;
+}
+
+fxb_status fxb_read_fft_weights(fxb_ctx *ctx, float *out, size_t nfloats)
+{
+	if(!ctx || !out) return FXB_ERR_ARG;
+	size_t n = (size_t)ctx->S * ctx->T;
+	if(nfloats < n) return FXB_ERR_ARG;
+	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	std::vector<FftParam> hp(n);
+	CK(ctx, cudaMemcpy(hp.data(), ctx->d_params, sizeof(FftParam) * n, cudaMemcpyDeviceToHost));
+	for(size_t i = 0; i < n; i++)
+		out[i] = hp[i].status == kFftOk ? hp[i].weight : 0.0f;
+	return FXB_OK;
+}
+
+fxb_status fxb_vdif_unpack(const uint8_t *data, int64_t nbytes, int32_t payload, int32_t header, int32_t nchan,
+                           int32_t nbits, int64_t offsetsamples, int32_t nsamp, float *out, int32_t *good)
+{
+	if(!data || !out || !good || nbytes <= 0 || nsamp <= 0 || offsetsamples < 0 || payload <= 0 || payload % 8 ||
+	   (nbits != 2 && nbits != 8) || nchan < 1 || (nchan & (nchan - 1)) || header < 0)
+		return FXB_ERR_ARG;
+	if((int64_t)payload * 8 % (nchan * nbits))
+		return FXB_ERR_ARG;
+	const int64_t fs = (int64_t)payload * 8 / (nchan * nbits);
+	const int64_t nf = (offsetsamples + nsamp - 1) / fs - offsetsamples / fs + 1;
+	if(nf > 40000)
+		return FXB_ERR_UNSUPPORTED;
+	uint8_t *d_data = nullptr;
+	float *d_out = nullptr;
+	int *d_good = nullptr;
+	cudaStream_t st = 0;
+	fxb_status rc = FXB_OK;
+	static bool lut_ready = false;
+	if(!lut_ready)
+	{
+		upload_lut8(0);
+		lut_ready = true;
+	}
+	if(cudaMalloc(&d_data, nbytes) != cudaSuccess || cudaMalloc(&d_out, sizeof(float) * nchan * (size_t)nsamp) != cudaSuccess ||
+	   cudaMalloc(&d_good, sizeof(int)) != cudaSuccess)
+		rc = FXB_ERR_NOMEM;
+	if(rc == FXB_OK && cudaMemcpy(d_data, data, nbytes, cudaMemcpyHostToDevice) != cudaSuccess)
+		rc = FXB_ERR_CUDA;
+	if(rc == FXB_OK)
+	{
+		launch_vdif_unpack(d_data, nbytes, payload, header, nchan, nbits, offsetsamples, nsamp, d_out, d_good, st);
+		if(cudaGetLastError() != cudaSuccess ||
+		   cudaMemcpy(out, d_out, sizeof(float) * nchan * (size_t)nsamp, cudaMemcpyDeviceToHost) != cudaSuccess ||
+		   cudaMemcpy(good, d_good, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+			rc = FXB_ERR_CUDA;
+	}
+	if(d_data) cudaFree(d_data);
+	if(d_out) cudaFree(d_out);
+	if(d_good) cudaFree(d_good);
+	return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// Internal structures shared by the host runtime and the sm_100a kernels.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fxb200.h"
+
+namespace fxb {
+
+constexpr int kFlagsPerInt = 30;          // mpifxcorr/src/mpifxcorr.h:39
+constexpr int kMaxStations = 64;
+constexpr int kMaxBandsPerStation = 64;
+constexpr int kMaxPolyOrder = 5;          // MAX_POLY_ORDER of the .im reader
+constexpr int kMaxPolys = 64;
+constexpr int kTile = 4;                  // rows per register tile in the FP32 XMAC
+
+// FFT status codes written by the delay kernel (why Mode::process zeroes an FFT).
+enum FftStatus : int32_t {
+	kFftZero = 0,        // flagged invalid, out of range, or zero weight
+	kFftOk = 1
+};
+
+// Per (station, FFT) parameters derived in FP64 by the delay kernel
+// (Mode::process, mode.cpp:671-840, and Mk5Mode::unpack, mk5mode.cpp:104-177).
+struct FftParam {
+	int32_t status;
+	int32_t nearest;      // nearest sample, relative to the start of the station buffer
+	int32_t stuck;        // samples [stuck, N) of the window decode to zero (8-bit 2/4-channel blanking)
+	float weight;         // Mode::getDataWeight
+	float fse;            // fractional sample error (us), float as in mode.cpp:772
+	float lofrac_unused;
+	double averagedelay;  // us
+	double a, b, c;       // fringe-rotation coefficients of the order in use
+	int32_t integerdelay;
+	int32_t pad;
+};
+
+// Station description on the device.
+struct DevStation {
+	int32_t nbits, payload, header, nband;
+	int32_t framebytes;
+	int32_t framesamples;
+	int32_t gran;           // samplegranularity
+	int32_t nchan;          // channels per band (common to all bands of a station)
+	int32_t fftchannels;    // 2*nchan
+	int32_t asl;            // array stride length (calcstridelength(nchan))
+	int32_t sticky;         // 8-bit 2/4-channel blank semantics
+	int32_t bpbn, bpbd;     // bytes-per-block numerator/denominator of Mode
+	double bw;              // MHz
+	double sampletime;      // us
+	int32_t npoly, order, interval;
+	double poly0;
+	double coeffs[kMaxPolys * (kMaxPolyOrder + 1)];
+};
+
+// One band of one station as the F kernel sees it.
+struct DevBand {
+	int32_t freq;           // frequency-table index
+	int32_t row;            // row of this band within its frequency's spectra
+	int32_t lsb;
+	int32_t pad;
+	double lofreq;          // MHz
+};
+
+// Per-subint inputs of one station.
+struct DevSubintStation {
+	const uint8_t *buf;
+	int64_t nbytes;
+	int32_t datasec, datans;
+	int32_t invalid_subint; // no delay model for this time (subint torched)
+	int32_t pad;
+	double interp[3];       // quadratic delay interpolator (Mode::setOffsets)
+};
+
+// Host-side job after validation.
+struct Job {
+	std::vector<fxb_freq> freqs;
+	struct Station {
+		int nbits, payload, header, nband;
+		std::vector<int> band_freq;
+		std::vector<char> band_pol;
+		int npoly = 0, order = 0, interval = 0;
+		double poly0 = 0.0;
+		std::vector<double> coeffs;
+	};
+	std::vector<Station> stations;
+	struct Baseline {
+		int ds1, ds2;
+		std::vector<int> prod_freq, prod_b1, prod_b2;
+	};
+	std::vector<Baseline> baselines;
+	int64_t subint_ns = 0;
+	int fringe_rot_order = 1;
+	int write_autocorrs = 1;
+	int xmac_kind = 0;
+	int inflight = 2;
+
+	// derived
+	int blockspersend = 0;
+	int maxproducts = 0;
+	int bandsperautocorr = 1;
+	bool fractionallofreq = false;
+	std::vector<int> freqused, equivused;
+	int64_t corelen = 0;
+	std::vector<int64_t> bloff, bwoff, acoff, acwoff;   // core-result offsets (complex index)
+
+	// rows of every used frequency: (station, band) in station order
+	struct Row { int station, band; };
+	std::vector<std::vector<Row>> rows;                  // [freq]
+	std::vector<std::vector<int>> band_row;              // [station][band] -> row in its freq
+	// XMAC outputs per frequency: accumulator offsets
+	struct FreqPlan {
+		int nrow = 0;
+		int nchan = 0;
+		int64_t spec_off = 0;      // offset (complex) of this freq's spectra [T][nrow][nchan]
+		int64_t acc_off = 0;       // offset (complex) of this freq's accumulators [nout][nchan]
+		int nout = 0;
+		std::vector<int> destA;    // [nrow*nrow] output index of V[i][j] (i<=j) or -1
+		std::vector<int> destB;    // [nrow*nrow] output index receiving conj(V[i][j]) or -1
+	};
+	std::vector<FreqPlan> plan;                           // [freq]
+	int64_t spec_total = 0;       // complex values of spectra for one subint
+	int64_t acc_total = 0;        // complex accumulators
+	// output descriptors for finalisation
+	struct OutMap {
+		int64_t acc;     // accumulator offset (complex) of the first channel
+		int64_t core;    // core-result offset (complex) of the first output channel
+		int nchan, avg;
+	};
+	std::vector<OutMap> outmap;
+	// weight plans
+	struct BWeight { int s1, s2; int64_t dst_float; };
+	std::vector<BWeight> bweights;
+	struct ACWeight { int s; int band; int64_t dst_float; };
+	std::vector<ACWeight> acweights;
+};
+
+bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st);
+int calcstridelength(unsigned int arraylength);
+
+}  // namespace fxb

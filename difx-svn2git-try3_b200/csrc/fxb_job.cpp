@@ -1,0 +1,376 @@
+// Job validation and the core-result layout.
+//
+// The layout restates Configuration::populateResultLengths
+// (mpifxcorr/src/configuration.cpp:2212-2440) for one configuration with one
+// phase centre, no pulsar bins, no zoom bands and no phase cal: cross
+// correlations [freq][baseline][product][nchan/avg], then baseline weights
+// (products/2 rounded up complex slots), then per datastream the
+// autocorrelations (parallel hands, then cross hands when the job has more
+// than two products), then the autocorrelation weights.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "fxb_internal.h"
+
+namespace fxb {
+
+// calcstridelength (configuration.cpp:46-58): the array stride used by
+// Mode's rotator tables; it enters the order-2 fringe phase.
+int calcstridelength(unsigned int arraylength)
+{
+	if(arraylength <= 16)
+		return (int)arraylength;
+	for(unsigned int guess = (unsigned int)std::sqrt(arraylength + 0.1); ; --guess)
+		if(arraylength % guess == 0)
+			return (int)(arraylength / guess);
+}
+
+static bool fail(std::string &err, fxb_status &st, fxb_status code, const std::string &msg)
+{
+	err = msg;
+	st = code;
+	return false;
+}
+
+static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st)
+{
+	st = FXB_OK;
+	if(!d || d->nfreq <= 0 || !d->freqs || d->nstation < 1 || !d->stations || d->nbaseline < 0)
+		return fail(err, st, FXB_ERR_ARG, "empty or null job description");
+	if(d->nstation > kMaxStations)
+		return fail(err, st, FXB_ERR_UNSUPPORTED, "too many stations");
+	if(d->fringe_rot_order < 0 || d->fringe_rot_order > 2)
+		return fail(err, st, FXB_ERR_ARG, "fringe rotation order must be 0, 1 or 2");
+	if(d->xmac_kind < FXB_XMAC_FP32 || d->xmac_kind > FXB_XMAC_FP8)
+		return fail(err, st, FXB_ERR_ARG, "unknown xmac kind");
+	job.freqs.assign(d->freqs, d->freqs + d->nfreq);
+	for(auto &f : job.freqs)
+	{
+		if(!(f.bw_mhz > 0.0) || f.nchan <= 0 || f.chans_to_avg <= 0 || f.nchan % f.chans_to_avg)
+			return fail(err, st, FXB_ERR_ARG, "bad frequency entry");
+		if(!is_pow2(f.nchan) || f.nchan < 16 || f.nchan > 8192)
+			return fail(err, st, FXB_ERR_UNSUPPORTED, "channel counts must be powers of two in [16, 8192]");
+	}
+	for(int s = 0; s < d->nstation; s++)
+	{
+		const fxb_station &in = d->stations[s];
+		Job::Station o;
+		o.nbits = in.nbits;
+		o.payload = in.payload_bytes;
+		o.header = in.header_bytes;
+		o.nband = in.nband;
+		if(in.nband < 1 || in.nband > kMaxBandsPerStation || !in.band_freq || !in.band_pol)
+			return fail(err, st, FXB_ERR_ARG, "station needs at least one band");
+		if(!is_pow2(in.nband))
+			return fail(err, st, FXB_ERR_UNSUPPORTED, "VDIF channel count must be a power of two");
+		if(in.nbits == 2)
+		{
+			if(in.nband > 64)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "2-bit VDIF supports up to 64 channels");
+		}
+		else if(in.nbits == 8)
+		{
+			if(in.nband > 4)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "8-bit VDIF supports up to 4 channels");
+		}
+		else
+			return fail(err, st, FXB_ERR_UNSUPPORTED, "only 2-bit and 8-bit samples are supported");
+		if(in.header_bytes != 32 && in.header_bytes != 16)
+			return fail(err, st, FXB_ERR_ARG, "VDIF header must be 16 or 32 bytes");
+		if(in.payload_bytes <= 0 || in.payload_bytes % 8 || ((int64_t)in.payload_bytes * 8) % (in.nbits * in.nband))
+			return fail(err, st, FXB_ERR_ARG, "payload must be a multiple of 8 bytes holding whole samples");
+		o.band_freq.assign(in.band_freq, in.band_freq + in.nband);
+		o.band_pol.assign(in.band_pol, in.band_pol + in.nband);
+		for(int b = 0; b < in.nband; b++)
+			if(o.band_freq[b] < 0 || o.band_freq[b] >= d->nfreq)
+				return fail(err, st, FXB_ERR_ARG, "band frequency index out of range");
+		const fxb_freq &f0 = job.freqs[o.band_freq[0]];
+		for(int b = 1; b < in.nband; b++)
+		{
+			const fxb_freq &fb = job.freqs[o.band_freq[b]];
+			if(fb.nchan != f0.nchan || fb.bw_mhz != f0.bw_mhz)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "all bands of one station share bandwidth and channels");
+		}
+		job.stations.push_back(o);
+	}
+	for(int b = 0; b < d->nbaseline; b++)
+	{
+		const fxb_baseline &in = d->baselines[b];
+		Job::Baseline o;
+		o.ds1 = in.ds1;
+		o.ds2 = in.ds2;
+		if(in.ds1 < 0 || in.ds2 < 0 || in.ds1 >= d->nstation || in.ds2 >= d->nstation || in.ds1 == in.ds2)
+			return fail(err, st, FXB_ERR_ARG, "baseline station index out of range");
+		if(in.nprod < 1 || !in.prod_freq || !in.prod_band1 || !in.prod_band2)
+			return fail(err, st, FXB_ERR_ARG, "baseline without products");
+		o.prod_freq.assign(in.prod_freq, in.prod_freq + in.nprod);
+		o.prod_b1.assign(in.prod_band1, in.prod_band1 + in.nprod);
+		o.prod_b2.assign(in.prod_band2, in.prod_band2 + in.nprod);
+		for(int p = 0; p < in.nprod; p++)
+		{
+			int f = o.prod_freq[p];
+			if(f < 0 || f >= d->nfreq)
+				return fail(err, st, FXB_ERR_ARG, "product frequency out of range");
+			if(p > 0 && f != o.prod_freq[p - 1])
+				for(int q = 0; q < p - 1; q++)
+					if(o.prod_freq[q] == f)
+						return fail(err, st, FXB_ERR_ARG, "products of one frequency must be contiguous");
+			int b1 = o.prod_b1[p], b2 = o.prod_b2[p];
+			if(b1 < 0 || b1 >= job.stations[o.ds1].nband || b2 < 0 || b2 >= job.stations[o.ds2].nband)
+				return fail(err, st, FXB_ERR_ARG, "product band index out of range");
+			if(job.stations[o.ds1].band_freq[b1] != f || job.stations[o.ds2].band_freq[b2] != f)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "product bands must record the product frequency");
+		}
+		job.baselines.push_back(o);
+	}
+	job.subint_ns = d->subint_ns;
+	job.fringe_rot_order = d->fringe_rot_order;
+	job.write_autocorrs = d->write_autocorrs ? 1 : 0;
+	job.xmac_kind = d->xmac_kind;
+	job.inflight = std::max(1, std::min(8, d->max_subints_in_flight));
+
+	// blockspersend (configuration.cpp:1852-1860); all stations must agree
+	{
+		const int S = (int)job.stations.size();
+		double bps0 = -1.0;
+		for(int s = 0; s < S; s++)
+		{
+			const fxb_freq &f = job.freqs[job.stations[s].band_freq[0]];
+			double fftns = 2.0 * f.nchan * 1000.0 / (2.0 * f.bw_mhz);
+			double bpsd = (double)d->subint_ns / fftns;
+			int bps = (int)(bpsd + 0.5);
+			if(std::fabs(bpsd - bps) > 1e-9 || bps < 1)
+				return fail(err, st, FXB_ERR_ARG, "subint must hold a whole number of FFTs");
+			if(bps0 >= 0 && bps != (int)bps0)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "all stations must have the same FFTs per subint");
+			bps0 = bps;
+			job.blockspersend = bps;
+			int64_t fsamp = (int64_t)job.stations[s].payload * 8 / (job.stations[s].nbits * job.stations[s].nband);
+			double sps = 2e6 * f.bw_mhz;
+			if(std::fabs(sps / fsamp - std::floor(sps / fsamp + 0.5)) > 1e-9)
+				return fail(err, st, FXB_ERR_ARG, "whole frames per second required");
+		}
+	}
+
+	// getMaxProducts (configuration.cpp:843-857)
+	const int F = (int)job.freqs.size(), B = (int)job.baselines.size(), S = (int)job.stations.size();
+	job.maxproducts = 0;
+	for(auto &bl : job.baselines)
+		for(int f = 0; f < F; f++)
+		{
+			int n = (int)std::count(bl.prod_freq.begin(), bl.prod_freq.end(), f);
+			job.maxproducts = std::max(job.maxproducts, n);
+		}
+	job.bandsperautocorr = job.maxproducts > 2 ? 2 : 1;
+
+	// frequency usage (configuration.cpp:325-368)
+	job.freqused.assign(F, 0);
+	job.equivused.assign(F, 0);
+	for(auto &bl : job.baselines)
+		for(int f : bl.prod_freq)
+			job.freqused[f] = 1;
+	for(int f = 0; f < F; f++)
+	{
+		if(job.freqused[f])
+			continue;
+		for(int k = 0; k < F; k++)
+		{
+			double bwdiff = job.freqs[f].bw_mhz - job.freqs[k].bw_mhz;
+			double freqdiff = job.freqs[f].freq_mhz - job.freqs[k].freq_mhz;
+			if(job.freqs[f].lower_sideband) freqdiff -= job.freqs[f].bw_mhz;
+			if(job.freqs[k].lower_sideband) freqdiff += job.freqs[k].bw_mhz;
+			if(bwdiff < 1e-9 && freqdiff < 1e-9 && job.freqs[f].nchan == job.freqs[k].nchan &&
+			   job.freqs[f].chans_to_avg == job.freqs[k].chans_to_avg && job.freqused[k])
+				job.equivused[f] = 1;
+		}
+	}
+
+	// core-result layout
+	int64_t idx = 0;
+	job.bloff.assign((size_t)F * B, -1);
+	job.bwoff.assign((size_t)F * B, -1);
+	job.acoff.assign(S, 0);
+	job.acwoff.assign(S, 0);
+	auto nprod_f = [&](const Job::Baseline &bl, int f) {
+		return (int)std::count(bl.prod_freq.begin(), bl.prod_freq.end(), f);
+	};
+	for(int f = 0; f < F; f++)
+	{
+		if(!job.freqused[f]) continue;
+		for(int b = 0; b < B; b++)
+		{
+			int n = nprod_f(job.baselines[b], f);
+			if(!n) continue;
+			job.bloff[(size_t)f * B + b] = idx;
+			idx += (int64_t)n * job.freqs[f].nchan / job.freqs[f].chans_to_avg;
+		}
+	}
+	for(int f = 0; f < F; f++)
+	{
+		if(!job.freqused[f]) continue;
+		for(int b = 0; b < B; b++)
+		{
+			int n = nprod_f(job.baselines[b], f);
+			if(!n) continue;
+			job.bwoff[(size_t)f * B + b] = idx;
+			idx += n / 2 + n % 2;
+		}
+	}
+	for(int s = 0; s < S; s++)
+	{
+		job.acoff[s] = idx;
+		for(int bnd = 0; bnd < job.stations[s].nband; bnd++)
+		{
+			int fi = job.stations[s].band_freq[bnd];
+			if(job.freqused[fi] || job.equivused[fi])
+				idx += (int64_t)job.bandsperautocorr * job.freqs[fi].nchan / job.freqs[fi].chans_to_avg;
+		}
+	}
+	for(int s = 0; s < S; s++)
+	{
+		job.acwoff[s] = idx;
+		int toadd = 0;
+		for(int bnd = 0; bnd < job.stations[s].nband; bnd++)
+		{
+			int fi = job.stations[s].band_freq[bnd];
+			if(job.freqused[fi] || job.equivused[fi])
+				toadd += job.bandsperautocorr;
+		}
+		toadd = (toadd + 1) / 2;
+		if(toadd == 0) toadd = 1;
+		idx += toadd;
+	}
+	job.corelen = idx;
+
+	// fractionalLoFreq (mode.cpp:89-105)
+	job.fractionallofreq = false;
+	for(auto &s : job.stations)
+		for(int f : s.band_freq)
+		{
+			double lo = job.freqs[f].freq_mhz;
+			if(std::fabs(lo - (int)(lo + 0.5)) > 0.000000001)
+				job.fractionallofreq = true;
+		}
+
+	// rows per frequency, spectra and accumulator plans
+	job.rows.assign(F, {});
+	job.band_row.assign(S, {});
+	for(int s = 0; s < S; s++)
+	{
+		job.band_row[s].assign(job.stations[s].nband, -1);
+		for(int bnd = 0; bnd < job.stations[s].nband; bnd++)
+		{
+			int f = job.stations[s].band_freq[bnd];
+			if(!(job.freqused[f] || job.equivused[f]))
+				continue;
+			job.band_row[s][bnd] = (int)job.rows[f].size();
+			job.rows[f].push_back({s, bnd});
+		}
+	}
+	job.plan.assign(F, {});
+	const int T = job.blockspersend;
+	std::vector<std::vector<int>> crossout(S);     // [s][band] -> cross-pol output index, -1
+	for(int s = 0; s < S; s++)
+		crossout[s].assign(job.stations[s].nband, -1);
+	int64_t spec = 0, acc = 0;
+	for(int f = 0; f < F; f++)
+	{
+		Job::FreqPlan &pl = job.plan[f];
+		pl.nrow = (int)job.rows[f].size();
+		pl.nchan = job.freqs[f].nchan;
+		if(pl.nrow == 0)
+			continue;
+		if(pl.nrow > 128)
+			return fail(err, st, FXB_ERR_UNSUPPORTED, "more than 128 inputs on one frequency");
+		pl.spec_off = spec;
+		spec += (int64_t)T * pl.nrow * pl.nchan;
+		pl.destA.assign((size_t)pl.nrow * pl.nrow, -1);
+		pl.destB.assign((size_t)pl.nrow * pl.nrow, -1);
+		pl.acc_off = acc;
+		int nout = 0;
+		// baseline products, in core-result order
+		for(int b = 0; b < B; b++)
+		{
+			const Job::Baseline &bl = job.baselines[b];
+			int pf = 0;
+			for(size_t p = 0; p < bl.prod_freq.size(); p++)
+			{
+				if(bl.prod_freq[p] != f) continue;
+				int r1 = job.band_row[bl.ds1][bl.prod_b1[p]], r2 = job.band_row[bl.ds2][bl.prod_b2[p]];
+				int o = nout++;
+				if(r1 < r2)
+				{
+					if(pl.destA[(size_t)r1 * pl.nrow + r2] >= 0)
+						return fail(err, st, FXB_ERR_UNSUPPORTED, "duplicate product");
+					pl.destA[(size_t)r1 * pl.nrow + r2] = o;
+				}
+				else
+				{
+					if(pl.destB[(size_t)r2 * pl.nrow + r1] >= 0)
+						return fail(err, st, FXB_ERR_UNSUPPORTED, "duplicate product");
+					pl.destB[(size_t)r2 * pl.nrow + r1] = o;
+				}
+				job.outmap.push_back({acc + (int64_t)o * pl.nchan,
+				                      job.bloff[(size_t)f * B + b] + (int64_t)pf * pl.nchan / job.freqs[f].chans_to_avg,
+				                      pl.nchan, job.freqs[f].chans_to_avg});
+				job.bweights.push_back({bl.ds1, bl.ds2, 2 * job.bwoff[(size_t)f * B + b] + pf});
+				pf++;
+			}
+		}
+		// autocorrelations: one output per row
+		for(int r = 0; r < pl.nrow; r++)
+			pl.destA[(size_t)r * pl.nrow + r] = nout++;
+		// cross-pol autocorrelations (mode.cpp:1356-1369): the first two bands
+		// of a station on this frequency; V[r0][r1] and its conjugate
+		if(job.write_autocorrs)
+			for(int s = 0; s < S; s++)
+			{
+				int idxs[2], cnt = 0;
+				for(int bnd = 0; bnd < job.stations[s].nband && cnt < 2; bnd++)
+					if(job.stations[s].band_freq[bnd] == f) idxs[cnt++] = bnd;
+				if(cnt < 2) continue;
+				int r0 = job.band_row[s][idxs[0]], r1 = job.band_row[s][idxs[1]];
+				int o01 = nout++, o10 = nout++;
+				// rows of one station are contiguous and ordered by band: r0 < r1
+				pl.destA[(size_t)r0 * pl.nrow + r1] = o01;
+				pl.destB[(size_t)r0 * pl.nrow + r1] = o10;
+				crossout[s][idxs[0]] = o01;
+				crossout[s][idxs[1]] = o10;
+			}
+		pl.nout = nout;
+		acc += (int64_t)nout * pl.nchan;
+	}
+	job.spec_total = spec;
+	job.acc_total = acc;
+
+	// autocorrelation outputs and weights (core.cpp:1266-1363)
+	bool writecross = job.write_autocorrs && job.maxproducts > 2;
+	for(int s = 0; s < S; s++)
+	{
+		int64_t ridx = job.acoff[s];
+		int64_t widx = 2 * job.acwoff[s];
+		for(int pass = 0; pass < (writecross ? 2 : 1); pass++)
+			for(int bnd = 0; bnd < job.stations[s].nband; bnd++)
+			{
+				int f = job.stations[s].band_freq[bnd];
+				if(!(job.freqused[f] || job.equivused[f])) continue;
+				const Job::FreqPlan &pl = job.plan[f];
+				int r = job.band_row[s][bnd];
+				int64_t a;
+				if(pass == 0)
+					a = pl.acc_off + (int64_t)pl.destA[(size_t)r * pl.nrow + r] * pl.nchan;
+				else
+					a = crossout[s][bnd] >= 0 ? pl.acc_off + (int64_t)crossout[s][bnd] * pl.nchan : -1;
+				job.outmap.push_back({a, ridx, pl.nchan, job.freqs[f].chans_to_avg});
+				ridx += pl.nchan / job.freqs[f].chans_to_avg;
+				job.acweights.push_back({s, bnd, widx++});
+			}
+	}
+	return true;
+}
+
+}  // namespace fxb

@@ -139,9 +139,10 @@ def lib():
     L.fxb_read_spectra.argtypes = [vp, i32, fp, ctypes.c_size_t, i32p, i32p]
     L.fxb_read_fft_weights.argtypes = [vp, fp, ctypes.c_size_t]
     L.fxb_vdif_unpack.argtypes = [ctypes.c_void_p, i64, i32, i32, i32, i32, i64, i32, fp, i32p]
+    L.fxb_job_layout.argtypes = [ctypes.POINTER(FxbJobDesc), i32p, ctypes.c_size_t, i64p]
     for name in ("fxb_set_delay_poly", "fxb_submit_subint", "fxb_submit_subint_device", "fxb_sync",
                  "fxb_core_result_length", "fxb_layout", "fxb_read_results", "fxb_reset", "fxb_last_timing",
-                 "fxb_read_spectra", "fxb_read_fft_weights", "fxb_vdif_unpack"):
+                 "fxb_read_spectra", "fxb_read_fft_weights", "fxb_vdif_unpack", "fxb_job_layout"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -245,7 +246,7 @@ class Correlator:
         nt, nr = ctypes.c_int32(), ctypes.c_int32()
         check(lib().fxb_read_spectra(self.ctx, freq, _fptr(out), out.size, ctypes.byref(nt), ctypes.byref(nr)),
               self.ctx, "read_spectra")
-        x = out.reshape(nt.value, nchan, nr.value, 2)
+        x = out.reshape(nt.value, nr.value, nchan, 2)
         return x[..., 0] + 1j * x[..., 1]
 
     def fft_weights(self) -> np.ndarray:
@@ -262,3 +263,14 @@ def vdif_unpack(data: np.ndarray, payload: int, header: int, nchan: int, nbits: 
     check(lib().fxb_vdif_unpack(data.ctypes.data, data.size, payload, header, nchan, nbits, offsetsamples,
                                 nsamp, _fptr(out), ctypes.byref(good)), None, "vdif_unpack")
     return out, good.value
+
+
+def job_layout(job: Job) -> Tuple[np.ndarray, int]:
+    """Core-result offsets and length from the job alone (no GPU needed)."""
+    holder = DescHolder(job)
+    nf, nb, ns = len(job.freqs), len(job.baselines), len(job.stations)
+    out = np.zeros(2 * nf * nb + 2 * ns, dtype=np.int32)
+    n = ctypes.c_int64(0)
+    check(lib().fxb_job_layout(holder.ptr(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), out.size,
+                               ctypes.byref(n)), None, "job_layout")
+    return out, n.value

@@ -20,6 +20,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define FXB_API __attribute__((visibility("default")))
+#else
+#define FXB_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -95,12 +101,12 @@ typedef struct fxb_ctx fxb_ctx;
  * computes the core-result layout and allocates device state.
  * Replaces Configuration::getMode + Mode::Mode + Core's result buffers
  * (configuration.cpp:954-1016, mode.cpp:43-462, core.cpp:33-197). */
-fxb_ctx *fxb_create(const fxb_job_desc *desc, fxb_status *status);
-void fxb_destroy(fxb_ctx *ctx);
+FXB_API fxb_ctx *fxb_create(const fxb_job_desc *desc, fxb_status *status);
+FXB_API void fxb_destroy(fxb_ctx *ctx);
 
 /* Text of the last error seen by this context (or by fxb_create when ctx is
  * NULL).  Valid until the next call on the context. */
-const char *fxb_last_error(const fxb_ctx *ctx);
+FXB_API const char *fxb_last_error(const fxb_ctx *ctx);
 
 /* Delay model of one station, in the .im convention read by
  * Model (model.cpp:600-856): npoly consecutive polynomials, each of order
@@ -109,7 +115,7 @@ const char *fxb_last_error(const fxb_ctx *ctx);
  * coeffs holds npoly*(order+1) values in microseconds.  The per-subint
  * quadratic interpolator is derived on the device in FP64 exactly as
  * Model::calculateDelayInterpolator does (model.cpp:229-299). */
-fxb_status fxb_set_delay_poly(fxb_ctx *ctx, int32_t station, int32_t npoly, int32_t order,
+FXB_API fxb_status fxb_set_delay_poly(fxb_ctx *ctx, int32_t station, int32_t npoly, int32_t order,
                               double poly0_sec, int32_t interval_s, const double *coeffs);
 
 /* Correlate one subintegration (Mode::setData/setValidFlags/setOffsets then
@@ -120,53 +126,59 @@ fxb_status fxb_set_delay_poly(fxb_ctx *ctx, int32_t station, int32_t npoly, int3
  * validflags[s]: the valid-FFT bitfield (30 flags per int32, may be NULL for
  * all valid); (sec, ns): subint start after the job start.  Returns once the
  * inputs have been copied; the work completes asynchronously. */
-fxb_status fxb_submit_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes,
+FXB_API fxb_status fxb_submit_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes,
                              const int32_t *datasec, const int32_t *datans,
                              const int32_t *const *validflags, int32_t sec, int32_t ns);
 
 /* As fxb_submit_subint but with the station buffers already in device
  * memory (pointers from cudaMalloc); they must stay valid until the next
  * fxb_sync.  validflags stay in host memory. */
-fxb_status fxb_submit_subint_device(fxb_ctx *ctx, const uint8_t *const *dev_bufs, const int64_t *nbytes,
+FXB_API fxb_status fxb_submit_subint_device(fxb_ctx *ctx, const uint8_t *const *dev_bufs, const int64_t *nbytes,
                                     const int32_t *datasec, const int32_t *datans,
                                     const int32_t *const *validflags, int32_t sec, int32_t ns);
 
 /* Wait for all submitted work. */
-fxb_status fxb_sync(fxb_ctx *ctx);
+FXB_API fxb_status fxb_sync(fxb_ctx *ctx);
 
 /* Number of complex values in the core-result buffer
  * (Configuration::getCoreResultLength). */
-fxb_status fxb_core_result_length(const fxb_ctx *ctx, int64_t *ncomplex);
+FXB_API fxb_status fxb_core_result_length(const fxb_ctx *ctx, int64_t *ncomplex);
 
 /* Offsets into the core result: for f in freqs, b in baselines the baseline
  * offset (or -1), then the same for the baseline-weight offsets, then the
  * autocorrelation offset and the autocorrelation-weight offset of every
  * datastream (Configuration::getCoreResult*Offset).  out holds
  * 2*nfreq*nbaseline + 2*nstation ints. */
-fxb_status fxb_layout(const fxb_ctx *ctx, int32_t *out, size_t nint);
+FXB_API fxb_status fxb_layout(const fxb_ctx *ctx, int32_t *out, size_t nint);
+
+/* The same layout computed from a job description alone, without a GPU or a
+ * context (Configuration::populateResultLengths,
+ * configuration.cpp:2212-2440): validates the job, writes the offsets as
+ * fxb_layout does and the core-result length in complex values. */
+FXB_API fxb_status fxb_job_layout(const fxb_job_desc *desc, int32_t *out, size_t nint, int64_t *ncomplex);
 
 /* Copy the accumulated core result (2*ncomplex floats) to host memory, in
  * the reference layout: cross-correlations, baseline weights,
  * autocorrelations, autocorrelation weights.  Synchronises. */
-fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats);
+FXB_API fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats);
 
 /* Zero the accumulators (Core::execute after each send, core.cpp:318-322). */
-fxb_status fxb_reset(fxb_ctx *ctx);
+FXB_API fxb_status fxb_reset(fxb_ctx *ctx);
 
 /* Device time in ms of the last subint's kernels (F stage, XMAC, total),
  * measured with CUDA events on the context's stream. */
-fxb_status fxb_last_timing(const fxb_ctx *ctx, float *fstage_ms, float *xmac_ms, float *total_ms);
+FXB_API fxb_status fxb_last_timing(const fxb_ctx *ctx, float *fstage_ms, float *xmac_ms, float *total_ms);
 
-/* F-stage output of the last subint for one frequency: spectra[t][c][row]
+/* F-stage output of the last subint for one frequency: spectra[t][row][c]
  * complex (FP32, converted from the XMAC operand type), rows = the
  * (station, band) inputs recording that frequency in station order.
  * Debug/parity access; synchronises. */
-fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloats,
+FXB_API fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloats,
                             int32_t *nfft, int32_t *nrow);
 
 /* Per-FFT station weights of the last subint: weights[s][t] (the data
  * weight of Mode::getDataWeight).  Synchronises. */
-fxb_status fxb_read_fft_weights(fxb_ctx *ctx, float *out, size_t nfloats);
+FXB_API fxb_status fxb_read_fft_weights(fxb_ctx *ctx, float *out, size_t nfloats);
 
 /* Decode VDIF payload samples on the GPU, the call Mk5Mode::unpack makes
  * into mark5access (mark5_unpack_with_offset,
@@ -174,7 +186,7 @@ fxb_status fxb_read_fft_weights(fxb_ctx *ctx, float *out, size_t nfloats);
  * decoders of format_vdif.c and the blanker of blanker_mark5.c:282-313).
  * data: nbytes of back-to-back VDIF frames (host memory); out: [nchan][nsamp]
  * floats (host memory); *good: good-sample count as mark5access returns it. */
-fxb_status fxb_vdif_unpack(const uint8_t *data, int64_t nbytes, int32_t payload_bytes, int32_t header_bytes,
+FXB_API fxb_status fxb_vdif_unpack(const uint8_t *data, int64_t nbytes, int32_t payload_bytes, int32_t header_bytes,
                            int32_t nchan, int32_t nbits, int64_t offsetsamples, int32_t nsamp,
                            float *out, int32_t *good);
 

@@ -660,7 +660,7 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 	int s, t, b, p, c;
 	dcx **spec = (dcx **)calloc(S, sizeof(dcx *));
 	double **acc_ac = (double **)calloc(S, sizeof(double *));     /* [band][2][nchan][2] */
-	double **acw = (double **)calloc(S, sizeof(double *));        /* [band][2] */
+	float **acw = (float **)calloc(S, sizeof(float *));           /* [band][2], float as Mode::weights */
 	float *w = (float *)calloc((size_t)S * T, sizeof(float));
 	int *ups = (int *)calloc(S, sizeof(int));
 	int *badsub = (int *)calloc(S, sizeof(int));
@@ -677,7 +677,7 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 		if(j->nband[s] > maxnb) maxnb = j->nband[s];
 		spec[s] = (dcx *)calloc((size_t)T * j->nband[s] * nchan, sizeof(dcx));
 		acc_ac[s] = (double *)calloc((size_t)j->nband[s] * 2 * nchan * 2, sizeof(double));
-		acw[s] = (double *)calloc((size_t)j->nband[s] * 2, sizeof(double));
+		acw[s] = (float *)calloc((size_t)j->nband[s] * 2, sizeof(float));
 		ups[s] = -999999999;
 		badsub[s] = fxo_interpolator(j, s, sec, ns, interp[s]) != 0;
 		if(!validflags || !validflags[s])
@@ -756,7 +756,7 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 			int f = j->prod_freq[b][p];
 			int nchan = j->freqs[f].nchan, avg = j->freqs[f].chans_to_avg;
 			int64_t base;
-			double wsum = 0.0;
+			float wsum = 0.0f;   /* float sequential sum, as core.cpp:1041 */
 			if(f != lastf) { pf = 0; lastf = f; }
 			base = j->bloff[f * B + b];
 			for(c = 0; c < nchan; c++)
@@ -773,7 +773,7 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 				coreresult[2 * (base + (int64_t)pf * nchan / avg + c / avg) + 1] += im / avg;
 			}
 			for(t = 0; t < T; t++)
-				wsum += (double)w[(size_t)s1 * T + t] * w[(size_t)s2 * T + t];
+				wsum += w[(size_t)s1 * T + t] * w[(size_t)s2 * T + t];
 			coreresult[2 * j->bwoff[f * B + b] + pf] += wsum;
 			pf++;
 		}

@@ -46,7 +46,27 @@ struct RefJob
 struct ThreadAcc
 {
 	std::vector<cf32> results;
+	std::vector<cf32> xc;        // full-resolution cross products, [f][b][p][nchan]
 };
+
+/* offset of (f, b) in the full-resolution thread buffer */
+static int64_t xc_offset(Configuration *c, int nfreq, int numbl, int f, int b, int64_t *total)
+{
+	int64_t off = 0, want = -1;
+	for(int ff = 0; ff < nfreq; ff++)
+	{
+		if(!c->isFrequencyUsed(0, ff)) continue;
+		for(int bb = 0; bb < numbl; bb++)
+		{
+			int lf = c->getBLocalFreqIndex(0, bb, ff);
+			if(lf < 0) continue;
+			if(ff == f && bb == b) want = off;
+			off += (int64_t)c->getBNumPolProducts(0, bb, lf) * c->getFNumChannels(ff);
+		}
+	}
+	if(total) *total = off;
+	return want;
+}
 
 Mode *make_mode(Configuration *c, int ds)
 {
@@ -113,7 +133,7 @@ void process_range(RefJob *j, int t, int startblock, int numblocks,
 					continue;
 				const Mode *m1 = modes[config->getBOrderedDataStream1Index(0, b)];
 				const Mode *m2 = modes[config->getBOrderedDataStream2Index(0, b)];
-				int base = config->getCoreResultBaselineOffset(0, f, b);
+				int64_t base = xc_offset(config, j->nfreq, j->numbl, f, b, 0);
 				for(int sub = 0; sub < nbuf; sub++)
 				{
 					int i = fftloop * nbuf + sub + startblock;
@@ -123,7 +143,7 @@ void process_range(RefJob *j, int t, int startblock, int numblocks,
 					{
 						const cf32 *v1 = m1->getFreqs(config->getBDataStream1BandIndex(0, b, lf, p), sub);
 						const cf32 *v2 = m2->getConjugatedFreqs(config->getBDataStream2BandIndex(0, b, lf, p), sub);
-						cf32 *a = &acc->results[base + p * nchan];
+						cf32 *a = &acc->xc[base + p * nchan];
 						for(int l = 0; l < nchan; l++)
 						{
 							a[l].re += v1[l].re * v2[l].re - v1[l].im * v2[l].im;
@@ -162,6 +182,41 @@ void process_range(RefJob *j, int t, int startblock, int numblocks,
 					}
 				}
 			}
+		}
+	}
+
+	/* thread results into the core layout with channel averaging
+	 * (core.cpp:1774-1802: mean over chans-to-average channels) */
+	for(int f = 0; f < j->nfreq; f++)
+	{
+		if(!config->isFrequencyUsed(0, f))
+			continue;
+		int nchan = config->getFNumChannels(f);
+		int avg = config->getFChannelsToAverage(f);
+		for(int b = 0; b < j->numbl; b++)
+		{
+			int lf = config->getBLocalFreqIndex(0, b, f);
+			if(lf < 0)
+				continue;
+			int64_t src = xc_offset(config, j->nfreq, j->numbl, f, b, 0);
+			int core = config->getCoreResultBaselineOffset(0, f, b);
+			for(int p = 0; p < config->getBNumPolProducts(0, b, lf); p++)
+				for(int k = 0; k < nchan / avg; k++)
+				{
+					const cf32 *x = &acc->xc[src + (int64_t)p * nchan + (int64_t)k * avg];
+					if(avg == 1)
+					{
+						acc->results[core + p * nchan + k].re += x[0].re;
+						acc->results[core + p * nchan + k].im += x[0].im;
+					}
+					else
+					{
+						f32 sr = 0.0f, si = 0.0f;
+						for(int l = 0; l < avg; l++) { sr += x[l].re; si += x[l].im; }
+						acc->results[core + (p * nchan) / avg + k].re += sr / avg;
+						acc->results[core + (p * nchan) / avg + k].im += si / avg;
+					}
+				}
 		}
 	}
 
@@ -301,6 +356,11 @@ int dref_process_subint(void *h, int nthreads,
 		int start = t * (bps / nthreads) + (t < bps % nthreads ? t : bps % nthreads);
 		int num = bps / nthreads + (t < bps % nthreads ? 1 : 0);
 		accs[t].results.assign(j->corelen, cf32{0.0f, 0.0f});
+		{
+			int64_t tot = 0;
+			xc_offset(j->config, j->nfreq, j->numbl, -1, -1, &tot);
+			accs[t].xc.assign(tot, cf32{0.0f, 0.0f});
+		}
 		if(nthreads == 1)
 			process_range(j, 0, start, num, bufs, nbytes, dscan, dsec, dns, validflags, scan, sec, ns, &accs[0]);
 		else

@@ -1,0 +1,80 @@
+"""Pins the oracle restatement to the reference's own compiled CPU code
+(oracle/_ref, built from the reference sources by oracle/Makefile.ref):
+layout, delay interpolator and data weights exact, VDIF decoding bit-exact
+against mark5access, spectra and core results within the FP32 rounding of
+the reference.  Skipped where the reference build is absent."""
+import numpy as np
+import pytest
+
+from fxb200 import synth
+from helpers import compare_core, rel_err, small_job
+
+import fxoracle
+import refcorr
+
+pytestmark = pytest.mark.skipif(not refcorr.available(), reason="reference build oracle/_ref absent")
+
+JOBS = {
+    "c0": dict(nstation=4),
+    "fullpol": dict(nstation=3, full_pol=True),
+    "order0": dict(nstation=3, order=0),
+    "order2": dict(nstation=3, order=2, seed=3),
+    "lsb_fraclo": dict(nstation=3, full_pol=True, lsb=True, freq0=8400.25),
+    "8bit": dict(nstation=3, nbits=8),
+    "avg4": dict(nstation=3, full_pol=True, avg=4),
+    "16ch_1024": dict(nstation=3, nchan=1024, bw=32.0, nfreq=8, full_pol=True, subint_ns=2_048_000),
+}
+
+
+@pytest.mark.parametrize("name", sorted(JOBS))
+def test_subint_matches_reference(name):
+    job = small_job(**JOBS[name])
+    ref = refcorr.RefCorrelator(job)
+    orc = fxoracle.OracleCorrelator(job)
+    assert np.array_equal(ref.layout(), orc.layout())
+    sec, ns = 0, 1_024_000
+    f0 = synth.subint_window(job, 0, sec, ns)[0]
+    invalid = {0: [f0 + 1]} if name in ("c0", "8bit") else None
+    inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=7, invalid=invalid)
+    vf = [synth.valid_flags(job) for _ in job.stations]
+    r = ref.process_subint(inputs, vf, 0, sec, ns)
+    o = orc.process_subint(inputs, sec, ns, validflags=vf)
+    for s in range(len(job.stations)):
+        assert np.array_equal(ref.interpolator(s, sec, ns), orc.interpolator(s, sec, ns))
+    compare_core(job, orc.layout(), orc.corelen, r.astype(np.float64), o, tol=2e-6)
+
+
+def test_mode_spectra_match_reference():
+    job = small_job(nstation=2, full_pol=True)
+    ref = refcorr.RefCorrelator(job)
+    orc = fxoracle.OracleCorrelator(job)
+    sec, ns = 0, 1_000_000
+    inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=9)
+    vf = synth.valid_flags(job)
+    for s in range(2):
+        buf, dsec, dns = inputs[s]
+        for t in (0, 3, 100, job.blocks_per_send() - 1):
+            rs, rw, _ = ref.mode_fft(s, buf, dsec, dns, vf, sec, ns, t)
+            os_, ow, _ = orc.mode_fft(s, buf, dsec, dns, sec, ns, t, validflags=vf)
+            assert rw == ow
+            assert rel_err(os_, rs) < 1e-6
+
+
+@pytest.mark.parametrize("nchan,nbits", [(1, 2), (2, 2), (4, 2), (8, 2), (16, 2), (32, 2), (64, 2),
+                                         (1, 8), (2, 8), (4, 8)])
+def test_vdif_decode_matches_mark5access(nchan, nbits):
+    from fxb200.job import Freq, Job, Station
+    st = Station("A", [(0, "R")] * nchan, nbits=nbits, payload_bytes=1024)
+    job = Job([Freq(1000.0, 1.024, 16)], [st], [], subint_ns=62_500)
+    synth.make_delay_polys(job, 1)
+    fs = job.frame_samples(0)
+    data = synth.gen_station_frames(job, 0, 0, 8, rho=0.1, seed=nchan + nbits, invalid=[3], fill=[5])
+    fmt = "VDIF_1024-%d-%d-%d" % (job.mbps(0), nchan, nbits)
+    for off, n in [(0, fs), (fs - 3, 10), (2 * fs + 1, fs + 5), (3 * fs - 7, 2 * fs)]:
+        gran = max(1, 8 // (nchan * nbits))
+        off -= off % gran
+        n -= n % gran
+        r, rgood = refcorr.unpack(fmt, data, off, n, nchan)
+        o, ogood = fxoracle.vdif_unpack(data, 1024, 32, nchan, nbits, off, n)
+        assert rgood == ogood, (off, n, rgood, ogood)
+        assert np.array_equal(r, o), (off, n)
