@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Throughput of the FX hot path on the 10-station production workload.
+
+Workload (config c1): 10 stations, eight 32 MHz bands, dual polarisation with
+full cross hands, 2-bit VDIF (8000-byte payload, 16 channels per frame),
+1024 channels (2048-point FFTs), 8 ms subintegrations, fringe rotation order 1.
+One step = 125 subintegrations = 1 s of data for every station.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fxb|reference]
+
+Prints one JSON line: value = station.MHz/s processed (whole job, all GPUs),
+with the real-time factor, the end-to-end figure through the C ABI with host
+buffers (host->device copies of the raw VDIF and the device->host read of the
+core result inside the timed region), the roofline of the dominant kernel,
+the reference CPU baseline and the SM clocks seen during the timed region.
+
+Inputs: a pool of 16 distinct subintegrations per station (bulk synthetic
+VDIF with the 2-bit quantiser's code statistics, 327 MB in device memory,
+larger than the 126 MB L2) cycled through in every step.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "difx-svn2git-try3_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+from fxb200 import configs, synth  # noqa: E402
+
+METRIC = "real-time factor & station.MHz/s (FX: unpack + fringe rotation + FFT + frac-sample + XMAC)"
+UNIT = "station.MHz/s"
+POOL = 16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fxb", choices=["fxb", "reference"])
+    ap.add_argument("--xmac", default="fp32", choices=["fp32", "bf16", "fp8"])
+    ap.add_argument("--subints-per-step", type=int, default=125)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def subint_time(job, k):
+    ns_total = k * job.subint_ns
+    return ns_total // 1_000_000_000, ns_total % 1_000_000_000
+
+
+def make_pool(job, npool, seed=1):
+    """Per pool entry: per station (bytes, datasec, datans) and the subint time."""
+    pool = []
+    for k in range(npool):
+        sec, ns = subint_time(job, k + 1)          # start one subint in: delays need earlier data
+        inputs = []
+        for s in range(len(job.stations)):
+            f0, nf, dsec, dns = synth.subint_window(job, s, sec, ns)
+            inputs.append((synth.bulk_station_frames(job, s, f0, nf, seed), dsec, dns))
+        pool.append(((sec, ns), inputs))
+    return pool
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.path) as fh:
+            for r in csv.reader(fh):
+                if len(r) >= 10:
+                    rows.append([x.strip() for x in r])
+        os.unlink(self.path)
+        if not rows:
+            return None
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return float("nan")
+        load = [r for r in rows if num(r[4]) >= 50.0] or rows
+        sm = [num(r[1]) for r in load if num(r[1]) == num(r[1])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in load for i in range(4) if r[6 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(rows[0][2]),
+                "samples": len(rows), "samples_under_load": len(load), "reasons": reasons,
+                "power_w_max": max(num(r[3]) for r in rows)}
+
+
+# ---------------------------------------------------------------- reference CPU path
+def cpu_reference(job, pool, seconds_target, nthreads):
+    """Time the reference's own compiled CPU path (oracle/_ref) on a bounded
+    sample of the workload; returns (station.MHz/s, cores, sample text, kind)."""
+    import refcorr
+    vf = [synth.valid_flags(job) for _ in job.stations]
+    if refcorr.available():
+        ref = refcorr.RefCorrelator(job, nthreads=nthreads)
+        (sec, ns), inputs = pool[0]
+        out = np.zeros(2 * ref.corelen, dtype=np.float32)
+        t0 = time.perf_counter()
+        ref.process_subint(inputs, vf, 0, sec, ns, coreresult=out, nthreads=nthreads)
+        one = time.perf_counter() - t0
+        n = max(1, min(len(pool) * 4, int(seconds_target / max(one, 1e-3))))
+        t0 = time.perf_counter()
+        for k in range(n):
+            (sec, ns), inputs = pool[k % len(pool)]
+            ref.process_subint(inputs, vf, 0, sec, ns, coreresult=out, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        ref.close()
+        kind = "reference"
+        cores = nthreads
+    else:
+        import fxoracle
+        orc = fxoracle.OracleCorrelator(job)
+        n = 1
+        (sec, ns), inputs = pool[0]
+        t0 = time.perf_counter()
+        orc.process_subint(inputs, sec, ns, validflags=vf)
+        dt = time.perf_counter() - t0
+        kind = "port"
+        cores = 1
+    data_s = n * job.subint_ns * 1e-9
+    value = job.station_mhz_per_sec() * data_s / dt
+    sample = "%d subints x %.0f ms of the workload (%.3f s of data), %.1f s wall" % (n, job.subint_ns / 1e6, data_s, dt)
+    return value, cores, sample, kind
+
+
+def reference_arm(args, job):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    pool = make_pool(job, 4)
+    nthreads = os.cpu_count() or 1
+    vals = []
+    t_all = []
+    for i in range(args.warmup + args.steps):
+        v, cores, sample, kind = cpu_reference(job, pool, max(2.0, args.cpu_seconds / max(1, args.steps)), nthreads)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    rtf = value / job.station_mhz_per_sec()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / rtf,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "rtf": rtf,
+        "config": workload_config(job),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(job):
+    return {"workload": "c1: 10 stations x 8 x 32 MHz x 2 pol (full cross hands), 2-bit VDIF 16ch, "
+                        "1024 channels, 8 ms subints, 1 s of data per step",
+            "stations": len(job.stations), "subbands": len(job.freqs), "bw_mhz": job.freqs[0].bw_mhz,
+            "nchan": job.freqs[0].nchan, "fringe_rot_order": job.fringe_rot_order,
+            "subint_ms": job.subint_ns / 1e6, "l2": "inputs larger than L2 (327 MB pool cycled)",
+            "parallelism": "time-sharded subints, one process per GPU"}
+
+
+def load_traffic(kernel):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh).get(kernel)
+    except Exception:
+        return None
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+# ---------------------------------------------------------------- GPU arm
+def gpu_arm(args, job):
+    import torch
+    import torch.distributed as dist
+    from fxb200.native import Correlator
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    pool = make_pool(job, POOL, seed=1 + rank)
+    S = len(job.stations)
+    dev = []        # [k][s] device tensors
+    host = []       # [k][s] pinned host tensors
+    for (_, inputs) in pool:
+        dev.append([torch.from_numpy(b).to("cuda") for b, _, _ in inputs])
+        host.append([torch.from_numpy(b).pin_memory() for b, _, _ in inputs])
+    nbytes = [[b.size for b, _, _ in inputs] for (_, inputs) in pool]
+    dsec = [[x for _, x, _ in inputs] for (_, inputs) in pool]
+    dns = [[x for _, _, x in inputs] for (_, inputs) in pool]
+    times = [t for (t, _) in pool]
+
+    corr = Correlator(job, xmac=args.xmac, inflight=3)
+    ext = torch.cuda.ExternalStream(corr.stream())
+    nsub = args.subints_per_step
+    core_dev = torch.zeros(2 * corr.corelen, dtype=torch.float32, device="cuda")
+
+    def step_device():
+        for j in range(nsub):
+            k = j % POOL
+            corr.submit_device([t.data_ptr() for t in dev[k]], nbytes[k], dsec[k], dns[k], times[k][0], times[k][1])
+        if world > 1:
+            corr.results_device(core_dev.data_ptr(), core_dev.numel())
+            with torch.cuda.stream(ext):
+                dist.reduce(core_dev, dst=0)
+
+    host_result = np.zeros(2 * corr.corelen, dtype=np.float32)
+
+    def step_host():
+        for j in range(nsub):
+            k = j % POOL
+            corr.submit_ptrs([t.data_ptr() for t in host[k]], nbytes[k], dsec[k], dns[k], times[k][0], times[k][1])
+        if world > 1:
+            corr.results_device(core_dev.data_ptr(), core_dev.numel())
+            with torch.cuda.stream(ext):
+                dist.reduce(core_dev, dst=0)
+        corr.results_into(host_result)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        corr.sync()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident throughput (value)
+    for _ in range(args.warmup):
+        step_device()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    corr.timing_enable(True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record(ext)
+    for _ in range(args.steps):
+        step_device()
+    ev1.record(ext)
+    ev1.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    nrec, prep_ms, f_ms, x_ms = corr.timing_read()
+    corr.timing_enable(False)
+    clk = clocks.stop()
+    ms = max_over_ranks(ms)
+    data_s = args.steps * nsub * job.subint_ns * 1e-9 * world
+    value = job.station_mhz_per_sec() * data_s / (ms * 1e-3)
+    rtf = data_s / (ms * 1e-3)
+
+    # ---- end-to-end through the C ABI with host buffers
+    corr.reset()
+    for _ in range(max(1, args.warmup // 2)):
+        step_host()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_host()
+    barrier()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3)
+    e2e_value = job.station_mhz_per_sec() * data_s / (e2e_ms * 1e-3)
+    h2d = sum(nbytes[j % POOL][s] for j in range(nsub) for s in range(S))
+    d2h = 2 * corr.corelen * 4
+
+    # ---- roofline of the dominant kernel
+    hbm_peak, tf_peak, peak_src = load_peaks()
+    T = job.blocks_per_send()
+    rows = sum(st.nband for st in job.stations)
+    in_bytes = sum(nbytes[k][s] for k in range(POOL) for s in range(S)) / POOL
+    spec_bytes = T * rows * job.freqs[0].nchan * 8
+    f_avg = f_ms / max(nrec, 1)
+    x_avg = x_ms / max(nrec, 1)
+    if f_avg >= x_avg:
+        kname = "k_fstage"
+        alg = in_bytes + spec_bytes
+        achieved = alg / (f_avg * 1e-3) / 1e9
+    else:
+        kname = "k_xmac_fp32"
+        alg = spec_bytes
+        achieved = alg / (x_avg * 1e-3) / 1e9
+    traffic = load_traffic(kname)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": alg,
+                "kernel_ms_per_subint": {"prep": prep_ms / max(nrec, 1), "fstage": f_avg, "xmac": x_avg}}
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, sample, kind = cpu_reference(job, pool, args.cpu_seconds, os.cpu_count() or 1)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    launches_per_subint = 5 + sum(1 for f in range(len(job.freqs)) if any(
+        fb == f for st in job.stations for fb, _ in st.bands))
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"fp32": "f32", "bf16": "bf16", "fp8": "fp8e4m3"}[args.xmac],
+            "data": "synthetic", "rtf": rtf, "xmac": args.xmac,
+            "config": workload_config(job),
+            "e2e": {"value": e2e_value, "unit": UNIT, "rtf": e2e_value / job.station_mhz_per_sec(),
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps},
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": launches_per_subint * nsub * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    corr.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    job = configs.c1()
+    if args.impl == "reference":
+        reference_arm(args, job)
+    else:
+        gpu_arm(args, job)
+
+
+if __name__ == "__main__":
+    main()

@@ -57,8 +57,12 @@ struct fxb_ctx {
 	int64_t valid_stride = 0;
 	std::vector<Slot> slots;
 	int next_slot = 0;
-	cudaEvent_t ev_f0 = nullptr, ev_f1 = nullptr, ev_x1 = nullptr;
+	cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_c = nullptr, ev_d = nullptr;
 	bool timed = false;
+	// per-subint kernel timing (fxb_timing_enable / fxb_timing_read)
+	bool timing_on = false;
+	std::vector<cudaEvent_t> tev;       // 4 per recorded subint
+	size_t tev_used = 0;
 	std::vector<bool> delay_set;
 };
 
@@ -120,9 +124,10 @@ static void free_ctx(fxb_ctx *ctx)
 		if(s.copied) cudaEventDestroy(s.copied);
 		if(s.done) cudaEventDestroy(s.done);
 	}
-	if(ctx->ev_f0) cudaEventDestroy(ctx->ev_f0);
-	if(ctx->ev_f1) cudaEventDestroy(ctx->ev_f1);
-	if(ctx->ev_x1) cudaEventDestroy(ctx->ev_x1);
+	for(cudaEvent_t e : {ctx->ev_a, ctx->ev_b, ctx->ev_c, ctx->ev_d})
+		if(e) cudaEventDestroy(e);
+	for(cudaEvent_t e : ctx->tev)
+		if(e) cudaEventDestroy(e);
 	if(ctx->stream) cudaStreamDestroy(ctx->stream);
 	if(ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
 	delete ctx;
@@ -134,9 +139,10 @@ static fxb_status setup_device(fxb_ctx *ctx)
 	CK(ctx, cudaGetDevice(&ctx->device));
 	CK(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
 	CK(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-	CK(ctx, cudaEventCreate(&ctx->ev_f0));
-	CK(ctx, cudaEventCreate(&ctx->ev_f1));
-	CK(ctx, cudaEventCreate(&ctx->ev_x1));
+	CK(ctx, cudaEventCreate(&ctx->ev_a));
+	CK(ctx, cudaEventCreate(&ctx->ev_b));
+	CK(ctx, cudaEventCreate(&ctx->ev_c));
+	CK(ctx, cudaEventCreate(&ctx->ev_d));
 	ctx->S = (int)job.stations.size();
 	ctx->T = job.blockspersend;
 	ctx->F = (int)job.freqs.size();
@@ -438,20 +444,37 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 	CK(ctx, cudaStreamWaitEvent(ctx->stream, sl.copied, 0));
 
 	cudaStream_t st = ctx->stream;
-	CK(ctx, cudaEventRecord(ctx->ev_f0, st));
+	cudaEvent_t *tv = nullptr;
+	if(ctx->timing_on && ctx->tev_used + 4 <= 4 * 8192)
+	{
+		while(ctx->tev.size() < ctx->tev_used + 4)
+		{
+			cudaEvent_t e;
+			CK(ctx, cudaEventCreate(&e));
+			ctx->tev.push_back(e);
+		}
+		tv = &ctx->tev[ctx->tev_used];
+		ctx->tev_used += 4;
+	}
+	CK(ctx, cudaEventRecord(ctx->ev_a, st));
+	if(tv) CK(ctx, cudaEventRecord(tv[0], st));
 	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, sec, ns, st);
 	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->valid_stride, ctx->S, st);
 	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->valid_stride, ctx->S, ctx->T,
 	                  sec, ns, job.fringe_rot_order, ctx->d_params, st);
+	CK(ctx, cudaEventRecord(ctx->ev_b, st));
+	if(tv) CK(ctx, cudaEventRecord(tv[1], st));
 	launch_fstage(ctx->d_st, sl.d_sub, ctx->d_bands, ctx->maxband, ctx->d_plans, ctx->d_valid, ctx->valid_stride,
 	              ctx->d_params, ctx->d_twiddle, ctx->maxN, ctx->S, ctx->T, job.fringe_rot_order, job.fractionallofreq,
 	              ctx->maxfft, ctx->d_spec, st);
-	CK(ctx, cudaEventRecord(ctx->ev_f1, st));
+	CK(ctx, cudaEventRecord(ctx->ev_c, st));
+	if(tv) CK(ctx, cudaEventRecord(tv[2], st));
 	for(int f = 0; f < ctx->F; f++)
 		if(ctx->h_plans[f].nrow > 0)
 			launch_xmac_fp32(ctx->h_plans[f], ctx->d_plans + f, ctx->T, ctx->d_spec, ctx->d_acc, st);
 	launch_weights(ctx->d_bw, ctx->nbw, ctx->d_acw, ctx->nacw, ctx->d_params, ctx->T, ctx->d_bwacc, ctx->d_acwacc, st);
-	CK(ctx, cudaEventRecord(ctx->ev_x1, st));
+	CK(ctx, cudaEventRecord(ctx->ev_d, st));
+	if(tv) CK(ctx, cudaEventRecord(tv[3], st));
 	CK(ctx, cudaGetLastError());
 	CK(ctx, cudaEventRecord(sl.done, st));
 	ctx->timed = true;
@@ -554,13 +577,67 @@ fxb_status fxb_last_timing(const fxb_ctx *ctx, float *fstage_ms, float *xmac_ms,
 {
 	if(!ctx || !ctx->timed) return FXB_ERR_STATE;
 	fxb_ctx *c = const_cast<fxb_ctx *>(ctx);
-	CK(c, cudaEventSynchronize(ctx->ev_x1));
-	float a = 0, b = 0;
-	CK(c, cudaEventElapsedTime(&a, ctx->ev_f0, ctx->ev_f1));
-	CK(c, cudaEventElapsedTime(&b, ctx->ev_f1, ctx->ev_x1));
+	CK(c, cudaEventSynchronize(ctx->ev_d));
+	float a = 0, b = 0, t = 0;
+	CK(c, cudaEventElapsedTime(&a, ctx->ev_b, ctx->ev_c));
+	CK(c, cudaEventElapsedTime(&b, ctx->ev_c, ctx->ev_d));
+	CK(c, cudaEventElapsedTime(&t, ctx->ev_a, ctx->ev_d));
 	if(fstage_ms) *fstage_ms = a;
 	if(xmac_ms) *xmac_ms = b;
-	if(total_ms) *total_ms = a + b;
+	if(total_ms) *total_ms = t;
+	return FXB_OK;
+}
+
+fxb_status fxb_timing_enable(fxb_ctx *ctx, int32_t on)
+{
+	if(!ctx) return FXB_ERR_ARG;
+	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	ctx->timing_on = on != 0;
+	ctx->tev_used = 0;
+	return FXB_OK;
+}
+
+fxb_status fxb_timing_read(fxb_ctx *ctx, int32_t *nsubint, double *prep_ms, double *fstage_ms, double *xmac_ms)
+{
+	if(!ctx) return FXB_ERR_ARG;
+	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	double p = 0, f = 0, x = 0;
+	for(size_t i = 0; i + 4 <= ctx->tev_used; i += 4)
+	{
+		float a = 0, b = 0, c = 0;
+		CK(ctx, cudaEventElapsedTime(&a, ctx->tev[i], ctx->tev[i + 1]));
+		CK(ctx, cudaEventElapsedTime(&b, ctx->tev[i + 1], ctx->tev[i + 2]));
+		CK(ctx, cudaEventElapsedTime(&c, ctx->tev[i + 2], ctx->tev[i + 3]));
+		p += a;
+		f += b;
+		x += c;
+	}
+	if(nsubint) *nsubint = (int32_t)(ctx->tev_used / 4);
+	if(prep_ms) *prep_ms = p;
+	if(fstage_ms) *fstage_ms = f;
+	if(xmac_ms) *xmac_ms = x;
+	ctx->tev_used = 0;
+	return FXB_OK;
+}
+
+fxb_status fxb_get_stream(const fxb_ctx *ctx, void **stream)
+{
+	if(!ctx || !stream) return FXB_ERR_ARG;
+	*stream = (void *)ctx->stream;
+	return FXB_OK;
+}
+
+fxb_status fxb_read_results_device(fxb_ctx *ctx, float *dev_out, size_t nfloats)
+{
+	if(!ctx || !dev_out) return FXB_ERR_ARG;
+	if(nfloats < (size_t)(2 * ctx->job.corelen))
+	{
+		ctx->err = "result buffer too small";
+		return FXB_ERR_ARG;
+	}
+	launch_finalise(ctx->d_om, ctx->nom, 0, ctx->d_acc, ctx->d_bw, ctx->nbw, ctx->d_bwacc, ctx->d_acw, ctx->nacw,
+	                ctx->d_acwacc, (float2 *)dev_out, ctx->job.corelen, ctx->stream);
+	CK(ctx, cudaGetLastError());
 	return FXB_OK;
 }
 

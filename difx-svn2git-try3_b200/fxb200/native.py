@@ -140,9 +140,14 @@ def lib():
     L.fxb_read_fft_weights.argtypes = [vp, fp, ctypes.c_size_t]
     L.fxb_vdif_unpack.argtypes = [ctypes.c_void_p, i64, i32, i32, i32, i32, i64, i32, fp, i32p]
     L.fxb_job_layout.argtypes = [ctypes.POINTER(FxbJobDesc), i32p, ctypes.c_size_t, i64p]
+    L.fxb_timing_enable.argtypes = [vp, i32]
+    L.fxb_timing_read.argtypes = [vp, i32p, dp, dp, dp]
+    L.fxb_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
+    L.fxb_read_results_device.argtypes = [vp, ctypes.c_void_p, ctypes.c_size_t]
     for name in ("fxb_set_delay_poly", "fxb_submit_subint", "fxb_submit_subint_device", "fxb_sync",
                  "fxb_core_result_length", "fxb_layout", "fxb_read_results", "fxb_reset", "fxb_last_timing",
-                 "fxb_read_spectra", "fxb_read_fft_weights", "fxb_vdif_unpack", "fxb_job_layout"):
+                 "fxb_read_spectra", "fxb_read_fft_weights", "fxb_vdif_unpack", "fxb_job_layout",
+                 "fxb_timing_enable", "fxb_timing_read", "fxb_get_stream", "fxb_read_results_device"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -222,6 +227,15 @@ class Correlator:
                       validflags=None) -> None:
         self._submit(lib().fxb_submit_subint_device, ptrs, nbytes, dsec, dns, validflags, sec, ns)
 
+    def submit_ptrs(self, ptrs: Sequence[int], nbytes: Sequence[int], dsec, dns, sec: int, ns: int,
+                    validflags=None) -> None:
+        """Submit from host memory given raw pointers (e.g. pinned buffers)."""
+        self._submit(lib().fxb_submit_subint, ptrs, nbytes, dsec, dns, validflags, sec, ns)
+
+    def results_into(self, out: np.ndarray) -> np.ndarray:
+        check(lib().fxb_read_results(self.ctx, _fptr(out), out.size), self.ctx, "read_results")
+        return out
+
     def sync(self):
         check(lib().fxb_sync(self.ctx), self.ctx, "sync")
 
@@ -237,6 +251,25 @@ class Correlator:
         a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
         check(lib().fxb_last_timing(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), self.ctx, "timing")
         return a.value, b.value, c.value
+
+    def timing_enable(self, on: bool = True):
+        check(lib().fxb_timing_enable(self.ctx, 1 if on else 0), self.ctx, "timing_enable")
+
+    def timing_read(self):
+        n = ctypes.c_int32(0)
+        p, f, x = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(lib().fxb_timing_read(self.ctx, ctypes.byref(n), ctypes.byref(p), ctypes.byref(f), ctypes.byref(x)),
+              self.ctx, "timing_read")
+        return n.value, p.value, f.value, x.value
+
+    def stream(self) -> int:
+        v = ctypes.c_void_p(0)
+        check(lib().fxb_get_stream(self.ctx, ctypes.byref(v)), self.ctx, "get_stream")
+        return v.value or 0
+
+    def results_device(self, dev_ptr: int, nfloats: int):
+        check(lib().fxb_read_results_device(self.ctx, ctypes.c_void_p(dev_ptr), nfloats), self.ctx,
+              "read_results_device")
 
     def spectra(self, freq: int) -> np.ndarray:
         T = self.job.blocks_per_send()

@@ -198,3 +198,42 @@ def valid_flags(job: Job, all_valid: bool = True, invalid_ffts: Sequence[int] = 
         if all_valid and i not in invalid_ffts:
             v[i // 30] |= (1 << (i % 30))
     return v
+
+
+# ---------------------------------------------------------------- bulk data
+def _code_byte_table(nbits: int) -> np.ndarray:
+    """65536-entry table whose uniform sampling yields payload bytes with the
+    code statistics of the quantiser on unit-variance Gaussian input: for
+    2-bit, four independent fields with P(outer) = 2*Phi(-0.98) each."""
+    from math import erf, sqrt
+    if nbits == 2:
+        p0 = 0.5 * (1.0 + erf(-THRESH / sqrt(2.0)))       # P(x < -0.98)
+        pc = np.array([p0, 0.5 - p0, 0.5 - p0, p0])
+        probs = np.ones(256)
+        for b in range(256):
+            for i in range(4):
+                probs[b] *= pc[(b >> (2 * i)) & 3]
+    else:
+        x = (np.arange(256) - 128) / 10.0
+        probs = np.exp(-0.5 * x * x)
+        probs /= probs.sum()
+    counts = np.floor(probs * 65536).astype(np.int64)
+    short = 65536 - counts.sum()
+    order = np.argsort(-(probs * 65536 - counts))
+    counts[order[:short]] += 1
+    return np.repeat(np.arange(256, dtype=np.uint8), counts)
+
+
+def bulk_station_frames(job: Job, s: int, frame0: int, nframes: int, seed: int) -> np.ndarray:
+    """nframes VDIF frames with valid headers whose payload bytes follow the
+    quantiser's code statistics (uncorrelated across stations): the bulk
+    stand-in input for throughput measurement."""
+    st = job.stations[s]
+    fb = job.frame_bytes(s)
+    table = _code_byte_table(st.nbits)
+    rng = _rng("bulk", seed, s, frame0)
+    out = np.empty((nframes, fb), dtype=np.uint8)
+    out[:, VDIF_HEADER:] = table[rng.integers(0, 65536, size=(nframes, st.payload_bytes), dtype=np.uint16)]
+    for k in range(nframes):
+        out[k, :VDIF_HEADER] = vdif_header(job, s, frame0 + k, station_id=s)
+    return out.reshape(-1)

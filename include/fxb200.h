@@ -169,6 +169,24 @@ FXB_API fxb_status fxb_reset(fxb_ctx *ctx);
  * measured with CUDA events on the context's stream. */
 FXB_API fxb_status fxb_last_timing(const fxb_ctx *ctx, float *fstage_ms, float *xmac_ms, float *total_ms);
 
+/* Per-subint kernel timing: while enabled, every submitted subint records
+ * CUDA events on the context's stream; fxb_timing_read synchronises and
+ * returns the number of subints and the summed device time of the FP64
+ * delay/parameter kernels (prep), the F-stage kernel and the XMAC + weight
+ * kernels, then clears the record. */
+FXB_API fxb_status fxb_timing_enable(fxb_ctx *ctx, int32_t on);
+FXB_API fxb_status fxb_timing_read(fxb_ctx *ctx, int32_t *nsubint, double *prep_ms, double *fstage_ms,
+                                   double *xmac_ms);
+
+/* The cudaStream_t (as void*) on which the context launches its kernels,
+ * so that callers can order their own work and events against it. */
+FXB_API fxb_status fxb_get_stream(const fxb_ctx *ctx, void **stream);
+
+/* As fxb_read_results, but the core result is written asynchronously (on
+ * the context's stream) into device memory, e.g. for a cross-GPU reduction
+ * of time-sharded subints. */
+FXB_API fxb_status fxb_read_results_device(fxb_ctx *ctx, float *dev_out, size_t nfloats);
+
 /* F-stage output of the last subint for one frequency: spectra[t][row][c]
  * complex (FP32, converted from the XMAC operand type), rows = the
  * (station, band) inputs recording that frequency in station order.
