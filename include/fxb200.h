@@ -208,6 +208,30 @@ FXB_API fxb_status fxb_vdif_unpack(const uint8_t *data, int64_t nbytes, int32_t 
                            int32_t nchan, int32_t nbits, int64_t offsetsamples, int32_t nsamp,
                            float *out, int32_t *good);
 
+/* Per-station F stage that allocates nothing (no counterpart in the
+ * reference: DiFX's Mode allocates its buffers in its constructor).  For
+ * callers that cannot call cudaMalloc -- a process whose device memory is all
+ * pre-assigned to its own pool, or a real-time pipeline that forbids
+ * allocation after set-up.  The caller owns every buffer: dev_vdif (the
+ * station's VDIF frames, device memory), dev_spectra (output,
+ * [fft][band][nchan] complex FP32, device memory) and dev_weights (output,
+ * per-FFT data weight, device memory, may be NULL).  All intermediates live
+ * in one fixed file-scope device array of under 1 MiB, so the call refuses
+ * (FXB_ERR_UNSUPPORTED) jobs beyond 8192 FFTs per subint, 131072 frames per
+ * buffer or 4096 channels.  The array is shared by every call on a device:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * Its device address is looked up on the first call on each device, which
+ * should therefore come before any stream capture.  Arguments otherwise mean
+ * what they mean for fxb_job_desc, fxb_set_delay_poly and fxb_submit_subint
+ * (one station).  Returns when the work on `stream` has completed. */
+FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, int32_t nfreq, const fxb_station *station,
+                                              int32_t fringe_rot_order, int64_t subint_ns, int32_t npoly,
+                                              int32_t order, double poly0_sec, int32_t interval_s,
+                                              const double *coeffs, const uint8_t *dev_vdif, int64_t nbytes,
+                                              int32_t datasec, int32_t datans, const int32_t *validflags,
+                                              int32_t sec, int32_t ns, float *dev_spectra, float *dev_weights,
+                                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif
