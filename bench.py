@@ -334,11 +334,11 @@ def gpu_arm(args, job):
     f_avg = f_ms / max(nrec, 1)
     x_avg = x_ms / max(nrec, 1)
     if f_avg >= x_avg:
-        kname = "k_fstage"
+        kname = "k_fstage2"
         alg = in_bytes + spec_bytes
         achieved = alg / (f_avg * 1e-3) / 1e9
     else:
-        kname = "k_xmac_fp32"
+        kname = "k_xmac_fp32v2"
         alg = spec_bytes
         achieved = alg / (x_avg * 1e-3) / 1e9
     traffic = load_traffic(kname)
@@ -353,8 +353,11 @@ def gpu_arm(args, job):
         v, cores, sample, kind = cpu_reference(job, pool, args.cpu_seconds, os.cpu_count() or 1)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
-    launches_per_subint = 5 + sum(1 for f in range(len(job.freqs)) if any(
-        fb == f for st in job.stations for fb, _ in st.bands))
+    # per subint: interpolators, frame validity, FFT parameters, F stage,
+    # one XMAC launch per group of equally shaped subbands, weights
+    shapes = {(sum(1 for st in job.stations for fb, _ in st.bands if fb == f), job.freqs[f].nchan)
+              for f in range(len(job.freqs)) if any(fb == f for st in job.stations for fb, _ in st.bands)}
+    launches_per_subint = 5 + len(shapes)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -64,6 +64,11 @@ struct fxb_ctx {
 	std::vector<cudaEvent_t> tev;       // 4 per recorded subint
 	size_t tev_used = 0;
 	std::vector<bool> delay_set;
+	// F stage v2 work items and FP32 XMAC v2 launch groups
+	void *d_groups = nullptr;
+	int ngroups = 0, nbufmax = 2, rawnband = 1, TQ = 8;
+	struct XGroup { int plan0; int32_t *d_idx; int nf; };
+	std::vector<XGroup> xgroups;
 };
 
 static std::mutex g_err_mutex;
@@ -207,8 +212,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 
 	// twiddles exp(-2 pi i k / maxN), computed in double
 	{
-		std::vector<float2> tw(ctx->maxN / 2);
-		for(int k = 0; k < ctx->maxN / 2; k++)
+		std::vector<float2> tw(ctx->maxN);
+		for(int k = 0; k < ctx->maxN; k++)
 		{
 			double ang = -2.0 * M_PI * (double)k / (double)ctx->maxN;
 			tw[k] = make_float2((float)cos(ang), (float)sin(ang));
@@ -231,6 +236,10 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		d.npair = d.ntr * (d.ntr + 1) / 2;
 		d.spec_off = p.spec_off;
 		d.acc_off = p.acc_off;
+		d.r2pad = (2 * p.nrow + 7) & ~7;
+		d.tpad = (ctx->T + 63) & ~63;
+		d.acc_cstride = 1;
+		d.acc_ostride = p.nchan;
 		int32_t *dA, *dB;
 		int16_t *pairs;
 		CK(ctx, dalloc(ctx, &dA, p.destA.size()));
@@ -252,6 +261,75 @@ static fxb_status setup_device(fxb_ctx *ctx)
 	}
 	CK(ctx, dalloc(ctx, &ctx->d_plans, ctx->F));
 	CK(ctx, cudaMemcpy(ctx->d_plans, ctx->h_plans.data(), sizeof(DevFreqPlan) * ctx->F, cudaMemcpyHostToDevice));
+
+	// F-stage work items: (station, subband) with up to two bands each
+	{
+		ctx->nbufmax = ctx->maxN <= 8192 ? 2 : 1;
+		int64_t maxrawbits = 0;
+		std::vector<unsigned char> hg;
+		const size_t gsz = fgroup_size();
+		for(int s = 0; s < ctx->S; s++)
+		{
+			const Job::Station &js = job.stations[s];
+			maxrawbits = std::max<int64_t>(maxrawbits, (int64_t)ctx->h_st[s].fftchannels * js.nband * js.nbits);
+			std::vector<int> done(js.nband, 0);
+			for(int b = 0; b < js.nband; b++)
+			{
+				if(done[b] || job.band_row[s][b] < 0)
+					continue;
+				int f = js.band_freq[b];
+				int b1 = -1;
+				if(ctx->nbufmax == 2)
+					for(int c = b + 1; c < js.nband; c++)
+						if(!done[c] && js.band_freq[c] == f && job.band_row[s][c] >= 0)
+						{
+							b1 = c;
+							break;
+						}
+				done[b] = 1;
+				if(b1 >= 0) done[b1] = 1;
+				size_t off = hg.size();
+				hg.resize(off + gsz);
+				make_fgroup(hg.data() + off, s, f, b, b1, job.band_row[s][b], b1 >= 0 ? job.band_row[s][b1] : -1,
+				            job.freqs[f].lower_sideband, job.freqs[f].freq_mhz);
+				ctx->ngroups++;
+			}
+		}
+		ctx->rawnband = (int)((maxrawbits + ctx->maxN - 1) / ctx->maxN);
+		unsigned char *dg = nullptr;
+		CK(ctx, dalloc(ctx, &dg, std::max<size_t>(hg.size(), 1)));
+		if(!hg.empty())
+			CK(ctx, cudaMemcpy(dg, hg.data(), hg.size(), cudaMemcpyHostToDevice));
+		ctx->d_groups = dg;
+	}
+	// FP32 XMAC launch groups: frequencies with equal shape share a launch
+	{
+		std::vector<int> used;
+		for(int f = 0; f < ctx->F; f++)
+			if(ctx->h_plans[f].nrow > 0) used.push_back(f);
+		std::vector<int> taken(used.size(), 0);
+		for(size_t i = 0; i < used.size(); i++)
+		{
+			if(taken[i]) continue;
+			const DevFreqPlan &a = ctx->h_plans[used[i]];
+			std::vector<int32_t> idx;
+			for(size_t j = i; j < used.size(); j++)
+			{
+				const DevFreqPlan &b = ctx->h_plans[used[j]];
+				if(!taken[j] && b.nrow == a.nrow && b.nchan == a.nchan)
+				{
+					taken[j] = 1;
+					idx.push_back(used[j]);
+				}
+			}
+			fxb_ctx::XGroup g;
+			g.plan0 = used[i];
+			g.nf = (int)idx.size();
+			CK(ctx, dalloc(ctx, &g.d_idx, idx.size()));
+			CK(ctx, cudaMemcpy(g.d_idx, idx.data(), sizeof(int32_t) * idx.size(), cudaMemcpyHostToDevice));
+			ctx->xgroups.push_back(g);
+		}
+	}
 
 	// big buffers
 	CK(ctx, dalloc(ctx, &ctx->d_params, (size_t)ctx->S * ctx->T));
@@ -464,14 +542,14 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 	                  sec, ns, job.fringe_rot_order, ctx->d_params, st);
 	CK(ctx, cudaEventRecord(ctx->ev_b, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[1], st));
-	launch_fstage(ctx->d_st, sl.d_sub, ctx->d_bands, ctx->maxband, ctx->d_plans, ctx->d_valid, ctx->valid_stride,
-	              ctx->d_params, ctx->d_twiddle, ctx->maxN, ctx->S, ctx->T, job.fringe_rot_order, job.fractionallofreq,
-	              ctx->maxfft, ctx->d_spec, st);
+	if(ctx->ngroups > 0)
+		launch_fstage2(ctx->d_st, sl.d_sub, ctx->d_groups, ctx->ngroups, ctx->d_plans, ctx->d_valid, ctx->valid_stride,
+		               ctx->d_params, ctx->d_twiddle, ctx->maxN, ctx->T, ctx->TQ, 0, job.fringe_rot_order,
+		               job.fractionallofreq, ctx->maxN, ctx->rawnband, 1, ctx->nbufmax, 0, ctx->d_spec, st);
 	CK(ctx, cudaEventRecord(ctx->ev_c, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[2], st));
-	for(int f = 0; f < ctx->F; f++)
-		if(ctx->h_plans[f].nrow > 0)
-			launch_xmac_fp32(ctx->h_plans[f], ctx->d_plans + f, ctx->T, ctx->d_spec, ctx->d_acc, st);
+	for(const auto &g : ctx->xgroups)
+		launch_xmac_fp32v2(ctx->h_plans[g.plan0], ctx->d_plans, g.d_idx, g.nf, ctx->T, ctx->d_spec, ctx->d_acc, st);
 	launch_weights(ctx->d_bw, ctx->nbw, ctx->d_acw, ctx->nacw, ctx->d_params, ctx->T, ctx->d_bwacc, ctx->d_acwacc, st);
 	CK(ctx, cudaEventRecord(ctx->ev_d, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[3], st));

@@ -11,6 +11,10 @@ namespace fxb {
 // Per-frequency XMAC plan on the device.
 struct DevFreqPlan {
 	int32_t nrow, nchan, ntr, npair;  // rows, channels, 4-row tiles, tile pairs
+	int32_t r2pad;                    // real rows per channel of the K-major BF16 spectra (2*nrow rounded up to 8)
+	int32_t tpad;                     // FFTs per subint rounded up to the K tile (64)
+	int32_t acc_cstride;              // accumulator stride between channels (1: [out][chan], nout: [chan][out])
+	int32_t acc_ostride;              // accumulator stride between outputs
 	int64_t spec_off;                 // complex offset of spectra [T][nrow][nchan]
 	int64_t acc_off;                  // complex offset of accumulators [nout][nchan]
 	const int32_t *destA;             // [nrow*nrow]
@@ -47,6 +51,20 @@ void launch_fstage(const DevStation *st, const DevSubintStation *sub, const DevB
                    const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride, const FftParam *params,
                    const float2 *twiddle, int maxN, int S, int T, int order, bool fractionallofreq, int maxfft,
                    float2 *spec, cudaStream_t stream);
+
+// F stage v2 (csrc/fxb_fstage.cu): CTA per (station, subband, chunk of TQ FFTs).
+// out 0: FP32 rows [t][row][chan]; out 1: BF16 K-major [chan][2 row + part][tpad].
+void launch_fstage2(const DevStation *st, const DevSubintStation *sub, const void *groups, int ngroups,
+                    const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride, const FftParam *params,
+                    const float2 *twiddle, int maxN, int T, int TQ, int Tpad, int order, bool fractionallofreq,
+                    int N, int nband_max, int nbits_max, int nbufmax, int out, void *spec, cudaStream_t stream);
+size_t fgroup_size();
+void make_fgroup(void *dst, int station, int freq, int b0, int b1, int r0, int r1, int lsb, double lofreq);
+
+// FP32 XMAC v2 over a set of frequencies with equal (rows, channels):
+// plan_idx[0..nf) index dplans.
+void launch_xmac_fp32v2(const DevFreqPlan &plan0, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int T,
+                        const float2 *spec, float2 *acc, cudaStream_t stream);
 
 // FP32 cross-multiply-accumulate of one frequency into acc.
 void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, const float2 *spec, float2 *acc,
