@@ -69,6 +69,14 @@ struct fxb_ctx {
 	int ngroups = 0, nbufmax = 2, rawnband = 1, TQ = 8;
 	struct XGroup { int plan0; int32_t *d_idx; int nf; };
 	std::vector<XGroup> xgroups;
+	// tensor-core (BF16) XMAC state
+	bool tc = false;
+	int Tpad = 0;
+	void *d_spec_bf16 = nullptr;
+	int64_t spec_bf16_elems = 0;
+	int64_t *d_rowbase = nullptr;
+	unsigned char tmap[128];
+	int32_t *d_err = nullptr;
 };
 
 static std::mutex g_err_mutex;
@@ -259,8 +267,67 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		d.destB = dB;
 		d.pairs = pairs;
 	}
+	// tensor-core form: BF16 K-major spectra [chan][R2][Tpad] per frequency and
+	// [chan][output] accumulators
+	ctx->tc = job.xmac_kind == FXB_XMAC_BF16;
+	ctx->Tpad = (ctx->T + 63) & ~63;
+	if(job.xmac_kind == FXB_XMAC_FP8)
+	{
+		ctx->err = "the FP8 XMAC is not available in this build";
+		return FXB_ERR_UNSUPPORTED;
+	}
+	std::vector<int64_t> rowbase(ctx->F, 0);
+	if(ctx->tc)
+	{
+		int64_t off = 0;
+		for(int f = 0; f < ctx->F; f++)
+		{
+			DevFreqPlan &d = ctx->h_plans[f];
+			if(d.nrow == 0) continue;
+			if(d.r2pad > 128 || d.nchan > 2048)
+			{
+				ctx->err = "tensor-core XMAC: at most 64 inputs and 2048 channels per subband";
+				return FXB_ERR_UNSUPPORTED;
+			}
+			d.spec_off = off;
+			rowbase[f] = off / ctx->Tpad;
+			off += (int64_t)d.nchan * d.r2pad * ctx->Tpad;
+			d.acc_ostride = 1;
+			d.acc_cstride = job.plan[f].nout;
+		}
+		ctx->spec_bf16_elems = off;
+	}
 	CK(ctx, dalloc(ctx, &ctx->d_plans, ctx->F));
 	CK(ctx, cudaMemcpy(ctx->d_plans, ctx->h_plans.data(), sizeof(DevFreqPlan) * ctx->F, cudaMemcpyHostToDevice));
+	if(ctx->tc)
+	{
+		unsigned char *sp = nullptr;
+		CK(ctx, dalloc(ctx, &sp, (size_t)ctx->spec_bf16_elems * 2 + 4096));
+		CK(ctx, cudaMemset(sp, 0, (size_t)ctx->spec_bf16_elems * 2 + 4096));
+		ctx->d_spec_bf16 = sp;
+		CK(ctx, dalloc(ctx, &ctx->d_rowbase, ctx->F));
+		CK(ctx, cudaMemcpy(ctx->d_rowbase, rowbase.data(), sizeof(int64_t) * ctx->F, cudaMemcpyHostToDevice));
+		CK(ctx, dalloc(ctx, &ctx->d_err, 1));
+		CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
+		int r2 = 0;
+		for(int f = 0; f < ctx->F; f++)
+			if(ctx->h_plans[f].nrow) r2 = ctx->h_plans[f].r2pad;
+		int G, NG, boxrows, cols;
+		size_t smem;
+		tc_geometry(r2, ctx->Tpad, &G, &NG, &boxrows, &cols, &smem);
+		if(tc_tensormap_size() > sizeof(ctx->tmap) ||
+		   !tc_make_tensormap(ctx->tmap, sp, ctx->spec_bf16_elems / ctx->Tpad, ctx->Tpad, boxrows))
+		{
+			ctx->err = "cuTensorMapEncodeTiled failed for the spectra buffer";
+			return FXB_ERR_CUDA;
+		}
+		for(int f = 0; f < ctx->F; f++)
+			if(ctx->h_plans[f].nrow && ctx->h_plans[f].r2pad != r2)
+			{
+				ctx->err = "tensor-core XMAC: all subbands must have the same number of inputs";
+				return FXB_ERR_UNSUPPORTED;
+			}
+	}
 
 	// F-stage work items: (station, subband) with up to two bands each
 	{
@@ -333,7 +400,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 
 	// big buffers
 	CK(ctx, dalloc(ctx, &ctx->d_params, (size_t)ctx->S * ctx->T));
-	CK(ctx, dalloc(ctx, &ctx->d_spec, (size_t)job.spec_total));
+	CK(ctx, dalloc(ctx, &ctx->d_spec, job.xmac_kind == FXB_XMAC_FP32 ? (size_t)job.spec_total : 1));
 	CK(ctx, dalloc(ctx, &ctx->d_acc, (size_t)job.acc_total));
 	CK(ctx, dalloc(ctx, &ctx->d_core, (size_t)job.corelen));
 	ctx->nbw = (int)job.bweights.size();
@@ -350,7 +417,17 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			hacw[i] = DevACWeight{job.acweights[i].s, 0, job.acweights[i].dst_float};
 		std::vector<DevOutMap> hom(ctx->nom);
 		for(int i = 0; i < ctx->nom; i++)
-			hom[i] = DevOutMap{job.outmap[i].acc, job.outmap[i].core, job.outmap[i].nchan, job.outmap[i].avg};
+		{
+			const Job::OutMap &m = job.outmap[i];
+			int64_t a = m.acc;
+			int cs = 1;
+			if(ctx->tc && m.out >= 0)
+			{
+				a = job.plan[m.freq].acc_off + m.out;
+				cs = job.plan[m.freq].nout;
+			}
+			hom[i] = DevOutMap{a, m.core, m.nchan, m.avg, cs, 0};
+		}
 		CK(ctx, dalloc(ctx, &ctx->d_bw, ctx->nbw));
 		CK(ctx, dalloc(ctx, &ctx->d_acw, ctx->nacw));
 		CK(ctx, dalloc(ctx, &ctx->d_om, ctx->nom));
@@ -544,12 +621,19 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 	if(tv) CK(ctx, cudaEventRecord(tv[1], st));
 	if(ctx->ngroups > 0)
 		launch_fstage2(ctx->d_st, sl.d_sub, ctx->d_groups, ctx->ngroups, ctx->d_plans, ctx->d_valid, ctx->valid_stride,
-		               ctx->d_params, ctx->d_twiddle, ctx->maxN, ctx->T, ctx->TQ, 0, job.fringe_rot_order,
-		               job.fractionallofreq, ctx->maxN, ctx->rawnband, 1, ctx->nbufmax, 0, ctx->d_spec, st);
+		               ctx->d_params, ctx->d_twiddle, ctx->maxN, ctx->T, ctx->TQ, ctx->Tpad, job.fringe_rot_order,
+		               job.fractionallofreq, ctx->maxN, ctx->rawnband, 1, ctx->nbufmax, ctx->tc ? 1 : 0,
+		               ctx->tc ? ctx->d_spec_bf16 : (void *)ctx->d_spec, st);
 	CK(ctx, cudaEventRecord(ctx->ev_c, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[2], st));
 	for(const auto &g : ctx->xgroups)
-		launch_xmac_fp32v2(ctx->h_plans[g.plan0], ctx->d_plans, g.d_idx, g.nf, ctx->T, ctx->d_spec, ctx->d_acc, st);
+	{
+		if(ctx->tc)
+			launch_xmac_tc(ctx->tmap, ctx->d_plans, g.d_idx, g.nf, ctx->h_plans[g.plan0].nchan, ctx->d_rowbase, ctx->Tpad,
+			               ctx->h_plans[g.plan0].r2pad, ctx->d_err, ctx->d_acc, st);
+		else
+			launch_xmac_fp32v2(ctx->h_plans[g.plan0], ctx->d_plans, g.d_idx, g.nf, ctx->T, ctx->d_spec, ctx->d_acc, st);
+	}
 	launch_weights(ctx->d_bw, ctx->nbw, ctx->d_acw, ctx->nacw, ctx->d_params, ctx->T, ctx->d_bwacc, ctx->d_acwacc, st);
 	CK(ctx, cudaEventRecord(ctx->ev_d, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[3], st));
@@ -572,12 +656,26 @@ fxb_status fxb_submit_subint_device(fxb_ctx *ctx, const uint8_t *const *dev_bufs
 	return submit(ctx, dev_bufs, nbytes, datasec, datans, validflags, sec, ns, true);
 }
 
+static fxb_status check_device_error(fxb_ctx *ctx)
+{
+	if(!ctx->d_err)
+		return FXB_OK;
+	int32_t e = 0;
+	CK(ctx, cudaMemcpy(&e, ctx->d_err, sizeof(e), cudaMemcpyDeviceToHost));
+	if(e)
+	{
+		ctx->err = "a bounded device wait expired in the tensor-core XMAC (code " + std::to_string(e) + ")";
+		return FXB_ERR_TIMEOUT;
+	}
+	return FXB_OK;
+}
+
 fxb_status fxb_sync(fxb_ctx *ctx)
 {
 	if(!ctx) return FXB_ERR_ARG;
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
 	CK(ctx, cudaStreamSynchronize(ctx->copy_stream));
-	return FXB_OK;
+	return check_device_error(ctx);
 }
 
 fxb_status fxb_core_result_length(const fxb_ctx *ctx, int64_t *ncomplex)
@@ -639,7 +737,7 @@ fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats)
 	CK(ctx, cudaGetLastError());
 	CK(ctx, cudaMemcpyAsync(coreresult, ctx->d_core, sizeof(float2) * ctx->job.corelen, cudaMemcpyDeviceToHost, ctx->stream));
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
-	return FXB_OK;
+	return check_device_error(ctx);
 }
 
 fxb_status fxb_reset(fxb_ctx *ctx)
@@ -726,7 +824,24 @@ fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloa
 	size_t n = (size_t)ctx->T * p.nrow * p.nchan;
 	if(nfloats < 2 * n) return FXB_ERR_ARG;
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
-	if(n)
+	if(n && ctx->tc)
+	{
+		// BF16 [chan][R2][Tpad] -> FP32 [t][row][chan]
+		const size_t nb = (size_t)p.nchan * p.r2pad * ctx->Tpad;
+		std::vector<uint16_t> h(nb);
+		CK(ctx, cudaMemcpy(h.data(), (const uint16_t *)ctx->d_spec_bf16 + p.spec_off, nb * 2, cudaMemcpyDeviceToHost));
+		auto bf = [](uint16_t v) { uint32_t u = (uint32_t)v << 16; float f; memcpy(&f, &u, 4); return f; };
+		for(int t = 0; t < ctx->T; t++)
+			for(int r = 0; r < p.nrow; r++)
+				for(int c = 0; c < p.nchan; c++)
+				{
+					size_t base = ((size_t)c * p.r2pad + 2 * r) * ctx->Tpad + t;
+					size_t o = 2 * (((size_t)t * p.nrow + r) * p.nchan + c);
+					out[o] = bf(h[base]);
+					out[o + 1] = bf(h[base + ctx->Tpad]);
+				}
+	}
+	else if(n)
 		CK(ctx, cudaMemcpy(out, ctx->d_spec + p.spec_off, sizeof(float2) * n, cudaMemcpyDeviceToHost));
 	if(nfft) *nfft = ctx->T;
 	if(nrow) *nrow = p.nrow;

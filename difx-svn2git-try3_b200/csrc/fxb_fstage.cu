@@ -204,7 +204,7 @@ struct FGroup {
 };
 
 template <int MAXE, int OUT>
-__global__ void __launch_bounds__(256) k_fstage2(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
+__global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
                                                  const FGroup *__restrict__ groups, const DevFreqPlan *__restrict__ plans,
                                                  const uint8_t *__restrict__ valid, int64_t valid_stride,
                                                  const FftParam *__restrict__ params, const float2 *__restrict__ twiddle,
@@ -212,6 +212,7 @@ __global__ void __launch_bounds__(256) k_fstage2(const DevStation *__restrict__ 
                                                  int nbufmax, int rawcap_words, void *__restrict__ spec_out)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
+	__shared__ unsigned fmask_s;
 	const FGroup G = groups[blockIdx.y];
 	const int s = G.station;
 	const DevStation &S = st[s];
@@ -257,28 +258,40 @@ __global__ void __launch_bounds__(256) k_fstage2(const DevStation *__restrict__ 
 			continue;
 		}
 		// ---- 1. stage the packed words of the window [nearest, nearest + N)
-		const int64_t fs = S.framesamples;
-		const int64_t g0 = p.nearest;
-		const int64_t fa = g0 / fs;
-		const int64_t so = g0 - fa * fs;                              // window start in stream samples
-		const int64_t sb0 = ((so * bits_per_time) >> 3) & ~(int64_t)7;  // first staged byte (8-aligned)
-		const int64_t sbe = ((so + N) * bits_per_time + 7) >> 3;
+		// (all offsets fit in 32 bits: a station buffer holds < 2^31 samples)
+		const uint32_t fs = (uint32_t)S.framesamples;
+		const uint32_t g0 = (uint32_t)p.nearest;
+		const uint32_t fa = g0 / fs;
+		const uint32_t so = g0 - fa * fs;                               // window start in stream samples
+		const uint32_t sb0 = ((so * (uint32_t)bits_per_time) >> 3) & ~7u;  // first staged byte (8-aligned)
+		const uint32_t sbe = ((so + (uint32_t)N) * (uint32_t)bits_per_time + 7) >> 3;
 		const int nw8 = (int)((sbe - sb0 + 7) >> 3);
 		const bool staged = 2 * nw8 <= rawcap_words;
+		const int nwf = (int)((so + (uint32_t)N - 1) / fs) + 1;           // frames touched by the window
 		if(staged)
 		{
+			const uint32_t payload = (uint32_t)S.payload;
 			for(int w = threadIdx.x; w < nw8; w += blockDim.x)
 			{
-				int64_t sb = sb0 + 8 * (int64_t)w;
-				int64_t k = sb / S.payload;
-				int64_t off = sb - k * S.payload;
-				int64_t fr = fa + k;
+				const uint32_t sb = sb0 + 8u * (uint32_t)w;
+				const uint32_t k = sb / payload;
+				const uint32_t off = sb - k * payload;
+				const int64_t fr = (int64_t)fa + k;
 				uint2 v = make_uint2(0u, 0u);
 				if(fr < nframes)
 					v = __ldg((const uint2 *)(buf + fr * S.framebytes + S.header + off));
 				raw[2 * w] = v.x;
 				raw[2 * w + 1] = v.y;
 			}
+		}
+		if(threadIdx.x < 32)
+		{
+			// validity of the window's frames, one bit per frame (nwf <= 32)
+			const int64_t fr = (int64_t)fa + threadIdx.x;
+			const bool v = threadIdx.x < nwf && fr < valid_stride && vrow[fr];
+			const unsigned m = __ballot_sync(0xffffffffu, v);
+			if(threadIdx.x == 0)
+				fmask_s = m;
 		}
 		__syncthreads();
 		// ---- 2/3. decode, rotate into the FFT buffers
@@ -300,12 +313,29 @@ __global__ void __launch_bounds__(256) k_fstage2(const DevStation *__restrict__ 
 			gamma = (float)(lo * p.b * asl / N);
 			eps = (float)(lo * p.a * X1 * X1);
 		}
-		const int64_t bitbase = so * bits_per_time - sb0 * 8;
+		const uint32_t fmask = fmask_s;
+		const bool wide = nwf > 32;                                       // tiny frames: look validity up per sample
+		const uint32_t bitbase = so * (uint32_t)bits_per_time - sb0 * 8u;
+		const uint32_t cmask = S.nbits == 2 ? 3u : 255u;
+		// frame (relative to fa) of the thread's first sample and its end
+		uint32_t kf = (so + threadIdx.x) / fs;
+		uint32_t kend = (kf + 1) * fs - so;                               // window index where frame kf ends
 		for(int n = threadIdx.x; n < N; n += blockDim.x)
 		{
-			const int64_t g = g0 + n;
-			const int64_t fr = g / fs;
-			const bool ok = n < p.stuck && fr < valid_stride && vrow[fr];
+			while((uint32_t)n >= kend)
+			{
+				kf++;
+				kend += fs;
+			}
+			bool ok;
+			if(!wide)
+				ok = (fmask >> kf) & 1u;
+			else
+			{
+				const int64_t fr = (int64_t)fa + kf;
+				ok = fr < valid_stride && vrow[fr];
+			}
+			ok = ok && n < p.stuck;
 			float sn = 0.0f, cs = 1.0f;
 			if(order != 0)
 			{
@@ -314,12 +344,13 @@ __global__ void __launch_bounds__(256) k_fstage2(const DevStation *__restrict__ 
 					ph = P0 + (float)n * alpha;
 				else
 				{
-					int kk = n / asl, jj = n - kk * asl;
+					const int kk = n / asl, jj = n - kk * asl;
 					ph = P0 + (float)jj * alpha + (float)(kk * jj) * beta + (float)kk * gamma + (float)(kk * kk) * eps;
 				}
 				ph -= rintf(ph);
 				__sincosf(-6.283185307179586f * ph, &sn, &cs);
 			}
+			const uint32_t nbit = bitbase + (uint32_t)n * (uint32_t)bits_per_time;
 			for(int k = 0; k < nbuf; k++)
 			{
 				float v = 0.0f;
@@ -328,14 +359,14 @@ __global__ void __launch_bounds__(256) k_fstage2(const DevStation *__restrict__ 
 					const int b = G.band[k];
 					if(staged)
 					{
-						const int64_t bit = bitbase + (int64_t)n * bits_per_time + (int64_t)b * S.nbits;
-						const uint32_t word = raw[bit >> 5];
-						const uint32_t code = (word >> (bit & 31)) & (S.nbits == 2 ? 3u : 255u);
+						const uint32_t bit = nbit + (uint32_t)(b * S.nbits);
+						const uint32_t code = (raw[bit >> 5] >> (bit & 31)) & cmask;
 						v = S.nbits == 2 ? c_lut2f[code] : c_lut8f.v[code];
 					}
 					else
 					{
-						const int64_t tin = g - fr * fs;
+						const int64_t fr = (int64_t)fa + kf;
+						const int64_t tin = (int64_t)so + n - (int64_t)kf * fs;
 						const uint8_t *plb = buf + fr * S.framebytes + S.header;
 						const int64_t q = tin * S.nband + b;
 						if(S.nbits == 2)

@@ -125,9 +125,10 @@ struct Job {
 	int64_t acc_total = 0;        // complex accumulators
 	// output descriptors for finalisation
 	struct OutMap {
-		int64_t acc;     // accumulator offset (complex) of the first channel
+		int64_t acc;     // accumulator offset (complex) of the first channel, [out][chan] layout
 		int64_t core;    // core-result offset (complex) of the first output channel
 		int nchan, avg;
+		int freq, out;   // frequency and output index within it (out < 0: no accumulator)
 	};
 	std::vector<OutMap> outmap;
 	// weight plans

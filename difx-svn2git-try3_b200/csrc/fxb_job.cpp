@@ -316,7 +316,7 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 				}
 				job.outmap.push_back({acc + (int64_t)o * pl.nchan,
 				                      job.bloff[(size_t)f * B + b] + (int64_t)pf * pl.nchan / job.freqs[f].chans_to_avg,
-				                      pl.nchan, job.freqs[f].chans_to_avg});
+				                      pl.nchan, job.freqs[f].chans_to_avg, f, o});
 				job.bweights.push_back({bl.ds1, bl.ds2, 2 * job.bwoff[(size_t)f * B + b] + pf});
 				pf++;
 			}
@@ -361,11 +361,13 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 				const Job::FreqPlan &pl = job.plan[f];
 				int r = job.band_row[s][bnd];
 				int64_t a;
+				int o;
 				if(pass == 0)
-					a = pl.acc_off + (int64_t)pl.destA[(size_t)r * pl.nrow + r] * pl.nchan;
+					o = pl.destA[(size_t)r * pl.nrow + r];
 				else
-					a = crossout[s][bnd] >= 0 ? pl.acc_off + (int64_t)crossout[s][bnd] * pl.nchan : -1;
-				job.outmap.push_back({a, ridx, pl.nchan, job.freqs[f].chans_to_avg});
+					o = crossout[s][bnd];
+				a = o >= 0 ? pl.acc_off + (int64_t)o * pl.nchan : -1;
+				job.outmap.push_back({a, ridx, pl.nchan, job.freqs[f].chans_to_avg, f, o});
 				ridx += pl.nchan / job.freqs[f].chans_to_avg;
 				job.acweights.push_back({s, bnd, widx++});
 			}

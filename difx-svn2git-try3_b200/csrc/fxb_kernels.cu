@@ -378,13 +378,13 @@ __global__ void k_finalise(const DevOutMap *__restrict__ om, const float2 *__res
 		if(m.acc >= 0)
 		{
 			if(m.avg == 1)
-				v = acc[m.acc + co];
+				v = acc[m.acc + (int64_t)co * m.cstride];
 			else
 			{
 				float sr = 0.0f, si = 0.0f;
 				for(int k = 0; k < m.avg; k++)
 				{
-					float2 a = acc[m.acc + (int64_t)co * m.avg + k];
+					float2 a = acc[m.acc + ((int64_t)co * m.avg + k) * m.cstride];
 					sr += a.x;
 					si += a.y;
 				}

@@ -25,6 +25,7 @@ struct DevFreqPlan {
 struct DevOutMap {
 	int64_t acc, core;
 	int32_t nchan, avg;
+	int32_t cstride, pad;
 };
 
 struct DevBWeight {
@@ -65,6 +66,13 @@ void make_fgroup(void *dst, int station, int freq, int b0, int b1, int r0, int r
 // plan_idx[0..nf) index dplans.
 void launch_xmac_fp32v2(const DevFreqPlan &plan0, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int T,
                         const float2 *spec, float2 *acc, cudaStream_t stream);
+
+// Tensor-core XMAC (csrc/fxb_xmac_tc.cu).
+bool tc_make_tensormap(void *map_out, const void *spec_bf16, int64_t total_rows, int Tpad, int boxrows);
+size_t tc_tensormap_size();
+void tc_geometry(int R2, int Tpad, int *G, int *NG, int *boxrows, int *tmem_cols, size_t *smem);
+void launch_xmac_tc(const void *tmap, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int nchan,
+                    const int64_t *rowbase, int Tpad, int R2, int32_t *err, float2 *acc, cudaStream_t stream);
 
 // FP32 cross-multiply-accumulate of one frequency into acc.
 void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, const float2 *spec, float2 *acc,

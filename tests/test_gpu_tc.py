@@ -1,0 +1,74 @@
+"""Tensor-core (BF16 tcgen05) form against the FP64 oracle.
+
+BF16 spectra carry ~2^-9 relative rounding per value, so a noise-dominated
+cross-correlation differs from the FP64 result by ~1e-3 of its own (noise)
+amplitude.  The meaningful error of a correlator output is in correlation-
+coefficient units: the error of V_ab relative to sqrt(A_aa A_bb), the
+autocorrelation scale.  Gates: cross-correlation error <= 1e-3 in those units,
+autocorrelations within 1e-3 relative, weights and layout exact."""
+import numpy as np
+import pytest
+
+from fxb200 import synth
+from fxb200.native import Correlator
+from helpers import regions, rel_err, small_job
+
+import fxoracle
+
+pytestmark = pytest.mark.gpu
+
+TC_TOL = 1e-3
+
+
+def run_tc(job, subints, rho=0.05, seed=5, xmac="bf16"):
+    corr = Correlator(job, xmac=xmac)
+    orc = fxoracle.OracleCorrelator(job)
+    ref = None
+    for (sec, ns) in subints:
+        inputs = synth.subint_inputs(job, sec, ns, rho=rho, seed=seed)
+        corr.submit(inputs, sec, ns)
+        ref = orc.process_subint(inputs, sec, ns, coreresult=ref)
+    got = corr.results()
+    layout = corr.layout()
+    n = corr.corelen
+    corr.close()
+    return got, ref, layout, n
+
+
+def tc_errors(job, layout, n, got, ref):
+    reg = dict(regions(job, layout, n))
+    xc, ac = reg["cross"], reg["auto"]
+    # correlation-coefficient units: cross error over the autocorrelation scale
+    auto_rms = np.sqrt(np.mean(ref[ac][0::2] ** 2))
+    cross_err = np.sqrt(np.mean((got[xc] - ref[xc]) ** 2)) / auto_rms
+    auto_err = rel_err(got[ac], ref[ac])
+    for name in ("bweight", "acweight"):
+        assert np.array_equal(got[reg[name]].astype(np.float32), ref[reg[name]].astype(np.float32)), name
+    return cross_err, auto_err
+
+
+@pytest.mark.parametrize("kw", [dict(nstation=4, full_pol=True),
+                                dict(nstation=10, full_pol=True, nchan=256),
+                                dict(nstation=3, nchan=1024, bw=32.0, nfreq=8, full_pol=True, subint_ns=2_048_000)])
+def test_bf16_tensor_core_vs_fp64(kw):
+    job = small_job(**kw)
+    got, ref, layout, n = run_tc(job, [(0, 1_024_000), (0, 3_072_000)])
+    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
+    assert cross_err <= TC_TOL, cross_err
+    assert auto_err <= TC_TOL, auto_err
+
+
+def test_bf16_spectra_readback_matches_oracle():
+    job = small_job(nstation=2, full_pol=True)
+    sec, ns = 0, 1_000_000
+    inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=9)
+    corr = Correlator(job, xmac="bf16")
+    corr.submit(inputs, sec, ns)
+    spec = corr.spectra(0)
+    corr.close()
+    orc = fxoracle.OracleCorrelator(job)
+    buf, dsec, dns = inputs[0]
+    for t in (0, 5, 100):
+        ref, _, _ = orc.mode_fft(0, buf, dsec, dns, sec, ns, t)
+        for b in range(2):
+            assert rel_err(spec[t, b], ref[b]) < 8e-3
