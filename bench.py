@@ -38,7 +38,7 @@ for p in (os.path.join(ROOT, "difx-svn2git-try3_b200"), os.path.join(ROOT, "orac
 
 import numpy as np  # noqa: E402
 
-from fxb200 import configs, synth  # noqa: E402
+from fxb200 import configs, shard, synth  # noqa: E402
 
 METRIC = "real-time factor & station.MHz/s (FX: unpack + fringe rotation + FFT + frac-sample + XMAC)"
 UNIT = "station.MHz/s"
@@ -51,7 +51,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fxb", choices=["fxb", "reference"])
-    ap.add_argument("--xmac", default="fp32", choices=["fp32", "bf16", "fp8"])
+    ap.add_argument("--xmac", default="fp32", choices=["fp32", "bf16", "fp8"],
+                    help="arithmetic of the headline form (fp32 = the reference's precision)")
+    ap.add_argument("--no-tc-form", action="store_true", help="skip measuring the tensor-core form beside it")
     ap.add_argument("--subints-per-step", type=int, default=125)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -252,14 +254,16 @@ def gpu_arm(args, job):
     nsub = args.subints_per_step
     core_dev = torch.zeros(2 * corr.corelen, dtype=torch.float32, device="cuda")
 
-    def step_device():
+    def step_device(c=None):
+        c = c or corr
         for j in range(nsub):
             k = j % POOL
-            corr.submit_device([t.data_ptr() for t in dev[k]], nbytes[k], dsec[k], dns[k], times[k][0], times[k][1])
+            c.submit_device([t.data_ptr() for t in dev[k]], nbytes[k], dsec[k], dns[k], times[k][0], times[k][1])
         if world > 1:
-            corr.results_device(core_dev.data_ptr(), core_dev.numel())
-            with torch.cuda.stream(ext):
-                dist.reduce(core_dev, dst=0)
+            # integration end: sum the ranks' core results (time-sharded subints)
+            c.results_device(core_dev.data_ptr(), core_dev.numel())
+            with torch.cuda.stream(torch.cuda.ExternalStream(c.stream())):
+                shard.reduce_core_result(core_dev, dst=0)
 
     host_result = np.zeros(2 * corr.corelen, dtype=np.float32)
 
@@ -270,7 +274,7 @@ def gpu_arm(args, job):
         if world > 1:
             corr.results_device(core_dev.data_ptr(), core_dev.numel())
             with torch.cuda.stream(ext):
-                dist.reduce(core_dev, dst=0)
+                shard.reduce_core_result(core_dev, dst=0)
         corr.results_into(host_result)
 
     def barrier():
@@ -325,6 +329,34 @@ def gpu_arm(args, job):
     h2d = sum(nbytes[j % POOL][s] for j in range(nsub) for s in range(S))
     d2h = 2 * corr.corelen * 4
 
+    # ---- the tensor-core form on the same workload (device-resident)
+    tc_form = None
+    if not args.no_tc_form and args.xmac == "fp32":
+        ctc = Correlator(job, xmac="bf16", inflight=3)
+        for _ in range(args.warmup):
+            step_device(ctc)
+        ctc.sync()
+        barrier()
+        ctc.timing_enable(True)
+        ext2 = torch.cuda.ExternalStream(ctc.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext2)
+        for _ in range(args.steps):
+            step_device(ctc)
+        e1.record(ext2)
+        e1.synchronize()
+        ctc.sync()
+        n2, p2, f2, x2 = ctc.timing_read()
+        tms = max_over_ranks(e0.elapsed_time(e1))
+        tval = job.station_mhz_per_sec() * data_s / (tms * 1e-3)
+        tc_form = {"value": tval, "unit": UNIT, "rtf": data_s / (tms * 1e-3), "dtype": "bf16 spectra, fp32 accumulate",
+                   "ms_per_step": tms / args.steps, "ratio_vs_fp32_form": tval / value,
+                   "kernel_ms_per_subint": {"prep": p2 / max(n2, 1), "fstage": f2 / max(n2, 1), "xmac": x2 / max(n2, 1)},
+                   "xmac_kernel": "k_xmac_tc (tcgen05.mma kind::f16, TMA)"}
+        ctc.close()
+        barrier()
+
     # ---- roofline of the dominant kernel
     hbm_peak, tf_peak, peak_src = load_peaks()
     T = job.blocks_per_send()
@@ -367,7 +399,7 @@ def gpu_arm(args, job):
             "config": workload_config(job),
             "e2e": {"value": e2e_value, "unit": UNIT, "rtf": e2e_value / job.station_mhz_per_sec(),
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps},
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "tc_form": tc_form,
             "gpu_launches": launches_per_subint * nsub * args.steps,
         }
         print(json.dumps(line), flush=True)

@@ -66,7 +66,7 @@ struct fxb_ctx {
 	std::vector<bool> delay_set;
 	// F stage v2 work items and FP32 XMAC v2 launch groups
 	void *d_groups = nullptr;
-	int ngroups = 0, nbufmax = 2, rawnband = 1, TQ = 8;
+	int ngroups = 0, npair = 0, nsingle = 0, nbufmax = 2, rawnband = 1, TQ = 8;
 	struct XGroup { int plan0; int32_t *d_idx; int nf; };
 	std::vector<XGroup> xgroups;
 	// tensor-core (BF16) XMAC state
@@ -75,7 +75,7 @@ struct fxb_ctx {
 	void *d_spec_bf16 = nullptr;
 	int64_t spec_bf16_elems = 0;
 	int64_t *d_rowbase = nullptr;
-	unsigned char tmap[128];
+	alignas(64) unsigned char tmap[128];     // CUtensorMap (64-byte aligned)
 	int32_t *d_err = nullptr;
 };
 
@@ -322,6 +322,12 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			return FXB_ERR_CUDA;
 		}
 		for(int f = 0; f < ctx->F; f++)
+			if(ctx->h_plans[f].nrow && (size_t)G * NG * job.plan[f].nout * sizeof(float2) > (smem - 1024))
+			{
+				ctx->err = "tensor-core XMAC: too many outputs per channel for the epilogue buffer";
+				return FXB_ERR_UNSUPPORTED;
+			}
+		for(int f = 0; f < ctx->F; f++)
 			if(ctx->h_plans[f].nrow && ctx->h_plans[f].r2pad != r2)
 			{
 				ctx->err = "tensor-core XMAC: all subbands must have the same number of inputs";
@@ -333,7 +339,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 	{
 		ctx->nbufmax = ctx->maxN <= 8192 ? 2 : 1;
 		int64_t maxrawbits = 0;
-		std::vector<unsigned char> hg;
+		std::vector<unsigned char> hpair, hsingle;
 		const size_t gsz = fgroup_size();
 		for(int s = 0; s < ctx->S; s++)
 		{
@@ -355,13 +361,17 @@ static fxb_status setup_device(fxb_ctx *ctx)
 						}
 				done[b] = 1;
 				if(b1 >= 0) done[b1] = 1;
+				std::vector<unsigned char> &hg = b1 >= 0 ? hpair : hsingle;
 				size_t off = hg.size();
 				hg.resize(off + gsz);
 				make_fgroup(hg.data() + off, s, f, b, b1, job.band_row[s][b], b1 >= 0 ? job.band_row[s][b1] : -1,
 				            job.freqs[f].lower_sideband, job.freqs[f].freq_mhz);
+				(b1 >= 0 ? ctx->npair : ctx->nsingle)++;
 				ctx->ngroups++;
 			}
 		}
+		std::vector<unsigned char> hg(hpair);
+		hg.insert(hg.end(), hsingle.begin(), hsingle.end());
 		ctx->rawnband = (int)((maxrawbits + ctx->maxN - 1) / ctx->maxN);
 		unsigned char *dg = nullptr;
 		CK(ctx, dalloc(ctx, &dg, std::max<size_t>(hg.size(), 1)));
@@ -620,7 +630,7 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 	CK(ctx, cudaEventRecord(ctx->ev_b, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[1], st));
 	if(ctx->ngroups > 0)
-		launch_fstage2(ctx->d_st, sl.d_sub, ctx->d_groups, ctx->ngroups, ctx->d_plans, ctx->d_valid, ctx->valid_stride,
+		launch_fstage2(ctx->d_st, sl.d_sub, ctx->d_groups, ctx->npair, ctx->nsingle, ctx->d_plans, ctx->d_valid, ctx->valid_stride,
 		               ctx->d_params, ctx->d_twiddle, ctx->maxN, ctx->T, ctx->TQ, ctx->Tpad, job.fringe_rot_order,
 		               job.fractionallofreq, ctx->maxN, ctx->rawnband, 1, ctx->nbufmax, ctx->tc ? 1 : 0,
 		               ctx->tc ? ctx->d_spec_bf16 : (void *)ctx->d_spec, st);

@@ -34,21 +34,6 @@ namespace fxb {
 
 namespace {
 
-// Decode tables of this module (constant memory is per module without
-// relocatable device code): 2-bit {-HiMag, -1, +1, +HiMag}, HiMag = 3.3359
-// (format_vdif.c:48,78) and 8-bit (b - 128)/3.3 (format_vdif.c:122), the
-// latter evaluated at compile time in double and rounded to float exactly as
-// mark5access's initialiser does at run time.
-struct Lut8 { float v[256]; };
-constexpr Lut8 make_lut8()
-{
-	Lut8 l{};
-	for(int b = 0; b < 256; b++)
-		l.v[b] = (float)((b - 128) / 3.3);
-	return l;
-}
-__constant__ float c_lut2f[4] = {-3.3359f, -1.0f, 1.0f, 3.3359f};
-__constant__ Lut8 c_lut8f = make_lut8();
 
 __device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
 
@@ -99,21 +84,22 @@ __device__ __forceinline__ void dft2(cf *x)
 	x[1] = csub(a, b);
 }
 
-// One pass of the radix-R Stockham autosort FFT (decimation in frequency), in
-// place in the padded SoA buffers re/im; tw[k] = exp(-2 pi i k / maxN).
-// With current length len = N/s: butterfly (p, q), x_r = X[q + s(p + r m)],
-// y = DFT_R(x), Y[q + s(R p + r)] = y_r w_len^{r p}.  Each thread holds KB
-// butterflies in registers across the barrier that separates reads from
-// writes.
-template <int R, int KB>
-__device__ __forceinline__ void fft_pass(float *re, float *im, int N, int s, int logs, const float2 *__restrict__ tw,
+// One pass of the radix-R Stockham autosort FFT (decimation in frequency) on
+// NB buffers at once, in place in padded SoA shared memory (buffer k: real
+// part at buf + 2k padN, imaginary part at buf + (2k+1) padN);
+// tw[k] = exp(-2 pi i k / maxN).  With current length len = N/s: butterfly
+// (p, q), x_r = X[q + s(p + r m)], y = DFT_R(x), Y[q + s(R p + r)] =
+// y_r w_len^{r p}.  Each thread holds KB butterflies per buffer in registers
+// across the barrier that separates the pass's reads from its writes; the
+// twiddles are shared by the buffers.
+template <int R, int KB, int NB>
+__device__ __forceinline__ void fft_pass(float *buf, int padN, int N, int s, int logs, const float2 *__restrict__ tw,
                                          int twscale)
 {
-	const int logR = R == 8 ? 3 : (R == 4 ? 2 : 1);
-	const int len = N >> logs;
-	const int m = len >> logR;
+	constexpr int logR = R == 8 ? 3 : (R == 4 ? 2 : 1);
+	const int m = (N >> logs) >> logR;
 	const int nb = N >> logR;
-	cf y[KB][R];
+	cf y[NB][KB][R];
 	int base[KB];
 #pragma unroll
 	for(int k = 0; k < KB; k++)
@@ -124,28 +110,35 @@ __device__ __forceinline__ void fft_pass(float *re, float *im, int N, int s, int
 		{
 			const int q = b & (s - 1);
 			const int p = b >> logs;
-			cf x[8];
-#pragma unroll
-			for(int r = 0; r < R; r++)
-			{
-				const int i = pad(q + s * (p + r * m));
-				x[r] = {re[i], im[i]};
-			}
-			if(R == 8)
-				dft8(x);
-			else if(R == 4)
-				dft4(x);
-			else
-				dft2(x);
+			cf w[R];
 #pragma unroll
 			for(int r = 1; r < R; r++)
 			{
-				const float2 w = __ldg(tw + (size_t)(r * p * s) * twscale);
-				x[r] = cmulf(x[r], {w.x, w.y});
+				const float2 t = __ldg(tw + (r * p * s) * twscale);
+				w[r] = {t.x, t.y};
 			}
 #pragma unroll
-			for(int r = 0; r < R; r++)
-				y[k][r] = x[r];
+			for(int j = 0; j < NB; j++)
+			{
+				const float *re = buf + 2 * j * padN, *im = re + padN;
+				cf x[8];
+#pragma unroll
+				for(int r = 0; r < R; r++)
+				{
+					const int i = pad(q + s * (p + r * m));
+					x[r] = {re[i], im[i]};
+				}
+				if(R == 8)
+					dft8(x);
+				else if(R == 4)
+					dft4(x);
+				else
+					dft2(x);
+				y[j][k][0] = x[0];
+#pragma unroll
+				for(int r = 1; r < R; r++)
+					y[j][k][r] = cmulf(x[r], w[r]);
+			}
 			base[k] = q + s * R * p;
 		}
 	}
@@ -155,33 +148,46 @@ __device__ __forceinline__ void fft_pass(float *re, float *im, int N, int s, int
 		if(base[k] >= 0)
 		{
 #pragma unroll
-			for(int r = 0; r < R; r++)
+			for(int j = 0; j < NB; j++)
 			{
-				const int o = pad(base[k] + s * r);
-				re[o] = y[k][r].x;
-				im[o] = y[k][r].y;
+				float *re = buf + 2 * j * padN, *im = re + padN;
+#pragma unroll
+				for(int r = 0; r < R; r++)
+				{
+					const int o = pad(base[k] + s * r);
+					re[o] = y[j][k][r].x;
+					im[o] = y[j][k][r].y;
+				}
 			}
 		}
 	__syncthreads();
 }
 
-// Complex forward FFT of N = 2^logN points: radix-8 passes, then one radix-4
-// or radix-2 pass for the remaining factor.  MAXE = N / blockDim (>= 8)
-// elements are held per thread in each pass.
-template <int MAXE>
-__device__ void fft_stockham(float *re, float *im, int N, int logN, const float2 *__restrict__ tw, int twscale)
+// Complex forward FFT of N = 2^logN points on NB buffers: radix-8 passes, then
+// one radix-4 or radix-2 pass for the remaining factor.  MAXE = N / blockDim
+// (>= 8) elements per buffer are held per thread in each pass.
+template <int MAXE, int NB>
+__device__ void fft_stockham(float *buf, int padN, int N, int logN, const float2 *__restrict__ tw, int twscale)
 {
 	int s = 1, logs = 0;
 	while(logN - logs >= 3)
 	{
-		fft_pass<8, (MAXE / 8 > 0 ? MAXE / 8 : 1)>(re, im, N, s, logs, tw, twscale);
+		fft_pass<8, (MAXE / 8 > 0 ? MAXE / 8 : 1), NB>(buf, padN, N, s, logs, tw, twscale);
 		s <<= 3;
 		logs += 3;
 	}
 	if(logN - logs == 2)
-		fft_pass<4, MAXE / 4>(re, im, N, s, logs, tw, twscale);
+		fft_pass<4, MAXE / 4, NB>(buf, padN, N, s, logs, tw, twscale);
 	else if(logN - logs == 1)
-		fft_pass<2, MAXE / 2>(re, im, N, s, logs, tw, twscale);
+		fft_pass<2, MAXE / 2, NB>(buf, padN, N, s, logs, tw, twscale);
+}
+
+// 2-bit code -> {-HiMag, -1, +1, +HiMag} (format_vdif.c:78) without a table:
+// sign from bit 1, magnitude HiMag for codes 0 and 3
+__device__ __forceinline__ float level2(uint32_t code)
+{
+	const float mag = ((code ^ (code >> 1)) & 1u) ? 1.0f : 3.3359f;
+	return (code & 2u) ? mag : -mag;
 }
 
 __device__ __forceinline__ float frac_centered(double x)
@@ -203,8 +209,8 @@ struct FGroup {
 	double lofreq;
 };
 
-template <int MAXE, int OUT>
-__global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
+template <int MAXE, int OUT, int NB>
+__global__ void __launch_bounds__(256, (NB == 2 && MAXE <= 8) ? 2 : 3) k_fstage2(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
                                                  const FGroup *__restrict__ groups, const DevFreqPlan *__restrict__ plans,
                                                  const uint8_t *__restrict__ valid, int64_t valid_stride,
                                                  const FftParam *__restrict__ params, const float2 *__restrict__ twiddle,
@@ -213,24 +219,45 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ unsigned fmask_s;
-	const FGroup G = groups[blockIdx.y];
-	const int s = G.station;
-	const DevStation &S = st[s];
-	const int N = S.fftchannels, nchan = S.nchan;
+	__shared__ float lut8_s[256];
+
+	// work item and station description, once into registers
+	const FGroup *gp = groups + blockIdx.y;
+	const int s = gp->station;
+	const int gfreq = gp->freq;
+	int band[2] = {gp->band[0], gp->band[1]};
+	int row[2] = {gp->row[0], gp->row[1]};
+	const bool lsb = gp->lsb != 0;
+	const double lo = gp->lofreq;
+	const DevStation *Sp = st + s;
+	const int N = Sp->fftchannels, nchan = Sp->nchan;
+	const uint32_t fs = (uint32_t)Sp->framesamples;
+	const int nbits = Sp->nbits, nband = Sp->nband;
+	const uint32_t payload = (uint32_t)Sp->payload;
+	const int header = Sp->header, framebytes = Sp->framebytes;
+	const int asl = Sp->asl;
+	const double bw = Sp->bw;
+	const uint8_t *buf = sub[s].buf;
+	const int64_t nframes = sub[s].nbytes / framebytes;
 	const int logN = 31 - __clz(N);
 	const int padN = N + (N >> 5);
-	const int nbuf = G.nb;
 	float *const fbuf = (float *)smem_raw;                          // buffer k: re at 2k padN, im at (2k+1) padN
 	uint32_t *raw = (uint32_t *)(fbuf + 2 * nbufmax * padN);        // staged packed words
-	__nv_bfloat16 *stage = (__nv_bfloat16 *)(raw + rawcap_words);   // OUT == 1: [nb][2][nchan][TQ]
-	const uint8_t *buf = sub[s].buf;
-	const int64_t nframes = sub[s].nbytes / S.framebytes;
+	__nv_bfloat16 *stage = (__nv_bfloat16 *)(raw + rawcap_words);   // OUT == 1: [NB*2][TQ][nchan]
 	const uint8_t *vrow = valid + (int64_t)s * valid_stride;
 	const int twscale = maxN / N;
-	const int bits_per_time = S.nband * S.nbits;
-	const DevFreqPlan &pl = plans[G.freq];
+	const uint32_t bits_per_time = (uint32_t)(nband * nbits);
+	const int64_t spec_off = plans[gfreq].spec_off;
+	const int prow = plans[gfreq].nrow;
+	const int r2pad = plans[gfreq].r2pad;
 	const int t0 = blockIdx.x * TQ;
 	const int tq_n = min(TQ, T - t0);
+	if(nbits == 8)
+	{
+		// (b - 128) / 3.3 in double, rounded to float (format_vdif.c:122)
+		for(int i = threadIdx.x; i < 256; i += blockDim.x)
+			lut8_s[i] = (float)((i - 128) / 3.3);
+	}
 
 	for(int tq = 0; tq < tq_n; tq++)
 	{
@@ -238,50 +265,53 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 		const FftParam p = params[(int64_t)s * T + t];
 		if(p.status != kFftOk)
 		{
-			if(OUT == 0)
-			{
-				float2 *o = (float2 *)spec_out;
-				for(int k = 0; k < nbuf; k++)
-					if(G.row[k] >= 0)
-						for(int c = threadIdx.x; c < nchan; c += blockDim.x)
-							o[pl.spec_off + ((int64_t)t * pl.nrow + G.row[k]) * nchan + c] = make_float2(0.0f, 0.0f);
-			}
-			else
-			{
-				for(int k = 0; k < nbuf; k++)
-					for(int c = threadIdx.x; c < nchan; c += blockDim.x)
+#pragma unroll
+			for(int k = 0; k < NB; k++)
+				for(int c = threadIdx.x; c < nchan; c += blockDim.x)
+				{
+					if(OUT == 0)
 					{
-						stage[(((size_t)k * 2 + 0) * nchan + c) * TQ + tq] = __float2bfloat16(0.0f);
-						stage[(((size_t)k * 2 + 1) * nchan + c) * TQ + tq] = __float2bfloat16(0.0f);
+						if(row[k] >= 0)
+							((float2 *)spec_out)[spec_off + ((int64_t)t * prow + row[k]) * nchan + c] =
+							    make_float2(0.0f, 0.0f);
 					}
-			}
+					else
+					{
+						stage[((size_t)(2 * k) * TQ + tq) * nchan + c] = __float2bfloat16_rn(0.0f);
+						stage[((size_t)(2 * k + 1) * TQ + tq) * nchan + c] = __float2bfloat16_rn(0.0f);
+					}
+				}
 			continue;
 		}
 		// ---- 1. stage the packed words of the window [nearest, nearest + N)
 		// (all offsets fit in 32 bits: a station buffer holds < 2^31 samples)
-		const uint32_t fs = (uint32_t)S.framesamples;
 		const uint32_t g0 = (uint32_t)p.nearest;
 		const uint32_t fa = g0 / fs;
 		const uint32_t so = g0 - fa * fs;                               // window start in stream samples
-		const uint32_t sb0 = ((so * (uint32_t)bits_per_time) >> 3) & ~7u;  // first staged byte (8-aligned)
-		const uint32_t sbe = ((so + (uint32_t)N) * (uint32_t)bits_per_time + 7) >> 3;
+		const uint32_t sb0 = ((so * bits_per_time) >> 3) & ~7u;         // first staged byte (8-aligned)
+		const uint32_t sbe = ((so + (uint32_t)N) * bits_per_time + 7) >> 3;
 		const int nw8 = (int)((sbe - sb0 + 7) >> 3);
 		const bool staged = 2 * nw8 <= rawcap_words;
 		const int nwf = (int)((so + (uint32_t)N - 1) / fs) + 1;           // frames touched by the window
 		if(staged)
 		{
-			const uint32_t payload = (uint32_t)S.payload;
+			uint32_t sb = sb0 + 8u * threadIdx.x;
+			uint32_t k = sb / payload;
+			uint32_t off = sb - k * payload;
 			for(int w = threadIdx.x; w < nw8; w += blockDim.x)
 			{
-				const uint32_t sb = sb0 + 8u * (uint32_t)w;
-				const uint32_t k = sb / payload;
-				const uint32_t off = sb - k * payload;
 				const int64_t fr = (int64_t)fa + k;
 				uint2 v = make_uint2(0u, 0u);
 				if(fr < nframes)
-					v = __ldg((const uint2 *)(buf + fr * S.framebytes + S.header + off));
+					v = __ldg((const uint2 *)(buf + fr * framebytes + header + off));
 				raw[2 * w] = v.x;
 				raw[2 * w + 1] = v.y;
+				off += 8u * blockDim.x;
+				while(off >= payload)
+				{
+					off -= payload;
+					k++;
+				}
 			}
 		}
 		if(threadIdx.x < 32)
@@ -295,10 +325,8 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 		}
 		__syncthreads();
 		// ---- 2/3. decode, rotate into the FFT buffers
-		const double lo = G.lofreq;
 		const double fraclo = fractionallofreq ? (lo - (int)lo) * (double)p.integerdelay : 0.0;
 		float P0 = 0.0f, alpha = 0.0f, beta = 0.0f, gamma = 0.0f, eps = 0.0f;
-		const int asl = S.asl;
 		if(order == 1)
 		{
 			P0 = frac_centered(lo * p.b + fraclo);
@@ -315,11 +343,14 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 		}
 		const uint32_t fmask = fmask_s;
 		const bool wide = nwf > 32;                                       // tiny frames: look validity up per sample
-		const uint32_t bitbase = so * (uint32_t)bits_per_time - sb0 * 8u;
-		const uint32_t cmask = S.nbits == 2 ? 3u : 255u;
-		// frame (relative to fa) of the thread's first sample and its end
-		uint32_t kf = (so + threadIdx.x) / fs;
-		uint32_t kend = (kf + 1) * fs - so;                               // window index where frame kf ends
+		const uint32_t bitbase = so * bits_per_time - sb0 * 8u;
+		const int stuck = p.stuck;
+		uint32_t boff[NB];
+#pragma unroll
+		for(int k = 0; k < NB; k++)
+			boff[k] = (uint32_t)(band[k] * nbits);
+		uint32_t kf = (so + threadIdx.x) / fs;                           // frame of the thread's sample (rel. fa)
+		uint32_t kend = (kf + 1) * fs - so;                               // window index where that frame ends
 		for(int n = threadIdx.x; n < N; n += blockDim.x)
 		{
 			while((uint32_t)n >= kend)
@@ -327,15 +358,8 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 				kf++;
 				kend += fs;
 			}
-			bool ok;
-			if(!wide)
-				ok = (fmask >> kf) & 1u;
-			else
-			{
-				const int64_t fr = (int64_t)fa + kf;
-				ok = fr < valid_stride && vrow[fr];
-			}
-			ok = ok && n < p.stuck;
+			bool ok = wide ? ((int64_t)fa + kf < valid_stride && vrow[(int64_t)fa + kf]) : ((fmask >> kf) & 1u);
+			ok = ok && n < stuck;
 			float sn = 0.0f, cs = 1.0f;
 			if(order != 0)
 			{
@@ -350,32 +374,32 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 				ph -= rintf(ph);
 				__sincosf(-6.283185307179586f * ph, &sn, &cs);
 			}
-			const uint32_t nbit = bitbase + (uint32_t)n * (uint32_t)bits_per_time;
-			for(int k = 0; k < nbuf; k++)
+			const uint32_t nbit = bitbase + (uint32_t)n * bits_per_time;
+#pragma unroll
+			for(int k = 0; k < NB; k++)
 			{
 				float v = 0.0f;
 				if(ok)
 				{
-					const int b = G.band[k];
 					if(staged)
 					{
-						const uint32_t bit = nbit + (uint32_t)(b * S.nbits);
-						const uint32_t code = (raw[bit >> 5] >> (bit & 31)) & cmask;
-						v = S.nbits == 2 ? c_lut2f[code] : c_lut8f.v[code];
+						const uint32_t bit = nbit + boff[k];
+						const uint32_t word = raw[bit >> 5] >> (bit & 31);
+						v = nbits == 2 ? level2(word & 3u) : lut8_s[word & 255u];
 					}
 					else
 					{
 						const int64_t fr = (int64_t)fa + kf;
 						const int64_t tin = (int64_t)so + n - (int64_t)kf * fs;
-						const uint8_t *plb = buf + fr * S.framebytes + S.header;
-						const int64_t q = tin * S.nband + b;
-						if(S.nbits == 2)
+						const uint8_t *plb = buf + fr * framebytes + header;
+						const int64_t q = tin * nband + band[k];
+						if(nbits == 2)
 						{
 							const int64_t bit = q * 2;
-							v = c_lut2f[(__ldg(plb + (bit >> 3)) >> (bit & 7)) & 3];
+							v = level2((__ldg(plb + (bit >> 3)) >> (bit & 7)) & 3u);
 						}
 						else
-							v = c_lut8f.v[__ldg(plb + q)];
+							v = lut8_s[__ldg(plb + q)];
 					}
 				}
 				fbuf[2 * k * padN + pad(n)] = v * cs;
@@ -383,11 +407,10 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 			}
 		}
 		__syncthreads();
-		// ---- 4. FFTs
-		for(int k = 0; k < nbuf; k++)
-			fft_stockham<MAXE>(fbuf + 2 * k * padN, fbuf + (2 * k + 1) * padN, N, logN, twiddle, twscale);
+		// ---- 4. FFTs of the NB bands together
+		fft_stockham<MAXE, NB>(fbuf, padN, N, logN, twiddle, twscale);
 		// ---- 5/6. sideband, fractional-sample rotation, output
-		const float dfs = (float)(S.bw / nchan * (double)p.fse);
+		const float dfs = (float)(bw / nchan * (double)p.fse);
 		float postf = 0.0f;
 		if(order == 0)
 		{
@@ -400,7 +423,7 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 		{
 			int src, ce;
 			float conj = 1.0f;
-			if(G.lsb)
+			if(lsb)
 			{
 				ce = c - nchan;
 				if(order == 0)
@@ -420,22 +443,21 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 			turns -= rintf(turns);
 			float sn, cs;
 			__sincosf(6.283185307179586f * turns, &sn, &cs);
-			for(int k = 0; k < nbuf; k++)
+			const int ps = pad(src);
+#pragma unroll
+			for(int k = 0; k < NB; k++)
 			{
-				const float xr = fbuf[2 * k * padN + pad(src)], xi = conj * fbuf[(2 * k + 1) * padN + pad(src)];
+				const float xr = fbuf[2 * k * padN + ps], xi = conj * fbuf[(2 * k + 1) * padN + ps];
 				const float yr = xr * cs - xi * sn, yi = xr * sn + xi * cs;
 				if(OUT == 0)
 				{
-					if(G.row[k] >= 0)
-					{
-						float2 *o = (float2 *)spec_out;
-						o[pl.spec_off + ((int64_t)t * pl.nrow + G.row[k]) * nchan + c] = make_float2(yr, yi);
-					}
+					if(row[k] >= 0)
+						((float2 *)spec_out)[spec_off + ((int64_t)t * prow + row[k]) * nchan + c] = make_float2(yr, yi);
 				}
 				else
 				{
-					stage[(((size_t)k * 2 + 0) * nchan + c) * TQ + tq] = __float2bfloat16_rn(yr);
-					stage[(((size_t)k * 2 + 1) * nchan + c) * TQ + tq] = __float2bfloat16_rn(yi);
+					stage[((size_t)(2 * k) * TQ + tq) * nchan + c] = __float2bfloat16_rn(yr);
+					stage[((size_t)(2 * k + 1) * TQ + tq) * nchan + c] = __float2bfloat16_rn(yi);
 				}
 			}
 		}
@@ -443,25 +465,31 @@ __global__ void __launch_bounds__(256, 3) k_fstage2(const DevStation *__restrict
 	}
 	if(OUT == 1)
 	{
-		// [chan][2*row + part][Tpad] bf16, TQ consecutive times per store
-		__syncthreads();
+		// [chan][2 row + part][Tpad] bf16: each (channel, real row) receives the
+		// chunk's TQ consecutive times in one 16-byte store
 		__nv_bfloat16 *o = (__nv_bfloat16 *)spec_out;
-		const int R2 = pl.r2pad;
-		const int nitems = nbuf * 2 * nchan;
+		const int nitems = NB * 2 * nchan;
 		for(int it = threadIdx.x; it < nitems; it += blockDim.x)
 		{
 			const int c = it % nchan;
 			const int kp = it / nchan;            // k * 2 + part
 			const int k = kp >> 1, part = kp & 1;
-			if(G.row[k] < 0)
+			const int rk = k == 0 ? row[0] : row[1];
+			if(rk < 0)
 				continue;
-			__nv_bfloat16 *dst = o + pl.spec_off + ((int64_t)c * R2 + 2 * G.row[k] + part) * Tpad + t0;
-			const __nv_bfloat16 *src = stage + ((size_t)kp * nchan + c) * TQ;
+			__nv_bfloat16 *dst = o + spec_off + ((int64_t)c * r2pad + 2 * rk + part) * Tpad + t0;
+			const __nv_bfloat16 *src = stage + (size_t)kp * TQ * nchan + c;
 			if(TQ == 8 && tq_n == 8)
-				*(uint4 *)dst = *(const uint4 *)src;
+			{
+				__align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+				for(int q = 0; q < 8; q++)
+					v[q] = src[(size_t)q * nchan];
+				*(uint4 *)dst = *(const uint4 *)v;
+			}
 			else
 				for(int q = 0; q < tq_n; q++)
-					dst[q] = src[q];
+					dst[q] = src[(size_t)q * nchan];
 		}
 	}
 }
@@ -476,50 +504,72 @@ size_t fstage2_smem(int N, int nband, int nbits, int nchan, int out, int TQ, int
 		rawb = 0;                    // decode from global memory instead
 	rawb = (rawb + 15) & ~(size_t)15;
 	*rawcap_words = (int)(rawb / 4);
-	size_t st = out == 1 ? (size_t)2 * 2 * nchan * TQ * sizeof(__nv_bfloat16) : 0;
-	return fft + rawb + st;
+	size_t stg = out == 1 ? (size_t)2 * 2 * nchan * TQ * sizeof(__nv_bfloat16) : 0;
+	return fft + rawb + stg;
 }
 
-template <int MAXE, int OUT>
+template <int MAXE, int OUT, int NB>
 static void launch_one(dim3 grid, size_t smem, cudaStream_t stream, const DevStation *st, const DevSubintStation *sub,
                        const FGroup *groups, const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride,
                        const FftParam *params, const float2 *twiddle, int maxN, int T, int TQ, int Tpad, int order,
                        int fraclo, int nbufmax, int rawcap, void *out)
 {
-	cudaFuncSetAttribute(k_fstage2<MAXE, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-	k_fstage2<MAXE, OUT><<<grid, 256, smem, stream>>>(st, sub, groups, plans, valid, valid_stride, params, twiddle,
-	                                                    maxN, T, TQ, Tpad, order, fraclo, nbufmax, rawcap, out);
+	cudaFuncSetAttribute(k_fstage2<MAXE, OUT, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+	k_fstage2<MAXE, OUT, NB><<<grid, 256, smem, stream>>>(st, sub, groups, plans, valid, valid_stride, params, twiddle,
+	                                                        maxN, T, TQ, Tpad, order, fraclo, nbufmax, rawcap, out);
 }
 
-void launch_fstage2(const DevStation *st, const DevSubintStation *sub, const void *groups, int ngroups,
+template <int MAXE>
+static void launch_maxe(int npair, int nsingle, int Tchunks, size_t smem, cudaStream_t stream, const DevStation *st,
+                        const DevSubintStation *sub, const FGroup *g, const DevFreqPlan *plans, const uint8_t *valid,
+                        int64_t valid_stride, const FftParam *params, const float2 *twiddle, int maxN, int T, int TQ,
+                        int Tpad, int order, int fl, int nbufmax, int rawcap, int out, void *spec)
+{
+	if(npair > 0)
+	{
+		dim3 grid(Tchunks, npair);
+		if(out == 0)
+			launch_one<MAXE, 0, 2>(grid, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN, T,
+			                       TQ, Tpad, order, fl, nbufmax, rawcap, spec);
+		else
+			launch_one<MAXE, 1, 2>(grid, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN, T,
+			                       TQ, Tpad, order, fl, nbufmax, rawcap, spec);
+	}
+	if(nsingle > 0)
+	{
+		dim3 grid(Tchunks, nsingle);
+		if(out == 0)
+			launch_one<MAXE, 0, 1>(grid, smem, stream, st, sub, g + npair, plans, valid, valid_stride, params, twiddle,
+			                       maxN, T, TQ, Tpad, order, fl, nbufmax, rawcap, spec);
+		else
+			launch_one<MAXE, 1, 1>(grid, smem, stream, st, sub, g + npair, plans, valid, valid_stride, params, twiddle,
+			                       maxN, T, TQ, Tpad, order, fl, nbufmax, rawcap, spec);
+	}
+}
+
+void launch_fstage2(const DevStation *st, const DevSubintStation *sub, const void *groups, int npair, int nsingle,
                     const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride, const FftParam *params,
                     const float2 *twiddle, int maxN, int T, int TQ, int Tpad, int order, bool fractionallofreq,
                     int N, int nband_max, int nbits_max, int nbufmax, int out, void *spec, cudaStream_t stream)
 {
 	int rawcap = 0;
 	size_t smem = fstage2_smem(N, nband_max, nbits_max, N / 2, out, TQ, nbufmax, &rawcap);
-	dim3 grid((T + TQ - 1) / TQ, ngroups);
 	const int me = N / 256;     // elements per thread and pass
 	const FGroup *g = (const FGroup *)groups;
 	const int fl = fractionallofreq ? 1 : 0;
-#define FX_LAUNCH(MB)                                                                                                   \
-	do {                                                                                                                \
-		if(out == 0)                                                                                                    \
-			launch_one<MB, 0>(grid, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN, T, TQ, \
-			                  Tpad, order, fl, nbufmax, rawcap, spec);                                                           \
-		else                                                                                                            \
-			launch_one<MB, 1>(grid, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN, T, TQ, \
-			                  Tpad, order, fl, nbufmax, rawcap, spec);                                                           \
-	} while(0)
+	const int tch = (T + TQ - 1) / TQ;
 	if(me <= 8)
-		FX_LAUNCH(8);
+		launch_maxe<8>(npair, nsingle, tch, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN,
+		               T, TQ, Tpad, order, fl, nbufmax, rawcap, out, spec);
 	else if(me <= 16)
-		FX_LAUNCH(16);
+		launch_maxe<16>(npair, nsingle, tch, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN,
+		                T, TQ, Tpad, order, fl, nbufmax, rawcap, out, spec);
 	else if(me <= 32)
-		FX_LAUNCH(32);
+		launch_maxe<32>(npair, nsingle, tch, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN,
+		                T, TQ, Tpad, order, fl, nbufmax, rawcap, out, spec);
 	else
-		FX_LAUNCH(64);
-#undef FX_LAUNCH
+		launch_maxe<64>(npair, nsingle, tch, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN,
+		                T, TQ, Tpad, order, fl, nbufmax, rawcap, out, spec);
 }
 
 size_t fgroup_size() { return sizeof(FGroup); }

@@ -55,7 +55,7 @@ void launch_fstage(const DevStation *st, const DevSubintStation *sub, const DevB
 
 // F stage v2 (csrc/fxb_fstage.cu): CTA per (station, subband, chunk of TQ FFTs).
 // out 0: FP32 rows [t][row][chan]; out 1: BF16 K-major [chan][2 row + part][tpad].
-void launch_fstage2(const DevStation *st, const DevSubintStation *sub, const void *groups, int ngroups,
+void launch_fstage2(const DevStation *st, const DevSubintStation *sub, const void *groups, int npair, int nsingle,
                     const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride, const FftParam *params,
                     const float2 *twiddle, int maxN, int T, int TQ, int Tpad, int order, bool fractionallofreq,
                     int N, int nband_max, int nbits_max, int nbufmax, int out, void *spec, cudaStream_t stream);

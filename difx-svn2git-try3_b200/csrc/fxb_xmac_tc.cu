@@ -241,6 +241,14 @@ __global__ void __launch_bounds__(128, 1) k_xmac_tc(const __grid_constant__ CUte
 	}
 	else
 	{
+		// results of the CTA's channels: [channel][output] in shared memory
+		// (the stage ring is idle: every load was consumed by an MMA)
+		const int nout = P.acc_cstride;
+		float2 *vbuf = (float2 *)stage0;
+		const int nval = ch_per_cta * nout;
+		for(int i = threadIdx.x; i < nval; i += blockDim.x)
+			vbuf[i] = make_float2(0.0f, 0.0f);
+		__syncthreads();
 		const int row = 32 * warp + lane;
 		const int nin = P.nrow;
 		for(int g = 0; g < tp.NG; g++)
@@ -250,44 +258,41 @@ __global__ void __launch_bounds__(128, 1) k_xmac_tc(const __grid_constant__ CUte
 			const int qhi = min(tp.G - 1, (32 * warp + 31) / tp.R2);
 			for(int q = qlo; q <= qhi; q++)
 			{
-				const int c = c_first + g * tp.G + q;
+				const int cl = g * tp.G + q;                 // channel within the CTA
 				const bool mine = row >= q * tp.R2 && row < (q + 1) * tp.R2;
-				const int r2 = row - q * tp.R2;          // real row within the channel
-				// P[row][q*R2 + j] for j < R2 (warp-uniform column range)
+				const int r2 = row - q * tp.R2;
 				float pv[128];
 				for(int j8 = 0; j8 < tp.R2; j8 += 8)
 					tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(g * 128 + q * tp.R2 + j8), pv + j8);
 				tmem_ld_wait();
-				if(c >= P.nchan)
-					continue;
 				const int a = r2 >> 1;
 				const bool even = (r2 & 1) == 0;
 				for(int b = 0; b < nin; b++)
 				{
-					// even lane (real row of input a) combines with its odd partner
-					const float p_e_re = pv[2 * b], p_e_im = pv[2 * b + 1];   // P[row][2b], P[row][2b+1]
-					const float o_re = __shfl_xor_sync(0xffffffffu, p_e_re, 1);  // partner's P[.][2b]
-					const float o_im = __shfl_xor_sync(0xffffffffu, p_e_im, 1);  // partner's P[.][2b+1]
+					const float p_e_re = pv[2 * b], p_e_im = pv[2 * b + 1];        // P[row][2b], P[row][2b+1]
+					const float o_re = __shfl_xor_sync(0xffffffffu, p_e_re, 1);    // partner's P[.][2b]
+					const float o_im = __shfl_xor_sync(0xffffffffu, p_e_im, 1);    // partner's P[.][2b+1]
 					if(!mine || !even || a >= nin || b < a)
 						continue;
-					const float vre = p_e_re + o_im;       // P[2a][2b] + P[2a+1][2b+1]
-					const float vim = o_re - p_e_im;       // P[2a+1][2b] - P[2a][2b+1]
+					const float vre = p_e_re + o_im;          // P[2a][2b] + P[2a+1][2b+1]
+					const float vim = o_re - p_e_im;          // P[2a+1][2b] - P[2a][2b+1]
 					const int dA = P.destA[a * nin + b];
 					const int dB = P.destB[a * nin + b];
 					if(dA >= 0)
-					{
-						float2 *d = acc + P.acc_off + (int64_t)dA * P.acc_ostride + (int64_t)c * P.acc_cstride;
-						float2 o = *d;
-						*d = make_float2(o.x + vre, o.y + vim);
-					}
+						vbuf[cl * nout + dA] = make_float2(vre, vim);
 					if(dB >= 0)
-					{
-						float2 *d = acc + P.acc_off + (int64_t)dB * P.acc_ostride + (int64_t)c * P.acc_cstride;
-						float2 o = *d;
-						*d = make_float2(o.x + vre, o.y - vim);
-					}
+						vbuf[cl * nout + dB] = make_float2(vre, -vim);
 				}
 			}
+		}
+		__syncthreads();
+		// coalesced accumulate into the contiguous [channel][output] block
+		const int nvalid = min(ch_per_cta, P.nchan - c_first) * nout;
+		float2 *dst = acc + P.acc_off + (int64_t)c_first * nout;
+		for(int i = threadIdx.x; i < nvalid; i += blockDim.x)
+		{
+			const float2 v = vbuf[i], o = dst[i];
+			dst[i] = make_float2(o.x + v.x, o.y + v.y);
 		}
 	}
 	asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -310,6 +315,8 @@ typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32
 
 bool tc_make_tensormap(void *map_out, const void *spec_bf16, int64_t total_rows, int Tpad, int boxrows)
 {
+	if(((uintptr_t)map_out & 63) != 0)
+		return false;                // CUtensorMap must be 64-byte aligned
 	static PFN_encodeTiled encode = nullptr;
 	if(!encode)
 	{
@@ -365,6 +372,8 @@ void launch_xmac_tc(const void *tmap, const DevFreqPlan *dplans, const int32_t *
 	tp.boxrows = boxrows;
 	tp.tmem_cols = cols;
 	tp.err = err;
+	if(((uintptr_t)tmap & 63) != 0)
+		return;                      // refused by tc_make_tensormap at set-up already
 	cudaFuncSetAttribute(k_xmac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 	const int per = G * NG;
 	dim3 grid((nchan + per - 1) / per, nf);
