@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -64,9 +65,11 @@ struct fxb_ctx {
 	std::vector<cudaEvent_t> tev;       // 4 per recorded subint
 	size_t tev_used = 0;
 	std::vector<bool> delay_set;
-	// F stage v2 work items and FP32 XMAC v2 launch groups
-	void *d_groups = nullptr;
-	int ngroups = 0, npair = 0, nsingle = 0, nbufmax = 2, rawnband = 1, TQ = 8;
+	// F-stage work items (by kind) and FP32 XMAC v2 launch groups
+	FGroup *d_groups = nullptr;
+	std::vector<FKind> fkinds;
+	void *d_tw16 = nullptr;              // FP16 twiddles of the tensor-core form
+	void *d_specn = nullptr;             // bf16x2 spectra [t][row][chan] of the tensor-core form
 	struct XGroup { int plan0; int32_t *d_idx; int nf; };
 	std::vector<XGroup> xgroups;
 	// tensor-core (BF16) XMAC state
@@ -228,6 +231,22 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		}
 		CK(ctx, dalloc(ctx, &ctx->d_twiddle, tw.size()));
 		CK(ctx, cudaMemcpy(ctx->d_twiddle, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
+		if(job.xmac_kind == FXB_XMAC_BF16)
+		{
+			std::vector<double> re(ctx->maxN), im(ctx->maxN);
+			for(int k = 0; k < ctx->maxN; k++)
+			{
+				double ang = -2.0 * M_PI * (double)k / (double)ctx->maxN;
+				re[k] = cos(ang);
+				im[k] = sin(ang);
+			}
+			std::vector<uint2> h(ctx->maxN);
+			make_fstage_twiddles16(re.data(), im.data(), ctx->maxN, h.data());
+			uint2 *d = nullptr;
+			CK(ctx, dalloc(ctx, &d, h.size()));
+			CK(ctx, cudaMemcpy(d, h.data(), sizeof(uint2) * h.size(), cudaMemcpyHostToDevice));
+			ctx->d_tw16 = d;
+		}
 	}
 
 	// per-frequency plans
@@ -289,7 +308,6 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				ctx->err = "tensor-core XMAC: at most 64 inputs and 2048 channels per subband";
 				return FXB_ERR_UNSUPPORTED;
 			}
-			d.spec_off = off;
 			rowbase[f] = off / ctx->Tpad;
 			off += (int64_t)d.nchan * d.r2pad * ctx->Tpad;
 			d.acc_ostride = 1;
@@ -335,24 +353,24 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			}
 	}
 
-	// F-stage work items: (station, subband) with up to two bands each
+	// F-stage work items: (station, subband) with up to two bands each, one
+	// launch per kind (FFT length, bands per item)
 	{
-		ctx->nbufmax = ctx->maxN <= 8192 ? 2 : 1;
-		int64_t maxrawbits = 0;
-		std::vector<unsigned char> hpair, hsingle;
-		const size_t gsz = fgroup_size();
+		const int out = ctx->tc ? 1 : 0;
+		std::map<std::pair<int, int>, std::vector<FGroup>> bykind;
 		for(int s = 0; s < ctx->S; s++)
 		{
 			const Job::Station &js = job.stations[s];
-			maxrawbits = std::max<int64_t>(maxrawbits, (int64_t)ctx->h_st[s].fftchannels * js.nband * js.nbits);
+			const int N = ctx->h_st[s].fftchannels;
+			const bool pairs = out == 1 || N <= 2048;
 			std::vector<int> done(js.nband, 0);
 			for(int b = 0; b < js.nband; b++)
 			{
 				if(done[b] || job.band_row[s][b] < 0)
 					continue;
-				int f = js.band_freq[b];
+				const int f = js.band_freq[b];
 				int b1 = -1;
-				if(ctx->nbufmax == 2)
+				if(pairs)
 					for(int c = b + 1; c < js.nband; c++)
 						if(!done[c] && js.band_freq[c] == f && job.band_row[s][c] >= 0)
 						{
@@ -361,23 +379,38 @@ static fxb_status setup_device(fxb_ctx *ctx)
 						}
 				done[b] = 1;
 				if(b1 >= 0) done[b1] = 1;
-				std::vector<unsigned char> &hg = b1 >= 0 ? hpair : hsingle;
-				size_t off = hg.size();
-				hg.resize(off + gsz);
-				make_fgroup(hg.data() + off, s, f, b, b1, job.band_row[s][b], b1 >= 0 ? job.band_row[s][b1] : -1,
-				            job.freqs[f].lower_sideband, job.freqs[f].freq_mhz);
-				(b1 >= 0 ? ctx->npair : ctx->nsingle)++;
-				ctx->ngroups++;
+				FGroup g;
+				memset(&g, 0, sizeof(g));
+				g.station = s;
+				g.freq = f;
+				g.band[0] = b;
+				g.band[1] = b1 >= 0 ? b1 : b;
+				g.row[0] = job.band_row[s][b];
+				g.row[1] = b1 >= 0 ? job.band_row[s][b1] : -1;
+				g.nb = b1 >= 0 ? 2 : 1;
+				g.lsb = job.freqs[f].lower_sideband;
+				g.lofreq = job.freqs[f].freq_mhz;
+				bykind[{N, out == 1 ? 2 : g.nb}].push_back(g);
 			}
 		}
-		std::vector<unsigned char> hg(hpair);
-		hg.insert(hg.end(), hsingle.begin(), hsingle.end());
-		ctx->rawnband = (int)((maxrawbits + ctx->maxN - 1) / ctx->maxN);
-		unsigned char *dg = nullptr;
-		CK(ctx, dalloc(ctx, &dg, std::max<size_t>(hg.size(), 1)));
+		std::vector<FGroup> hg;
+		for(const auto &kv : bykind)
+		{
+			FKind k;
+			memset(&k, 0, sizeof(k));
+			if(!fstage_plan(kv.first.first, kv.first.second, out, &k))
+			{
+				ctx->err = "F stage: no kernel shape for FFT length " + std::to_string(kv.first.first);
+				return FXB_ERR_UNSUPPORTED;
+			}
+			k.first = (int)hg.size();
+			k.count = (int)kv.second.size();
+			hg.insert(hg.end(), kv.second.begin(), kv.second.end());
+			ctx->fkinds.push_back(k);
+		}
+		CK(ctx, dalloc(ctx, &ctx->d_groups, std::max<size_t>(hg.size(), 1)));
 		if(!hg.empty())
-			CK(ctx, cudaMemcpy(dg, hg.data(), hg.size(), cudaMemcpyHostToDevice));
-		ctx->d_groups = dg;
+			CK(ctx, cudaMemcpy(ctx->d_groups, hg.data(), sizeof(FGroup) * hg.size(), cudaMemcpyHostToDevice));
 	}
 	// FP32 XMAC launch groups: frequencies with equal shape share a launch
 	{
@@ -411,6 +444,12 @@ static fxb_status setup_device(fxb_ctx *ctx)
 	// big buffers
 	CK(ctx, dalloc(ctx, &ctx->d_params, (size_t)ctx->S * ctx->T));
 	CK(ctx, dalloc(ctx, &ctx->d_spec, job.xmac_kind == FXB_XMAC_FP32 ? (size_t)job.spec_total : 1));
+	if(ctx->tc)
+	{
+		uint32_t *sn = nullptr;
+		CK(ctx, dalloc(ctx, &sn, (size_t)job.spec_total));
+		ctx->d_specn = sn;
+	}
 	CK(ctx, dalloc(ctx, &ctx->d_acc, (size_t)job.acc_total));
 	CK(ctx, dalloc(ctx, &ctx->d_core, (size_t)job.corelen));
 	ctx->nbw = (int)job.bweights.size();
@@ -629,11 +668,30 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 	                  sec, ns, job.fringe_rot_order, ctx->d_params, st);
 	CK(ctx, cudaEventRecord(ctx->ev_b, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[1], st));
-	if(ctx->ngroups > 0)
-		launch_fstage2(ctx->d_st, sl.d_sub, ctx->d_groups, ctx->npair, ctx->nsingle, ctx->d_plans, ctx->d_valid, ctx->valid_stride,
-		               ctx->d_params, ctx->d_twiddle, ctx->maxN, ctx->T, ctx->TQ, ctx->Tpad, job.fringe_rot_order,
-		               job.fractionallofreq, ctx->maxN, ctx->rawnband, 1, ctx->nbufmax, ctx->tc ? 1 : 0,
-		               ctx->tc ? ctx->d_spec_bf16 : (void *)ctx->d_spec, st);
+	{
+		FsArgs fa;
+		memset(&fa, 0, sizeof(fa));
+		fa.st = ctx->d_st;
+		fa.sub = sl.d_sub;
+		fa.groups = ctx->d_groups;
+		fa.plans = ctx->d_plans;
+		fa.valid = ctx->d_valid;
+		fa.valid_stride = ctx->valid_stride;
+		fa.params = ctx->d_params;
+		fa.tw = ctx->tc ? ctx->d_tw16 : (const void *)ctx->d_twiddle;
+		fa.maxN = ctx->maxN;
+		fa.T = ctx->T;
+		fa.order = job.fringe_rot_order;
+		fa.fraclo = job.fractionallofreq ? 1 : 0;
+		fa.spec = ctx->tc ? ctx->d_specn : (void *)ctx->d_spec;
+		for(const FKind &k : ctx->fkinds)
+			launch_fstage_kind(k, fa, st);
+		if(ctx->tc)
+			for(const auto &g : ctx->xgroups)
+				launch_spec_kmajor(ctx->d_plans, g.d_idx, g.nf, ctx->h_plans[g.plan0].nrow, ctx->h_plans[g.plan0].nchan,
+				                   ctx->T, ctx->Tpad, ctx->d_rowbase, (const uint32_t *)ctx->d_specn,
+				                   (uint16_t *)ctx->d_spec_bf16, st);
+	}
 	CK(ctx, cudaEventRecord(ctx->ev_c, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[2], st));
 	for(const auto &g : ctx->xgroups)
@@ -836,20 +894,15 @@ fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloa
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
 	if(n && ctx->tc)
 	{
-		// BF16 [chan][R2][Tpad] -> FP32 [t][row][chan]
-		const size_t nb = (size_t)p.nchan * p.r2pad * ctx->Tpad;
-		std::vector<uint16_t> h(nb);
-		CK(ctx, cudaMemcpy(h.data(), (const uint16_t *)ctx->d_spec_bf16 + p.spec_off, nb * 2, cudaMemcpyDeviceToHost));
-		auto bf = [](uint16_t v) { uint32_t u = (uint32_t)v << 16; float f; memcpy(&f, &u, 4); return f; };
-		for(int t = 0; t < ctx->T; t++)
-			for(int r = 0; r < p.nrow; r++)
-				for(int c = 0; c < p.nchan; c++)
-				{
-					size_t base = ((size_t)c * p.r2pad + 2 * r) * ctx->Tpad + t;
-					size_t o = 2 * (((size_t)t * p.nrow + r) * p.nchan + c);
-					out[o] = bf(h[base]);
-					out[o + 1] = bf(h[base + ctx->Tpad]);
-				}
+		// bf16x2 [t][row][chan] -> FP32
+		std::vector<uint32_t> h(n);
+		CK(ctx, cudaMemcpy(h.data(), (const uint32_t *)ctx->d_specn + p.spec_off, n * 4, cudaMemcpyDeviceToHost));
+		auto bf = [](uint32_t v) { uint32_t u = v << 16; float f; memcpy(&f, &u, 4); return f; };
+		for(size_t i = 0; i < n; i++)
+		{
+			out[2 * i] = bf(h[i] & 0xFFFFu);
+			out[2 * i + 1] = bf(h[i] >> 16);
+		}
 	}
 	else if(n)
 		CK(ctx, cudaMemcpy(out, ctx->d_spec + p.spec_off, sizeof(float2) * n, cudaMemcpyDeviceToHost));

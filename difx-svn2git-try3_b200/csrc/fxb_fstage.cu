@@ -1,31 +1,38 @@
 // F stage (Mode::process, mpifxcorr/src/mode.cpp:845-1308) for sm_100a.
 //
-// One CTA per (station, subband, chunk of TQ consecutive FFTs).  For each FFT
-// of the chunk the CTA
-//   1. stages the station's packed VDIF words of the FFT window in shared
-//      memory (8-byte loads, frame headers skipped),
-//   2. decodes the subband's one or two polarisation bands from those words
-//      (2-bit / 8-bit tables of format_vdif.c:74-149), zeroing samples of
+// One CTA per (station, subband, chunk of FFTs); a subband's one or two
+// polarisation bands are transformed together.  Each thread owns KB radix-8
+// butterflies of every pass of one FFT ("slot"): an FFT of N points takes
+// N / (8 KB) threads, and a CTA runs several slots side by side when N is
+// small.  Per FFT a thread
+//   1. decodes its 8 KB samples x[b + r N/8] straight from the VDIF words in
+//      global memory (2-bit / 8-bit levels of format_vdif.c:74-149; samples of
 //      invalid frames and, for 8-bit 2/4-channel streams, every sample after
-//      the first blanked one (format_vdif.c:1879-1922),
-//   3. multiplies by the fringe rotator exp(-2 pi i phi(n)) of the order in use
-//      (mode.cpp:906-1051; phi reduced to [-1/2, 1/2) turns in FP64 at the FFT
-//      start, per sample in FP32),
-//   4. runs a complex FFT of N = 2*nchan points as a radix-8 Stockham
-//      transform in padded structure-of-arrays shared memory (one butterfly
-//      per thread and pass, held in registers across the pass barrier),
-//   5. selects the sideband (USB bins 0..nchan-1, LSB nchan..2nchan-1; order 0
-//      takes the conjugate mirror) and applies the fractional-sample rotator
-//      exp(+2 pi i f_c fse) (mode.cpp:1053-1097, 1279-1286), with the post-F
-//      fringe phase for order 0 (mode.cpp:1061-1070),
-//   6. writes the spectra: FP32 rows [t][row][chan] for the FP32 XMAC, or
-//      BF16 K-major [chan][2*row + re/im][t] (time contiguous, the operand
-//      layout of the tensor-core XMAC), staged in shared memory so that each
-//      (channel, real row) receives TQ consecutive times in one store.
+//      the first blanked one, read as zero: format_vdif.c:1879-1922),
+//   2. multiplies them by the fringe rotator exp(-2 pi i phi(n)) of the order
+//      in use (mode.cpp:906-1051; phi reduced to [-1/2, 1/2) turns in FP64 at
+//      the FFT start, per sample in FP32),
+//   3. runs the first radix-8 pass of a Stockham autosort FFT in registers
+//      and exchanges through padded shared memory for the remaining passes
+//      (two buffers used alternately: one barrier per exchange),
+//   4. in the last pass selects the sideband (USB bins 0..nchan-1, LSB
+//      nchan..2nchan-1, order-0 LSB the conjugate mirror), applies the
+//      fractional-sample rotator exp(+2 pi i f_c fse) (mode.cpp:1053-1097,
+//      1279-1286) and the post-F fringe phase of order 0 (mode.cpp:1061-1070),
+//      and stores its channels to the spectra [t][row][chan].
+//
+// Two arithmetic forms:
+//   out 0: FP32 FFT, spectra as float2 (the plain FP32 form);
+//   out 1: FP16 FFT with the two bands packed in half2 lanes (one instruction
+//          advances both polarisations), spectra as bf16x2 (re, im) for the
+//          tensor-core XMAC.  Samples are scaled by 2^-e so that no FFT value
+//          can leave the FP16 range; the outputs are scaled back exactly.
 
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cstdint>
+#include <type_traits>
 
 #include "fxb_internal.h"
 #include "fxb_kernels.h"
@@ -34,559 +41,579 @@ namespace fxb {
 
 namespace {
 
+// padded index of 8-byte element i: every exchange of the pass schedule
+// below is free of bank conflicts, and runs of 8 starting at multiples of 8
+// stay contiguous and 16-byte aligned (the first pass stores them as pairs)
+__host__ __device__ __forceinline__ int xpad(int i) { return i + 2 * (i >> 4); }
 
-__device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
-
+// ---- lane values: FP32 complex (one band), packed FP16 complex (two bands)
 struct cf { float x, y; };
+struct hc { __half2 x, y; };      // x = (re band0, re band1), y = (im band0, im band1)
+struct hw { __half2 r, i; };      // twiddle as (wr, wr), (wi, wi)
 
-__device__ __forceinline__ cf cmulf(cf a, cf b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
-__device__ __forceinline__ cf cadd(cf a, cf b) { return {a.x + b.x, a.y + b.y}; }
-__device__ __forceinline__ cf csub(cf a, cf b) { return {a.x - b.x, a.y - b.y}; }
-__device__ __forceinline__ cf mul_mi(cf a) { return {a.y, -a.x}; }   // -i * a
-__device__ __forceinline__ cf mul_pi(cf a) { return {-a.y, a.x}; }   // +i * a
-
-// forward 8-point DFT in place
-__device__ __forceinline__ void dft8(cf *x)
+__device__ __forceinline__ cf add(cf a, cf b) { return {a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ cf sub(cf a, cf b) { return {a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ cf add_mi(cf a, cf b) { return {a.x + b.y, a.y - b.x}; }   // a - i b
+__device__ __forceinline__ cf add_pi(cf a, cf b) { return {a.x - b.y, a.y + b.x}; }   // a + i b
+__device__ __forceinline__ cf rot45(cf a)                                               // a (1 - i) / sqrt2
 {
 	const float r = 0.70710678118654752440f;
-	cf a0 = cadd(x[0], x[4]), a4 = csub(x[0], x[4]);
-	cf a1 = cadd(x[1], x[5]), a5 = csub(x[1], x[5]);
-	cf a2 = cadd(x[2], x[6]), a6 = csub(x[2], x[6]);
-	cf a3 = cadd(x[3], x[7]), a7 = csub(x[3], x[7]);
-	cf b0 = cadd(a0, a2), b2 = csub(a0, a2), b1 = cadd(a1, a3), b3 = csub(a1, a3);
-	x[0] = cadd(b0, b1);
-	x[4] = csub(b0, b1);
-	x[2] = cadd(b2, mul_mi(b3));
-	x[6] = cadd(b2, mul_pi(b3));
-	cf t5 = {(a5.x + a5.y) * r, (a5.y - a5.x) * r};      // a5 * (1 - i)/sqrt2
-	cf t6 = mul_mi(a6);                                  // a6 * -i
-	cf t7 = {(a7.y - a7.x) * r, -(a7.x + a7.y) * r};     // a7 * (-1 - i)/sqrt2
-	cf c0 = cadd(a4, t6), c2 = csub(a4, t6), c1 = cadd(t5, t7), c3 = csub(t5, t7);
-	x[1] = cadd(c0, c1);
-	x[5] = csub(c0, c1);
-	x[3] = cadd(c2, mul_mi(c3));
-	x[7] = cadd(c2, mul_pi(c3));
+	return {(a.x + a.y) * r, (a.y - a.x) * r};
 }
+__device__ __forceinline__ cf twid(cf a, float2 w) { return {a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x}; }
 
-__device__ __forceinline__ void dft4(cf *x)
+__device__ __forceinline__ hc add(hc a, hc b) { return {__hadd2(a.x, b.x), __hadd2(a.y, b.y)}; }
+__device__ __forceinline__ hc sub(hc a, hc b) { return {__hsub2(a.x, b.x), __hsub2(a.y, b.y)}; }
+__device__ __forceinline__ hc add_mi(hc a, hc b) { return {__hadd2(a.x, b.y), __hsub2(a.y, b.x)}; }
+__device__ __forceinline__ hc add_pi(hc a, hc b) { return {__hsub2(a.x, b.y), __hadd2(a.y, b.x)}; }
+__device__ __forceinline__ hc rot45(hc a)
 {
-	cf b0 = cadd(x[0], x[2]), b2 = csub(x[0], x[2]), b1 = cadd(x[1], x[3]), b3 = csub(x[1], x[3]);
-	x[0] = cadd(b0, b1);
-	x[2] = csub(b0, b1);
-	x[1] = cadd(b2, mul_mi(b3));
-	x[3] = cadd(b2, mul_pi(b3));
+	const __half2 r = __float2half2_rn(0.70710678118654752440f);
+	return {__hmul2(__hadd2(a.x, a.y), r), __hmul2(__hsub2(a.y, a.x), r)};
 }
-
-__device__ __forceinline__ void dft2(cf *x)
+__device__ __forceinline__ hc twid(hc a, hw w)
 {
-	cf a = x[0], b = x[1];
-	x[0] = cadd(a, b);
-	x[1] = csub(a, b);
+	return {__hfma2(a.x, w.r, __hneg2(__hmul2(a.y, w.i))), __hfma2(a.x, w.i, __hmul2(a.y, w.r))};
 }
 
-// One pass of the radix-R Stockham autosort FFT (decimation in frequency) on
-// NB buffers at once, in place in padded SoA shared memory (buffer k: real
-// part at buf + 2k padN, imaginary part at buf + (2k+1) padN);
-// tw[k] = exp(-2 pi i k / maxN).  With current length len = N/s: butterfly
-// (p, q), x_r = X[q + s(p + r m)], y = DFT_R(x), Y[q + s(R p + r)] =
-// y_r w_len^{r p}.  Each thread holds KB butterflies per buffer in registers
-// across the barrier that separates the pass's reads from its writes; the
-// twiddles are shared by the buffers.
-template <int R, int KB, int NB>
-__device__ __forceinline__ void fft_pass(float *buf, int padN, int N, int s, int logs, const float2 *__restrict__ tw,
-                                         int twscale)
+__device__ __forceinline__ float2 ldtw(const float2 *t, int i) { return __ldg(t + i); }
+__device__ __forceinline__ hw ldtw(const hw *t, int i)
 {
-	constexpr int logR = R == 8 ? 3 : (R == 4 ? 2 : 1);
-	const int m = (N >> logs) >> logR;
-	const int nb = N >> logR;
-	cf y[NB][KB][R];
-	int base[KB];
-#pragma unroll
-	for(int k = 0; k < KB; k++)
-	{
-		const int b = threadIdx.x + k * blockDim.x;
-		base[k] = -1;
-		if(b < nb)
-		{
-			const int q = b & (s - 1);
-			const int p = b >> logs;
-			cf w[R];
-#pragma unroll
-			for(int r = 1; r < R; r++)
-			{
-				const float2 t = __ldg(tw + (r * p * s) * twscale);
-				w[r] = {t.x, t.y};
-			}
-#pragma unroll
-			for(int j = 0; j < NB; j++)
-			{
-				const float *re = buf + 2 * j * padN, *im = re + padN;
-				cf x[8];
-#pragma unroll
-				for(int r = 0; r < R; r++)
-				{
-					const int i = pad(q + s * (p + r * m));
-					x[r] = {re[i], im[i]};
-				}
-				if(R == 8)
-					dft8(x);
-				else if(R == 4)
-					dft4(x);
-				else
-					dft2(x);
-				y[j][k][0] = x[0];
-#pragma unroll
-				for(int r = 1; r < R; r++)
-					y[j][k][r] = cmulf(x[r], w[r]);
-			}
-			base[k] = q + s * R * p;
-		}
-	}
-	__syncthreads();
-#pragma unroll
-	for(int k = 0; k < KB; k++)
-		if(base[k] >= 0)
-		{
-#pragma unroll
-			for(int j = 0; j < NB; j++)
-			{
-				float *re = buf + 2 * j * padN, *im = re + padN;
-#pragma unroll
-				for(int r = 0; r < R; r++)
-				{
-					const int o = pad(base[k] + s * r);
-					re[o] = y[j][k][r].x;
-					im[o] = y[j][k][r].y;
-				}
-			}
-		}
-	__syncthreads();
+	const uint2 u = __ldg((const uint2 *)t + i);
+	hw w;
+	w.r = *(const __half2 *)&u.x;
+	w.i = *(const __half2 *)&u.y;
+	return w;
 }
 
-// Complex forward FFT of N = 2^logN points on NB buffers: radix-8 passes, then
-// one radix-4 or radix-2 pass for the remaining factor.  MAXE = N / blockDim
-// (>= 8) elements per buffer are held per thread in each pass.
-template <int MAXE, int NB>
-__device__ void fft_stockham(float *buf, int padN, int N, int logN, const float2 *__restrict__ tw, int twscale)
+// 8-byte shared-memory element <-> lane value
+template <typename C> __device__ __forceinline__ C lds(const uint2 *p);
+template <> __device__ __forceinline__ cf lds<cf>(const uint2 *p)
 {
-	int s = 1, logs = 0;
-	while(logN - logs >= 3)
-	{
-		fft_pass<8, (MAXE / 8 > 0 ? MAXE / 8 : 1), NB>(buf, padN, N, s, logs, tw, twscale);
-		s <<= 3;
-		logs += 3;
-	}
-	if(logN - logs == 2)
-		fft_pass<4, MAXE / 4, NB>(buf, padN, N, s, logs, tw, twscale);
-	else if(logN - logs == 1)
-		fft_pass<2, MAXE / 2, NB>(buf, padN, N, s, logs, tw, twscale);
+	const float2 v = *(const float2 *)p;
+	return {v.x, v.y};
+}
+template <> __device__ __forceinline__ hc lds<hc>(const uint2 *p)
+{
+	const uint2 u = *p;
+	hc v;
+	v.x = *(const __half2 *)&u.x;
+	v.y = *(const __half2 *)&u.y;
+	return v;
+}
+__device__ __forceinline__ uint2 bits(cf v) { return make_uint2(__float_as_uint(v.x), __float_as_uint(v.y)); }
+__device__ __forceinline__ uint2 bits(hc v) { return make_uint2(*(const uint32_t *)&v.x, *(const uint32_t *)&v.y); }
+template <typename C> __device__ __forceinline__ void sts(uint2 *p, C v) { *p = bits(v); }
+template <typename C> __device__ __forceinline__ void sts2(uint2 *p, C a, C b)
+{
+	const uint2 u = bits(a), w = bits(b);
+	*(uint4 *)p = make_uint4(u.x, u.y, w.x, w.y);
 }
 
-// 2-bit code -> {-HiMag, -1, +1, +HiMag} (format_vdif.c:78) without a table:
-// sign from bit 1, magnitude HiMag for codes 0 and 3
+// forward DFTs in place (w = exp(-2 pi i / R))
+template <typename C>
+__device__ __forceinline__ void dft8(C *x)
+{
+	const C a0 = add(x[0], x[4]), d0 = sub(x[0], x[4]);
+	const C a1 = add(x[1], x[5]), d1 = sub(x[1], x[5]);
+	const C a2 = add(x[2], x[6]), d2 = sub(x[2], x[6]);
+	const C a3 = add(x[3], x[7]), d3 = sub(x[3], x[7]);
+	const C b0 = add(a0, a2), b2 = sub(a0, a2), b1 = add(a1, a3), b3 = sub(a1, a3);
+	x[0] = add(b0, b1);
+	x[4] = sub(b0, b1);
+	x[2] = add_mi(b2, b3);
+	x[6] = add_pi(b2, b3);
+	// odd bins: DFT4 of d_k w^k, with d1 w + d3 w^3 = (d1 - i d3) w and d1 w - d3 w^3 = (d1 + i d3) w
+	const C f0 = add_mi(d0, d2), f2 = add_pi(d0, d2);
+	const C f1 = rot45(add_mi(d1, d3)), f3 = rot45(add_pi(d1, d3));
+	x[1] = add(f0, f1);
+	x[5] = sub(f0, f1);
+	x[3] = add_mi(f2, f3);
+	x[7] = add_pi(f2, f3);
+}
+
+template <typename C>
+__device__ __forceinline__ void dft4(C *x)
+{
+	const C b0 = add(x[0], x[2]), b2 = sub(x[0], x[2]), b1 = add(x[1], x[3]), b3 = sub(x[1], x[3]);
+	x[0] = add(b0, b1);
+	x[2] = sub(b0, b1);
+	x[1] = add_mi(b2, b3);
+	x[3] = add_pi(b2, b3);
+}
+
+template <typename C>
+__device__ __forceinline__ void dft2(C *x)
+{
+	const C a = x[0], b = x[1];
+	x[0] = add(a, b);
+	x[1] = sub(a, b);
+}
+
+template <int R, typename C>
+__device__ __forceinline__ void dftR(C *x)
+{
+	if(R == 8)
+		dft8(x);
+	else if(R == 4)
+		dft4(x);
+	else
+		dft2(x);
+}
+
+// 2-bit code -> {-HiMag, -1, +1, +HiMag} (format_vdif.c:78): sign from bit 1,
+// magnitude HiMag for codes 0 and 3
 __device__ __forceinline__ float level2(uint32_t code)
 {
 	const float mag = ((code ^ (code >> 1)) & 1u) ? 1.0f : 3.3359f;
 	return (code & 2u) ? mag : -mag;
 }
 
-__device__ __forceinline__ float frac_centered(double x)
+__device__ __forceinline__ float frac_centered(double x) { return (float)(x - rint(x)); }
+
+// per-FFT constants of one slot
+struct SlotConst {
+	int t;
+	bool tok;         // t < T
+	float dfs;        // fractional-sample rotation turns per channel
+	float postf;      // order-0 post-F fringe turns
+};
+
+// One radix-8 butterfly of a middle pass (stride s = 2^logs, m = N / (8 s)):
+// x_r = X[q + s (p + r m)], y = DFT8(x), y_r *= w_N^(r p s).
+template <typename C, int NV, typename TW>
+__device__ __forceinline__ void radix8_step(const uint2 *src, int padN, int q, int s, int p8, int m, const TW *tw,
+                                            int twscale, C (&x)[NV][8])
 {
-	return (float)(x - rint(x));
+#pragma unroll
+	for(int j = 0; j < NV; j++)
+	{
+#pragma unroll
+		for(int r = 0; r < 8; r++)
+			x[j][r] = lds<C>(src + j * padN + xpad(q + s * (p8 + r * m)));
+		dft8(x[j]);
+	}
+#pragma unroll
+	for(int r = 1; r < 8; r++)
+	{
+		const TW w = ldtw(tw, r * p8 * s * twscale);
+#pragma unroll
+		for(int j = 0; j < NV; j++)
+			x[j][r] = twid(x[j][r], w);
+	}
+}
+
+// Output of the last pass (radix R, stride sL = N/R, no twiddles): bins
+// q + sL r of the butterflies q = bt + j TPF go to their channels.
+template <typename C, int NV, int KB, int R>
+__device__ __forceinline__ void last_pass(const uint2 *src, int padN, int N, int nchan, int TPF, int bt, bool lsb,
+                                          int order, const SlotConst &sc, const int row[2], int prow,
+                                          int64_t spec_off, float hout, void *spec)
+{
+	constexpr bool H = std::is_same<C, hc>::value;
+	constexpr int J = (KB * 8) / R;
+	const int sL = N / R;
+#pragma unroll
+	for(int jj = 0; jj < J; jj++)
+	{
+		const int q = bt + jj * TPF;
+		C y[NV][R];
+#pragma unroll
+		for(int j = 0; j < NV; j++)
+		{
+#pragma unroll
+			for(int r = 0; r < R; r++)
+				y[j][r] = lds<C>(src + j * padN + xpad(q + sL * r));
+			dftR<R>(y[j]);
+		}
+#pragma unroll
+		for(int r = 0; r < R; r++)
+		{
+			const int k = q + sL * r;
+			int c, ce;
+			bool use;
+			float cj = 1.0f;
+			if(!lsb)
+			{
+				use = k < nchan;
+				c = k;
+				ce = k;
+			}
+			else if(order != 0)
+			{
+				use = k >= nchan;
+				c = k - nchan;
+				ce = c - nchan;
+			}
+			else
+			{
+				use = k >= 1 && k <= nchan;
+				c = nchan - k;
+				ce = c - nchan;
+				cj = -1.0f;
+			}
+			if(!use || !sc.tok)
+				continue;
+			float turns = (float)ce * sc.dfs + sc.postf;
+			turns -= rintf(turns);
+			float sn, cs;
+			__sincosf(6.283185307179586f * turns, &sn, &cs);
+			const int64_t o0 = spec_off + ((int64_t)sc.t * prow) * nchan + c;
+			if constexpr(H)
+			{
+				const hc v = y[0][r];
+				const float xr[2] = {__low2float(v.x) * hout, __high2float(v.x) * hout};
+				const float xi[2] = {cj * __low2float(v.y) * hout, cj * __high2float(v.y) * hout};
+#pragma unroll
+				for(int b = 0; b < 2; b++)
+					if(row[b] >= 0)
+						((__nv_bfloat162 *)spec)[o0 + (int64_t)row[b] * nchan] =
+						    __floats2bfloat162_rn(xr[b] * cs - xi[b] * sn, xr[b] * sn + xi[b] * cs);
+			}
+			else
+			{
+#pragma unroll
+				for(int j = 0; j < NV; j++)
+					if(row[j] >= 0)
+					{
+						const cf v = y[j][r];
+						const float xr = v.x, xi = cj * v.y;
+						((float2 *)spec)[o0 + (int64_t)row[j] * nchan] = make_float2(xr * cs - xi * sn, xr * sn + xi * cs);
+					}
+			}
+		}
+	}
 }
 
 }  // namespace
 
-// Work item of the F stage: one subband (frequency) of one station, with the
-// station bands recording it (at most two are processed together; a third
-// band of the same frequency gets its own item).
-struct FGroup {
-	int32_t station, freq;
-	int32_t band[2];
-	int32_t row[2];          // rows within the frequency's spectra (-1: band not output)
-	int32_t nb;
-	int32_t lsb;
-	double lofreq;
-};
-
-template <int MAXE, int OUT, int NB>
-__global__ void __launch_bounds__(256, (NB == 2 && MAXE <= 8) ? 2 : 3) k_fstage2(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
-                                                 const FGroup *__restrict__ groups, const DevFreqPlan *__restrict__ plans,
-                                                 const uint8_t *__restrict__ valid, int64_t valid_stride,
-                                                 const FftParam *__restrict__ params, const float2 *__restrict__ twiddle,
-                                                 int maxN, int T, int TQ, int Tpad, int order, int fractionallofreq,
-                                                 int nbufmax, int rawcap_words, void *__restrict__ spec_out)
+// C: lane type (cf: FP32, one band per value; hc: FP16, both bands per value)
+// NV: values per point (cf: bands of the item; hc: 1); KB: butterflies per
+// thread and radix-8 pass.
+template <typename C, int NV, int KB>
+__global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage(const FsArgs a)
 {
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	__shared__ unsigned fmask_s;
-	__shared__ float lut8_s[256];
+	using TW = typename std::conditional<std::is_same<C, hc>::value, hw, float2>::type;
+	constexpr bool H = std::is_same<C, hc>::value;
+	extern __shared__ __align__(16) uint2 fsm[];
+	__shared__ float lut8[256];
 
-	// work item and station description, once into registers
-	const FGroup *gp = groups + blockIdx.y;
-	const int s = gp->station;
-	const int gfreq = gp->freq;
-	int band[2] = {gp->band[0], gp->band[1]};
-	int row[2] = {gp->row[0], gp->row[1]};
-	const bool lsb = gp->lsb != 0;
-	const double lo = gp->lofreq;
-	const DevStation *Sp = st + s;
+	const FGroup g = a.groups[a.first + blockIdx.y];
+	const DevStation *Sp = a.st + g.station;
 	const int N = Sp->fftchannels, nchan = Sp->nchan;
 	const uint32_t fs = (uint32_t)Sp->framesamples;
-	const int nbits = Sp->nbits, nband = Sp->nband;
-	const uint32_t payload = (uint32_t)Sp->payload;
-	const int header = Sp->header, framebytes = Sp->framebytes;
-	const int asl = Sp->asl;
+	const int nbits = Sp->nbits;
+	const uint32_t bpt = (uint32_t)(Sp->nband * nbits);
+	const int header = Sp->header, framebytes = Sp->framebytes, asl = Sp->asl;
 	const double bw = Sp->bw;
-	const uint8_t *buf = sub[s].buf;
-	const int64_t nframes = sub[s].nbytes / framebytes;
+	const uint8_t *buf = a.sub[g.station].buf;
+	const int64_t nframes = a.sub[g.station].nbytes / framebytes;
 	const int logN = 31 - __clz(N);
-	const int padN = N + (N >> 5);
-	float *const fbuf = (float *)smem_raw;                          // buffer k: re at 2k padN, im at (2k+1) padN
-	uint32_t *raw = (uint32_t *)(fbuf + 2 * nbufmax * padN);        // staged packed words
-	__nv_bfloat16 *stage = (__nv_bfloat16 *)(raw + rawcap_words);   // OUT == 1: [NB*2][TQ][nchan]
-	const uint8_t *vrow = valid + (int64_t)s * valid_stride;
-	const int twscale = maxN / N;
-	const uint32_t bits_per_time = (uint32_t)(nband * nbits);
-	const int64_t spec_off = plans[gfreq].spec_off;
-	const int prow = plans[gfreq].nrow;
-	const int r2pad = plans[gfreq].r2pad;
-	const int t0 = blockIdx.x * TQ;
-	const int tq_n = min(TQ, T - t0);
+	const int padN = xpad(N);
+	const int TPF = N / (8 * KB);
+	const int FPC = blockDim.x / TPF;
+	const int slot = threadIdx.x / TPF, bt = threadIdx.x - slot * TPF;
+	uint2 *const side0 = fsm + (size_t)slot * NV * padN;
+	uint2 *const side1 = a.pp ? side0 + (size_t)FPC * NV * padN : side0;
+	const uint8_t *vrow = a.valid + (int64_t)g.station * a.valid_stride;
+	const int twscale = a.maxN / N;
+	const TW *tw = (const TW *)a.tw;
+	const int64_t spec_off = a.plans[g.freq].spec_off;
+	const int prow = a.plans[g.freq].nrow;
+	const bool lsb = g.lsb != 0;
+	const double lo = g.lofreq;
+	const int row[2] = {g.row[0], g.row[1]};
+	const uint32_t boff0 = (uint32_t)(g.band[0] * nbits), boff1 = (uint32_t)(g.band[1] * nbits);
+	const bool oneword = bpt <= 32;       // all bands of a sample time in one 32-bit word
+	const int order = a.order;
+	int hexp = 0;
+	if(H)
+	{
+		// largest |X| is N times the largest level; keep it below 2^15
+		const float lvl = nbits == 2 ? 3.3359f : 38.8f;
+		while(lvl * (float)N > 32768.0f * (float)(1 << hexp))
+			hexp++;
+	}
+	const float hin = H ? ldexpf(1.0f, -hexp) : 1.0f, hout = H ? ldexpf(1.0f, hexp) : 1.0f;
 	if(nbits == 8)
 	{
 		// (b - 128) / 3.3 in double, rounded to float (format_vdif.c:122)
 		for(int i = threadIdx.x; i < 256; i += blockDim.x)
-			lut8_s[i] = (float)((i - 128) / 3.3);
+			lut8[i] = (float)((i - 128) / 3.3);
 	}
+	__syncthreads();
 
-	for(int tq = 0; tq < tq_n; tq++)
+	const int t0 = blockIdx.x * a.tq * FPC;
+	const int nit = min(a.tq, (a.T - t0 + FPC - 1) / FPC);
+	int wb = 0;
+	for(int it = 0; it < nit; it++)
 	{
-		const int t = t0 + tq;
-		const FftParam p = params[(int64_t)s * T + t];
-		if(p.status != kFftOk)
-		{
-#pragma unroll
-			for(int k = 0; k < NB; k++)
-				for(int c = threadIdx.x; c < nchan; c += blockDim.x)
-				{
-					if(OUT == 0)
-					{
-						if(row[k] >= 0)
-							((float2 *)spec_out)[spec_off + ((int64_t)t * prow + row[k]) * nchan + c] =
-							    make_float2(0.0f, 0.0f);
-					}
-					else
-					{
-						stage[((size_t)(2 * k) * TQ + tq) * nchan + c] = __float2bfloat16_rn(0.0f);
-						stage[((size_t)(2 * k + 1) * TQ + tq) * nchan + c] = __float2bfloat16_rn(0.0f);
-					}
-				}
-			continue;
-		}
-		// ---- 1. stage the packed words of the window [nearest, nearest + N)
-		// (all offsets fit in 32 bits: a station buffer holds < 2^31 samples)
-		const uint32_t g0 = (uint32_t)p.nearest;
-		const uint32_t fa = g0 / fs;
-		const uint32_t so = g0 - fa * fs;                               // window start in stream samples
-		const uint32_t sb0 = ((so * bits_per_time) >> 3) & ~7u;         // first staged byte (8-aligned)
-		const uint32_t sbe = ((so + (uint32_t)N) * bits_per_time + 7) >> 3;
-		const int nw8 = (int)((sbe - sb0 + 7) >> 3);
-		const bool staged = 2 * nw8 <= rawcap_words;
-		const int nwf = (int)((so + (uint32_t)N - 1) / fs) + 1;           // frames touched by the window
-		if(staged)
-		{
-			uint32_t sb = sb0 + 8u * threadIdx.x;
-			uint32_t k = sb / payload;
-			uint32_t off = sb - k * payload;
-			for(int w = threadIdx.x; w < nw8; w += blockDim.x)
-			{
-				const int64_t fr = (int64_t)fa + k;
-				uint2 v = make_uint2(0u, 0u);
-				if(fr < nframes)
-					v = __ldg((const uint2 *)(buf + fr * framebytes + header + off));
-				raw[2 * w] = v.x;
-				raw[2 * w + 1] = v.y;
-				off += 8u * blockDim.x;
-				while(off >= payload)
-				{
-					off -= payload;
-					k++;
-				}
-			}
-		}
-		if(threadIdx.x < 32)
-		{
-			// validity of the window's frames, one bit per frame (nwf <= 32)
-			const int64_t fr = (int64_t)fa + threadIdx.x;
-			const bool v = threadIdx.x < nwf && fr < valid_stride && vrow[fr];
-			const unsigned m = __ballot_sync(0xffffffffu, v);
-			if(threadIdx.x == 0)
-				fmask_s = m;
-		}
-		__syncthreads();
-		// ---- 2/3. decode, rotate into the FFT buffers
-		const double fraclo = fractionallofreq ? (lo - (int)lo) * (double)p.integerdelay : 0.0;
+		SlotConst sc;
+		sc.t = t0 + it * FPC + slot;
+		sc.tok = sc.t < a.T;
+		FftParam p;
+		if(sc.tok)
+			p = a.params[(int64_t)g.station * a.T + sc.t];
+		const bool active = sc.tok && p.status == kFftOk;
+		// ---- 1/2. decode and fringe-rotate x[b + r N/8] into registers
+		uint32_t fa = 0, so = 0;
+		int stuck = 0;
 		float P0 = 0.0f, alpha = 0.0f, beta = 0.0f, gamma = 0.0f, eps = 0.0f;
-		if(order == 1)
+		sc.dfs = 0.0f;
+		sc.postf = 0.0f;
+		if(active)
 		{
-			P0 = frac_centered(lo * p.b + fraclo);
-			alpha = (float)(lo * p.a / N);
-		}
-		else if(order == 2)
-		{
-			const double X1 = (double)asl / (double)N;
-			P0 = frac_centered(lo * p.c + fraclo);
-			alpha = (float)(lo * (p.b + p.a * X1) / N);
-			beta = (float)(lo * 2.0 * p.a * X1 / N);
-			gamma = (float)(lo * p.b * asl / N);
-			eps = (float)(lo * p.a * X1 * X1);
-		}
-		const uint32_t fmask = fmask_s;
-		const bool wide = nwf > 32;                                       // tiny frames: look validity up per sample
-		const uint32_t bitbase = so * bits_per_time - sb0 * 8u;
-		const int stuck = p.stuck;
-		uint32_t boff[NB];
-#pragma unroll
-		for(int k = 0; k < NB; k++)
-			boff[k] = (uint32_t)(band[k] * nbits);
-		uint32_t kf = (so + threadIdx.x) / fs;                           // frame of the thread's sample (rel. fa)
-		uint32_t kend = (kf + 1) * fs - so;                               // window index where that frame ends
-		for(int n = threadIdx.x; n < N; n += blockDim.x)
-		{
-			while((uint32_t)n >= kend)
+			const uint32_t g0 = (uint32_t)p.nearest;
+			fa = g0 / fs;
+			so = g0 - fa * fs;
+			stuck = p.stuck;
+			const double fraclo = a.fraclo ? (lo - (int)lo) * (double)p.integerdelay : 0.0;
+			if(order == 1)
 			{
-				kf++;
-				kend += fs;
+				P0 = frac_centered(lo * p.b + fraclo);
+				alpha = (float)(lo * p.a / N);
 			}
-			bool ok = wide ? ((int64_t)fa + kf < valid_stride && vrow[(int64_t)fa + kf]) : ((fmask >> kf) & 1u);
-			ok = ok && n < stuck;
-			float sn = 0.0f, cs = 1.0f;
-			if(order != 0)
+			else if(order == 2)
 			{
-				float ph;
-				if(order == 1)
-					ph = P0 + (float)n * alpha;
-				else
-				{
-					const int kk = n / asl, jj = n - kk * asl;
-					ph = P0 + (float)jj * alpha + (float)(kk * jj) * beta + (float)kk * gamma + (float)(kk * kk) * eps;
-				}
-				ph -= rintf(ph);
-				__sincosf(-6.283185307179586f * ph, &sn, &cs);
+				const double X1 = (double)asl / (double)N;
+				P0 = frac_centered(lo * p.c + fraclo);
+				alpha = (float)(lo * (p.b + p.a * X1) / N);
+				beta = (float)(lo * 2.0 * p.a * X1 / N);
+				gamma = (float)(lo * p.b * asl / N);
+				eps = (float)(lo * p.a * X1 * X1);
 			}
-			const uint32_t nbit = bitbase + (uint32_t)n * bits_per_time;
-#pragma unroll
-			for(int k = 0; k < NB; k++)
+			sc.dfs = (float)(bw / nchan * (double)p.fse);
+			if(order == 0)
 			{
-				float v = 0.0f;
-				if(ok)
+				double pr = (p.averagedelay - p.integerdelay) * lo;
+				if(a.fraclo)
+					pr += p.integerdelay * (lo - (int)lo);
+				sc.postf = -(float)(pr - (int)pr);
+			}
+		}
+		// ---- 1-3. decode, fringe-rotate and run the first radix-8 pass (s = 1:
+		// butterfly b, twiddle w_N^(r b)), one butterfly at a time
+		{
+			uint2 *dst = wb ? side1 : side0;
+			if(!a.pp)
+				__syncthreads();              // the single buffer has been read by the last FFT
+#pragma unroll
+			for(int k = 0; k < KB; k++)
+			{
+				const int b = bt + k * TPF;
+				const uint32_t xs = so + (uint32_t)b;
+				uint32_t kf = xs / fs, tin = xs - kf * fs;
+				C x[NV][8];
+#pragma unroll
+				for(int r = 0; r < 8; r++)
 				{
-					if(staged)
+					const int n = b + r * (N >> 3);
+					const int64_t fr = (int64_t)fa + kf;
+					bool ok = active && n < stuck && fr < nframes && fr < a.valid_stride;
+					ok = ok && __ldg(vrow + fr) != 0;
+					float v0 = 0.0f, v1 = 0.0f;
+					if(ok)
 					{
-						const uint32_t bit = nbit + boff[k];
-						const uint32_t word = raw[bit >> 5] >> (bit & 31);
-						v = nbits == 2 ? level2(word & 3u) : lut8_s[word & 255u];
+						const uint32_t *wp = (const uint32_t *)(buf + fr * framebytes + header);
+						const uint32_t bit0 = tin * bpt + boff0;
+						const uint32_t raw0 = __ldg(wp + (bit0 >> 5));
+						const uint32_t w0 = raw0 >> (bit0 & 31u);
+						v0 = nbits == 2 ? level2(w0 & 3u) : lut8[w0 & 255u];
+						if(H || NV == 2)
+						{
+							const uint32_t bit1 = tin * bpt + boff1;
+							const uint32_t w1 = (oneword ? raw0 : __ldg(wp + (bit1 >> 5))) >> (bit1 & 31u);
+							v1 = nbits == 2 ? level2(w1 & 3u) : lut8[w1 & 255u];
+						}
+					}
+					float sn = 0.0f, cs = 1.0f;
+					if(order != 0)
+					{
+						float ph;
+						if(order == 1)
+							ph = P0 + (float)n * alpha;
+						else
+						{
+							const int kk = n / asl, jj = n - kk * asl;
+							ph = P0 + (float)jj * alpha + (float)(kk * jj) * beta + (float)kk * gamma + (float)(kk * kk) * eps;
+						}
+						ph -= rintf(ph);
+						__sincosf(-6.283185307179586f * ph, &sn, &cs);
+					}
+					if constexpr(H)
+					{
+						x[0][r].x = __floats2half2_rn(v0 * cs * hin, v1 * cs * hin);
+						x[0][r].y = __floats2half2_rn(v0 * sn * hin, v1 * sn * hin);
 					}
 					else
 					{
-						const int64_t fr = (int64_t)fa + kf;
-						const int64_t tin = (int64_t)so + n - (int64_t)kf * fs;
-						const uint8_t *plb = buf + fr * framebytes + header;
-						const int64_t q = tin * nband + band[k];
-						if(nbits == 2)
-						{
-							const int64_t bit = q * 2;
-							v = level2((__ldg(plb + (bit >> 3)) >> (bit & 7)) & 3u);
-						}
-						else
-							v = lut8_s[__ldg(plb + q)];
+						x[0][r] = cf{v0 * cs, v0 * sn};
+						if constexpr(NV == 2)
+							x[1][r] = cf{v1 * cs, v1 * sn};
+					}
+					tin += (uint32_t)(N >> 3);
+					while(tin >= fs)
+					{
+						tin -= fs;
+						kf++;
 					}
 				}
-				fbuf[2 * k * padN + pad(n)] = v * cs;
-				fbuf[(2 * k + 1) * padN + pad(n)] = v * sn;
-			}
-		}
-		__syncthreads();
-		// ---- 4. FFTs of the NB bands together
-		fft_stockham<MAXE, NB>(fbuf, padN, N, logN, twiddle, twscale);
-		// ---- 5/6. sideband, fractional-sample rotation, output
-		const float dfs = (float)(bw / nchan * (double)p.fse);
-		float postf = 0.0f;
-		if(order == 0)
-		{
-			double pr = (p.averagedelay - p.integerdelay) * lo;
-			if(fractionallofreq)
-				pr += p.integerdelay * (lo - (int)lo);
-			postf = -(float)(pr - (int)pr);
-		}
-		for(int c = threadIdx.x; c < nchan; c += blockDim.x)
-		{
-			int src, ce;
-			float conj = 1.0f;
-			if(lsb)
-			{
-				ce = c - nchan;
-				if(order == 0)
+#pragma unroll
+				for(int j = 0; j < NV; j++)
+					dft8(x[j]);
+#pragma unroll
+				for(int r = 1; r < 8; r++)
 				{
-					src = nchan - c;
-					conj = -1.0f;
+					const TW w = ldtw(tw, r * b * twscale);
+#pragma unroll
+					for(int j = 0; j < NV; j++)
+						x[j][r] = twid(x[j][r], w);
 				}
-				else
-					src = nchan + c;
+				const int o = xpad(8 * b);
+#pragma unroll
+				for(int j = 0; j < NV; j++)
+				{
+					uint2 *q = dst + j * padN + o;
+					sts2(q, x[j][0], x[j][1]);
+					sts2(q + 2, x[j][2], x[j][3]);
+					sts2(q + 4, x[j][4], x[j][5]);
+					sts2(q + 6, x[j][6], x[j][7]);
+				}
+			}
+			__syncthreads();
+		}
+		// ---- middle radix-8 passes through shared memory
+		int logs = 3;
+		const int nmid = (logN % 3 == 0) ? logN / 3 - 2 : logN / 3 - 1;
+		for(int ps = 0; ps < nmid; ps++)
+		{
+			const int s = 1 << logs;
+			const int m = N >> (logs + 3);
+			const uint2 *src = wb ? side1 : side0;
+			wb ^= 1;
+			uint2 *dst = wb ? side1 : side0;
+			if(a.pp)
+			{
+				// two buffers: each butterfly reads, transforms and writes on its own
+#pragma unroll
+				for(int k = 0; k < KB; k++)
+				{
+					const int b = bt + k * TPF;
+					const int q = b & (s - 1), p8 = b >> logs;
+					C x[NV][8];
+					radix8_step<C, NV>(src, padN, q, s, p8, m, tw, twscale, x);
+#pragma unroll
+					for(int j = 0; j < NV; j++)
+#pragma unroll
+						for(int r = 0; r < 8; r++)
+							sts(dst + j * padN + xpad(q + s * (8 * p8 + r)), x[j][r]);
+				}
 			}
 			else
 			{
-				ce = c;
-				src = c;
-			}
-			float turns = (float)ce * dfs + postf;
-			turns -= rintf(turns);
-			float sn, cs;
-			__sincosf(6.283185307179586f * turns, &sn, &cs);
-			const int ps = pad(src);
+				// one buffer: all reads of the pass before any write
+				C x[KB][NV][8];
 #pragma unroll
-			for(int k = 0; k < NB; k++)
-			{
-				const float xr = fbuf[2 * k * padN + ps], xi = conj * fbuf[(2 * k + 1) * padN + ps];
-				const float yr = xr * cs - xi * sn, yi = xr * sn + xi * cs;
-				if(OUT == 0)
+				for(int k = 0; k < KB; k++)
 				{
-					if(row[k] >= 0)
-						((float2 *)spec_out)[spec_off + ((int64_t)t * prow + row[k]) * nchan + c] = make_float2(yr, yi);
+					const int b = bt + k * TPF;
+					radix8_step<C, NV>(src, padN, b & (s - 1), s, b >> logs, m, tw, twscale, x[k]);
 				}
-				else
+				__syncthreads();
+#pragma unroll
+				for(int k = 0; k < KB; k++)
 				{
-					stage[((size_t)(2 * k) * TQ + tq) * nchan + c] = __float2bfloat16_rn(yr);
-					stage[((size_t)(2 * k + 1) * TQ + tq) * nchan + c] = __float2bfloat16_rn(yi);
+					const int b = bt + k * TPF;
+					const int q = b & (s - 1), p8 = b >> logs;
+#pragma unroll
+					for(int j = 0; j < NV; j++)
+#pragma unroll
+						for(int r = 0; r < 8; r++)
+							sts(dst + j * padN + xpad(q + s * (8 * p8 + r)), x[k][j][r]);
 				}
 			}
+			__syncthreads();
+			logs += 3;
 		}
-		__syncthreads();
-	}
-	if(OUT == 1)
-	{
-		// [chan][2 row + part][Tpad] bf16: each (channel, real row) receives the
-		// chunk's TQ consecutive times in one 16-byte store
-		__nv_bfloat16 *o = (__nv_bfloat16 *)spec_out;
-		const int nitems = NB * 2 * nchan;
-		for(int it = threadIdx.x; it < nitems; it += blockDim.x)
+		// ---- 4. last pass, sideband selection, fractional-sample rotation, output
 		{
-			const int c = it % nchan;
-			const int kp = it / nchan;            // k * 2 + part
-			const int k = kp >> 1, part = kp & 1;
-			const int rk = k == 0 ? row[0] : row[1];
-			if(rk < 0)
-				continue;
-			__nv_bfloat16 *dst = o + spec_off + ((int64_t)c * r2pad + 2 * rk + part) * Tpad + t0;
-			const __nv_bfloat16 *src = stage + (size_t)kp * TQ * nchan + c;
-			if(TQ == 8 && tq_n == 8)
-			{
-				__align__(16) __nv_bfloat16 v[8];
-#pragma unroll
-				for(int q = 0; q < 8; q++)
-					v[q] = src[(size_t)q * nchan];
-				*(uint4 *)dst = *(const uint4 *)v;
-			}
+			const uint2 *src = wb ? side1 : side0;
+			const int rl = logN - logs;
+			if(rl == 3)
+				last_pass<C, NV, KB, 8>(src, padN, N, nchan, TPF, bt, lsb, order, sc, row, prow, spec_off, hout, a.spec);
+			else if(rl == 2)
+				last_pass<C, NV, KB, 4>(src, padN, N, nchan, TPF, bt, lsb, order, sc, row, prow, spec_off, hout, a.spec);
 			else
-				for(int q = 0; q < tq_n; q++)
-					dst[q] = src[(size_t)q * nchan];
+				last_pass<C, NV, KB, 2>(src, padN, N, nchan, TPF, bt, lsb, order, sc, row, prow, spec_off, hout, a.spec);
+			wb ^= 1;
 		}
 	}
 }
 
-size_t fstage2_smem(int N, int nband, int nbits, int nchan, int out, int TQ, int nbufmax, int *rawcap_words)
+bool fstage_plan(int N, int nb, int out, FKind *k)
 {
-	const int padN = N + (N >> 5);
-	size_t fft = (size_t)2 * nbufmax * padN * sizeof(float);
-	// raw window: N samples x bits + 16 bytes slack, capped at 48 KB
-	size_t rawb = ((size_t)N * nband * nbits + 7) / 8 + 32;
-	if(rawb > 48 * 1024)
-		rawb = 0;                    // decode from global memory instead
-	rawb = (rawb + 15) & ~(size_t)15;
-	*rawcap_words = (int)(rawb / 4);
-	size_t stg = out == 1 ? (size_t)2 * 2 * nchan * TQ * sizeof(__nv_bfloat16) : 0;
-	return fft + rawb + stg;
+	k->N = N;
+	k->nb = nb;
+	k->kb = N <= 2048 ? 1 : (N == 4096 ? 2 : 4);
+	if(out == 0 && nb == 2 && k->kb != 1)
+		return false;                               // FP32 items of long FFTs hold one band
+	const int tpf = N / (8 * k->kb);
+	k->threads = tpf >= 256 ? tpf : 256;
+	k->fpc = k->threads / tpf;
+	const int nv = out == 1 ? 1 : nb;
+	const size_t side = (size_t)k->fpc * nv * xpad(N) * 8;
+	k->pp = 2 * side <= 80 * 1024 ? 1 : 0;
+	k->smem = side * (k->pp ? 2 : 1);
+	k->tq = 4;
+	k->out = out;
+	return k->smem <= 200 * 1024 && k->threads <= 512;
 }
 
-template <int MAXE, int OUT, int NB>
-static void launch_one(dim3 grid, size_t smem, cudaStream_t stream, const DevStation *st, const DevSubintStation *sub,
-                       const FGroup *groups, const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride,
-                       const FftParam *params, const float2 *twiddle, int maxN, int T, int TQ, int Tpad, int order,
-                       int fraclo, int nbufmax, int rawcap, void *out)
+template <typename C, int NV, int KB>
+static void launch_t(const FKind &k, int T, const FsArgs &a, cudaStream_t stream)
 {
-	cudaFuncSetAttribute(k_fstage2<MAXE, OUT, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-	k_fstage2<MAXE, OUT, NB><<<grid, 256, smem, stream>>>(st, sub, groups, plans, valid, valid_stride, params, twiddle,
-	                                                        maxN, T, TQ, Tpad, order, fraclo, nbufmax, rawcap, out);
+	cudaFuncSetAttribute(k_fstage<C, NV, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+	const int per = k.tq * k.fpc;
+	dim3 grid((T + per - 1) / per, k.count);
+	k_fstage<C, NV, KB><<<grid, k.threads, k.smem, stream>>>(a);
 }
 
-template <int MAXE>
-static void launch_maxe(int npair, int nsingle, int Tchunks, size_t smem, cudaStream_t stream, const DevStation *st,
-                        const DevSubintStation *sub, const FGroup *g, const DevFreqPlan *plans, const uint8_t *valid,
-                        int64_t valid_stride, const FftParam *params, const float2 *twiddle, int maxN, int T, int TQ,
-                        int Tpad, int order, int fl, int nbufmax, int rawcap, int out, void *spec)
+void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream)
 {
-	if(npair > 0)
+	if(k.count <= 0 || a.T <= 0)
+		return;
+	a.first = k.first;
+	a.tq = k.tq;
+	a.pp = k.pp;
+	if(k.out == 1)
 	{
-		dim3 grid(Tchunks, npair);
-		if(out == 0)
-			launch_one<MAXE, 0, 2>(grid, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN, T,
-			                       TQ, Tpad, order, fl, nbufmax, rawcap, spec);
+		if(k.kb == 1)
+			launch_t<hc, 1, 1>(k, a.T, a, stream);
+		else if(k.kb == 2)
+			launch_t<hc, 1, 2>(k, a.T, a, stream);
 		else
-			launch_one<MAXE, 1, 2>(grid, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN, T,
-			                       TQ, Tpad, order, fl, nbufmax, rawcap, spec);
+			launch_t<hc, 1, 4>(k, a.T, a, stream);
 	}
-	if(nsingle > 0)
-	{
-		dim3 grid(Tchunks, nsingle);
-		if(out == 0)
-			launch_one<MAXE, 0, 1>(grid, smem, stream, st, sub, g + npair, plans, valid, valid_stride, params, twiddle,
-			                       maxN, T, TQ, Tpad, order, fl, nbufmax, rawcap, spec);
-		else
-			launch_one<MAXE, 1, 1>(grid, smem, stream, st, sub, g + npair, plans, valid, valid_stride, params, twiddle,
-			                       maxN, T, TQ, Tpad, order, fl, nbufmax, rawcap, spec);
-	}
-}
-
-void launch_fstage2(const DevStation *st, const DevSubintStation *sub, const void *groups, int npair, int nsingle,
-                    const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride, const FftParam *params,
-                    const float2 *twiddle, int maxN, int T, int TQ, int Tpad, int order, bool fractionallofreq,
-                    int N, int nband_max, int nbits_max, int nbufmax, int out, void *spec, cudaStream_t stream)
-{
-	int rawcap = 0;
-	size_t smem = fstage2_smem(N, nband_max, nbits_max, N / 2, out, TQ, nbufmax, &rawcap);
-	const int me = N / 256;     // elements per thread and pass
-	const FGroup *g = (const FGroup *)groups;
-	const int fl = fractionallofreq ? 1 : 0;
-	const int tch = (T + TQ - 1) / TQ;
-	if(me <= 8)
-		launch_maxe<8>(npair, nsingle, tch, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN,
-		               T, TQ, Tpad, order, fl, nbufmax, rawcap, out, spec);
-	else if(me <= 16)
-		launch_maxe<16>(npair, nsingle, tch, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN,
-		                T, TQ, Tpad, order, fl, nbufmax, rawcap, out, spec);
-	else if(me <= 32)
-		launch_maxe<32>(npair, nsingle, tch, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN,
-		                T, TQ, Tpad, order, fl, nbufmax, rawcap, out, spec);
+	else if(k.nb == 2)
+		launch_t<cf, 2, 1>(k, a.T, a, stream);
+	else if(k.kb == 1)
+		launch_t<cf, 1, 1>(k, a.T, a, stream);
+	else if(k.kb == 2)
+		launch_t<cf, 1, 2>(k, a.T, a, stream);
 	else
-		launch_maxe<64>(npair, nsingle, tch, smem, stream, st, sub, g, plans, valid, valid_stride, params, twiddle, maxN,
-		                T, TQ, Tpad, order, fl, nbufmax, rawcap, out, spec);
+		launch_t<cf, 1, 4>(k, a.T, a, stream);
 }
 
-size_t fgroup_size() { return sizeof(FGroup); }
-
-void make_fgroup(void *dst, int station, int freq, int b0, int b1, int r0, int r1, int lsb, double lofreq)
+void make_fstage_twiddles16(const double *re, const double *im, int n, void *out)
 {
-	FGroup g;
-	g.station = station;
-	g.freq = freq;
-	g.band[0] = b0;
-	g.band[1] = b1 < 0 ? b0 : b1;
-	g.row[0] = r0;
-	g.row[1] = r1;
-	g.nb = b1 < 0 ? 1 : 2;
-	g.lsb = lsb;
-	g.lofreq = lofreq;
-	*(FGroup *)dst = g;
+	uint2 *o = (uint2 *)out;
+	for(int i = 0; i < n; i++)
+	{
+		const __half r = __double2half(re[i]), q = __double2half(im[i]);
+		const __half2 rr = __halves2half2(r, r), qq = __halves2half2(q, q);
+		o[i].x = *(const uint32_t *)&rr;
+		o[i].y = *(const uint32_t *)&qq;
+	}
 }
 
 }  // namespace fxb

@@ -53,14 +53,44 @@ void launch_fstage(const DevStation *st, const DevSubintStation *sub, const DevB
                    const float2 *twiddle, int maxN, int S, int T, int order, bool fractionallofreq, int maxfft,
                    float2 *spec, cudaStream_t stream);
 
-// F stage v2 (csrc/fxb_fstage.cu): CTA per (station, subband, chunk of TQ FFTs).
-// out 0: FP32 rows [t][row][chan]; out 1: BF16 K-major [chan][2 row + part][tpad].
-void launch_fstage2(const DevStation *st, const DevSubintStation *sub, const void *groups, int npair, int nsingle,
-                    const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride, const FftParam *params,
-                    const float2 *twiddle, int maxN, int T, int TQ, int Tpad, int order, bool fractionallofreq,
-                    int N, int nband_max, int nbits_max, int nbufmax, int out, void *spec, cudaStream_t stream);
-size_t fgroup_size();
-void make_fgroup(void *dst, int station, int freq, int b0, int b1, int r0, int r1, int lsb, double lofreq);
+// F stage (csrc/fxb_fstage.cu).  A work item is one subband of one station
+// with the one or two bands recording it; items of the same kind (FFT length,
+// band packing) share a launch.
+struct FGroup {
+	int32_t station, freq;
+	int32_t band[2];
+	int32_t row[2];          // rows within the frequency's spectra (-1: band not output)
+	int32_t nb;
+	int32_t lsb;
+	double lofreq;
+};
+
+struct FKind {
+	int32_t first, count;    // range of work items in the item table
+	int32_t N, nb;           // FFT length, bands per item
+	int32_t kb, fpc;         // radix-8 butterflies per thread and pass, FFTs side by side per CTA
+	int32_t threads, tq;     // CTA size, FFT iterations per CTA
+	int32_t pp, out;         // two exchange buffers (else one), output form (0 FP32, 1 FP16 FFT -> bf16x2)
+	size_t smem;
+};
+
+struct FsArgs {
+	const DevStation *st;
+	const DevSubintStation *sub;
+	const FGroup *groups;
+	const DevFreqPlan *plans;
+	const uint8_t *valid;
+	int64_t valid_stride;
+	const FftParam *params;
+	const void *tw;          // exp(-2 pi i k / maxN): float2 (out 0) or half2 pairs (wr, wr), (wi, wi) (out 1)
+	int32_t maxN, T, tq, order;
+	int32_t fraclo, pp, first, pad;
+	void *spec;              // [t][row][chan]: float2 (out 0) or bf16x2 (out 1)
+};
+
+bool fstage_plan(int N, int nb, int out, FKind *k);
+void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream);
+void make_fstage_twiddles16(const double *re, const double *im, int n, void *out);
 
 // FP32 XMAC v2 over a set of frequencies with equal (rows, channels):
 // plan_idx[0..nf) index dplans.
@@ -73,6 +103,9 @@ size_t tc_tensormap_size();
 void tc_geometry(int R2, int Tpad, int *G, int *NG, int *boxrows, int *tmem_cols, size_t *smem);
 void launch_xmac_tc(const void *tmap, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int nchan,
                     const int64_t *rowbase, int Tpad, int R2, int32_t *err, float2 *acc, cudaStream_t stream);
+
+void launch_spec_kmajor(const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int nrow, int nchan, int T,
+                        int Tpad, const int64_t *rowbase, const uint32_t *specn, uint16_t *kmaj, cudaStream_t stream);
 
 // FP32 cross-multiply-accumulate of one frequency into acc.
 void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, const float2 *spec, float2 *acc,

@@ -380,4 +380,45 @@ void launch_xmac_tc(const void *tmap, const DevFreqPlan *dplans, const int32_t *
 	k_xmac_tc<<<grid, 128, smem, stream>>>(*(const CUtensorMap *)tmap, dplans, plan_idx, rowbase, tp, acc);
 }
 
+// bf16x2 spectra [t][row][chan] -> K-major bf16 [chan][2 row + part][Tpad]
+// starting at row rowbase[f] of the K-major buffer (32 x 32 tiles through
+// shared memory: coalesced along channels on the read, along time on the write)
+__global__ void k_spec_kmajor(const DevFreqPlan *__restrict__ plans, const int32_t *__restrict__ idx, int nrow,
+                              int nchan, int T, int Tpad, const int64_t *__restrict__ rowbase,
+                              const uint32_t *__restrict__ specn, uint16_t *__restrict__ kmaj)
+{
+	__shared__ uint32_t tile[32][33];
+	const int f = idx[blockIdx.z / nrow];
+	const int row = blockIdx.z % nrow;
+	const int64_t spec_off = plans[f].spec_off;
+	const int r2pad = plans[f].r2pad;
+	const int c0 = blockIdx.x * 32, t0 = blockIdx.y * 32;
+	for(int i = threadIdx.y; i < 32; i += blockDim.y)
+	{
+		const int t = t0 + i, c = c0 + threadIdx.x;
+		tile[i][threadIdx.x] = (t < T && c < nchan) ? specn[spec_off + ((int64_t)t * nrow + row) * nchan + c] : 0u;
+	}
+	__syncthreads();
+	for(int i = threadIdx.y; i < 32; i += blockDim.y)
+	{
+		const int c = c0 + i, t = t0 + threadIdx.x;
+		if(c < nchan && t < T)
+		{
+			const uint32_t v = tile[threadIdx.x][i];
+			const int64_t base = (rowbase[f] + (int64_t)c * r2pad + 2 * row) * Tpad + t;
+			kmaj[base] = (uint16_t)(v & 0xFFFFu);
+			kmaj[base + Tpad] = (uint16_t)(v >> 16);
+		}
+	}
+}
+
+void launch_spec_kmajor(const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int nrow, int nchan, int T,
+                        int Tpad, const int64_t *rowbase, const uint32_t *specn, uint16_t *kmaj, cudaStream_t stream)
+{
+	if(nf <= 0 || nrow <= 0)
+		return;
+	dim3 grid((nchan + 31) / 32, (T + 31) / 32, nf * nrow);
+	k_spec_kmajor<<<grid, dim3(32, 8), 0, stream>>>(dplans, plan_idx, nrow, nchan, T, Tpad, rowbase, specn, kmaj);
+}
+
 }  // namespace fxb
