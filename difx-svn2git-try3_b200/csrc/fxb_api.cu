@@ -68,7 +68,6 @@ struct fxb_ctx {
 	// F-stage work items (by kind) and FP32 XMAC v2 launch groups
 	FGroup *d_groups = nullptr;
 	std::vector<FKind> fkinds;
-	void *d_tw16 = nullptr;              // FP16 twiddles of the tensor-core form
 	void *d_specn = nullptr;             // bf16x2 spectra [t][row][chan] of the tensor-core form
 	struct XGroup { int plan0; int32_t *d_idx; int nf; };
 	std::vector<XGroup> xgroups;
@@ -231,22 +230,6 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		}
 		CK(ctx, dalloc(ctx, &ctx->d_twiddle, tw.size()));
 		CK(ctx, cudaMemcpy(ctx->d_twiddle, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
-		if(job.xmac_kind == FXB_XMAC_BF16)
-		{
-			std::vector<double> re(ctx->maxN), im(ctx->maxN);
-			for(int k = 0; k < ctx->maxN; k++)
-			{
-				double ang = -2.0 * M_PI * (double)k / (double)ctx->maxN;
-				re[k] = cos(ang);
-				im[k] = sin(ang);
-			}
-			std::vector<uint2> h(ctx->maxN);
-			make_fstage_twiddles16(re.data(), im.data(), ctx->maxN, h.data());
-			uint2 *d = nullptr;
-			CK(ctx, dalloc(ctx, &d, h.size()));
-			CK(ctx, cudaMemcpy(d, h.data(), sizeof(uint2) * h.size(), cudaMemcpyHostToDevice));
-			ctx->d_tw16 = d;
-		}
 	}
 
 	// per-frequency plans
@@ -405,6 +388,24 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			}
 			k.first = (int)hg.size();
 			k.count = (int)kv.second.size();
+			if(out == 1)
+			{
+				std::vector<uint2> h((size_t)k.twn);
+				make_fstage_twiddles(k.N, nullptr, h.data());
+				uint2 *d = nullptr;
+				CK(ctx, dalloc(ctx, &d, h.size()));
+				CK(ctx, cudaMemcpy(d, h.data(), sizeof(uint2) * h.size(), cudaMemcpyHostToDevice));
+				k.tw = d;
+			}
+			else
+			{
+				std::vector<float2> h((size_t)k.twn);
+				make_fstage_twiddles(k.N, h.data(), nullptr);
+				float2 *d = nullptr;
+				CK(ctx, dalloc(ctx, &d, h.size()));
+				CK(ctx, cudaMemcpy(d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
+				k.tw = d;
+			}
 			hg.insert(hg.end(), kv.second.begin(), kv.second.end());
 			ctx->fkinds.push_back(k);
 		}
@@ -678,7 +679,6 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 		fa.valid = ctx->d_valid;
 		fa.valid_stride = ctx->valid_stride;
 		fa.params = ctx->d_params;
-		fa.tw = ctx->tc ? ctx->d_tw16 : (const void *)ctx->d_twiddle;
 		fa.maxN = ctx->maxN;
 		fa.T = ctx->T;
 		fa.order = job.fringe_rot_order;

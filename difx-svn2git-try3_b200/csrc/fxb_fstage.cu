@@ -1,10 +1,11 @@
 // F stage (Mode::process, mpifxcorr/src/mode.cpp:845-1308) for sm_100a.
 //
 // One CTA per (station, subband, chunk of FFTs); a subband's one or two
-// polarisation bands are transformed together.  Each thread owns KB radix-8
-// butterflies of every pass of one FFT ("slot"): an FFT of N points takes
-// N / (8 KB) threads, and a CTA runs several slots side by side when N is
-// small.  Per FFT a thread
+// polarisation bands are transformed together.  The FFT length is a template
+// parameter, so the pass schedule and every shared-memory index fold to
+// constants.  Each thread owns KB radix-8 butterflies of every pass of one
+// FFT ("slot"): an FFT of N points takes N / (8 KB) threads, and a CTA runs
+// several slots side by side when N is small.  Per FFT a thread
 //   1. decodes its 8 KB samples x[b + r N/8] straight from the VDIF words in
 //      global memory (2-bit / 8-bit levels of format_vdif.c:74-149; samples of
 //      invalid frames and, for 8-bit 2/4-channel streams, every sample after
@@ -27,6 +28,10 @@
 //          advances both polarisations), spectra as bf16x2 (re, im) for the
 //          tensor-core XMAC.  Samples are scaled by 2^-e so that no FFT value
 //          can leave the FP16 range; the outputs are scaled back exactly.
+//
+// Twiddles come from a per-length table laid out [pass][r - 1][p] (entry
+// w_N^(r p s) for pass stride s), so that the twiddle loads of a warp are
+// coalesced (first pass) or broadcasts (later passes).
 
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
@@ -44,7 +49,33 @@ namespace {
 // padded index of 8-byte element i: every exchange of the pass schedule
 // below is free of bank conflicts, and runs of 8 starting at multiples of 8
 // stay contiguous and 16-byte aligned (the first pass stores them as pairs)
-__host__ __device__ __forceinline__ int xpad(int i) { return i + 2 * (i >> 4); }
+__host__ __device__ constexpr int xpad(int i) { return i + 2 * (i >> 4); }
+
+// Compile-time shape of the F stage for FFT length 2^LOGN.
+template <int LOGN>
+struct FShape {
+	static constexpr int N = 1 << LOGN;
+	static constexpr int KB = N <= 2048 ? 1 : (N == 4096 ? 2 : 4);
+	static constexpr int TPF = N / (8 * KB);                 // threads per FFT
+	static constexpr int NT = TPF >= 256 ? TPF : 256;        // threads per CTA
+	static constexpr int FPC = NT / TPF;                     // FFTs side by side
+	static constexpr int PADN = xpad(N);
+	static constexpr int NMID = (LOGN % 3 == 0) ? LOGN / 3 - 2 : LOGN / 3 - 1;
+	static constexpr int RL = (LOGN % 3 == 0) ? 8 : (1 << (LOGN % 3));
+	static constexpr int MINB = KB == 1 ? 3 : (NT == 256 ? 2 : 1);
+};
+
+// offset of the twiddles of radix-8 pass `pass` (stride 8^pass) in the table
+__host__ __device__ constexpr int tw_offset(int N, int pass)
+{
+	int o = 0, n8 = N / 8;
+	for(int i = 0; i < pass; i++)
+	{
+		o += 7 * n8;
+		n8 /= 8;
+	}
+	return o;
+}
 
 // ---- lane values: FP32 complex (one band), packed FP16 complex (two bands)
 struct cf { float x, y; };
@@ -153,9 +184,9 @@ __device__ __forceinline__ void dft2(C *x)
 template <int R, typename C>
 __device__ __forceinline__ void dftR(C *x)
 {
-	if(R == 8)
+	if constexpr(R == 8)
 		dft8(x);
-	else if(R == 4)
+	else if constexpr(R == 4)
 		dft4(x);
 	else
 		dft2(x);
@@ -163,7 +194,7 @@ __device__ __forceinline__ void dftR(C *x)
 
 // 2-bit code -> {-HiMag, -1, +1, +HiMag} (format_vdif.c:78): sign from bit 1,
 // magnitude HiMag for codes 0 and 3
-__device__ __forceinline__ float level2(uint32_t code)
+__host__ __device__ inline float level2(uint32_t code)
 {
 	const float mag = ((code ^ (code >> 1)) & 1u) ? 1.0f : 3.3359f;
 	return (code & 2u) ? mag : -mag;
@@ -171,160 +202,128 @@ __device__ __forceinline__ float level2(uint32_t code)
 
 __device__ __forceinline__ float frac_centered(double x) { return (float)(x - rint(x)); }
 
-// per-FFT constants of one slot
-struct SlotConst {
-	int t;
-	bool tok;         // t < T
-	float dfs;        // fractional-sample rotation turns per channel
-	float postf;      // order-0 post-F fringe turns
+// One middle radix-8 pass (stride s = 2^LOGS, m = N / (8 s)) over the
+// thread's KB butterflies: x_r = X[q + s (p + r m)], y = DFT8(x),
+// Y[q + s (8 p + r)] = y_r w_N^(r p s).  With two buffers each butterfly
+// reads, transforms and writes on its own; with one buffer all reads of the
+// pass come before any write.
+template <typename C, int NV, int LOGN, int LOGS, typename TW>
+__device__ __forceinline__ void mid_pass(int &wb, uint2 *side0, uint2 *side1, int pp, int bt, const TW *twp)
+{
+	using SH = FShape<LOGN>;
+	constexpr int N = SH::N, KB = SH::KB, TPF = SH::TPF, PADN = SH::PADN;
+	constexpr int s = 1 << LOGS;
+	constexpr int m = N >> (LOGS + 3);
+	constexpr int np = N / (8 * s);
+	const uint2 *src = wb ? side1 : side0;
+	wb ^= 1;
+	uint2 *dst = wb ? side1 : side0;
+	C x[KB][NV][8];
+#pragma unroll
+	for(int k = 0; k < KB; k++)
+	{
+		const int b = bt + k * TPF;
+		const int q = b & (s - 1), p8 = b >> LOGS;
+#pragma unroll
+		for(int j = 0; j < NV; j++)
+		{
+#pragma unroll
+			for(int r = 0; r < 8; r++)
+			{
+				// for N >= 128 the stride s m = N/8 is a multiple of 16, so the
+				// padding of point r is a constant offset from that of point 0
+				if constexpr(N >= 128)
+					x[k][j][r] = lds<C>(src + j * PADN + xpad(q + s * p8) + r * xpad(s * m));
+				else
+					x[k][j][r] = lds<C>(src + j * PADN + xpad(q + s * (p8 + r * m)));
+			}
+			dft8(x[k][j]);
+		}
+#pragma unroll
+		for(int r = 1; r < 8; r++)
+		{
+			const TW w = ldtw(twp, (r - 1) * np + p8);
+#pragma unroll
+			for(int j = 0; j < NV; j++)
+				x[k][j][r] = twid(x[k][j][r], w);
+		}
+		if(pp)
+		{
+#pragma unroll
+			for(int j = 0; j < NV; j++)
+#pragma unroll
+				for(int r = 0; r < 8; r++)
+					sts(dst + j * PADN + xpad(q + s * (8 * p8 + r)), x[k][j][r]);
+		}
+	}
+	if(!pp)
+	{
+		__syncthreads();
+#pragma unroll
+		for(int k = 0; k < KB; k++)
+		{
+			const int b = bt + k * TPF;
+			const int q = b & (s - 1), p8 = b >> LOGS;
+#pragma unroll
+			for(int j = 0; j < NV; j++)
+#pragma unroll
+				for(int r = 0; r < 8; r++)
+					sts(dst + j * PADN + xpad(q + s * (8 * p8 + r)), x[k][j][r]);
+		}
+	}
+	__syncthreads();
+}
+
+template <typename C, int NV, int LOGN, int PS>
+struct MidPasses {
+	template <typename TW>
+	__device__ static __forceinline__ void run(int &wb, uint2 *side0, uint2 *side1, int pp, int bt, const TW *tw)
+	{
+		if constexpr(PS < FShape<LOGN>::NMID)
+		{
+			mid_pass<C, NV, LOGN, 3 * (PS + 1)>(wb, side0, side1, pp, bt, tw + tw_offset(1 << LOGN, PS + 1));
+			MidPasses<C, NV, LOGN, PS + 1>::run(wb, side0, side1, pp, bt, tw);
+		}
+	}
 };
-
-// One radix-8 butterfly of a middle pass (stride s = 2^logs, m = N / (8 s)):
-// x_r = X[q + s (p + r m)], y = DFT8(x), y_r *= w_N^(r p s).
-template <typename C, int NV, typename TW>
-__device__ __forceinline__ void radix8_step(const uint2 *src, int padN, int q, int s, int p8, int m, const TW *tw,
-                                            int twscale, C (&x)[NV][8])
-{
-#pragma unroll
-	for(int j = 0; j < NV; j++)
-	{
-#pragma unroll
-		for(int r = 0; r < 8; r++)
-			x[j][r] = lds<C>(src + j * padN + xpad(q + s * (p8 + r * m)));
-		dft8(x[j]);
-	}
-#pragma unroll
-	for(int r = 1; r < 8; r++)
-	{
-		const TW w = ldtw(tw, r * p8 * s * twscale);
-#pragma unroll
-		for(int j = 0; j < NV; j++)
-			x[j][r] = twid(x[j][r], w);
-	}
-}
-
-// Output of the last pass (radix R, stride sL = N/R, no twiddles): bins
-// q + sL r of the butterflies q = bt + j TPF go to their channels.
-template <typename C, int NV, int KB, int R>
-__device__ __forceinline__ void last_pass(const uint2 *src, int padN, int N, int nchan, int TPF, int bt, bool lsb,
-                                          int order, const SlotConst &sc, const int row[2], int prow,
-                                          int64_t spec_off, float hout, void *spec)
-{
-	constexpr bool H = std::is_same<C, hc>::value;
-	constexpr int J = (KB * 8) / R;
-	const int sL = N / R;
-#pragma unroll
-	for(int jj = 0; jj < J; jj++)
-	{
-		const int q = bt + jj * TPF;
-		C y[NV][R];
-#pragma unroll
-		for(int j = 0; j < NV; j++)
-		{
-#pragma unroll
-			for(int r = 0; r < R; r++)
-				y[j][r] = lds<C>(src + j * padN + xpad(q + sL * r));
-			dftR<R>(y[j]);
-		}
-#pragma unroll
-		for(int r = 0; r < R; r++)
-		{
-			const int k = q + sL * r;
-			int c, ce;
-			bool use;
-			float cj = 1.0f;
-			if(!lsb)
-			{
-				use = k < nchan;
-				c = k;
-				ce = k;
-			}
-			else if(order != 0)
-			{
-				use = k >= nchan;
-				c = k - nchan;
-				ce = c - nchan;
-			}
-			else
-			{
-				use = k >= 1 && k <= nchan;
-				c = nchan - k;
-				ce = c - nchan;
-				cj = -1.0f;
-			}
-			if(!use || !sc.tok)
-				continue;
-			float turns = (float)ce * sc.dfs + sc.postf;
-			turns -= rintf(turns);
-			float sn, cs;
-			__sincosf(6.283185307179586f * turns, &sn, &cs);
-			const int64_t o0 = spec_off + ((int64_t)sc.t * prow) * nchan + c;
-			if constexpr(H)
-			{
-				const hc v = y[0][r];
-				const float xr[2] = {__low2float(v.x) * hout, __high2float(v.x) * hout};
-				const float xi[2] = {cj * __low2float(v.y) * hout, cj * __high2float(v.y) * hout};
-#pragma unroll
-				for(int b = 0; b < 2; b++)
-					if(row[b] >= 0)
-						((__nv_bfloat162 *)spec)[o0 + (int64_t)row[b] * nchan] =
-						    __floats2bfloat162_rn(xr[b] * cs - xi[b] * sn, xr[b] * sn + xi[b] * cs);
-			}
-			else
-			{
-#pragma unroll
-				for(int j = 0; j < NV; j++)
-					if(row[j] >= 0)
-					{
-						const cf v = y[j][r];
-						const float xr = v.x, xi = cj * v.y;
-						((float2 *)spec)[o0 + (int64_t)row[j] * nchan] = make_float2(xr * cs - xi * sn, xr * sn + xi * cs);
-					}
-			}
-		}
-	}
-}
 
 }  // namespace
 
-// C: lane type (cf: FP32, one band per value; hc: FP16, both bands per value)
-// NV: values per point (cf: bands of the item; hc: 1); KB: butterflies per
-// thread and radix-8 pass.
-template <typename C, int NV, int KB>
-__global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage(const FsArgs a)
+// C: lane type (cf: FP32, one band per value; hc: FP16, both bands per value);
+// NV: values per point (cf: bands of the item; hc: 1).
+template <typename C, int NV, int LOGN>
+__global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage(const FsArgs a)
 {
-	using TW = typename std::conditional<std::is_same<C, hc>::value, hw, float2>::type;
+	using SH = FShape<LOGN>;
+	constexpr int N = SH::N, KB = SH::KB, TPF = SH::TPF, FPC = SH::FPC, PADN = SH::PADN, RL = SH::RL;
 	constexpr bool H = std::is_same<C, hc>::value;
+	using TW = typename std::conditional<H, hw, float2>::type;
 	extern __shared__ __align__(16) uint2 fsm[];
 	__shared__ float lut8[256];
+	__shared__ float2 lut4[16];            // two adjacent 2-bit bands -> (band0, band1) levels
 
 	const FGroup g = a.groups[a.first + blockIdx.y];
 	const DevStation *Sp = a.st + g.station;
-	const int N = Sp->fftchannels, nchan = Sp->nchan;
+	constexpr int nchan = N / 2;
 	const uint32_t fs = (uint32_t)Sp->framesamples;
 	const int nbits = Sp->nbits;
 	const uint32_t bpt = (uint32_t)(Sp->nband * nbits);
 	const int header = Sp->header, framebytes = Sp->framebytes, asl = Sp->asl;
 	const double bw = Sp->bw;
 	const uint8_t *buf = a.sub[g.station].buf;
-	const int64_t nframes = a.sub[g.station].nbytes / framebytes;
-	const int logN = 31 - __clz(N);
-	const int padN = xpad(N);
-	const int TPF = N / (8 * KB);
-	const int FPC = blockDim.x / TPF;
 	const int slot = threadIdx.x / TPF, bt = threadIdx.x - slot * TPF;
-	uint2 *const side0 = fsm + (size_t)slot * NV * padN;
-	uint2 *const side1 = a.pp ? side0 + (size_t)FPC * NV * padN : side0;
+	uint2 *const side0 = fsm + (size_t)slot * NV * PADN;
+	uint2 *const side1 = a.pp ? side0 + (size_t)FPC * NV * PADN : side0;
 	const uint8_t *vrow = a.valid + (int64_t)g.station * a.valid_stride;
-	const int twscale = a.maxN / N;
 	const TW *tw = (const TW *)a.tw;
 	const int64_t spec_off = a.plans[g.freq].spec_off;
 	const int prow = a.plans[g.freq].nrow;
 	const bool lsb = g.lsb != 0;
 	const double lo = g.lofreq;
-	const int row[2] = {g.row[0], g.row[1]};
+	const int row0 = g.row[0], row1 = g.row[1];
 	const uint32_t boff0 = (uint32_t)(g.band[0] * nbits), boff1 = (uint32_t)(g.band[1] * nbits);
 	const bool oneword = bpt <= 32;       // all bands of a sample time in one 32-bit word
+	const bool pair4 = (H || NV == 2) && nbits == 2 && oneword && boff1 == boff0 + 2;
 	const int order = a.order;
 	int hexp = 0;
 	if(H)
@@ -341,6 +340,8 @@ __global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage
 		for(int i = threadIdx.x; i < 256; i += blockDim.x)
 			lut8[i] = (float)((i - 128) / 3.3);
 	}
+	if(threadIdx.x < 16)
+		lut4[threadIdx.x] = make_float2(level2(threadIdx.x & 3u), level2(threadIdx.x >> 2));
 	__syncthreads();
 
 	const int t0 = blockIdx.x * a.tq * FPC;
@@ -348,48 +349,62 @@ __global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage
 	int wb = 0;
 	for(int it = 0; it < nit; it++)
 	{
-		SlotConst sc;
-		sc.t = t0 + it * FPC + slot;
-		sc.tok = sc.t < a.T;
-		FftParam p;
-		if(sc.tok)
-			p = a.params[(int64_t)g.station * a.T + sc.t];
-		const bool active = sc.tok && p.status == kFftOk;
-		// ---- 1/2. decode and fringe-rotate x[b + r N/8] into registers
+		const int t = t0 + it * FPC + slot;
+		const bool tok = t < a.T;
+		// ---- per-FFT constants
+		bool active = false;
 		uint32_t fa = 0, so = 0;
 		int stuck = 0;
-		float P0 = 0.0f, alpha = 0.0f, beta = 0.0f, gamma = 0.0f, eps = 0.0f;
-		sc.dfs = 0.0f;
-		sc.postf = 0.0f;
-		if(active)
+		float P0 = 0.0f, alpha = 0.0f, beta = 0.0f, gamma = 0.0f, eps = 0.0f, dfs = 0.0f, postf = 0.0f;
+		if(tok)
 		{
-			const uint32_t g0 = (uint32_t)p.nearest;
-			fa = g0 / fs;
-			so = g0 - fa * fs;
-			stuck = p.stuck;
-			const double fraclo = a.fraclo ? (lo - (int)lo) * (double)p.integerdelay : 0.0;
-			if(order == 1)
+			const FftParam *pq = a.params + (int64_t)g.station * a.T + t;
+			active = pq->status == kFftOk;
+			if(active)
 			{
-				P0 = frac_centered(lo * p.b + fraclo);
-				alpha = (float)(lo * p.a / N);
+				const uint32_t g0 = (uint32_t)pq->nearest;
+				fa = g0 / fs;
+				so = g0 - fa * fs;
+				stuck = pq->stuck;
+				const double invN = 1.0 / N;
+				const int idl = pq->integerdelay;
+				const double fraclo = a.fraclo ? (lo - (int)lo) * (double)idl : 0.0;
+				if(order == 1)
+				{
+					P0 = frac_centered(lo * pq->b + fraclo);
+					alpha = (float)(lo * pq->a * invN);
+				}
+				else if(order == 2)
+				{
+					const double pa = pq->a, pb = pq->b;
+					const double X1 = (double)asl * invN;
+					P0 = frac_centered(lo * pq->c + fraclo);
+					alpha = (float)(lo * (pb + pa * X1) * invN);
+					beta = (float)(lo * 2.0 * pa * X1 * invN);
+					gamma = (float)(lo * pb * asl * invN);
+					eps = (float)(lo * pa * X1 * X1);
+				}
+				dfs = (float)(bw * (1.0 / nchan) * (double)pq->fse);
+				if(order == 0)
+				{
+					double pr = (pq->averagedelay - idl) * lo;
+					if(a.fraclo)
+						pr += idl * (lo - (int)lo);
+					postf = -(float)(pr - (int)pr);
+				}
 			}
-			else if(order == 2)
-			{
-				const double X1 = (double)asl / (double)N;
-				P0 = frac_centered(lo * p.c + fraclo);
-				alpha = (float)(lo * (p.b + p.a * X1) / N);
-				beta = (float)(lo * 2.0 * p.a * X1 / N);
-				gamma = (float)(lo * p.b * asl / N);
-				eps = (float)(lo * p.a * X1 * X1);
-			}
-			sc.dfs = (float)(bw / nchan * (double)p.fse);
-			if(order == 0)
-			{
-				double pr = (p.averagedelay - p.integerdelay) * lo;
-				if(a.fraclo)
-					pr += p.integerdelay * (lo - (int)lo);
-				sc.postf = -(float)(pr - (int)pr);
-			}
+		}
+		// validity of the window's frames, one bit per frame relative to fa
+		// (a warp holds one slot when TPF >= 32; otherwise looked up per sample)
+		const uint32_t nwf = (so + (uint32_t)N - 1) / fs + 1;
+		uint32_t fmask = 0;
+		const bool narrow = TPF >= 32 && nwf <= 32;
+		if constexpr(TPF >= 32)
+		{
+			const int lane = threadIdx.x & 31;
+			const int64_t fr = (int64_t)fa + lane;
+			const bool v = active && (uint32_t)lane < nwf && fr < a.valid_stride && vrow[fr] != 0;
+			fmask = __ballot_sync(0xffffffffu, v);
 		}
 		// ---- 1-3. decode, fringe-rotate and run the first radix-8 pass (s = 1:
 		// butterfly b, twiddle w_N^(r b)), one butterfly at a time
@@ -403,27 +418,43 @@ __global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage
 				const int b = bt + k * TPF;
 				const uint32_t xs = so + (uint32_t)b;
 				uint32_t kf = xs / fs, tin = xs - kf * fs;
+				const uint8_t *fp = buf + ((int64_t)fa + kf) * framebytes + header;
 				C x[NV][8];
 #pragma unroll
 				for(int r = 0; r < 8; r++)
 				{
-					const int n = b + r * (N >> 3);
-					const int64_t fr = (int64_t)fa + kf;
-					bool ok = active && n < stuck && fr < nframes && fr < a.valid_stride;
-					ok = ok && __ldg(vrow + fr) != 0;
+					const int n = b + r * (N / 8);
+					bool ok;
+					if(narrow)
+						ok = (fmask >> kf) & 1u;
+					else
+					{
+						const int64_t fr = (int64_t)fa + kf;
+						ok = active && fr < a.valid_stride && vrow[fr] != 0;
+					}
+					ok = ok && n < stuck;
 					float v0 = 0.0f, v1 = 0.0f;
 					if(ok)
 					{
-						const uint32_t *wp = (const uint32_t *)(buf + fr * framebytes + header);
 						const uint32_t bit0 = tin * bpt + boff0;
-						const uint32_t raw0 = __ldg(wp + (bit0 >> 5));
+						const uint32_t raw0 = __ldg((const uint32_t *)fp + (bit0 >> 5));
 						const uint32_t w0 = raw0 >> (bit0 & 31u);
-						v0 = nbits == 2 ? level2(w0 & 3u) : lut8[w0 & 255u];
-						if(H || NV == 2)
+						if(pair4)
 						{
-							const uint32_t bit1 = tin * bpt + boff1;
-							const uint32_t w1 = (oneword ? raw0 : __ldg(wp + (bit1 >> 5))) >> (bit1 & 31u);
-							v1 = nbits == 2 ? level2(w1 & 3u) : lut8[w1 & 255u];
+							const float2 l = lut4[w0 & 15u];
+							v0 = l.x;
+							v1 = l.y;
+						}
+						else
+						{
+							v0 = nbits == 2 ? level2(w0 & 3u) : lut8[w0 & 255u];
+							if(H || NV == 2)
+							{
+								const uint32_t bit1 = tin * bpt + boff1;
+								const uint32_t w1 =
+								    (oneword ? raw0 : __ldg((const uint32_t *)fp + (bit1 >> 5))) >> (bit1 & 31u);
+								v1 = nbits == 2 ? level2(w1 & 3u) : lut8[w1 & 255u];
+							}
 						}
 					}
 					float sn = 0.0f, cs = 1.0f;
@@ -435,7 +466,8 @@ __global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage
 						else
 						{
 							const int kk = n / asl, jj = n - kk * asl;
-							ph = P0 + (float)jj * alpha + (float)(kk * jj) * beta + (float)kk * gamma + (float)(kk * kk) * eps;
+							ph = P0 + (float)jj * alpha + (float)(kk * jj) * beta + (float)kk * gamma +
+							     (float)(kk * kk) * eps;
 						}
 						ph -= rintf(ph);
 						__sincosf(-6.283185307179586f * ph, &sn, &cs);
@@ -451,11 +483,15 @@ __global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage
 						if constexpr(NV == 2)
 							x[1][r] = cf{v1 * cs, v1 * sn};
 					}
-					tin += (uint32_t)(N >> 3);
-					while(tin >= fs)
+					if(r < 7)
 					{
-						tin -= fs;
-						kf++;
+						tin += (uint32_t)(N / 8);
+						while(tin >= fs)
+						{
+							tin -= fs;
+							kf++;
+							fp += framebytes;
+						}
 					}
 				}
 #pragma unroll
@@ -464,7 +500,7 @@ __global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage
 #pragma unroll
 				for(int r = 1; r < 8; r++)
 				{
-					const TW w = ldtw(tw, r * b * twscale);
+					const TW w = ldtw(tw, (r - 1) * (N / 8) + b);
 #pragma unroll
 					for(int j = 0; j < NV; j++)
 						x[j][r] = twid(x[j][r], w);
@@ -473,7 +509,7 @@ __global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage
 #pragma unroll
 				for(int j = 0; j < NV; j++)
 				{
-					uint2 *q = dst + j * padN + o;
+					uint2 *q = dst + j * PADN + o;
 					sts2(q, x[j][0], x[j][1]);
 					sts2(q + 2, x[j][2], x[j][3]);
 					sts2(q + 4, x[j][4], x[j][5]);
@@ -483,75 +519,104 @@ __global__ void __launch_bounds__(KB == 4 ? 512 : 256, KB == 4 ? 1 : 2) k_fstage
 			__syncthreads();
 		}
 		// ---- middle radix-8 passes through shared memory
-		int logs = 3;
-		const int nmid = (logN % 3 == 0) ? logN / 3 - 2 : logN / 3 - 1;
-		for(int ps = 0; ps < nmid; ps++)
-		{
-			const int s = 1 << logs;
-			const int m = N >> (logs + 3);
-			const uint2 *src = wb ? side1 : side0;
-			wb ^= 1;
-			uint2 *dst = wb ? side1 : side0;
-			if(a.pp)
-			{
-				// two buffers: each butterfly reads, transforms and writes on its own
-#pragma unroll
-				for(int k = 0; k < KB; k++)
-				{
-					const int b = bt + k * TPF;
-					const int q = b & (s - 1), p8 = b >> logs;
-					C x[NV][8];
-					radix8_step<C, NV>(src, padN, q, s, p8, m, tw, twscale, x);
-#pragma unroll
-					for(int j = 0; j < NV; j++)
-#pragma unroll
-						for(int r = 0; r < 8; r++)
-							sts(dst + j * padN + xpad(q + s * (8 * p8 + r)), x[j][r]);
-				}
-			}
-			else
-			{
-				// one buffer: all reads of the pass before any write
-				C x[KB][NV][8];
-#pragma unroll
-				for(int k = 0; k < KB; k++)
-				{
-					const int b = bt + k * TPF;
-					radix8_step<C, NV>(src, padN, b & (s - 1), s, b >> logs, m, tw, twscale, x[k]);
-				}
-				__syncthreads();
-#pragma unroll
-				for(int k = 0; k < KB; k++)
-				{
-					const int b = bt + k * TPF;
-					const int q = b & (s - 1), p8 = b >> logs;
-#pragma unroll
-					for(int j = 0; j < NV; j++)
-#pragma unroll
-						for(int r = 0; r < 8; r++)
-							sts(dst + j * padN + xpad(q + s * (8 * p8 + r)), x[k][j][r]);
-				}
-			}
-			__syncthreads();
-			logs += 3;
-		}
+		MidPasses<C, NV, LOGN, 0>::run(wb, side0, side1, a.pp, bt, tw);
 		// ---- 4. last pass, sideband selection, fractional-sample rotation, output
 		{
+			constexpr int sL = N / RL;
+			constexpr int J = (KB * 8) / RL;
 			const uint2 *src = wb ? side1 : side0;
-			const int rl = logN - logs;
-			if(rl == 3)
-				last_pass<C, NV, KB, 8>(src, padN, N, nchan, TPF, bt, lsb, order, sc, row, prow, spec_off, hout, a.spec);
-			else if(rl == 2)
-				last_pass<C, NV, KB, 4>(src, padN, N, nchan, TPF, bt, lsb, order, sc, row, prow, spec_off, hout, a.spec);
-			else
-				last_pass<C, NV, KB, 2>(src, padN, N, nchan, TPF, bt, lsb, order, sc, row, prow, spec_off, hout, a.spec);
 			wb ^= 1;
+			const int64_t obase = spec_off + (int64_t)t * prow * nchan;
+#pragma unroll
+			for(int jj = 0; jj < J; jj++)
+			{
+				const int q = bt + jj * TPF;
+				C y[NV][RL];
+#pragma unroll
+				for(int j = 0; j < NV; j++)
+				{
+#pragma unroll
+					for(int r = 0; r < RL; r++)
+						y[j][r] = lds<C>(src + j * PADN + xpad(q + sL * r));
+					dftR<RL>(y[j]);
+				}
+				if(!tok)
+					continue;
+#pragma unroll
+				for(int r = 0; r < RL; r++)
+				{
+					const int k = q + sL * r;
+					int c, ce;
+					float cj = 1.0f;
+					if(!lsb)
+					{
+						if(r >= RL / 2)
+							continue;                  // bins >= nchan
+						c = k;
+						ce = k;
+					}
+					else if(order != 0)
+					{
+						if(r < RL / 2)
+							continue;
+						c = k - nchan;
+						ce = c - nchan;
+					}
+					else
+					{
+						if(!(k >= 1 && k <= nchan))
+							continue;
+						c = nchan - k;
+						ce = c - nchan;
+						cj = -1.0f;
+					}
+					float turns = (float)ce * dfs + postf;
+					turns -= rintf(turns);
+					float sn, cs;
+					__sincosf(6.283185307179586f * turns, &sn, &cs);
+					if constexpr(H)
+					{
+						const hc v = y[0][r];
+						const float xr0 = __low2float(v.x) * hout, xi0 = cj * __low2float(v.y) * hout;
+						const float xr1 = __high2float(v.x) * hout, xi1 = cj * __high2float(v.y) * hout;
+						__nv_bfloat162 *o = (__nv_bfloat162 *)a.spec + obase + c;
+						if(row0 >= 0)
+							o[(int64_t)row0 * nchan] = __floats2bfloat162_rn(xr0 * cs - xi0 * sn, xr0 * sn + xi0 * cs);
+						if(row1 >= 0)
+							o[(int64_t)row1 * nchan] = __floats2bfloat162_rn(xr1 * cs - xi1 * sn, xr1 * sn + xi1 * cs);
+					}
+					else
+					{
+						float2 *o = (float2 *)a.spec + obase + c;
+#pragma unroll
+						for(int j = 0; j < NV; j++)
+						{
+							const int rw = j == 0 ? row0 : row1;
+							if(rw >= 0)
+							{
+								const float xr = y[j][r].x, xi = cj * y[j][r].y;
+								o[(int64_t)rw * nchan] = make_float2(xr * cs - xi * sn, xr * sn + xi * cs);
+							}
+						}
+					}
+				}
+			}
 		}
 	}
 }
 
+static int ilog2(int n)
+{
+	int l = 0;
+	while((1 << l) < n)
+		l++;
+	return l;
+}
+
 bool fstage_plan(int N, int nb, int out, FKind *k)
 {
+	if(N < 32 || N > 16384 || (N & (N - 1)))
+		return false;
 	k->N = N;
 	k->nb = nb;
 	k->kb = N <= 2048 ? 1 : (N == 4096 ? 2 : 4);
@@ -566,16 +631,74 @@ bool fstage_plan(int N, int nb, int out, FKind *k)
 	k->smem = side * (k->pp ? 2 : 1);
 	k->tq = 4;
 	k->out = out;
+	k->twn = tw_offset(N, ilog2(N) / 3);
 	return k->smem <= 200 * 1024 && k->threads <= 512;
 }
 
-template <typename C, int NV, int KB>
-static void launch_t(const FKind &k, int T, const FsArgs &a, cudaStream_t stream)
+// Twiddle table of FFT length N in the kernel's [pass][r - 1][p] layout
+// (values computed in double): n = tw_offset(N, npass) entries.
+void make_fstage_twiddles(int N, float2 *out32, void *out16)
 {
-	cudaFuncSetAttribute(k_fstage<C, NV, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+	int n8 = N / 8, s = 1, o = 0;
+	while(n8 >= 1)
+	{
+		for(int r = 1; r < 8; r++)
+			for(int p = 0; p < n8; p++)
+			{
+				const double ang = -2.0 * M_PI * (double)((int64_t)r * p * s % N) / (double)N;
+				const double c = cos(ang), sn = sin(ang);
+				const int i = o + (r - 1) * n8 + p;
+				if(out32)
+					out32[i] = make_float2((float)c, (float)sn);
+				if(out16)
+				{
+					const __half hr = __double2half(c), hi = __double2half(sn);
+					const __half2 rr = __halves2half2(hr, hr), ii = __halves2half2(hi, hi);
+					uint2 *u = (uint2 *)out16 + i;
+					u->x = *(const uint32_t *)&rr;
+					u->y = *(const uint32_t *)&ii;
+				}
+			}
+		o += 7 * n8;
+		n8 /= 8;
+		s *= 8;
+	}
+}
+
+template <typename C, int NV, int LOGN>
+static void launch_t(const FKind &k, const FsArgs &a, cudaStream_t stream)
+{
+	cudaFuncSetAttribute(k_fstage<C, NV, LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+	cudaFuncSetAttribute(k_fstage<C, NV, LOGN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 	const int per = k.tq * k.fpc;
-	dim3 grid((T + per - 1) / per, k.count);
-	k_fstage<C, NV, KB><<<grid, k.threads, k.smem, stream>>>(a);
+	dim3 grid((a.T + per - 1) / per, k.count);
+	k_fstage<C, NV, LOGN><<<grid, k.threads, k.smem, stream>>>(a);
+}
+
+template <typename C, int NV>
+static void launch_n(const FKind &k, const FsArgs &a, cudaStream_t stream)
+{
+	switch(k.N)
+	{
+	case 32: launch_t<C, NV, 5>(k, a, stream); break;
+	case 64: launch_t<C, NV, 6>(k, a, stream); break;
+	case 128: launch_t<C, NV, 7>(k, a, stream); break;
+	case 256: launch_t<C, NV, 8>(k, a, stream); break;
+	case 512: launch_t<C, NV, 9>(k, a, stream); break;
+	case 1024: launch_t<C, NV, 10>(k, a, stream); break;
+	case 2048: launch_t<C, NV, 11>(k, a, stream); break;
+	default:
+		if constexpr(NV == 1)
+		{
+			if(k.N == 4096)
+				launch_t<C, NV, 12>(k, a, stream);
+			else if(k.N == 8192)
+				launch_t<C, NV, 13>(k, a, stream);
+			else if(k.N == 16384)
+				launch_t<C, NV, 14>(k, a, stream);
+		}
+		break;
+	}
 }
 
 void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream)
@@ -585,35 +708,13 @@ void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream)
 	a.first = k.first;
 	a.tq = k.tq;
 	a.pp = k.pp;
+	a.tw = k.tw;
 	if(k.out == 1)
-	{
-		if(k.kb == 1)
-			launch_t<hc, 1, 1>(k, a.T, a, stream);
-		else if(k.kb == 2)
-			launch_t<hc, 1, 2>(k, a.T, a, stream);
-		else
-			launch_t<hc, 1, 4>(k, a.T, a, stream);
-	}
+		launch_n<hc, 1>(k, a, stream);
 	else if(k.nb == 2)
-		launch_t<cf, 2, 1>(k, a.T, a, stream);
-	else if(k.kb == 1)
-		launch_t<cf, 1, 1>(k, a.T, a, stream);
-	else if(k.kb == 2)
-		launch_t<cf, 1, 2>(k, a.T, a, stream);
+		launch_n<cf, 2>(k, a, stream);
 	else
-		launch_t<cf, 1, 4>(k, a.T, a, stream);
-}
-
-void make_fstage_twiddles16(const double *re, const double *im, int n, void *out)
-{
-	uint2 *o = (uint2 *)out;
-	for(int i = 0; i < n; i++)
-	{
-		const __half r = __double2half(re[i]), q = __double2half(im[i]);
-		const __half2 rr = __halves2half2(r, r), qq = __halves2half2(q, q);
-		o[i].x = *(const uint32_t *)&rr;
-		o[i].y = *(const uint32_t *)&qq;
-	}
+		launch_n<cf, 1>(k, a, stream);
 }
 
 }  // namespace fxb

@@ -71,7 +71,9 @@ struct FKind {
 	int32_t kb, fpc;         // radix-8 butterflies per thread and pass, FFTs side by side per CTA
 	int32_t threads, tq;     // CTA size, FFT iterations per CTA
 	int32_t pp, out;         // two exchange buffers (else one), output form (0 FP32, 1 FP16 FFT -> bf16x2)
+	int32_t twn, pad;        // twiddle entries of length N
 	size_t smem;
+	const void *tw;          // twiddle table of length N (make_fstage_twiddles layout)
 };
 
 struct FsArgs {
@@ -82,7 +84,7 @@ struct FsArgs {
 	const uint8_t *valid;
 	int64_t valid_stride;
 	const FftParam *params;
-	const void *tw;          // exp(-2 pi i k / maxN): float2 (out 0) or half2 pairs (wr, wr), (wi, wi) (out 1)
+	const void *tw;          // set from FKind::tw by launch_fstage_kind
 	int32_t maxN, T, tq, order;
 	int32_t fraclo, pp, first, pad;
 	void *spec;              // [t][row][chan]: float2 (out 0) or bf16x2 (out 1)
@@ -90,7 +92,9 @@ struct FsArgs {
 
 bool fstage_plan(int N, int nb, int out, FKind *k);
 void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream);
-void make_fstage_twiddles16(const double *re, const double *im, int n, void *out);
+// twiddles of FFT length N: float2 (out 0) or half2 pairs (wr, wr), (wi, wi)
+// (out 1), FKind::twn entries
+void make_fstage_twiddles(int N, float2 *out32, void *out16);
 
 // FP32 XMAC v2 over a set of frequencies with equal (rows, channels):
 // plan_idx[0..nf) index dplans.
