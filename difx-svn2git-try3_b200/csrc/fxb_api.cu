@@ -69,15 +69,20 @@ struct fxb_ctx {
 	FGroup *d_groups = nullptr;
 	std::vector<FKind> fkinds;
 	void *d_specn = nullptr;             // bf16x2 spectra [t][row][chan] of the tensor-core form
-	struct XGroup { int plan0; int32_t *d_idx; int nf; };
+	// XMAC launch groups (subbands of equal rows and channels); the
+	// tensor-core form also keeps each group's spectra in one block
+	struct XGroup {
+		int plan0 = 0, nf = 0;
+		int32_t *d_idx = nullptr;
+		TcShape shape{};
+		int64_t spec_base = 0;                    // first bf16x2 value of the group's block
+		alignas(64) unsigned char tmap[128];     // CUtensorMap of the block (64-byte aligned)
+	};
 	std::vector<XGroup> xgroups;
 	// tensor-core (BF16) XMAC state
 	bool tc = false;
-	int Tpad = 0;
-	void *d_spec_bf16 = nullptr;
-	int64_t spec_bf16_elems = 0;
-	int64_t *d_rowbase = nullptr;
-	alignas(64) unsigned char tmap[128];     // CUtensorMap (64-byte aligned)
+	int nsm = 0;
+	int64_t specn_elems = 0;
 	int32_t *d_err = nullptr;
 };
 
@@ -269,70 +274,93 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		d.destB = dB;
 		d.pairs = pairs;
 	}
-	// tensor-core form: BF16 K-major spectra [chan][R2][Tpad] per frequency and
-	// [chan][output] accumulators
+	// XMAC launch groups: frequencies with equal shape share a launch
 	ctx->tc = job.xmac_kind == FXB_XMAC_BF16;
-	ctx->Tpad = (ctx->T + 63) & ~63;
 	if(job.xmac_kind == FXB_XMAC_FP8)
 	{
 		ctx->err = "the FP8 XMAC is not available in this build";
 		return FXB_ERR_UNSUPPORTED;
 	}
-	std::vector<int64_t> rowbase(ctx->F, 0);
+	std::vector<std::vector<int32_t>> gidx;
+	{
+		std::vector<int> used;
+		for(int f = 0; f < ctx->F; f++)
+			if(ctx->h_plans[f].nrow > 0) used.push_back(f);
+		std::vector<int> taken(used.size(), 0);
+		for(size_t i = 0; i < used.size(); i++)
+		{
+			if(taken[i]) continue;
+			const DevFreqPlan &a = ctx->h_plans[used[i]];
+			std::vector<int32_t> idx;
+			for(size_t j = i; j < used.size(); j++)
+			{
+				const DevFreqPlan &b = ctx->h_plans[used[j]];
+				if(!taken[j] && b.nrow == a.nrow && b.nchan == a.nchan)
+				{
+					taken[j] = 1;
+					idx.push_back(used[j]);
+				}
+			}
+			ctx->xgroups.emplace_back();
+			ctx->xgroups.back().plan0 = used[i];
+			ctx->xgroups.back().nf = (int)idx.size();
+			gidx.push_back(idx);
+		}
+	}
+	// tensor-core form: bf16x2 spectra, per group one block
+	// [subband][Tpad][nrow][nchan] (times past T stay zero), and
+	// [chan][output] accumulators
 	if(ctx->tc)
 	{
 		int64_t off = 0;
-		for(int f = 0; f < ctx->F; f++)
+		for(size_t gi = 0; gi < ctx->xgroups.size(); gi++)
 		{
-			DevFreqPlan &d = ctx->h_plans[f];
-			if(d.nrow == 0) continue;
-			if(d.r2pad > 128 || d.nchan > 2048)
+			fxb_ctx::XGroup &g = ctx->xgroups[gi];
+			const DevFreqPlan &p0 = ctx->h_plans[g.plan0];
+			int nout_max = 0;
+			for(int32_t f : gidx[gi])
+				nout_max = std::max(nout_max, job.plan[f].nout);
+			if(!tc_shape(p0.nrow, p0.nchan, ctx->T, nout_max, &g.shape))
 			{
-				ctx->err = "tensor-core XMAC: at most 64 inputs and 2048 channels per subband";
+				ctx->err = "tensor-core XMAC: at most 64 inputs per subband, and the outputs of 4 G channels must "
+				           "fit the epilogue buffer";
 				return FXB_ERR_UNSUPPORTED;
 			}
-			rowbase[f] = off / ctx->Tpad;
-			off += (int64_t)d.nchan * d.r2pad * ctx->Tpad;
-			d.acc_ostride = 1;
-			d.acc_cstride = job.plan[f].nout;
+			g.spec_base = off;
+			const int64_t per = (int64_t)g.shape.Tpad * p0.nrow * p0.nchan;
+			for(size_t i = 0; i < gidx[gi].size(); i++)
+			{
+				DevFreqPlan &d = ctx->h_plans[gidx[gi][i]];
+				d.spec_off = off + (int64_t)i * per;
+				d.acc_ostride = 1;
+				d.acc_cstride = job.plan[gidx[gi][i]].nout;
+			}
+			off += per * (int64_t)gidx[gi].size();
 		}
-		ctx->spec_bf16_elems = off;
+		ctx->specn_elems = off;
 	}
 	CK(ctx, dalloc(ctx, &ctx->d_plans, ctx->F));
 	CK(ctx, cudaMemcpy(ctx->d_plans, ctx->h_plans.data(), sizeof(DevFreqPlan) * ctx->F, cudaMemcpyHostToDevice));
+	for(size_t gi = 0; gi < ctx->xgroups.size(); gi++)
+	{
+		fxb_ctx::XGroup &g = ctx->xgroups[gi];
+		CK(ctx, dalloc(ctx, &g.d_idx, gidx[gi].size()));
+		CK(ctx, cudaMemcpy(g.d_idx, gidx[gi].data(), sizeof(int32_t) * gidx[gi].size(), cudaMemcpyHostToDevice));
+	}
 	if(ctx->tc)
 	{
-		unsigned char *sp = nullptr;
-		CK(ctx, dalloc(ctx, &sp, (size_t)ctx->spec_bf16_elems * 2 + 4096));
-		CK(ctx, cudaMemset(sp, 0, (size_t)ctx->spec_bf16_elems * 2 + 4096));
-		ctx->d_spec_bf16 = sp;
-		CK(ctx, dalloc(ctx, &ctx->d_rowbase, ctx->F));
-		CK(ctx, cudaMemcpy(ctx->d_rowbase, rowbase.data(), sizeof(int64_t) * ctx->F, cudaMemcpyHostToDevice));
+		uint32_t *sn = nullptr;
+		CK(ctx, dalloc(ctx, &sn, (size_t)ctx->specn_elems));
+		CK(ctx, cudaMemset(sn, 0, sizeof(uint32_t) * (size_t)ctx->specn_elems));
+		ctx->d_specn = sn;
 		CK(ctx, dalloc(ctx, &ctx->d_err, 1));
 		CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
-		int r2 = 0;
-		for(int f = 0; f < ctx->F; f++)
-			if(ctx->h_plans[f].nrow) r2 = ctx->h_plans[f].r2pad;
-		int G, NG, boxrows, cols;
-		size_t smem;
-		tc_geometry(r2, ctx->Tpad, &G, &NG, &boxrows, &cols, &smem);
-		if(tc_tensormap_size() > sizeof(ctx->tmap) ||
-		   !tc_make_tensormap(ctx->tmap, sp, ctx->spec_bf16_elems / ctx->Tpad, ctx->Tpad, boxrows))
-		{
-			ctx->err = "cuTensorMapEncodeTiled failed for the spectra buffer";
-			return FXB_ERR_CUDA;
-		}
-		for(int f = 0; f < ctx->F; f++)
-			if(ctx->h_plans[f].nrow && (size_t)G * NG * job.plan[f].nout * sizeof(float2) > (smem - 1024))
+		CK(ctx, cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+		for(fxb_ctx::XGroup &g : ctx->xgroups)
+			if(tc_tensormap_size() > sizeof(g.tmap) || !tc_make_tensormap(g.tmap, sn + g.spec_base, g.shape, g.nf))
 			{
-				ctx->err = "tensor-core XMAC: too many outputs per channel for the epilogue buffer";
-				return FXB_ERR_UNSUPPORTED;
-			}
-		for(int f = 0; f < ctx->F; f++)
-			if(ctx->h_plans[f].nrow && ctx->h_plans[f].r2pad != r2)
-			{
-				ctx->err = "tensor-core XMAC: all subbands must have the same number of inputs";
-				return FXB_ERR_UNSUPPORTED;
+				ctx->err = "cuTensorMapEncodeTiled failed for the spectra buffer";
+				return FXB_ERR_CUDA;
 			}
 	}
 
@@ -413,44 +441,9 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		if(!hg.empty())
 			CK(ctx, cudaMemcpy(ctx->d_groups, hg.data(), sizeof(FGroup) * hg.size(), cudaMemcpyHostToDevice));
 	}
-	// FP32 XMAC launch groups: frequencies with equal shape share a launch
-	{
-		std::vector<int> used;
-		for(int f = 0; f < ctx->F; f++)
-			if(ctx->h_plans[f].nrow > 0) used.push_back(f);
-		std::vector<int> taken(used.size(), 0);
-		for(size_t i = 0; i < used.size(); i++)
-		{
-			if(taken[i]) continue;
-			const DevFreqPlan &a = ctx->h_plans[used[i]];
-			std::vector<int32_t> idx;
-			for(size_t j = i; j < used.size(); j++)
-			{
-				const DevFreqPlan &b = ctx->h_plans[used[j]];
-				if(!taken[j] && b.nrow == a.nrow && b.nchan == a.nchan)
-				{
-					taken[j] = 1;
-					idx.push_back(used[j]);
-				}
-			}
-			fxb_ctx::XGroup g;
-			g.plan0 = used[i];
-			g.nf = (int)idx.size();
-			CK(ctx, dalloc(ctx, &g.d_idx, idx.size()));
-			CK(ctx, cudaMemcpy(g.d_idx, idx.data(), sizeof(int32_t) * idx.size(), cudaMemcpyHostToDevice));
-			ctx->xgroups.push_back(g);
-		}
-	}
-
 	// big buffers
 	CK(ctx, dalloc(ctx, &ctx->d_params, (size_t)ctx->S * ctx->T));
 	CK(ctx, dalloc(ctx, &ctx->d_spec, job.xmac_kind == FXB_XMAC_FP32 ? (size_t)job.spec_total : 1));
-	if(ctx->tc)
-	{
-		uint32_t *sn = nullptr;
-		CK(ctx, dalloc(ctx, &sn, (size_t)job.spec_total));
-		ctx->d_specn = sn;
-	}
 	CK(ctx, dalloc(ctx, &ctx->d_acc, (size_t)job.acc_total));
 	CK(ctx, dalloc(ctx, &ctx->d_core, (size_t)job.corelen));
 	ctx->nbw = (int)job.bweights.size();
@@ -686,19 +679,13 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 		fa.spec = ctx->tc ? ctx->d_specn : (void *)ctx->d_spec;
 		for(const FKind &k : ctx->fkinds)
 			launch_fstage_kind(k, fa, st);
-		if(ctx->tc)
-			for(const auto &g : ctx->xgroups)
-				launch_spec_kmajor(ctx->d_plans, g.d_idx, g.nf, ctx->h_plans[g.plan0].nrow, ctx->h_plans[g.plan0].nchan,
-				                   ctx->T, ctx->Tpad, ctx->d_rowbase, (const uint32_t *)ctx->d_specn,
-				                   (uint16_t *)ctx->d_spec_bf16, st);
 	}
 	CK(ctx, cudaEventRecord(ctx->ev_c, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[2], st));
 	for(const auto &g : ctx->xgroups)
 	{
 		if(ctx->tc)
-			launch_xmac_tc(ctx->tmap, ctx->d_plans, g.d_idx, g.nf, ctx->h_plans[g.plan0].nchan, ctx->d_rowbase, ctx->Tpad,
-			               ctx->h_plans[g.plan0].r2pad, ctx->d_err, ctx->d_acc, st);
+			launch_xmac_tc(g.tmap, g.shape, ctx->d_plans, g.d_idx, g.nf, ctx->nsm, ctx->d_err, ctx->d_acc, st);
 		else
 			launch_xmac_fp32v2(ctx->h_plans[g.plan0], ctx->d_plans, g.d_idx, g.nf, ctx->T, ctx->d_spec, ctx->d_acc, st);
 	}

@@ -101,15 +101,18 @@ void make_fstage_twiddles(int N, float2 *out32, void *out16);
 void launch_xmac_fp32v2(const DevFreqPlan &plan0, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int T,
                         const float2 *spec, float2 *acc, cudaStream_t stream);
 
-// Tensor-core XMAC (csrc/fxb_xmac_tc.cu).
-bool tc_make_tensormap(void *map_out, const void *spec_bf16, int64_t total_rows, int Tpad, int boxrows);
+// Tensor-core XMAC (csrc/fxb_xmac_tc.cu) over one group of equally shaped
+// subbands whose bf16x2 spectra lie in one block [subband][Tpad][nrow][nchan].
+struct TcShape {
+	int32_t nrow, nchan, r2p, G, CB, Tpad;
+	int32_t raw_bytes, raw_stride, vbuf_floats;
+	size_t smem;
+};
+bool tc_shape(int nrow, int nchan, int T, int nout_max, TcShape *s);
+bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf);
 size_t tc_tensormap_size();
-void tc_geometry(int R2, int Tpad, int *G, int *NG, int *boxrows, int *tmem_cols, size_t *smem);
-void launch_xmac_tc(const void *tmap, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int nchan,
-                    const int64_t *rowbase, int Tpad, int R2, int32_t *err, float2 *acc, cudaStream_t stream);
-
-void launch_spec_kmajor(const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int nrow, int nchan, int T,
-                        int Tpad, const int64_t *rowbase, const uint32_t *specn, uint16_t *kmaj, cudaStream_t stream);
+void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf,
+                    int nsm, int32_t *err, float2 *acc, cudaStream_t stream);
 
 // FP32 cross-multiply-accumulate of one frequency into acc.
 void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, const float2 *spec, float2 *acc,
