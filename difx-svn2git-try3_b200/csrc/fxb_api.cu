@@ -251,8 +251,6 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		d.npair = d.ntr * (d.ntr + 1) / 2;
 		d.spec_off = p.spec_off;
 		d.acc_off = p.acc_off;
-		d.r2pad = (2 * p.nrow + 7) & ~7;
-		d.tpad = (ctx->T + 63) & ~63;
 		d.acc_cstride = 1;
 		d.acc_ostride = p.nchan;
 		int32_t *dA, *dB;
@@ -273,6 +271,21 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		d.destA = dA;
 		d.destB = dB;
 		d.pairs = pairs;
+		// inverse of destA / destB: which input pair (and whether conjugated) feeds each output
+		{
+			std::vector<int32_t> src((size_t)std::max(p.nout, 1), -1);
+			for(int a = 0; a < p.nrow; a++)
+				for(int b = a; b < p.nrow; b++)
+				{
+					const int oA = p.destA[(size_t)a * p.nrow + b], oB = p.destB[(size_t)a * p.nrow + b];
+					if(oA >= 0 && oA < p.nout) src[oA] = a | (b << 8);
+					if(oB >= 0 && oB < p.nout) src[oB] = a | (b << 8) | (1 << 16);
+				}
+			int32_t *ds = nullptr;
+			CK(ctx, dalloc(ctx, &ds, src.size()));
+			CK(ctx, cudaMemcpy(ds, src.data(), sizeof(int32_t) * src.size(), cudaMemcpyHostToDevice));
+			d.outsrc = ds;
+		}
 	}
 	// XMAC launch groups: frequencies with equal shape share a launch
 	ctx->tc = job.xmac_kind == FXB_XMAC_BF16;
@@ -317,21 +330,20 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		{
 			fxb_ctx::XGroup &g = ctx->xgroups[gi];
 			const DevFreqPlan &p0 = ctx->h_plans[g.plan0];
-			int nout_max = 0;
-			for(int32_t f : gidx[gi])
-				nout_max = std::max(nout_max, job.plan[f].nout);
-			if(!tc_shape(p0.nrow, p0.nchan, ctx->T, nout_max, &g.shape))
+			if(!tc_shape(p0.nrow, p0.nchan, ctx->T, &g.shape))
 			{
-				ctx->err = "tensor-core XMAC: at most 64 inputs per subband, and the outputs of 4 G channels must "
-				           "fit the epilogue buffer";
+				ctx->err = "tensor-core XMAC: at most 64 inputs per subband";
 				return FXB_ERR_UNSUPPORTED;
 			}
 			g.spec_base = off;
-			const int64_t per = (int64_t)g.shape.Tpad * p0.nrow * p0.nchan;
+			const int nblk = (p0.nchan + g.shape.CB - 1) / g.shape.CB;
+			const int64_t per = (int64_t)g.shape.Tpad * nblk * p0.nrow * g.shape.CB;
 			for(size_t i = 0; i < gidx[gi].size(); i++)
 			{
 				DevFreqPlan &d = ctx->h_plans[gidx[gi][i]];
 				d.spec_off = off + (int64_t)i * per;
+				d.tcb = g.shape.CB;
+				d.tnblk = nblk;
 				d.acc_ostride = 1;
 				d.acc_cstride = job.plan[gidx[gi][i]].nout;
 			}
@@ -405,6 +417,14 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			}
 		}
 		std::vector<FGroup> hg;
+		if(out == 1)
+		{
+			// all stations of a subband side by side in the grid: their rows of
+			// one spectra block are written close together in time
+			for(auto &kv : bykind)
+				std::stable_sort(kv.second.begin(), kv.second.end(),
+				                 [](const FGroup &x, const FGroup &y) { return x.freq < y.freq; });
+		}
 		for(const auto &kv : bykind)
 		{
 			FKind k;
@@ -881,15 +901,20 @@ fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloa
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
 	if(n && ctx->tc)
 	{
-		// bf16x2 [t][row][chan] -> FP32
-		std::vector<uint32_t> h(n);
-		CK(ctx, cudaMemcpy(h.data(), (const uint32_t *)ctx->d_specn + p.spec_off, n * 4, cudaMemcpyDeviceToHost));
+		// bf16x2 [t][block][row][tcb] -> FP32 [t][row][chan]
+		const size_t nb = (size_t)ctx->T * p.tnblk * p.nrow * p.tcb;
+		std::vector<uint32_t> h(nb);
+		CK(ctx, cudaMemcpy(h.data(), (const uint32_t *)ctx->d_specn + p.spec_off, nb * 4, cudaMemcpyDeviceToHost));
 		auto bf = [](uint32_t v) { uint32_t u = v << 16; float f; memcpy(&f, &u, 4); return f; };
-		for(size_t i = 0; i < n; i++)
-		{
-			out[2 * i] = bf(h[i] & 0xFFFFu);
-			out[2 * i + 1] = bf(h[i] >> 16);
-		}
+		for(int t = 0; t < ctx->T; t++)
+			for(int r = 0; r < p.nrow; r++)
+				for(int c = 0; c < p.nchan; c++)
+				{
+					const uint32_t v = h[(((size_t)t * p.tnblk + c / p.tcb) * p.nrow + r) * p.tcb + c % p.tcb];
+					const size_t o = ((size_t)t * p.nrow + r) * p.nchan + c;
+					out[2 * o] = bf(v & 0xFFFFu);
+					out[2 * o + 1] = bf(v >> 16);
+				}
 	}
 	else if(n)
 		CK(ctx, cudaMemcpy(out, ctx->d_spec + p.spec_off, sizeof(float2) * n, cudaMemcpyDeviceToHost));

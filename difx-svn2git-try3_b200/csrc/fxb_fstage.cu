@@ -302,7 +302,11 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage
 	__shared__ float lut8[256];
 	__shared__ float2 lut4[16];            // two adjacent 2-bit bands -> (band0, band1) levels
 
-	const FGroup g = a.groups[a.first + blockIdx.y];
+	// grid: (time chunks, items), or (items, time chunks) when the stations of a
+	// subband should run side by side (blocked tensor-core spectra)
+	const int item = a.items_fast ? blockIdx.x : blockIdx.y;
+	const int tchunk = a.items_fast ? blockIdx.y : blockIdx.x;
+	const FGroup g = a.groups[a.first + item];
 	const DevStation *Sp = a.st + g.station;
 	constexpr int nchan = N / 2;
 	const uint32_t fs = (uint32_t)Sp->framesamples;
@@ -318,6 +322,9 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage
 	const TW *tw = (const TW *)a.tw;
 	const int64_t spec_off = a.plans[g.freq].spec_off;
 	const int prow = a.plans[g.freq].nrow;
+	// tensor-core form: spectra blocked [t][block][row][tcb] (tcb channels per block)
+	const uint32_t tcb = (uint32_t)a.plans[g.freq].tcb, tnblk = (uint32_t)a.plans[g.freq].tnblk;
+	const uint32_t tcb_magic = tcb ? 0xFFFFFFFFu / tcb + 1u : 0u;    // c / tcb = umulhi(c, magic) for c < 2^16
 	const bool lsb = g.lsb != 0;
 	const double lo = g.lofreq;
 	const int row0 = g.row[0], row1 = g.row[1];
@@ -344,7 +351,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage
 		lut4[threadIdx.x] = make_float2(level2(threadIdx.x & 3u), level2(threadIdx.x >> 2));
 	__syncthreads();
 
-	const int t0 = blockIdx.x * a.tq * FPC;
+	const int t0 = tchunk * a.tq * FPC;
 	const int nit = min(a.tq, (a.T - t0 + FPC - 1) / FPC);
 	int wb = 0;
 	for(int it = 0; it < nit; it++)
@@ -579,11 +586,23 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage
 						const hc v = y[0][r];
 						const float xr0 = __low2float(v.x) * hout, xi0 = cj * __low2float(v.y) * hout;
 						const float xr1 = __high2float(v.x) * hout, xi1 = cj * __high2float(v.y) * hout;
-						__nv_bfloat162 *o = (__nv_bfloat162 *)a.spec + obase + c;
+						__nv_bfloat162 *o;
+						int64_t rstride;
+						if(tcb)
+						{
+							const uint32_t blk = __umulhi((uint32_t)c, tcb_magic), cl = (uint32_t)c - blk * tcb;
+							o = (__nv_bfloat162 *)a.spec + spec_off + (((int64_t)t * tnblk + blk) * prow) * tcb + cl;
+							rstride = tcb;
+						}
+						else
+						{
+							o = (__nv_bfloat162 *)a.spec + obase + c;
+							rstride = nchan;
+						}
 						if(row0 >= 0)
-							o[(int64_t)row0 * nchan] = __floats2bfloat162_rn(xr0 * cs - xi0 * sn, xr0 * sn + xi0 * cs);
+							o[(int64_t)row0 * rstride] = __floats2bfloat162_rn(xr0 * cs - xi0 * sn, xr0 * sn + xi0 * cs);
 						if(row1 >= 0)
-							o[(int64_t)row1 * nchan] = __floats2bfloat162_rn(xr1 * cs - xi1 * sn, xr1 * sn + xi1 * cs);
+							o[(int64_t)row1 * rstride] = __floats2bfloat162_rn(xr1 * cs - xi1 * sn, xr1 * sn + xi1 * cs);
 					}
 					else
 					{
@@ -671,7 +690,8 @@ static void launch_t(const FKind &k, const FsArgs &a, cudaStream_t stream)
 	cudaFuncSetAttribute(k_fstage<C, NV, LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
 	cudaFuncSetAttribute(k_fstage<C, NV, LOGN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 	const int per = k.tq * k.fpc;
-	dim3 grid((a.T + per - 1) / per, k.count);
+	const int nt = (a.T + per - 1) / per;
+	const dim3 grid = a.items_fast ? dim3(k.count, nt) : dim3(nt, k.count);
 	k_fstage<C, NV, LOGN><<<grid, k.threads, k.smem, stream>>>(a);
 }
 
@@ -709,6 +729,7 @@ void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream)
 	a.tq = k.tq;
 	a.pp = k.pp;
 	a.tw = k.tw;
+	a.items_fast = k.out == 1 ? 1 : 0;
 	if(k.out == 1)
 		launch_n<hc, 1>(k, a, stream);
 	else if(k.nb == 2)

@@ -11,15 +11,16 @@ namespace fxb {
 // Per-frequency XMAC plan on the device.
 struct DevFreqPlan {
 	int32_t nrow, nchan, ntr, npair;  // rows, channels, 4-row tiles, tile pairs
-	int32_t r2pad;                    // real rows per channel of the K-major BF16 spectra (2*nrow rounded up to 8)
-	int32_t tpad;                     // FFTs per subint rounded up to the K tile (64)
+	int32_t tcb;                      // tensor-core form: channels per spectra block (0: spectra [t][row][chan])
+	int32_t tnblk;                    // tensor-core form: blocks per time, spectra [t][block][row][tcb]
 	int32_t acc_cstride;              // accumulator stride between channels (1: [out][chan], nout: [chan][out])
 	int32_t acc_ostride;              // accumulator stride between outputs
-	int64_t spec_off;                 // complex offset of spectra [T][nrow][nchan]
+	int64_t spec_off;                 // complex offset of this frequency's spectra
 	int64_t acc_off;                  // complex offset of accumulators [nout][nchan]
 	const int32_t *destA;             // [nrow*nrow]
 	const int32_t *destB;             // [nrow*nrow]
 	const int16_t *pairs;             // [npair*2] tile pairs (ti <= tj)
+	const int32_t *outsrc;            // [nout] source of each output: a | b << 8 | conj << 16 (a <= b), or -1
 };
 
 struct DevOutMap {
@@ -86,7 +87,7 @@ struct FsArgs {
 	const FftParam *params;
 	const void *tw;          // set from FKind::tw by launch_fstage_kind
 	int32_t maxN, T, tq, order;
-	int32_t fraclo, pp, first, pad;
+	int32_t fraclo, pp, first, items_fast;
 	void *spec;              // [t][row][chan]: float2 (out 0) or bf16x2 (out 1)
 };
 
@@ -105,10 +106,12 @@ void launch_xmac_fp32v2(const DevFreqPlan &plan0, const DevFreqPlan *dplans, con
 // subbands whose bf16x2 spectra lie in one block [subband][Tpad][nrow][nchan].
 struct TcShape {
 	int32_t nrow, nchan, r2p, G, CB, Tpad;
-	int32_t raw_bytes, raw_stride, vbuf_floats;
+	int32_t raw_bytes, raw_stride;    // bytes of one TMA box, stride of the raw stages
+	int32_t nrs, nas;                 // raw and operand stages
+	int32_t dstride, dump_off;        // accumulator copy: floats per row, byte offset
 	size_t smem;
 };
-bool tc_shape(int nrow, int nchan, int T, int nout_max, TcShape *s);
+bool tc_shape(int nrow, int nchan, int T, TcShape *s);
 bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf);
 size_t tc_tensormap_size();
 void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf,

@@ -8,24 +8,26 @@
 //     Re V[a][b] = P[2a][2b] + P[2a+1][2b+1],  Im V[a][b] = P[2a+1][2b] - P[2a][2b+1].
 //
 // Input: the F stage's bf16x2 spectra, per group of equally shaped subbands
-// one block [subband][Tpad][nrow][nchan] (times T..Tpad-1 zero).  A work unit
-// is 4 G consecutive channels of one subband, G = floor(128 / R2p) with R2p
-// the real rows per channel rounded up to 8: four M = 128 operand tiles of G
-// channels each (the rows past G R2p stay zero).  One tcgen05.mma (kind::f16,
-// M = N = 128, K = 16) uses the same shared-memory tile as A and B, so the G
-// diagonal R2p x R2p blocks of each 128 x 128 FP32 accumulator are the G
-// channels' A A^T; the four accumulators fill the 512 columns of tensor memory.
+// one block [subband][Tpad][block][nrow][CB] (times T..Tpad-1 zero), with CB
+// the channels of one work unit.  A unit is two M = 128 operand tiles of
+// G = floor(128 / R2p) channels each, R2p the real rows per channel rounded up
+// to 8 (rows past G R2p stay zero).  One tcgen05.mma (kind::f16, M = N = 128,
+// K = 16) uses the same shared-memory tile as A and B, so the G diagonal
+// R2p x R2p blocks of each 128 x 128 FP32 accumulator are the G channels'
+// A A^T.  A unit's two accumulators take 256 tensor-memory columns; two units
+// alternate, so the epilogue of one overlaps the MMAs of the next.
 //
 // One persistent CTA per SM, warp-specialised:
-//   warp 0     TMA producer: 3D boxes {4G channels, nrow, 32 times} of the
-//              spectra (no multicast) into a 3-stage ring,
+//   warp 0     TMA producer: 3D boxes {nrow * CB values, 1 block, 32 times}
+//              (each of the 32 rows one contiguous run; no multicast) into a
+//              ring of raw stages,
 //   warp 1     tensor-memory owner and MMA issuer,
 //   warps 2-5  transposers: raw boxes -> K-major operand tiles with 64-byte
-//              swizzle (2-stage ring),
-//   warps 6-9  epilogue: tcgen05.ld of each accumulator (released tile by tile
-//              so that the next unit's MMAs start while the rest drain),
-//              recombination into complex products, coalesced accumulation
-//              into the [channel][output] accumulators.
+//              swizzle (a ring of operand stages),
+//   warps 6-9  epilogue: copy the unit's accumulator rows of its channels to
+//              shared memory and release the tensor memory at once, then form
+//              every output V[a][b] from its four real products and add it
+//              to the [channel][output] accumulators with vector reductions.
 // Every wait is bounded: on timeout the CTA records an error code, drains its
 // TMA loads and MMAs, and still releases its tensor memory.
 
@@ -41,9 +43,9 @@ namespace fxb {
 namespace {
 
 constexpr int kKT = 32;                    // times per K tile (64 bytes of BF16 per operand row)
-constexpr int kRS = 3;                     // raw stages
-constexpr int kAS = 2;                     // operand stages
-constexpr int kNG = 4;                     // M tiles per work unit
+constexpr int kRS = 6;                     // raw stages at most (tc_shape picks how many fit)
+constexpr int kAS = 4;                     // operand stages at most
+constexpr int kNG = 2;                     // M tiles per work unit
 constexpr int kTileBytes = 128 * kKT * 2;  // one operand tile: 128 rows x 64 bytes
 constexpr int kThreads = 320;
 constexpr uint32_t kWaitLimit = 1u << 22;
@@ -165,7 +167,8 @@ struct TcParams {
 	int32_t nchan, Tpad, nkt, nf;   // channels, padded times, K tiles, subbands in the group
 	int32_t nblk, nunits;           // channel blocks per subband, work units
 	int32_t raw_bytes, raw_stride;  // bytes per raw box, stage stride
-	int32_t vbuf_floats;            // epilogue buffer capacity (floats)
+	int32_t nrs, nas;               // raw and operand stages in use
+	int32_t dstride, dump_off;      // floats per row of the accumulator copy, its byte offset in shared memory
 	int32_t *err;
 };
 
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
                                                          float2 *__restrict__ acc)
 {
 	extern __shared__ __align__(1024) unsigned char smem_tc[];
-	__shared__ uint64_t full_raw[kRS], empty_raw[kRS], full_a[kAS], empty_a[kAS], acc_full, acc_empty[kNG], mma_done;
+	__shared__ uint64_t full_raw[kRS], empty_raw[kRS], full_a[kAS], empty_a[kAS], acc_full[2], acc_empty[2], mma_done;
 	__shared__ uint32_t tmem_base_s;
 	__shared__ volatile int fail_s;
 	__shared__ int issued_s, consumed_s;
@@ -183,27 +186,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	unsigned char *base = (unsigned char *)(((uintptr_t)smem_tc + 1023) & ~(uintptr_t)1023);
 	unsigned char *raw0 = base;
-	unsigned char *a0 = raw0 + (size_t)kRS * tp.raw_stride;
-	float2 *vbuf = (float2 *)(a0 + (size_t)kAS * kNG * kTileBytes);
+	unsigned char *a0 = raw0 + (size_t)tp.nrs * tp.raw_stride;
+	float *dump = (float *)(base + tp.dump_off);
+	const int nrs = tp.nrs, nas = tp.nas;
+	constexpr int kStageBytes = kNG * kTileBytes;
 
 	// operand tiles start zero: rows past G R2p and padding rows are never written
-	for(int i = threadIdx.x; i < kAS * kNG * kTileBytes / 16; i += blockDim.x)
+	for(int i = threadIdx.x; i < nas * kStageBytes / 16; i += blockDim.x)
 		((uint4 *)a0)[i] = make_uint4(0u, 0u, 0u, 0u);
 	if(threadIdx.x == 0)
 	{
-		for(int s = 0; s < kRS; s++)
+		for(int s = 0; s < nrs; s++)
 		{
 			mbar_init(&full_raw[s], 1);
 			mbar_init(&empty_raw[s], 4);
 		}
-		for(int s = 0; s < kAS; s++)
+		for(int s = 0; s < nas; s++)
 		{
 			mbar_init(&full_a[s], 4);
 			mbar_init(&empty_a[s], 1);
 		}
-		mbar_init(&acc_full, 1);
-		for(int g = 0; g < kNG; g++)
-			mbar_init(&acc_empty[g], 4);
+		for(int b = 0; b < 2; b++)
+		{
+			mbar_init(&acc_full[b], 1);
+			mbar_init(&acc_empty[b], 4);
+		}
 		mbar_init(&mma_done, 1);
 		fail_s = 0;
 		issued_s = 0;
@@ -234,16 +241,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 				const int fi = u / tp.nblk, blk = u - fi * tp.nblk;
 				for(int kt = 0; kt < nkt; kt++, kk++)
 				{
-					const int s = kk % kRS;
-					if(kk >= kRS && !mbar_wait(&empty_raw[s], ((kk / kRS) - 1) & 1, &fail_s))
+					const int s = kk % nrs;
+					if(kk >= nrs && !mbar_wait(&empty_raw[s], ((kk / nrs) - 1) & 1, &fail_s))
 					{
 						fail_s = 1;
 						ok = false;
 						break;
 					}
 					mbar_expect_tx(&full_raw[s], (uint32_t)tp.raw_bytes);
-					tma_load_3d(raw0 + (size_t)s * tp.raw_stride, &tmap, blk * tp.CB, 0, fi * tp.Tpad + kt * kKT,
-					            &full_raw[s]);
+					tma_load_3d(raw0 + (size_t)s * tp.raw_stride, &tmap, 0, blk, fi * tp.Tpad + kt * kKT, &full_raw[s]);
 					issued_s = kk + 1;
 				}
 			}
@@ -253,47 +259,48 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 	{
 		if(lane == 0)
 		{
-			// ---- MMA issuer: M = N = 128, BF16 x BF16 -> FP32, A and B K-major
+			// ---- MMA issuer: M = N = 128, BF16 x BF16 -> FP32, A and B K-major;
+			// unit ku accumulates into columns 256 (ku & 1)
 			const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 			int kk = 0, ku = 0;
 			bool ok = true;
 			for(int u = blockIdx.x; u < tp.nunits && ok; u += gridDim.x, ku++)
 			{
-				for(int kt = 0; kt < nkt && ok; kt++, kk++)
+				const int buf = ku & 1;
+				if(ku >= 2)
 				{
-					const int s = kk % kAS;
-					if(!mbar_wait(&full_a[s], (kk / kAS) & 1, &fail_s))
+					// the epilogue has copied out this buffer's previous unit
+					if(!mbar_wait(&acc_empty[buf], ((ku >> 1) - 1) & 1, &fail_s))
+					{
+						fail_s = 3;
+						ok = false;
+						break;
+					}
+					asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+				}
+				for(int kt = 0; kt < nkt; kt++, kk++)
+				{
+					const int s = kk % nas;
+					if(!mbar_wait(&full_a[s], (kk / nas) & 1, &fail_s))
 					{
 						fail_s = 2;
 						ok = false;
 						break;
 					}
 					asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-					const uint32_t sbase = smem_u32(a0 + (size_t)s * kNG * kTileBytes);
+					const uint32_t sbase = smem_u32(a0 + (size_t)s * kStageBytes);
+#pragma unroll
 					for(int g = 0; g < kNG; g++)
-					{
-						if(kt == 0 && ku > 0)
-						{
-							// the epilogue has read this accumulator of the previous unit
-							if(!mbar_wait(&acc_empty[g], (ku - 1) & 1, &fail_s))
-							{
-								fail_s = 3;
-								ok = false;
-								break;
-							}
-							asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-						}
 #pragma unroll
 						for(int k2 = 0; k2 < kKT / 16; k2++)
 						{
 							const uint64_t d = make_sdesc64(sbase + (uint32_t)(g * kTileBytes + k2 * 32));
-							mma_bf16(tmem + (uint32_t)(g * 128), d, d, idesc, (kt > 0 || k2 > 0) ? 1u : 0u);
+							mma_bf16(tmem + (uint32_t)(buf * 256 + g * 128), d, d, idesc, (kt > 0 || k2 > 0) ? 1u : 0u);
 						}
-					}
 					mma_commit(&empty_a[s]);
 				}
 				if(ok)
-					mma_commit(&acc_full);
+					mma_commit(&acc_full[buf]);
 			}
 			// every MMA issued by this thread has completed once this arrives
 			mma_commit(&mma_done);
@@ -303,36 +310,65 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 	}
 	else if(warp < 6)
 	{
-		// ---- transposers: raw [32 t][nrow][CB] bf16x2 -> operand rows
-		// m = q R2p + 2 row + part of tile g (channel g G + q), 64-byte swizzle
+		// ---- transposers: raw [32 t][nrow][CB] bf16x2 -> operand rows.
+		// Input `row` of channel cl (tile g = cl / G, slot q = cl % G) sits at
+		// position p = (row + cl) mod nrow of its channel block: rows
+		// m = q R2p + 2 p (real) and m + 1 (imaginary), 64-byte swizzle.  The
+		// rotation by cl, and the alternating order of the two stores, spread
+		// the 16-byte stores of neighbouring threads over all banks.
 		const int tt = threadIdx.x - 64;
 		const int rc = tp.nrow * tp.CB;
-		const int items = 4 * rc;
+		const int items = 4 * rc;                      // (8-time chunk, row, channel)
+		constexpr int kMaxItems = 8;                   // 4 * 256 / 128
+		int src_off[kMaxItems], dst_lo[kMaxItems], dst_hi[kMaxItems];
+#pragma unroll
+		for(int j = 0; j < kMaxItems; j++)
+		{
+			const int i = tt + 128 * j;
+			src_off[j] = -1;
+			if(i < items)
+			{
+				const int tc = i / rc, rem = i - tc * rc;
+				const int row = rem / tp.CB, cl = rem - row * tp.CB;
+				const int g = cl / tp.G, q = cl - g * tp.G;
+				const int pos = (row + cl) % tp.nrow;
+				const int m = q * tp.r2p + 2 * pos;
+				const int sw = (tc ^ ((m >> 1) & 3)) << 4;     // rows m, m+1 share the swizzle phase
+				const int re_off = g * kTileBytes + m * 64 + sw, im_off = re_off + 64;
+				const bool swap = (rem >> 2) & 1;
+				src_off[j] = tc * 8 * rc + rem;
+				dst_lo[j] = swap ? im_off : re_off;            // first store: real part unless swapped
+				dst_hi[j] = swap ? re_off : im_off;
+				if(swap)
+					src_off[j] |= 1 << 30;                     // flag: first store takes the imaginary halves
+			}
+		}
 		int kk = 0;
 		bool ok = true;
 		for(int u = blockIdx.x; u < tp.nunits && ok; u += gridDim.x)
 		{
 			for(int kt = 0; kt < nkt; kt++, kk++)
 			{
-				const int rs = kk % kRS, as = kk % kAS;
-				if(!mbar_wait(&full_raw[rs], (kk / kRS) & 1, &fail_s) ||
-				   (kk >= kAS && !mbar_wait(&empty_a[as], ((kk / kAS) - 1) & 1, &fail_s)))
+				const int rs = kk % nrs, as = kk % nas;
+				if(!mbar_wait(&full_raw[rs], (kk / nrs) & 1, &fail_s) ||
+				   (kk >= nas && !mbar_wait(&empty_a[as], ((kk / nas) - 1) & 1, &fail_s)))
 				{
 					fail_s = 5;
 					ok = false;
 					break;
 				}
 				const uint32_t *raw = (const uint32_t *)(raw0 + (size_t)rs * tp.raw_stride);
-				unsigned char *A = a0 + (size_t)as * kNG * kTileBytes;
-				for(int i = tt; i < items; i += 128)
+				unsigned char *A = a0 + (size_t)as * kStageBytes;
+#pragma unroll
+				for(int j = 0; j < kMaxItems; j++)
 				{
-					const int tc = i / rc, rem = i - tc * rc;
-					const int row = rem / tp.CB, cl = rem - row * tp.CB;
-					const int g = cl / tp.G, q = cl - g * tp.G;
+					if(src_off[j] < 0)
+						continue;
+					const uint32_t *src = raw + (src_off[j] & ((1 << 30) - 1));
 					uint32_t w[8];
 #pragma unroll
-					for(int j = 0; j < 8; j++)
-						w[j] = raw[(tc * 8 + j) * rc + rem];
+					for(int t = 0; t < 8; t++)
+						w[t] = src[t * rc];
 					uint4 re, im;
 					re.x = __byte_perm(w[0], w[1], 0x5410);
 					re.y = __byte_perm(w[2], w[3], 0x5410);
@@ -342,11 +378,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 					im.y = __byte_perm(w[2], w[3], 0x7632);
 					im.z = __byte_perm(w[4], w[5], 0x7632);
 					im.w = __byte_perm(w[6], w[7], 0x7632);
-					const int m = q * tp.r2p + 2 * row;
-					const int sw = (tc ^ ((m >> 1) & 3)) << 4;     // rows m, m+1 share the swizzle phase
-					unsigned char *tile = A + g * kTileBytes;
-					*(uint4 *)(tile + m * 64 + sw) = re;
-					*(uint4 *)(tile + (m + 1) * 64 + sw) = im;
+					const bool swap = (src_off[j] >> 30) & 1;
+					*(uint4 *)(A + dst_lo[j]) = swap ? im : re;
+					*(uint4 *)(A + dst_hi[j]) = swap ? re : im;
 				}
 				// generic-proxy writes -> visible to the tensor core's async proxy
 				asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -367,22 +401,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 		const int lq = warp & 3;
 		const int et = threadIdx.x - 192;
 		const int row = 32 * lq + lane;          // accumulator row of this thread
+		const int nin = tp.nrow, ds = tp.dstride;
 		int ku = 0;
 		for(int u = blockIdx.x; u < tp.nunits; u += gridDim.x, ku++)
 		{
+			const int buf = ku & 1;
 			const int fi = u / tp.nblk, blk = u - fi * tp.nblk;
 			const DevFreqPlan &P = plans[plan_idx[fi]];
 			const int nout = P.acc_cstride;
 			const int c_first = blk * tp.CB;
-			for(int i = et; i < tp.CB * nout; i += 128)
-				vbuf[i] = make_float2(0.0f, 0.0f);
-			bool bad = !mbar_wait(&acc_full, ku & 1, &fail_s);
+			const int ncv = min(tp.CB, tp.nchan - c_first);
+			bool bad = !mbar_wait(&acc_full[buf], (ku >> 1) & 1, &fail_s);
 			if(bad)
 				fail_s = 6;
 			if(epi_sync_or(bad))
 				break;                        // all four warps leave together
 			asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-			const int nin = tp.nrow;
+			// 1. copy each channel's 2 nin x 2 nin block of the accumulators to
+			// dump[cl][r2][c2] (rows of ds floats), then release the buffer
 			for(int g = 0; g < kNG; g++)
 			{
 				const int qlo = (32 * lq) / tp.r2p;
@@ -391,49 +427,67 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 				{
 					const int cl = g * tp.G + q;
 					const int r2 = row - q * tp.r2p;
-					const bool mine = r2 >= 0 && r2 < 2 * nin && (r2 & 1) == 0 && c_first + cl < tp.nchan;
-					const int a = r2 >> 1;
-					for(int j8 = 0; j8 < 2 * nin; j8 += 8)
+					const bool keep = r2 >= 0 && r2 < 2 * nin && cl < ncv;
+					float *drow = dump + ((size_t)cl * 2 * nin + (keep ? r2 : 0)) * ds;
+					const uint32_t tbase =
+					    tmem + ((uint32_t)(32 * lq) << 16) + (uint32_t)(buf * 256 + g * 128 + q * tp.r2p);
+					for(int j0 = 0; j0 < 2 * nin; j0 += 32)
 					{
-						float pv[8];
-						tmem_ld8(tmem + ((uint32_t)(32 * lq) << 16) + (uint32_t)(g * 128 + q * tp.r2p + j8), pv);
-						tmem_ld_wait();
+						float pv[32];
+						const int nl = min(4, (2 * nin - j0 + 7) >> 3);
 #pragma unroll
-						for(int h = 0; h < 4; h++)
+						for(int c = 0; c < 4; c++)
+							if(c < nl)
+								tmem_ld8(tbase + (uint32_t)(j0 + 8 * c), pv + 8 * c);
+						tmem_ld_wait();
+						if(keep)
 						{
-							const int b = (j8 >> 1) + h;
-							const float p_re = pv[2 * h], p_im = pv[2 * h + 1];         // P[row][2b], P[row][2b+1]
-							const float o_re = __shfl_xor_sync(0xffffffffu, p_re, 1);   // partner row's P[.][2b]
-							const float o_im = __shfl_xor_sync(0xffffffffu, p_im, 1);   // partner row's P[.][2b+1]
-							if(!mine || b >= nin || b < a)
-								continue;
-							const float vre = p_re + o_im;      // P[2a][2b] + P[2a+1][2b+1]
-							const float vim = o_re - p_im;      // P[2a+1][2b] - P[2a][2b+1]
-							const int dA = P.destA[a * nin + b];
-							const int dB = P.destB[a * nin + b];
-							if(dA >= 0)
-								vbuf[cl * nout + dA] = make_float2(vre, vim);
-							if(dB >= 0)
-								vbuf[cl * nout + dB] = make_float2(vre, -vim);
+#pragma unroll
+							for(int c = 0; c < 4; c++)
+								if(c < nl)
+								{
+									*(float4 *)(drow + j0 + 8 * c) = make_float4(pv[8 * c], pv[8 * c + 1], pv[8 * c + 2], pv[8 * c + 3]);
+									*(float4 *)(drow + j0 + 8 * c + 4) =
+									    make_float4(pv[8 * c + 4], pv[8 * c + 5], pv[8 * c + 6], pv[8 * c + 7]);
+								}
 						}
 					}
 				}
-				// this warp is done with accumulator g
-				asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-				__syncwarp();
-				if(lane == 0)
-					mbar_arrive(&acc_empty[g]);
 			}
+			asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+			__syncwarp();
+			if(lane == 0)
+				mbar_arrive(&acc_empty[buf]);
 			epi_sync();
-			// coalesced accumulate into the contiguous [channel][output] block
-			const int nvalid = min(tp.CB, tp.nchan - c_first) * nout;
+			// 2. outputs: V[a][b] = (P[2a][2b] + P[2a+1][2b+1], P[2a+1][2b] - P[2a][2b+1]) with
+			// input a of channel cl at position (a + cl) mod nin; vector reductions
+			// into the contiguous [channel][output] block (one addition per output
+			// and subint, so the sum is that of a load-add-store)
+			const int32_t *outsrc = P.outsrc;
 			float2 *dst = acc + P.acc_off + (int64_t)c_first * nout;
-			for(int i = et; i < nvalid; i += 128)
+			for(int cl = 0; cl < ncv; cl++)
 			{
-				const float2 v = vbuf[i], o = dst[i];
-				dst[i] = make_float2(o.x + v.x, o.y + v.y);
+				const int cln = cl % nin;
+				const float *D = dump + (size_t)cl * 2 * nin * ds;
+				for(int o = et; o < nout; o += 128)
+				{
+					const int src = __ldg(outsrc + o);
+					if(src < 0)
+						continue;
+					int pa = (src & 0xFF) + cln, pb = ((src >> 8) & 0xFF) + cln;
+					if(pa >= nin)
+						pa -= nin;
+					if(pb >= nin)
+						pb -= nin;
+					const float *r0 = D + (2 * pa) * ds + 2 * pb, *r1 = r0 + ds;
+					const float vre = r0[0] + r1[1];
+					float vim = r1[0] - r0[1];
+					if(src >> 16)
+						vim = -vim;
+					atomicAdd(dst + (int64_t)cl * nout + o, make_float2(vre, vim));
+				}
 			}
-			epi_sync();
+			epi_sync();                       // the copy area is free for the next unit
 		}
 	}
 
@@ -443,7 +497,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 	{
 		// on the error path, wait (bounded) for TMA loads that nobody consumed
 		for(int kk = consumed_s; kk < issued_s; kk++)
-			mbar_wait(&full_raw[kk % kRS], (kk / kRS) & 1, &fail_s);
+			mbar_wait(&full_raw[kk % nrs], (kk / nrs) & 1, &fail_s);
 		if(fail_s && tp.err)
 			atomicExch(tp.err, fail_s);
 	}
@@ -458,7 +512,7 @@ typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32
                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-bool tc_shape(int nrow, int nchan, int T, int nout_max, TcShape *s)
+bool tc_shape(int nrow, int nchan, int T, TcShape *s)
 {
 	s->nrow = nrow;
 	s->nchan = nchan;
@@ -470,14 +524,28 @@ bool tc_shape(int nrow, int nchan, int T, int nout_max, TcShape *s)
 	s->Tpad = (T + kKT - 1) / kKT * kKT;
 	s->raw_bytes = s->CB * nrow * kKT * 4;
 	s->raw_stride = (s->raw_bytes + 1023) & ~1023;
-	s->vbuf_floats = 2 * s->CB * nout_max;
-	s->smem = 1024 + (size_t)kRS * s->raw_stride + (size_t)kAS * kNG * kTileBytes + (size_t)s->vbuf_floats * 4;
-	return s->smem <= 227 * 1024;
+	s->dstride = s->r2p + 4;
+	const size_t dump = (size_t)s->CB * 2 * nrow * s->dstride * 4;
+	// deepest rings that fit beside the accumulator copy
+	static const int order[][2] = {{6, 4}, {6, 3}, {5, 3}, {5, 2}, {4, 2}, {3, 2}, {2, 2}};
+	for(const auto &o : order)
+	{
+		const size_t rings = (size_t)o[0] * s->raw_stride + (size_t)o[1] * kNG * kTileBytes;
+		if(1024 + rings + dump <= 227 * 1024)
+		{
+			s->nrs = o[0];
+			s->nas = o[1];
+			s->dump_off = (int32_t)rings;
+			s->smem = 1024 + rings + dump;
+			return true;
+		}
+	}
+	return false;
 }
 
-// 3D map over one group's spectra [nf * Tpad][nrow][nchan] of 4-byte bf16x2
-// values; box {CB channels, nrow, 32 times}.  The x coordinate (first
-// channel of a unit) is a multiple of CB = 4 G, i.e. of 16 bytes.
+// 3D map over one group's spectra [nf * Tpad][nblk][nrow * CB] of 4-byte
+// bf16x2 values; box {nrow * CB, 1 block, 32 times}: each of its 32 rows is
+// one contiguous run of nrow * CB <= 256 values.
 bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf)
 {
 	if(((uintptr_t)map_out & 63) != 0 || ((uintptr_t)spec & 15) != 0)
@@ -492,9 +560,13 @@ bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf
 			return false;
 		encode = (PFN_encodeTiled)fn;
 	}
-	cuuint64_t dims[3] = {(cuuint64_t)s.nchan, (cuuint64_t)s.nrow, (cuuint64_t)s.Tpad * nf};
-	cuuint64_t strides[2] = {(cuuint64_t)s.nchan * 4, (cuuint64_t)s.nrow * s.nchan * 4};
-	cuuint32_t box[3] = {(cuuint32_t)s.CB, (cuuint32_t)s.nrow, (cuuint32_t)kKT};
+	const cuuint64_t W = (cuuint64_t)s.nrow * s.CB;
+	const cuuint64_t nblk = (cuuint64_t)((s.nchan + s.CB - 1) / s.CB);
+	if(W > 256)
+		return false;
+	cuuint64_t dims[3] = {W, nblk, (cuuint64_t)s.Tpad * nf};
+	cuuint64_t strides[2] = {W * 4, nblk * W * 4};
+	cuuint32_t box[3] = {(cuuint32_t)W, 1, (cuuint32_t)kKT};
 	cuuint32_t estr[3] = {1, 1, 1};
 	CUresult r = encode((CUtensorMap *)map_out, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, (void *)spec, dims, strides, box,
 	                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -522,7 +594,10 @@ void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplan
 	tp.nunits = tp.nblk * nf;
 	tp.raw_bytes = s.raw_bytes;
 	tp.raw_stride = s.raw_stride;
-	tp.vbuf_floats = s.vbuf_floats;
+	tp.nrs = s.nrs;
+	tp.nas = s.nas;
+	tp.dstride = s.dstride;
+	tp.dump_off = s.dump_off;
 	tp.err = err;
 	cudaFuncSetAttribute(k_xmac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
 	const int grid = tp.nunits < nsm ? tp.nunits : nsm;
