@@ -331,28 +331,48 @@ void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, 
 // Baseline weights sum_t w1*w2 (core.cpp:998-1045) and autocorrelation
 // weights sum_t w (mode.cpp:1304-1307), each as a sequential float sum in FFT
 // order, added to the running totals (core.cpp:1068-1086, 1310-1363).
+// Baseline and autocorrelation weights of one subint: the float sums of
+// w1(t) * w2(t) (baseline) and of w(t) over valid FFTs (autocorrelation), added
+// in FFT order as Core does.  One warp per weight: the lanes load and multiply
+// 256 FFTs at a time in parallel, then lane 0 adds them in order (adding 0 for
+// an invalid FFT leaves a non-negative float sum unchanged).
 __global__ void k_weights(const DevBWeight *__restrict__ bw, int nbw, const DevACWeight *__restrict__ acw, int nacw,
                           const FftParam *__restrict__ params, int T, float *__restrict__ bwacc, float *__restrict__ acwacc)
 {
-	int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if(k < nbw)
+	__shared__ float buf[4][256];
+	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int k = blockIdx.x * 4 + w;
+	if(k >= nbw + nacw)
+		return;
+	const bool isb = k < nbw;
+	const FftParam *p1 = params + (int64_t)(isb ? bw[k].s1 : acw[k - nbw].s) * T;
+	const FftParam *p2 = params + (int64_t)(isb ? bw[k].s2 : 0) * T;
+	float sum = 0.0f;
+	for(int t0 = 0; t0 < T; t0 += 256)
 	{
-		const FftParam *p1 = params + (int64_t)bw[k].s1 * T;
-		const FftParam *p2 = params + (int64_t)bw[k].s2 * T;
-		float sum = 0.0f;
-		for(int t = 0; t < T; t++)
-			sum = __fadd_rn(sum, __fmul_rn(p1[t].weight, p2[t].weight));
-		bwacc[k] = __fadd_rn(bwacc[k], sum);
+		const int n = min(256, T - t0);
+		for(int j = lane; j < n; j += 32)
+		{
+			const int t = t0 + j;
+			float v;
+			if(isb)
+				v = __fmul_rn(p1[t].weight, p2[t].weight);
+			else
+				v = p1[t].status == kFftOk ? p1[t].weight : 0.0f;
+			buf[w][j] = v;
+		}
+		__syncwarp();
+		if(lane == 0)
+			for(int j = 0; j < n; j++)
+				sum = __fadd_rn(sum, buf[w][j]);
+		__syncwarp();
 	}
-	else if(k < nbw + nacw)
+	if(lane == 0)
 	{
-		int a = k - nbw;
-		const FftParam *p = params + (int64_t)acw[a].s * T;
-		float sum = 0.0f;
-		for(int t = 0; t < T; t++)
-			if(p[t].status == kFftOk)
-				sum = __fadd_rn(sum, p[t].weight);
-		acwacc[a] = __fadd_rn(acwacc[a], sum);
+		if(isb)
+			bwacc[k] = __fadd_rn(bwacc[k], sum);
+		else
+			acwacc[k - nbw] = __fadd_rn(acwacc[k - nbw], sum);
 	}
 }
 
@@ -362,7 +382,7 @@ void launch_weights(const DevBWeight *bw, int nbw, const DevACWeight *acw, int n
 	int n = nbw + nacw;
 	if(n == 0)
 		return;
-	k_weights<<<(n + 127) / 128, 128, 0, stream>>>(bw, nbw, acw, nacw, params, T, bwacc, acwacc);
+	k_weights<<<(n + 3) / 4, 128, 0, stream>>>(bw, nbw, acw, nacw, params, T, bwacc, acwacc);
 }
 
 // Core-result assembly (core.cpp:1774-1802 channel averaging, 1266-1363):

@@ -317,30 +317,37 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 		// rotation by cl, and the alternating order of the two stores, spread
 		// the 16-byte stores of neighbouring threads over all banks.
 		const int tt = threadIdx.x - 64;
-		const int rc = tp.nrow * tp.CB;
-		const int items = 4 * rc;                      // (8-time chunk, row, channel)
-		constexpr int kMaxItems = 8;                   // 4 * 256 / 128
-		int src_off[kMaxItems], dst_lo[kMaxItems], dst_hi[kMaxItems];
+		const int rc = tp.nrow * tp.CB;                // even: CB = 2 G
+		const int npairs = rc >> 1;
+		const int items = 4 * npairs;                  // (8-time chunk, pair of neighbouring values)
+		constexpr int kMaxItems = 2;                   // 4 * 128 / 2 / 128
+		int src_off[kMaxItems], dst_a[kMaxItems][2], dst_b[kMaxItems][2];
+		uint32_t swapm[kMaxItems];
 #pragma unroll
 		for(int j = 0; j < kMaxItems; j++)
 		{
 			const int i = tt + 128 * j;
 			src_off[j] = -1;
+			swapm[j] = 0;
 			if(i < items)
 			{
-				const int tc = i / rc, rem = i - tc * rc;
-				const int row = rem / tp.CB, cl = rem - row * tp.CB;
-				const int g = cl / tp.G, q = cl - g * tp.G;
-				const int pos = (row + cl) % tp.nrow;
-				const int m = q * tp.r2p + 2 * pos;
-				const int sw = (tc ^ ((m >> 1) & 3)) << 4;     // rows m, m+1 share the swizzle phase
-				const int re_off = g * kTileBytes + m * 64 + sw, im_off = re_off + 64;
-				const bool swap = (rem >> 2) & 1;
-				src_off[j] = tc * 8 * rc + rem;
-				dst_lo[j] = swap ? im_off : re_off;            // first store: real part unless swapped
-				dst_hi[j] = swap ? re_off : im_off;
-				if(swap)
-					src_off[j] |= 1 << 30;                     // flag: first store takes the imaginary halves
+				const int tc = i / npairs, pr = i - tc * npairs;
+				src_off[j] = (tc * 8 * rc + 2 * pr) >> 1;      // in 8-byte units
+#pragma unroll
+				for(int e = 0; e < 2; e++)
+				{
+					const int rem = 2 * pr + e;
+					const int row = rem / tp.CB, cl = rem - row * tp.CB;
+					const int g = cl / tp.G, q = cl - g * tp.G;
+					const int pos = (row + cl) % tp.nrow;
+					const int m = q * tp.r2p + 2 * pos;
+					const int sw = (tc ^ ((m >> 1) & 3)) << 4;     // rows m, m+1 share the swizzle phase
+					const int re_off = g * kTileBytes + m * 64 + sw, im_off = re_off + 64;
+					const bool swp = (rem >> 2) & 1;               // first store takes the imaginary row
+					dst_a[j][e] = swp ? im_off : re_off;
+					dst_b[j][e] = swp ? re_off : im_off;
+					swapm[j] |= (uint32_t)swp << e;
+				}
 			}
 		}
 		int kk = 0;
@@ -357,30 +364,40 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 					ok = false;
 					break;
 				}
-				const uint32_t *raw = (const uint32_t *)(raw0 + (size_t)rs * tp.raw_stride);
+				const uint2 *raw = (const uint2 *)(raw0 + (size_t)rs * tp.raw_stride);
 				unsigned char *A = a0 + (size_t)as * kStageBytes;
 #pragma unroll
 				for(int j = 0; j < kMaxItems; j++)
 				{
 					if(src_off[j] < 0)
 						continue;
-					const uint32_t *src = raw + (src_off[j] & ((1 << 30) - 1));
-					uint32_t w[8];
+					const uint2 *src = raw + src_off[j];
+					uint2 w[8];
 #pragma unroll
 					for(int t = 0; t < 8; t++)
-						w[t] = src[t * rc];
-					uint4 re, im;
-					re.x = __byte_perm(w[0], w[1], 0x5410);
-					re.y = __byte_perm(w[2], w[3], 0x5410);
-					re.z = __byte_perm(w[4], w[5], 0x5410);
-					re.w = __byte_perm(w[6], w[7], 0x5410);
-					im.x = __byte_perm(w[0], w[1], 0x7632);
-					im.y = __byte_perm(w[2], w[3], 0x7632);
-					im.z = __byte_perm(w[4], w[5], 0x7632);
-					im.w = __byte_perm(w[6], w[7], 0x7632);
-					const bool swap = (src_off[j] >> 30) & 1;
-					*(uint4 *)(A + dst_lo[j]) = swap ? im : re;
-					*(uint4 *)(A + dst_hi[j]) = swap ? re : im;
+						w[t] = src[t * npairs];
+					uint4 re0, im0, re1, im1;
+					re0.x = __byte_perm(w[0].x, w[1].x, 0x5410);
+					re0.y = __byte_perm(w[2].x, w[3].x, 0x5410);
+					re0.z = __byte_perm(w[4].x, w[5].x, 0x5410);
+					re0.w = __byte_perm(w[6].x, w[7].x, 0x5410);
+					im0.x = __byte_perm(w[0].x, w[1].x, 0x7632);
+					im0.y = __byte_perm(w[2].x, w[3].x, 0x7632);
+					im0.z = __byte_perm(w[4].x, w[5].x, 0x7632);
+					im0.w = __byte_perm(w[6].x, w[7].x, 0x7632);
+					re1.x = __byte_perm(w[0].y, w[1].y, 0x5410);
+					re1.y = __byte_perm(w[2].y, w[3].y, 0x5410);
+					re1.z = __byte_perm(w[4].y, w[5].y, 0x5410);
+					re1.w = __byte_perm(w[6].y, w[7].y, 0x5410);
+					im1.x = __byte_perm(w[0].y, w[1].y, 0x7632);
+					im1.y = __byte_perm(w[2].y, w[3].y, 0x7632);
+					im1.z = __byte_perm(w[4].y, w[5].y, 0x7632);
+					im1.w = __byte_perm(w[6].y, w[7].y, 0x7632);
+					const bool s0 = swapm[j] & 1u, s1 = (swapm[j] >> 1) & 1u;
+					*(uint4 *)(A + dst_a[j][0]) = s0 ? im0 : re0;
+					*(uint4 *)(A + dst_b[j][0]) = s0 ? re0 : im0;
+					*(uint4 *)(A + dst_a[j][1]) = s1 ? im1 : re1;
+					*(uint4 *)(A + dst_b[j][1]) = s1 ? re1 : im1;
 				}
 				// generic-proxy writes -> visible to the tensor core's async proxy
 				asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -465,26 +482,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 			// and subint, so the sum is that of a load-add-store)
 			const int32_t *outsrc = P.outsrc;
 			float2 *dst = acc + P.acc_off + (int64_t)c_first * nout;
-			for(int cl = 0; cl < ncv; cl++)
+			for(int o = et; o < nout; o += 128)
 			{
-				const int cln = cl % nin;
-				const float *D = dump + (size_t)cl * 2 * nin * ds;
-				for(int o = et; o < nout; o += 128)
+				const int src = __ldg(outsrc + o);
+				if(src < 0)
+					continue;
+				const int a = src & 0xFF, b = (src >> 8) & 0xFF;
+				const bool cj = (src >> 16) != 0;
+				int cln = 0;                      // cl mod nin
+				for(int cl = 0; cl < ncv; cl++)
 				{
-					const int src = __ldg(outsrc + o);
-					if(src < 0)
-						continue;
-					int pa = (src & 0xFF) + cln, pb = ((src >> 8) & 0xFF) + cln;
+					int pa = a + cln, pb = b + cln;
 					if(pa >= nin)
 						pa -= nin;
 					if(pb >= nin)
 						pb -= nin;
-					const float *r0 = D + (2 * pa) * ds + 2 * pb, *r1 = r0 + ds;
+					const float *r0 = dump + ((size_t)cl * 2 * nin + 2 * pa) * ds + 2 * pb, *r1 = r0 + ds;
 					const float vre = r0[0] + r1[1];
-					float vim = r1[0] - r0[1];
-					if(src >> 16)
-						vim = -vim;
-					atomicAdd(dst + (int64_t)cl * nout + o, make_float2(vre, vim));
+					const float vim = r1[0] - r0[1];
+					atomicAdd(dst + (int64_t)cl * nout + o, make_float2(vre, cj ? -vim : vim));
+					if(++cln == nin)
+						cln = 0;
 				}
 			}
 			epi_sync();                       // the copy area is free for the next unit
