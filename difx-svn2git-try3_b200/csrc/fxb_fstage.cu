@@ -202,6 +202,18 @@ __host__ __device__ inline float level2(uint32_t code)
 
 __device__ __forceinline__ float frac_centered(double x) { return (float)(x - rint(x)); }
 
+constexpr int kMaxTQ = 4;         // FFT iterations per CTA at most
+
+// Constants of one FFT, computed once per CTA (one warp per FFT).
+struct FftConst {
+	float P0, alpha, beta, gamma, eps;   // fringe phase (turns): start and per-sample terms
+	float dfs, postf;                    // fractional-sample turns per channel, order-0 post-F turns
+	uint32_t fa, so;                     // first frame of the window, window start within it
+	uint32_t fmask;                      // validity of the window's frames (bit k: frame fa + k)
+	int32_t stuck;                       // samples [stuck, N) read as zero
+	int32_t flags;                       // 1: valid FFT, 2: fmask covers the window
+};
+
 // One middle radix-8 pass (stride s = 2^LOGS, m = N / (8 s)) over the
 // thread's KB butterflies: x_r = X[q + s (p + r m)], y = DFT8(x),
 // Y[q + s (8 p + r)] = y_r w_N^(r p s).  With two buffers each butterfly
@@ -353,66 +365,82 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage
 
 	const int t0 = tchunk * a.tq * FPC;
 	const int nit = min(a.tq, (a.T - t0 + FPC - 1) / FPC);
+	// ---- constants of the CTA's FFTs (FFT f is time t0 + f), one warp per FFT
+	__shared__ FftConst fcs[kMaxTQ * FPC];
+	{
+		const int lane = threadIdx.x & 31;
+		const int nfc = nit * FPC;
+		for(int f = threadIdx.x >> 5; f < nfc; f += blockDim.x >> 5)
+		{
+			const int t = t0 + f;
+			FftConst c;
+			c.P0 = c.alpha = c.beta = c.gamma = c.eps = c.dfs = c.postf = 0.0f;
+			c.fa = c.so = c.fmask = 0u;
+			c.stuck = 0;
+			c.flags = 0;
+			if(t < a.T)
+			{
+				const FftParam *pq = a.params + (int64_t)g.station * a.T + t;
+				if(pq->status == kFftOk)
+				{
+					c.flags = 1;
+					const uint32_t g0 = (uint32_t)pq->nearest;
+					c.fa = g0 / fs;
+					c.so = g0 - c.fa * fs;
+					c.stuck = pq->stuck;
+					const double invN = 1.0 / N;
+					const int idl = pq->integerdelay;
+					const double fraclo = a.fraclo ? (lo - (int)lo) * (double)idl : 0.0;
+					if(order == 1)
+					{
+						c.P0 = frac_centered(lo * pq->b + fraclo);
+						c.alpha = (float)(lo * pq->a * invN);
+					}
+					else if(order == 2)
+					{
+						const double pa = pq->a, pb = pq->b;
+						const double X1 = (double)asl * invN;
+						c.P0 = frac_centered(lo * pq->c + fraclo);
+						c.alpha = (float)(lo * (pb + pa * X1) * invN);
+						c.beta = (float)(lo * 2.0 * pa * X1 * invN);
+						c.gamma = (float)(lo * pb * asl * invN);
+						c.eps = (float)(lo * pa * X1 * X1);
+					}
+					c.dfs = (float)(bw * (1.0 / nchan) * (double)pq->fse);
+					if(order == 0)
+					{
+						double pr = (pq->averagedelay - idl) * lo;
+						if(a.fraclo)
+							pr += idl * (lo - (int)lo);
+						c.postf = -(float)(pr - (int)pr);
+					}
+				}
+			}
+			// validity of the window's frames, one bit per frame relative to fa
+			const uint32_t nwf = (c.so + (uint32_t)N - 1) / fs + 1;
+			const int64_t fr = (int64_t)c.fa + lane;
+			const bool v = (c.flags & 1) && (uint32_t)lane < nwf && fr < a.valid_stride && vrow[fr] != 0;
+			c.fmask = __ballot_sync(0xffffffffu, v);
+			if(nwf <= 32)
+				c.flags |= 2;
+			if(lane == 0)
+				fcs[f] = c;
+		}
+		__syncthreads();
+	}
 	int wb = 0;
 	for(int it = 0; it < nit; it++)
 	{
 		const int t = t0 + it * FPC + slot;
 		const bool tok = t < a.T;
 		// ---- per-FFT constants
-		bool active = false;
-		uint32_t fa = 0, so = 0;
-		int stuck = 0;
-		float P0 = 0.0f, alpha = 0.0f, beta = 0.0f, gamma = 0.0f, eps = 0.0f, dfs = 0.0f, postf = 0.0f;
-		if(tok)
-		{
-			const FftParam *pq = a.params + (int64_t)g.station * a.T + t;
-			active = pq->status == kFftOk;
-			if(active)
-			{
-				const uint32_t g0 = (uint32_t)pq->nearest;
-				fa = g0 / fs;
-				so = g0 - fa * fs;
-				stuck = pq->stuck;
-				const double invN = 1.0 / N;
-				const int idl = pq->integerdelay;
-				const double fraclo = a.fraclo ? (lo - (int)lo) * (double)idl : 0.0;
-				if(order == 1)
-				{
-					P0 = frac_centered(lo * pq->b + fraclo);
-					alpha = (float)(lo * pq->a * invN);
-				}
-				else if(order == 2)
-				{
-					const double pa = pq->a, pb = pq->b;
-					const double X1 = (double)asl * invN;
-					P0 = frac_centered(lo * pq->c + fraclo);
-					alpha = (float)(lo * (pb + pa * X1) * invN);
-					beta = (float)(lo * 2.0 * pa * X1 * invN);
-					gamma = (float)(lo * pb * asl * invN);
-					eps = (float)(lo * pa * X1 * X1);
-				}
-				dfs = (float)(bw * (1.0 / nchan) * (double)pq->fse);
-				if(order == 0)
-				{
-					double pr = (pq->averagedelay - idl) * lo;
-					if(a.fraclo)
-						pr += idl * (lo - (int)lo);
-					postf = -(float)(pr - (int)pr);
-				}
-			}
-		}
-		// validity of the window's frames, one bit per frame relative to fa
-		// (a warp holds one slot when TPF >= 32; otherwise looked up per sample)
-		const uint32_t nwf = (so + (uint32_t)N - 1) / fs + 1;
-		uint32_t fmask = 0;
-		const bool narrow = TPF >= 32 && nwf <= 32;
-		if constexpr(TPF >= 32)
-		{
-			const int lane = threadIdx.x & 31;
-			const int64_t fr = (int64_t)fa + lane;
-			const bool v = active && (uint32_t)lane < nwf && fr < a.valid_stride && vrow[fr] != 0;
-			fmask = __ballot_sync(0xffffffffu, v);
-		}
+		const FftConst &fc = fcs[it * FPC + slot];
+		const bool active = (fc.flags & 1) != 0;
+		const uint32_t fa = fc.fa, so = fc.so, fmask = fc.fmask;
+		const int stuck = fc.stuck;
+		const float P0 = fc.P0, alpha = fc.alpha, beta = fc.beta, gamma = fc.gamma, eps = fc.eps;
+		const float dfs = fc.dfs, postf = fc.postf;
+		const bool narrow = (fc.flags & 2) != 0;
 		// ---- 1-3. decode, fringe-rotate and run the first radix-8 pass (s = 1:
 		// butterfly b, twiddle w_N^(r b)), one butterfly at a time
 		{
@@ -426,7 +454,9 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage
 				const uint32_t xs = so + (uint32_t)b;
 				uint32_t kf = xs / fs, tin = xs - kf * fs;
 				const uint8_t *fp = buf + ((int64_t)fa + kf) * framebytes + header;
-				C x[NV][8];
+				// phase A: frame tracking and every word load of the 8 samples
+				// (nothing waits on a load before all are issued)
+				uint32_t raw0[8], raw1[8], pk[8];
 #pragma unroll
 				for(int r = 0; r < 8; r++)
 				{
@@ -440,12 +470,32 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage
 						ok = active && fr < a.valid_stride && vrow[fr] != 0;
 					}
 					ok = ok && n < stuck;
-					float v0 = 0.0f, v1 = 0.0f;
-					if(ok)
+					const uint32_t bit0 = tin * bpt + boff0, bit1 = tin * bpt + boff1;
+					const uint32_t *wp = (const uint32_t *)fp;
+					raw0[r] = ok ? __ldg(wp + (bit0 >> 5)) : 0u;
+					raw1[r] = (ok && !oneword && (H || NV == 2)) ? __ldg(wp + (bit1 >> 5)) : 0u;
+					pk[r] = (bit0 & 31u) | ((bit1 & 31u) << 8) | ((uint32_t)ok << 16);
+					if(r < 7)
 					{
-						const uint32_t bit0 = tin * bpt + boff0;
-						const uint32_t raw0 = __ldg((const uint32_t *)fp + (bit0 >> 5));
-						const uint32_t w0 = raw0 >> (bit0 & 31u);
+						tin += (uint32_t)(N / 8);
+						while(tin >= fs)
+						{
+							tin -= fs;
+							kf++;
+							fp += framebytes;
+						}
+					}
+				}
+				// phase B: levels, fringe rotation
+				C x[NV][8];
+#pragma unroll
+				for(int r = 0; r < 8; r++)
+				{
+					const int n = b + r * (N / 8);
+					float v0 = 0.0f, v1 = 0.0f;
+					if((pk[r] >> 16) & 1u)
+					{
+						const uint32_t w0 = raw0[r] >> (pk[r] & 31u);
 						if(pair4)
 						{
 							const float2 l = lut4[w0 & 15u];
@@ -457,9 +507,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage
 							v0 = nbits == 2 ? level2(w0 & 3u) : lut8[w0 & 255u];
 							if(H || NV == 2)
 							{
-								const uint32_t bit1 = tin * bpt + boff1;
-								const uint32_t w1 =
-								    (oneword ? raw0 : __ldg((const uint32_t *)fp + (bit1 >> 5))) >> (bit1 & 31u);
+								const uint32_t w1 = (oneword ? raw0[r] : raw1[r]) >> ((pk[r] >> 8) & 31u);
 								v1 = nbits == 2 ? level2(w1 & 3u) : lut8[w1 & 255u];
 							}
 						}
@@ -489,16 +537,6 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, FShape<LOGN>::MINB) k_fstage
 						x[0][r] = cf{v0 * cs, v0 * sn};
 						if constexpr(NV == 2)
 							x[1][r] = cf{v1 * cs, v1 * sn};
-					}
-					if(r < 7)
-					{
-						tin += (uint32_t)(N / 8);
-						while(tin >= fs)
-						{
-							tin -= fs;
-							kf++;
-							fp += framebytes;
-						}
 					}
 				}
 #pragma unroll
