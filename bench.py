@@ -8,11 +8,15 @@ One step = 125 subintegrations = 1 s of data for every station.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fxb|reference]
 
-Prints one JSON line: value = station.MHz/s processed (whole job, all GPUs),
-with the real-time factor, the end-to-end figure through the C ABI with host
-buffers (host->device copies of the raw VDIF and the device->host read of the
-core result inside the timed region), the roofline of the dominant kernel,
-the reference CPU baseline and the SM clocks seen during the timed region.
+Prints one JSON line: value = station.MHz/s processed (whole job, all GPUs)
+by the headline form -- by default the tensor-core form (FP16 FFT, BF16
+spectra, tcgen05 XMAC with FP32 accumulation; --xmac fp32 selects the plain
+FP32 form) -- with the real-time factor, the other form measured beside it on
+the same workload (other_form, tc_vs_fp32), the end-to-end figure through the
+C ABI with host buffers (host->device copies of the raw VDIF and the
+device->host read of the core result inside the timed region), the rooflines
+of the F stage (HBM) and of the XMAC (tensor pipe), the reference CPU baseline
+and the SM clocks seen during the timed region.
 
 Inputs: a pool of 16 distinct subintegrations per station (bulk synthetic
 VDIF with the 2-bit quantiser's code statistics, 327 MB in device memory,
@@ -51,9 +55,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fxb", choices=["fxb", "reference"])
-    ap.add_argument("--xmac", default="fp32", choices=["fp32", "bf16", "fp8"],
-                    help="arithmetic of the headline form (fp32 = the reference's precision)")
-    ap.add_argument("--no-tc-form", action="store_true", help="skip measuring the tensor-core form beside it")
+    ap.add_argument("--xmac", default="bf16", choices=["fp32", "bf16"],
+                    help="headline form: bf16 = tensor-core form (FP16 FFT, BF16 spectra, tcgen05 XMAC with FP32 "
+                         "accumulation), fp32 = the plain FP32 form; the other form is measured beside it")
+    ap.add_argument("--no-other-form", "--no-tc-form", dest="no_other_form", action="store_true",
+                    help="skip measuring the other form beside the headline")
     ap.add_argument("--subints-per-step", type=int, default=125)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -329,10 +335,11 @@ def gpu_arm(args, job):
     h2d = sum(nbytes[j % POOL][s] for j in range(nsub) for s in range(S))
     d2h = 2 * corr.corelen * 4
 
-    # ---- the tensor-core form on the same workload (device-resident)
-    tc_form = None
-    if not args.no_tc_form and args.xmac == "fp32":
-        ctc = Correlator(job, xmac="bf16", inflight=3)
+    # ---- the other form on the same workload (device-resident)
+    other = None
+    other_name = "fp32" if args.xmac == "bf16" else "bf16"
+    if not args.no_other_form:
+        ctc = Correlator(job, xmac=other_name, inflight=3)
         for _ in range(args.warmup):
             step_device(ctc)
         ctc.sync()
@@ -350,34 +357,47 @@ def gpu_arm(args, job):
         n2, p2, f2, x2 = ctc.timing_read()
         tms = max_over_ranks(e0.elapsed_time(e1))
         tval = job.station_mhz_per_sec() * data_s / (tms * 1e-3)
-        tc_form = {"value": tval, "unit": UNIT, "rtf": data_s / (tms * 1e-3), "dtype": "bf16 spectra, fp32 accumulate",
-                   "ms_per_step": tms / args.steps, "ratio_vs_fp32_form": tval / value,
-                   "kernel_ms_per_subint": {"prep": p2 / max(n2, 1), "fstage": f2 / max(n2, 1), "xmac": x2 / max(n2, 1)},
-                   "xmac_kernel": "k_xmac_tc (tcgen05.mma kind::f16, TMA)"}
+        other = {"xmac": other_name, "value": tval, "unit": UNIT, "rtf": data_s / (tms * 1e-3),
+                 "ms_per_step": tms / args.steps,
+                 "kernel_ms_per_subint": {"prep": p2 / max(n2, 1), "fstage": f2 / max(n2, 1), "xmac": x2 / max(n2, 1)}}
         ctc.close()
         barrier()
+    if other is not None:
+        tc_v, fp_v = (value, other["value"]) if args.xmac == "bf16" else (other["value"], value)
+        tc_vs_fp32 = tc_v / fp_v
+    else:
+        tc_vs_fp32 = None
 
-    # ---- roofline of the dominant kernel
+    # ---- rooflines: F stage against HBM (its design bound), XMAC against the
+    # tensor (bf16) or FP32 pipes
     hbm_peak, tf_peak, peak_src = load_peaks()
     T = job.blocks_per_send()
     rows = sum(st.nband for st in job.stations)
     in_bytes = sum(nbytes[k][s] for k in range(POOL) for s in range(S)) / POOL
-    spec_bytes = T * rows * job.freqs[0].nchan * 8
+    s_out = 4 if args.xmac == "bf16" else 8
+    spec_bytes = T * rows * job.freqs[0].nchan * s_out
     f_avg = f_ms / max(nrec, 1)
     x_avg = x_ms / max(nrec, 1)
-    if f_avg >= x_avg:
-        kname = "k_fstage2"
-        alg = in_bytes + spec_bytes
-        achieved = alg / (f_avg * 1e-3) / 1e9
-    else:
-        kname = "k_xmac_fp32v2"
-        alg = spec_bytes
-        achieved = alg / (x_avg * 1e-3) / 1e9
-    traffic = load_traffic(kname)
-    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": alg,
+    fname = "k_fstage"
+    alg = in_bytes + spec_bytes
+    achieved = alg / (f_avg * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": fname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": load_traffic(fname + ("_bf16" if args.xmac == "bf16" else "_fp32")),
+                "peak_source": peak_src, "algorithmic_bytes_per_launch": alg,
+                "note": "achieved = (packed VDIF bytes read + spectra bytes written) per subint / F-stage time",
                 "kernel_ms_per_subint": {"prep": prep_ms / max(nrec, 1), "fstage": f_avg, "xmac": x_avg}}
+    # useful XMAC flops: 8 per Hermitian-unique input pair, channel and FFT
+    useful = 0
+    for f in range(len(job.freqs)):
+        I = sum(1 for st in job.stations for fb, _ in st.bands if fb == f)
+        useful += 8 * (I * (I + 1) // 2) * job.freqs[f].nchan * T
+    xname = "k_xmac_tc" if args.xmac == "bf16" else "k_xmac_fp32v2"
+    xmac_roofline = {"bound": "tensor" if args.xmac == "bf16" else "fp32 pipe", "kernel": xname,
+                     "achieved": useful / (x_avg * 1e-3) / 1e12, "unit": "TFLOP/s",
+                     "peak": tf_peak if args.xmac == "bf16" else None,
+                     "frac": (useful / (x_avg * 1e-3) / 1e12 / tf_peak) if args.xmac == "bf16" else None,
+                     "useful_flops_per_subint": useful,
+                     "note": "useful flops only (8 per Hermitian-unique pair); the time includes the weights kernel"}
 
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
@@ -385,21 +405,24 @@ def gpu_arm(args, job):
         v, cores, sample, kind = cpu_reference(job, pool, args.cpu_seconds, os.cpu_count() or 1)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
-    # per subint: interpolators, frame validity, FFT parameters, F stage,
-    # one XMAC launch per group of equally shaped subbands, weights
+    # per subint: interpolators, frame validity, FFT parameters, one F-stage
+    # launch per FFT length, one XMAC launch per group of equally shaped
+    # subbands, weights
     shapes = {(sum(1 for st in job.stations for fb, _ in st.bands if fb == f), job.freqs[f].nchan)
               for f in range(len(job.freqs)) if any(fb == f for st in job.stations for fb, _ in st.bands)}
-    launches_per_subint = 5 + len(shapes)
+    flens = {2 * job.freqs[st.bands[0][0]].nchan for st in job.stations}
+    launches_per_subint = 3 + len(flens) + len(shapes) + 1
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"fp32": "f32", "bf16": "bf16", "fp8": "fp8e4m3"}[args.xmac],
+            "vs_baseline": None, "dtype": {"fp32": "f32", "bf16": "bf16"}[args.xmac],
             "data": "synthetic", "rtf": rtf, "xmac": args.xmac,
             "config": workload_config(job),
             "e2e": {"value": e2e_value, "unit": UNIT, "rtf": e2e_value / job.station_mhz_per_sec(),
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps},
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "tc_form": tc_form,
+            "roofline": roofline, "xmac_roofline": xmac_roofline, "cpu_baseline": cpu, "clocks": clk,
+            "other_form": other, "tc_vs_fp32": tc_vs_fp32,
             "gpu_launches": launches_per_subint * nsub * args.steps,
         }
         print(json.dumps(line), flush=True)
