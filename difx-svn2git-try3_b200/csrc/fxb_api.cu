@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -68,7 +69,8 @@ struct fxb_ctx {
 	// F-stage work items (by kind) and FP32 XMAC v2 launch groups
 	FGroup *d_groups = nullptr;
 	std::vector<FKind> fkinds;
-	void *d_specn = nullptr;             // bf16x2 spectra [t][row][chan] of the tensor-core form
+	void *d_specn = nullptr;             // bf16x2 spectra of the tensor-core form
+	void *d_tctab = nullptr;             // constant tables of the tensor-core FFT kernel
 	// XMAC launch groups (subbands of equal rows and channels); the
 	// tensor-core form also keeps each group's spectra in one block
 	struct XGroup {
@@ -436,6 +438,31 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			}
 			k.first = (int)hg.size();
 			k.count = (int)kv.second.size();
+			// tensor-core form at N = 2048: FXB_TC_FFT=1 runs the FFT on the
+			// tensor cores (fxb_fstage_tc.cu); the default is the CUDA-core FP16
+			// F stage, which is faster on the B200 today
+			if(out == 1)
+			{
+				bool any_lsb = false;
+				for(const FGroup &gg : kv.second)
+					any_lsb = any_lsb || gg.lsb;
+				const char *env = getenv("FXB_TC_FFT");
+				const bool allow = env && env[0] == '1';
+				if(allow && fstage_tc_eligible(k.N, job.fringe_rot_order, any_lsb))
+				{
+					if(!ctx->d_tctab)
+					{
+						std::vector<unsigned char> h(fstage_tc_tables_bytes());
+						make_fstage_tc_tables(h.data());
+						unsigned char *d = nullptr;
+						CK(ctx, dalloc(ctx, &d, h.size()));
+						CK(ctx, cudaMemcpy(d, h.data(), h.size(), cudaMemcpyHostToDevice));
+						ctx->d_tctab = d;
+					}
+					k.tcfft = 1;
+					k.tctab = ctx->d_tctab;
+				}
+			}
 			if(out == 1)
 			{
 				std::vector<uint2> h((size_t)k.twn);
@@ -697,8 +724,14 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 		fa.order = job.fringe_rot_order;
 		fa.fraclo = job.fractionallofreq ? 1 : 0;
 		fa.spec = ctx->tc ? ctx->d_specn : (void *)ctx->d_spec;
+		fa.err = ctx->d_err;
 		for(const FKind &k : ctx->fkinds)
-			launch_fstage_kind(k, fa, st);
+		{
+			if(k.tcfft)
+				launch_fstage_tc(k, fa, ctx->nsm, st);
+			else
+				launch_fstage_kind(k, fa, st);
+		}
 	}
 	CK(ctx, cudaEventRecord(ctx->ev_c, st));
 	if(tv) CK(ctx, cudaEventRecord(tv[2], st));

@@ -137,11 +137,11 @@ __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintS
 	p.stuck = 0;
 	p.weight = 0.0f;
 	p.fse = 0.0f;
-	p.lofrac_unused = 0.0f;
+	p.fmask = 0u;
 	p.averagedelay = 0.0;
 	p.a = p.b = p.c = 0.0;
 	p.integerdelay = 0;
-	p.pad = 0;
+	p.mflags = 0;
 
 	if(U.nbytes <= 1 || U.invalid_subint || !flag_valid(vf, i))
 	{
@@ -215,6 +215,20 @@ __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintS
 	p.status = kFftOk;
 	p.nearest = nearest;
 	p.stuck = stuck;
+	{
+		// frame-validity mask of the FFT window for the F stage
+		const int64_t fa = nearest / S.framesamples;
+		const int64_t nwf = (nearest - fa * S.framesamples + N - 1) / S.framesamples + 1;
+		uint32_t m = 0u;
+		for(int k = 0; k < 32 && k < nwf; k++)
+		{
+			const int64_t fr = fa + k;
+			if(fr < valid_stride && valid[(int64_t)s * valid_stride + fr])
+				m |= 1u << k;
+		}
+		p.fmask = m;
+		p.mflags = nwf <= 32 ? 1 : 0;
+	}
 	p.weight = weight;
 	p.fse = (float)(nr.starttime - nearest * S.sampletime);
 	p.averagedelay = nr.averagedelay;

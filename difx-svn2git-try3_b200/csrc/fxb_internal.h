@@ -30,11 +30,11 @@ struct FftParam {
 	int32_t stuck;        // samples [stuck, N) of the window decode to zero (8-bit 2/4-channel blanking)
 	float weight;         // Mode::getDataWeight
 	float fse;            // fractional sample error (us), float as in mode.cpp:772
-	float lofrac_unused;
+	uint32_t fmask;       // validity of the frames of the window [nearest, nearest + N): bit k = frame nearest/fs + k
 	double averagedelay;  // us
 	double a, b, c;       // fringe-rotation coefficients of the order in use
 	int32_t integerdelay;
-	int32_t pad;
+	int32_t mflags;       // 1: fmask covers every frame of the window (at most 32 frames)
 };
 
 // Station description on the device.

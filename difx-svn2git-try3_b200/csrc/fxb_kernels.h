@@ -72,9 +72,10 @@ struct FKind {
 	int32_t kb, fpc;         // radix-8 butterflies per thread and pass, FFTs side by side per CTA
 	int32_t threads, tq;     // CTA size, FFT iterations per CTA
 	int32_t pp, out;         // two exchange buffers (else one), output form (0 FP32, 1 FP16 FFT -> bf16x2)
-	int32_t twn, pad;        // twiddle entries of length N
+	int32_t twn, tcfft;      // twiddle entries of length N; 1: tensor-core FFT kernel (fxb_fstage_tc.cu)
 	size_t smem;
 	const void *tw;          // twiddle table of length N (make_fstage_twiddles layout)
+	const void *tctab;       // constant tables of the tensor-core FFT kernel
 };
 
 struct FsArgs {
@@ -89,10 +90,18 @@ struct FsArgs {
 	int32_t maxN, T, tq, order;
 	int32_t fraclo, pp, first, items_fast;
 	void *spec;              // [t][row][chan]: float2 (out 0) or bf16x2 (out 1)
+	int32_t *err;            // device error flag (bounded waits of the tensor-core FFT kernel)
 };
 
 bool fstage_plan(int N, int nb, int out, FKind *k);
 void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream);
+// F stage of the tensor-core form with the FFT on the tensor cores (N = 2048;
+// csrc/fxb_fstage_tc.cu)
+size_t fstage_tc_tables_bytes();
+void make_fstage_tc_tables(void *out);
+bool fstage_tc_eligible(int N, int order, bool any_lsb);
+void launch_fstage_tc(const FKind &k, FsArgs a, int nsm, cudaStream_t stream);
+
 // twiddles of FFT length N: float2 (out 0) or half2 pairs (wr, wr), (wi, wi)
 // (out 1), FKind::twn entries
 void make_fstage_twiddles(int N, float2 *out32, void *out16);

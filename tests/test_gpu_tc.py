@@ -72,3 +72,46 @@ def test_bf16_spectra_readback_matches_oracle():
         ref, _, _ = orc.mode_fft(0, buf, dsec, dns, sec, ns, t)
         for b in range(2):
             assert rel_err(spec[t, b], ref[b]) < 8e-3
+
+
+def _tc_fft_job(lsb=False, order=1):
+    # 1024 channels -> 2048-point FFTs: the F stage runs its FFT on the tensor cores
+    return small_job(nstation=3, nchan=1024, bw=32.0, nfreq=2, full_pol=True, subint_ns=2_048_000, lsb=lsb, order=order)
+
+
+@pytest.mark.parametrize("lsb,order", [(False, 1), (True, 1), (False, 0)])
+def test_tensor_core_fft_spectra_match_oracle(lsb, order, monkeypatch):
+    """Spectra of the tensor-core FFT (FXB_TC_FFT=1: FP16 operands, FP32
+    accumulation, BF16 out) against the FP64 oracle's Mode FFT output, both
+    sidebands."""
+    monkeypatch.setenv("FXB_TC_FFT", "1")
+    job = _tc_fft_job(lsb=lsb, order=order)
+    sec, ns = 0, 1_024_000
+    inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=11)
+    corr = Correlator(job, xmac="bf16")
+    corr.submit(inputs, sec, ns)
+    spec = corr.spectra(0)
+    corr.close()
+    orc = fxoracle.OracleCorrelator(job)
+    buf, dsec, dns = inputs[0]
+    for t in (0, 7, 31):
+        ref, _, _ = orc.mode_fft(0, buf, dsec, dns, sec, ns, t)
+        for b in range(2):
+            assert rel_err(spec[t, b], ref[b]) < 8e-3, (t, b)
+
+
+def test_tensor_core_fft_matches_cuda_core_fstage(monkeypatch):
+    """The same subints through the tensor-core FFT (FXB_TC_FFT=1) and through
+    the default CUDA-core FP16 F stage: both within the tensor-core tolerance
+    of the FP64 oracle and of each other."""
+    job = _tc_fft_job()
+    subints = [(0, 1_024_000), (0, 3_072_000)]
+    got_cc, ref, layout, n = run_tc(job, subints)
+    monkeypatch.setenv("FXB_TC_FFT", "1")
+    got_tc, _, _, _ = run_tc(job, subints)
+    for got in (got_tc, got_cc):
+        cross_err, auto_err = tc_errors(job, layout, n, got, ref)
+        assert cross_err <= TC_TOL, cross_err
+        assert auto_err <= TC_TOL, auto_err
+    reg = dict(regions(job, layout, n))
+    assert rel_err(got_tc[reg["auto"]], got_cc[reg["auto"]]) < 2e-3
