@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--subints-per-step", type=int, default=125)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (p50/p99 job latency)")
+    ap.add_argument("--serving-jobs", type=int, default=16)
     return ap.parse_args()
 
 
@@ -227,6 +229,32 @@ def load_peaks():
         return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
     except Exception:
         return 6650.0, 1590.0, "fallback"
+
+
+# ---------------------------------------------------------------- serving leg
+def serving_leg(args):
+    """p50/p99 job latency and sustained throughput of the serving loop on a
+    seeded Poisson stream of jobs of different shapes (a bounded sample of
+    the serving workload: the full job ranges -- up to 32 stations, 16
+    subbands of 64 MHz, 2 s -- would need tens of GB of host VDIF)."""
+    from fxb200 import serving
+    rng = np.random.default_rng(11)
+    jobs = []
+    for k in range(args.serving_jobs):
+        job, nsub = serving.serving_job(rng, seed=100 + k, stations=(4, 10), subbands=(1, 4), bws=(16.0, 32.0),
+                                        nchans=(256, 512, 1024, 2048), seconds=(0.05, 0.15))
+        jobs.append((job, serving.job_subints(job, nsub, seed=100 + k)))
+    rate = 40.0
+    arrivals = serving.poisson_arrivals(rng, len(jobs), rate)
+    srv = serving.Server(budget_bytes=48 << 30, max_active=4)
+    st = serving.run_stream(srv, jobs, arrivals, xmac=args.xmac)
+    srv.close()
+    smhz = sum(job.station_mhz_per_sec() * len(subs) * job.subint_ns * 1e-9 for job, subs in jobs)
+    return {"jobs": st["completed"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "rtf": st["rtf"], "station_mhz_per_s": smhz / st["wall_seconds"] if st["wall_seconds"] > 0 else None,
+            "arrival_rate_hz": rate, "max_active": 4, "xmac": args.xmac,
+            "sample": "%d seeded jobs, Poisson arrivals at %.0f/s; 4-10 stations, 1-4 subbands of 16-32 MHz, "
+                      "256-2048 channels, 0.05-0.15 s each, dual pol with cross hands" % (len(jobs), rate)}
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -405,6 +433,10 @@ def gpu_arm(args, job):
         v, cores, sample, kind = cpu_reference(job, pool, args.cpu_seconds, os.cpu_count() or 1)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        serve = serving_leg(args)
+
     # per subint: interpolators, frame validity, FFT parameters, one F-stage
     # launch per FFT length, one XMAC launch per group of equally shaped
     # subbands, weights
@@ -422,7 +454,7 @@ def gpu_arm(args, job):
             "e2e": {"value": e2e_value, "unit": UNIT, "rtf": e2e_value / job.station_mhz_per_sec(),
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps},
             "roofline": roofline, "xmac_roofline": xmac_roofline, "cpu_baseline": cpu, "clocks": clk,
-            "other_form": other, "tc_vs_fp32": tc_vs_fp32,
+            "other_form": other, "tc_vs_fp32": tc_vs_fp32, "serving": serve,
             "gpu_launches": launches_per_subint * nsub * args.steps,
         }
         print(json.dumps(line), flush=True)

@@ -832,6 +832,40 @@ fxb_status fxb_job_layout(const fxb_job_desc *desc, int32_t *out, size_t nint, i
 	return FXB_OK;
 }
 
+fxb_status fxb_job_footprint(const fxb_job_desc *desc, size_t *bytes)
+{
+	if(!desc || !bytes)
+		return FXB_ERR_ARG;
+	Job job;
+	std::string err;
+	fxb_status st = FXB_OK;
+	if(!build_job(desc, job, err, st))
+	{
+		std::lock_guard<std::mutex> lk(g_err_mutex);
+		g_create_err = err;
+		return st;
+	}
+	const int64_t T = job.blockspersend;
+	const int S = (int)job.stations.size();
+	// spectra (the blocked tensor-core layout pads times to 32 and channels to
+	// whole blocks: at most +25 %), accumulators, core result, FFT parameters
+	double b = (double)job.spec_total * (job.xmac_kind == FXB_XMAC_FP32 ? 8.0 : 4.0 * 1.25);
+	b += (double)job.acc_total * 8.0 + (double)job.corelen * 16.0 + (double)S * T * 64.0;
+	// raw VDIF staging of the in-flight subints (payload plus headers, 1/8 slack)
+	for(int s = 0; s < S; s++)
+	{
+		const Job::Station &js = job.stations[s];
+		const fxb_freq &f = job.freqs[js.band_freq[0]];
+		const double sps = 2.0 * f.bw_mhz * 1e6;
+		const double per = (double)job.subint_ns * 1e-9 * sps * js.nbits * js.nband / 8.0 *
+		                   (double)(js.payload + js.header) / js.payload;
+		b += job.inflight * (per * 1.125 + 2.0 * (js.payload + js.header) + 4096.0);
+	}
+	b += 16.0 * 1024 * 1024;           // plans, tables, validity bytes, alignment
+	*bytes = (size_t)b;
+	return FXB_OK;
+}
+
 fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats)
 {
 	if(!ctx || !coreresult) return FXB_ERR_ARG;

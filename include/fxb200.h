@@ -232,6 +232,59 @@ FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, int32_t nfr
                                               int32_t sec, int32_t ns, float *dev_spectra, float *dev_weights,
                                               void *stream);
 
+/* ------------------------------------------------------------------ serving
+ * A request loop that takes correlation jobs of different shapes as they
+ * arrive (the boundary's fxb_server_* calls; no counterpart in mpifxcorr,
+ * whose FxManager schedules one configuration at a time, fxmanager.cpp:
+ * 334-337).  Each admitted job gets its own context (device state and
+ * accumulators resident until it completes) and stream; the server's worker
+ * thread submits the subints of every admitted job in turn, so the work of
+ * jobs that arrive while others run overlaps on the device.  Jobs are
+ * admitted in arrival order while their device footprint fits the HBM budget
+ * and fewer than max_active run. */
+typedef struct fxb_server fxb_server;
+
+typedef struct {
+	const fxb_job_desc *desc;
+	/* delay model of each station, as for fxb_set_delay_poly */
+	const int32_t *poly_npoly;       /* [nstation] */
+	const int32_t *poly_order;       /* [nstation] */
+	const double *poly0_sec;         /* [nstation] */
+	const int32_t *poly_interval;    /* [nstation] */
+	const double *const *poly_coeffs;/* [nstation] */
+	int32_t nsubint;
+	const uint8_t *const *bufs;      /* [nsubint * nstation] host VDIF of each subint and station */
+	const int64_t *nbytes;           /* [nsubint * nstation] */
+	const int32_t *datasec, *datans; /* [nsubint * nstation] first-sample times */
+	const int32_t *subsec, *subns;   /* [nsubint] subint start times */
+	float *coreresult;               /* out: 2 * corelen floats, written when the job completes */
+} fxb_job_request;
+
+/* Device footprint of a job (bytes) as used by admission. */
+FXB_API fxb_status fxb_job_footprint(const fxb_job_desc *desc, size_t *bytes);
+
+/* Start a server on `device` with an HBM budget (bytes) for the admitted
+ * jobs and at most max_active jobs on the device at once. */
+FXB_API fxb_server *fxb_server_create(int32_t device, size_t hbm_budget_bytes, int32_t max_active,
+                                      fxb_status *status);
+/* Queue a job.  Every array of the request (and the job description) is
+ * borrowed until the job has completed; returns its id. */
+FXB_API fxb_status fxb_server_submit(fxb_server *srv, const fxb_job_request *req, uint64_t *job_id);
+/* state: 0 queued, 1 running, 2 done, 3 failed; latency_ms = submit to
+ * completion (done jobs). */
+FXB_API fxb_status fxb_server_poll(fxb_server *srv, uint64_t job_id, int32_t *state, double *latency_ms);
+/* Block until the job is done or failed, or timeout_s passes
+ * (FXB_ERR_TIMEOUT). */
+FXB_API fxb_status fxb_server_wait(fxb_server *srv, uint64_t job_id, double timeout_s);
+/* Completed jobs, p50 / p99 latency (ms), data seconds correlated, and wall
+ * seconds from the first submit to the last completion. */
+FXB_API fxb_status fxb_server_stats(fxb_server *srv, int32_t *ncompleted, double *p50_ms, double *p99_ms,
+                                    double *data_seconds, double *wall_seconds);
+/* Text of the server's last error (e.g. of a failed job). */
+FXB_API const char *fxb_server_last_error(const fxb_server *srv);
+/* Finish the running jobs, fail the queued ones, stop the worker. */
+FXB_API void fxb_server_destroy(fxb_server *srv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,79 @@
+"""Serving loop on the GPU (fxb_server_* through the C ABI): jobs of
+different shapes submitted while others run give the same core result as
+each job run alone, admission against a small HBM budget still completes
+every job, and a served job matches the FP64 oracle."""
+import numpy as np
+import pytest
+
+from fxb200 import serving
+from fxb200.native import Correlator
+from helpers import small_job
+from test_gpu_tc import TC_TOL, tc_errors
+
+import fxoracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _jobs():
+    # three shapes: stations, subbands, channels and bits differ
+    specs = [dict(nstation=3, nchan=256, bw=16.0, nfreq=2, full_pol=True, seed=2),
+             dict(nstation=4, nchan=1024, bw=32.0, nfreq=1, full_pol=True, subint_ns=2_048_000, seed=3),
+             dict(nstation=2, nchan=128, bw=8.0, nfreq=2, full_pol=True, nbits=8, subint_ns=2_048_000, seed=4)]
+    out = []
+    for k, kw in enumerate(specs):
+        job = small_job(**kw)
+        out.append((job, serving.job_subints(job, 3, seed=20 + k, rho=0.05)))
+    return out
+
+
+def _alone(job, subints, xmac):
+    c = Correlator(job, xmac=xmac)
+    for inputs, sec, ns in subints:
+        c.submit(inputs, sec, ns)
+    r = c.results()
+    c.close()
+    return r
+
+
+@pytest.mark.parametrize("xmac", ["bf16", "fp32"])
+def test_results_same_alone_and_in_the_mix(xmac):
+    jobs = _jobs()
+    alone = [_alone(j, s, xmac) for j, s in jobs]
+    srv = serving.Server(budget_bytes=8 << 30, max_active=3)
+    handles = [srv.submit(j, s, xmac=xmac) for j, s in jobs]
+    for h, ref in zip(handles, alone):
+        got = srv.wait(h, 120.0)
+        assert np.array_equal(got, ref)
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == 3 and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_admission_under_a_small_budget_completes_every_job():
+    jobs = _jobs()
+    need = max(serving.job_footprint(j) for j, _ in jobs)
+    srv = serving.Server(budget_bytes=need, max_active=3)     # one job at a time fits
+    handles = [srv.submit(j, s) for j, s in jobs]
+    for h in handles:
+        srv.wait(h, 120.0)
+        assert srv.poll(h)[0] == 2
+    assert srv.stats()["completed"] == 3
+    srv.close()
+
+
+def test_served_job_matches_oracle():
+    job, subints = _jobs()[1]
+    srv = serving.Server(budget_bytes=4 << 30, max_active=2)
+    h = srv.submit(job, subints)
+    got = srv.wait(h, 120.0)
+    srv.close()
+    orc = fxoracle.OracleCorrelator(job)
+    ref = None
+    for inputs, sec, ns in subints:
+        ref = orc.process_subint(inputs, sec, ns, coreresult=ref)
+    c = Correlator(job, xmac="bf16")
+    layout, n = c.layout(), c.corelen
+    c.close()
+    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
+    assert cross_err <= TC_TOL and auto_err <= TC_TOL
