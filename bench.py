@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (p50/p99 job latency)")
-    ap.add_argument("--serving-jobs", type=int, default=16)
+    ap.add_argument("--serving-jobs", type=int, default=32)
     return ap.parse_args()
 
 
@@ -243,18 +243,21 @@ def serving_leg(args):
     for k in range(args.serving_jobs):
         job, nsub = serving.serving_job(rng, seed=100 + k, stations=(4, 10), subbands=(1, 4), bws=(16.0, 32.0),
                                         nchans=(256, 512, 1024, 2048), seconds=(0.05, 0.15))
-        jobs.append((job, serving.job_subints(job, nsub, seed=100 + k)))
+        jobs.append((job, serving.job_subints(job, nsub, seed=100 + k, pinned=True)))
     rate = 40.0
     arrivals = serving.poisson_arrivals(rng, len(jobs), rate)
     srv = serving.Server(budget_bytes=48 << 30, max_active=4)
     st = serving.run_stream(srv, jobs, arrivals, xmac=args.xmac)
+    phases = [srv.job_times(h) for h in srv.jobs]
     srv.close()
+    phase_p50 = {k: float(np.median([p[k] for p in phases])) for k in phases[0]} if phases else {}
     smhz = sum(job.station_mhz_per_sec() * len(subs) * job.subint_ns * 1e-9 for job, subs in jobs)
     return {"jobs": st["completed"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "rtf": st["rtf"], "station_mhz_per_s": smhz / st["wall_seconds"] if st["wall_seconds"] > 0 else None,
-            "arrival_rate_hz": rate, "max_active": 4, "xmac": args.xmac,
+            "arrival_rate_hz": rate, "max_active": 4, "xmac": args.xmac, "phase_ms_p50": phase_p50,
             "sample": "%d seeded jobs, Poisson arrivals at %.0f/s; 4-10 stations, 1-4 subbands of 16-32 MHz, "
-                      "256-2048 channels, 0.05-0.15 s each, dual pol with cross hands" % (len(jobs), rate)}
+                      "256-2048 channels, 0.05-0.15 s each, dual pol with cross hands; station buffers in "
+                      "page-locked host memory; latency = submit to core result in host memory" % (len(jobs), rate)}
 
 
 # ---------------------------------------------------------------- GPU arm

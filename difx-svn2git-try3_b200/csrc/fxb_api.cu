@@ -27,8 +27,10 @@ struct Slot {
 	std::vector<int64_t> rawcap;
 	DevSubintStation *d_sub = nullptr;
 	int32_t *d_vflags = nullptr;
-	DevSubintStation *h_sub = nullptr; // pinned
-	int32_t *h_vflags = nullptr;       // pinned
+	// host side of d_sub / d_vflags: pageable, the driver stages each copy
+	// before cudaMemcpyAsync returns
+	DevSubintStation *h_sub = nullptr;
+	int32_t *h_vflags = nullptr;
 	cudaEvent_t copied = nullptr, done = nullptr;
 	bool used = false;
 };
@@ -38,6 +40,10 @@ struct fxb_ctx {
 	std::string err;
 	int device = 0;
 	cudaStream_t stream = nullptr, copy_stream = nullptr;
+	// device memory comes from this pool (a server's, whose memory stays
+	// mapped between jobs) or, when null, the device's default pool; every
+	// allocation and free is stream-ordered, so none synchronises the device
+	cudaMemPool_t pool = nullptr;
 	int S = 0, T = 0, F = 0, nflagint = 0, maxband = 0, maxN = 0, maxfft = 0;
 	DevStation *d_st = nullptr;
 	std::vector<DevStation> h_st;
@@ -112,11 +118,17 @@ static fxb_status cuda_fail(fxb_ctx *ctx, cudaError_t e, const char *what)
 			return cuda_fail((ctx), e_, #call);        \
 	} while(0)
 
+static cudaError_t pool_alloc(fxb_ctx *ctx, void **p, size_t bytes, cudaStream_t s)
+{
+	bytes = std::max<size_t>(bytes, 1);
+	return ctx->pool ? cudaMallocFromPoolAsync(p, bytes, ctx->pool, s) : cudaMallocAsync(p, bytes, s);
+}
+
 template <typename T>
 static cudaError_t dalloc(fxb_ctx *ctx, T **p, size_t n)
 {
 	void *v = nullptr;
-	cudaError_t e = cudaMalloc(&v, std::max<size_t>(n, 1) * sizeof(T));
+	cudaError_t e = pool_alloc(ctx, &v, n * sizeof(T), ctx->stream);
 	if(e == cudaSuccess)
 	{
 		ctx->owned.push_back(v);
@@ -133,16 +145,21 @@ static void free_ctx(fxb_ctx *ctx)
 		cudaStreamSynchronize(ctx->stream);
 	if(ctx->copy_stream)
 		cudaStreamSynchronize(ctx->copy_stream);
+	// every stream is idle: the frees, ordered on the compute stream, return
+	// the memory to its pool
 	for(void *p : ctx->owned)
-		cudaFree(p);
+		cudaFreeAsync(p, ctx->stream);
 	if(ctx->d_valid)
-		cudaFree(ctx->d_valid);
+		cudaFreeAsync(ctx->d_valid, ctx->stream);
+	for(auto &s : ctx->slots)
+		for(auto *p : s.raw)
+			if(p) cudaFreeAsync(p, ctx->stream);
+	if(ctx->stream)
+		cudaStreamSynchronize(ctx->stream);
 	for(auto &s : ctx->slots)
 	{
-		for(auto *p : s.raw)
-			if(p) cudaFree(p);
-		if(s.h_sub) cudaFreeHost(s.h_sub);
-		if(s.h_vflags) cudaFreeHost(s.h_vflags);
+		std::free(s.h_sub);
+		std::free(s.h_vflags);
 		if(s.copied) cudaEventDestroy(s.copied);
 		if(s.done) cudaEventDestroy(s.done);
 	}
@@ -207,7 +224,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 	}
 	ctx->maxfft = ctx->maxN;
 	CK(ctx, dalloc(ctx, &ctx->d_st, ctx->S));
-	CK(ctx, cudaMemcpy(ctx->d_st, ctx->h_st.data(), sizeof(DevStation) * ctx->S, cudaMemcpyHostToDevice));
+	CK(ctx, cudaMemcpyAsync(ctx->d_st, ctx->h_st.data(), sizeof(DevStation) * ctx->S, cudaMemcpyHostToDevice, ctx->stream));
 
 	// bands
 	std::vector<DevBand> hb((size_t)ctx->S * ctx->maxband);
@@ -225,7 +242,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			d.lofreq = job.freqs[f].freq_mhz;
 		}
 	CK(ctx, dalloc(ctx, &ctx->d_bands, hb.size()));
-	CK(ctx, cudaMemcpy(ctx->d_bands, hb.data(), sizeof(DevBand) * hb.size(), cudaMemcpyHostToDevice));
+	CK(ctx, cudaMemcpyAsync(ctx->d_bands, hb.data(), sizeof(DevBand) * hb.size(), cudaMemcpyHostToDevice, ctx->stream));
 
 	// twiddles exp(-2 pi i k / maxN), computed in double
 	{
@@ -236,7 +253,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			tw[k] = make_float2((float)cos(ang), (float)sin(ang));
 		}
 		CK(ctx, dalloc(ctx, &ctx->d_twiddle, tw.size()));
-		CK(ctx, cudaMemcpy(ctx->d_twiddle, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
+		CK(ctx, cudaMemcpyAsync(ctx->d_twiddle, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice, ctx->stream));
 	}
 
 	// per-frequency plans
@@ -259,8 +276,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		int16_t *pairs;
 		CK(ctx, dalloc(ctx, &dA, p.destA.size()));
 		CK(ctx, dalloc(ctx, &dB, p.destB.size()));
-		CK(ctx, cudaMemcpy(dA, p.destA.data(), sizeof(int32_t) * p.destA.size(), cudaMemcpyHostToDevice));
-		CK(ctx, cudaMemcpy(dB, p.destB.data(), sizeof(int32_t) * p.destB.size(), cudaMemcpyHostToDevice));
+		CK(ctx, cudaMemcpyAsync(dA, p.destA.data(), sizeof(int32_t) * p.destA.size(), cudaMemcpyHostToDevice, ctx->stream));
+		CK(ctx, cudaMemcpyAsync(dB, p.destB.data(), sizeof(int32_t) * p.destB.size(), cudaMemcpyHostToDevice, ctx->stream));
 		std::vector<int16_t> hp;
 		for(int i = 0; i < d.ntr; i++)
 			for(int j = i; j < d.ntr; j++)
@@ -269,7 +286,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				hp.push_back((int16_t)j);
 			}
 		CK(ctx, dalloc(ctx, &pairs, hp.size()));
-		CK(ctx, cudaMemcpy(pairs, hp.data(), sizeof(int16_t) * hp.size(), cudaMemcpyHostToDevice));
+		CK(ctx, cudaMemcpyAsync(pairs, hp.data(), sizeof(int16_t) * hp.size(), cudaMemcpyHostToDevice, ctx->stream));
 		d.destA = dA;
 		d.destB = dB;
 		d.pairs = pairs;
@@ -285,7 +302,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				}
 			int32_t *ds = nullptr;
 			CK(ctx, dalloc(ctx, &ds, src.size()));
-			CK(ctx, cudaMemcpy(ds, src.data(), sizeof(int32_t) * src.size(), cudaMemcpyHostToDevice));
+			CK(ctx, cudaMemcpyAsync(ds, src.data(), sizeof(int32_t) * src.size(), cudaMemcpyHostToDevice, ctx->stream));
 			d.outsrc = ds;
 		}
 	}
@@ -354,21 +371,21 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		ctx->specn_elems = off;
 	}
 	CK(ctx, dalloc(ctx, &ctx->d_plans, ctx->F));
-	CK(ctx, cudaMemcpy(ctx->d_plans, ctx->h_plans.data(), sizeof(DevFreqPlan) * ctx->F, cudaMemcpyHostToDevice));
+	CK(ctx, cudaMemcpyAsync(ctx->d_plans, ctx->h_plans.data(), sizeof(DevFreqPlan) * ctx->F, cudaMemcpyHostToDevice, ctx->stream));
 	for(size_t gi = 0; gi < ctx->xgroups.size(); gi++)
 	{
 		fxb_ctx::XGroup &g = ctx->xgroups[gi];
 		CK(ctx, dalloc(ctx, &g.d_idx, gidx[gi].size()));
-		CK(ctx, cudaMemcpy(g.d_idx, gidx[gi].data(), sizeof(int32_t) * gidx[gi].size(), cudaMemcpyHostToDevice));
+		CK(ctx, cudaMemcpyAsync(g.d_idx, gidx[gi].data(), sizeof(int32_t) * gidx[gi].size(), cudaMemcpyHostToDevice, ctx->stream));
 	}
 	if(ctx->tc)
 	{
 		uint32_t *sn = nullptr;
 		CK(ctx, dalloc(ctx, &sn, (size_t)ctx->specn_elems));
-		CK(ctx, cudaMemset(sn, 0, sizeof(uint32_t) * (size_t)ctx->specn_elems));
+		CK(ctx, cudaMemsetAsync(sn, 0, sizeof(uint32_t) * (size_t)ctx->specn_elems, ctx->stream));
 		ctx->d_specn = sn;
 		CK(ctx, dalloc(ctx, &ctx->d_err, 1));
-		CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
+		CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int32_t), ctx->stream));
 		CK(ctx, cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device));
 		for(fxb_ctx::XGroup &g : ctx->xgroups)
 			if(tc_tensormap_size() > sizeof(g.tmap) || !tc_make_tensormap(g.tmap, sn + g.spec_base, g.shape, g.nf))
@@ -456,7 +473,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 						make_fstage_tc_tables(h.data());
 						unsigned char *d = nullptr;
 						CK(ctx, dalloc(ctx, &d, h.size()));
-						CK(ctx, cudaMemcpy(d, h.data(), h.size(), cudaMemcpyHostToDevice));
+						CK(ctx, cudaMemcpyAsync(d, h.data(), h.size(), cudaMemcpyHostToDevice, ctx->stream));
 						ctx->d_tctab = d;
 					}
 					k.tcfft = 1;
@@ -469,7 +486,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				make_fstage_twiddles(k.N, nullptr, h.data());
 				uint2 *d = nullptr;
 				CK(ctx, dalloc(ctx, &d, h.size()));
-				CK(ctx, cudaMemcpy(d, h.data(), sizeof(uint2) * h.size(), cudaMemcpyHostToDevice));
+				CK(ctx, cudaMemcpyAsync(d, h.data(), sizeof(uint2) * h.size(), cudaMemcpyHostToDevice, ctx->stream));
 				k.tw = d;
 			}
 			else
@@ -478,7 +495,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				make_fstage_twiddles(k.N, h.data(), nullptr);
 				float2 *d = nullptr;
 				CK(ctx, dalloc(ctx, &d, h.size()));
-				CK(ctx, cudaMemcpy(d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
+				CK(ctx, cudaMemcpyAsync(d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice, ctx->stream));
 				k.tw = d;
 			}
 			hg.insert(hg.end(), kv.second.begin(), kv.second.end());
@@ -486,7 +503,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		}
 		CK(ctx, dalloc(ctx, &ctx->d_groups, std::max<size_t>(hg.size(), 1)));
 		if(!hg.empty())
-			CK(ctx, cudaMemcpy(ctx->d_groups, hg.data(), sizeof(FGroup) * hg.size(), cudaMemcpyHostToDevice));
+			CK(ctx, cudaMemcpyAsync(ctx->d_groups, hg.data(), sizeof(FGroup) * hg.size(), cudaMemcpyHostToDevice, ctx->stream));
 	}
 	// big buffers
 	CK(ctx, dalloc(ctx, &ctx->d_params, (size_t)ctx->S * ctx->T));
@@ -521,9 +538,9 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		CK(ctx, dalloc(ctx, &ctx->d_bw, ctx->nbw));
 		CK(ctx, dalloc(ctx, &ctx->d_acw, ctx->nacw));
 		CK(ctx, dalloc(ctx, &ctx->d_om, ctx->nom));
-		if(ctx->nbw) CK(ctx, cudaMemcpy(ctx->d_bw, hbw.data(), sizeof(DevBWeight) * ctx->nbw, cudaMemcpyHostToDevice));
-		if(ctx->nacw) CK(ctx, cudaMemcpy(ctx->d_acw, hacw.data(), sizeof(DevACWeight) * ctx->nacw, cudaMemcpyHostToDevice));
-		if(ctx->nom) CK(ctx, cudaMemcpy(ctx->d_om, hom.data(), sizeof(DevOutMap) * ctx->nom, cudaMemcpyHostToDevice));
+		if(ctx->nbw) CK(ctx, cudaMemcpyAsync(ctx->d_bw, hbw.data(), sizeof(DevBWeight) * ctx->nbw, cudaMemcpyHostToDevice, ctx->stream));
+		if(ctx->nacw) CK(ctx, cudaMemcpyAsync(ctx->d_acw, hacw.data(), sizeof(DevACWeight) * ctx->nacw, cudaMemcpyHostToDevice, ctx->stream));
+		if(ctx->nom) CK(ctx, cudaMemcpyAsync(ctx->d_om, hom.data(), sizeof(DevOutMap) * ctx->nom, cudaMemcpyHostToDevice, ctx->stream));
 	}
 
 	// staging slots
@@ -534,8 +551,13 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		sl.rawcap.assign(ctx->S, 0);
 		CK(ctx, dalloc(ctx, &sl.d_sub, ctx->S));
 		CK(ctx, dalloc(ctx, &sl.d_vflags, (size_t)ctx->S * ctx->nflagint));
-		CK(ctx, cudaMallocHost(&sl.h_sub, sizeof(DevSubintStation) * ctx->S));
-		CK(ctx, cudaMallocHost(&sl.h_vflags, sizeof(int32_t) * ctx->S * ctx->nflagint));
+		sl.h_sub = (DevSubintStation *)std::calloc(ctx->S, sizeof(DevSubintStation));
+		sl.h_vflags = (int32_t *)std::calloc((size_t)ctx->S * ctx->nflagint, sizeof(int32_t));
+		if(!sl.h_sub || !sl.h_vflags)
+		{
+			ctx->err = "host allocation failed";
+			return FXB_ERR_NOMEM;
+		}
 		CK(ctx, cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));
 		CK(ctx, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
 	}
@@ -547,11 +569,12 @@ static fxb_status setup_device(fxb_ctx *ctx)
 	return FXB_OK;
 }
 
-extern "C" {
+namespace fxb {
 
-fxb_ctx *fxb_create(const fxb_job_desc *desc, fxb_status *status)
+fxb_ctx *create_ctx(const fxb_job_desc *desc, void *pool, fxb_status *status)
 {
 	fxb_ctx *ctx = new fxb_ctx;
+	ctx->pool = (cudaMemPool_t)pool;
 	fxb_status st = FXB_OK;
 	std::string err;
 	if(!build_job(desc, ctx->job, err, st))
@@ -578,6 +601,18 @@ fxb_ctx *fxb_create(const fxb_job_desc *desc, fxb_status *status)
 	if(status) *status = FXB_OK;
 	return ctx;
 }
+
+bool ctx_slot_free(fxb_ctx *ctx)
+{
+	const auto &sl = ctx->slots[ctx->next_slot];
+	return !sl.used || cudaEventQuery(sl.done) != cudaErrorNotReady;
+}
+
+}  // namespace fxb
+
+extern "C" {
+
+fxb_ctx *fxb_create(const fxb_job_desc *desc, fxb_status *status) { return fxb::create_ctx(desc, nullptr, status); }
 
 void fxb_destroy(fxb_ctx *ctx) { free_ctx(ctx); }
 
@@ -607,7 +642,7 @@ fxb_status fxb_set_delay_poly(fxb_ctx *ctx, int32_t station, int32_t npoly, int3
 	d.poly0 = poly0_sec;
 	memset(d.coeffs, 0, sizeof(d.coeffs));
 	memcpy(d.coeffs, coeffs, sizeof(double) * npoly * (order + 1));
-	CK(ctx, cudaMemcpy(ctx->d_st + station, &d, sizeof(DevStation), cudaMemcpyHostToDevice));
+	CK(ctx, cudaMemcpyAsync(ctx->d_st + station, &d, sizeof(DevStation), cudaMemcpyHostToDevice, ctx->stream));
 	ctx->delay_set[station] = true;
 	return FXB_OK;
 }
@@ -643,13 +678,13 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 	}
 	if(need > ctx->valid_stride)
 	{
-		CK(ctx, cudaStreamSynchronize(ctx->stream));
+		// stream-ordered: the earlier subints' kernels finish with the old array first
 		if(ctx->d_valid)
 		{
-			cudaFree(ctx->d_valid);
+			CK(ctx, cudaFreeAsync(ctx->d_valid, ctx->stream));
 			ctx->d_valid = nullptr;
 		}
-		CK(ctx, cudaMalloc(&ctx->d_valid, (size_t)need * ctx->S));
+		CK(ctx, pool_alloc(ctx, (void **)&ctx->d_valid, (size_t)need * ctx->S, ctx->stream));
 		ctx->valid_stride = need;
 	}
 
@@ -666,10 +701,13 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 		{
 			if(sl.rawcap[s] < nbytes[s])
 			{
-				if(sl.raw[s]) cudaFree(sl.raw[s]);
+				// the slot is idle (its done event has completed), so the old
+				// buffer can go back at once; the new one is ordered on the
+				// copy stream ahead of the copy into it
+				if(sl.raw[s]) CK(ctx, cudaFreeAsync(sl.raw[s], ctx->copy_stream));
 				sl.raw[s] = nullptr;
 				int64_t cap = nbytes[s] + nbytes[s] / 8 + 4096;
-				CK(ctx, cudaMalloc(&sl.raw[s], cap));
+				CK(ctx, pool_alloc(ctx, (void **)&sl.raw[s], cap, ctx->copy_stream));
 				sl.rawcap[s] = cap;
 			}
 			u.buf = sl.raw[s];
@@ -943,6 +981,20 @@ fxb_status fxb_get_stream(const fxb_ctx *ctx, void **stream)
 	if(!ctx || !stream) return FXB_ERR_ARG;
 	*stream = (void *)ctx->stream;
 	return FXB_OK;
+}
+
+void *fxb_host_alloc(size_t bytes, fxb_status *status)
+{
+	void *p = nullptr;
+	const cudaError_t e = cudaHostAlloc(&p, std::max<size_t>(bytes, 1), cudaHostAllocPortable);
+	if(status) *status = e == cudaSuccess ? FXB_OK : e == cudaErrorMemoryAllocation ? FXB_ERR_NOMEM : FXB_ERR_CUDA;
+	return e == cudaSuccess ? p : nullptr;
+}
+
+void fxb_host_free(void *p)
+{
+	if(p)
+		cudaFreeHost(p);
 }
 
 fxb_status fxb_read_results_device(fxb_ctx *ctx, float *dev_out, size_t nfloats)

@@ -139,6 +139,17 @@ struct Job {
 };
 
 bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st);
+
+// fxb_create with the context's device memory taken from a cudaMemPool_t
+// (passed as void*; null: the device's default pool).  A server's pool keeps
+// its memory mapped between jobs, so that creating and destroying contexts
+// makes no allocation calls into the driver once the pool has grown.
+fxb_ctx *create_ctx(const fxb_job_desc *desc, void *pool, fxb_status *status);
+
+// Whether the context's next subint slot is free, i.e. whether a submit would
+// start at once rather than wait for an earlier subint to finish (an error
+// of the slot's event also reads as free, so that the submit reports it).
+bool ctx_slot_free(fxb_ctx *ctx);
 int calcstridelength(unsigned int arraylength);
 
 }  // namespace fxb

@@ -144,6 +144,9 @@ def lib():
     L.fxb_timing_read.argtypes = [vp, i32p, dp, dp, dp]
     L.fxb_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
     L.fxb_read_results_device.argtypes = [vp, ctypes.c_void_p, ctypes.c_size_t]
+    L.fxb_host_alloc.restype = vp
+    L.fxb_host_alloc.argtypes = [ctypes.c_size_t, i32p]
+    L.fxb_host_free.argtypes = [vp]
     for name in ("fxb_set_delay_poly", "fxb_submit_subint", "fxb_submit_subint_device", "fxb_sync",
                  "fxb_core_result_length", "fxb_layout", "fxb_read_results", "fxb_reset", "fxb_last_timing",
                  "fxb_read_spectra", "fxb_read_fft_weights", "fxb_vdif_unpack", "fxb_job_layout",
@@ -151,6 +154,37 @@ def lib():
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
+
+
+class _PinnedBlock:
+    """A page-locked host allocation (fxb_host_alloc), freed with its last view."""
+
+    def __init__(self, nbytes: int):
+        st = ctypes.c_int32(0)
+        self.ptr = lib().fxb_host_alloc(max(nbytes, 1), ctypes.byref(st))
+        if not self.ptr:
+            raise FxbError("fxb_host_alloc(%d) failed: %s" % (nbytes, FXB_STATUS.get(st.value, st.value)))
+        self.nbytes = nbytes
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().fxb_host_free(self.ptr)
+            self.ptr = None
+
+
+class PinnedArray(np.ndarray):
+    """ndarray over page-locked host memory; views keep the block alive."""
+    _block = None
+
+
+def pinned_empty(nbytes: int) -> PinnedArray:
+    """nbytes of page-locked host memory as a uint8 array (station buffers in
+    this memory are copied to the device asynchronously)."""
+    blk = _PinnedBlock(nbytes)
+    raw = (ctypes.c_uint8 * max(nbytes, 1)).from_address(blk.ptr)
+    a = np.frombuffer(raw, dtype=np.uint8, count=nbytes).view(PinnedArray)
+    a._block = blk
+    return a
 
 
 def check(rc: int, ctx=None, what: str = "") -> None:

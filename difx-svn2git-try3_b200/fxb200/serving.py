@@ -18,7 +18,7 @@ import numpy as np
 
 from . import synth
 from .job import Freq, Job, full_job
-from .native import DescHolder, FxbError, FxbJobDesc, FXB_STATUS, lib, poly_arrays
+from .native import DescHolder, FxbError, FxbJobDesc, FXB_STATUS, lib, pinned_empty, poly_arrays
 
 _c = ctypes
 
@@ -49,10 +49,12 @@ def _bind():
     L.fxb_server_poll.argtypes = [vp, _c.c_uint64, _c.POINTER(i32), dp]
     L.fxb_server_wait.argtypes = [vp, _c.c_uint64, _c.c_double]
     L.fxb_server_stats.argtypes = [vp, _c.POINTER(i32), dp, dp, dp, dp]
+    L.fxb_server_job_times.argtypes = [vp, _c.c_uint64, dp]
     L.fxb_server_last_error.restype = _c.c_char_p
     L.fxb_server_last_error.argtypes = [vp]
     L.fxb_server_destroy.argtypes = [vp]
-    for name in ("fxb_job_footprint", "fxb_server_submit", "fxb_server_poll", "fxb_server_wait", "fxb_server_stats"):
+    for name in ("fxb_job_footprint", "fxb_server_submit", "fxb_server_poll", "fxb_server_wait", "fxb_server_stats",
+                 "fxb_server_job_times"):
         getattr(L, name).restype = _c.c_int
     _bound = True
     return L
@@ -141,6 +143,12 @@ class Server:
         self._check(_bind().fxb_server_wait(self.srv, sj.id, timeout_s), "server_wait")
         return sj.result
 
+    def job_times(self, sj: ServedJob) -> dict:
+        """Phases of a done job's latency (ms)."""
+        out = (_c.c_double * 5)()
+        self._check(_bind().fxb_server_job_times(self.srv, sj.id, out), "server_job_times")
+        return dict(zip(("queued", "create", "submit", "drain", "release"), list(out)))
+
     def stats(self) -> dict:
         n = _c.c_int32(0)
         p50, p99, ds, ws = _c.c_double(0), _c.c_double(0), _c.c_double(0), _c.c_double(0)
@@ -190,10 +198,11 @@ def serving_job(rng: np.random.Generator, seed: int, stations=(4, 32), subbands=
     return job, nsub
 
 
-def job_subints(job: Job, nsub: int, seed: int, rho: float = 0.0) -> List[Tuple[list, int, int]]:
+def job_subints(job: Job, nsub: int, seed: int, rho: float = 0.0, pinned: bool = False) -> List[Tuple[list, int, int]]:
     """Host VDIF of nsub consecutive subints (starting one subint in): the bulk
     code-statistics generator for rho = 0, the correlated sky + noise model
-    otherwise."""
+    otherwise.  pinned=True places every buffer in one page-locked block, as
+    a datastream's receive ring would be."""
     out = []
     for k in range(nsub):
         t = (k + 1) * job.subint_ns
@@ -206,6 +215,16 @@ def job_subints(job: Job, nsub: int, seed: int, rho: float = 0.0) -> List[Tuple[
         else:
             inputs = synth.subint_inputs(job, sec, ns, rho=rho, seed=seed)
         out.append((inputs, sec, ns))
+    if pinned:
+        total = sum(b.nbytes for inputs, _, _ in out for b, _, _ in inputs)
+        block = pinned_empty(total)
+        off = 0
+        for inputs, _, _ in out:
+            for k, (b, dsec, dns) in enumerate(inputs):
+                v = block[off:off + b.nbytes]
+                v[:] = np.frombuffer(np.ascontiguousarray(b).data, dtype=np.uint8)
+                inputs[k] = (v, dsec, dns)
+                off += b.nbytes
     return out
 
 

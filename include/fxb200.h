@@ -178,6 +178,12 @@ FXB_API fxb_status fxb_timing_enable(fxb_ctx *ctx, int32_t on);
 FXB_API fxb_status fxb_timing_read(fxb_ctx *ctx, int32_t *nsubint, double *prep_ms, double *fstage_ms,
                                    double *xmac_ms);
 
+/* Page-locked host memory for station buffers: fxb_submit_subint copies from
+ * it asynchronously at full link speed, where a pageable buffer is staged by
+ * the driver on the calling thread.  Free with fxb_host_free. */
+FXB_API void *fxb_host_alloc(size_t bytes, fxb_status *status);
+FXB_API void fxb_host_free(void *p);
+
 /* The cudaStream_t (as void*) on which the context launches its kernels,
  * so that callers can order their own work and events against it. */
 FXB_API fxb_status fxb_get_stream(const fxb_ctx *ctx, void **stream);
@@ -276,6 +282,10 @@ FXB_API fxb_status fxb_server_poll(fxb_server *srv, uint64_t job_id, int32_t *st
 /* Block until the job is done or failed, or timeout_s passes
  * (FXB_ERR_TIMEOUT). */
 FXB_API fxb_status fxb_server_wait(fxb_server *srv, uint64_t job_id, double timeout_s);
+/* Where a done job's latency went, phase_ms[5]: queued (submit to admission),
+ * context creation, subint submission (start to last subint queued), drain
+ * (last subint queued to completion seen), result read and release. */
+FXB_API fxb_status fxb_server_job_times(fxb_server *srv, uint64_t job_id, double *phase_ms);
 /* Completed jobs, p50 / p99 latency (ms), data seconds correlated, and wall
  * seconds from the first submit to the last completion. */
 FXB_API fxb_status fxb_server_stats(fxb_server *srv, int32_t *ncompleted, double *p50_ms, double *p99_ms,

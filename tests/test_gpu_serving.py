@@ -77,3 +77,44 @@ def test_served_job_matches_oracle():
     c.close()
     cross_err, auto_err = tc_errors(job, layout, n, got, ref)
     assert cross_err <= TC_TOL and auto_err <= TC_TOL
+
+
+def test_pinned_buffers_give_the_same_result_and_phases_add_up():
+    jobs = _jobs()
+    pinned = []
+    for k, (job, _) in enumerate(jobs):
+        pinned.append((job, serving.job_subints(job, 3, seed=20 + k, rho=0.05, pinned=True)))
+    alone = [_alone(j, s, "bf16") for j, s in jobs]
+    srv = serving.Server(budget_bytes=8 << 30, max_active=3)
+    handles = [srv.submit(j, s) for j, s in pinned]
+    for h, ref in zip(handles, alone):
+        assert np.array_equal(srv.wait(h, 120.0), ref)
+        t = srv.job_times(h)
+        lat = srv.poll(h)[1]
+        assert all(v >= 0 for v in t.values())
+        assert abs(sum(t.values()) - lat) < 1e-3 * max(lat, 1.0) + 1e-3
+    srv.close()
+
+
+def test_a_failing_job_is_reported_and_the_others_complete():
+    import ctypes
+    from fxb200.native import FxbError
+    jobs = _jobs()
+    srv = serving.Server(budget_bytes=8 << 30, max_active=3)
+    good = srv.submit(*jobs[0])
+    job, subints = jobs[1]
+    bad = serving.ServedJob(job, subints, "bf16", 2)
+    bad.nbytes[len(job.stations)] = -1            # second subint, first station: rejected by the host check
+    jid = ctypes.c_uint64(0)
+    assert serving._bind().fxb_server_submit(srv.srv, ctypes.byref(bad.req), ctypes.byref(jid)) == 0
+    bad.id = jid.value
+    srv.jobs.append(bad)
+    last = srv.submit(*jobs[2])
+    with pytest.raises(FxbError):
+        srv.wait(bad, 120.0)
+    assert srv.poll(bad)[0] == 3
+    for h in (good, last):
+        srv.wait(h, 120.0)
+        assert srv.poll(h)[0] == 2
+    assert "bad station buffer" in serving._bind().fxb_server_last_error(srv.srv).decode()
+    srv.close()
