@@ -33,6 +33,11 @@ struct Slot {
 	int32_t *h_vflags = nullptr;
 	cudaEvent_t copied = nullptr, done = nullptr;
 	bool used = false;
+	// this slot's subint kernels as one CUDA graph, valid while the
+	// frame-validity array it was captured with is current
+	cudaGraphExec_t gexec = nullptr;
+	const uint8_t *g_valid = nullptr;
+	int64_t g_stride = 0;
 };
 
 struct fxb_ctx {
@@ -69,6 +74,8 @@ struct fxb_ctx {
 	bool timed = false;
 	// per-subint kernel timing (fxb_timing_enable / fxb_timing_read)
 	bool timing_on = false;
+	bool graphs = true;       // replay each slot's kernels as a CUDA graph (eager launches while timing)
+	bool batched = false;     // a member of an fxb_batch: subints arrive through the batch
 	std::vector<cudaEvent_t> tev;       // 4 per recorded subint
 	size_t tev_used = 0;
 	std::vector<bool> delay_set;
@@ -160,6 +167,7 @@ static void free_ctx(fxb_ctx *ctx)
 	{
 		std::free(s.h_sub);
 		std::free(s.h_vflags);
+		if(s.gexec) cudaGraphExecDestroy(s.gexec);
 		if(s.copied) cudaEventDestroy(s.copied);
 		if(s.done) cudaEventDestroy(s.done);
 	}
@@ -647,8 +655,12 @@ fxb_status fxb_set_delay_poly(fxb_ctx *ctx, int32_t station, int32_t npoly, int3
 	return FXB_OK;
 }
 
-static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes, const int32_t *datasec,
-                         const int32_t *datans, const int32_t *const *validflags, int32_t sec, int32_t ns, bool device)
+// Waits for the next slot, fills its per-station records and queues the
+// copies of this subint's station buffers on the copy stream; the slot's
+// `copied` event marks their end.
+static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes,
+                               const int32_t *datasec, const int32_t *datans, const int32_t *const *validflags,
+                               int32_t sec, int32_t ns, bool device, Slot **slot)
 {
 	if(!ctx || !bufs || !nbytes || !datasec || !datans)
 		return FXB_ERR_ARG;
@@ -695,6 +707,8 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 		u.nbytes = nbytes[s];
 		u.datasec = datasec[s];
 		u.datans = datans[s];
+		u.subsec = sec;
+		u.subns = ns;
 		if(device)
 			u.buf = bufs[s];
 		else
@@ -724,29 +738,28 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 	CK(ctx, cudaMemcpyAsync(sl.d_vflags, sl.h_vflags, sizeof(int32_t) * ctx->S * ctx->nflagint, cudaMemcpyHostToDevice,
 	                        ctx->copy_stream));
 	CK(ctx, cudaEventRecord(sl.copied, ctx->copy_stream));
-	CK(ctx, cudaStreamWaitEvent(ctx->stream, sl.copied, 0));
+	*slot = &sl;
+	return FXB_OK;
+}
 
-	cudaStream_t st = ctx->stream;
-	cudaEvent_t *tv = nullptr;
-	if(ctx->timing_on && ctx->tev_used + 4 <= 4 * 8192)
-	{
-		while(ctx->tev.size() < ctx->tev_used + 4)
-		{
-			cudaEvent_t e;
-			CK(ctx, cudaEventCreate(&e));
-			ctx->tev.push_back(e);
-		}
-		tv = &ctx->tev[ctx->tev_used];
-		ctx->tev_used += 4;
-	}
-	CK(ctx, cudaEventRecord(ctx->ev_a, st));
-	if(tv) CK(ctx, cudaEventRecord(tv[0], st));
-	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, sec, ns, st);
+// Every kernel of one subint whose inputs sit in slot sl, on stream st.  No
+// host synchronisation and no argument that changes between subints (the
+// subint time travels in the slot's records), so that the sequence can be
+// captured once per slot and replayed.  capture: the four timing events
+// become event-record nodes of the graph; tv: per-subint timing events
+// (eager launches only).
+static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, cudaEvent_t *tv, bool capture)
+{
+	const Job &job = ctx->job;
+	const unsigned evf = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
+	cudaEventRecordWithFlags(ctx->ev_a, st, evf);
+	if(tv) cudaEventRecord(tv[0], st);
+	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, st);
 	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->valid_stride, ctx->S, st);
 	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->valid_stride, ctx->S, ctx->T,
-	                  sec, ns, job.fringe_rot_order, ctx->d_params, st);
-	CK(ctx, cudaEventRecord(ctx->ev_b, st));
-	if(tv) CK(ctx, cudaEventRecord(tv[1], st));
+	                  job.fringe_rot_order, ctx->d_params, st);
+	cudaEventRecordWithFlags(ctx->ev_b, st, evf);
+	if(tv) cudaEventRecord(tv[1], st);
 	{
 		FsArgs fa;
 		memset(&fa, 0, sizeof(fa));
@@ -771,8 +784,8 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 				launch_fstage_kind(k, fa, st);
 		}
 	}
-	CK(ctx, cudaEventRecord(ctx->ev_c, st));
-	if(tv) CK(ctx, cudaEventRecord(tv[2], st));
+	cudaEventRecordWithFlags(ctx->ev_c, st, evf);
+	if(tv) cudaEventRecord(tv[2], st);
 	for(const auto &g : ctx->xgroups)
 	{
 		if(ctx->tc)
@@ -781,11 +794,89 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 			launch_xmac_fp32v2(ctx->h_plans[g.plan0], ctx->d_plans, g.d_idx, g.nf, ctx->T, ctx->d_spec, ctx->d_acc, st);
 	}
 	launch_weights(ctx->d_bw, ctx->nbw, ctx->d_acw, ctx->nacw, ctx->d_params, ctx->T, ctx->d_bwacc, ctx->d_acwacc, st);
-	CK(ctx, cudaEventRecord(ctx->ev_d, st));
-	if(tv) CK(ctx, cudaEventRecord(tv[3], st));
+	cudaEventRecordWithFlags(ctx->ev_d, st, evf);
+	if(tv) cudaEventRecord(tv[3], st);
+}
+
+// The slot's graph, captured (again) when missing or when the frame-validity
+// array has been reallocated since.  A capture that fails turns graphs off
+// for the context and leaves the stream as it was.
+static fxb_status slot_graph(fxb_ctx *ctx, Slot &sl)
+{
+	if(sl.gexec && sl.g_valid == ctx->d_valid && sl.g_stride == ctx->valid_stride)
+		return FXB_OK;
+	if(sl.gexec)
+	{
+		cudaGraphExecDestroy(sl.gexec);
+		sl.gexec = nullptr;
+	}
+	CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+	launch_compute(ctx, sl, ctx->stream, nullptr, true);
+	cudaGraph_t g = nullptr;
+	cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+	if(e == cudaSuccess)
+		e = cudaGraphInstantiate(&sl.gexec, g, 0);
+	if(g)
+		cudaGraphDestroy(g);
+	if(e != cudaSuccess)
+	{
+		cudaGetLastError();
+		sl.gexec = nullptr;
+		ctx->graphs = false;
+		return FXB_OK;
+	}
+	sl.g_valid = ctx->d_valid;
+	sl.g_stride = ctx->valid_stride;
+	return FXB_OK;
+}
+
+static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes, const int32_t *datasec,
+                         const int32_t *datans, const int32_t *const *validflags, int32_t sec, int32_t ns, bool device)
+{
+	if(ctx && ctx->batched)
+	{
+		ctx->err = "context belongs to a batch: submit through fxb_batch_submit";
+		return FXB_ERR_STATE;
+	}
+	Slot *slp = nullptr;
+	const fxb_status rc = stage_subint(ctx, bufs, nbytes, datasec, datans, validflags, sec, ns, device, &slp);
+	if(rc != FXB_OK)
+		return rc;
+	Slot &sl = *slp;
+	cudaStream_t st = ctx->stream;
+	CK(ctx, cudaStreamWaitEvent(st, sl.copied, 0));
+	cudaEvent_t *tv = nullptr;
+	if(ctx->timing_on && ctx->tev_used + 4 <= 4 * 8192)
+	{
+		while(ctx->tev.size() < ctx->tev_used + 4)
+		{
+			cudaEvent_t e;
+			CK(ctx, cudaEventCreate(&e));
+			ctx->tev.push_back(e);
+		}
+		tv = &ctx->tev[ctx->tev_used];
+		ctx->tev_used += 4;
+	}
+	if(!tv && ctx->graphs)
+	{
+		const fxb_status gs = slot_graph(ctx, sl);
+		if(gs != FXB_OK)
+			return gs;
+	}
+	if(!tv && ctx->graphs)
+		CK(ctx, cudaGraphLaunch(sl.gexec, st));
+	else
+		launch_compute(ctx, sl, st, tv, false);
 	CK(ctx, cudaGetLastError());
 	CK(ctx, cudaEventRecord(sl.done, st));
 	ctx->timed = true;
+	return FXB_OK;
+}
+
+fxb_status fxb_set_graphs(fxb_ctx *ctx, int32_t on)
+{
+	if(!ctx) return FXB_ERR_ARG;
+	ctx->graphs = on != 0;
 	return FXB_OK;
 }
 
@@ -1095,6 +1186,234 @@ fxb_status fxb_vdif_unpack(const uint8_t *data, int64_t nbytes, int32_t payload,
 	if(d_out) cudaFree(d_out);
 	if(d_good) cudaFree(d_good);
 	return rc;
+}
+
+// ---------------------------------------------------------------- batches
+// Several contexts (e.g. one per subband shape: width, channels, bits) whose
+// subints are submitted together.  Per subint every member stages its copies
+// on its own copy stream; then ONE graph launch on the batch stream runs all
+// members' kernels, each member a parallel branch of the graph (captured once
+// per slot, replayed after).  Members stay ordinary contexts for reading and
+// resetting results; their streams are ordered after every batch launch.
+struct fxb_batch {
+	std::vector<fxb_ctx *> m;
+	cudaStream_t stream = nullptr;
+	cudaEvent_t fork = nullptr, done = nullptr;
+	std::vector<cudaEvent_t> join;                    // [member]
+	std::vector<cudaGraphExec_t> gexec;               // [slot]
+	std::vector<std::vector<const uint8_t *>> g_valid; // [slot][member] validity arrays captured with
+	std::vector<std::vector<int64_t>> g_stride;
+	bool graphs = true;
+	std::string err;
+};
+
+static void free_batch(fxb_batch *b)
+{
+	if(b->stream)
+		cudaStreamSynchronize(b->stream);
+	for(cudaGraphExec_t g : b->gexec)
+		if(g) cudaGraphExecDestroy(g);
+	for(cudaEvent_t e : b->join)
+		if(e) cudaEventDestroy(e);
+	if(b->fork) cudaEventDestroy(b->fork);
+	if(b->done) cudaEventDestroy(b->done);
+	if(b->stream) cudaStreamDestroy(b->stream);
+	for(fxb_ctx *c : b->m)
+		c->batched = false;
+	delete b;
+}
+
+#define BK(b, call)                                                          \
+	do {                                                                     \
+		cudaError_t e_ = (call);                                             \
+		if(e_ != cudaSuccess)                                                \
+		{                                                                    \
+			(b)->err = std::string(#call) + ": " + cudaGetErrorString(e_);   \
+			return e_ == cudaErrorMemoryAllocation ? FXB_ERR_NOMEM : FXB_ERR_CUDA; \
+		}                                                                    \
+	} while(0)
+
+// capture every member's kernels for slot k as parallel branches
+static fxb_status batch_graph(fxb_batch *b, int k, const std::vector<Slot *> &slots)
+{
+	const size_t n = b->m.size();
+	bool ok = b->gexec[k] != nullptr;
+	for(size_t i = 0; ok && i < n; i++)
+		ok = b->g_valid[k][i] == b->m[i]->d_valid && b->g_stride[k][i] == b->m[i]->valid_stride;
+	if(ok)
+		return FXB_OK;
+	if(b->gexec[k])
+	{
+		cudaGraphExecDestroy(b->gexec[k]);
+		b->gexec[k] = nullptr;
+	}
+	BK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+	for(size_t i = 0; i < n; i++)
+	{
+		fxb_ctx *c = b->m[i];
+		cudaEventRecord(b->fork, b->stream);
+		cudaStreamWaitEvent(c->stream, b->fork, 0);
+		launch_compute(c, *slots[i], c->stream, nullptr, true);
+		cudaEventRecord(b->join[i], c->stream);
+		cudaStreamWaitEvent(b->stream, b->join[i], 0);
+	}
+	cudaGraph_t g = nullptr;
+	cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+	if(e == cudaSuccess)
+		e = cudaGraphInstantiate(&b->gexec[k], g, 0);
+	if(g)
+		cudaGraphDestroy(g);
+	if(e != cudaSuccess)
+	{
+		cudaGetLastError();
+		b->gexec[k] = nullptr;
+		b->graphs = false;              // eager launches from now on
+		return FXB_OK;
+	}
+	for(size_t i = 0; i < n; i++)
+	{
+		b->g_valid[k][i] = b->m[i]->d_valid;
+		b->g_stride[k][i] = b->m[i]->valid_stride;
+	}
+	return FXB_OK;
+}
+
+fxb_batch *fxb_batch_create(fxb_ctx *const *members, int32_t n, fxb_status *status)
+{
+	auto fail = [&](fxb_status st) -> fxb_batch * {
+		if(status) *status = st;
+		return nullptr;
+	};
+	if(!members || n < 1)
+		return fail(FXB_ERR_ARG);
+	for(int i = 0; i < n; i++)
+	{
+		if(!members[i] || members[i]->batched || members[i]->slots.size() != members[0]->slots.size() ||
+		   members[i]->next_slot != members[0]->next_slot)
+			return fail(FXB_ERR_ARG);
+		for(int j = 0; j < i; j++)
+			if(members[j] == members[i])
+				return fail(FXB_ERR_ARG);
+	}
+	fxb_batch *b = new fxb_batch;
+	b->m.assign(members, members + n);
+	const size_t nslot = members[0]->slots.size();
+	b->gexec.assign(nslot, nullptr);
+	b->g_valid.assign(nslot, std::vector<const uint8_t *>(n, nullptr));
+	b->g_stride.assign(nslot, std::vector<int64_t>(n, 0));
+	b->join.assign(n, nullptr);
+	bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+	          cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
+	          cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
+	for(int i = 0; ok && i < n; i++)
+		ok = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
+	if(!ok)
+	{
+		free_batch(b);
+		return fail(FXB_ERR_CUDA);
+	}
+	for(fxb_ctx *c : b->m)
+		c->batched = true;
+	if(status) *status = FXB_OK;
+	return b;
+}
+
+fxb_status fxb_batch_submit(fxb_batch *b, const fxb_member_subint *data, int32_t sec, int32_t ns)
+{
+	if(!b || !data)
+		return FXB_ERR_ARG;
+	const size_t n = b->m.size();
+	// argument checks first, so that a rejected call stages nothing and the
+	// members' slots stay in step
+	for(size_t i = 0; i < n; i++)
+	{
+		const fxb_member_subint &d = data[i];
+		if(!d.bufs || !d.nbytes || !d.datasec || !d.datans)
+			return FXB_ERR_ARG;
+		for(int s = 0; s < b->m[i]->S; s++)
+		{
+			if(!b->m[i]->delay_set[s])
+			{
+				b->err = "delay model not set for every station of every member";
+				return FXB_ERR_STATE;
+			}
+			if(d.nbytes[s] < 0 || (d.nbytes[s] > 0 && !d.bufs[s]))
+			{
+				b->err = "bad station buffer";
+				return FXB_ERR_ARG;
+			}
+		}
+	}
+	const int k = b->m[0]->next_slot;
+	std::vector<Slot *> slots(n, nullptr);
+	for(size_t i = 0; i < n; i++)
+	{
+		fxb_ctx *c = b->m[i];
+		const fxb_member_subint &d = data[i];
+		const fxb_status rc = stage_subint(c, d.bufs, d.nbytes, d.datasec, d.datans, d.validflags, sec, ns, false,
+		                                   &slots[i]);
+		if(rc != FXB_OK)
+		{
+			b->err = std::string("member ") + std::to_string(i) + ": " + c->err;
+			return rc;
+		}
+		BK(b, cudaStreamWaitEvent(b->stream, slots[i]->copied, 0));
+		// and after whatever the member's own stream still holds (a reset, a read)
+		BK(b, cudaEventRecord(b->join[i], c->stream));
+		BK(b, cudaStreamWaitEvent(b->stream, b->join[i], 0));
+	}
+	if(b->graphs)
+	{
+		const fxb_status rc = batch_graph(b, k, slots);
+		if(rc != FXB_OK)
+			return rc;
+	}
+	if(b->graphs)
+		BK(b, cudaGraphLaunch(b->gexec[k], b->stream));
+	else
+		for(size_t i = 0; i < n; i++)
+			launch_compute(b->m[i], *slots[i], b->stream, nullptr, false);
+	BK(b, cudaGetLastError());
+	BK(b, cudaEventRecord(b->done, b->stream));
+	for(size_t i = 0; i < n; i++)
+	{
+		BK(b, cudaEventRecord(slots[i]->done, b->stream));
+		BK(b, cudaStreamWaitEvent(b->m[i]->stream, b->done, 0));
+		b->m[i]->timed = true;
+	}
+	return FXB_OK;
+}
+
+fxb_status fxb_batch_sync(fxb_batch *b)
+{
+	if(!b)
+		return FXB_ERR_ARG;
+	BK(b, cudaStreamSynchronize(b->stream));
+	for(fxb_ctx *c : b->m)
+	{
+		const fxb_status st = check_device_error(c);
+		if(st != FXB_OK)
+		{
+			b->err = c->err;
+			return st;
+		}
+	}
+	return FXB_OK;
+}
+
+fxb_status fxb_batch_set_graphs(fxb_batch *b, int32_t on)
+{
+	if(!b) return FXB_ERR_ARG;
+	b->graphs = on != 0;
+	return FXB_OK;
+}
+
+const char *fxb_batch_last_error(const fxb_batch *b) { return b ? b->err.c_str() : ""; }
+
+void fxb_batch_destroy(fxb_batch *b)
+{
+	if(b)
+		free_batch(b);
 }
 
 }  // extern "C"

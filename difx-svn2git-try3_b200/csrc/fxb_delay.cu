@@ -78,13 +78,13 @@ __device__ bool delay_interpolator(const DevStation &S, int blockspersend, int s
 }
 
 __global__ void k_interpolators(const DevStation *__restrict__ st, DevSubintStation *__restrict__ sub, int S,
-                                int blockspersend, int sec, int ns)
+                                int blockspersend)
 {
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
 	if(s >= S)
 		return;
 	double c[3] = {0.0, 0.0, 0.0};
-	bool ok = delay_interpolator(st[s], blockspersend, sec, ns, c);
+	bool ok = delay_interpolator(st[s], blockspersend, sub[s].subsec, sub[s].subns, c);
 	sub[s].interp[0] = c[0];
 	sub[s].interp[1] = c[1];
 	sub[s].interp[2] = c[2];
@@ -122,7 +122,7 @@ __device__ inline bool flag_valid(const int32_t *vf, int i)
 // (mode.cpp:671-840) and the Mk5Mode::unpack weight (mk5mode.cpp:104-177).
 __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
                              const int32_t *__restrict__ validflags, int nflagint, const uint8_t *__restrict__ valid,
-                             int64_t valid_stride, int T, int offsetsec, int offsetns, int order, FftParam *__restrict__ out)
+                             int64_t valid_stride, int T, int order, FftParam *__restrict__ out)
 {
 	const int s = blockIdx.y;
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -130,6 +130,7 @@ __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintS
 		return;
 	const DevStation &S = st[s];
 	const DevSubintStation &U = sub[s];
+	const int offsetsec = U.subsec, offsetns = U.subns;
 	const int32_t *vf = validflags + (int64_t)s * nflagint;
 	FftParam p;
 	p.status = kFftZero;
@@ -270,18 +271,17 @@ void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8
 	k_frame_valid<<<grid, 256, 0, stream>>>(st, sub, valid, valid_stride);
 }
 
-void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, int sec, int ns,
-                          cudaStream_t stream)
+void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, cudaStream_t stream)
 {
-	k_interpolators<<<(S + 63) / 64, 64, 0, stream>>>(st, sub, S, blockspersend, sec, ns);
+	k_interpolators<<<(S + 63) / 64, 64, 0, stream>>>(st, sub, S, blockspersend);
 }
 
 void launch_fft_params(const DevStation *st, const DevSubintStation *sub, const int32_t *validflags, int nflagint,
-                       const uint8_t *valid, int64_t valid_stride, int S, int T, int sec, int ns, int order,
-                       FftParam *out, cudaStream_t stream)
+                       const uint8_t *valid, int64_t valid_stride, int S, int T, int order, FftParam *out,
+                       cudaStream_t stream)
 {
 	dim3 grid((T + 127) / 128, S);
-	k_fft_params<<<grid, 128, 0, stream>>>(st, sub, validflags, nflagint, valid, valid_stride, T, sec, ns, order, out);
+	k_fft_params<<<grid, 128, 0, stream>>>(st, sub, validflags, nflagint, valid, valid_stride, T, order, out);
 }
 
 }  // namespace fxb

@@ -70,6 +70,7 @@ struct DevSubintStation {
 	int64_t nbytes;
 	int32_t datasec, datans;
 	int32_t invalid_subint; // no delay model for this time (subint torched)
+	int32_t subsec, subns;  // subint start (the setOffsets time), the same for every station
 	int32_t pad;
 	double interp[3];       // quadratic delay interpolator (Mode::setOffsets)
 };

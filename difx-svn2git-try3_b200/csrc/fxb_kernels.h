@@ -41,11 +41,11 @@ struct DevACWeight {
 
 void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8_t *valid, int64_t valid_stride,
                         int S, cudaStream_t stream);
-void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, int sec, int ns,
-                          cudaStream_t stream);
+// the subint time is read from sub[s].subsec / subns
+void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, cudaStream_t stream);
 void launch_fft_params(const DevStation *st, const DevSubintStation *sub, const int32_t *validflags, int nflagint,
-                       const uint8_t *valid, int64_t valid_stride, int S, int T, int sec, int ns, int order,
-                       FftParam *out, cudaStream_t stream);
+                       const uint8_t *valid, int64_t valid_stride, int S, int T, int order, FftParam *out,
+                       cudaStream_t stream);
 
 // Fused unpack -> fringe rotation -> FFT -> fractional-sample correction.
 // One CTA per (station, FFT); writes FP32 spectra into spec.

@@ -176,6 +176,8 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
 	hsub.nbytes = nbytes;
 	hsub.datasec = datasec;
 	hsub.datans = datans;
+	hsub.subsec = sec;
+	hsub.subns = ns;
 
 	// spectra [t][band][nchan]: every band is a row of one shared plan
 	DevBand hb[kMaxBandsPerStation];
@@ -231,9 +233,9 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
 	   cudaMemcpyAsync(d_flags, hflags, sizeof(int32_t) * nflagint, cudaMemcpyHostToDevice, cs) != cudaSuccess)
 		return FXB_ERR_CUDA;
 
-	launch_interpolators(d_st, d_sub, 1, T, sec, ns, cs);
+	launch_interpolators(d_st, d_sub, 1, T, cs);
 	launch_frame_valid(d_st, d_sub, d_valid, valid_stride, 1, cs);
-	launch_fft_params(d_st, d_sub, d_flags, nflagint, d_valid, valid_stride, 1, T, sec, ns, fringe_rot_order,
+	launch_fft_params(d_st, d_sub, d_flags, nflagint, d_valid, valid_stride, 1, T, fringe_rot_order,
 	                  d_params, cs);
 	launch_fstage(d_st, d_sub, d_bands, st.nband, d_plans, d_valid, valid_stride, d_params, d_tw, N, 1, T,
 	              fringe_rot_order, fraclo, N, (float2 *)dev_spectra, cs);

@@ -110,6 +110,12 @@ class FxbError(RuntimeError):
     pass
 
 
+class FxbMemberSubint(ctypes.Structure):
+    _fields_ = [("bufs", ctypes.POINTER(ctypes.c_void_p)), ("nbytes", ctypes.POINTER(ctypes.c_int64)),
+                ("datasec", ctypes.POINTER(ctypes.c_int32)), ("datans", ctypes.POINTER(ctypes.c_int32)),
+                ("validflags", ctypes.POINTER(ctypes.c_void_p))]
+
+
 def lib():
     """Load libfxb200.so; raises when it is missing (no fallback)."""
     global _lib
@@ -144,6 +150,18 @@ def lib():
     L.fxb_timing_read.argtypes = [vp, i32p, dp, dp, dp]
     L.fxb_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
     L.fxb_read_results_device.argtypes = [vp, ctypes.c_void_p, ctypes.c_size_t]
+    L.fxb_set_graphs.argtypes = [vp, i32]
+    L.fxb_set_graphs.restype = ctypes.c_int
+    L.fxb_batch_create.restype = vp
+    L.fxb_batch_create.argtypes = [ctypes.POINTER(vp), i32, i32p]
+    L.fxb_batch_submit.argtypes = [vp, ctypes.POINTER(FxbMemberSubint), i32, i32]
+    L.fxb_batch_sync.argtypes = [vp]
+    L.fxb_batch_set_graphs.argtypes = [vp, i32]
+    for name in ("fxb_batch_submit", "fxb_batch_sync", "fxb_batch_set_graphs"):
+        getattr(L, name).restype = ctypes.c_int
+    L.fxb_batch_last_error.restype = ctypes.c_char_p
+    L.fxb_batch_last_error.argtypes = [vp]
+    L.fxb_batch_destroy.argtypes = [vp]
     L.fxb_host_alloc.restype = vp
     L.fxb_host_alloc.argtypes = [ctypes.c_size_t, i32p]
     L.fxb_host_free.argtypes = [vp]
@@ -266,6 +284,10 @@ class Correlator:
         """Submit from host memory given raw pointers (e.g. pinned buffers)."""
         self._submit(lib().fxb_submit_subint, ptrs, nbytes, dsec, dns, validflags, sec, ns)
 
+    def set_graphs(self, on: bool = True):
+        """Replay each slot's subint kernels as a CUDA graph (default) or launch them one by one."""
+        check(lib().fxb_set_graphs(self.ctx, 1 if on else 0), self.ctx, "set_graphs")
+
     def results_into(self, out: np.ndarray) -> np.ndarray:
         check(lib().fxb_read_results(self.ctx, _fptr(out), out.size), self.ctx, "read_results")
         return out
@@ -341,3 +363,52 @@ def job_layout(job: Job) -> Tuple[np.ndarray, int]:
     check(lib().fxb_job_layout(holder.ptr(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), out.size,
                                ctypes.byref(n)), None, "job_layout")
     return out, n.value
+
+
+class Batch:
+    """An fxb_batch: member Correlators whose subints are submitted together
+    and run as one CUDA graph launch per subint."""
+
+    def __init__(self, members: Sequence[Correlator]):
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.ctx for m in self.members])
+        st = ctypes.c_int32(0)
+        self.b = lib().fxb_batch_create(arr, len(self.members), ctypes.byref(st))
+        if not self.b:
+            raise FxbError("fxb_batch_create: %s" % FXB_STATUS.get(st.value, st.value))
+
+    def _check(self, rc, what):
+        if rc != 0:
+            m = lib().fxb_batch_last_error(self.b)
+            raise FxbError("%s failed: %s %s" % (what, FXB_STATUS.get(rc, rc), m.decode() if m else ""))
+
+    def submit(self, member_inputs: Sequence[List[Tuple[np.ndarray, int, int]]], sec: int, ns: int) -> None:
+        """member_inputs[i]: member i's [(buffer, datasec, datans)] per station."""
+        keep, recs = [], (FxbMemberSubint * len(self.members))()
+        for i, inputs in enumerate(member_inputs):
+            n = len(inputs)
+            bufs = (ctypes.c_void_p * n)(*[b.ctypes.data for b, _, _ in inputs])
+            nb = (ctypes.c_int64 * n)(*[b.size for b, _, _ in inputs])
+            ds = (ctypes.c_int32 * n)(*[x for _, x, _ in inputs])
+            dn = (ctypes.c_int32 * n)(*[x for _, _, x in inputs])
+            keep += [bufs, nb, ds, dn]
+            recs[i].bufs, recs[i].nbytes, recs[i].datasec, recs[i].datans = bufs, nb, ds, dn
+            recs[i].validflags = None
+        self._check(lib().fxb_batch_submit(self.b, recs, sec, ns), "batch_submit")
+
+    def sync(self):
+        self._check(lib().fxb_batch_sync(self.b), "batch_sync")
+
+    def set_graphs(self, on: bool = True):
+        self._check(lib().fxb_batch_set_graphs(self.b, 1 if on else 0), "batch_set_graphs")
+
+    def close(self):
+        if getattr(self, "b", None):
+            lib().fxb_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -140,6 +140,34 @@ FXB_API fxb_status fxb_submit_subint_device(fxb_ctx *ctx, const uint8_t *const *
 /* Wait for all submitted work. */
 FXB_API fxb_status fxb_sync(fxb_ctx *ctx);
 
+/* Each staging slot's subint kernels are captured once into a CUDA graph and
+ * replayed (default on; kernels are launched one by one while per-subint
+ * timing is enabled).  on = 0 launches them one by one always. */
+FXB_API fxb_status fxb_set_graphs(fxb_ctx *ctx, int32_t on);
+
+/* Batches: contexts whose subints are submitted together, e.g. one context
+ * per subband shape (bandwidth, channels, bits) of an observation whose
+ * subbands are uneven.  Per subint every member copies its station buffers
+ * on its own copy stream, then one CUDA graph launch runs every member's
+ * kernels as parallel branches.  A member takes no fxb_submit_subint of its
+ * own while it belongs to a batch; its results are read and reset through
+ * the usual calls (ordered after the batch's launches).  All members need
+ * the same max_subints_in_flight. */
+typedef struct fxb_batch fxb_batch;
+typedef struct {
+	const uint8_t *const *bufs;       /* [nstation] host station buffers */
+	const int64_t *nbytes;            /* [nstation] */
+	const int32_t *datasec, *datans;  /* [nstation] start of each buffer */
+	const int32_t *const *validflags; /* [nstation] or NULL */
+} fxb_member_subint;
+FXB_API fxb_batch *fxb_batch_create(fxb_ctx *const *members, int32_t nmember, fxb_status *status);
+/* data[nmember]: every member's buffers of the subint starting at (sec, ns). */
+FXB_API fxb_status fxb_batch_submit(fxb_batch *batch, const fxb_member_subint *data, int32_t sec, int32_t ns);
+FXB_API fxb_status fxb_batch_sync(fxb_batch *batch);
+FXB_API fxb_status fxb_batch_set_graphs(fxb_batch *batch, int32_t on);
+FXB_API const char *fxb_batch_last_error(const fxb_batch *batch);
+FXB_API void fxb_batch_destroy(fxb_batch *batch);
+
 /* Number of complex values in the core-result buffer
  * (Configuration::getCoreResultLength). */
 FXB_API fxb_status fxb_core_result_length(const fxb_ctx *ctx, int64_t *ncomplex);

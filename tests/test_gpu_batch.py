@@ -1,0 +1,121 @@
+"""CUDA graphs and batches (fxb_set_graphs, fxb_batch_*).
+
+A context's subints replayed as per-slot CUDA graphs give exactly the result
+of launching the kernels one by one.  A batch of contexts with uneven
+subband shapes (width, channels, bits), run as one graph launch per subint,
+gives every member exactly the result it has alone, matches the FP64 oracle,
+and keeps doing so after a reset."""
+import numpy as np
+import pytest
+
+from fxb200 import synth
+from fxb200.job import Freq, full_job
+from fxb200.native import Batch, Correlator
+from helpers import compare_core, small_job
+from test_gpu_tc import TC_TOL, tc_errors
+
+import fxoracle
+
+pytestmark = pytest.mark.gpu
+
+SUBINT_NS = 2_048_000
+SUBINTS = [(0, SUBINT_NS), (0, 2 * SUBINT_NS), (0, 3 * SUBINT_NS)]
+# (width MHz, channels, bits): FFTs of 32, 64 and 4 us, all dividing the subint
+SHAPES = [(4.0, 128, 2), (16.0, 1024, 8), (64.0, 256, 2)]
+
+
+def _uneven_jobs(nstation=3):
+    jobs = []
+    for k, (bw, nchan, bits) in enumerate(SHAPES):
+        job = full_job(nstation, [Freq(8400.0 + 100.0 * k, bw, nchan)], full_pol=True, subint_ns=SUBINT_NS,
+                       nbits=bits)
+        synth.make_delay_polys(job, seed=30 + k)
+        job.validate()
+        jobs.append(job)
+    return jobs
+
+
+def _inputs(job, k, sec, ns):
+    return synth.subint_inputs(job, sec, ns, rho=0.05, seed=60 + k)
+
+
+def _alone(job, k, xmac, graphs=True):
+    c = Correlator(job, xmac=xmac)
+    c.set_graphs(graphs)
+    for sec, ns in SUBINTS:
+        c.submit(_inputs(job, k, sec, ns), sec, ns)
+    r = c.results()
+    c.close()
+    return r
+
+
+@pytest.mark.parametrize("xmac", ["fp32", "bf16"])
+def test_graph_replay_matches_eager_launches(xmac):
+    job = small_job(nstation=4, nchan=256, bw=16.0, nfreq=2, full_pol=True, subint_ns=SUBINT_NS)
+    eager = _alone(job, 0, xmac, graphs=False)
+    graph = _alone(job, 0, xmac, graphs=True)
+    assert np.array_equal(graph, eager)
+
+
+@pytest.mark.parametrize("xmac", ["fp32", "bf16"])
+def test_batch_members_match_each_job_alone(xmac):
+    jobs = _uneven_jobs()
+    alone = [_alone(j, k, xmac) for k, j in enumerate(jobs)]
+    members = [Correlator(j, xmac=xmac) for j in jobs]
+    batch = Batch(members)
+    for sec, ns in SUBINTS:
+        batch.submit([_inputs(j, k, sec, ns) for k, j in enumerate(jobs)], sec, ns)
+    batch.sync()
+    got = [m.results() for m in members]
+    # after a reset the batch starts again from zero
+    for m in members:
+        m.reset()
+    for sec, ns in SUBINTS:
+        batch.submit([_inputs(j, k, sec, ns) for k, j in enumerate(jobs)], sec, ns)
+    again = [m.results() for m in members]
+    batch.close()
+    for m in members:
+        m.close()
+    for g, a, r in zip(got, again, alone):
+        assert np.array_equal(g, r)
+        assert np.array_equal(a, r)
+
+
+@pytest.mark.parametrize("xmac", ["fp32", "bf16"])
+def test_batch_matches_oracle(xmac):
+    jobs = _uneven_jobs()
+    members = [Correlator(j, xmac=xmac) for j in jobs]
+    batch = Batch(members)
+    refs = [None] * len(jobs)
+    orcs = [fxoracle.OracleCorrelator(j) for j in jobs]
+    for sec, ns in SUBINTS:
+        ins = [_inputs(j, k, sec, ns) for k, j in enumerate(jobs)]
+        batch.submit(ins, sec, ns)
+        for k in range(len(jobs)):
+            refs[k] = orcs[k].process_subint(ins[k], sec, ns, coreresult=refs[k])
+    batch.sync()
+    for k, (job, m) in enumerate(zip(jobs, members)):
+        got, layout, n = m.results(), m.layout(), m.corelen
+        if xmac == "fp32":
+            compare_core(job, layout, n, got, refs[k])
+        else:
+            cross_err, auto_err = tc_errors(job, layout, n, got, refs[k])
+            assert cross_err <= TC_TOL and auto_err <= TC_TOL, (k, cross_err, auto_err)
+    batch.close()
+    for m in members:
+        m.close()
+
+
+def test_member_refuses_its_own_submit_while_batched():
+    from fxb200.native import FxbError
+    jobs = _uneven_jobs()[:2]
+    members = [Correlator(j, xmac="bf16") for j in jobs]
+    batch = Batch(members)
+    sec, ns = SUBINTS[0]
+    with pytest.raises(FxbError):
+        members[0].submit(_inputs(jobs[0], 0, sec, ns), sec, ns)
+    batch.close()
+    members[0].submit(_inputs(jobs[0], 0, sec, ns), sec, ns)      # free again once the batch is gone
+    members[0].sync()
+    for m in members:
+        m.close()
