@@ -91,11 +91,15 @@ struct fxb_ctx {
 		int32_t *d_idx = nullptr;
 		TcShape shape{};
 		int64_t spec_base = 0;                    // first bf16x2 value of the group's block
+		int64_t spec8_base = 0;                   // FP8 form: first e4m3x2 word of the group's block
 		alignas(64) unsigned char tmap[128];     // CUtensorMap of the block (64-byte aligned)
 	};
 	std::vector<XGroup> xgroups;
-	// tensor-core (BF16) XMAC state
+	// tensor-core XMAC state
 	bool tc = false;
+	bool f8 = false;                     // FP8 form: quantise the bf16x2 spectra to e4m3 pairs for the XMAC
+	uint16_t *d_spec8 = nullptr;
+	int64_t spec8_elems = 0, iscale_elems = 0;
 	int nsm = 0;
 	int64_t specn_elems = 0;
 	int32_t *d_err = nullptr;
@@ -315,12 +319,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		}
 	}
 	// XMAC launch groups: frequencies with equal shape share a launch
-	ctx->tc = job.xmac_kind == FXB_XMAC_BF16;
-	if(job.xmac_kind == FXB_XMAC_FP8)
-	{
-		ctx->err = "the FP8 XMAC is not available in this build";
-		return FXB_ERR_UNSUPPORTED;
-	}
+	ctx->tc = job.xmac_kind == FXB_XMAC_BF16 || job.xmac_kind == FXB_XMAC_FP8;
+	ctx->f8 = job.xmac_kind == FXB_XMAC_FP8;
 	std::vector<std::vector<int32_t>> gidx;
 	{
 		std::vector<int> used;
@@ -353,30 +353,47 @@ static fxb_status setup_device(fxb_ctx *ctx)
 	if(ctx->tc)
 	{
 		int64_t off = 0;
+		std::vector<int64_t> isoff(ctx->F, -1);   // FP8 form: each subband's first scale
 		for(size_t gi = 0; gi < ctx->xgroups.size(); gi++)
 		{
 			fxb_ctx::XGroup &g = ctx->xgroups[gi];
 			const DevFreqPlan &p0 = ctx->h_plans[g.plan0];
-			if(!tc_shape(p0.nrow, p0.nchan, ctx->T, &g.shape))
+			if(!tc_shape(p0.nrow, p0.nchan, ctx->T, ctx->f8, &g.shape))
 			{
 				ctx->err = "tensor-core XMAC: at most 64 inputs per subband";
 				return FXB_ERR_UNSUPPORTED;
 			}
 			g.spec_base = off;
+			g.spec8_base = ctx->spec8_elems;
 			const int nblk = (p0.nchan + g.shape.CB - 1) / g.shape.CB;
 			const int64_t per = (int64_t)g.shape.Tpad * nblk * p0.nrow * g.shape.CB;
+			const int64_t per8 = (int64_t)g.shape.Tpad * nblk * g.shape.w8;
 			for(size_t i = 0; i < gidx[gi].size(); i++)
 			{
 				DevFreqPlan &d = ctx->h_plans[gidx[gi][i]];
 				d.spec_off = off + (int64_t)i * per;
+				d.spec8_off = ctx->spec8_elems + (int64_t)i * per8;
+				isoff[gidx[gi][i]] = ctx->iscale_elems;
+				ctx->iscale_elems += (int64_t)d.nchan * d.nrow;
 				d.tcb = g.shape.CB;
 				d.tnblk = nblk;
 				d.acc_ostride = 1;
 				d.acc_cstride = job.plan[gidx[gi][i]].nout;
 			}
 			off += per * (int64_t)gidx[gi].size();
+			ctx->spec8_elems += per8 * (int64_t)gidx[gi].size();
 		}
 		ctx->specn_elems = off;
+		if(ctx->f8)
+		{
+			// e4m3x2 spectra (times past T stay zero) and the per-(channel, input) scales
+			CK(ctx, dalloc(ctx, &ctx->d_spec8, (size_t)ctx->spec8_elems));
+			CK(ctx, cudaMemsetAsync(ctx->d_spec8, 0, sizeof(uint16_t) * (size_t)ctx->spec8_elems, ctx->stream));
+			float *isc = nullptr;
+			CK(ctx, dalloc(ctx, &isc, (size_t)ctx->iscale_elems));
+			for(int f = 0; f < ctx->F; f++)
+				ctx->h_plans[f].iscale = isoff[f] >= 0 ? isc + isoff[f] : nullptr;
+		}
 	}
 	CK(ctx, dalloc(ctx, &ctx->d_plans, ctx->F));
 	CK(ctx, cudaMemcpyAsync(ctx->d_plans, ctx->h_plans.data(), sizeof(DevFreqPlan) * ctx->F, cudaMemcpyHostToDevice, ctx->stream));
@@ -396,7 +413,9 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int32_t), ctx->stream));
 		CK(ctx, cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device));
 		for(fxb_ctx::XGroup &g : ctx->xgroups)
-			if(tc_tensormap_size() > sizeof(g.tmap) || !tc_make_tensormap(g.tmap, sn + g.spec_base, g.shape, g.nf))
+			if(tc_tensormap_size() > sizeof(g.tmap) ||
+			   !tc_make_tensormap(g.tmap, ctx->f8 ? (const void *)(ctx->d_spec8 + g.spec8_base) : (const void *)(sn + g.spec_base),
+			                      g.shape, g.nf))
 			{
 				ctx->err = "cuTensorMapEncodeTiled failed for the spectra buffer";
 				return FXB_ERR_CUDA;
@@ -786,6 +805,9 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, cudaEv
 	}
 	cudaEventRecordWithFlags(ctx->ev_c, st, evf);
 	if(tv) cudaEventRecord(tv[2], st);
+	if(ctx->f8)
+		for(const auto &g : ctx->xgroups)
+			launch_quant_fp8(g.shape, ctx->d_plans, g.d_idx, g.nf, ctx->T, (const uint32_t *)ctx->d_specn, ctx->d_spec8, st);
 	for(const auto &g : ctx->xgroups)
 	{
 		if(ctx->tc)
@@ -976,9 +998,14 @@ fxb_status fxb_job_footprint(const fxb_job_desc *desc, size_t *bytes)
 	}
 	const int64_t T = job.blockspersend;
 	const int S = (int)job.stations.size();
-	// spectra (the blocked tensor-core layout pads times to 32 and channels to
-	// whole blocks: at most +25 %), accumulators, core result, FFT parameters
-	double b = (double)job.spec_total * (job.xmac_kind == FXB_XMAC_FP32 ? 8.0 : 4.0 * 1.25);
+	// spectra (the blocked tensor-core layout pads times to 32 -- 64 for the
+	// e4m3 copy of the FP8 form -- and channels to whole blocks: at most
+	// +25 %), accumulators, core result, FFT parameters
+	const double pad32 = (double)((T + 31) / 32 * 32) / (double)std::max<int64_t>(T, 1);
+	const double pad64 = (double)((T + 63) / 64 * 64) / (double)std::max<int64_t>(T, 1);
+	double b = (double)job.spec_total * (job.xmac_kind == FXB_XMAC_FP32 ? 8.0
+	                                     : job.xmac_kind == FXB_XMAC_BF16 ? 4.0 * 1.25 * pad32
+	                                                                      : (4.0 * pad64 + 2.0 * pad64 + 0.5) * 1.25);
 	b += (double)job.acc_total * 8.0 + (double)job.corelen * 16.0 + (double)S * T * 64.0;
 	// raw VDIF staging of the in-flight subints (payload plus headers, 1/8 slack)
 	for(int s = 0; s < S; s++)

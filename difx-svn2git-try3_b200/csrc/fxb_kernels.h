@@ -21,6 +21,8 @@ struct DevFreqPlan {
 	const int32_t *destB;             // [nrow*nrow]
 	const int16_t *pairs;             // [npair*2] tile pairs (ti <= tj)
 	const int32_t *outsrc;            // [nout] source of each output: a | b << 8 | conj << 16 (a <= b), or -1
+	int64_t spec8_off;                // FP8 form: offset (16-bit words) of this frequency's e4m3 spectra
+	float *iscale;                    // FP8 form: [nchan][nrow] 1 / quantisation scale of the subint
 };
 
 struct DevOutMap {
@@ -114,17 +116,25 @@ void launch_xmac_fp32v2(const DevFreqPlan &plan0, const DevFreqPlan *dplans, con
 // Tensor-core XMAC (csrc/fxb_xmac_tc.cu) over one group of equally shaped
 // subbands whose bf16x2 spectra lie in one block [subband][Tpad][nrow][nchan].
 struct TcShape {
+	int32_t f8;                       // FP8 form: e4m3 pairs, K tiles of 64 times
+	int32_t w8;                       // FP8 form: values per time of a block, nrow * CB padded to 8
 	int32_t nrow, nchan, r2p, G, CB, Tpad;
 	int32_t raw_bytes, raw_stride;    // bytes of one TMA box, stride of the raw stages
 	int32_t nrs, nas;                 // raw and operand stages
 	int32_t dstride, dump_off;        // accumulator copy: floats per row, byte offset
 	size_t smem;
 };
-bool tc_shape(int nrow, int nchan, int T, TcShape *s);
+bool tc_shape(int nrow, int nchan, int T, bool f8, TcShape *s);
 bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf);
 size_t tc_tensormap_size();
 void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf,
                     int nsm, int32_t *err, float2 *acc, cudaStream_t stream);
+// FP8 form: per subband of the group (plan_idx[nf]), the bf16x2 spectra
+// [Tpad][nblk][nrow][CB] at spec_off -> e4m3x2 [Tpad][nblk][w8] at spec8_off,
+// scaled per (channel, input) so that the input's largest component over the
+// subint's T times maps to 240; writes 1 / scale to iscale[channel][input]
+void launch_quant_fp8(const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int T,
+                      const uint32_t *spec16, uint16_t *spec8, cudaStream_t stream);
 
 // FP32 cross-multiply-accumulate of one frequency into acc.
 void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, const float2 *spec, float2 *acc,

@@ -7,6 +7,11 @@
 // every product: for inputs a, b
 //     Re V[a][b] = P[2a][2b] + P[2a+1][2b+1],  Im V[a][b] = P[2a+1][2b] - P[2a][2b+1].
 //
+// FP8 form: the same, with the spectra quantised to e4m3 pairs (one 16-bit
+// word per complex value) with a scale per (channel, input) by k_quant_fp8,
+// K tiles of 64 times (still 64-byte operand rows), kind::f8f6f4 MMAs of
+// K = 32, and the epilogue dividing each product by the two inputs' scales.
+//
 // Input: the F stage's bf16x2 spectra, per group of equally shaped subbands
 // one block [subband][Tpad][block][nrow][CB] (times T..Tpad-1 zero), with CB
 // the channels of one work unit.  A unit is two M = 128 operand tiles of
@@ -33,6 +38,8 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cstdint>
 
 #include "fxb_internal.h"
@@ -43,6 +50,7 @@ namespace fxb {
 namespace {
 
 constexpr int kKT = 32;                    // times per K tile (64 bytes of BF16 per operand row)
+constexpr int kKT8 = 64;                   // FP8 form: times per K tile (64 bytes of e4m3 per operand row)
 constexpr int kRS = 6;                     // raw stages at most (tc_shape picks how many fit)
 constexpr int kAS = 4;                     // operand stages at most
 constexpr int kNG = 2;                     // M tiles per work unit
@@ -123,6 +131,16 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
 	    "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
+__device__ __forceinline__ void mma_f8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate)
+{
+	asm volatile(
+	    "{\n\t.reg .pred p;\n\t"
+	    "setp.ne.b32 p, %4, 0;\n\t"
+	    "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+	    "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t *bar)
 {
 	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
@@ -141,6 +159,17 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v)
 }
 
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+// FP8 form: from four consecutive times' words of two neighbouring values
+// (bytes: value 0 re, im, value 1 re, im), the four real bytes and the four
+// imaginary bytes of one value in time order; sel 0x5140 picks value 0,
+// 0x7362 value 1
+__device__ __forceinline__ void split4(const uint32_t *w, uint32_t sel, uint32_t &re, uint32_t &im)
+{
+	const uint32_t p01 = __byte_perm(w[0], w[1], sel), p23 = __byte_perm(w[2], w[3], sel);
+	re = __byte_perm(p01, p23, 0x5410);
+	im = __byte_perm(p01, p23, 0x7632);
+}
 
 // named barrier of the four epilogue warps
 __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
@@ -169,9 +198,11 @@ struct TcParams {
 	int32_t raw_bytes, raw_stride;  // bytes per raw box, stage stride
 	int32_t nrs, nas;               // raw and operand stages in use
 	int32_t dstride, dump_off;      // floats per row of the accumulator copy, its byte offset in shared memory
+	int32_t rpitch;                 // values per time of one raw box (FP8 form: padded to 8)
 	int32_t *err;
 };
 
+template <bool F8>
 __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__ CUtensorMap tmap,
                                                          const DevFreqPlan *__restrict__ plans,
                                                          const int32_t *__restrict__ plan_idx, TcParams tp,
@@ -228,6 +259,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 	asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 	const uint32_t tmem = tmem_base_s;
 	const int nkt = tp.nkt;
+	constexpr int KT = F8 ? kKT8 : kKT;
 
 	if(warp == 0)
 	{
@@ -249,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 						break;
 					}
 					mbar_expect_tx(&full_raw[s], (uint32_t)tp.raw_bytes);
-					tma_load_3d(raw0 + (size_t)s * tp.raw_stride, &tmap, 0, blk, fi * tp.Tpad + kt * kKT, &full_raw[s]);
+					tma_load_3d(raw0 + (size_t)s * tp.raw_stride, &tmap, 0, blk, fi * tp.Tpad + kt * KT, &full_raw[s]);
 					issued_s = kk + 1;
 				}
 			}
@@ -259,9 +291,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 	{
 		if(lane == 0)
 		{
-			// ---- MMA issuer: M = N = 128, BF16 x BF16 -> FP32, A and B K-major;
-			// unit ku accumulates into columns 256 (ku & 1)
-			const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+			// ---- MMA issuer: M = N = 128, BF16 x BF16 (FP8 form: e4m3 x e4m3)
+			// -> FP32, A and B K-major; unit ku accumulates into columns 256 (ku & 1)
+			const uint32_t idesc = (1u << 4) | (F8 ? 0u : (1u << 7) | (1u << 10)) | ((128u >> 3) << 17) |
+			                       ((128u >> 4) << 24);
 			int kk = 0, ku = 0;
 			bool ok = true;
 			for(int u = blockIdx.x; u < tp.nunits && ok; u += gridDim.x, ku++)
@@ -292,10 +325,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 #pragma unroll
 					for(int g = 0; g < kNG; g++)
 #pragma unroll
-						for(int k2 = 0; k2 < kKT / 16; k2++)
+						for(int k2 = 0; k2 < 2; k2++)
 						{
+							// each MMA takes 32 bytes of every operand row (K = 16 BF16 or 32 e4m3)
 							const uint64_t d = make_sdesc64(sbase + (uint32_t)(g * kTileBytes + k2 * 32));
-							mma_bf16(tmem + (uint32_t)(buf * 256 + g * 128), d, d, idesc, (kt > 0 || k2 > 0) ? 1u : 0u);
+							if constexpr(F8)
+								mma_f8(tmem + (uint32_t)(buf * 256 + g * 128), d, d, idesc, (kt > 0 || k2 > 0) ? 1u : 0u);
+							else
+								mma_bf16(tmem + (uint32_t)(buf * 256 + g * 128), d, d, idesc,
+								         (kt > 0 || k2 > 0) ? 1u : 0u);
 						}
 					mma_commit(&empty_a[s]);
 				}
@@ -319,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 		const int tt = threadIdx.x - 64;
 		const int rc = tp.nrow * tp.CB;                // even: CB = 2 G
 		const int npairs = rc >> 1;
-		const int items = 4 * npairs;                  // (8-time chunk, pair of neighbouring values)
+		const int items = 4 * npairs;                  // (8-time chunk (FP8: 16 times), pair of neighbouring values)
 		constexpr int kMaxItems = 2;                   // 4 * 128 / 2 / 128
 		int src_off[kMaxItems], dst_a[kMaxItems][2], dst_b[kMaxItems][2];
 		uint32_t swapm[kMaxItems];
@@ -332,7 +370,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 			if(i < items)
 			{
 				const int tc = i / npairs, pr = i - tc * npairs;
-				src_off[j] = (tc * 8 * rc + 2 * pr) >> 1;      // in 8-byte units
+				if constexpr(F8)
+					src_off[j] = tc * 16 * (tp.rpitch >> 1) + pr;  // in 4-byte units
+				else
+					src_off[j] = (tc * 8 * rc + 2 * pr) >> 1;      // in 8-byte units
 #pragma unroll
 				for(int e = 0; e < 2; e++)
 				{
@@ -366,6 +407,38 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 				}
 				const uint2 *raw = (const uint2 *)(raw0 + (size_t)rs * tp.raw_stride);
 				unsigned char *A = a0 + (size_t)as * kStageBytes;
+				if constexpr(F8)
+				{
+					const uint32_t *raw32 = (const uint32_t *)(raw0 + (size_t)rs * tp.raw_stride);
+					const int tstep = tp.rpitch >> 1;
+#pragma unroll
+					for(int j = 0; j < kMaxItems; j++)
+					{
+						if(src_off[j] < 0)
+							continue;
+						const uint32_t *src = raw32 + src_off[j];
+						uint32_t w[16];
+#pragma unroll
+						for(int t = 0; t < 16; t++)
+							w[t] = src[t * tstep];
+						uint4 re0, im0, re1, im1;
+						split4(w + 0, 0x5140, re0.x, im0.x);
+						split4(w + 4, 0x5140, re0.y, im0.y);
+						split4(w + 8, 0x5140, re0.z, im0.z);
+						split4(w + 12, 0x5140, re0.w, im0.w);
+						split4(w + 0, 0x7362, re1.x, im1.x);
+						split4(w + 4, 0x7362, re1.y, im1.y);
+						split4(w + 8, 0x7362, re1.z, im1.z);
+						split4(w + 12, 0x7362, re1.w, im1.w);
+						const bool s0 = swapm[j] & 1u, s1 = (swapm[j] >> 1) & 1u;
+						*(uint4 *)(A + dst_a[j][0]) = s0 ? im0 : re0;
+						*(uint4 *)(A + dst_b[j][0]) = s0 ? re0 : im0;
+						*(uint4 *)(A + dst_a[j][1]) = s1 ? im1 : re1;
+						*(uint4 *)(A + dst_b[j][1]) = s1 ? re1 : im1;
+					}
+				}
+				else
+				{
 #pragma unroll
 				for(int j = 0; j < kMaxItems; j++)
 				{
@@ -398,6 +471,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 					*(uint4 *)(A + dst_b[j][0]) = s0 ? re0 : im0;
 					*(uint4 *)(A + dst_a[j][1]) = s1 ? im1 : re1;
 					*(uint4 *)(A + dst_b[j][1]) = s1 ? re1 : im1;
+				}
 				}
 				// generic-proxy writes -> visible to the tensor core's async proxy
 				asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -481,6 +555,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 			// into the contiguous [channel][output] block (one addition per output
 			// and subint, so the sum is that of a load-add-store)
 			const int32_t *outsrc = P.outsrc;
+			const float *isc = F8 ? P.iscale + (int64_t)c_first * nin : nullptr;   // FP8 form: [channel][input] 1 / scale
 			float2 *dst = acc + P.acc_off + (int64_t)c_first * nout;
 			for(int o = et; o < nout; o += 128)
 			{
@@ -498,8 +573,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 					if(pb >= nin)
 						pb -= nin;
 					const float *r0 = dump + ((size_t)cl * 2 * nin + 2 * pa) * ds + 2 * pb, *r1 = r0 + ds;
-					const float vre = r0[0] + r1[1];
-					const float vim = r1[0] - r0[1];
+					float vre = r0[0] + r1[1];
+					float vim = r1[0] - r0[1];
+					if constexpr(F8)
+					{
+						const float f = isc[cl * nin + a] * isc[cl * nin + b];
+						vre *= f;
+						vim *= f;
+					}
 					atomicAdd(dst + (int64_t)cl * nout + o, make_float2(vre, cj ? -vim : vim));
 					if(++cln == nin)
 						cln = 0;
@@ -530,8 +611,9 @@ typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32
                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-bool tc_shape(int nrow, int nchan, int T, TcShape *s)
+bool tc_shape(int nrow, int nchan, int T, bool f8, TcShape *s)
 {
+	s->f8 = f8 ? 1 : 0;
 	s->nrow = nrow;
 	s->nchan = nchan;
 	s->r2p = (2 * nrow + 7) & ~7;
@@ -539,8 +621,10 @@ bool tc_shape(int nrow, int nchan, int T, TcShape *s)
 		return false;
 	s->G = 128 / s->r2p;
 	s->CB = kNG * s->G;
-	s->Tpad = (T + kKT - 1) / kKT * kKT;
-	s->raw_bytes = s->CB * nrow * kKT * 4;
+	const int kt = f8 ? kKT8 : kKT;
+	s->Tpad = (T + kt - 1) / kt * kt;
+	s->w8 = (nrow * s->CB + 7) & ~7;
+	s->raw_bytes = f8 ? s->w8 * kKT8 * 2 : s->CB * nrow * kKT * 4;
 	s->raw_stride = (s->raw_bytes + 1023) & ~1023;
 	s->dstride = s->r2p + 4;
 	const size_t dump = (size_t)s->CB * 2 * nrow * s->dstride * 4;
@@ -578,15 +662,18 @@ bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf
 			return false;
 		encode = (PFN_encodeTiled)fn;
 	}
-	const cuuint64_t W = (cuuint64_t)s.nrow * s.CB;
+	// FP8 form: 16-bit e4m3 pairs, rows padded to w8 values (16 bytes), 64 times
+	const cuuint64_t W = s.f8 ? (cuuint64_t)s.w8 : (cuuint64_t)s.nrow * s.CB;
+	const cuuint64_t esz = s.f8 ? 2 : 4;
 	const cuuint64_t nblk = (cuuint64_t)((s.nchan + s.CB - 1) / s.CB);
-	if(W > 256)
+	if(W > 256 || (W * esz) % 16 != 0)
 		return false;
 	cuuint64_t dims[3] = {W, nblk, (cuuint64_t)s.Tpad * nf};
-	cuuint64_t strides[2] = {W * 4, nblk * W * 4};
-	cuuint32_t box[3] = {(cuuint32_t)W, 1, (cuuint32_t)kKT};
+	cuuint64_t strides[2] = {W * esz, nblk * W * esz};
+	cuuint32_t box[3] = {(cuuint32_t)W, 1, (cuuint32_t)(s.f8 ? kKT8 : kKT)};
 	cuuint32_t estr[3] = {1, 1, 1};
-	CUresult r = encode((CUtensorMap *)map_out, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, (void *)spec, dims, strides, box,
+	CUresult r = encode((CUtensorMap *)map_out, s.f8 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT32,
+	                    3, (void *)spec, dims, strides, box,
 	                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
 	                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 	return r == CUDA_SUCCESS;
@@ -606,7 +693,8 @@ void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplan
 	tp.CB = s.CB;
 	tp.nchan = s.nchan;
 	tp.Tpad = s.Tpad;
-	tp.nkt = s.Tpad / kKT;
+	tp.nkt = s.Tpad / (s.f8 ? kKT8 : kKT);
+	tp.rpitch = s.f8 ? s.w8 : s.nrow * s.CB;
 	tp.nf = nf;
 	tp.nblk = (s.nchan + s.CB - 1) / s.CB;
 	tp.nunits = tp.nblk * nf;
@@ -617,9 +705,64 @@ void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplan
 	tp.dstride = s.dstride;
 	tp.dump_off = s.dump_off;
 	tp.err = err;
-	cudaFuncSetAttribute(k_xmac_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
 	const int grid = tp.nunits < nsm ? tp.nunits : nsm;
-	k_xmac_tc<<<grid, kThreads, s.smem, stream>>>(*(const CUtensorMap *)tmap, dplans, plan_idx, tp, acc);
+	if(s.f8)
+	{
+		cudaFuncSetAttribute(k_xmac_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+		k_xmac_tc<true><<<grid, kThreads, s.smem, stream>>>(*(const CUtensorMap *)tmap, dplans, plan_idx, tp, acc);
+	}
+	else
+	{
+		cudaFuncSetAttribute(k_xmac_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+		k_xmac_tc<false><<<grid, kThreads, s.smem, stream>>>(*(const CUtensorMap *)tmap, dplans, plan_idx, tp, acc);
+	}
+}
+
+// ---------------------------------------------------------------- FP8 quantisation
+// One CTA per (channel block, subband); thread = one (input, channel) column
+// of the block.  Two passes over the subint's T times: the column's largest
+// |re| or |im|, then the scaled e4m3 pairs (saturating, round to nearest).
+// Columns of channels past nchan hold zeros and keep scale 1.
+__global__ void k_quant_fp8(const DevFreqPlan *__restrict__ plans, const int32_t *__restrict__ plan_idx, int T,
+                            int w8, const uint32_t *__restrict__ spec16, uint16_t *__restrict__ spec8)
+{
+	const DevFreqPlan &P = plans[plan_idx[blockIdx.y]];
+	const int blk = blockIdx.x;
+	const int W = P.nrow * P.tcb;
+	const int col = threadIdx.x;
+	if(col >= W || blk >= P.tnblk)
+		return;
+	const int row = col / P.tcb, cl = col - row * P.tcb;
+	const int64_t ts16 = (int64_t)P.tnblk * W, ts8 = (int64_t)P.tnblk * w8;
+	const uint32_t *src = spec16 + P.spec_off + (int64_t)blk * W + col;
+	float amax = 0.0f;
+	for(int t = 0; t < T; t++)
+	{
+		const uint32_t w = __ldg(src + t * ts16);
+		const float2 v = __bfloat1622float2(*(const __nv_bfloat162 *)&w);
+		amax = fmaxf(amax, fmaxf(fabsf(v.x), fabsf(v.y)));
+	}
+	const float sc = amax > 0.0f ? 240.0f / amax : 1.0f;
+	uint16_t *dst = spec8 + P.spec8_off + (int64_t)blk * w8 + col;
+	for(int t = 0; t < T; t++)
+	{
+		const uint32_t w = __ldg(src + t * ts16);
+		const float2 v = __bfloat1622float2(*(const __nv_bfloat162 *)&w);
+		dst[t * ts8] = (uint16_t)__nv_cvt_float2_to_fp8x2(make_float2(v.x * sc, v.y * sc), __NV_SATFINITE, __NV_E4M3);
+	}
+	const int c = blk * P.tcb + cl;
+	if(c < P.nchan)
+		P.iscale[(int64_t)c * P.nrow + row] = 1.0f / sc;
+}
+
+void launch_quant_fp8(const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int T,
+                      const uint32_t *spec16, uint16_t *spec8, cudaStream_t stream)
+{
+	if(nf <= 0 || T <= 0)
+		return;
+	const int W = s.nrow * s.CB;
+	const int nblk = (s.nchan + s.CB - 1) / s.CB;
+	k_quant_fp8<<<dim3(nblk, nf), (W + 31) / 32 * 32, 0, stream>>>(dplans, plan_idx, T, s.w8, spec16, spec8);
 }
 
 }  // namespace fxb

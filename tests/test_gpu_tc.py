@@ -115,3 +115,21 @@ def test_tensor_core_fft_matches_cuda_core_fstage(monkeypatch):
         assert auto_err <= TC_TOL, auto_err
     reg = dict(regions(job, layout, n))
     assert rel_err(got_tc[reg["auto"]], got_cc[reg["auto"]]) < 2e-3
+
+
+# FP8 e4m3 keeps 3 mantissa bits: a value's rounding error is ~3.6 % rms, so a
+# visibility averaged over N products carries ~sqrt(2) * 0.036 / sqrt(N) in
+# correlation-coefficient units.  Gate: well inside that for the test sizes,
+# and far below what a wrong scale or layout would give (order 1).
+FP8_TOL = 2e-2
+
+
+@pytest.mark.parametrize("kw", [dict(nstation=4, full_pol=True),
+                                dict(nstation=5, nchan=512, bw=32.0, nfreq=2, full_pol=True, subint_ns=2_048_000),
+                                dict(nstation=10, full_pol=True, nchan=256)])
+def test_fp8_tensor_core_vs_fp64(kw):
+    job = small_job(**kw)
+    got, ref, layout, n = run_tc(job, [(0, 1_024_000), (0, 3_072_000)], xmac="fp8")
+    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
+    assert cross_err <= FP8_TOL, cross_err
+    assert auto_err <= FP8_TOL, auto_err
