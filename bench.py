@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (p50/p99 job latency)")
+    ap.add_argument("--no-c3", action="store_true", help="skip the batched uneven-subband leg")
     ap.add_argument("--serving-jobs", type=int, default=32)
     return ap.parse_args()
 
@@ -260,6 +261,96 @@ def serving_leg(args):
                       "page-locked host memory; latency = submit to core result in host memory" % (len(jobs), rate)}
 
 
+# ---------------------------------------------------------------- batched uneven subbands
+def c3_leg(args):
+    """The c3 batch (20 stations, 16 subbands of mixed width, channels and
+    bits as 12 jobs) with device-resident inputs: the tensor-core form as one
+    batch (one CUDA graph launch per subint), the tensor-core form job by job
+    and the plain FP32 form job by job (kernels launched one by one), each
+    timed with CUDA events that bracket every stream involved."""
+    import torch
+    from fxb200.native import Batch, Correlator
+    jobs = configs.c3()
+    npool, nsub = 3, 16
+    pools = [make_pool(j, npool, seed=7 + m) for m, j in enumerate(jobs)]
+    dev = [[[torch.from_numpy(b).to("cuda") for b, _, _ in inputs] for (_, inputs) in pool] for pool in pools]
+    meta = [[([t.data_ptr() for t in dev[m][k]], [b.size for b, _, _ in pools[m][k][1]],
+              [x for _, x, _ in pools[m][k][1]], [x for _, _, x in pools[m][k][1]]) for k in range(npool)]
+            for m in range(len(jobs))]
+    times = [t for (t, _) in pools[0]]
+    smhz = sum(j.station_mhz_per_sec() for j in jobs)
+    data_s = args.steps * nsub * jobs[0].subint_ns * 1e-9
+
+    def run(form, batched):
+        members = [Correlator(j, xmac=form, inflight=3) for j in jobs]
+        batch = Batch(members) if batched else None
+        if not batched and form == "fp32":
+            for m in members:
+                m.set_graphs(False)
+        # scheduling tuned online during the warm-up subints (results unchanged)
+        for m in members:
+            m.autotune(2)
+        streams = [torch.cuda.ExternalStream(batch.stream())] if batched else \
+            [torch.cuda.ExternalStream(m.stream()) for m in members]
+
+        def step():
+            for j in range(nsub):
+                k = j % npool
+                if batched:
+                    batch.submit_device([meta[m][k] for m in range(len(jobs))], *times[k])
+                else:
+                    for m, c in enumerate(members):
+                        c.submit_device(*meta[m][k], *times[k])
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        for m in members:
+            m.timing_enable(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        cur = torch.cuda.current_stream()
+        e0.record(cur)
+        for st in streams:
+            st.wait_event(e0)
+        for _ in range(args.steps):
+            step()
+        for st in streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            cur.wait_event(ev)
+        e1.record(cur)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        kern = [0.0, 0.0, 0.0]
+        for m in members:
+            n, p, f, x = m.timing_read()
+            kern = [kern[0] + p, kern[1] + f, kern[2] + x]
+        tuning = [m.tuning_report() for m in members] if batched else None
+        if batch is not None:
+            batch.close()
+        for m in members:
+            m.close()
+        nrun = args.steps * nsub
+        out = {"value": smhz * data_s / (ms * 1e-3), "unit": UNIT, "rtf": data_s / (ms * 1e-3),
+               "ms_per_subint": ms / nrun,
+               "kernel_ms_per_subint_summed": {"prep": kern[0] / nrun, "fstage": kern[1] / nrun, "xmac": kern[2] / nrun}}
+        if tuning:
+            out["tuning"] = [line for rp in tuning for line in rp.strip().split("\n") if "|" in line]
+        return out
+
+    out = {"workload": "c3: 20 stations, 16 subbands (seeded widths 4/16/64 MHz, 128/1024/4096 channels, "
+                       "2/8-bit), dual pol with full cross hands, 8.192 ms subints, as %d jobs" % len(jobs),
+           "station_mhz": smhz, "subints_timed": args.steps * nsub,
+           "l2": "inputs larger than L2 (%d MB pool cycled)" % int(sum(sum(x[1]) for mm in meta for x in mm) / 1e6)}
+    out["tc_batched_graph"] = run(args.xmac if args.xmac != "fp32" else "bf16", True)
+    out["tc_per_job"] = run(args.xmac if args.xmac != "fp32" else "bf16", False)
+    out["fp32_per_job_eager"] = run("fp32", False)
+    out["tc_batched_vs_fp32"] = out["tc_batched_graph"]["rtf"] / out["fp32_per_job_eager"]["rtf"]
+    del dev
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm
 def gpu_arm(args, job):
     import torch
@@ -287,6 +378,7 @@ def gpu_arm(args, job):
     times = [t for (t, _) in pool]
 
     corr = Correlator(job, xmac=args.xmac, inflight=3)
+    corr.autotune(2)                  # scheduling tuned online during the warm-up (results unchanged)
     ext = torch.cuda.ExternalStream(corr.stream())
     nsub = args.subints_per_step
     core_dev = torch.zeros(2 * corr.corelen, dtype=torch.float32, device="cuda")
@@ -345,6 +437,7 @@ def gpu_arm(args, job):
     barrier()
     ms = ev0.elapsed_time(ev1)
     nrec, prep_ms, f_ms, x_ms = corr.timing_read()
+    tuning = [line for line in corr.tuning_report().strip().split("\n")]
     corr.timing_enable(False)
     clk = clocks.stop()
     ms = max_over_ranks(ms)
@@ -371,6 +464,7 @@ def gpu_arm(args, job):
     other_name = "fp32" if args.xmac == "bf16" else "bf16"
     if not args.no_other_form:
         ctc = Correlator(job, xmac=other_name, inflight=3)
+        ctc.autotune(2)
         for _ in range(args.warmup):
             step_device(ctc)
         ctc.sync()
@@ -439,6 +533,9 @@ def gpu_arm(args, job):
     serve = None
     if rank == 0 and world == 1 and not args.no_serving:
         serve = serving_leg(args)
+    c3 = None
+    if rank == 0 and world == 1 and not args.no_c3:
+        c3 = c3_leg(args)
 
     # per subint: interpolators, frame validity, FFT parameters, one F-stage
     # launch per FFT length, one XMAC launch per group of equally shaped
@@ -457,7 +554,7 @@ def gpu_arm(args, job):
             "e2e": {"value": e2e_value, "unit": UNIT, "rtf": e2e_value / job.station_mhz_per_sec(),
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps},
             "roofline": roofline, "xmac_roofline": xmac_roofline, "cpu_baseline": cpu, "clocks": clk,
-            "other_form": other, "tc_vs_fp32": tc_vs_fp32, "serving": serve,
+            "other_form": other, "tc_vs_fp32": tc_vs_fp32, "tuning": tuning, "serving": serve, "batched_c3": c3,
             "gpu_launches": launches_per_subint * nsub * args.steps,
         }
         print(json.dumps(line), flush=True)

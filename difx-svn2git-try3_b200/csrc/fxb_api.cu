@@ -33,11 +33,32 @@ struct Slot {
 	int32_t *h_vflags = nullptr;
 	cudaEvent_t copied = nullptr, done = nullptr;
 	bool used = false;
+	// kernel timing of the slot's last subint: starts of prep, F stage and
+	// XMAC, end of the subint (recorded on every launch, graph nodes included);
+	// tpending: recorded while timing was on and not yet added to the sums
+	cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};
+	bool tpending = false;
 	// this slot's subint kernels as one CUDA graph, valid while the
 	// frame-validity array it was captured with is current
 	cudaGraphExec_t gexec = nullptr;
 	const uint8_t *g_valid = nullptr;
 	int64_t g_stride = 0;
+	int g_gen = -1;
+};
+
+// Online autotuner (fxb_autotune): over its first subints a context tries
+// scheduling candidates -- F stage: FFT iterations per CTA and grid order;
+// tensor-core XMAC: raw and operand ring depths -- timing every launch with
+// events, and keeps the fastest per F-stage kind and XMAC group.  None of
+// them changes any arithmetic, so every candidate gives identical results.
+struct Tuner {
+	int iter = 0, total = 0;                             // tuning while iter < total
+	std::vector<std::pair<int, int>> fc;                 // F candidates: (iterations per CTA, items fastest)
+	std::vector<std::vector<float>> fms;                 // [kind][candidate] fastest launch seen (ms)
+	std::vector<std::vector<std::pair<int, int>>> xc;    // [group] XMAC candidates: (raw, operand) ring depths
+	std::vector<std::vector<float>> xms;                 // [group][candidate]
+	std::vector<cudaEvent_t> ev;                         // boundaries: kinds (nk + 1), then groups (ng + 1)
+	bool done = false;
 };
 
 struct fxb_ctx {
@@ -70,14 +91,16 @@ struct fxb_ctx {
 	int64_t valid_stride = 0;
 	std::vector<Slot> slots;
 	int next_slot = 0;
-	cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_c = nullptr, ev_d = nullptr;
+	int last_slot = -1;              // slot of the last submitted subint
 	bool timed = false;
 	// per-subint kernel timing (fxb_timing_enable / fxb_timing_read)
 	bool timing_on = false;
 	bool graphs = true;       // replay each slot's kernels as a CUDA graph (eager launches while timing)
 	bool batched = false;     // a member of an fxb_batch: subints arrive through the batch
-	std::vector<cudaEvent_t> tev;       // 4 per recorded subint
-	size_t tev_used = 0;
+	Tuner tune;
+	int gen = 0;              // bumped whenever launch parameters change: graphs are captured again
+	double t_prep = 0, t_f = 0, t_x = 0; // per-stage sums over timed subints (ms)
+	int32_t t_n = 0;
 	std::vector<bool> delay_set;
 	// F-stage work items (by kind) and FP32 XMAC v2 launch groups
 	FGroup *d_groups = nullptr;
@@ -175,9 +198,10 @@ static void free_ctx(fxb_ctx *ctx)
 		if(s.copied) cudaEventDestroy(s.copied);
 		if(s.done) cudaEventDestroy(s.done);
 	}
-	for(cudaEvent_t e : {ctx->ev_a, ctx->ev_b, ctx->ev_c, ctx->ev_d})
-		if(e) cudaEventDestroy(e);
-	for(cudaEvent_t e : ctx->tev)
+	for(auto &s : ctx->slots)
+		for(cudaEvent_t e : s.tev)
+			if(e) cudaEventDestroy(e);
+	for(cudaEvent_t e : ctx->tune.ev)
 		if(e) cudaEventDestroy(e);
 	if(ctx->stream) cudaStreamDestroy(ctx->stream);
 	if(ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
@@ -188,12 +212,9 @@ static fxb_status setup_device(fxb_ctx *ctx)
 {
 	Job &job = ctx->job;
 	CK(ctx, cudaGetDevice(&ctx->device));
+	CK(ctx, cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device));
 	CK(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
 	CK(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-	CK(ctx, cudaEventCreate(&ctx->ev_a));
-	CK(ctx, cudaEventCreate(&ctx->ev_b));
-	CK(ctx, cudaEventCreate(&ctx->ev_c));
-	CK(ctx, cudaEventCreate(&ctx->ev_d));
 	ctx->S = (int)job.stations.size();
 	ctx->T = job.blockspersend;
 	ctx->F = (int)job.freqs.size();
@@ -482,6 +503,14 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			}
 			k.first = (int)hg.size();
 			k.count = (int)kv.second.size();
+			// FFT iterations per CTA: as many as still leave two CTAs per SM
+			for(int tq : {4, 2, 1})
+			{
+				k.tq = tq;
+				const int per = tq * k.fpc;
+				if((int64_t)((ctx->T + per - 1) / per) * k.count >= 2 * (int64_t)ctx->nsm)
+					break;
+			}
 			// tensor-core form at N = 2048: FXB_TC_FFT=1 runs the FFT on the
 			// tensor cores (fxb_fstage_tc.cu); the default is the CUDA-core FP16
 			// F stage, which is faster on the B200 today
@@ -587,6 +616,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		}
 		CK(ctx, cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));
 		CK(ctx, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+		for(cudaEvent_t &e : sl.tev)
+			CK(ctx, cudaEventCreate(&e));
 	}
 	upload_lut8(ctx->stream);
 	CK(ctx, cudaMemsetAsync(ctx->d_acc, 0, sizeof(float2) * std::max<int64_t>(job.acc_total, 1), ctx->stream));
@@ -674,6 +705,26 @@ fxb_status fxb_set_delay_poly(fxb_ctx *ctx, int32_t station, int32_t npoly, int3
 	return FXB_OK;
 }
 
+// Adds a completed slot's kernel times to the context's sums (timing on).
+static void slot_account(fxb_ctx *ctx, Slot &sl)
+{
+	if(!sl.tpending)
+		return;
+	sl.tpending = false;
+	float a = 0, b = 0, c = 0;
+	if(cudaEventElapsedTime(&a, sl.tev[0], sl.tev[1]) == cudaSuccess &&
+	   cudaEventElapsedTime(&b, sl.tev[1], sl.tev[2]) == cudaSuccess &&
+	   cudaEventElapsedTime(&c, sl.tev[2], sl.tev[3]) == cudaSuccess)
+	{
+		ctx->t_prep += a;
+		ctx->t_f += b;
+		ctx->t_x += c;
+		ctx->t_n++;
+	}
+	else
+		cudaGetLastError();
+}
+
 // Waits for the next slot, fills its per-station records and queues the
 // copies of this subint's station buffers on the copy stream; the slot's
 // `copied` event marks their end.
@@ -694,6 +745,7 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 	ctx->next_slot = (ctx->next_slot + 1) % (int)ctx->slots.size();
 	if(sl.used)
 		CK(ctx, cudaEventSynchronize(sl.done));
+	slot_account(ctx, sl);
 	sl.used = true;
 
 	// frame-validity array sized for the largest buffer of this subint
@@ -764,21 +816,21 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 // Every kernel of one subint whose inputs sit in slot sl, on stream st.  No
 // host synchronisation and no argument that changes between subints (the
 // subint time travels in the slot's records), so that the sequence can be
-// captured once per slot and replayed.  capture: the four timing events
-// become event-record nodes of the graph; tv: per-subint timing events
-// (eager launches only).
-static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, cudaEvent_t *tv, bool capture)
+// captured once per slot and replayed.  capture: the slot's four timing
+// events become event-record nodes of the graph.
+static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool capture)
 {
 	const Job &job = ctx->job;
+	Tuner &tn = ctx->tune;
+	const bool tuning = !capture && tn.iter < tn.total;
+	const size_t nk = ctx->fkinds.size();
 	const unsigned evf = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
-	cudaEventRecordWithFlags(ctx->ev_a, st, evf);
-	if(tv) cudaEventRecord(tv[0], st);
+	cudaEventRecordWithFlags(sl.tev[0], st, evf);
 	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, st);
 	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->valid_stride, ctx->S, st);
 	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->valid_stride, ctx->S, ctx->T,
 	                  job.fringe_rot_order, ctx->d_params, st);
-	cudaEventRecordWithFlags(ctx->ev_b, st, evf);
-	if(tv) cudaEventRecord(tv[1], st);
+	cudaEventRecordWithFlags(sl.tev[1], st, evf);
 	{
 		FsArgs fa;
 		memset(&fa, 0, sizeof(fa));
@@ -795,29 +847,97 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, cudaEv
 		fa.fraclo = job.fractionallofreq ? 1 : 0;
 		fa.spec = ctx->tc ? ctx->d_specn : (void *)ctx->d_spec;
 		fa.err = ctx->d_err;
-		for(const FKind &k : ctx->fkinds)
+		for(size_t i = 0; i < nk; i++)
 		{
+			FKind k = ctx->fkinds[i];
+			if(tuning)
+			{
+				cudaEventRecord(tn.ev[i], st);
+				if(!k.tcfft)
+				{
+					const auto &c = tn.fc[tn.iter % tn.fc.size()];
+					k.tq = c.first;
+					k.items_fast = c.second;
+				}
+			}
 			if(k.tcfft)
 				launch_fstage_tc(k, fa, ctx->nsm, st);
 			else
 				launch_fstage_kind(k, fa, st);
 		}
+		if(tuning)
+			cudaEventRecord(tn.ev[nk], st);
 	}
-	cudaEventRecordWithFlags(ctx->ev_c, st, evf);
-	if(tv) cudaEventRecord(tv[2], st);
+	cudaEventRecordWithFlags(sl.tev[2], st, evf);
 	if(ctx->f8)
 		for(const auto &g : ctx->xgroups)
 			launch_quant_fp8(g.shape, ctx->d_plans, g.d_idx, g.nf, ctx->T, (const uint32_t *)ctx->d_specn, ctx->d_spec8, st);
-	for(const auto &g : ctx->xgroups)
+	for(size_t gi = 0; gi < ctx->xgroups.size(); gi++)
 	{
+		const auto &g = ctx->xgroups[gi];
+		TcShape sh = g.shape;
+		if(tuning)
+		{
+			cudaEventRecord(tn.ev[nk + 1 + gi], st);
+			if(ctx->tc && !tn.xc[gi].empty())
+			{
+				const auto &c = tn.xc[gi][tn.iter % tn.xc[gi].size()];
+				tc_stages(&sh, c.first, c.second);
+			}
+		}
 		if(ctx->tc)
-			launch_xmac_tc(g.tmap, g.shape, ctx->d_plans, g.d_idx, g.nf, ctx->nsm, ctx->d_err, ctx->d_acc, st);
+			launch_xmac_tc(g.tmap, sh, ctx->d_plans, g.d_idx, g.nf, ctx->nsm, ctx->d_err, ctx->d_acc, st);
 		else
 			launch_xmac_fp32v2(ctx->h_plans[g.plan0], ctx->d_plans, g.d_idx, g.nf, ctx->T, ctx->d_spec, ctx->d_acc, st);
 	}
+	if(tuning)
+		cudaEventRecord(tn.ev[nk + 1 + ctx->xgroups.size()], st);
 	launch_weights(ctx->d_bw, ctx->nbw, ctx->d_acw, ctx->nacw, ctx->d_params, ctx->T, ctx->d_bwacc, ctx->d_acwacc, st);
-	cudaEventRecordWithFlags(ctx->ev_d, st, evf);
-	if(tv) cudaEventRecord(tv[3], st);
+	cudaEventRecordWithFlags(sl.tev[3], st, evf);
+}
+
+// Reads one tuning subint's launch times (waits for it), and after the last
+// one keeps each kind's and group's fastest candidate.
+static void tune_collect(fxb_ctx *ctx)
+{
+	Tuner &t = ctx->tune;
+	const size_t nk = ctx->fkinds.size(), ng = ctx->xgroups.size();
+	if(cudaEventSynchronize(t.ev.back()) == cudaSuccess)
+	{
+		float ms = 0;
+		for(size_t i = 0; i < nk; i++)
+			if(cudaEventElapsedTime(&ms, t.ev[i], t.ev[i + 1]) == cudaSuccess)
+			{
+				float &best = t.fms[i][t.iter % t.fc.size()];
+				best = std::min(best, ms);
+			}
+		for(size_t g = 0; g < ng; g++)
+			if(!t.xc[g].empty() && cudaEventElapsedTime(&ms, t.ev[nk + 1 + g], t.ev[nk + 2 + g]) == cudaSuccess)
+			{
+				float &best = t.xms[g][t.iter % t.xc[g].size()];
+				best = std::min(best, ms);
+			}
+	}
+	cudaGetLastError();
+	if(++t.iter < t.total)
+		return;
+	for(size_t i = 0; i < nk; i++)
+	{
+		if(ctx->fkinds[i].tcfft)
+			continue;
+		const size_t c = std::min_element(t.fms[i].begin(), t.fms[i].end()) - t.fms[i].begin();
+		ctx->fkinds[i].tq = t.fc[c].first;
+		ctx->fkinds[i].items_fast = t.fc[c].second;
+	}
+	for(size_t g = 0; g < ng; g++)
+	{
+		if(t.xc[g].empty())
+			continue;
+		const size_t c = std::min_element(t.xms[g].begin(), t.xms[g].end()) - t.xms[g].begin();
+		tc_stages(&ctx->xgroups[g].shape, t.xc[g][c].first, t.xc[g][c].second);
+	}
+	t.done = true;
+	ctx->gen++;
 }
 
 // The slot's graph, captured (again) when missing or when the frame-validity
@@ -825,7 +945,7 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, cudaEv
 // for the context and leaves the stream as it was.
 static fxb_status slot_graph(fxb_ctx *ctx, Slot &sl)
 {
-	if(sl.gexec && sl.g_valid == ctx->d_valid && sl.g_stride == ctx->valid_stride)
+	if(sl.gexec && sl.g_valid == ctx->d_valid && sl.g_stride == ctx->valid_stride && sl.g_gen == ctx->gen)
 		return FXB_OK;
 	if(sl.gexec)
 	{
@@ -833,7 +953,7 @@ static fxb_status slot_graph(fxb_ctx *ctx, Slot &sl)
 		sl.gexec = nullptr;
 	}
 	CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-	launch_compute(ctx, sl, ctx->stream, nullptr, true);
+	launch_compute(ctx, sl, ctx->stream, true);
 	cudaGraph_t g = nullptr;
 	cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
 	if(e == cudaSuccess)
@@ -849,6 +969,7 @@ static fxb_status slot_graph(fxb_ctx *ctx, Slot &sl)
 	}
 	sl.g_valid = ctx->d_valid;
 	sl.g_stride = ctx->valid_stride;
+	sl.g_gen = ctx->gen;
 	return FXB_OK;
 }
 
@@ -867,30 +988,23 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 	Slot &sl = *slp;
 	cudaStream_t st = ctx->stream;
 	CK(ctx, cudaStreamWaitEvent(st, sl.copied, 0));
-	cudaEvent_t *tv = nullptr;
-	if(ctx->timing_on && ctx->tev_used + 4 <= 4 * 8192)
-	{
-		while(ctx->tev.size() < ctx->tev_used + 4)
-		{
-			cudaEvent_t e;
-			CK(ctx, cudaEventCreate(&e));
-			ctx->tev.push_back(e);
-		}
-		tv = &ctx->tev[ctx->tev_used];
-		ctx->tev_used += 4;
-	}
-	if(!tv && ctx->graphs)
+	const bool tuning = ctx->tune.iter < ctx->tune.total;
+	if(ctx->graphs && !tuning)
 	{
 		const fxb_status gs = slot_graph(ctx, sl);
 		if(gs != FXB_OK)
 			return gs;
 	}
-	if(!tv && ctx->graphs)
+	if(ctx->graphs && !tuning)
 		CK(ctx, cudaGraphLaunch(sl.gexec, st));
 	else
-		launch_compute(ctx, sl, st, tv, false);
+		launch_compute(ctx, sl, st, false);
+	if(tuning)
+		tune_collect(ctx);
 	CK(ctx, cudaGetLastError());
 	CK(ctx, cudaEventRecord(sl.done, st));
+	sl.tpending = ctx->timing_on;
+	ctx->last_slot = (int)(slp - ctx->slots.data());
 	ctx->timed = true;
 	return FXB_OK;
 }
@@ -899,6 +1013,95 @@ fxb_status fxb_set_graphs(fxb_ctx *ctx, int32_t on)
 {
 	if(!ctx) return FXB_ERR_ARG;
 	ctx->graphs = on != 0;
+	return FXB_OK;
+}
+
+fxb_status fxb_autotune(fxb_ctx *ctx, int32_t rounds)
+{
+	if(!ctx || rounds < 0)
+		return FXB_ERR_ARG;
+	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	Tuner &t = ctx->tune;
+	for(cudaEvent_t e : t.ev)
+		if(e) cudaEventDestroy(e);
+	t = Tuner();
+	if(rounds == 0)
+		return FXB_OK;
+	const size_t nk = ctx->fkinds.size(), ng = ctx->xgroups.size();
+	t.fc = {{4, 1}, {4, 0}, {2, 1}, {2, 0}, {1, 1}, {1, 0}};
+	t.fms.assign(nk, std::vector<float>(t.fc.size(), 1e30f));
+	t.xc.assign(ng, {});
+	size_t most = t.fc.size();
+	for(size_t g = 0; g < ng && ctx->tc; g++)
+	{
+		static const int depth[][2] = {{6, 4}, {6, 3}, {4, 3}, {4, 2}, {3, 2}, {2, 2}};
+		for(const auto &d : depth)
+		{
+			TcShape sh = ctx->xgroups[g].shape;
+			if(tc_stages(&sh, d[0], d[1]))
+				t.xc[g].push_back({d[0], d[1]});
+		}
+		most = std::max(most, t.xc[g].size());
+	}
+	t.xms.assign(ng, std::vector<float>(most, 1e30f));
+	t.ev.assign(nk + ng + 2, nullptr);
+	for(cudaEvent_t &e : t.ev)
+		CK(ctx, cudaEventCreate(&e));
+	t.total = rounds * (int)most;
+	return FXB_OK;
+}
+
+fxb_status fxb_tuning_report(const fxb_ctx *ctx, char *buf, size_t len, size_t *needed)
+{
+	if(!ctx)
+		return FXB_ERR_ARG;
+	const Tuner &t = ctx->tune;
+	std::string r;
+	char line[256];
+	for(size_t i = 0; i < ctx->fkinds.size(); i++)
+	{
+		const FKind &k = ctx->fkinds[i];
+		snprintf(line, sizeof(line), "fstage N=%d items=%d%s: %d FFT iterations per CTA, %s fastest", k.N, k.count,
+		         k.tcfft ? " tensor-core FFT" : "", k.tq, k.items_fast ? "items" : "times");
+		r += line;
+		if(t.done && !k.tcfft)
+			for(size_t c = 0; c < t.fc.size(); c++)
+			{
+				snprintf(line, sizeof(line), "%s(%d,%s) %.4f ms", c ? ", " : " | ", t.fc[c].first,
+				         t.fc[c].second ? "items" : "times", (double)t.fms[i][c]);
+				r += line;
+			}
+		r += "\n";
+	}
+	for(size_t g = 0; g < ctx->xgroups.size(); g++)
+	{
+		const TcShape &sh = ctx->xgroups[g].shape;
+		if(!ctx->tc)
+		{
+			snprintf(line, sizeof(line), "xmac group %zu: FP32 form\n", g);
+			r += line;
+			continue;
+		}
+		snprintf(line, sizeof(line), "xmac group %zu (%d inputs, %d channels): rings %d raw / %d operand", g, sh.nrow,
+		         sh.nchan, sh.nrs, sh.nas);
+		r += line;
+		if(t.done)
+			for(size_t c = 0; c < t.xc[g].size(); c++)
+			{
+				snprintf(line, sizeof(line), "%s(%d,%d) %.4f ms", c ? ", " : " | ", t.xc[g][c].first, t.xc[g][c].second,
+				         (double)t.xms[g][c]);
+				r += line;
+			}
+		r += "\n";
+	}
+	if(needed)
+		*needed = r.size() + 1;
+	if(buf && len)
+	{
+		const size_t n = std::min(len - 1, r.size());
+		memcpy(buf, r.data(), n);
+		buf[n] = 0;
+	}
 	return FXB_OK;
 }
 
@@ -1049,13 +1252,14 @@ fxb_status fxb_reset(fxb_ctx *ctx)
 
 fxb_status fxb_last_timing(const fxb_ctx *ctx, float *fstage_ms, float *xmac_ms, float *total_ms)
 {
-	if(!ctx || !ctx->timed) return FXB_ERR_STATE;
+	if(!ctx || !ctx->timed || ctx->last_slot < 0) return FXB_ERR_STATE;
 	fxb_ctx *c = const_cast<fxb_ctx *>(ctx);
-	CK(c, cudaEventSynchronize(ctx->ev_d));
+	const Slot &sl = ctx->slots[ctx->last_slot];
+	CK(c, cudaEventSynchronize(sl.tev[3]));
 	float a = 0, b = 0, t = 0;
-	CK(c, cudaEventElapsedTime(&a, ctx->ev_b, ctx->ev_c));
-	CK(c, cudaEventElapsedTime(&b, ctx->ev_c, ctx->ev_d));
-	CK(c, cudaEventElapsedTime(&t, ctx->ev_a, ctx->ev_d));
+	CK(c, cudaEventElapsedTime(&a, sl.tev[1], sl.tev[2]));
+	CK(c, cudaEventElapsedTime(&b, sl.tev[2], sl.tev[3]));
+	CK(c, cudaEventElapsedTime(&t, sl.tev[0], sl.tev[3]));
 	if(fstage_ms) *fstage_ms = a;
 	if(xmac_ms) *xmac_ms = b;
 	if(total_ms) *total_ms = t;
@@ -1066,8 +1270,11 @@ fxb_status fxb_timing_enable(fxb_ctx *ctx, int32_t on)
 {
 	if(!ctx) return FXB_ERR_ARG;
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
+	for(Slot &sl : ctx->slots)
+		sl.tpending = false;
 	ctx->timing_on = on != 0;
-	ctx->tev_used = 0;
+	ctx->t_prep = ctx->t_f = ctx->t_x = 0;
+	ctx->t_n = 0;
 	return FXB_OK;
 }
 
@@ -1075,22 +1282,14 @@ fxb_status fxb_timing_read(fxb_ctx *ctx, int32_t *nsubint, double *prep_ms, doub
 {
 	if(!ctx) return FXB_ERR_ARG;
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
-	double p = 0, f = 0, x = 0;
-	for(size_t i = 0; i + 4 <= ctx->tev_used; i += 4)
-	{
-		float a = 0, b = 0, c = 0;
-		CK(ctx, cudaEventElapsedTime(&a, ctx->tev[i], ctx->tev[i + 1]));
-		CK(ctx, cudaEventElapsedTime(&b, ctx->tev[i + 1], ctx->tev[i + 2]));
-		CK(ctx, cudaEventElapsedTime(&c, ctx->tev[i + 2], ctx->tev[i + 3]));
-		p += a;
-		f += b;
-		x += c;
-	}
-	if(nsubint) *nsubint = (int32_t)(ctx->tev_used / 4);
-	if(prep_ms) *prep_ms = p;
-	if(fstage_ms) *fstage_ms = f;
-	if(xmac_ms) *xmac_ms = x;
-	ctx->tev_used = 0;
+	for(Slot &sl : ctx->slots)
+		slot_account(ctx, sl);
+	if(nsubint) *nsubint = ctx->t_n;
+	if(prep_ms) *prep_ms = ctx->t_prep;
+	if(fstage_ms) *fstage_ms = ctx->t_f;
+	if(xmac_ms) *xmac_ms = ctx->t_x;
+	ctx->t_prep = ctx->t_f = ctx->t_x = 0;
+	ctx->t_n = 0;
 	return FXB_OK;
 }
 
@@ -1230,6 +1429,7 @@ struct fxb_batch {
 	std::vector<cudaGraphExec_t> gexec;               // [slot]
 	std::vector<std::vector<const uint8_t *>> g_valid; // [slot][member] validity arrays captured with
 	std::vector<std::vector<int64_t>> g_stride;
+	std::vector<std::vector<int>> g_gen;
 	bool graphs = true;
 	std::string err;
 };
@@ -1266,7 +1466,8 @@ static fxb_status batch_graph(fxb_batch *b, int k, const std::vector<Slot *> &sl
 	const size_t n = b->m.size();
 	bool ok = b->gexec[k] != nullptr;
 	for(size_t i = 0; ok && i < n; i++)
-		ok = b->g_valid[k][i] == b->m[i]->d_valid && b->g_stride[k][i] == b->m[i]->valid_stride;
+		ok = b->g_valid[k][i] == b->m[i]->d_valid && b->g_stride[k][i] == b->m[i]->valid_stride &&
+		     b->g_gen[k][i] == b->m[i]->gen;
 	if(ok)
 		return FXB_OK;
 	if(b->gexec[k])
@@ -1274,14 +1475,18 @@ static fxb_status batch_graph(fxb_batch *b, int k, const std::vector<Slot *> &sl
 		cudaGraphExecDestroy(b->gexec[k]);
 		b->gexec[k] = nullptr;
 	}
+	// one fork for all members, then every join: the branches are independent
 	BK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+	cudaEventRecord(b->fork, b->stream);
 	for(size_t i = 0; i < n; i++)
 	{
 		fxb_ctx *c = b->m[i];
-		cudaEventRecord(b->fork, b->stream);
 		cudaStreamWaitEvent(c->stream, b->fork, 0);
-		launch_compute(c, *slots[i], c->stream, nullptr, true);
-		cudaEventRecord(b->join[i], c->stream);
+		launch_compute(c, *slots[i], c->stream, true);
+	}
+	for(size_t i = 0; i < n; i++)
+	{
+		cudaEventRecord(b->join[i], b->m[i]->stream);
 		cudaStreamWaitEvent(b->stream, b->join[i], 0);
 	}
 	cudaGraph_t g = nullptr;
@@ -1301,6 +1506,7 @@ static fxb_status batch_graph(fxb_batch *b, int k, const std::vector<Slot *> &sl
 	{
 		b->g_valid[k][i] = b->m[i]->d_valid;
 		b->g_stride[k][i] = b->m[i]->valid_stride;
+		b->g_gen[k][i] = b->m[i]->gen;
 	}
 	return FXB_OK;
 }
@@ -1328,6 +1534,7 @@ fxb_batch *fxb_batch_create(fxb_ctx *const *members, int32_t n, fxb_status *stat
 	b->gexec.assign(nslot, nullptr);
 	b->g_valid.assign(nslot, std::vector<const uint8_t *>(n, nullptr));
 	b->g_stride.assign(nslot, std::vector<int64_t>(n, 0));
+	b->g_gen.assign(nslot, std::vector<int>(n, -1));
 	b->join.assign(n, nullptr);
 	bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
 	          cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
@@ -1345,7 +1552,7 @@ fxb_batch *fxb_batch_create(fxb_ctx *const *members, int32_t n, fxb_status *stat
 	return b;
 }
 
-fxb_status fxb_batch_submit(fxb_batch *b, const fxb_member_subint *data, int32_t sec, int32_t ns)
+static fxb_status batch_submit(fxb_batch *b, const fxb_member_subint *data, int32_t sec, int32_t ns, bool device)
 {
 	if(!b || !data)
 		return FXB_ERR_ARG;
@@ -1377,7 +1584,7 @@ fxb_status fxb_batch_submit(fxb_batch *b, const fxb_member_subint *data, int32_t
 	{
 		fxb_ctx *c = b->m[i];
 		const fxb_member_subint &d = data[i];
-		const fxb_status rc = stage_subint(c, d.bufs, d.nbytes, d.datasec, d.datans, d.validflags, sec, ns, false,
+		const fxb_status rc = stage_subint(c, d.bufs, d.nbytes, d.datasec, d.datans, d.validflags, sec, ns, device,
 		                                   &slots[i]);
 		if(rc != FXB_OK)
 		{
@@ -1389,26 +1596,46 @@ fxb_status fxb_batch_submit(fxb_batch *b, const fxb_member_subint *data, int32_t
 		BK(b, cudaEventRecord(b->join[i], c->stream));
 		BK(b, cudaStreamWaitEvent(b->stream, b->join[i], 0));
 	}
-	if(b->graphs)
+	// a member still tuning runs eagerly (one member after the other, so
+	// that its launch times are its own)
+	bool tuning = false;
+	for(fxb_ctx *c : b->m)
+		tuning = tuning || c->tune.iter < c->tune.total;
+	if(b->graphs && !tuning)
 	{
 		const fxb_status rc = batch_graph(b, k, slots);
 		if(rc != FXB_OK)
 			return rc;
 	}
-	if(b->graphs)
+	if(b->graphs && !tuning)
 		BK(b, cudaGraphLaunch(b->gexec[k], b->stream));
 	else
 		for(size_t i = 0; i < n; i++)
-			launch_compute(b->m[i], *slots[i], b->stream, nullptr, false);
+			launch_compute(b->m[i], *slots[i], b->stream, false);
+	for(fxb_ctx *c : b->m)
+		if(c->tune.iter < c->tune.total)
+			tune_collect(c);
 	BK(b, cudaGetLastError());
 	BK(b, cudaEventRecord(b->done, b->stream));
 	for(size_t i = 0; i < n; i++)
 	{
 		BK(b, cudaEventRecord(slots[i]->done, b->stream));
 		BK(b, cudaStreamWaitEvent(b->m[i]->stream, b->done, 0));
+		slots[i]->tpending = b->m[i]->timing_on;
+		b->m[i]->last_slot = (int)(slots[i] - b->m[i]->slots.data());
 		b->m[i]->timed = true;
 	}
 	return FXB_OK;
+}
+
+fxb_status fxb_batch_submit(fxb_batch *b, const fxb_member_subint *data, int32_t sec, int32_t ns)
+{
+	return batch_submit(b, data, sec, ns, false);
+}
+
+fxb_status fxb_batch_submit_device(fxb_batch *b, const fxb_member_subint *data, int32_t sec, int32_t ns)
+{
+	return batch_submit(b, data, sec, ns, true);
 }
 
 fxb_status fxb_batch_sync(fxb_batch *b)
@@ -1428,6 +1655,22 @@ fxb_status fxb_batch_sync(fxb_batch *b)
 	return FXB_OK;
 }
 
+fxb_status fxb_batch_autotune(fxb_batch *b, int32_t rounds)
+{
+	if(!b)
+		return FXB_ERR_ARG;
+	for(fxb_ctx *c : b->m)
+	{
+		const fxb_status st = fxb_autotune(c, rounds);
+		if(st != FXB_OK)
+		{
+			b->err = c->err;
+			return st;
+		}
+	}
+	return FXB_OK;
+}
+
 fxb_status fxb_batch_set_graphs(fxb_batch *b, int32_t on)
 {
 	if(!b) return FXB_ERR_ARG;
@@ -1436,6 +1679,13 @@ fxb_status fxb_batch_set_graphs(fxb_batch *b, int32_t on)
 }
 
 const char *fxb_batch_last_error(const fxb_batch *b) { return b ? b->err.c_str() : ""; }
+
+fxb_status fxb_batch_get_stream(const fxb_batch *b, void **stream)
+{
+	if(!b || !stream) return FXB_ERR_ARG;
+	*stream = (void *)b->stream;
+	return FXB_OK;
+}
 
 void fxb_batch_destroy(fxb_batch *b)
 {

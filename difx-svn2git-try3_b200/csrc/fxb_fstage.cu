@@ -688,6 +688,7 @@ bool fstage_plan(int N, int nb, int out, FKind *k)
 	k->smem = side * (k->pp ? 2 : 1);
 	k->tq = 4;
 	k->out = out;
+	k->items_fast = out == 1 ? 1 : 0;
 	k->twn = tw_offset(N, ilog2(N) / 3);
 	return k->smem <= 200 * 1024 && k->threads <= 512;
 }
@@ -767,7 +768,7 @@ void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream)
 	a.tq = k.tq;
 	a.pp = k.pp;
 	a.tw = k.tw;
-	a.items_fast = k.out == 1 ? 1 : 0;
+	a.items_fast = k.items_fast;
 	if(k.out == 1)
 		launch_n<hc, 1>(k, a, stream);
 	else if(k.nb == 2)

@@ -74,6 +74,7 @@ struct FKind {
 	int32_t kb, fpc;         // radix-8 butterflies per thread and pass, FFTs side by side per CTA
 	int32_t threads, tq;     // CTA size, FFT iterations per CTA
 	int32_t pp, out;         // two exchange buffers (else one), output form (0 FP32, 1 FP16 FFT -> bf16x2)
+	int32_t items_fast;      // grid order: work items fastest (else time chunks); scheduling only
 	int32_t twn, tcfft;      // twiddle entries of length N; 1: tensor-core FFT kernel (fxb_fstage_tc.cu)
 	size_t smem;
 	const void *tw;          // twiddle table of length N (make_fstage_twiddles layout)
@@ -125,6 +126,9 @@ struct TcShape {
 	size_t smem;
 };
 bool tc_shape(int nrow, int nchan, int T, bool f8, TcShape *s);
+// set the raw / operand ring depths of a shape (and its shared-memory plan);
+// false if they do not fit in 227 KB
+bool tc_stages(TcShape *s, int nrs, int nas);
 bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf);
 size_t tc_tensormap_size();
 void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf,

@@ -627,22 +627,27 @@ bool tc_shape(int nrow, int nchan, int T, bool f8, TcShape *s)
 	s->raw_bytes = f8 ? s->w8 * kKT8 * 2 : s->CB * nrow * kKT * 4;
 	s->raw_stride = (s->raw_bytes + 1023) & ~1023;
 	s->dstride = s->r2p + 4;
-	const size_t dump = (size_t)s->CB * 2 * nrow * s->dstride * 4;
 	// deepest rings that fit beside the accumulator copy
 	static const int order[][2] = {{6, 4}, {6, 3}, {5, 3}, {5, 2}, {4, 2}, {3, 2}, {2, 2}};
 	for(const auto &o : order)
-	{
-		const size_t rings = (size_t)o[0] * s->raw_stride + (size_t)o[1] * kNG * kTileBytes;
-		if(1024 + rings + dump <= 227 * 1024)
-		{
-			s->nrs = o[0];
-			s->nas = o[1];
-			s->dump_off = (int32_t)rings;
-			s->smem = 1024 + rings + dump;
+		if(tc_stages(s, o[0], o[1]))
 			return true;
-		}
-	}
 	return false;
+}
+
+bool tc_stages(TcShape *s, int nrs, int nas)
+{
+	if(nrs < 1 || nrs > kRS || nas < 1 || nas > kAS)
+		return false;
+	const size_t dump = (size_t)s->CB * 2 * s->nrow * s->dstride * 4;
+	const size_t rings = (size_t)nrs * s->raw_stride + (size_t)nas * kNG * kTileBytes;
+	if(1024 + rings + dump > 227 * 1024)
+		return false;
+	s->nrs = nrs;
+	s->nas = nas;
+	s->dump_off = (int32_t)rings;
+	s->smem = 1024 + rings + dump;
+	return true;
 }
 
 // 3D map over one group's spectra [nf * Tpad][nblk][nrow * CB] of 4-byte

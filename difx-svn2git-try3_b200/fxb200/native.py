@@ -152,13 +152,23 @@ def lib():
     L.fxb_read_results_device.argtypes = [vp, ctypes.c_void_p, ctypes.c_size_t]
     L.fxb_set_graphs.argtypes = [vp, i32]
     L.fxb_set_graphs.restype = ctypes.c_int
+    L.fxb_autotune.argtypes = [vp, i32]
+    L.fxb_autotune.restype = ctypes.c_int
+    L.fxb_tuning_report.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+    L.fxb_tuning_report.restype = ctypes.c_int
+    L.fxb_batch_autotune.argtypes = [vp, i32]
+    L.fxb_batch_autotune.restype = ctypes.c_int
     L.fxb_batch_create.restype = vp
     L.fxb_batch_create.argtypes = [ctypes.POINTER(vp), i32, i32p]
     L.fxb_batch_submit.argtypes = [vp, ctypes.POINTER(FxbMemberSubint), i32, i32]
+    L.fxb_batch_submit_device.argtypes = [vp, ctypes.POINTER(FxbMemberSubint), i32, i32]
+    L.fxb_batch_submit_device.restype = ctypes.c_int
     L.fxb_batch_sync.argtypes = [vp]
     L.fxb_batch_set_graphs.argtypes = [vp, i32]
     for name in ("fxb_batch_submit", "fxb_batch_sync", "fxb_batch_set_graphs"):
         getattr(L, name).restype = ctypes.c_int
+    L.fxb_batch_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
+    L.fxb_batch_get_stream.restype = ctypes.c_int
     L.fxb_batch_last_error.restype = ctypes.c_char_p
     L.fxb_batch_last_error.argtypes = [vp]
     L.fxb_batch_destroy.argtypes = [vp]
@@ -288,6 +298,17 @@ class Correlator:
         """Replay each slot's subint kernels as a CUDA graph (default) or launch them one by one."""
         check(lib().fxb_set_graphs(self.ctx, 1 if on else 0), self.ctx, "set_graphs")
 
+    def autotune(self, rounds: int = 2):
+        """Time the scheduling candidates over the next subints and keep the fastest (fxb_autotune)."""
+        check(lib().fxb_autotune(self.ctx, rounds), self.ctx, "autotune")
+
+    def tuning_report(self) -> str:
+        need = ctypes.c_size_t(0)
+        check(lib().fxb_tuning_report(self.ctx, None, 0, ctypes.byref(need)), self.ctx, "tuning_report")
+        buf = ctypes.create_string_buffer(need.value)
+        check(lib().fxb_tuning_report(self.ctx, buf, need.value, None), self.ctx, "tuning_report")
+        return buf.value.decode()
+
     def results_into(self, out: np.ndarray) -> np.ndarray:
         check(lib().fxb_read_results(self.ctx, _fptr(out), out.size), self.ctx, "read_results")
         return out
@@ -382,25 +403,43 @@ class Batch:
             m = lib().fxb_batch_last_error(self.b)
             raise FxbError("%s failed: %s %s" % (what, FXB_STATUS.get(rc, rc), m.decode() if m else ""))
 
-    def submit(self, member_inputs: Sequence[List[Tuple[np.ndarray, int, int]]], sec: int, ns: int) -> None:
-        """member_inputs[i]: member i's [(buffer, datasec, datans)] per station."""
+    def _records(self, member_ptrs):
         keep, recs = [], (FxbMemberSubint * len(self.members))()
-        for i, inputs in enumerate(member_inputs):
-            n = len(inputs)
-            bufs = (ctypes.c_void_p * n)(*[b.ctypes.data for b, _, _ in inputs])
-            nb = (ctypes.c_int64 * n)(*[b.size for b, _, _ in inputs])
-            ds = (ctypes.c_int32 * n)(*[x for _, x, _ in inputs])
-            dn = (ctypes.c_int32 * n)(*[x for _, _, x in inputs])
+        for i, (ptrs, nbytes, dsec, dns) in enumerate(member_ptrs):
+            n = len(ptrs)
+            bufs = (ctypes.c_void_p * n)(*ptrs)
+            nb = (ctypes.c_int64 * n)(*nbytes)
+            ds = (ctypes.c_int32 * n)(*dsec)
+            dn = (ctypes.c_int32 * n)(*dns)
             keep += [bufs, nb, ds, dn]
             recs[i].bufs, recs[i].nbytes, recs[i].datasec, recs[i].datans = bufs, nb, ds, dn
             recs[i].validflags = None
+        return keep, recs
+
+    def submit(self, member_inputs: Sequence[List[Tuple[np.ndarray, int, int]]], sec: int, ns: int) -> None:
+        """member_inputs[i]: member i's [(buffer, datasec, datans)] per station."""
+        keep, recs = self._records([([b.ctypes.data for b, _, _ in inp], [b.size for b, _, _ in inp],
+                                     [x for _, x, _ in inp], [x for _, _, x in inp]) for inp in member_inputs])
         self._check(lib().fxb_batch_submit(self.b, recs, sec, ns), "batch_submit")
+
+    def submit_device(self, member_ptrs, sec: int, ns: int) -> None:
+        """member_ptrs[i]: (device pointers, nbytes, datasec, datans) of member i's stations."""
+        keep, recs = self._records(member_ptrs)
+        self._check(lib().fxb_batch_submit_device(self.b, recs, sec, ns), "batch_submit_device")
 
     def sync(self):
         self._check(lib().fxb_batch_sync(self.b), "batch_sync")
 
     def set_graphs(self, on: bool = True):
         self._check(lib().fxb_batch_set_graphs(self.b, 1 if on else 0), "batch_set_graphs")
+
+    def autotune(self, rounds: int = 2):
+        self._check(lib().fxb_batch_autotune(self.b, rounds), "batch_autotune")
+
+    def stream(self) -> int:
+        v = ctypes.c_void_p(0)
+        self._check(lib().fxb_batch_get_stream(self.b, ctypes.byref(v)), "batch_get_stream")
+        return v.value or 0
 
     def close(self):
         if getattr(self, "b", None):

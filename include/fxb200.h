@@ -141,9 +141,22 @@ FXB_API fxb_status fxb_submit_subint_device(fxb_ctx *ctx, const uint8_t *const *
 FXB_API fxb_status fxb_sync(fxb_ctx *ctx);
 
 /* Each staging slot's subint kernels are captured once into a CUDA graph and
- * replayed (default on; kernels are launched one by one while per-subint
- * timing is enabled).  on = 0 launches them one by one always. */
+ * replayed (default on); on = 0 launches them one by one. */
 FXB_API fxb_status fxb_set_graphs(fxb_ctx *ctx, int32_t on);
+
+/* Online autotuning of the kernels' scheduling: the next rounds x C subints
+ * (C candidates, at most 6) run eagerly with every launch timed, each F-stage
+ * kind trying FFT iterations per CTA (4, 2, 1) x grid order and each
+ * tensor-core XMAC group its ring depths; then each keeps its fastest
+ * candidate and the graphs are captured again.  No candidate changes the
+ * arithmetic: results are identical whatever is chosen.  rounds = 0 stops
+ * tuning (the choices made so far stay).  Without tuning, the F stage takes
+ * as many FFT iterations per CTA as leave two CTAs per SM. */
+FXB_API fxb_status fxb_autotune(fxb_ctx *ctx, int32_t rounds);
+/* The current choices (and, after tuning, each candidate's fastest time) as
+ * text, one line per F-stage kind and XMAC group; *needed = bytes with the
+ * terminating 0. */
+FXB_API fxb_status fxb_tuning_report(const fxb_ctx *ctx, char *buf, size_t len, size_t *needed);
 
 /* Batches: contexts whose subints are submitted together, e.g. one context
  * per subband shape (bandwidth, channels, bits) of an observation whose
@@ -160,12 +173,20 @@ typedef struct {
 	const int32_t *datasec, *datans;  /* [nstation] start of each buffer */
 	const int32_t *const *validflags; /* [nstation] or NULL */
 } fxb_member_subint;
+/* Destroy a batch before any of its members. */
 FXB_API fxb_batch *fxb_batch_create(fxb_ctx *const *members, int32_t nmember, fxb_status *status);
 /* data[nmember]: every member's buffers of the subint starting at (sec, ns). */
 FXB_API fxb_status fxb_batch_submit(fxb_batch *batch, const fxb_member_subint *data, int32_t sec, int32_t ns);
+/* As fxb_batch_submit with every station buffer in device memory (valid
+ * until the next fxb_batch_sync), as fxb_submit_subint_device. */
+FXB_API fxb_status fxb_batch_submit_device(fxb_batch *batch, const fxb_member_subint *data, int32_t sec, int32_t ns);
 FXB_API fxb_status fxb_batch_sync(fxb_batch *batch);
 FXB_API fxb_status fxb_batch_set_graphs(fxb_batch *batch, int32_t on);
+/* fxb_autotune on every member (members still tuning run eagerly). */
+FXB_API fxb_status fxb_batch_autotune(fxb_batch *batch, int32_t rounds);
 FXB_API const char *fxb_batch_last_error(const fxb_batch *batch);
+/* The cudaStream_t (as void*) of the batch's graph launches. */
+FXB_API fxb_status fxb_batch_get_stream(const fxb_batch *batch, void **stream);
 FXB_API void fxb_batch_destroy(fxb_batch *batch);
 
 /* Number of complex values in the core-result buffer
@@ -197,11 +218,13 @@ FXB_API fxb_status fxb_reset(fxb_ctx *ctx);
  * measured with CUDA events on the context's stream. */
 FXB_API fxb_status fxb_last_timing(const fxb_ctx *ctx, float *fstage_ms, float *xmac_ms, float *total_ms);
 
-/* Per-subint kernel timing: while enabled, every submitted subint records
- * CUDA events on the context's stream; fxb_timing_read synchronises and
- * returns the number of subints and the summed device time of the FP64
- * delay/parameter kernels (prep), the F-stage kernel and the XMAC + weight
- * kernels, then clears the record. */
+/* Per-subint kernel timing: every subint records four CUDA events on the
+ * stream that runs it (event-record nodes of the graph when graphs are on);
+ * while timing is enabled their intervals are summed as slots come round
+ * again.  fxb_timing_read synchronises and returns the number of subints
+ * and the summed device time of the FP64 delay/parameter kernels (prep),
+ * the F stage and the XMAC (with the FP8 quantisation and the weight
+ * kernels), then clears the sums. */
 FXB_API fxb_status fxb_timing_enable(fxb_ctx *ctx, int32_t on);
 FXB_API fxb_status fxb_timing_read(fxb_ctx *ctx, int32_t *nsubint, double *prep_ms, double *fstage_ms,
                                    double *xmac_ms);

@@ -119,3 +119,70 @@ def test_member_refuses_its_own_submit_while_batched():
     members[0].sync()
     for m in members:
         m.close()
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_kernel_timing_counts_every_subint(graphs):
+    job = small_job(nstation=4, nchan=256, bw=16.0, nfreq=2, full_pol=True, subint_ns=SUBINT_NS)
+    c = Correlator(job, xmac="bf16")
+    c.set_graphs(graphs)
+    c.timing_enable(True)
+    for sec, ns in SUBINTS:
+        c.submit(_inputs(job, 0, sec, ns), sec, ns)
+    n, prep, fst, xm = c.timing_read()
+    f_last, x_last, total = c.timing()
+    c.close()
+    assert n == len(SUBINTS)
+    assert prep > 0 and fst > 0 and xm > 0
+    assert 0 < f_last <= total and 0 < x_last <= total
+
+
+def _many(job, k, c, n):
+    for j in range(n):
+        sec, ns = 0, (j + 1) * SUBINT_NS
+        c.submit(_inputs(job, k, sec, ns), sec, ns)
+
+
+@pytest.mark.parametrize("xmac", ["fp32", "bf16", "fp8"])
+def test_autotuned_result_is_identical(xmac):
+    # the tuner tries 6 candidates per round: 2 rounds take 12 subints
+    job = small_job(nstation=4, nchan=256, bw=16.0, nfreq=2, full_pol=True, subint_ns=SUBINT_NS)
+    plain = Correlator(job, xmac=xmac)
+    _many(job, 0, plain, 14)
+    ref = plain.results()
+    plain.close()
+    tuned = Correlator(job, xmac=xmac)
+    tuned.autotune(2)
+    _many(job, 0, tuned, 14)
+    got = tuned.results()
+    report = tuned.tuning_report()
+    tuned.close()
+    assert np.array_equal(got, ref)
+    assert "fstage N=512" in report and " ms" in report
+    if xmac != "fp32":
+        assert "xmac group 0" in report and "rings" in report
+
+
+def test_batch_autotune_keeps_results():
+    jobs = _uneven_jobs()
+    alone = []
+    for k, j in enumerate(jobs):
+        c = Correlator(j, xmac="bf16")
+        _many(j, k, c, 13)
+        alone.append(c.results())
+        c.close()
+    members = [Correlator(j, xmac="bf16") for j in jobs]
+    batch = Batch(members)
+    batch.autotune(2)
+    for n in range(13):
+        sec, ns = 0, (n + 1) * SUBINT_NS
+        batch.submit([_inputs(j, k, sec, ns) for k, j in enumerate(jobs)], sec, ns)
+    batch.sync()
+    got = [m.results() for m in members]
+    reports = [m.tuning_report() for m in members]
+    batch.close()
+    for m in members:
+        m.close()
+    for g, r in zip(got, alone):
+        assert np.array_equal(g, r)
+    assert all(" ms" in rp for rp in reports)
