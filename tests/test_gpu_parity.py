@@ -135,3 +135,13 @@ def test_layout_without_gpu_matches_context():
     corr = Correlator(job)
     assert np.array_equal(lay, corr.layout()) and n == corr.corelen
     corr.close()
+
+
+@pytest.mark.parametrize("nchan", [2048, 4096, 8192])
+def test_long_ffts(nchan):
+    # 4096-, 8192- and 16384-point FFTs: several butterflies per thread, one
+    # band per work item in the FP32 form
+    job = small_job(nstation=3, nchan=nchan, bw=16.0, nfreq=2, full_pol=True, subint_ns=2_048_000)
+    got, ref, layout, n, w, wref = run_both(job, [(0, 2_048_000), (0, 4_096_000)])
+    compare_core(job, layout, n, got, ref)
+    assert np.array_equal(w, wref)

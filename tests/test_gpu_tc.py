@@ -133,3 +133,15 @@ def test_fp8_tensor_core_vs_fp64(kw):
     cross_err, auto_err = tc_errors(job, layout, n, got, ref)
     assert cross_err <= FP8_TOL, cross_err
     assert auto_err <= FP8_TOL, auto_err
+
+
+@pytest.mark.parametrize("nchan", [2048, 4096, 8192])
+def test_bf16_long_ffts_vs_fp64(nchan):
+    # the FP16 FFT's rounding over 12..14 radix stages averages down with the
+    # number of FFTs integrated: 8.192 ms subints give 8..32 per subint (a 1 s
+    # integration has 60..250 times more)
+    job = small_job(nstation=3, nchan=nchan, bw=16.0, nfreq=2, full_pol=True, subint_ns=8_192_000)
+    got, ref, layout, n = run_tc(job, [(0, 8_192_000), (0, 16_384_000)])
+    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
+    assert cross_err <= TC_TOL, cross_err
+    assert auto_err <= TC_TOL, auto_err
