@@ -1300,6 +1300,44 @@ fxb_status fxb_get_stream(const fxb_ctx *ctx, void **stream)
 	return FXB_OK;
 }
 
+static fxb_status job_of(const fxb_job_desc *desc, Job &job)
+{
+	if(!desc) return FXB_ERR_ARG;
+	std::string err;
+	fxb_status st = FXB_OK;
+	if(!build_job(desc, job, err, st))
+	{
+		std::lock_guard<std::mutex> lk(g_err_mutex);
+		g_create_err = err;
+		return st;
+	}
+	return FXB_OK;
+}
+
+fxb_status fxb_vis_calibrate(const fxb_job_desc *desc, const fxb_vis_params *params, float *coreresult)
+{
+	Job job;
+	const fxb_status st = job_of(desc, job);
+	return st != FXB_OK ? st : vis_calibrate(job, params, coreresult);
+}
+
+fxb_status fxb_vis_write_swin(const fxb_job_desc *desc, const fxb_vis_params *params, const float *coreresult,
+                              const char *dir)
+{
+	Job job;
+	fxb_status st = job_of(desc, job);
+	if(st != FXB_OK)
+		return st;
+	std::string err;
+	st = vis_swin_write(job, params, coreresult, dir, err);
+	if(st != FXB_OK)
+	{
+		std::lock_guard<std::mutex> lk(g_err_mutex);
+		g_create_err = err;
+	}
+	return st;
+}
+
 void *fxb_host_alloc(size_t bytes, fxb_status *status)
 {
 	void *p = nullptr;

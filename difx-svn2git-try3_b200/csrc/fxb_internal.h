@@ -141,6 +141,11 @@ struct Job {
 
 bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st);
 
+// integration output (fxb_vis.cpp)
+fxb_status vis_calibrate(const Job &job, const fxb_vis_params *p, float *coreresult);
+fxb_status vis_swin_write(const Job &job, const fxb_vis_params *p, const float *coreresult, const char *dir,
+                          std::string &err);
+
 // fxb_create with the context's device memory taken from a cudaMemPool_t
 // (passed as void*; null: the device's default pool).  A server's pool keeps
 // its memory mapped between jobs, so that creating and destroying contexts

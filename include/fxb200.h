@@ -229,6 +229,36 @@ FXB_API fxb_status fxb_timing_enable(fxb_ctx *ctx, int32_t on);
 FXB_API fxb_status fxb_timing_read(fxb_ctx *ctx, int32_t *nsubint, double *prep_ms, double *fstage_ms,
                                    double *xmac_ms);
 
+/* ---- integration output (Visibility::writedata / writedifx,
+ * mpifxcorr/src/visibility.cpp:348-620, 716-900, 1060-1140).  A context's
+ * accumulators hold the sum of every subint since fxb_reset -- the
+ * reference's Visibility::addData (visibility.cpp:181-194) -- so an
+ * integration is: reset, submit its subints, fxb_read_results, then the two
+ * calls below on that buffer. */
+typedef struct {
+	double int_time_s;            /* INT TIME (SEC) of the configuration */
+	int32_t start_mjd, start_sec; /* START MJD / START SECONDS of the job */
+	int32_t scan_start_sec;       /* scan start, seconds after the job start */
+	int32_t int_start_sec;        /* integration start within the scan: seconds */
+	int32_t int_start_ns;         /*   and nanoseconds */
+	int32_t config_index, source_index;
+	const double *tsys;           /* [ndatastream] a-priori Tsys (TSYS), NULL: none */
+	const int32_t *telescope;     /* [ndatastream] telescope index, NULL: the datastream index */
+	const double *uvw;            /* [nbaseline * 3] u, v, w (m) at the integration centre, NULL: 0 */
+} fxb_vis_params;
+/* Amplitude-calibrate an integrated core result of the job in place:
+ * baseline and autocorrelation weights normalised by the FFTs per
+ * integration, products scaled to correlation coefficients, or with Tsys by
+ * the band-averaged autocorrelations and the quantisation decorrelation
+ * (weights stay raw).  Needs no GPU: the caller may be the process that
+ * writes the output rather than the one correlating. */
+FXB_API fxb_status fxb_vis_calibrate(const fxb_job_desc *desc, const fxb_vis_params *params, float *coreresult);
+/* Append the calibrated integration to <dir>/DIFX_<mjd>_<sec>.s0000.b0000 as
+ * SWIN records: every baseline product with weight > 0, then every
+ * autocorrelation with weight > 0 (message via fxb_last_error(NULL)). */
+FXB_API fxb_status fxb_vis_write_swin(const fxb_job_desc *desc, const fxb_vis_params *params, const float *coreresult,
+                                      const char *dir);
+
 /* Page-locked host memory for station buffers: fxb_submit_subint copies from
  * it asynchronously at full link speed, where a pageable buffer is staged by
  * the driver on the calling thread.  Free with fxb_host_free. */

@@ -23,7 +23,7 @@ def _kv(key: str, val) -> str:
 def write_job_files(job: Job, outdir: str, name: str = "job",
                     xmac_stride: int = 0, array_stride: int = 0,
                     ac_avg_ns: int = 2_000_000_000, uvshift_ns: int = 2_000_000_000,
-                    scan_dur_s: int = 100) -> str:
+                    scan_dur_s: int = 100, tsys=None) -> str:
     job.validate()
     os.makedirs(outdir, exist_ok=True)
     base = os.path.join(os.path.abspath(outdir), name)
@@ -89,7 +89,8 @@ def write_job_files(job: Job, outdir: str, name: str = "job",
     s.append(_kv("NUM DATA SEGMENTS", 8))
     for i, st in enumerate(job.stations):
         s.append(_kv("TELESCOPE INDEX", i))
-        s.append(_kv("TSYS", "0.000000"))
+        ts = 0.0 if tsys is None else (tsys[i] if hasattr(tsys, "__len__") else tsys)
+        s.append(_kv("TSYS", "%.6f" % ts))
         s.append(_kv("DATA FORMAT", "VDIF"))
         s.append(_kv("QUANTISATION BITS", st.nbits))
         s.append(_kv("DATA FRAME SIZE", st.payload_bytes + st.header_bytes))

@@ -29,6 +29,7 @@
 #include <mutex>
 #include "configuration.h"
 #include "mode.h"
+#include "visibility.h"
 #include "mk5mode.h"
 #include "model.h"
 #include "mark5access.h"
@@ -435,6 +436,31 @@ int dref_unpack(const char *formatname, const unsigned char *data, int offsetsam
 	int good = mark5_unpack_with_offset(ms, data, offsetsamples, &ptrs[0], nsamp);
 	delete_mark5_stream(ms);
 	return good;
+}
+
+/* The reference's integration output: a Visibility for configuration 0 whose
+ * integration starts at the start of scan 0 (visibility.cpp:46-117) takes the
+ * nsub subint core results (2*corelen floats each) through addData, then
+ * writedata() calibrates them and appends the SWIN records to
+ * <OUTPUT FILENAME>/DIFX_<mjd>_<sec>.s0000.b0000 (visibility.cpp:348-900). */
+int dref_visibility_write(void *h, const float *const *subints, int nsub)
+{
+	RefJob *j = (RefJob *)h;
+	Configuration *c = j->config;
+	static const std::string pnames[4] = {"RR", "LL", "RL", "LR"};
+	const size_t nfl = 2 * (size_t)c->getMaxCoreResultLength();
+	std::vector<char> disk(nfl * 4 * 2 + (1 << 20));
+	Visibility v(c, 0, 1, disk.data(), (int)disk.size(), c->getExecuteSeconds(), 0, 0, 0, pnames);
+	if(!v.configuredOK())
+		return 1;
+	std::vector<float> tmp(nfl);
+	for(int k = 0; k < nsub; k++)
+	{
+		memcpy(tmp.data(), subints[k], sizeof(float) * 2 * j->corelen);
+		v.addData((cf32 *)tmp.data());
+	}
+	v.writedata();
+	return 0;
 }
 
 } // extern "C"

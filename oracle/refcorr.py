@@ -40,6 +40,7 @@ def lib():
                                     ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp, fp, fp]
         L.dref_interpolator.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         L.dref_unpack.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp]
+        L.dref_visibility_write.argtypes = [vp, ctypes.POINTER(fp), ctypes.c_int]
         _lib = L
     return _lib
 
@@ -55,14 +56,14 @@ def _iarr(v: Sequence[int]):
 class RefCorrelator:
     """The reference Configuration + Mode objects for one job (config 0)."""
 
-    def __init__(self, job, nthreads: int = 1, workdir: Optional[str] = None):
+    def __init__(self, job, nthreads: int = 1, workdir: Optional[str] = None, **input_kw):
         from difxinput import write_job_files
         self._tmp = None
         if workdir is None:
             self._tmp = tempfile.TemporaryDirectory(prefix="fxref_")
             workdir = self._tmp.name
         self.job = job
-        self.input_path = write_job_files(job, workdir)
+        self.input_path = write_job_files(job, workdir, **input_kw)
         self.h = lib().dref_open(self.input_path.encode(), nthreads)
         if not self.h:
             raise RuntimeError("reference rejected the job (set ORACLE_REF_VERBOSE=1 for its alerts)")
@@ -83,6 +84,25 @@ class RefCorrelator:
             self.close()
         except Exception:
             pass
+
+    def visibility_write(self, subint_results: List[np.ndarray]) -> bytes:
+        """The reference Visibility: addData of each subint core result, then
+        writedata; returns the bytes of the SWIN file it wrote."""
+        import glob
+        outdir = os.path.splitext(self.input_path)[0] + ".difx"
+        os.makedirs(outdir, exist_ok=True)
+        for f in glob.glob(os.path.join(outdir, "DIFX_*")):
+            os.remove(f)
+        arrs = [np.ascontiguousarray(r, dtype=np.float32) for r in subint_results]
+        ptrs = (ctypes.POINTER(ctypes.c_float) * len(arrs))(*[_fptr(a) for a in arrs])
+        rc = lib().dref_visibility_write(self.h, ptrs, len(arrs))
+        if rc != 0:
+            raise RuntimeError("reference Visibility not configured")
+        files = glob.glob(os.path.join(outdir, "DIFX_*"))
+        if not files:
+            return b""
+        with open(files[0], "rb") as f:
+            return f.read()
 
     def layout(self) -> np.ndarray:
         nf = len(self.job.freqs)

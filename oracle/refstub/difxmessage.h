@@ -1,6 +1,8 @@
 /* Stand-in for the difxmessage UDP status library: alert levels and the one
- * send call that the reference's Alert streams make. The oracle build routes
- * alerts to stderr (level <= ERROR) or drops them. */
+ * send call that the reference's Alert streams make, plus what Visibility
+ * and core.h name (the status send, its state value, the STA record type,
+ * left incomplete). The oracle build routes alerts to stderr (level <= ERROR)
+ * or drops them, and drops status messages. */
 #ifndef ORACLE_REFSTUB_DIFXMESSAGE_H
 #define ORACLE_REFSTUB_DIFXMESSAGE_H
 #define DIFX_ALERT_LEVEL_FATAL 0
@@ -12,10 +14,14 @@
 #define DIFX_ALERT_LEVEL_DEBUG 6
 #define DIFX_ALERT_LEVEL_DO_NOT_SEND 7
 #define DIFX_MESSAGE_PARAM_LENGTH 32
+#define DIFX_STATE_RUNNING 4
+typedef struct DifxMessageSTARecord DifxMessageSTARecord;
 #ifdef __cplusplus
 extern "C" {
 #endif
 int difxMessageSendDifxAlert(const char *alertMessage, int severity);
+int difxMessageSendDifxStatus3(int state, const char *message, double visMJD, int numdatastreams, float *weight,
+                               double mjdStart, double mjdStop);
 #ifdef __cplusplus
 }
 #endif

@@ -14,3 +14,10 @@ int difxMessageSendDifxAlert(const char *alertMessage, int severity)
 		fprintf(stderr, "[ref alert %d] %s\n", severity, alertMessage);
 	return 0;
 }
+
+int difxMessageSendDifxStatus3(int state, const char *message, double visMJD, int numdatastreams, float *weight,
+                               double mjdStart, double mjdStop)
+{
+	(void)state; (void)message; (void)visMJD; (void)numdatastreams; (void)weight; (void)mjdStart; (void)mjdStop;
+	return 0;
+}

@@ -1,0 +1,80 @@
+"""Integration output against the reference's own Visibility (compiled from
+mpifxcorr/src/visibility.cpp into oracle/_ref): for the same integrated
+core result, the calibrated SWIN records written by fxb_vis_calibrate +
+fxb_vis_write_swin are byte-identical to what Visibility::writedata writes --
+headers (baseline number, time, indices, polarisation pair, weight, uvw) and
+data -- with correlation-coefficient scaling and with a-priori Tsys.  Runs on
+the CPU (no GPU: calibration needs only the job layout)."""
+import os
+
+import numpy as np
+import pytest
+
+from fxb200 import synth, visibility
+from helpers import small_job
+
+import refcorr
+
+pytestmark = pytest.mark.skipif(not refcorr.available(), reason="reference build oracle/_ref absent")
+
+CASES = {
+    "fullpol": (dict(nstation=3, full_pol=True), None),
+    "fullpol_tsys": (dict(nstation=3, full_pol=True), [40.0, 55.0, 70.0]),
+    "parallel_8bit_tsys": (dict(nstation=3, nbits=8), [30.0, 30.0, 45.0]),
+    "avg4_two_freqs": (dict(nstation=3, full_pol=True, avg=4, nfreq=2), None),
+}
+
+
+def _subints(job, ref, n=2):
+    out = []
+    for k in range(n):
+        sec, ns = 0, (k + 1) * job.subint_ns
+        inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=11 + k)
+        vf = [synth.valid_flags(job) for _ in job.stations]
+        out.append(ref.process_subint(inputs, vf, 0, sec, ns))
+    return out
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_swin_records_match_reference_visibility(name, tmp_path):
+    kw, tsys = CASES[name]
+    job = small_job(**kw)
+    ref = refcorr.RefCorrelator(job, tsys=tsys)
+    subs = _subints(job, ref)
+    expect = ref.visibility_write(subs)
+    ref.close()
+    integ = np.zeros_like(subs[0])
+    for s in subs:
+        integ += s                                  # Visibility::addData, in order
+    params = visibility.VisParams.for_job(job, tsys=tsys)
+    cal = visibility.calibrate(job, params, integ)
+    visibility.write_swin(job, params, cal, str(tmp_path))
+    with open(os.path.join(str(tmp_path), "DIFX_%05d_%06d.s0000.b0000" % (job.start_mjd, job.start_sec)), "rb") as f:
+        got = f.read()
+    assert len(expect) > 0
+    assert got == expect
+    nch = {f: fr.nchan // fr.chans_to_avg for f, fr in enumerate(job.freqs)}
+    recs = visibility.read_swin(got, nch.__getitem__)
+    nprod = sum(len(b.products[0][1]) * len(b.products) for b in job.baselines)
+    assert sum(1 for r in recs if r.baseline % 257) == nprod
+    assert all(r.weight > 0 for r in recs)
+
+
+def test_records_append_per_integration(tmp_path):
+    job = small_job(nstation=2, full_pol=False)
+    ref = refcorr.RefCorrelator(job)
+    integ = sum(_subints(job, ref))
+    ref.close()
+    p0 = visibility.VisParams.for_job(job)
+    p1 = visibility.VisParams.for_job(job, int_start_sec=1)
+    cal = visibility.calibrate(job, p0, integ)
+    visibility.write_swin(job, p0, cal, str(tmp_path))
+    visibility.write_swin(job, p1, cal, str(tmp_path))
+    path = os.path.join(str(tmp_path), "DIFX_%05d_%06d.s0000.b0000" % (job.start_mjd, job.start_sec))
+    nch = {f: fr.nchan for f, fr in enumerate(job.freqs)}
+    with open(path, "rb") as f:
+        recs = visibility.read_swin(f.read(), nch.__getitem__)
+    half = len(recs) // 2
+    assert half > 0 and len(recs) == 2 * half
+    assert all(abs(r.seconds - (job.duration_s / 2)) < 1e-9 for r in recs[:half])
+    assert all(abs(r.seconds - (1 + job.duration_s / 2)) < 1e-9 for r in recs[half:])
