@@ -47,10 +47,12 @@ def test_device_integration_to_swin_matches_reference(xmac, tol, tmp_path):
                 a.pulsar_bin, a.weight, a.uvw) == (b.baseline, b.mjd, b.seconds, b.config_index, b.source_index,
                                                    b.freq_index, b.polpair, b.pulsar_bin, b.weight, b.uvw)
         err = np.linalg.norm(a.vis - b.vis) / np.linalg.norm(b.vis)
-        if xmac == "fp32" or a.baseline % 257 == 0:
+        parallel_auto = a.baseline % 257 == 0 and a.polpair[0] == a.polpair[1]
+        if xmac == "fp32" or parallel_auto:
             assert err <= tol, (a.baseline, a.polpair, err)
     if xmac == "bf16":
-        # cross products: error relative to the autocorrelation scale (1)
-        cross = [(a, b) for a, b in zip(g, e) if a.baseline % 257]
+        # cross products and cross-hand autocorrelations (noise-sized): error
+        # in correlation-coefficient units (the calibrated autocorrelation scale is 1)
+        cross = [(a, b) for a, b in zip(g, e) if a.baseline % 257 or a.polpair[0] != a.polpair[1]]
         err = np.sqrt(np.mean([np.mean(np.abs(a.vis - b.vis) ** 2) for a, b in cross]))
         assert err <= tol, err
