@@ -1300,6 +1300,21 @@ fxb_status fxb_get_stream(const fxb_ctx *ctx, void **stream)
 	return FXB_OK;
 }
 
+fxb_status fxb_vdif_mux(const uint8_t *dev_in, int64_t inbytes, int32_t nthreads, const int32_t *thread_ids,
+                        int32_t inframebytes, int32_t frames_per_second, int32_t nbits, uint8_t *dev_out,
+                        int64_t outcap, int64_t *outbytes, void *stream)
+{
+	std::string err;
+	const fxb_status st = vdif_mux(dev_in, inbytes, nthreads, thread_ids, inframebytes, frames_per_second, nbits,
+	                               dev_out, outcap, outbytes, stream, err);
+	if(st != FXB_OK)
+	{
+		std::lock_guard<std::mutex> lk(g_err_mutex);
+		g_create_err = err.empty() ? "fxb_vdif_mux: bad arguments or CUDA error" : err;
+	}
+	return st;
+}
+
 static fxb_status job_of(const fxb_job_desc *desc, Job &job)
 {
 	if(!desc) return FXB_ERR_ARG;

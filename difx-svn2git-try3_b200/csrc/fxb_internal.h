@@ -141,6 +141,11 @@ struct Job {
 
 bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st);
 
+// multi-thread VDIF muxing (fxb_mux.cu); stream is a cudaStream_t
+fxb_status vdif_mux(const uint8_t *dev_in, int64_t inbytes, int32_t nthreads, const int32_t *thread_ids,
+                    int32_t inframebytes, int32_t fps, int32_t nbits, uint8_t *dev_out, int64_t outcap,
+                    int64_t *outbytes, void *stream, std::string &err);
+
 // integration output (fxb_vis.cpp)
 fxb_status vis_calibrate(const Job &job, const fxb_vis_params *p, float *coreresult);
 fxb_status vis_swin_write(const Job &job, const fxb_vis_params *p, const float *coreresult, const char *dir,

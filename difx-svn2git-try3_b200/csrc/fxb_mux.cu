@@ -1,0 +1,282 @@
+// Multi-thread VDIF to single-thread multi-channel VDIF on the device: the
+// reference's VDIFMuxer (mpifxcorr/src/datamuxer.cpp:106-848), which the
+// DataStream runs on every read of an INTERLACEDVDIF stream before its frames
+// reach Mode.  One call takes one read: nin frames of the wanted threads
+// (interleaved in any order, other threads skipped) and writes nin / nthreads
+// output frames of nthreads channels each, in three launches:
+//   k_mux_index    every input frame finds its place: frame slot (time since
+//                  the first frame of the read, in frames) and thread
+//                  (VDIFMuxer::deinterlace, datamuxer.cpp:765-846); where a
+//                  slot is filled twice the later input frame wins, as the
+//                  reference's in-order copy does;
+//   k_mux_headers  one thread walks the output frames in order and writes
+//                  their headers (VDIFMuxer::multiplex, datamuxer.cpp:680-763):
+//                  complete slots take thread 0's header with one channel per
+//                  thread, incomplete ones the first present thread's header
+//                  marked invalid, empty ones the previous output header one
+//                  frame later, marked invalid (empty slots before the first
+//                  output frame are dropped);
+//   k_mux_turn     corner turn of the complete slots' payloads
+//                  (VDIFMuxer::cornerturn_generic, datamuxer.cpp:253-274):
+//                  one CUDA thread per (output frame, input word), reading the
+//                  word of every thread and writing nthreads output words.
+// Byte work: HBM-bound by design (every payload byte read once, written once).
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+
+#include "fxb_internal.h"
+
+namespace fxb {
+
+namespace {
+
+constexpr int kMaxMuxThreads = 64;
+
+struct MuxArgs {
+	const uint8_t *in;
+	uint8_t *out;
+	int32_t *slot;                // [nslot][nthreads] input frame index or -1
+	int32_t *status;              // [0] error code, [1] output frames
+	int32_t tmap[kMaxMuxThreads]; // VDIF thread id of each channel
+	int32_t nthreads, inframebytes, outframebytes, nin, nslot, nproc, fps, nbits;
+	int32_t wordsin, spow;        // payload words per input frame, samples per output word and thread
+};
+
+// VDIF header fields (vdifio.h:58-80)
+__device__ __forceinline__ uint32_t hw(const uint8_t *h, int w) { return ((const uint32_t *)h)[w]; }
+
+// MJD of the first day of a VDIF epoch (half years from 2000): days since
+// 1858-11-17 of (2000 + e / 2)-(1 or 7)-01, by the civil-from-days count
+__device__ __forceinline__ int epoch_mjd(int e)
+{
+	const int y0 = 2000 + e / 2, m = (e % 2) * 6 + 1;
+	const int y = y0 - (m <= 2);
+	const int era = y / 400;
+	const int yoe = y - era * 400;
+	const int doy = (153 * (m + (m > 2 ? -3 : 9)) + 2) / 5;
+	const int doe = yoe * 365 + yoe / 4 - yoe / 100 + doy;
+	return era * 146097 + doe - 678882 + 1;     // days since 0000-03-01 -> MJD
+}
+
+__device__ __forceinline__ void frame_time(const uint8_t *h, int *mjd, int *sec, int *frame)
+{
+	const uint32_t w0 = hw(h, 0), w1 = hw(h, 1);
+	const int seconds = (int)(w0 & 0x3FFFFFFFu);
+	*mjd = epoch_mjd((int)((w1 >> 24) & 0x3Fu)) + seconds / 86400;
+	*sec = seconds % 86400;
+	*frame = (int)(w1 & 0xFFFFFFu);
+}
+
+__global__ void k_mux_index(const MuxArgs a)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if(i >= a.nin)
+		return;
+	const uint8_t *h = a.in + (int64_t)i * a.inframebytes;
+	const int tid = (int)((hw(h, 3) >> 16) & 0x3FFu);
+	const int fbytes = (int)(hw(h, 2) & 0xFFFFFFu) * 8;
+	if(fbytes != a.inframebytes)
+	{
+		atomicCAS(a.status, 0, 1);             // frame size changed: the reference aborts
+		return;
+	}
+	int ti = -1;
+	for(int j = 0; j < a.nthreads; j++)
+		if(a.tmap[j] == tid)
+		{
+			ti = j;
+			break;
+		}
+	if(ti < 0)
+		return;                                 // a thread nobody asked for
+	int m0, s0, f0, m, s, f;
+	frame_time(a.in, &m0, &s0, &f0);
+	frame_time(h, &m, &s, &f);
+	const int64_t cur = ((int64_t)(m - m0) * 86400 + s - s0) * a.fps + f - f0;
+	if(cur < 0)
+		return;                                 // earlier than the read's first frame
+	if(cur >= a.nslot)
+	{
+		atomicCAS(a.status, 0, 2);             // beyond the buffer: the reference aborts
+		return;
+	}
+	atomicMax(a.slot + cur * a.nthreads + ti, i);
+}
+
+__device__ __forceinline__ void put_header(uint32_t *o, const uint32_t *src)
+{
+	for(int w = 0; w < 8; w++)
+		o[w] = src[w];
+}
+
+// one thread: output headers in order, the list of output frames to corner
+// turn (src[k] = output index of slot k, -1 when not complete)
+__global__ void k_mux_headers(const MuxArgs a, int32_t *outidx)
+{
+	if(threadIdx.x != 0 || blockIdx.x != 0 || *a.status != 0)
+		return;
+	int nout = 0;
+	int logch = 0;                              // vdifio setVDIFNumChannels: floor(log2)
+	for(int n = a.nthreads; n > 1; n /= 2)
+		logch++;
+	for(int k = 0; k < a.nproc; k++)
+	{
+		const int32_t *sl = a.slot + (int64_t)k * a.nthreads;
+		bool all = true;
+		int first = -1;
+		for(int j = 0; j < a.nthreads; j++)
+		{
+			if(sl[j] < 0)
+				all = false;
+			else if(first < 0)
+				first = j;
+		}
+		outidx[k] = -1;
+		uint32_t *o = (uint32_t *)(a.out + (int64_t)nout * a.outframebytes);
+		if(all || first >= 0)
+		{
+			put_header(o, (const uint32_t *)(a.in + (int64_t)sl[all ? 0 : first] * a.inframebytes));
+			o[0] = (o[0] & 0x7FFFFFFFu) | (all ? 0u : 0x80000000u);                       // invalid
+			if(all)
+				o[2] = (o[2] & ~(0x1Fu << 24)) | ((uint32_t)logch << 24);             // channels
+			o[2] = (o[2] & ~0xFFFFFFu) | ((uint32_t)(a.outframebytes / 8) & 0xFFFFFFu);   // frame bytes
+			o[3] &= ~(0x3FFu << 16);                                                  // thread 0
+			if(all)
+				outidx[k] = nout;
+			else
+				for(int w = 8; w < a.outframebytes / 4; w++)
+					o[w] = 0u;
+			nout++;
+		}
+		else if(nout > 0)
+		{
+			// the preceding output header, one frame later, invalid
+			const uint32_t *p = (const uint32_t *)(a.out + (int64_t)(nout - 1) * a.outframebytes);
+			put_header(o, p);
+			o[0] |= 0x80000000u;
+			uint32_t fr = (o[1] & 0xFFFFFFu) + 1u;
+			if((int)fr == a.fps)
+			{
+				fr = 0u;
+				// next second (vdifio setVDIFFrameSecond of second + 1)
+				o[0] = (o[0] & 0xC0000000u) | (((o[0] & 0x3FFFFFFFu) + 1u) & 0x3FFFFFFFu);
+			}
+			o[1] = (o[1] & ~0xFFFFFFu) | fr;
+			for(int w = 8; w < a.outframebytes / 4; w++)
+				o[w] = 0u;
+			nout++;
+		}
+	}
+	a.status[1] = nout;
+}
+
+// corner turn: x = input word, y = slot; output word (i nthreads + j) of the
+// slot's output frame packs, for k < spow and thread l, sample j spow + k of
+// thread l at bit (k nthreads + l) nbits
+__global__ void k_mux_turn(const MuxArgs a, const int32_t *outidx)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	const int k = blockIdx.y;
+	if(i >= a.wordsin || *a.status != 0)
+		return;
+	const int o = outidx[k];
+	if(o < 0)
+		return;
+	const int32_t *sl = a.slot + (int64_t)k * a.nthreads;
+	uint32_t w[kMaxMuxThreads];
+	for(int l = 0; l < a.nthreads; l++)
+		w[l] = ((const uint32_t *)(a.in + (int64_t)sl[l] * a.inframebytes + 32))[i];
+	const uint32_t mask = (1u << a.nbits) - 1u;
+	uint32_t *dst = (uint32_t *)(a.out + (int64_t)o * a.outframebytes + 32) + (int64_t)i * a.nthreads;
+	for(int j = 0; j < a.nthreads; j++)
+	{
+		uint32_t word = 0u;
+		for(int kk = 0; kk < a.spow; kk++)
+			for(int l = 0; l < a.nthreads; l++)
+				word |= ((w[l] >> ((j * a.spow + kk) * a.nbits)) & mask) << ((kk * a.nthreads + l) * a.nbits);
+		dst[j] = word;
+	}
+}
+
+}  // namespace
+
+fxb_status vdif_mux(const uint8_t *dev_in, int64_t inbytes, int32_t nthreads, const int32_t *thread_ids,
+                    int32_t inframebytes, int32_t fps, int32_t nbits, uint8_t *dev_out, int64_t outcap,
+                    int64_t *outbytes, void *stream, std::string &err)
+{
+	cudaStream_t st = (cudaStream_t)stream;
+	if(!dev_in || !dev_out || !thread_ids || !outbytes || nthreads < 1 || nthreads > kMaxMuxThreads ||
+	   inframebytes <= 32 || (inframebytes - 32) % 4 != 0 || fps < 1 || nbits < 1 || nbits > 16 || inbytes < 0)
+		return FXB_ERR_ARG;
+	MuxArgs a;
+	memset(&a, 0, sizeof(a));
+	a.nthreads = nthreads;
+	a.inframebytes = inframebytes;
+	a.outframebytes = (inframebytes - 32) * nthreads + 32;
+	a.nin = (int32_t)(inbytes / inframebytes);
+	// threads' frame slots (numthreadbufframes = readframes x DEMUX_BUFFER_FACTOR / nthreads)
+	a.nslot = a.nin * 4 / nthreads;
+	a.fps = fps;
+	a.nbits = nbits;
+	a.wordsin = (inframebytes - 32) / 4;
+	const int samplesperframe = ((inframebytes - 32) * 8) / nbits;
+	const int spiw = samplesperframe / a.wordsin;
+	a.spow = spiw / nthreads;
+	if(a.spow == 0)
+	{
+		err = "too many threads or bits for one time step per 32-bit word";
+		return FXB_ERR_UNSUPPORTED;
+	}
+	for(int j = 0; j < nthreads; j++)
+		a.tmap[j] = thread_ids[j];
+	const int nproc = a.nin / nthreads;         // one read's output frames
+	a.nproc = nproc;
+	if((int64_t)nproc * a.outframebytes > outcap)
+		return FXB_ERR_ARG;
+	*outbytes = 0;
+	if(a.nin == 0)
+		return FXB_OK;
+	int32_t *scratch = nullptr;
+	const size_t nsl = (size_t)a.nslot * nthreads;
+	cudaError_t e = cudaMallocAsync(&scratch, sizeof(int32_t) * (nsl + 2 + (size_t)nproc), st);
+	if(e != cudaSuccess)
+		return e == cudaErrorMemoryAllocation ? FXB_ERR_NOMEM : FXB_ERR_CUDA;
+	a.slot = scratch;
+	a.status = scratch + nsl;
+	int32_t *outidx = scratch + nsl + 2;
+	a.in = dev_in;
+	a.out = dev_out;
+	int32_t hst[2] = {0, 0};
+	bool ok = cudaMemsetAsync(a.slot, 0xFF, sizeof(int32_t) * nsl, st) == cudaSuccess &&
+	          cudaMemsetAsync(a.status, 0, sizeof(int32_t) * 2, st) == cudaSuccess;
+	if(ok)
+	{
+		k_mux_index<<<(a.nin + 255) / 256, 256, 0, st>>>(a);
+		k_mux_headers<<<1, 32, 0, st>>>(a, outidx);
+		if(nproc > 0)
+			k_mux_turn<<<dim3((a.wordsin + 127) / 128, nproc), 128, 0, st>>>(a, outidx);
+		ok = cudaGetLastError() == cudaSuccess &&
+		     cudaMemcpyAsync(hst, a.status, sizeof(hst), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+		     cudaStreamSynchronize(st) == cudaSuccess;
+	}
+	cudaFreeAsync(scratch, st);
+	if(!ok)
+		return FXB_ERR_CUDA;
+	if(hst[0] == 1)
+	{
+		err = "VDIF frame size changed within the read";
+		return FXB_ERR_DATA;
+	}
+	if(hst[0] == 2)
+	{
+		err = "VDIF frame time beyond the muxer's buffer (a large jump in the stream)";
+		return FXB_ERR_DATA;
+	}
+	*outbytes = (int64_t)hst[1] * a.outframebytes;
+	return FXB_OK;
+}
+
+}  // namespace fxb

@@ -172,6 +172,8 @@ def lib():
     L.fxb_batch_last_error.restype = ctypes.c_char_p
     L.fxb_batch_last_error.argtypes = [vp]
     L.fxb_batch_destroy.argtypes = [vp]
+    L.fxb_vdif_mux.argtypes = [vp, i64, i32, i32p, i32, i32, i32, vp, i64, i64p, vp]
+    L.fxb_vdif_mux.restype = ctypes.c_int
     L.fxb_host_alloc.restype = vp
     L.fxb_host_alloc.argtypes = [ctypes.c_size_t, i32p]
     L.fxb_host_free.argtypes = [vp]
@@ -451,3 +453,16 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def vdif_mux_device(dev_in: int, inbytes: int, thread_ids: Sequence[int], framebytes: int, fps: int, nbits: int,
+                    dev_out: int, outcap: int, stream: int = 0) -> int:
+    """fxb_vdif_mux on device pointers (one read of multi-thread VDIF to
+    single-thread frames); returns the output bytes."""
+    n = len(thread_ids)
+    ids = (ctypes.c_int32 * n)(*thread_ids)
+    out = ctypes.c_int64(0)
+    rc = lib().fxb_vdif_mux(dev_in, inbytes, n, ids, framebytes, fps, nbits, dev_out, outcap, ctypes.byref(out),
+                            stream or None)
+    check(rc, None, "vdif_mux")
+    return out.value

@@ -237,3 +237,49 @@ def bulk_station_frames(job: Job, s: int, frame0: int, nframes: int, seed: int) 
     for k in range(nframes):
         out[k, :VDIF_HEADER] = vdif_header(job, s, frame0 + k, station_id=s)
     return out.reshape(-1)
+
+
+def vdif_header_words(seconds: int, frame: int, epoch: int, framebytes: int, nchan: int, nbits: int,
+                      threadid: int, stationid: int = 0, invalid: bool = False) -> np.ndarray:
+    """The 8 words of a VDIF header (vdifio.h:58-80)."""
+    logch = 0
+    while (1 << logch) < nchan:
+        logch += 1
+    w = np.zeros(8, dtype=np.uint32)
+    w[0] = (seconds & 0x3FFFFFFF) | (int(invalid) << 31)
+    w[1] = (frame & 0xFFFFFF) | ((epoch & 0x3F) << 24)
+    w[2] = ((framebytes // 8) & 0xFFFFFF) | (logch << 24)
+    w[3] = (stationid & 0xFFFF) | ((threadid & 0x3FF) << 16) | (((nbits - 1) & 0x1F) << 26)
+    return w
+
+
+def interlaced_vdif(nthreads: int, nframes: int, payload: int = 8000, nbits: int = 2, fps: int = 4000,
+                    seconds0: int = 1000, frame0: int = 0, epoch: int = 35, seed: int = 0, thread_ids=None,
+                    shuffle: bool = True, drop=(), extra_thread: bool = False, duplicate=()) -> np.ndarray:
+    """A multi-thread VDIF stream: nframes frame times of nthreads single-channel
+    threads (random payload bytes), each time's frames in a seeded random
+    thread order.  drop: (time, thread index) frames left out (thread index
+    None: every thread of that time); duplicate: (time, thread index) frames
+    sent twice with different payloads; extra_thread adds one more thread
+    nobody asks for."""
+    rng = np.random.default_rng(seed)
+    ids = list(thread_ids) if thread_ids is not None else list(range(nthreads))
+    fb = payload + 32
+    dropped = set(drop)
+    frames = []
+    for t in range(nframes):
+        fr = frame0 + t
+        sec = seconds0 + fr // fps
+        order = list(range(nthreads)) + ([nthreads] if extra_thread else [])
+        if shuffle:
+            rng.shuffle(order)
+        for j in order:
+            if (t, j) in dropped or (t, None) in dropped:
+                continue
+            tid = ids[j] if j < nthreads else max(ids) + 1
+            reps = 2 if (t, j) in duplicate else 1
+            for _ in range(reps):
+                h = vdif_header_words(sec, fr % fps, epoch, fb, 1, nbits, tid)
+                body = rng.integers(0, 256, size=payload, dtype=np.uint8)
+                frames.append(np.concatenate([h.view(np.uint8), body]))
+    return np.concatenate(frames) if frames else np.zeros(0, dtype=np.uint8)

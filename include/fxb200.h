@@ -259,6 +259,19 @@ FXB_API fxb_status fxb_vis_calibrate(const fxb_job_desc *desc, const fxb_vis_par
 FXB_API fxb_status fxb_vis_write_swin(const fxb_job_desc *desc, const fxb_vis_params *params, const float *coreresult,
                                       const char *dir);
 
+/* ---- INTERLACEDVDIF: multi-thread VDIF to the single-thread, multi-channel
+ * frames the correlator takes (VDIFMuxer::deinterlace, multiplex and the
+ * corner turn, mpifxcorr/src/datamuxer.cpp:106-848), on the device.  One
+ * call is one read: dev_in holds inbytes of inframebytes-byte frames of the
+ * threads thread_ids[nthreads] (any order; other threads are skipped), the
+ * first frame giving the read's start; dev_out receives inbytes / inframebytes
+ * / nthreads output frames of (inframebytes - 32) * nthreads + 32 bytes at
+ * most (*outbytes: written), frames missing a thread marked invalid.
+ * Synchronises the stream (a cudaStream_t, may be NULL). */
+FXB_API fxb_status fxb_vdif_mux(const uint8_t *dev_in, int64_t inbytes, int32_t nthreads, const int32_t *thread_ids,
+                                int32_t inframebytes, int32_t frames_per_second, int32_t nbits, uint8_t *dev_out,
+                                int64_t outcap, int64_t *outbytes, void *stream);
+
 /* Page-locked host memory for station buffers: fxb_submit_subint copies from
  * it asynchronously at full link speed, where a pageable buffer is staged by
  * the driver on the calling thread.  Free with fxb_host_free. */

@@ -30,6 +30,7 @@
 #include "configuration.h"
 #include "mode.h"
 #include "visibility.h"
+#include "datamuxer.h"
 #include "mk5mode.h"
 #include "model.h"
 #include "mark5access.h"
@@ -461,6 +462,23 @@ int dref_visibility_write(void *h, const float *const *subints, int nsub)
 	}
 	v.writedata();
 	return 0;
+}
+
+/* The reference's INTERLACEDVDIF muxer on one read (VDIFMuxer,
+ * datamuxer.cpp:106-848): inbytes of iframebytes-byte frames of the threads
+ * tmap[nthreads] go through initialise, deinterlace and multiplex; out
+ * receives the single-thread frames.  Returns the bytes written, or -1 when
+ * the reference rejects the read. */
+int dref_vdif_mux(const unsigned char *in, int inbytes, int nthreads, const int *tmap, int iframebytes, int fps,
+                  int nbits, unsigned char *out)
+{
+	const int rframes = inbytes / iframebytes;
+	VDIFMuxer m(0, 0, 0, nthreads, iframebytes, rframes, fps, nbits, (int *)tmap);
+	DataMuxer *dm = &m;                    // the public interface (VDIFMuxer's overrides are protected)
+	memcpy(dm->getCurrentDemuxBuffer(), in, (size_t)inbytes);
+	if(!dm->initialise() || !dm->deinterlace(inbytes))
+		return -1;
+	return dm->multiplex(out);
 }
 
 } // extern "C"

@@ -41,6 +41,8 @@ def lib():
         L.dref_interpolator.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         L.dref_unpack.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp]
         L.dref_visibility_write.argtypes = [vp, ctypes.POINTER(fp), ctypes.c_int]
+        L.dref_vdif_mux.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ip, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -147,3 +149,16 @@ def unpack(formatname: str, data: np.ndarray, offsetsamples: int, nsamp: int, nc
     out = np.zeros((nchan, nsamp), dtype=np.float32)
     good = lib().dref_unpack(formatname.encode(), data.ctypes.data, offsetsamples, nsamp, _fptr(out))
     return out, good
+
+
+def vdif_mux(data: np.ndarray, nthreads: int, thread_ids: Sequence[int], framebytes: int, fps: int,
+             nbits: int) -> bytes:
+    """The reference VDIFMuxer on one read: the single-thread frames it writes."""
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    nout = (data.size // framebytes) // nthreads
+    out = np.zeros(max(1, nout * ((framebytes - 32) * nthreads + 32)), dtype=np.uint8)
+    n = lib().dref_vdif_mux(data.ctypes.data, data.size, nthreads, _iarr(list(thread_ids)), framebytes, fps, nbits,
+                            out.ctypes.data)
+    if n < 0:
+        raise RuntimeError("reference VDIF muxer rejected the read")
+    return out[:n].tobytes()
