@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (p50/p99 job latency)")
     ap.add_argument("--no-c3", action="store_true", help="skip the batched uneven-subband leg")
+    ap.add_argument("--no-mux", action="store_true", help="skip the INTERLACEDVDIF muxing leg")
     ap.add_argument("--serving-jobs", type=int, default=32)
     return ap.parse_args()
 
@@ -351,6 +352,41 @@ def c3_leg(args):
     return out
 
 
+# ---------------------------------------------------------------- INTERLACEDVDIF muxing
+def mux_leg(args):
+    """fxb_vdif_mux on one station of the c1 shape recorded as 16 single-channel
+    VDIF threads (2-bit, 64 Ms/s each, 8000-byte payloads, 2000 frames/s per
+    thread), one read of 0.5 s (128 MB, larger than L2) resident on the device;
+    bytes moved = read + written, against the measured HBM copy bandwidth."""
+    import torch
+    from fxb200.native import vdif_mux_device
+    nthr, payload, fps, nt = 16, 8000, 2000, 1000
+    data = synth.interlaced_vdif(nthr, nt, payload=payload, nbits=2, fps=fps, seed=5)
+    fb = payload + 32
+    din = torch.from_numpy(data).cuda()
+    cap = (data.size // fb) // nthr * (payload * nthr + 32)
+    dout = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    ids = list(range(nthr))
+    for _ in range(args.warmup):
+        vdif_mux_device(din.data_ptr(), data.size, ids, fb, fps, 2, dout.data_ptr(), cap)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = 0
+    e0.record()
+    for _ in range(args.steps):
+        n = vdif_mux_device(din.data_ptr(), data.size, ids, fb, fps, 2, dout.data_ptr(), cap)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    hbm_peak, _, src = load_peaks()
+    gbs = (data.size + n) / (ms * 1e-3) / 1e9
+    return {"workload": "16 threads x 1 channel, 2-bit, 64 Ms/s, 8000-byte payloads, one 0.5 s read (%d MB)"
+                        % (data.size // 1000000),
+            "ms_per_read": ms, "rtf": 0.5 / (ms * 1e-3), "bytes_in": int(data.size), "bytes_out": int(n),
+            "achieved_gbs": gbs, "hbm_peak_gbs": hbm_peak, "frac": gbs / hbm_peak, "peak_source": src,
+            "note": "three launches per read (placement, headers, corner turn) plus one 8-byte status read"}
+
+
 # ---------------------------------------------------------------- GPU arm
 def gpu_arm(args, job):
     import torch
@@ -536,6 +572,9 @@ def gpu_arm(args, job):
     c3 = None
     if rank == 0 and world == 1 and not args.no_c3:
         c3 = c3_leg(args)
+    mux = None
+    if rank == 0 and world == 1 and not args.no_mux:
+        mux = mux_leg(args)
 
     # per subint: interpolators, frame validity, FFT parameters, one F-stage
     # launch per FFT length, one XMAC launch per group of equally shaped
@@ -554,7 +593,7 @@ def gpu_arm(args, job):
             "e2e": {"value": e2e_value, "unit": UNIT, "rtf": e2e_value / job.station_mhz_per_sec(),
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps},
             "roofline": roofline, "xmac_roofline": xmac_roofline, "cpu_baseline": cpu, "clocks": clk,
-            "other_form": other, "tc_vs_fp32": tc_vs_fp32, "tuning": tuning, "serving": serve, "batched_c3": c3,
+            "other_form": other, "tc_vs_fp32": tc_vs_fp32, "tuning": tuning, "serving": serve, "batched_c3": c3, "vdif_mux": mux,
             "gpu_launches": launches_per_subint * nsub * args.steps,
         }
         print(json.dumps(line), flush=True)

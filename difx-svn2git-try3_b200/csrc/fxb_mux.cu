@@ -43,6 +43,7 @@ struct MuxArgs {
 	int32_t tmap[kMaxMuxThreads]; // VDIF thread id of each channel
 	int32_t nthreads, inframebytes, outframebytes, nin, nslot, nproc, fps, nbits;
 	int32_t wordsin, spow;        // payload words per input frame, samples per output word and thread
+	int32_t vec;                  // output words 16-byte aligned: vector stores
 };
 
 // VDIF header fields (vdifio.h:58-80)
@@ -112,70 +113,111 @@ __device__ __forceinline__ void put_header(uint32_t *o, const uint32_t *src)
 		o[w] = src[w];
 }
 
-// one thread: output headers in order, the list of output frames to corner
-// turn (src[k] = output index of slot k, -1 when not complete)
+// first slot holding any frame (output frames before it are dropped)
+__global__ void k_mux_first(const MuxArgs a)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if(k >= a.nproc || *a.status != 0)
+		return;
+	const int32_t *sl = a.slot + (int64_t)k * a.nthreads;
+	for(int j = 0; j < a.nthreads; j++)
+		if(sl[j] >= 0)
+		{
+			atomicMin(a.status + 2, k);
+			return;
+		}
+}
+
+// the header slot k's output frame starts from, before the empty-slot step:
+// complete -> thread 0's, incomplete -> the first present thread's
+__device__ __forceinline__ void slot_header(const MuxArgs &a, int k, int logch, uint32_t *o, bool *all_out,
+                                            bool *any_out)
+{
+	const int32_t *sl = a.slot + (int64_t)k * a.nthreads;
+	bool all = true;
+	int first = -1;
+	for(int j = 0; j < a.nthreads; j++)
+	{
+		if(sl[j] < 0)
+			all = false;
+		else if(first < 0)
+			first = j;
+	}
+	*all_out = all;
+	*any_out = first >= 0;
+	if(first < 0)
+		return;
+	put_header(o, (const uint32_t *)(a.in + (int64_t)sl[all ? 0 : first] * a.inframebytes));
+	o[0] = (o[0] & 0x7FFFFFFFu) | (all ? 0u : 0x80000000u);                       // invalid
+	if(all)
+		o[2] = (o[2] & ~(0x1Fu << 24)) | ((uint32_t)logch << 24);             // channels
+	o[2] = (o[2] & ~0xFFFFFFu) | ((uint32_t)(a.outframebytes / 8) & 0xFFFFFFu);   // frame bytes
+	o[3] &= ~(0x3FFu << 16);                                                  // thread 0
+}
+
+// one thread per slot k from the first filled one: output frame k - first.
+// An empty slot takes the nearest earlier filled slot's header advanced one
+// frame per slot between them (the reference increments the preceding output
+// header, itself such a copy), invalid; outidx[k] = output frame to corner
+// turn, or -1
 __global__ void k_mux_headers(const MuxArgs a, int32_t *outidx)
 {
-	if(threadIdx.x != 0 || blockIdx.x != 0 || *a.status != 0)
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if(k >= a.nproc || *a.status != 0)
 		return;
-	int nout = 0;
+	const int k0 = a.status[2];
+	outidx[k] = -1;
+	if(k < k0)
+		return;
 	int logch = 0;                              // vdifio setVDIFNumChannels: floor(log2)
 	for(int n = a.nthreads; n > 1; n /= 2)
 		logch++;
-	for(int k = 0; k < a.nproc; k++)
+	uint32_t *o = (uint32_t *)(a.out + (int64_t)(k - k0) * a.outframebytes);
+	uint32_t h[8];
+	bool all, any;
+	slot_header(a, k, logch, h, &all, &any);
+	if(!any)
 	{
-		const int32_t *sl = a.slot + (int64_t)k * a.nthreads;
-		bool all = true;
-		int first = -1;
-		for(int j = 0; j < a.nthreads; j++)
+		int g = k - 1;
+		bool ga = false, gy = false;
+		while(true)
 		{
-			if(sl[j] < 0)
-				all = false;
-			else if(first < 0)
-				first = j;
+			slot_header(a, g, logch, h, &ga, &gy);
+			if(gy)
+				break;
+			g--;
 		}
-		outidx[k] = -1;
-		uint32_t *o = (uint32_t *)(a.out + (int64_t)nout * a.outframebytes);
-		if(all || first >= 0)
+		h[0] |= 0x80000000u;
+		uint32_t fr = h[1] & 0xFFFFFFu;
+		uint32_t secs = h[0] & 0x3FFFFFFFu;
+		for(int step = 0; step < k - g; step++)
 		{
-			put_header(o, (const uint32_t *)(a.in + (int64_t)sl[all ? 0 : first] * a.inframebytes));
-			o[0] = (o[0] & 0x7FFFFFFFu) | (all ? 0u : 0x80000000u);                       // invalid
-			if(all)
-				o[2] = (o[2] & ~(0x1Fu << 24)) | ((uint32_t)logch << 24);             // channels
-			o[2] = (o[2] & ~0xFFFFFFu) | ((uint32_t)(a.outframebytes / 8) & 0xFFFFFFu);   // frame bytes
-			o[3] &= ~(0x3FFu << 16);                                                  // thread 0
-			if(all)
-				outidx[k] = nout;
-			else
-				for(int w = 8; w < a.outframebytes / 4; w++)
-					o[w] = 0u;
-			nout++;
-		}
-		else if(nout > 0)
-		{
-			// the preceding output header, one frame later, invalid
-			const uint32_t *p = (const uint32_t *)(a.out + (int64_t)(nout - 1) * a.outframebytes);
-			put_header(o, p);
-			o[0] |= 0x80000000u;
-			uint32_t fr = (o[1] & 0xFFFFFFu) + 1u;
+			fr = (fr + 1u) & 0xFFFFFFu;
 			if((int)fr == a.fps)
 			{
 				fr = 0u;
-				// next second (vdifio setVDIFFrameSecond of second + 1)
-				o[0] = (o[0] & 0xC0000000u) | (((o[0] & 0x3FFFFFFFu) + 1u) & 0x3FFFFFFFu);
+				secs = (secs + 1u) & 0x3FFFFFFFu;      // vdifio setVDIFFrameSecond(second + 1)
 			}
-			o[1] = (o[1] & ~0xFFFFFFu) | fr;
-			for(int w = 8; w < a.outframebytes / 4; w++)
-				o[w] = 0u;
-			nout++;
 		}
+		h[0] = (h[0] & 0xC0000000u) | secs;
+		h[1] = (h[1] & ~0xFFFFFFu) | fr;
 	}
-	a.status[1] = nout;
+	put_header(o, h);
+	if(all)
+		outidx[k] = k - k0;
+	else
+		for(int w = 8; w < a.outframebytes / 4; w++)
+			o[w] = 0u;
+	if(k == a.nproc - 1)
+		a.status[1] = a.nproc - k0;
 }
 
 // corner turn: x = input word, y = slot; output word (i nthreads + j) of the
 // slot's output frame packs, for k < spow and thread l, sample j spow + k of
 // thread l at bit (k nthreads + l) nbits
+// NT > 0: nthreads known at compile time (the words stay in registers);
+// NT = 0: any count up to kMaxMuxThreads
+template <int NT>
 __global__ void k_mux_turn(const MuxArgs a, const int32_t *outidx)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -185,19 +227,51 @@ __global__ void k_mux_turn(const MuxArgs a, const int32_t *outidx)
 	const int o = outidx[k];
 	if(o < 0)
 		return;
-	const int32_t *sl = a.slot + (int64_t)k * a.nthreads;
-	uint32_t w[kMaxMuxThreads];
-	for(int l = 0; l < a.nthreads; l++)
-		w[l] = ((const uint32_t *)(a.in + (int64_t)sl[l] * a.inframebytes + 32))[i];
+	const int nt = NT > 0 ? NT : a.nthreads;
+	const int32_t *sl = a.slot + (int64_t)k * nt;
+	uint32_t w[NT > 0 ? NT : kMaxMuxThreads];
+#pragma unroll
+	for(int l = 0; l < nt; l++)
+		w[l] = __ldg((const uint32_t *)(a.in + (int64_t)sl[l] * a.inframebytes + 32) + i);
 	const uint32_t mask = (1u << a.nbits) - 1u;
-	uint32_t *dst = (uint32_t *)(a.out + (int64_t)o * a.outframebytes + 32) + (int64_t)i * a.nthreads;
-	for(int j = 0; j < a.nthreads; j++)
+	uint32_t *dst = (uint32_t *)(a.out + (int64_t)o * a.outframebytes + 32) + (int64_t)i * nt;
+	if constexpr(NT >= 4)
 	{
-		uint32_t word = 0u;
-		for(int kk = 0; kk < a.spow; kk++)
-			for(int l = 0; l < a.nthreads; l++)
-				word |= ((w[l] >> ((j * a.spow + kk) * a.nbits)) & mask) << ((kk * a.nthreads + l) * a.nbits);
-		dst[j] = word;
+		// NT words per input word: 16-byte stores (frames start 16-byte aligned
+		// when the payload is a multiple of 16 bytes, checked on the host)
+#pragma unroll
+		for(int j0 = 0; j0 < NT; j0 += 4)
+		{
+			uint32_t v[4];
+#pragma unroll
+			for(int q = 0; q < 4; q++)
+			{
+				uint32_t word = 0u;
+				for(int kk = 0; kk < a.spow; kk++)
+#pragma unroll
+					for(int l = 0; l < NT; l++)
+						word |= ((w[l] >> (((j0 + q) * a.spow + kk) * a.nbits)) & mask) << ((kk * NT + l) * a.nbits);
+				v[q] = word;
+			}
+			if(a.vec)
+				*(uint4 *)(dst + j0) = make_uint4(v[0], v[1], v[2], v[3]);
+			else
+				for(int q = 0; q < 4; q++)
+					dst[j0 + q] = v[q];
+		}
+	}
+	else
+	{
+#pragma unroll
+		for(int j = 0; j < nt; j++)
+		{
+			uint32_t word = 0u;
+			for(int kk = 0; kk < a.spow; kk++)
+#pragma unroll
+				for(int l = 0; l < nt; l++)
+					word |= ((w[l] >> ((j * a.spow + kk) * a.nbits)) & mask) << ((kk * nt + l) * a.nbits);
+			dst[j] = word;
+		}
 	}
 }
 
@@ -232,6 +306,7 @@ fxb_status vdif_mux(const uint8_t *dev_in, int64_t inbytes, int32_t nthreads, co
 	}
 	for(int j = 0; j < nthreads; j++)
 		a.tmap[j] = thread_ids[j];
+	a.vec = ((uintptr_t)dev_out % 16 == 0 && a.outframebytes % 16 == 0) ? 1 : 0;
 	const int nproc = a.nin / nthreads;         // one read's output frames
 	a.nproc = nproc;
 	if((int64_t)nproc * a.outframebytes > outcap)
@@ -241,23 +316,37 @@ fxb_status vdif_mux(const uint8_t *dev_in, int64_t inbytes, int32_t nthreads, co
 		return FXB_OK;
 	int32_t *scratch = nullptr;
 	const size_t nsl = (size_t)a.nslot * nthreads;
-	cudaError_t e = cudaMallocAsync(&scratch, sizeof(int32_t) * (nsl + 2 + (size_t)nproc), st);
+	cudaError_t e = cudaMallocAsync(&scratch, sizeof(int32_t) * (nsl + 4 + (size_t)nproc), st);
 	if(e != cudaSuccess)
 		return e == cudaErrorMemoryAllocation ? FXB_ERR_NOMEM : FXB_ERR_CUDA;
 	a.slot = scratch;
 	a.status = scratch + nsl;
-	int32_t *outidx = scratch + nsl + 2;
+	int32_t *outidx = scratch + nsl + 4;
 	a.in = dev_in;
 	a.out = dev_out;
 	int32_t hst[2] = {0, 0};
+	// status: [0] error, [1] output frames, [2] first filled slot
+	const int32_t init[4] = {0, 0, nproc, 0};
 	bool ok = cudaMemsetAsync(a.slot, 0xFF, sizeof(int32_t) * nsl, st) == cudaSuccess &&
-	          cudaMemsetAsync(a.status, 0, sizeof(int32_t) * 2, st) == cudaSuccess;
+	          cudaMemcpyAsync(a.status, init, sizeof(init), cudaMemcpyHostToDevice, st) == cudaSuccess;
 	if(ok)
 	{
 		k_mux_index<<<(a.nin + 255) / 256, 256, 0, st>>>(a);
-		k_mux_headers<<<1, 32, 0, st>>>(a, outidx);
 		if(nproc > 0)
-			k_mux_turn<<<dim3((a.wordsin + 127) / 128, nproc), 128, 0, st>>>(a, outidx);
+		{
+			k_mux_first<<<(nproc + 255) / 256, 256, 0, st>>>(a);
+			k_mux_headers<<<(nproc + 127) / 128, 128, 0, st>>>(a, outidx);
+			const dim3 grid((a.wordsin + 127) / 128, nproc);
+			switch(nthreads)
+			{
+			case 1: k_mux_turn<1><<<grid, 128, 0, st>>>(a, outidx); break;
+			case 2: k_mux_turn<2><<<grid, 128, 0, st>>>(a, outidx); break;
+			case 4: k_mux_turn<4><<<grid, 128, 0, st>>>(a, outidx); break;
+			case 8: k_mux_turn<8><<<grid, 128, 0, st>>>(a, outidx); break;
+			case 16: k_mux_turn<16><<<grid, 128, 0, st>>>(a, outidx); break;
+			default: k_mux_turn<0><<<grid, 128, 0, st>>>(a, outidx); break;
+			}
+		}
 		ok = cudaGetLastError() == cudaSuccess &&
 		     cudaMemcpyAsync(hst, a.status, sizeof(hst), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
 		     cudaStreamSynchronize(st) == cudaSuccess;
