@@ -55,7 +55,8 @@ struct Tuner {
 	int iter = 0, total = 0;                             // tuning while iter < total
 	std::vector<std::pair<int, int>> fc;                 // F candidates: (iterations per CTA, items fastest)
 	std::vector<std::vector<float>> fms;                 // [kind][candidate] fastest launch seen (ms)
-	std::vector<std::vector<std::pair<int, int>>> xc;    // [group] XMAC candidates: (raw, operand) ring depths
+	struct XCand { int nrs, nas, nb; };
+	std::vector<std::vector<XCand>> xc;                  // [group] XMAC candidates: ring depths, accumulator buffers
 	std::vector<std::vector<float>> xms;                 // [group][candidate]
 	std::vector<cudaEvent_t> ev;                         // boundaries: kinds (nk + 1), then groups (ng + 1)
 	bool done = false;
@@ -882,7 +883,7 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 			if(ctx->tc && !tn.xc[gi].empty())
 			{
 				const auto &c = tn.xc[gi][tn.iter % tn.xc[gi].size()];
-				tc_stages(&sh, c.first, c.second);
+				tc_stages(&sh, c.nrs, c.nas, c.nb);
 			}
 		}
 		if(ctx->tc)
@@ -934,7 +935,7 @@ static void tune_collect(fxb_ctx *ctx)
 		if(t.xc[g].empty())
 			continue;
 		const size_t c = std::min_element(t.xms[g].begin(), t.xms[g].end()) - t.xms[g].begin();
-		tc_stages(&ctx->xgroups[g].shape, t.xc[g][c].first, t.xc[g][c].second);
+		tc_stages(&ctx->xgroups[g].shape, t.xc[g][c].nrs, t.xc[g][c].nas, t.xc[g][c].nb);
 	}
 	t.done = true;
 	ctx->gen++;
@@ -1034,12 +1035,14 @@ fxb_status fxb_autotune(fxb_ctx *ctx, int32_t rounds)
 	size_t most = t.fc.size();
 	for(size_t g = 0; g < ng && ctx->tc; g++)
 	{
-		static const int depth[][2] = {{6, 4}, {6, 3}, {4, 3}, {4, 2}, {3, 2}, {2, 2}};
+		// one CTA per SM with double-buffered accumulators, or two per SM
+		static const int depth[][3] = {{6, 4, 2}, {6, 3, 2}, {4, 3, 2}, {4, 2, 2}, {3, 2, 2}, {2, 2, 2},
+		                               {4, 2, 1}, {3, 2, 1}, {2, 2, 1}};
 		for(const auto &d : depth)
 		{
 			TcShape sh = ctx->xgroups[g].shape;
-			if(tc_stages(&sh, d[0], d[1]))
-				t.xc[g].push_back({d[0], d[1]});
+			if(tc_stages(&sh, d[0], d[1], d[2]))
+				t.xc[g].push_back({d[0], d[1], d[2]});
 		}
 		most = std::max(most, t.xc[g].size());
 	}
@@ -1082,14 +1085,14 @@ fxb_status fxb_tuning_report(const fxb_ctx *ctx, char *buf, size_t len, size_t *
 			r += line;
 			continue;
 		}
-		snprintf(line, sizeof(line), "xmac group %zu (%d inputs, %d channels): rings %d raw / %d operand", g, sh.nrow,
-		         sh.nchan, sh.nrs, sh.nas);
+		snprintf(line, sizeof(line), "xmac group %zu (%d inputs, %d channels): rings %d raw / %d operand, %d CTA(s) per SM",
+		         g, sh.nrow, sh.nchan, sh.nrs, sh.nas, sh.nb == 1 ? 2 : 1);
 		r += line;
 		if(t.done)
 			for(size_t c = 0; c < t.xc[g].size(); c++)
 			{
-				snprintf(line, sizeof(line), "%s(%d,%d) %.4f ms", c ? ", " : " | ", t.xc[g][c].first, t.xc[g][c].second,
-				         (double)t.xms[g][c]);
+				snprintf(line, sizeof(line), "%s(%d,%d,%s) %.4f ms", c ? ", " : " | ", t.xc[g][c].nrs, t.xc[g][c].nas,
+				         t.xc[g][c].nb == 1 ? "2/SM" : "1/SM", (double)t.xms[g][c]);
 				r += line;
 			}
 		r += "\n";

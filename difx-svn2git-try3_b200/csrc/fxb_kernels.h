@@ -122,13 +122,15 @@ struct TcShape {
 	int32_t nrow, nchan, r2p, G, CB, Tpad;
 	int32_t raw_bytes, raw_stride;    // bytes of one TMA box, stride of the raw stages
 	int32_t nrs, nas;                 // raw and operand stages
+	int32_t nb;                       // accumulator buffers: 2 (one CTA per SM) or 1 (two CTAs per SM)
 	int32_t dstride, dump_off;        // accumulator copy: floats per row, byte offset
 	size_t smem;
 };
 bool tc_shape(int nrow, int nchan, int T, bool f8, TcShape *s);
-// set the raw / operand ring depths of a shape (and its shared-memory plan);
-// false if they do not fit in 227 KB
-bool tc_stages(TcShape *s, int nrs, int nas);
+// set the raw / operand ring depths and accumulator buffers of a shape (and
+// its shared-memory plan); false if they do not fit (227 KB for one CTA per
+// SM, 112 KB each for two)
+bool tc_stages(TcShape *s, int nrs, int nas, int nb = 2);
 bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf);
 size_t tc_tensormap_size();
 void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf,

@@ -202,14 +202,17 @@ struct TcParams {
 	int32_t *err;
 };
 
-template <bool F8>
-__global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__ CUtensorMap tmap,
+// NB: accumulator buffers per CTA.  2: 512 tensor-memory columns, the
+// epilogue of one unit overlaps the MMAs of the next, one CTA per SM; 1: 256
+// columns, two CTAs per SM overlap each other instead
+template <bool F8, int NB>
+__global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_constant__ CUtensorMap tmap,
                                                          const DevFreqPlan *__restrict__ plans,
                                                          const int32_t *__restrict__ plan_idx, TcParams tp,
                                                          float2 *__restrict__ acc)
 {
 	extern __shared__ __align__(1024) unsigned char smem_tc[];
-	__shared__ uint64_t full_raw[kRS], empty_raw[kRS], full_a[kAS], empty_a[kAS], acc_full[2], acc_empty[2], mma_done;
+	__shared__ uint64_t full_raw[kRS], empty_raw[kRS], full_a[kAS], empty_a[kAS], acc_full[NB], acc_empty[NB], mma_done;
 	__shared__ uint32_t tmem_base_s;
 	__shared__ volatile int fail_s;
 	__shared__ int issued_s, consumed_s;
@@ -237,7 +240,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 			mbar_init(&full_a[s], 4);
 			mbar_init(&empty_a[s], 1);
 		}
-		for(int b = 0; b < 2; b++)
+		for(int b = 0; b < NB; b++)
 		{
 			mbar_init(&acc_full[b], 1);
 			mbar_init(&acc_empty[b], 4);
@@ -251,7 +254,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 	if(warp == 1)
 	{
 		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_s)),
-		             "r"(512u));
+		             "r"(256u * NB));
 		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
 	}
 	asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -299,11 +302,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 			bool ok = true;
 			for(int u = blockIdx.x; u < tp.nunits && ok; u += gridDim.x, ku++)
 			{
-				const int buf = ku & 1;
-				if(ku >= 2)
+				const int buf = ku % NB;
+				if(ku >= NB)
 				{
 					// the epilogue has copied out this buffer's previous unit
-					if(!mbar_wait(&acc_empty[buf], ((ku >> 1) - 1) & 1, &fail_s))
+					if(!mbar_wait(&acc_empty[buf], ((ku / NB) - 1) & 1, &fail_s))
 					{
 						fail_s = 3;
 						ok = false;
@@ -496,13 +499,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 		int ku = 0;
 		for(int u = blockIdx.x; u < tp.nunits; u += gridDim.x, ku++)
 		{
-			const int buf = ku & 1;
+			const int buf = ku % NB;
 			const int fi = u / tp.nblk, blk = u - fi * tp.nblk;
 			const DevFreqPlan &P = plans[plan_idx[fi]];
 			const int nout = P.acc_cstride;
 			const int c_first = blk * tp.CB;
 			const int ncv = min(tp.CB, tp.nchan - c_first);
-			bool bad = !mbar_wait(&acc_full[buf], (ku >> 1) & 1, &fail_s);
+			bool bad = !mbar_wait(&acc_full[buf], (ku / NB) & 1, &fail_s);
 			if(bad)
 				fail_s = 6;
 			if(epi_sync_or(bad))
@@ -603,7 +606,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_xmac_tc(const __grid_constant__
 	__syncthreads();
 	asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 	if(warp == 1)
-		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512u));
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(256u * NB));
 }
 
 // ---------------------------------------------------------------- host side
@@ -635,16 +638,17 @@ bool tc_shape(int nrow, int nchan, int T, bool f8, TcShape *s)
 	return false;
 }
 
-bool tc_stages(TcShape *s, int nrs, int nas)
+bool tc_stages(TcShape *s, int nrs, int nas, int nb)
 {
-	if(nrs < 1 || nrs > kRS || nas < 1 || nas > kAS)
+	if(nrs < 1 || nrs > kRS || nas < 1 || nas > kAS || nb < 1 || nb > 2)
 		return false;
 	const size_t dump = (size_t)s->CB * 2 * s->nrow * s->dstride * 4;
 	const size_t rings = (size_t)nrs * s->raw_stride + (size_t)nas * kNG * kTileBytes;
-	if(1024 + rings + dump > 227 * 1024)
+	if(1024 + rings + dump > (nb == 2 ? 227 : 112) * 1024)
 		return false;
 	s->nrs = nrs;
 	s->nas = nas;
+	s->nb = nb;
 	s->dump_off = (int32_t)rings;
 	s->smem = 1024 + rings + dump;
 	return true;
@@ -710,16 +714,28 @@ void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplan
 	tp.dstride = s.dstride;
 	tp.dump_off = s.dump_off;
 	tp.err = err;
-	const int grid = tp.nunits < nsm ? tp.nunits : nsm;
-	if(s.f8)
+	const int ctas = nsm * (s.nb == 1 ? 2 : 1);
+	const int grid = tp.nunits < ctas ? tp.nunits : ctas;
+	const CUtensorMap &map = *(const CUtensorMap *)tmap;
+	if(s.f8 && s.nb == 1)
 	{
-		cudaFuncSetAttribute(k_xmac_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-		k_xmac_tc<true><<<grid, kThreads, s.smem, stream>>>(*(const CUtensorMap *)tmap, dplans, plan_idx, tp, acc);
+		cudaFuncSetAttribute(k_xmac_tc<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+		k_xmac_tc<true, 1><<<grid, kThreads, s.smem, stream>>>(map, dplans, plan_idx, tp, acc);
+	}
+	else if(s.f8)
+	{
+		cudaFuncSetAttribute(k_xmac_tc<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+		k_xmac_tc<true, 2><<<grid, kThreads, s.smem, stream>>>(map, dplans, plan_idx, tp, acc);
+	}
+	else if(s.nb == 1)
+	{
+		cudaFuncSetAttribute(k_xmac_tc<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+		k_xmac_tc<false, 1><<<grid, kThreads, s.smem, stream>>>(map, dplans, plan_idx, tp, acc);
 	}
 	else
 	{
-		cudaFuncSetAttribute(k_xmac_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-		k_xmac_tc<false><<<grid, kThreads, s.smem, stream>>>(*(const CUtensorMap *)tmap, dplans, plan_idx, tp, acc);
+		cudaFuncSetAttribute(k_xmac_tc<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+		k_xmac_tc<false, 2><<<grid, kThreads, s.smem, stream>>>(map, dplans, plan_idx, tp, acc);
 	}
 }
 

@@ -145,15 +145,15 @@ def _many(job, k, c, n):
 
 @pytest.mark.parametrize("xmac", ["fp32", "bf16", "fp8"])
 def test_autotuned_result_is_identical(xmac):
-    # the tuner tries 6 candidates per round: 2 rounds take 12 subints
+    # the tuner tries up to 9 candidates per round: 2 rounds take 18 subints
     job = small_job(nstation=4, nchan=256, bw=16.0, nfreq=2, full_pol=True, subint_ns=SUBINT_NS)
     plain = Correlator(job, xmac=xmac)
-    _many(job, 0, plain, 14)
+    _many(job, 0, plain, 20)
     ref = plain.results()
     plain.close()
     tuned = Correlator(job, xmac=xmac)
     tuned.autotune(2)
-    _many(job, 0, tuned, 14)
+    _many(job, 0, tuned, 20)
     got = tuned.results()
     report = tuned.tuning_report()
     tuned.close()
@@ -168,13 +168,13 @@ def test_batch_autotune_keeps_results():
     alone = []
     for k, j in enumerate(jobs):
         c = Correlator(j, xmac="bf16")
-        _many(j, k, c, 13)
+        _many(j, k, c, 20)
         alone.append(c.results())
         c.close()
     members = [Correlator(j, xmac="bf16") for j in jobs]
     batch = Batch(members)
     batch.autotune(2)
-    for n in range(13):
+    for n in range(20):
         sec, ns = 0, (n + 1) * SUBINT_NS
         batch.submit([_inputs(j, k, sec, ns) for k, j in enumerate(jobs)], sec, ns)
     batch.sync()
