@@ -219,6 +219,7 @@ constexpr int kMaxTQ = 4;         // FFT iterations per CTA at most
 // Constants of one FFT, computed once per CTA (one warp per FFT).
 struct FftConst {
 	float P0, alpha, beta, gamma, eps;   // fringe phase (turns): start and per-sample terms
+	float stc, sts;                      // order 1: rotator step over N/8 samples, exp(-2 pi i alpha N/8)
 	float dfs, postf;                    // fractional-sample turns per channel, order-0 post-F turns
 	uint32_t fa, so;                     // first frame of the window, window start within it
 	uint32_t fmask;                      // validity of the window's frames (bit k: frame fa + k)
@@ -387,6 +388,8 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 			const int t = t0 + f;
 			FftConst c;
 			c.P0 = c.alpha = c.beta = c.gamma = c.eps = c.dfs = c.postf = 0.0f;
+			c.stc = 1.0f;
+			c.sts = 0.0f;
 			c.fa = c.so = c.fmask = 0u;
 			c.stuck = 0;
 			c.flags = 0;
@@ -407,6 +410,12 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 					{
 						c.P0 = frac_centered(lo * pq->b + fraclo);
 						c.alpha = (float)(lo * pq->a * invN);
+						// each thread's samples are N/8 apart: one step phasor per FFT
+						const double st = (double)c.alpha * (double)(N / 8);
+						double ss, sc;
+						sincospi(-2.0 * (st - rint(st)), &ss, &sc);
+						c.stc = (float)sc;
+						c.sts = (float)ss;
 					}
 					else if(order == 2)
 					{
@@ -451,6 +460,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 		const uint32_t fa = fc.fa, so = fc.so, fmask = fc.fmask;
 		const int stuck = fc.stuck;
 		const float P0 = fc.P0, alpha = fc.alpha, beta = fc.beta, gamma = fc.gamma, eps = fc.eps;
+		const float stc = fc.stc, sts = fc.sts;
 		const float dfs = fc.dfs, postf = fc.postf;
 		const bool narrow = (fc.flags & 2) != 0;
 		// ---- 1-3. decode, fringe-rotate and run the first radix-8 pass (s = 1:
@@ -498,7 +508,15 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 						}
 					}
 				}
-				// phase B: levels, fringe rotation
+				// phase B: levels, fringe rotation (order 1: the rotator of sample b,
+				// then one complex step per N/8 samples)
+				float rc = 1.0f, rs = 0.0f;
+				if(order == 1)
+				{
+					float ph0 = P0 + (float)b * alpha;
+					ph0 -= rintf(ph0);
+					__sincosf(-6.283185307179586f * ph0, &rs, &rc);
+				}
 				C x[NV][8];
 #pragma unroll
 				for(int r = 0; r < 8; r++)
@@ -525,17 +543,19 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 						}
 					}
 					float sn = 0.0f, cs = 1.0f;
-					if(order != 0)
+					if(order == 1)
 					{
-						float ph;
-						if(order == 1)
-							ph = P0 + (float)n * alpha;
-						else
-						{
-							const int kk = n / asl, jj = n - kk * asl;
-							ph = P0 + (float)jj * alpha + (float)(kk * jj) * beta + (float)kk * gamma +
-							     (float)(kk * kk) * eps;
-						}
+						cs = rc;
+						sn = rs;
+						const float nc = rc * stc - rs * sts;
+						rs = rc * sts + rs * stc;
+						rc = nc;
+					}
+					else if(order == 2)
+					{
+						const int kk = n / asl, jj = n - kk * asl;
+						float ph = P0 + (float)jj * alpha + (float)(kk * jj) * beta + (float)kk * gamma +
+						           (float)(kk * kk) * eps;
 						ph -= rintf(ph);
 						__sincosf(-6.283185307179586f * ph, &sn, &cs);
 					}
