@@ -407,7 +407,11 @@ def gpu_arm(args, job):
     host = []       # [k][s] pinned host tensors
     for (_, inputs) in pool:
         dev.append([torch.from_numpy(b).to("cuda") for b, _, _ in inputs])
-        host.append([torch.from_numpy(b).pin_memory() for b, _, _ in inputs])
+        # the subint's station buffers one after the other in one page-locked
+        # block, as a datastream's receive ring holds them: one copy per subint
+        blk = torch.from_numpy(np.concatenate([b for b, _, _ in inputs])).pin_memory()
+        offs = np.cumsum([0] + [b.size for b, _, _ in inputs])
+        host.append([blk[int(offs[i]):int(offs[i + 1])] for i in range(len(inputs))])
     nbytes = [[b.size for b, _, _ in inputs] for (_, inputs) in pool]
     dsec = [[x for _, x, _ in inputs] for (_, inputs) in pool]
     dns = [[x for _, _, x in inputs] for (_, inputs) in pool]

@@ -25,6 +25,8 @@ using namespace fxb;
 struct Slot {
 	std::vector<uint8_t *> raw;        // device staging per station
 	std::vector<int64_t> rawcap;
+	uint8_t *rawall = nullptr;         // device staging of a subint whose station buffers are adjacent
+	int64_t rawallcap = 0;
 	DevSubintStation *d_sub = nullptr;
 	int32_t *d_vflags = nullptr;
 	// host side of d_sub / d_vflags: pageable, the driver stages each copy
@@ -187,8 +189,11 @@ static void free_ctx(fxb_ctx *ctx)
 	if(ctx->d_valid)
 		cudaFreeAsync(ctx->d_valid, ctx->stream);
 	for(auto &s : ctx->slots)
+	{
 		for(auto *p : s.raw)
 			if(p) cudaFreeAsync(p, ctx->stream);
+		if(s.rawall) cudaFreeAsync(s.rawall, ctx->stream);
+	}
 	if(ctx->stream)
 		cudaStreamSynchronize(ctx->stream);
 	for(auto &s : ctx->slots)
@@ -772,6 +777,29 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 		ctx->valid_stride = need;
 	}
 
+	// host buffers one after the other (as a datastream's receive ring holds
+	// them) with 16-byte aligned starts: one copy for the whole subint
+	bool merged = !device && ctx->S > 1;
+	int64_t total = 0;
+	for(int s = 0; s < ctx->S && merged; s++)
+	{
+		if(bufs[s] != bufs[0] + total || (total & 15) != 0)
+			merged = false;
+		total += nbytes[s];
+	}
+	if(merged && total > 0)
+	{
+		if(sl.rawallcap < total)
+		{
+			if(sl.rawall) CK(ctx, cudaFreeAsync(sl.rawall, ctx->copy_stream));
+			sl.rawall = nullptr;
+			const int64_t cap = total + total / 8 + 4096;
+			CK(ctx, pool_alloc(ctx, (void **)&sl.rawall, cap, ctx->copy_stream));
+			sl.rawallcap = cap;
+		}
+		CK(ctx, cudaMemcpyAsync(sl.rawall, bufs[0], total, cudaMemcpyHostToDevice, ctx->copy_stream));
+	}
+	int64_t off = 0;
 	for(int s = 0; s < ctx->S; s++)
 	{
 		DevSubintStation &u = sl.h_sub[s];
@@ -783,6 +811,11 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 		u.subns = ns;
 		if(device)
 			u.buf = bufs[s];
+		else if(merged)
+		{
+			u.buf = sl.rawall + off;
+			off += nbytes[s];
+		}
 		else
 		{
 			if(sl.rawcap[s] < nbytes[s])

@@ -145,3 +145,24 @@ def test_long_ffts(nchan):
     got, ref, layout, n, w, wref = run_both(job, [(0, 2_048_000), (0, 4_096_000)])
     compare_core(job, layout, n, got, ref)
     assert np.array_equal(w, wref)
+
+
+@pytest.mark.parametrize("xmac", ["fp32", "bf16"])
+def test_adjacent_station_buffers_give_the_same_result(xmac):
+    # station buffers one after the other in one block take one copy per subint
+    job = small_job(nstation=4, full_pol=True, nfreq=2)
+    subs = [(0, 1_000_000), (0, 5_000_000)]
+    res = []
+    for adjacent in (False, True):
+        corr = Correlator(job, xmac=xmac)
+        for sec, ns in subs:
+            inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=13)
+            if adjacent:
+                blk = np.concatenate([b for b, _, _ in inputs])
+                offs = np.cumsum([0] + [b.size for b, _, _ in inputs])
+                assert all(o % 16 == 0 for o in offs)
+                inputs = [(blk[offs[i]:offs[i + 1]], d, n) for i, (_, d, n) in enumerate(inputs)]
+            corr.submit(inputs, sec, ns)
+        res.append(corr.results())
+        corr.close()
+    assert np.array_equal(res[0], res[1])
