@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (p50/p99 job latency)")
     ap.add_argument("--no-c3", action="store_true", help="skip the batched uneven-subband leg")
     ap.add_argument("--no-mux", action="store_true", help="skip the INTERLACEDVDIF muxing leg")
-    ap.add_argument("--serving-jobs", type=int, default=32)
+    ap.add_argument("--serving-jobs", type=int, default=12)
     return ap.parse_args()
 
 
@@ -236,29 +236,36 @@ def load_peaks():
 # ---------------------------------------------------------------- serving leg
 def serving_leg(args):
     """p50/p99 job latency and sustained throughput of the serving loop on a
-    seeded Poisson stream of jobs of different shapes (a bounded sample of
-    the serving workload: the full job ranges -- up to 32 stations, 16
-    subbands of 64 MHz, 2 s -- would need tens of GB of host VDIF)."""
+    seeded Poisson stream of jobs drawn from the serving workload's shape
+    ranges (4-32 stations, 1-16 subbands of 8-64 MHz, 256-8192 channels,
+    dual polarisation with cross hands); integrations of 0.1 s, the short end
+    of its 0.1-2 s range, so that the stream's VDIF (14 GB for 12 jobs) fits
+    in page-locked host memory (a 32-station, 16 x 64 MHz job holds 33 GB
+    per second of data)."""
     from fxb200 import serving
     rng = np.random.default_rng(11)
     jobs = []
     for k in range(args.serving_jobs):
-        job, nsub = serving.serving_job(rng, seed=100 + k, stations=(4, 10), subbands=(1, 4), bws=(16.0, 32.0),
-                                        nchans=(256, 512, 1024, 2048), seconds=(0.05, 0.15))
+        job, nsub = serving.serving_job(rng, seed=100 + k, stations=(4, 32), subbands=(1, 16),
+                                        bws=(8.0, 16.0, 32.0, 64.0), nchans=(256, 512, 1024, 2048, 4096, 8192),
+                                        seconds=(0.1, 0.1))
         jobs.append((job, serving.job_subints(job, nsub, seed=100 + k, pinned=True)))
-    rate = 40.0
+    rate = 20.0
     arrivals = serving.poisson_arrivals(rng, len(jobs), rate)
-    srv = serving.Server(budget_bytes=48 << 30, max_active=4)
+    srv = serving.Server(budget_bytes=96 << 30, max_active=4)
     st = serving.run_stream(srv, jobs, arrivals, xmac=args.xmac)
     phases = [srv.job_times(h) for h in srv.jobs]
     srv.close()
     phase_p50 = {k: float(np.median([p[k] for p in phases])) for k in phases[0]} if phases else {}
     smhz = sum(job.station_mhz_per_sec() * len(subs) * job.subint_ns * 1e-9 for job, subs in jobs)
+    host_gb = sum(b.nbytes for _, subs in jobs for inputs, _, _ in subs for b, _, _ in inputs) / 1e9
+    shapes = [(len(j.stations), len(j.freqs), j.freqs[0].bw_mhz, j.freqs[0].nchan) for j, _ in jobs]
     return {"jobs": st["completed"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "rtf": st["rtf"], "station_mhz_per_s": smhz / st["wall_seconds"] if st["wall_seconds"] > 0 else None,
-            "arrival_rate_hz": rate, "max_active": 4, "xmac": args.xmac, "phase_ms_p50": phase_p50,
-            "sample": "%d seeded jobs, Poisson arrivals at %.0f/s; 4-10 stations, 1-4 subbands of 16-32 MHz, "
-                      "256-2048 channels, 0.05-0.15 s each, dual pol with cross hands; station buffers in "
+            "arrival_rate_hz": rate, "max_active": 4, "hbm_budget_gb": 96, "xmac": args.xmac,
+            "phase_ms_p50": phase_p50, "vdif_gb": host_gb, "shapes": shapes,
+            "sample": "%d seeded jobs, Poisson arrivals at %.0f/s; 4-32 stations, 1-16 subbands of 8-64 MHz, "
+                      "256-8192 channels, 0.1 s each, dual pol with cross hands; station buffers in "
                       "page-locked host memory; latency = submit to core result in host memory" % (len(jobs), rate)}
 
 

@@ -224,18 +224,43 @@ def _code_byte_table(nbits: int) -> np.ndarray:
     return np.repeat(np.arange(256, dtype=np.uint8), counts)
 
 
+_CODE_POOL = {}
+
+
+def _code_pool(nbits: int) -> np.ndarray:
+    """32 MiB of payload bytes with the quantiser's code statistics (seeded)."""
+    if nbits not in _CODE_POOL:
+        table = _code_byte_table(nbits)
+        rng = _rng("codepool", nbits)
+        _CODE_POOL[nbits] = table[rng.integers(0, 65536, size=32 << 20, dtype=np.uint16)]
+    return _CODE_POOL[nbits]
+
+
 def bulk_station_frames(job: Job, s: int, frame0: int, nframes: int, seed: int) -> np.ndarray:
     """nframes VDIF frames with valid headers whose payload bytes follow the
-    quantiser's code statistics (uncorrelated across stations): the bulk
-    stand-in input for throughput measurement."""
+    quantiser's code statistics: the bulk stand-in input for throughput
+    measurement.  Payloads are runs of a seeded 32 MiB pool of code bytes
+    taken at seeded offsets (per station and block of frames), so that
+    gigabytes are produced at memory speed."""
     st = job.stations[s]
     fb = job.frame_bytes(s)
-    table = _code_byte_table(st.nbits)
+    pool = _code_pool(st.nbits)
     rng = _rng("bulk", seed, s, frame0)
     out = np.empty((nframes, fb), dtype=np.uint8)
-    out[:, VDIF_HEADER:] = table[rng.integers(0, 65536, size=(nframes, st.payload_bytes), dtype=np.uint16)]
-    for k in range(nframes):
-        out[k, :VDIF_HEADER] = vdif_header(job, s, frame0 + k, station_id=s)
+    per = max(1, (len(pool) // 2) // st.payload_bytes)          # frames per block
+    for i in range(0, nframes, per):
+        n = min(per, nframes - i)
+        off = int(rng.integers(0, len(pool) - n * st.payload_bytes + 1))
+        out[i:i + n, VDIF_HEADER:] = pool[off:off + n * st.payload_bytes].reshape(n, st.payload_bytes)
+    fps = job.frames_per_sec(s)
+    g = frame0 + np.arange(nframes, dtype=np.int64)
+    h = np.zeros((nframes, 8), dtype=np.uint32)
+    h[:, 0] = (g // fps).astype(np.uint32) & 0x3FFFFFFF
+    h[:, 1] = (g % fps).astype(np.uint32) & 0xFFFFFF
+    log2ch = int(np.log2(st.nband)) if st.nband & (st.nband - 1) == 0 else 0
+    h[:, 2] = (1 << 29) | (log2ch << 24) | ((fb // 8) & 0xFFFFFF)
+    h[:, 3] = ((st.nbits - 1) << 26) | (s & 0xFFFF)
+    out[:, :VDIF_HEADER] = h.view(np.uint8)
     return out.reshape(-1)
 
 
