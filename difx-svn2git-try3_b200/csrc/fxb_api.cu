@@ -89,6 +89,8 @@ struct fxb_ctx {
 	DevACWeight *d_acw = nullptr;
 	DevOutMap *d_om = nullptr;
 	int nbw = 0, nacw = 0, nom = 0;
+	DevZoomCopy *d_zoom = nullptr;       // zoom-band rows gathered after the F stage
+	int nzoom = 0;
 	float2 *d_core = nullptr;
 	uint8_t *d_valid = nullptr;
 	int64_t valid_stride = 0;
@@ -114,6 +116,7 @@ struct fxb_ctx {
 	// tensor-core form also keeps each group's spectra in one block
 	struct XGroup {
 		int plan0 = 0, nf = 0;
+		bool xmac = true;                         // false: spectra only (zoom-band parents), no XMAC
 		int32_t *d_idx = nullptr;
 		TcShape shape{};
 		int64_t spec_base = 0;                    // first bf16x2 value of the group's block
@@ -359,10 +362,11 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			if(taken[i]) continue;
 			const DevFreqPlan &a = ctx->h_plans[used[i]];
 			std::vector<int32_t> idx;
+			const bool ax = job.plan[used[i]].xmac;
 			for(size_t j = i; j < used.size(); j++)
 			{
 				const DevFreqPlan &b = ctx->h_plans[used[j]];
-				if(!taken[j] && b.nrow == a.nrow && b.nchan == a.nchan)
+				if(!taken[j] && b.nrow == a.nrow && b.nchan == a.nchan && job.plan[used[j]].xmac == ax)
 				{
 					taken[j] = 1;
 					idx.push_back(used[j]);
@@ -371,6 +375,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			ctx->xgroups.emplace_back();
 			ctx->xgroups.back().plan0 = used[i];
 			ctx->xgroups.back().nf = (int)idx.size();
+			ctx->xgroups.back().xmac = ax;
 			gidx.push_back(idx);
 		}
 	}
@@ -603,6 +608,18 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		if(ctx->nbw) CK(ctx, cudaMemcpyAsync(ctx->d_bw, hbw.data(), sizeof(DevBWeight) * ctx->nbw, cudaMemcpyHostToDevice, ctx->stream));
 		if(ctx->nacw) CK(ctx, cudaMemcpyAsync(ctx->d_acw, hacw.data(), sizeof(DevACWeight) * ctx->nacw, cudaMemcpyHostToDevice, ctx->stream));
 		if(ctx->nom) CK(ctx, cudaMemcpyAsync(ctx->d_om, hom.data(), sizeof(DevOutMap) * ctx->nom, cudaMemcpyHostToDevice, ctx->stream));
+		ctx->nzoom = (int)job.zooms.size();
+		if(ctx->nzoom)
+		{
+			std::vector<DevZoomCopy> hz(ctx->nzoom);
+			for(int i = 0; i < ctx->nzoom; i++)
+			{
+				const Job::ZoomCopy &z = job.zooms[i];
+				hz[i] = DevZoomCopy{z.src_freq, z.src_row, z.dst_freq, z.dst_row, z.choff, z.nchan};
+			}
+			CK(ctx, dalloc(ctx, &ctx->d_zoom, ctx->nzoom));
+			CK(ctx, cudaMemcpyAsync(ctx->d_zoom, hz.data(), sizeof(DevZoomCopy) * ctx->nzoom, cudaMemcpyHostToDevice, ctx->stream));
+		}
 	}
 
 	// staging slots
@@ -902,17 +919,24 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 		if(tuning)
 			cudaEventRecord(tn.ev[nk], st);
 	}
+	launch_zoom_gather(ctx->d_zoom, ctx->nzoom, ctx->d_plans, ctx->T, ctx->tc,
+	                   ctx->tc ? ctx->d_specn : (void *)ctx->d_spec, st);
 	cudaEventRecordWithFlags(sl.tev[2], st, evf);
 	if(ctx->f8)
 		for(const auto &g : ctx->xgroups)
-			launch_quant_fp8(g.shape, ctx->d_plans, g.d_idx, g.nf, ctx->T, (const uint32_t *)ctx->d_specn, ctx->d_spec8, st);
+			if(g.xmac)
+				launch_quant_fp8(g.shape, ctx->d_plans, g.d_idx, g.nf, ctx->T, (const uint32_t *)ctx->d_specn,
+				                 ctx->d_spec8, st);
 	for(size_t gi = 0; gi < ctx->xgroups.size(); gi++)
 	{
 		const auto &g = ctx->xgroups[gi];
 		TcShape sh = g.shape;
 		if(tuning)
-		{
 			cudaEventRecord(tn.ev[nk + 1 + gi], st);
+		if(!g.xmac)
+			continue;
+		if(tuning)
+		{
 			if(ctx->tc && !tn.xc[gi].empty())
 			{
 				const auto &c = tn.xc[gi][tn.iter % tn.xc[gi].size()];
@@ -1068,6 +1092,8 @@ fxb_status fxb_autotune(fxb_ctx *ctx, int32_t rounds)
 	size_t most = t.fc.size();
 	for(size_t g = 0; g < ng && ctx->tc; g++)
 	{
+		if(!ctx->xgroups[g].xmac)
+			continue;
 		// one CTA per SM with double-buffered accumulators, or two per SM
 		static const int depth[][3] = {{6, 4, 2}, {6, 3, 2}, {4, 3, 2}, {4, 2, 2}, {3, 2, 2}, {2, 2, 2},
 		                               {4, 2, 1}, {3, 2, 1}, {2, 2, 1}};
@@ -1112,6 +1138,13 @@ fxb_status fxb_tuning_report(const fxb_ctx *ctx, char *buf, size_t len, size_t *
 	for(size_t g = 0; g < ctx->xgroups.size(); g++)
 	{
 		const TcShape &sh = ctx->xgroups[g].shape;
+		if(!ctx->xgroups[g].xmac)
+		{
+			snprintf(line, sizeof(line), "xmac group %zu (%d inputs, %d channels): spectra only (zoom-band parents)\n",
+			         g, sh.nrow, sh.nchan);
+			r += line;
+			continue;
+		}
 		if(!ctx->tc)
 		{
 			snprintf(line, sizeof(line), "xmac group %zu: FP32 form\n", g);

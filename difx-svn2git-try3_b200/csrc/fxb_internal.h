@@ -82,6 +82,13 @@ struct Job {
 		int nbits, payload, header, nband;
 		std::vector<int> band_freq;
 		std::vector<char> band_pol;
+		// zoom bands: frequency, polarisation, parent recorded band and the
+		// parent channel of the zoom band's first channel
+		std::vector<int> zoom_freq, zoom_parent, zoom_choff;
+		std::vector<char> zoom_pol;
+		int nzoom() const { return (int)zoom_freq.size(); }
+		// frequency of band k: recorded bands, then zoom bands
+		int total_freq(int k) const { return k < nband ? band_freq[k] : zoom_freq[k - nband]; }
 		int npoly = 0, order = 0, interval = 0;
 		double poly0 = 0.0;
 		std::vector<double> coeffs;
@@ -110,7 +117,7 @@ struct Job {
 	// rows of every used frequency: (station, band) in station order
 	struct Row { int station, band; };
 	std::vector<std::vector<Row>> rows;                  // [freq]
-	std::vector<std::vector<int>> band_row;              // [station][band] -> row in its freq
+	std::vector<std::vector<int>> band_row;              // [station][band, then zoom band] -> row in its freq
 	// XMAC outputs per frequency: accumulator offsets
 	struct FreqPlan {
 		int nrow = 0;
@@ -120,6 +127,7 @@ struct Job {
 		int nout = 0;
 		std::vector<int> destA;    // [nrow*nrow] output index of V[i][j] (i<=j) or -1
 		std::vector<int> destB;    // [nrow*nrow] output index receiving conj(V[i][j]) or -1
+		bool xmac = false;         // false: spectra only (parents of zoom bands), no XMAC
 	};
 	std::vector<FreqPlan> plan;                           // [freq]
 	int64_t spec_total = 0;       // complex values of spectra for one subint
@@ -132,6 +140,9 @@ struct Job {
 		int freq, out;   // frequency and output index within it (out < 0: no accumulator)
 	};
 	std::vector<OutMap> outmap;
+	// zoom bands: spectra rows gathered from the parent band's spectra
+	struct ZoomCopy { int src_freq, src_row, dst_freq, dst_row, choff, nchan; };
+	std::vector<ZoomCopy> zooms;
 	// weight plans
 	struct BWeight { int s1, s2; int64_t dst_float; };
 	std::vector<BWeight> bweights;

@@ -2,11 +2,17 @@
 //
 // The layout restates Configuration::populateResultLengths
 // (mpifxcorr/src/configuration.cpp:2212-2440) for one configuration with one
-// phase centre, no pulsar bins, no zoom bands and no phase cal: cross
-// correlations [freq][baseline][product][nchan/avg], then baseline weights
-// (products/2 rounded up complex slots), then per datastream the
-// autocorrelations (parallel hands, then cross hands when the job has more
-// than two products), then the autocorrelation weights.
+// phase centre, no pulsar bins and no phase cal: cross correlations
+// [freq][baseline][product][nchan/avg], then baseline weights (products/2
+// rounded up complex slots), then per datastream the autocorrelations of its
+// recorded and then its zoom bands (parallel hands, then cross hands when the
+// job has more than two products), then the autocorrelation weights.
+//
+// A zoom band is a channel window of a recorded band (mode.cpp:169-208).  Its
+// frequency gets an XMAC plan of its own whose spectra rows are copied from
+// the parent bands' spectra, so that stations whose zoom bands have different
+// parents (a 16 MHz band of one station zoomed onto an 8 MHz band of another)
+// correlate like any other frequency.
 
 #include <algorithm>
 #include <cmath>
@@ -95,6 +101,63 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 			if(fb.nchan != f0.nchan || fb.bw_mhz != f0.bw_mhz)
 				return fail(err, st, FXB_ERR_UNSUPPORTED, "all bands of one station share bandwidth and channels");
 		}
+		if(in.nzoom < 0 || in.nzoom > kMaxBandsPerStation || (in.nzoom > 0 && (!in.zoom_freq || !in.zoom_pol)))
+			return fail(err, st, FXB_ERR_ARG, "bad zoom band list");
+		for(int z = 0; z < in.nzoom; z++)
+		{
+			const int zf = in.zoom_freq[z];
+			if(zf < 0 || zf >= d->nfreq)
+				return fail(err, st, FXB_ERR_ARG, "zoom frequency index out of range");
+			// zoom frequencies come after the recorded ones (configuration.cpp:2598-2610)
+			for(int b = 0; b < in.nband; b++)
+				if(zf < o.band_freq[b])
+					return fail(err, st, FXB_ERR_ARG, "a zoom frequency precedes a recorded frequency in the table");
+			// parent: the last recorded frequency, in the station's order, whose
+			// range holds the zoom band; offset in channels of the first recorded
+			// frequency (configuration.cpp:1734-1754)
+			const fxb_freq &zq = job.freqs[zf];
+			const double lo = zq.freq_mhz - (zq.lower_sideband ? zq.bw_mhz : 0.0), hi = lo + zq.bw_mhz;
+			int parent = -1, off = 0;
+			for(int b = 0; b < in.nband; b++)
+			{
+				if(std::find(o.band_freq.begin(), o.band_freq.begin() + b, o.band_freq[b]) != o.band_freq.begin() + b)
+					continue;
+				const fxb_freq &pf = job.freqs[o.band_freq[b]];
+				const double plo = pf.freq_mhz - (pf.lower_sideband ? pf.bw_mhz : 0.0), phi = plo + pf.bw_mhz;
+				if(hi <= phi && lo >= plo)
+				{
+					parent = o.band_freq[b];
+					off = (int)(((lo - plo) / f0.bw_mhz) * f0.nchan + 0.5);
+				}
+			}
+			if(parent < 0)
+				return fail(err, st, FXB_ERR_ARG, "zoom band outside every recorded band");
+			const fxb_freq &pf = job.freqs[parent];
+			if(std::fabs(zq.bw_mhz / zq.nchan - pf.bw_mhz / pf.nchan) > 1e-9)
+				return fail(err, st, FXB_ERR_ARG, "zoom channel width differs from its parent's");
+			// the parent band: the first recorded band of that frequency in the
+			// zoom band's polarisation (configuration.cpp:1245-1258)
+			int pb = -1;
+			for(int b = 0; b < in.nband && pb < 0; b++)
+				if(o.band_freq[b] == parent && o.band_pol[b] == in.zoom_pol[z])
+					pb = b;
+			if(pb < 0)
+				return fail(err, st, FXB_ERR_ARG, "zoom band without a parent band of its polarisation");
+			if(zq.lower_sideband || pf.lower_sideband)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "zoom bands of lower-sideband bands");
+			if(off < 0 || off + zq.nchan > pf.nchan)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "zoom band channels outside its parent");
+			// the zoom band's autocorrelation is the parent's, averaged by the
+			// station's first recorded frequency (mode.cpp:389-397, 1399-1424):
+			// the same as averaging the window itself only when the averaging
+			// agrees and the window starts on an averaging boundary
+			if(zq.chans_to_avg != f0.chans_to_avg || off % f0.chans_to_avg)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "zoom averaging differs from the station's recorded averaging");
+			o.zoom_freq.push_back(zf);
+			o.zoom_pol.push_back(in.zoom_pol[z]);
+			o.zoom_parent.push_back(pb);
+			o.zoom_choff.push_back(off);
+		}
 		job.stations.push_back(o);
 	}
 	for(int b = 0; b < d->nbaseline; b++)
@@ -120,9 +183,10 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 					if(o.prod_freq[q] == f)
 						return fail(err, st, FXB_ERR_ARG, "products of one frequency must be contiguous");
 			int b1 = o.prod_b1[p], b2 = o.prod_b2[p];
-			if(b1 < 0 || b1 >= job.stations[o.ds1].nband || b2 < 0 || b2 >= job.stations[o.ds2].nband)
+			const Job::Station &s1 = job.stations[o.ds1], &s2 = job.stations[o.ds2];
+			if(b1 < 0 || b1 >= s1.nband + s1.nzoom() || b2 < 0 || b2 >= s2.nband + s2.nzoom())
 				return fail(err, st, FXB_ERR_ARG, "product band index out of range");
-			if(job.stations[o.ds1].band_freq[b1] != f || job.stations[o.ds2].band_freq[b2] != f)
+			if(s1.total_freq(b1) != f || s2.total_freq(b2) != f)
 				return fail(err, st, FXB_ERR_UNSUPPORTED, "product bands must record the product frequency");
 		}
 		job.baselines.push_back(o);
@@ -223,9 +287,9 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 	for(int s = 0; s < S; s++)
 	{
 		job.acoff[s] = idx;
-		for(int bnd = 0; bnd < job.stations[s].nband; bnd++)
+		for(int bnd = 0; bnd < job.stations[s].nband + job.stations[s].nzoom(); bnd++)
 		{
-			int fi = job.stations[s].band_freq[bnd];
+			int fi = job.stations[s].total_freq(bnd);
 			if(job.freqused[fi] || job.equivused[fi])
 				idx += (int64_t)job.bandsperautocorr * job.freqs[fi].nchan / job.freqs[fi].chans_to_avg;
 		}
@@ -234,9 +298,9 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 	{
 		job.acwoff[s] = idx;
 		int toadd = 0;
-		for(int bnd = 0; bnd < job.stations[s].nband; bnd++)
+		for(int bnd = 0; bnd < job.stations[s].nband + job.stations[s].nzoom(); bnd++)
 		{
-			int fi = job.stations[s].band_freq[bnd];
+			int fi = job.stations[s].total_freq(bnd);
 			if(job.freqused[fi] || job.equivused[fi])
 				toadd += job.bandsperautocorr;
 		}
@@ -257,25 +321,71 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 		}
 
 	// rows per frequency, spectra and accumulator plans
+	// (F-stage rows: recorded bands of frequencies with output, and recorded
+	// bands that parent a zoom band with output; then the zoom bands of
+	// frequencies with output, whose rows are gathered from their parents)
+	auto fout = [&](int f) { return job.freqused[f] || job.equivused[f]; };
+	const bool writecross = job.write_autocorrs && job.maxproducts > 2;
 	job.rows.assign(F, {});
 	job.band_row.assign(S, {});
 	for(int s = 0; s < S; s++)
 	{
-		job.band_row[s].assign(job.stations[s].nband, -1);
-		for(int bnd = 0; bnd < job.stations[s].nband; bnd++)
+		const Job::Station &js = job.stations[s];
+		job.band_row[s].assign(js.nband + js.nzoom(), -1);
+		std::vector<int> parent(js.nband, 0);
+		for(int z = 0; z < js.nzoom(); z++)
+			if(fout(js.zoom_freq[z]))
+				parent[js.zoom_parent[z]] = 1;
+		for(int bnd = 0; bnd < js.nband; bnd++)
 		{
-			int f = job.stations[s].band_freq[bnd];
-			if(!(job.freqused[f] || job.equivused[f]))
+			int f = js.band_freq[bnd];
+			if(!(fout(f) || parent[bnd]))
 				continue;
 			job.band_row[s][bnd] = (int)job.rows[f].size();
 			job.rows[f].push_back({s, bnd});
+		}
+	}
+	for(int s = 0; s < S; s++)
+	{
+		const Job::Station &js = job.stations[s];
+		for(int z = 0; z < js.nzoom(); z++)
+		{
+			const int f = js.zoom_freq[z];
+			for(int y = 0; y < z; y++)
+				if(js.zoom_freq[y] == f && js.zoom_pol[y] == js.zoom_pol[z])
+					return fail(err, st, FXB_ERR_ARG, "duplicate zoom band");
+			if(!fout(f))
+				continue;
+			// a zoom band's cross-hand autocorrelation is its parent's
+			// (mode.cpp:389-397): the station's first two zoom bands on this
+			// frequency must then zoom the parent frequency's first two bands
+			if(writecross)
+			{
+				const int pf = js.band_freq[js.zoom_parent[z]];
+				std::vector<int> rec, zb;
+				for(int b = 0; b < js.nband; b++)
+					if(js.band_freq[b] == pf) rec.push_back(b);
+				for(int y = 0; y < js.nzoom(); y++)
+					if(js.zoom_freq[y] == f) zb.push_back(js.zoom_parent[y]);
+				if(rec.size() >= 2)
+				{
+					std::vector<int> a(rec.begin(), rec.begin() + 2);
+					std::sort(a.begin(), a.end());
+					std::sort(zb.begin(), zb.end());
+					if(zb != a)
+						return fail(err, st, FXB_ERR_UNSUPPORTED,
+						            "cross-hand autocorrelations need each zoom frequency in the parent's first two bands");
+				}
+			}
+			job.band_row[s][js.nband + z] = (int)job.rows[f].size();
+			job.rows[f].push_back({s, js.nband + z});
 		}
 	}
 	job.plan.assign(F, {});
 	const int T = job.blockspersend;
 	std::vector<std::vector<int>> crossout(S);     // [s][band] -> cross-pol output index, -1
 	for(int s = 0; s < S; s++)
-		crossout[s].assign(job.stations[s].nband, -1);
+		crossout[s].assign(job.stations[s].nband + job.stations[s].nzoom(), -1);
 	int64_t spec = 0, acc = 0;
 	for(int f = 0; f < F; f++)
 	{
@@ -291,6 +401,18 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 		pl.destA.assign((size_t)pl.nrow * pl.nrow, -1);
 		pl.destB.assign((size_t)pl.nrow * pl.nrow, -1);
 		pl.acc_off = acc;
+		pl.xmac = fout(f);
+		for(int r = 0; r < pl.nrow; r++)
+		{
+			const Job::Row &row = job.rows[f][r];
+			const Job::Station &js = job.stations[row.station];
+			if(row.band < js.nband)
+				continue;
+			const int z = row.band - js.nband, pb = js.zoom_parent[z];
+			job.zooms.push_back({js.band_freq[pb], job.band_row[row.station][pb], f, r, js.zoom_choff[z], pl.nchan});
+		}
+		if(!pl.xmac)
+			continue;
 		int nout = 0;
 		// baseline products, in core-result order
 		for(int b = 0; b < B; b++)
@@ -330,8 +452,9 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 			for(int s = 0; s < S; s++)
 			{
 				int idxs[2], cnt = 0;
-				for(int bnd = 0; bnd < job.stations[s].nband && cnt < 2; bnd++)
-					if(job.stations[s].band_freq[bnd] == f) idxs[cnt++] = bnd;
+				const Job::Station &js = job.stations[s];
+				for(int bnd = 0; bnd < js.nband + js.nzoom() && cnt < 2; bnd++)
+					if(js.total_freq(bnd) == f) idxs[cnt++] = bnd;
 				if(cnt < 2) continue;
 				int r0 = job.band_row[s][idxs[0]], r1 = job.band_row[s][idxs[1]];
 				int o01 = nout++, o10 = nout++;
@@ -347,16 +470,17 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 	job.spec_total = spec;
 	job.acc_total = acc;
 
-	// autocorrelation outputs and weights (core.cpp:1266-1363)
-	bool writecross = job.write_autocorrs && job.maxproducts > 2;
+	// autocorrelation outputs and weights (core.cpp:1266-1363); a zoom band's
+	// weight is its parent band's (core.cpp:1311-1322), which is the
+	// station's FFT weight like every band's
 	for(int s = 0; s < S; s++)
 	{
 		int64_t ridx = job.acoff[s];
 		int64_t widx = 2 * job.acwoff[s];
 		for(int pass = 0; pass < (writecross ? 2 : 1); pass++)
-			for(int bnd = 0; bnd < job.stations[s].nband; bnd++)
+			for(int bnd = 0; bnd < job.stations[s].nband + job.stations[s].nzoom(); bnd++)
 			{
-				int f = job.stations[s].band_freq[bnd];
+				int f = job.stations[s].total_freq(bnd);
 				if(!(job.freqused[f] || job.equivused[f])) continue;
 				const Job::FreqPlan &pl = job.plan[f];
 				int r = job.band_row[s][bnd];

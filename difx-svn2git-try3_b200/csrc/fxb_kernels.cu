@@ -525,6 +525,41 @@ void launch_vdif_unpack(const uint8_t *data, int64_t nbytes, int payload, int he
 	k_vdif_unpack<<<1, 256, nf, stream>>>(data, nbytes, payload, header, nchan, nbits, offsetsamples, nsamp, out, good);
 }
 
+// ---------------------------------------------------------------- zoom bands
+// A zoom band's spectra are the channels [choff, choff + nchan) of its parent
+// band's (mode.cpp:169-208): one CTA per (FFT, zoom row) copies them into the
+// zoom frequency's own spectra rows, FP32 [t][row][chan] (float2) or the
+// tensor-core form's blocked [t][block][row][tcb] (bf16x2 as uint32).
+__device__ __forceinline__ int64_t spec_index(const DevFreqPlan &p, int t, int row, int c)
+{
+	if(p.tcb == 0)
+		return p.spec_off + ((int64_t)t * p.nrow + row) * p.nchan + c;
+	return p.spec_off + (((int64_t)t * p.tnblk + c / p.tcb) * p.nrow + row) * p.tcb + c % p.tcb;
+}
+
+template <typename V>
+__global__ void __launch_bounds__(256) k_zoom_gather(const DevZoomCopy *__restrict__ zc,
+                                                     const DevFreqPlan *__restrict__ plans, V *__restrict__ spec)
+{
+	const DevZoomCopy z = zc[blockIdx.y];
+	const int t = blockIdx.x;
+	const DevFreqPlan src = plans[z.src_plan], dst = plans[z.dst_plan];
+	for(int c = threadIdx.x; c < z.nchan; c += blockDim.x)
+		spec[spec_index(dst, t, z.dst_row, c)] = spec[spec_index(src, t, z.src_row, z.choff + c)];
+}
+
+void launch_zoom_gather(const DevZoomCopy *zc, int nzc, const DevFreqPlan *plans, int T, bool tc, void *spec,
+                        cudaStream_t stream)
+{
+	if(nzc <= 0 || T <= 0)
+		return;
+	const dim3 grid(T, nzc);
+	if(tc)
+		k_zoom_gather<uint32_t><<<grid, 256, 0, stream>>>(zc, plans, (uint32_t *)spec);
+	else
+		k_zoom_gather<float2><<<grid, 256, 0, stream>>>(zc, plans, (float2 *)spec);
+}
+
 void upload_lut8(cudaStream_t stream)
 {
 	float lut[256];

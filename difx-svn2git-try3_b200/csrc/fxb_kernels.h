@@ -41,6 +41,12 @@ struct DevACWeight {
 	int64_t dst;
 };
 
+// One zoom-band row: spectra channels [choff, choff + nchan) of row src_row
+// of plan src_plan, copied to row dst_row of plan dst_plan.
+struct DevZoomCopy {
+	int32_t src_plan, src_row, dst_plan, dst_row, choff, nchan;
+};
+
 void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8_t *valid, int64_t valid_stride,
                         int S, cudaStream_t stream);
 // the subint time is read from sub[s].subsec / subns
@@ -145,6 +151,11 @@ void launch_quant_fp8(const TcShape &s, const DevFreqPlan *dplans, const int32_t
 // FP32 cross-multiply-accumulate of one frequency into acc.
 void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, const float2 *spec, float2 *acc,
                       cudaStream_t stream);
+
+// Zoom-band spectra from their parents' (after the F stage, before the
+// XMAC): tc selects the tensor-core form's bf16x2 spectra.
+void launch_zoom_gather(const DevZoomCopy *zc, int nzc, const DevFreqPlan *plans, int T, bool tc, void *spec,
+                        cudaStream_t stream);
 
 void launch_weights(const DevBWeight *bw, int nbw, const DevACWeight *acw, int nacw, const FftParam *params, int T,
                     float *bwacc, float *acwacc, cudaStream_t stream);

@@ -52,6 +52,9 @@ class Station:
     header_bytes: int = 32
     polys: List[DelayPoly] = dataclasses.field(default_factory=list)
     clock_us: float = 0.0             # constant clock offset folded into the model
+    # zoom bands (freq index, pol): channel windows of a recorded band of the
+    # same polarisation; a baseline names zoom band z as band nband + z
+    zoom_bands: List[Tuple[int, str]] = dataclasses.field(default_factory=list)
 
     def recorded_freqs(self) -> List[int]:
         seen: List[int] = []
@@ -63,6 +66,10 @@ class Station:
     @property
     def nband(self) -> int:
         return len(self.bands)
+
+    def band(self, b: int) -> Tuple[int, str]:
+        """(freq index, pol) of band b: recorded bands, then zoom bands."""
+        return self.bands[b] if b < len(self.bands) else self.zoom_bands[b - len(self.bands)]
 
 
 @dataclasses.dataclass
@@ -159,12 +166,40 @@ class Job:
                 raise ValueError("payload must hold whole samples")
             if self.samples_per_sec(s) % self.frame_samples(s):
                 raise ValueError("whole frames per second required")
+            for f, pol in st.zoom_bands:
+                if self.zoom_parent(s, f, pol) is None:
+                    raise ValueError("zoom band outside every recorded band of its polarisation")
         for b in self.baselines:
             for f, pp in b.products:
                 for b1, b2 in pp:
-                    if self.stations[b.ds1].bands[b1][0] != f or self.stations[b.ds2].bands[b2][0] != f:
+                    if self.stations[b.ds1].band(b1)[0] != f or self.stations[b.ds2].band(b2)[0] != f:
                         raise ValueError("product bands must record the baseline frequency")
         self.blocks_per_send()
+
+    def zoom_parent(self, s: int, f: int, pol: str):
+        """(recorded band index, channel offset) of station s's zoom band on
+        frequency f in pol: the last recorded frequency whose range contains
+        the zoom band, its band of the same polarisation, and the offset of the
+        zoom band edge in parent channels (configuration.cpp:1734-1754)."""
+        st = self.stations[s]
+        z = self.freqs[f]
+        lo = z.freq_mhz - (z.bw_mhz if z.sideband == "L" else 0.0)
+        parent = None
+        for rf in st.recorded_freqs():
+            p = self.freqs[rf]
+            plo = p.freq_mhz - (p.bw_mhz if p.sideband == "L" else 0.0)
+            if lo + z.bw_mhz <= plo + p.bw_mhz and lo >= plo:
+                parent = rf
+        if parent is None:
+            return None
+        r0 = self.freqs[st.bands[0][0]]
+        p = self.freqs[parent]
+        plo = p.freq_mhz - (p.bw_mhz if p.sideband == "L" else 0.0)
+        off = int((lo - plo) / r0.bw_mhz * r0.nchan + 0.5)
+        for k, (ff, pp) in enumerate(st.bands):
+            if ff == parent and pp == pol:
+                return k, off
+        return None
 
 
 def full_job(nstation: int, freqs: Sequence[Freq], pols: str = "RL", full_pol: bool = True,
@@ -208,3 +243,41 @@ def gcd_list(v: Sequence[int]) -> int:
     for x in v:
         g = math.gcd(g, x)
     return g
+
+
+def add_zoom_bands(job: Job, zooms: Sequence[Tuple[int, float, float]], keep_parents: bool = True,
+                   chans_to_avg: int = 1) -> Job:
+    """Append zoom frequencies to a job, as vex2difx writes them.
+
+    Each (parent freq index, offset MHz, width MHz) becomes a frequency-table
+    entry after the recorded ones, with the parent's channel width.  Every
+    station that records the parent gets one zoom band per recorded
+    polarisation, in the parent bands' order.  Every baseline correlates the
+    zoom frequency with the parent frequency's products mapped onto the zoom
+    bands.  Without keep_parents the parents' own products are dropped, so
+    that only the zoom windows are correlated."""
+    nrec = len(job.freqs)
+    zfreqs = []
+    for parent, off, bw in zooms:
+        p = job.freqs[parent]
+        nchan = int(round(bw / p.bw_mhz * p.nchan))
+        job.freqs.append(Freq(p.freq_mhz + off, bw, nchan, p.sideband, chans_to_avg))
+        zfreqs.append((parent, len(job.freqs) - 1))
+    zindex = []                      # per station: {(parent, band): zoom band index}
+    for st in job.stations:
+        m = {}
+        for parent, zf in zfreqs:
+            for k, (f, pol) in enumerate(st.bands):
+                if f == parent:
+                    m[(parent, zf, k)] = st.nband + len(st.zoom_bands)
+                    st.zoom_bands.append((zf, pol))
+        zindex.append(m)
+    for b in job.baselines:
+        prods = [x for x in b.products if keep_parents or x[0] >= nrec]
+        for parent, zf in zfreqs:
+            for f, pp in b.products:
+                if f == parent:
+                    prods.append((zf, [(zindex[b.ds1][(parent, zf, b1)], zindex[b.ds2][(parent, zf, b2)])
+                                       for b1, b2 in pp]))
+        b.products = prods
+    return job

@@ -32,7 +32,8 @@ class FxbFreq(ctypes.Structure):
 class FxbStation(ctypes.Structure):
     _fields_ = [("nbits", ctypes.c_int32), ("payload_bytes", ctypes.c_int32), ("header_bytes", ctypes.c_int32),
                 ("nband", ctypes.c_int32), ("band_freq", ctypes.POINTER(ctypes.c_int32)),
-                ("band_pol", ctypes.c_char_p)]
+                ("band_pol", ctypes.c_char_p), ("nzoom", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("zoom_freq", ctypes.POINTER(ctypes.c_int32)), ("zoom_pol", ctypes.c_char_p)]
 
 
 class FxbBaseline(ctypes.Structure):
@@ -63,9 +64,14 @@ class DescHolder:
         for i, s in enumerate(job.stations):
             bf = (ctypes.c_int32 * s.nband)(*[b[0] for b in s.bands])
             bp = ctypes.create_string_buffer("".join(b[1] for b in s.bands).encode(), s.nband + 1)
-            self.keep += [bf, bp]
+            nz = len(s.zoom_bands)
+            zf = (ctypes.c_int32 * max(nz, 1))(*[b[0] for b in s.zoom_bands])
+            zp = ctypes.create_string_buffer("".join(b[1] for b in s.zoom_bands).encode(), nz + 1)
+            self.keep += [bf, bp, zf, zp]
             st[i] = FxbStation(s.nbits, s.payload_bytes, s.header_bytes, s.nband,
-                               ctypes.cast(bf, ctypes.POINTER(ctypes.c_int32)), ctypes.cast(bp, ctypes.c_char_p))
+                               ctypes.cast(bf, ctypes.POINTER(ctypes.c_int32)), ctypes.cast(bp, ctypes.c_char_p),
+                               nz, 0, ctypes.cast(zf, ctypes.POINTER(ctypes.c_int32)),
+                               ctypes.cast(zp, ctypes.c_char_p))
         bl = (FxbBaseline * len(job.baselines))()
         for i, b in enumerate(job.baselines):
             pf, p1, p2 = [], [], []
@@ -353,12 +359,13 @@ class Correlator:
     def spectra(self, freq: int) -> np.ndarray:
         T = self.job.blocks_per_send()
         nchan = self.job.freqs[freq].nchan
-        rows = sum(1 for st in self.job.stations for f, _ in st.bands if f == freq)
-        out = np.zeros(T * nchan * rows * 2, dtype=np.float32)
+        # rows: the recorded and zoom bands on this frequency (at most)
+        rows = sum(1 for st in self.job.stations for f, _ in st.bands + st.zoom_bands if f == freq)
+        out = np.zeros(T * nchan * max(rows, 1) * 2, dtype=np.float32)
         nt, nr = ctypes.c_int32(), ctypes.c_int32()
         check(lib().fxb_read_spectra(self.ctx, freq, _fptr(out), out.size, ctypes.byref(nt), ctypes.byref(nr)),
               self.ctx, "read_spectra")
-        x = out.reshape(nt.value, nr.value, nchan, 2)
+        x = out[:nt.value * nr.value * nchan * 2].reshape(nt.value, nr.value, nchan, 2)
         return x[..., 0] + 1j * x[..., 1]
 
     def fft_weights(self) -> np.ndarray:

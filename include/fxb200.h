@@ -61,7 +61,17 @@ typedef struct {
 } fxb_freq;
 
 /* One datastream: a single-thread VDIF stream whose channels are the
- * recorded bands (DATASTREAM TABLE, configuration.cpp:1433-1800). */
+ * recorded bands (DATASTREAM TABLE, configuration.cpp:1433-1800).
+ *
+ * Zoom bands (ZOOM FREQ / ZOOM BAND entries, configuration.cpp:1719-1770)
+ * are channel windows of a recorded band: zoom band z is the frequency-table
+ * entry zoom_freq[z] in polarisation zoom_pol[z].  Its parent is the recorded
+ * band of the same polarisation whose frequency range contains it, and its
+ * first channel is the zoom band edge's offset into the parent, in parent
+ * channels (configuration.cpp:1734-1754); its channel width must equal the
+ * parent's.  A baseline product names zoom band z of a station as band index
+ * nband + z.  Zoom frequencies must come after the station's recorded
+ * frequencies in the frequency table (configuration.cpp:2598-2610). */
 typedef struct {
 	int32_t nbits;            /* 2 or 8 */
 	int32_t payload_bytes;    /* VDIF payload bytes per frame */
@@ -69,6 +79,10 @@ typedef struct {
 	int32_t nband;            /* recorded bands = VDIF channels */
 	const int32_t *band_freq; /* [nband] frequency-table index of each band */
 	const char *band_pol;     /* [nband] 'R'/'L'/'X'/'Y' */
+	int32_t nzoom;            /* zoom bands (0: none; the pointers may be null) */
+	int32_t reserved;
+	const int32_t *zoom_freq; /* [nzoom] frequency-table index of each zoom band */
+	const char *zoom_pol;     /* [nzoom] polarisation of each zoom band */
 } fxb_station;
 
 /* One baseline (BASELINE TABLE, configuration.cpp:1059-1120): products are
@@ -77,8 +91,8 @@ typedef struct {
 	int32_t ds1, ds2;         /* datastream indices, ds1 < ds2 */
 	int32_t nprod;
 	const int32_t *prod_freq; /* [nprod] frequency-table index */
-	const int32_t *prod_band1;/* [nprod] band index within ds1 */
-	const int32_t *prod_band2;/* [nprod] band index within ds2 */
+	const int32_t *prod_band1;/* [nprod] band index within ds1 (>= nband: zoom band) */
+	const int32_t *prod_band2;/* [nprod] band index within ds2 (>= nband: zoom band) */
 } fxb_baseline;
 
 typedef struct {

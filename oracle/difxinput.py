@@ -109,7 +109,17 @@ def write_job_files(job: Job, outdir: str, name: str = "job",
         for k, (f, pol) in enumerate(st.bands):
             s.append(_kv("REC BAND %d POL" % k, pol))
             s.append(_kv("REC BAND %d INDEX" % k, rf.index(f)))
-        s.append(_kv("NUM ZOOM FREQS", 0))
+        zf = []
+        for f, _ in st.zoom_bands:
+            if f not in zf:
+                zf.append(f)
+        s.append(_kv("NUM ZOOM FREQS", len(zf)))
+        for j, f in enumerate(zf):
+            s.append(_kv("ZOOM FREQ INDEX %d" % j, f))
+            s.append(_kv("NUM ZOOM POLS %d" % j, sum(1 for ff, _ in st.zoom_bands if ff == f)))
+        for k, (f, pol) in enumerate(st.zoom_bands):
+            s.append(_kv("ZOOM BAND %d POL" % k, pol))
+            s.append(_kv("ZOOM BAND %d INDEX" % k, zf.index(f)))
     s.append("\n# BASELINE TABLE ###!\n")
     s.append(_kv("BASELINE ENTRIES", nbl))
     for i, b in enumerate(job.baselines):

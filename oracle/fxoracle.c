@@ -6,8 +6,8 @@
  * library never links or calls it.
  *
  * It restates, for the job subset described by include/fxb200.h (single
- * configuration, VDIF single-thread datastreams, real sampling, no zoom bands,
- * no pulsar binning, one phase centre, no phase cal), the algorithm of:
+ * configuration, VDIF single-thread datastreams, real sampling, no pulsar
+ * binning, one phase centre, no phase cal), the algorithm of:
  *   - the core-result layout   Configuration::populateResultLengths
  *                              (mpifxcorr/src/configuration.cpp:2212-2440)
  *   - the delay interpolator   Model::calculateDelayInterpolator
@@ -24,6 +24,11 @@
  *   - the XMAC and weights     Core::processdata (core.cpp:877-972, 998-1045)
  *                              and the result merges (core.cpp:1774-1787,
  *                              1068-1086, 1266-1363)
+ *   - zoom bands               parent and channel offset
+ *                              (configuration.cpp:1734-1754), spectra and
+ *                              autocorrelations as views into the parent band
+ *                              (mode.cpp:169-208, 380-398), weights from the
+ *                              parent band (core.cpp:1311-1322)
  *
  * Integer and index decisions (frame validity, sample offsets, nearest
  * sample, integer delay, weights, channel order) follow the reference's
@@ -62,6 +67,8 @@ typedef struct fxo_job {
 	int *nbits, *payload, *header, *nband;
 	int **band_freq;
 	char **band_pol;
+	int *nzoom;
+	int **zoom_freq, **zoom_parent, **zoom_choff;   /* parent: recorded band index */
 	oracle_poly *poly;
 	/* baselines: products grouped per freq in given order */
 	int *ds1, *ds2, *nprod;
@@ -112,6 +119,12 @@ static void dfft(dcx *x, int n)
 }
 
 static int station_nchan(const fxo_job *j, int s) { return j->freqs[j->band_freq[s][0]].nchan; }
+/* frequency of band k of station s: recorded bands, then zoom bands
+ * (Configuration::getDTotalFreqIndex) */
+static int total_band_freq(const fxo_job *j, int s, int k)
+{
+	return k < j->nband[s] ? j->band_freq[s][k] : j->zoom_freq[s][k - j->nband[s]];
+}
 static double station_bw(const fxo_job *j, int s) { return j->freqs[j->band_freq[s][0]].bw_mhz; }
 
 /* samplegranularity (format_vdif.c:3845-3849) */
@@ -246,6 +259,53 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 		memcpy(j->band_freq[s], st->band_freq, sizeof(int) * st->nband);
 		memcpy(j->band_pol[s], st->band_pol, st->nband);
 	}
+	/* zoom bands: the last recorded frequency (in local order) whose range
+	 * holds the zoom band is its parent, the offset counts channels of the
+	 * first recorded frequency (configuration.cpp:1734-1754); the parent band
+	 * is the first recorded band of that frequency in the zoom band's
+	 * polarisation (configuration.cpp:1245-1258) */
+	j->nzoom = (int *)calloc(d->nstation, sizeof(int));
+	j->zoom_freq = (int **)calloc(d->nstation, sizeof(int *));
+	j->zoom_parent = (int **)calloc(d->nstation, sizeof(int *));
+	j->zoom_choff = (int **)calloc(d->nstation, sizeof(int *));
+	for(s = 0; s < d->nstation; s++)
+	{
+		const fxb_station *st = &d->stations[s];
+		int z, nz = st->nzoom > 0 ? st->nzoom : 0;
+		j->nzoom[s] = nz;
+		j->zoom_freq[s] = (int *)calloc(nz + 1, sizeof(int));
+		j->zoom_parent[s] = (int *)calloc(nz + 1, sizeof(int));
+		j->zoom_choff[s] = (int *)calloc(nz + 1, sizeof(int));
+		for(z = 0; z < nz; z++)
+		{
+			const fxb_freq *zf = &d->freqs[st->zoom_freq[z]];
+			const fxb_freq *r0 = &d->freqs[st->band_freq[0]];
+			double lo = zf->freq_mhz - (zf->lower_sideband ? zf->bw_mhz : 0.0), hi = lo + zf->bw_mhz;
+			int k, parent = -1, off = 0;
+			j->zoom_freq[s][z] = st->zoom_freq[z];
+			for(k = 0; k < st->nband; k++)
+			{
+				int q, first = 1;
+				const fxb_freq *pf = &d->freqs[st->band_freq[k]];
+				double plo = pf->freq_mhz - (pf->lower_sideband ? pf->bw_mhz : 0.0), phi = plo + pf->bw_mhz;
+				for(q = 0; q < k; q++) if(st->band_freq[q] == st->band_freq[k]) first = 0;
+				if(!first) continue;
+				if(hi <= phi && lo >= plo)
+				{
+					parent = st->band_freq[k];
+					off = (int)(((lo - plo) / r0->bw_mhz) * r0->nchan + 0.5);
+				}
+			}
+			j->zoom_parent[s][z] = -1;
+			for(k = 0; k < st->nband && parent >= 0; k++)
+				if(st->band_freq[k] == parent && st->band_pol[k] == st->zoom_pol[z])
+				{
+					j->zoom_parent[s][z] = k;
+					break;
+				}
+			j->zoom_choff[s][z] = off;
+		}
+	}
 	j->ds1 = (int *)calloc(d->nbaseline, sizeof(int));
 	j->ds2 = (int *)calloc(d->nbaseline, sizeof(int));
 	j->nprod = (int *)calloc(d->nbaseline, sizeof(int));
@@ -347,9 +407,9 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 		{
 			int k;
 			j->acoff[s] = idx;
-			for(k = 0; k < j->nband[s]; k++)
+			for(k = 0; k < j->nband[s] + j->nzoom[s]; k++)
 			{
-				int fi = j->band_freq[s][k];
+				int fi = total_band_freq(j, s, k);
 				if(j->freqused[fi] || j->equivused[fi])
 					idx += (int64_t)j->bandsperautocorr * j->freqs[fi].nchan / j->freqs[fi].chans_to_avg;
 			}
@@ -358,9 +418,9 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 		{
 			int k, toadd = 0;
 			j->acwoff[s] = idx;
-			for(k = 0; k < j->nband[s]; k++)
+			for(k = 0; k < j->nband[s] + j->nzoom[s]; k++)
 			{
-				int fi = j->band_freq[s][k];
+				int fi = total_band_freq(j, s, k);
 				if(j->freqused[fi] || j->equivused[fi])
 					toadd += j->bandsperautocorr;
 			}
@@ -394,6 +454,9 @@ void fxo_destroy(fxo_job *j)
 	{
 		free(j->band_freq[i]);
 		free(j->band_pol[i]);
+		free(j->zoom_freq[i]);
+		free(j->zoom_parent[i]);
+		free(j->zoom_choff[i]);
 		free(j->poly[i].coeffs);
 	}
 	for(i = 0; i < j->nbaseline; i++)
@@ -404,6 +467,7 @@ void fxo_destroy(fxo_job *j)
 	}
 	free(j->freqs); free(j->nbits); free(j->payload); free(j->header); free(j->nband);
 	free(j->band_freq); free(j->band_pol); free(j->poly);
+	free(j->nzoom); free(j->zoom_freq); free(j->zoom_parent); free(j->zoom_choff);
 	free(j->ds1); free(j->ds2); free(j->nprod); free(j->prod_freq); free(j->prod_b1); free(j->prod_b2);
 	free(j->freqused); free(j->equivused); free(j->bloff); free(j->bwoff); free(j->acoff); free(j->acwoff);
 	free(j);
@@ -759,13 +823,18 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 			float wsum = 0.0f;   /* float sequential sum, as core.cpp:1041 */
 			if(f != lastf) { pf = 0; lastf = f; }
 			base = j->bloff[f * B + b];
+			/* a zoom band reads its parent's spectrum from its first channel */
+			int k1 = j->prod_b1[b][p], k2 = j->prod_b2[b][p], o1 = 0, o2 = 0;
+			int n1 = station_nchan(j, s1), n2 = station_nchan(j, s2);
+			if(k1 >= nb1) { o1 = j->zoom_choff[s1][k1 - nb1]; k1 = j->zoom_parent[s1][k1 - nb1]; }
+			if(k2 >= nb2) { o2 = j->zoom_choff[s2][k2 - nb2]; k2 = j->zoom_parent[s2][k2 - nb2]; }
 			for(c = 0; c < nchan; c++)
 			{
 				double re = 0.0, im = 0.0;
 				for(t = 0; t < T; t++)
 				{
-					dcx x1 = spec[s1][((size_t)t * nb1 + j->prod_b1[b][p]) * nchan + c];
-					dcx x2 = spec[s2][((size_t)t * nb2 + j->prod_b2[b][p]) * nchan + c];
+					dcx x1 = spec[s1][((size_t)t * nb1 + k1) * n1 + o1 + c];
+					dcx x2 = spec[s2][((size_t)t * nb2 + k2) * n2 + o2 + c];
 					re += x1.re * x2.re + x1.im * x2.im;
 					im += x1.im * x2.re - x1.re * x2.im;
 				}
@@ -787,26 +856,53 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 			int nchan = station_nchan(j, s), nb = j->nband[s], pass;
 			int64_t ridx = j->acoff[s];
 			int64_t widx = j->acwoff[s] * 2;
+			/* the station's averaging of its recorded bands (Mode::averageFrequency,
+			 * mode.cpp:1399-1424, channelstoaverage of the first recorded band) */
+			int savg = j->freqs[j->band_freq[s][0]].chans_to_avg;
 			for(pass = 0; pass < (writecross ? 2 : 1); pass++)
-				for(b = 0; b < nb; b++)
+				for(b = 0; b < nb + j->nzoom[s]; b++)
 				{
-					int fi = j->band_freq[s][b];
+					int fi = total_band_freq(j, s, b);
 					int avg = j->freqs[fi].chans_to_avg;
-					double *ac = acc_ac[s] + ((size_t)b * 2 + pass) * nchan * 2;
 					if(!(j->freqused[fi] || j->equivused[fi])) continue;
-					for(c = 0; c < nchan; c++)
+					if(b < nb)
 					{
-						coreresult[2 * (ridx + c / avg)] += ac[2 * c] / avg;
-						coreresult[2 * (ridx + c / avg) + 1] += ac[2 * c + 1] / avg;
+						double *ac = acc_ac[s] + ((size_t)b * 2 + pass) * nchan * 2;
+						for(c = 0; c < nchan; c++)
+						{
+							coreresult[2 * (ridx + c / avg)] += ac[2 * c] / avg;
+							coreresult[2 * (ridx + c / avg) + 1] += ac[2 * c + 1] / avg;
+						}
+						ridx += nchan / avg;
 					}
-					ridx += nchan / avg;
+					else
+					{
+						/* a zoom band's autocorrelation points into the parent's
+						 * averaged one at choff / channelstoaverage and copies
+						 * the zoom frequency's output channels (mode.cpp:389-397,
+						 * core.cpp:1266-1290) */
+						int z = b - nb, par = j->zoom_parent[s][z];
+						int nout = j->freqs[fi].nchan / avg, first = j->zoom_choff[s][z] / savg, k;
+						double *ac = acc_ac[s] + ((size_t)par * 2 + pass) * nchan * 2;
+						for(k = 0; k < nout; k++)
+						{
+							int m = first + k;
+							for(c = m * savg; c < (m + 1) * savg && c < nchan; c++)
+							{
+								coreresult[2 * (ridx + k)] += ac[2 * c] / savg;
+								coreresult[2 * (ridx + k) + 1] += ac[2 * c + 1] / savg;
+							}
+						}
+						ridx += nout;
+					}
 				}
+			/* weights: a zoom band takes its parent band's (core.cpp:1311-1322) */
 			for(pass = 0; pass < (writecross ? 2 : 1); pass++)
-				for(b = 0; b < nb; b++)
+				for(b = 0; b < nb + j->nzoom[s]; b++)
 				{
-					int fi = j->band_freq[s][b];
+					int fi = total_band_freq(j, s, b);
 					if(!(j->freqused[fi] || j->equivused[fi])) continue;
-					coreresult[widx++] += acw[s][2 * b];
+					coreresult[widx++] += acw[s][2 * (b < nb ? b : j->zoom_parent[s][b - nb])];
 				}
 		}
 	}

@@ -253,6 +253,17 @@ void process_range(RefJob *j, int t, int startblock, int numblocks,
 					continue;
 				if(k < nrec)
 					fres[widx] += modes[d]->getWeight(false, k);
+				else
+				{
+					/* a zoom band takes the weight of its parent band
+					 * (core.cpp:1311-1322) */
+					int lf = config->getDLocalZoomFreqIndex(0, d, k - nrec);
+					int parent = config->getDZoomFreqParentFreqIndex(0, d, lf);
+					for(int l = 0; l < nrec; l++)
+						if(config->getDLocalRecordedFreqIndex(0, d, l) == parent &&
+						   config->getDZoomBandPol(0, d, k - nrec) == config->getDRecordedBandPol(0, d, l))
+							fres[widx] += modes[d]->getWeight(false, l);
+				}
 				widx++;
 			}
 	}

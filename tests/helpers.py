@@ -57,3 +57,39 @@ def compare_core(job, layout, corelen, got, ref, tol=FP32_TOL, weights_exact=Tru
                 m = float(np.max(np.abs(g - r)) / scale)
                 assert m <= 10 * tol, "%s max error %.3g" % (name, m)
     return out
+
+
+# zoom windows of the two 16 MHz subbands of small_job(nfreq=2):
+# (parent freq, offset MHz, width MHz)
+ZOOMS = [(0, 4.0, 4.0), (1, 0.0, 8.0), (1, 12.0, 4.0)]
+
+
+def zoom_job(keep_parents=True, nstation=3, avg=1, zooms=ZOOMS, **kw) -> Job:
+    """small_job with two 16 MHz subbands, dual polarisation with cross hands,
+    and zoom windows correlated on every baseline (optionally without the
+    parent subbands' own products)."""
+    from fxb200.job import add_zoom_bands
+    kw.setdefault("subint_ns", 2_048_000)
+    job = small_job(nstation=nstation, nchan=256, bw=16.0, nfreq=2, full_pol=True, avg=avg, **kw)
+    add_zoom_bands(job, zooms, keep_parents=keep_parents, chans_to_avg=avg)
+    job.validate()
+    return job
+
+
+def mixed_bw_zoom_job(seed=4) -> Job:
+    """Stations 0 and 1 record 16 MHz at 8400 MHz (256 channels), station 2
+    records 8 MHz at 8404 MHz (128 channels: the same channel width and FFT
+    duration).  Stations 0 and 1 zoom their band onto station 2's, so every
+    baseline correlates 8404-8412 MHz, and 0-1 also the full 16 MHz."""
+    from fxb200.job import Baseline, Station
+    freqs = [Freq(8400.0, 16.0, 256), Freq(8404.0, 8.0, 128)]
+    wide = lambda n: Station(n, [(0, "R"), (0, "L")], zoom_bands=[(1, "R"), (1, "L")])
+    st = [wide("A"), wide("B"), Station("C", [(1, "R"), (1, "L")])]
+    par = [(0, 0), (0, 1), (1, 0), (1, 1)]       # RR, RL, LR, LL
+    zz = [(2 + a, 2 + b) for a, b in par]
+    zr = [(2 + a, b) for a, b in par]
+    bls = [Baseline(0, 1, [(0, par), (1, zz)]), Baseline(0, 2, [(1, zr)]), Baseline(1, 2, [(1, zr)])]
+    job = Job(freqs, st, bls, subint_ns=2_048_000)
+    synth.make_delay_polys(job, seed=seed)
+    job.validate()
+    return job

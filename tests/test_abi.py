@@ -42,6 +42,40 @@ def test_layout_matches_oracle(kw):
     assert np.array_equal(lay, orc.layout())
 
 
+@pytest.mark.parametrize("name", ["zoom", "zoom_only", "zoom_avg4", "zoom_mixed_bw"])
+def test_zoom_layout_matches_oracle(name):
+    from helpers import mixed_bw_zoom_job, zoom_job
+    job = {"zoom": lambda: zoom_job(), "zoom_only": lambda: zoom_job(keep_parents=False),
+           "zoom_avg4": lambda: zoom_job(avg=4), "zoom_mixed_bw": mixed_bw_zoom_job}[name]()
+    lay, n = native.job_layout(job)
+    orc = fxoracle.OracleCorrelator(job)
+    assert n == orc.corelen
+    assert np.array_equal(lay, orc.layout())
+
+
+def test_zoom_rejections():
+    from fxb200.job import Freq
+    from helpers import zoom_job
+    # one polarisation of a dual-polarisation parent while cross-hand
+    # autocorrelations are written: the reference would output the parent's
+    # cross-hand spectrum for it, which a single zoom band cannot form
+    job = zoom_job(zooms=[(0, 4.0, 4.0)])
+    job.stations[0].zoom_bands = job.stations[0].zoom_bands[:1]
+    job.baselines = [b for b in job.baselines if b.ds1 != 0]
+    with pytest.raises(native.FxbError, match="UNSUPPORTED"):
+        native.job_layout(job)
+    # a zoom band outside every recorded band
+    job = zoom_job(zooms=[(0, 4.0, 4.0)])
+    job.freqs[-1] = Freq(9000.0, 4.0, 64)
+    with pytest.raises(Exception):
+        native.job_layout(job)
+    # zoom averaging that differs from the station's
+    job = zoom_job(zooms=[(0, 4.0, 4.0)])
+    job.freqs[-1].chans_to_avg = 2
+    with pytest.raises(native.FxbError, match="UNSUPPORTED"):
+        native.job_layout(job)
+
+
 def test_job_rejections():
     job = small_job()
     job.subint_ns = 4_000_100          # not a whole number of FFTs

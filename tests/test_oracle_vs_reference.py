@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from fxb200 import synth
-from helpers import compare_core, rel_err, small_job
+from helpers import compare_core, mixed_bw_zoom_job, rel_err, small_job, zoom_job
 
 import fxoracle
 import refcorr
@@ -41,6 +41,31 @@ def test_subint_matches_reference(name):
     o = orc.process_subint(inputs, sec, ns, validflags=vf)
     for s in range(len(job.stations)):
         assert np.array_equal(ref.interpolator(s, sec, ns), orc.interpolator(s, sec, ns))
+    compare_core(job, orc.layout(), orc.corelen, r.astype(np.float64), o, tol=2e-6)
+
+
+ZOOM_JOBS = {
+    "zoom": lambda: zoom_job(),
+    "zoom_only": lambda: zoom_job(keep_parents=False),
+    "zoom_avg4": lambda: zoom_job(avg=4),
+    "zoom_mixed_bw": lambda: mixed_bw_zoom_job(),
+}
+
+
+@pytest.mark.parametrize("name", sorted(ZOOM_JOBS))
+def test_zoom_subint_matches_reference(name):
+    # zoom bands: windows of recorded bands correlated as frequencies of their
+    # own, with or without their parents, averaged, and across stations that
+    # record different bandwidths (mode.cpp:169-208, core.cpp:1266-1363)
+    job = ZOOM_JOBS[name]()
+    ref = refcorr.RefCorrelator(job)
+    orc = fxoracle.OracleCorrelator(job)
+    assert np.array_equal(ref.layout(), orc.layout())
+    sec, ns = 0, 1_024_000
+    inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=7)
+    vf = [synth.valid_flags(job) for _ in job.stations]
+    r = ref.process_subint(inputs, vf, 0, sec, ns)
+    o = orc.process_subint(inputs, sec, ns, validflags=vf)
     compare_core(job, orc.layout(), orc.corelen, r.astype(np.float64), o, tol=2e-6)
 
 
