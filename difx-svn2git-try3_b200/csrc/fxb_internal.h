@@ -89,6 +89,8 @@ struct Job {
 		int nzoom() const { return (int)zoom_freq.size(); }
 		// frequency of band k: recorded bands, then zoom bands
 		int total_freq(int k) const { return k < nband ? band_freq[k] : zoom_freq[k - nband]; }
+		char total_pol(int k) const { return k < nband ? band_pol[k] : zoom_pol[k - nband]; }
+		int total_bands() const { return nband + nzoom(); }
 		int npoly = 0, order = 0, interval = 0;
 		double poly0 = 0.0;
 		std::vector<double> coeffs;

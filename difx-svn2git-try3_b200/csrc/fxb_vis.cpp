@@ -85,21 +85,37 @@ int matching_band(const Job &job, int s, int k)
 	return k;
 }
 
-// autocorrelation weights [station][j][band] (visibility.cpp:426-443)
+// autocorrelation weights [station][j][band] over the recorded and then the
+// zoom bands (visibility.cpp:415-432)
 std::vector<std::vector<std::vector<float>>> ac_weights(const Job &job, const Integration &in, const float *fr)
 {
 	const int S = (int)job.stations.size(), W = job.bandsperautocorr;
 	std::vector<std::vector<std::vector<float>>> w(S);
 	for(int i = 0; i < S; i++)
 	{
+		const Job::Station &st = job.stations[i];
 		int64_t ri = job.acwoff[i] * 2;
-		w[i].assign(W, std::vector<float>(job.stations[i].nband, 0.0f));
+		w[i].assign(W, std::vector<float>(st.total_bands(), 0.0f));
 		for(int j = 0; j < W; j++)
-			for(int k = 0; k < job.stations[i].nband; k++)
-				if(used(job, job.stations[i].band_freq[k]))
+			for(int k = 0; k < st.total_bands(); k++)
+				if(used(job, st.total_freq(k)))
 					w[i][j][k] = fr[ri++] / in.ffts;
 	}
 	return w;
+}
+
+// A zoom band carries a fraction of its parent's samples: the visibility
+// normalisation multiplies by zoom / parent bandwidth in float
+// (visibility.cpp:486-499, 560-566); 1 for a recorded band.
+float zoom_modifier(const Job &job, int s, int k)
+{
+	const Job::Station &st = job.stations[s];
+	if(k < st.nband)
+		return 1.0f;
+	float m = 1.0f;
+	m = (float)(m * job.freqs[st.total_freq(k)].bw_mhz);
+	m = (float)(m / job.freqs[st.band_freq[st.zoom_parent[k - st.nband]]].bw_mhz);
+	return m;
 }
 
 float baseline_weight(const Job &job, const Integration &in, const float *fr, int b, int f, int pp)
@@ -115,6 +131,16 @@ static fxb_status calibrate(const Job &job, const fxb_vis_params *p, float *fr)
 	const Integration in = integration(job, p);
 	const int S = (int)job.stations.size(), B = (int)job.baselines.size(), W = job.bandsperautocorr;
 	auto tsys = [&](int s) { return p->tsys ? p->tsys[s] : 0.0; };
+	// The reference looks up the opposite-hand band of a zoom band with the
+	// band's index into the zoom band tables (Configuration::getDMatchingBand,
+	// configuration.cpp:907-922), which reads past them: Tsys scaling of the
+	// cross-hand autocorrelations of zoom bands has no defined result there.
+	if(job.write_autocorrs && W == 2)
+		for(int i = 0; i < S; i++)
+			if(tsys(i) > 0.0)
+				for(int k = job.stations[i].nband; k < job.stations[i].total_bands(); k++)
+					if(used(job, job.stations[i].total_freq(k)))
+						return FXB_ERR_UNSUPPORTED;
 	const auto acw = ac_weights(job, in, fr);
 
 	// band averages of the (parallel-hand) autocorrelations, for Tsys scaling
@@ -122,13 +148,13 @@ static fxb_status calibrate(const Job &job, const fxb_vis_params *p, float *fr)
 	std::vector<std::vector<float>> accal(S);
 	for(int i = 0; i < S; i++)
 	{
-		accal[i].assign(job.stations[i].nband, 0.0f);
+		accal[i].assign(job.stations[i].total_bands(), 0.0f);
 		if(tsys(i) > 0.0)
 		{
 			int64_t ri = job.acoff[i];
-			for(int k = 0; k < job.stations[i].nband; k++)
+			for(int k = 0; k < job.stations[i].total_bands(); k++)
 			{
-				const int f = job.stations[i].band_freq[k];
+				const int f = job.stations[i].total_freq(k);
 				if(!used(job, f))
 					continue;
 				const int fc = job.freqs[f].nchan / job.freqs[f].chans_to_avg;
@@ -169,8 +195,14 @@ static fxb_status calibrate(const Job &job, const fxb_vis_params *p, float *fr)
 						scale = 0.0f;
 				}
 				else if(bw > 0.0f)
+				{
 					scale = (float)(1.0 / (bw * in.meansubints *
 					                       ((float)(job.blockspersend * 2 * fc * job.freqs[f].chans_to_avg))));
+					if(b1 >= job.stations[ds1].nband)
+						scale *= std::sqrt(zoom_modifier(job, ds1, b1));
+					if(b2 >= job.stations[ds2].nband)
+						scale *= std::sqrt(zoom_modifier(job, ds2, b2));
+				}
 				else
 					scale = 0.0f;
 				if(scale > 0.0f)
@@ -188,9 +220,9 @@ static fxb_status calibrate(const Job &job, const fxb_vis_params *p, float *fr)
 		{
 			int64_t ri = job.acoff[i] * 2;
 			for(int j = 0; j < W; j++)
-				for(int k = 0; k < job.stations[i].nband; k++)
+				for(int k = 0; k < job.stations[i].total_bands(); k++)
 				{
-					const int f = job.stations[i].band_freq[k];
+					const int f = job.stations[i].total_freq(k);
 					if(!used(job, f))
 						continue;
 					const int fc = job.freqs[f].nchan / job.freqs[f].chans_to_avg;
@@ -202,8 +234,12 @@ static fxb_status calibrate(const Job &job, const fxb_vis_params *p, float *fr)
 							scale = (float)(tsys(i) / divisor);
 					}
 					else if(acw[i][j][k] > 0.0f)
+					{
 						scale = (float)(1.0 / (acw[i][j][k] * in.meansubints *
 						                       ((float)(job.blockspersend * 2 * fc * job.freqs[f].chans_to_avg))));
+						if(k >= job.stations[i].nband)
+							scale *= zoom_modifier(job, i, k);
+					}
 					if(scale > 0.0f)
 						for(int c = 0; c < 2 * fc; c++)
 							fr[ri + c] *= scale;
@@ -275,8 +311,8 @@ static fxb_status swin_write(const Job &job, const fxb_vis_params *p, const floa
 				if(bw > 0.0f)
 				{
 					const int b1 = bl.prod_b1[bf.prods[k]], b2 = bl.prod_b2[bf.prods[k]];
-					header(o, bnum, mjd, sec, p->config_index, p->source_index, f, job.stations[bl.ds1].band_pol[b1],
-					       job.stations[bl.ds2].band_pol[b2], 0, bw, uvw);
+					header(o, bnum, mjd, sec, p->config_index, p->source_index, f, job.stations[bl.ds1].total_pol(b1),
+					       job.stations[bl.ds2].total_pol(b2), 0, bw, uvw);
 					put(o, fr + 2 * ri, sizeof(float) * 2 * fc);
 				}
 				ri += fc;
@@ -292,15 +328,15 @@ static fxb_status swin_write(const Job &job, const fxb_vis_params *p, const floa
 			const int bnum = 257 * (tel(i) + 1);
 			int64_t ri = job.acoff[i];
 			for(int j = 0; j < W; j++)
-				for(int k = 0; k < job.stations[i].nband; k++)
+				for(int k = 0; k < job.stations[i].total_bands(); k++)
 				{
-					const int f = job.stations[i].band_freq[k];
+					const int f = job.stations[i].total_freq(k);
 					if(!used(job, f))
 						continue;
 					const int fc = job.freqs[f].nchan / job.freqs[f].chans_to_avg;
 					if(acw[i][j][k] > 0.0f)
 					{
-						const char p0 = job.stations[i].band_pol[k];
+						const char p0 = job.stations[i].total_pol(k);
 						header(o, bnum, mjd, sec, p->config_index, p->source_index, f, p0, j == 0 ? p0 : opposite_pol(p0),
 						       0, acw[i][j][k], zero);
 						put(o, fr + 2 * ri, sizeof(float) * 2 * fc);

@@ -64,13 +64,13 @@ def compare_core(job, layout, corelen, got, ref, tol=FP32_TOL, weights_exact=Tru
 ZOOMS = [(0, 4.0, 4.0), (1, 0.0, 8.0), (1, 12.0, 4.0)]
 
 
-def zoom_job(keep_parents=True, nstation=3, avg=1, zooms=ZOOMS, **kw) -> Job:
+def zoom_job(keep_parents=True, nstation=3, avg=1, zooms=ZOOMS, full_pol=True, **kw) -> Job:
     """small_job with two 16 MHz subbands, dual polarisation with cross hands,
     and zoom windows correlated on every baseline (optionally without the
     parent subbands' own products)."""
     from fxb200.job import add_zoom_bands
     kw.setdefault("subint_ns", 2_048_000)
-    job = small_job(nstation=nstation, nchan=256, bw=16.0, nfreq=2, full_pol=True, avg=avg, **kw)
+    job = small_job(nstation=nstation, nchan=256, bw=16.0, nfreq=2, full_pol=full_pol, avg=avg, **kw)
     add_zoom_bands(job, zooms, keep_parents=keep_parents, chans_to_avg=avg)
     job.validate()
     return job

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from fxb200 import synth, visibility
-from helpers import small_job
+from helpers import mixed_bw_zoom_job, small_job, zoom_job
 
 import refcorr
 
@@ -35,10 +35,25 @@ def _subints(job, ref, n=2):
     return out
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+ZOOM_CASES = {
+    "zoom": (lambda: zoom_job(), None),
+    "zoom_only": (lambda: zoom_job(keep_parents=False), None),
+    "zoom_mixed_bw": (lambda: mixed_bw_zoom_job(), None),
+    "zoom_parallel_tsys": (lambda: zoom_job(full_pol=False), [40.0, 55.0, 70.0]),
+}
+
+
+def _job(name):
+    if name in CASES:
+        kw, tsys = CASES[name]
+        return small_job(**kw), tsys
+    build, tsys = ZOOM_CASES[name]
+    return build(), tsys
+
+
+@pytest.mark.parametrize("name", sorted(CASES) + sorted(ZOOM_CASES))
 def test_swin_records_match_reference_visibility(name, tmp_path):
-    kw, tsys = CASES[name]
-    job = small_job(**kw)
+    job, tsys = _job(name)
     ref = refcorr.RefCorrelator(job, tsys=tsys)
     subs = _subints(job, ref)
     expect = ref.visibility_write(subs)
@@ -55,7 +70,7 @@ def test_swin_records_match_reference_visibility(name, tmp_path):
     assert got == expect
     nch = {f: fr.nchan // fr.chans_to_avg for f, fr in enumerate(job.freqs)}
     recs = visibility.read_swin(got, nch.__getitem__)
-    nprod = sum(len(b.products[0][1]) * len(b.products) for b in job.baselines)
+    nprod = sum(len(pp) for b in job.baselines for _, pp in b.products)
     assert sum(1 for r in recs if r.baseline % 257) == nprod
     assert all(r.weight > 0 for r in recs)
 
@@ -78,3 +93,18 @@ def test_records_append_per_integration(tmp_path):
     assert half > 0 and len(recs) == 2 * half
     assert all(abs(r.seconds - (job.duration_s / 2)) < 1e-9 for r in recs[:half])
     assert all(abs(r.seconds - (1 + job.duration_s / 2)) < 1e-9 for r in recs[half:])
+
+
+def test_tsys_with_zoom_cross_hand_autos_is_refused():
+    # the reference's opposite-hand lookup for a zoom band reads past its
+    # zoom band tables (configuration.cpp:907-922): no defined result
+    job = zoom_job()
+    params = visibility.VisParams.for_job(job, tsys=[40.0, 55.0, 70.0])
+    from fxb200.native import FxbError
+    with pytest.raises(FxbError, match="UNSUPPORTED"):
+        visibility.calibrate(job, params, np.zeros(2 * _corelen(job), dtype=np.float32))
+
+
+def _corelen(job):
+    from fxb200.native import job_layout
+    return job_layout(job)[1]
