@@ -91,6 +91,14 @@ struct fxb_ctx {
 	int nbw = 0, nacw = 0, nom = 0;
 	DevZoomCopy *d_zoom = nullptr;       // zoom-band rows gathered after the F stage
 	int nzoom = 0;
+	// phase cal: binning groups, bands, and the FP64 bins of the integration
+	std::vector<DevPcalGroup> h_pgroups;
+	DevPcalGroup *d_pgroups = nullptr;
+	DevPcalBand *d_pbands = nullptr;
+	int npbands = 0;
+	int pchunks = 1;                     // chunks of FFTs, each with its own slice of the bins
+	size_t psmem = 0;
+	double *d_pbins = nullptr;           // [pchunks][job.pcal_bins]
 	float2 *d_core = nullptr;
 	uint8_t *d_valid = nullptr;
 	int64_t valid_stride = 0;
@@ -215,6 +223,52 @@ static void free_ctx(fxb_ctx *ctx)
 	if(ctx->stream) cudaStreamDestroy(ctx->stream);
 	if(ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
 	delete ctx;
+}
+
+// Phase-cal binning groups: a station's bands with tones and equal bin
+// counts, as many as fit one CTA's shared memory and kPcalGroupBands.
+static std::vector<DevPcalGroup> pcal_groups(const Job &job)
+{
+	std::vector<DevPcalGroup> out;
+	for(const Job::PcalBand &p : job.pcal)
+	{
+		if(p.nbins <= 0)
+			continue;
+		DevPcalGroup *g = nullptr;
+		for(DevPcalGroup &c : out)
+			if(c.station == p.station && c.nbins == p.nbins && c.nb < kPcalGroupBands)
+			{
+				DevPcalGroup t = c;
+				t.nb++;
+				if(pcal_group_smem(t) <= kPcalSmemMax)
+					g = &c;
+			}
+		if(!g)
+		{
+			out.push_back(DevPcalGroup{});
+			g = &out.back();
+			memset(g, 0, sizeof(*g));
+			g->station = p.station;
+			g->nbins = p.nbins;
+		}
+		g->band[g->nb] = p.band;
+		g->bin_off[g->nb] = p.bin_off;
+		g->nb++;
+	}
+	return out;
+}
+
+// Chunks of FFTs per subint for the phase-cal binning: about four CTAs per SM
+// over all groups, at most one FFT per chunk, and at most 64 MB of bins.
+static int pcal_chunks(const Job &job, size_t ngroups)
+{
+	if(ngroups == 0 || job.pcal_bins <= 0)
+		return 1;
+	int n = (int)((600 + ngroups - 1) / ngroups);
+	n = std::min(n, std::max(job.blockspersend, 1));
+	const int64_t cap = (int64_t)(64 << 20) / (8 * job.pcal_bins);
+	n = (int)std::min<int64_t>(n, std::max<int64_t>(cap, 1));
+	return std::max(n, 1);
 }
 
 static fxb_status setup_device(fxb_ctx *ctx)
@@ -608,6 +662,32 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		if(ctx->nbw) CK(ctx, cudaMemcpyAsync(ctx->d_bw, hbw.data(), sizeof(DevBWeight) * ctx->nbw, cudaMemcpyHostToDevice, ctx->stream));
 		if(ctx->nacw) CK(ctx, cudaMemcpyAsync(ctx->d_acw, hacw.data(), sizeof(DevACWeight) * ctx->nacw, cudaMemcpyHostToDevice, ctx->stream));
 		if(ctx->nom) CK(ctx, cudaMemcpyAsync(ctx->d_om, hom.data(), sizeof(DevOutMap) * ctx->nom, cudaMemcpyHostToDevice, ctx->stream));
+		// phase cal: binning groups, every band's tones for the DFT, and one
+		// slice of FP64 bins per chunk of FFTs
+		{
+			std::vector<DevPcalBand> hb;
+			for(const Job::PcalBand &p : job.pcal)
+				hb.push_back(DevPcalBand{p.ntones, p.nbins, p.first, p.step, p.bin_off, p.core});
+			ctx->h_pgroups = pcal_groups(job);
+			ctx->pchunks = pcal_chunks(job, ctx->h_pgroups.size());
+			ctx->npbands = (int)hb.size();
+			if(ctx->npbands)
+			{
+				for(const DevPcalGroup &g : ctx->h_pgroups)
+					ctx->psmem = std::max(ctx->psmem, pcal_group_smem(g));
+				if(ctx->psmem)
+					CK(ctx, pcal_init(ctx->psmem));
+				CK(ctx, dalloc(ctx, &ctx->d_pbands, hb.size()));
+				CK(ctx, cudaMemcpyAsync(ctx->d_pbands, hb.data(), sizeof(DevPcalBand) * hb.size(), cudaMemcpyHostToDevice, ctx->stream));
+				CK(ctx, dalloc(ctx, &ctx->d_pgroups, std::max<size_t>(ctx->h_pgroups.size(), 1)));
+				if(!ctx->h_pgroups.empty())
+					CK(ctx, cudaMemcpyAsync(ctx->d_pgroups, ctx->h_pgroups.data(), sizeof(DevPcalGroup) * ctx->h_pgroups.size(),
+					                        cudaMemcpyHostToDevice, ctx->stream));
+				const size_t nbins = (size_t)ctx->pchunks * (size_t)std::max<int64_t>(job.pcal_bins, 1);
+				CK(ctx, dalloc(ctx, &ctx->d_pbins, nbins));
+				CK(ctx, cudaMemsetAsync(ctx->d_pbins, 0, sizeof(double) * nbins, ctx->stream));
+			}
+		}
 		ctx->nzoom = (int)job.zooms.size();
 		if(ctx->nzoom)
 		{
@@ -919,6 +999,8 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 		if(tuning)
 			cudaEventRecord(tn.ev[nk], st);
 	}
+	launch_pcal_bin(ctx->d_pgroups, (int)ctx->h_pgroups.size(), ctx->psmem, ctx->pchunks, ctx->d_st, sl.d_sub,
+	                ctx->d_params, ctx->d_valid, ctx->valid_stride, ctx->T, job.pcal_bins, ctx->d_pbins, st);
 	launch_zoom_gather(ctx->d_zoom, ctx->nzoom, ctx->d_plans, ctx->T, ctx->tc,
 	                   ctx->tc ? ctx->d_specn : (void *)ctx->d_spec, st);
 	cudaEventRecordWithFlags(sl.tev[2], st, evf);
@@ -1216,18 +1298,25 @@ fxb_status fxb_core_result_length(const fxb_ctx *ctx, int64_t *ncomplex)
 	return FXB_OK;
 }
 
-fxb_status fxb_layout(const fxb_ctx *ctx, int32_t *out, size_t nint)
+// The layout offsets; the phase-cal offsets too when out has room for them.
+static fxb_status write_layout(const Job &j, int32_t *out, size_t nint)
 {
-	if(!ctx || !out) return FXB_ERR_ARG;
-	const Job &j = ctx->job;
-	size_t need = 2 * j.bloff.size() + 2 * j.acoff.size();
+	const size_t need = 2 * j.bloff.size() + 2 * j.acoff.size();
 	if(nint < need) return FXB_ERR_ARG;
 	size_t k = 0;
 	for(auto v : j.bloff) out[k++] = (int32_t)v;
 	for(auto v : j.bwoff) out[k++] = (int32_t)v;
 	for(auto v : j.acoff) out[k++] = (int32_t)v;
 	for(auto v : j.acwoff) out[k++] = (int32_t)v;
+	if(nint >= need + j.pcoff.size())
+		for(auto v : j.pcoff) out[k++] = (int32_t)v;
 	return FXB_OK;
+}
+
+fxb_status fxb_layout(const fxb_ctx *ctx, int32_t *out, size_t nint)
+{
+	if(!ctx || !out) return FXB_ERR_ARG;
+	return write_layout(ctx->job, out, nint);
 }
 
 fxb_status fxb_job_layout(const fxb_job_desc *desc, int32_t *out, size_t nint, int64_t *ncomplex)
@@ -1241,15 +1330,10 @@ fxb_status fxb_job_layout(const fxb_job_desc *desc, int32_t *out, size_t nint, i
 		g_create_err = err;
 		return st;
 	}
-	size_t need = 2 * job.bloff.size() + 2 * job.acoff.size();
 	if(out)
 	{
-		if(nint < need) return FXB_ERR_ARG;
-		size_t k = 0;
-		for(auto v : job.bloff) out[k++] = (int32_t)v;
-		for(auto v : job.bwoff) out[k++] = (int32_t)v;
-		for(auto v : job.acoff) out[k++] = (int32_t)v;
-		for(auto v : job.acwoff) out[k++] = (int32_t)v;
+		const fxb_status ls = write_layout(job, out, nint);
+		if(ls != FXB_OK) return ls;
 	}
 	if(ncomplex) *ncomplex = job.corelen;
 	return FXB_OK;
@@ -1278,7 +1362,8 @@ fxb_status fxb_job_footprint(const fxb_job_desc *desc, size_t *bytes)
 	double b = (double)job.spec_total * (job.xmac_kind == FXB_XMAC_FP32 ? 8.0
 	                                     : job.xmac_kind == FXB_XMAC_BF16 ? 4.0 * 1.25 * pad32
 	                                                                      : (4.0 * pad64 + 2.0 * pad64 + 0.5) * 1.25);
-	b += (double)job.acc_total * 8.0 + (double)job.corelen * 16.0 + (double)S * T * 64.0;
+	b += (double)job.acc_total * 8.0 + (double)job.corelen * 16.0 + (double)S * T * 64.0 +
+	     (double)job.pcal_bins * 8.0 * pcal_chunks(job, pcal_groups(job).size());
 	// raw VDIF staging of the in-flight subints (payload plus headers, 1/8 slack)
 	for(int s = 0; s < S; s++)
 	{
@@ -1304,6 +1389,7 @@ fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats)
 	}
 	launch_finalise(ctx->d_om, ctx->nom, 0, ctx->d_acc, ctx->d_bw, ctx->nbw, ctx->d_bwacc, ctx->d_acw, ctx->nacw,
 	                ctx->d_acwacc, ctx->d_core, ctx->job.corelen, ctx->stream);
+	launch_pcal_final(ctx->d_pbands, ctx->npbands, ctx->pchunks, ctx->job.pcal_bins, ctx->d_pbins, ctx->d_core, ctx->stream);
 	CK(ctx, cudaGetLastError());
 	CK(ctx, cudaMemcpyAsync(coreresult, ctx->d_core, sizeof(float2) * ctx->job.corelen, cudaMemcpyDeviceToHost, ctx->stream));
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1316,6 +1402,10 @@ fxb_status fxb_reset(fxb_ctx *ctx)
 	CK(ctx, cudaMemsetAsync(ctx->d_acc, 0, sizeof(float2) * std::max<int64_t>(ctx->job.acc_total, 1), ctx->stream));
 	CK(ctx, cudaMemsetAsync(ctx->d_bwacc, 0, sizeof(float) * std::max(ctx->nbw, 1), ctx->stream));
 	CK(ctx, cudaMemsetAsync(ctx->d_acwacc, 0, sizeof(float) * std::max(ctx->nacw, 1), ctx->stream));
+	if(ctx->d_pbins)
+		CK(ctx, cudaMemsetAsync(ctx->d_pbins, 0,
+		                        sizeof(double) * (size_t)ctx->pchunks * (size_t)std::max<int64_t>(ctx->job.pcal_bins, 1),
+		                        ctx->stream));
 	return FXB_OK;
 }
 
@@ -1446,6 +1536,8 @@ fxb_status fxb_read_results_device(fxb_ctx *ctx, float *dev_out, size_t nfloats)
 	}
 	launch_finalise(ctx->d_om, ctx->nom, 0, ctx->d_acc, ctx->d_bw, ctx->nbw, ctx->d_bwacc, ctx->d_acw, ctx->nacw,
 	                ctx->d_acwacc, (float2 *)dev_out, ctx->job.corelen, ctx->stream);
+	launch_pcal_final(ctx->d_pbands, ctx->npbands, ctx->pchunks, ctx->job.pcal_bins, ctx->d_pbins, (float2 *)dev_out,
+	                  ctx->stream);
 	CK(ctx, cudaGetLastError());
 	return FXB_OK;
 }

@@ -87,6 +87,7 @@ struct Job {
 		std::vector<int> zoom_freq, zoom_parent, zoom_choff;
 		std::vector<char> zoom_pol;
 		int nzoom() const { return (int)zoom_freq.size(); }
+		float pcal_interval = 0.0f, pcal_base = 0.0f;   // phase-cal comb (MHz), float as the reference
 		// frequency of band k: recorded bands, then zoom bands
 		int total_freq(int k) const { return k < nband ? band_freq[k] : zoom_freq[k - nband]; }
 		char total_pol(int k) const { return k < nband ? band_pol[k] : zoom_pol[k - nband]; }
@@ -145,6 +146,17 @@ struct Job {
 	// zoom bands: spectra rows gathered from the parent band's spectra
 	struct ZoomCopy { int src_freq, src_row, dst_freq, dst_row, choff, nchan; };
 	std::vector<ZoomCopy> zooms;
+	// phase cal: per recorded band of a station with extraction, the tones,
+	// the bins the samples are folded into (0: no tone in the band, one zero
+	// tone), the DFT bin of the first tone and the bin step between tones
+	struct PcalBand {
+		int station, band, ntones, nbins, first, step;
+		int64_t core;       // core-result offset (complex) of the band's first tone
+		int64_t bin_off;    // offset of the band's bins in the bin accumulator
+	};
+	std::vector<PcalBand> pcal;
+	int64_t pcal_bins = 0;
+	std::vector<int64_t> pcoff;   // core-result offset of each station's tones, -1 without phase cal
 	// weight plans
 	struct BWeight { int s1, s2; int64_t dst_float; };
 	std::vector<BWeight> bweights;

@@ -42,6 +42,90 @@ static bool fail(std::string &err, fxb_status &st, fxb_status code, const std::s
 
 static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
+// ------------------------------------------------------------------ phase cal
+// Greatest common divisor of doubles rounded to integers (mathutil.cpp:8-30).
+static long long gcd_rounded(double a, double b)
+{
+	long x = (long)std::floor(a + 0.5), y = (long)std::floor(b + 0.5);
+	if(x == 0 || y == 0)
+		return std::max(x, y);
+	while(y != 0)
+	{
+		const long r = x % y;
+		x = y;
+		y = r;
+	}
+	return x;
+}
+
+// Comb tones from offset up to the band edge, a tone on both edges counted
+// once (PCal::calcNumTones, pcal.cpp:205-222).
+static int comb_tones(double bw, double offset, double step)
+{
+	if(bw <= 0.0 || step <= 0.0)
+		return 0;
+	int n = 0;
+	double f = offset;
+	while(f <= bw)
+	{
+		n++;
+		f += step;
+	}
+	if(offset == 0.0 && f - step == bw)
+		n--;
+	return n;
+}
+
+constexpr int kMaxPcalBins = 32768;
+
+// One recorded band's tones and extractor: the comb tones of the band
+// (configuration.cpp:1813-1846) and, for the extractor PCal::getNew picks
+// (pcal.cpp:139-191, with Mode's 1 MHz minimum frequency resolution), the
+// bin count and tone bins of the implicit-shift extractor
+// (pcal.cpp:927-958, 1073-1086).  A band without a tone reads as one zero
+// tone (the dummy extractor).
+static bool pcal_band(const fxb_freq &f, float interval, float base, Job::PcalBand &pb, std::string &err,
+                      fxb_status &st)
+{
+	pb.nbins = pb.first = pb.step = 0;
+	if(f.lower_sideband)
+		return fail(err, st, FXB_ERR_UNSUPPORTED, "phase cal of lower-sideband bands");
+	const double lo = f.freq_mhz, bw = f.bw_mhz;
+	double tonefreq = (double)((int)(lo / interval)) * interval;
+	if(tonefreq <= lo)
+		tonefreq += interval;
+	int n = 0;
+	if(tonefreq <= lo + bw)
+		while(tonefreq + (float)(n * interval) <= lo + bw)
+			n++;
+	if(n == 0)
+	{
+		pb.ntones = 1;
+		return true;
+	}
+	pb.ntones = n;
+	const double tone0 = 1e6 * tonefreq + 0 * 1e6 * interval + 1e6 * base;
+	const int off = (int)(long)(tone0 - 1e6 * lo + 0.5);
+	const double fs = 2.0 * 1e6 * bw, sp = 1e6 * interval;
+	int nbins = (int)(fs / gcd_rounded(fs, (double)off));
+	const int nspacing = (int)(fs / gcd_rounded(fs, sp));
+	const int nt = comb_tones(1e6 * bw, (double)off, sp);
+	while(fs / (2 * nbins) > 1e6)
+		nbins *= 2;
+	if(nt == 0)
+		return true;
+	if(off == 0 || nbins % nspacing != 0)
+		return fail(err, st, FXB_ERR_UNSUPPORTED, "phase-cal comb needs the trivial or the shifting extractor");
+	if(nt != n)
+		return fail(err, st, FXB_ERR_UNSUPPORTED, "phase-cal tone count differs between extractor and configuration");
+	if(nbins > kMaxPcalBins)
+		return fail(err, st, FXB_ERR_UNSUPPORTED, "phase-cal offset repeats after too many samples");
+	pb.nbins = nbins;
+	pb.step = (int)std::floor((double)nbins * (sp / fs));
+	pb.first = (int)std::floor((double)nbins * ((double)off / fs));
+	return true;
+}
+
 bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st)
 {
 	st = FXB_OK;
@@ -158,6 +242,10 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 			o.zoom_parent.push_back(pb);
 			o.zoom_choff.push_back(off);
 		}
+		if(!(in.pcal_interval_mhz >= 0.0) || !(in.pcal_base_mhz == in.pcal_base_mhz))
+			return fail(err, st, FXB_ERR_ARG, "bad phase-cal interval");
+		o.pcal_interval = (float)in.pcal_interval_mhz;
+		o.pcal_base = (float)in.pcal_base_mhz;
 		job.stations.push_back(o);
 	}
 	for(int b = 0; b < d->nbaseline; b++)
@@ -307,6 +395,28 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 		toadd = (toadd + 1) / 2;
 		if(toadd == 0) toadd = 1;
 		idx += toadd;
+	}
+	// then each station's phase-cal tones, band by band (configuration.cpp:2423-2431)
+	job.pcoff.assign(S, -1);
+	for(int s = 0; s < S; s++)
+	{
+		const Job::Station &js = job.stations[s];
+		if(!(js.pcal_interval > 0.0f))
+			continue;
+		job.pcoff[s] = idx;
+		for(int bnd = 0; bnd < js.nband; bnd++)
+		{
+			Job::PcalBand pb;
+			pb.station = s;
+			pb.band = bnd;
+			if(!pcal_band(job.freqs[js.band_freq[bnd]], js.pcal_interval, js.pcal_base, pb, err, st))
+				return false;
+			pb.core = idx;
+			pb.bin_off = job.pcal_bins;
+			job.pcal_bins += pb.nbins;
+			idx += pb.ntones;
+			job.pcal.push_back(pb);
+		}
 	}
 	job.corelen = idx;
 

@@ -152,6 +152,31 @@ void launch_quant_fp8(const TcShape &s, const DevFreqPlan *dplans, const int32_t
 void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, const float2 *spec, float2 *acc,
                       cudaStream_t stream);
 
+// Phase cal (csrc/fxb_pcal.cu).  A group is up to kPcalGroupBands recorded
+// bands of one station with the same bin count; a band is one band's tones.
+constexpr int kPcalGroupBands = 16;
+struct DevPcalGroup {
+	int32_t station, nb, nbins, pad;
+	int32_t band[kPcalGroupBands];
+	int64_t bin_off[kPcalGroupBands];   // first bin of each band in the bin accumulator
+};
+struct DevPcalBand {
+	int32_t ntones, nbins, first, step;
+	int64_t bin_off, core;
+};
+size_t pcal_group_smem(const DevPcalGroup &g);
+constexpr size_t kPcalSmemMax = 192 * 1024;   // shared memory of one group at most
+// allows the binning kernel smem bytes of dynamic shared memory (once per context)
+cudaError_t pcal_init(size_t smem);
+// folds the subint's samples into the FP64 bins: the FFTs are split into
+// nchunk chunks, chunk c adds to bins + c * chunk_stride
+void launch_pcal_bin(const DevPcalGroup *groups, int ngroups, size_t smem, int nchunk, const DevStation *st,
+                     const DevSubintStation *sub, const FftParam *params, const uint8_t *valid, int64_t valid_stride,
+                     int T, int64_t chunk_stride, double *bins, cudaStream_t stream);
+// writes the tones of every band into the core result
+void launch_pcal_final(const DevPcalBand *bands, int nbands, int nchunk, int64_t chunk_stride, const double *bins,
+                       float2 *core, cudaStream_t stream);
+
 // Zoom-band spectra from their parents' (after the F stage, before the
 // XMAC): tc selects the tensor-core form's bf16x2 spectra.
 void launch_zoom_gather(const DevZoomCopy *zc, int nzc, const DevFreqPlan *plans, int T, bool tc, void *spec,

@@ -55,6 +55,10 @@ class Station:
     # zoom bands (freq index, pol): channel windows of a recorded band of the
     # same polarisation; a baseline names zoom band z as band nband + z
     zoom_bands: List[Tuple[int, str]] = dataclasses.field(default_factory=list)
+    # phase-cal comb: tones every pcal_interval_mhz (0: no extraction),
+    # shifted by pcal_base_mhz
+    pcal_interval_mhz: float = 0.0
+    pcal_base_mhz: float = 0.0
 
     def recorded_freqs(self) -> List[int]:
         seen: List[int] = []

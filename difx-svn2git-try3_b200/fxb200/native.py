@@ -33,7 +33,8 @@ class FxbStation(ctypes.Structure):
     _fields_ = [("nbits", ctypes.c_int32), ("payload_bytes", ctypes.c_int32), ("header_bytes", ctypes.c_int32),
                 ("nband", ctypes.c_int32), ("band_freq", ctypes.POINTER(ctypes.c_int32)),
                 ("band_pol", ctypes.c_char_p), ("nzoom", ctypes.c_int32), ("reserved", ctypes.c_int32),
-                ("zoom_freq", ctypes.POINTER(ctypes.c_int32)), ("zoom_pol", ctypes.c_char_p)]
+                ("zoom_freq", ctypes.POINTER(ctypes.c_int32)), ("zoom_pol", ctypes.c_char_p),
+                ("pcal_interval_mhz", ctypes.c_double), ("pcal_base_mhz", ctypes.c_double)]
 
 
 class FxbBaseline(ctypes.Structure):
@@ -71,7 +72,7 @@ class DescHolder:
             st[i] = FxbStation(s.nbits, s.payload_bytes, s.header_bytes, s.nband,
                                ctypes.cast(bf, ctypes.POINTER(ctypes.c_int32)), ctypes.cast(bp, ctypes.c_char_p),
                                nz, 0, ctypes.cast(zf, ctypes.POINTER(ctypes.c_int32)),
-                               ctypes.cast(zp, ctypes.c_char_p))
+                               ctypes.cast(zp, ctypes.c_char_p), s.pcal_interval_mhz, s.pcal_base_mhz)
         bl = (FxbBaseline * len(job.baselines))()
         for i, b in enumerate(job.baselines):
             pf, p1, p2 = [], [], []
@@ -271,7 +272,7 @@ class Correlator:
 
     def layout(self) -> np.ndarray:
         nf, nb, ns = len(self.job.freqs), len(self.job.baselines), len(self.job.stations)
-        out = np.zeros(2 * nf * nb + 2 * ns, dtype=np.int32)
+        out = np.zeros(2 * nf * nb + 3 * ns, dtype=np.int32)
         check(lib().fxb_layout(self.ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), out.size),
               self.ctx, "layout")
         return out
@@ -388,7 +389,7 @@ def job_layout(job: Job) -> Tuple[np.ndarray, int]:
     """Core-result offsets and length from the job alone (no GPU needed)."""
     holder = DescHolder(job)
     nf, nb, ns = len(job.freqs), len(job.baselines), len(job.stations)
-    out = np.zeros(2 * nf * nb + 2 * ns, dtype=np.int32)
+    out = np.zeros(2 * nf * nb + 3 * ns, dtype=np.int32)
     n = ctypes.c_int64(0)
     check(lib().fxb_job_layout(holder.ptr(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), out.size,
                                ctypes.byref(n)), None, "job_layout")

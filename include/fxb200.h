@@ -83,6 +83,15 @@ typedef struct {
 	int32_t reserved;
 	const int32_t *zoom_freq; /* [nzoom] frequency-table index of each zoom band */
 	const char *zoom_pol;     /* [nzoom] polarisation of each zoom band */
+	/* Phase-cal extraction (PHASE CAL INT (MHZ), PHASE CAL BASE(MHZ);
+	 * configuration.cpp:1600-1625, 1771-1846): comb tones every
+	 * pcal_interval_mhz, shifted by pcal_base_mhz; 0 = off.  The tones of
+	 * each recorded band, from its lowest in-band comb tone upwards, are
+	 * extracted from the unpacked samples of every valid FFT (mode.cpp:773-787,
+	 * pcal.cpp) and appended to the core result after the autocorrelation
+	 * weights, band by band (core.cpp:1124-1150). */
+	double pcal_interval_mhz;
+	double pcal_base_mhz;
 } fxb_station;
 
 /* One baseline (BASELINE TABLE, configuration.cpp:1059-1120): products are
@@ -211,7 +220,8 @@ FXB_API fxb_status fxb_core_result_length(const fxb_ctx *ctx, int64_t *ncomplex)
  * offset (or -1), then the same for the baseline-weight offsets, then the
  * autocorrelation offset and the autocorrelation-weight offset of every
  * datastream (Configuration::getCoreResult*Offset).  out holds
- * 2*nfreq*nbaseline + 2*nstation ints. */
+ * 2*nfreq*nbaseline + 2*nstation ints; when it holds nstation more, the
+ * phase-cal offset of every datastream (-1 without phase cal) follows. */
 FXB_API fxb_status fxb_layout(const fxb_ctx *ctx, int32_t *out, size_t nint);
 
 /* The same layout computed from a job description alone, without a GPU or a
@@ -222,7 +232,7 @@ FXB_API fxb_status fxb_job_layout(const fxb_job_desc *desc, int32_t *out, size_t
 
 /* Copy the accumulated core result (2*ncomplex floats) to host memory, in
  * the reference layout: cross-correlations, baseline weights,
- * autocorrelations, autocorrelation weights.  Synchronises. */
+ * autocorrelations, autocorrelation weights, phase-cal tones.  Synchronises. */
 FXB_API fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats);
 
 /* Zero the accumulators (Core::execute after each send, core.cpp:318-322). */

@@ -97,7 +97,9 @@ def write_job_files(job: Job, outdir: str, name: str = "job",
         s.append(_kv("DATA SAMPLING", "REAL"))
         s.append(_kv("DATA SOURCE", "FILE"))
         s.append(_kv("FILTERBANK USED", "FALSE"))
-        s.append(_kv("PHASE CAL INT (MHZ)", 0))
+        s.append(_kv("PHASE CAL INT (MHZ)", ("%.6f" % st.pcal_interval_mhz) if st.pcal_interval_mhz else 0))
+        if st.pcal_base_mhz:
+            s.append(_kv("PHASE CAL BASE(MHZ)", "%.6f" % st.pcal_base_mhz))
         rf = st.recorded_freqs()
         s.append(_kv("NUM RECORDED FREQS", len(rf)))
         for j, f in enumerate(rf):

@@ -7,7 +7,7 @@
  *
  * It restates, for the job subset described by include/fxb200.h (single
  * configuration, VDIF single-thread datastreams, real sampling, no pulsar
- * binning, one phase centre, no phase cal), the algorithm of:
+ * binning, one phase centre), the algorithm of:
  *   - the core-result layout   Configuration::populateResultLengths
  *                              (mpifxcorr/src/configuration.cpp:2212-2440)
  *   - the delay interpolator   Model::calculateDelayInterpolator
@@ -24,6 +24,12 @@
  *   - the XMAC and weights     Core::processdata (core.cpp:877-972, 998-1045)
  *                              and the result merges (core.cpp:1774-1787,
  *                              1068-1086, 1266-1363)
+ *   - phase cal                tones per recorded band (configuration.cpp:
+ *                              1771-1846), the extractor choice (pcal.cpp:
+ *                              139-191) and the implicit-shift extractor
+ *                              (pcal.cpp:927-1105), fed from Mode::process
+ *                              (mode.cpp:773-787), copied band by band
+ *                              (core.cpp:1124-1150)
  *   - zoom bands               parent and channel offset
  *                              (configuration.cpp:1734-1754), spectra and
  *                              autocorrelations as views into the parent band
@@ -69,6 +75,11 @@ typedef struct fxo_job {
 	char **band_pol;
 	int *nzoom;
 	int **zoom_freq, **zoom_parent, **zoom_choff;   /* parent: recorded band index */
+	/* phase cal per station and recorded band: tones, bins (0: the dummy
+	 * extractor's zeros), first tone bin and bin step */
+	double *pcal_interval, *pcal_base;
+	int **pc_ntones, **pc_nbins, **pc_first, **pc_step;
+	int64_t *pcoff;       /* core-result offset of each station's tones, or -1 */
 	oracle_poly *poly;
 	/* baselines: products grouped per freq in given order */
 	int *ds1, *ds2, *nprod;
@@ -126,6 +137,89 @@ static int total_band_freq(const fxo_job *j, int s, int k)
 	return k < j->nband[s] ? j->band_freq[s][k] : j->zoom_freq[s][k - j->nband[s]];
 }
 static double station_bw(const fxo_job *j, int s) { return j->freqs[j->band_freq[s][0]].bw_mhz; }
+
+/* ------------------------------------------------------------ phase cal */
+
+/* gcd of integers, and of doubles rounded to integers (mathutil.cpp:8-30) */
+static long long lgcd(long a, long b)
+{
+	if(a == 0 || b == 0) return a > b ? a : b;
+	for(;;)
+	{
+		a = a % b;
+		if(a == 0) return b;
+		b = b % a;
+		if(b == 0) return a;
+	}
+}
+static long long dgcd(double a, double b) { return lgcd((long)floor(a + 0.5), (long)floor(b + 0.5)); }
+
+/* PCal::calcNumTones (pcal.cpp:205-222) */
+static int calc_num_tones(double bw, double offset, double step)
+{
+	int n = 0;
+	double ftone = offset;
+	if(bw <= 0.0f || step <= 0.0f) return 0;
+	while(ftone <= bw)
+	{
+		n++;
+		ftone += step;
+	}
+	if(offset == 0.0 && ftone - step == bw)
+		n--;
+	return n;
+}
+
+/* Tones of one recorded band and its extractor (configuration.cpp:1813-1846
+ * for the upper sideband, PCal::getNew pcal.cpp:139-191 with the minimum
+ * frequency resolution of 1 MHz set by Mode, PCalExtractorImplicitShift
+ * pcal.cpp:927-958, 1073-1086).  nbins 0: the band has no tone and reads as
+ * one zero tone (the dummy extractor); nbins -1: an extractor this oracle
+ * does not restate (lower sideband, trivial or shifting extractor). */
+static void pcal_plan(const fxb_freq *f, double interval_d, double base_d, int *ntones, int *nbins, int *first,
+                      int *step)
+{
+	const float interval = (float)interval_d, base = (float)base_d;
+	const double lo = f->freq_mhz, bw = f->bw_mhz;
+	double tonefreq;
+	int n = 0, off;
+	*nbins = -1;
+	*first = *step = 0;
+	if(f->lower_sideband)
+	{
+		tonefreq = (double)((int)(lo / interval)) * interval;
+		if(tonefreq == lo) tonefreq -= interval;
+		if(tonefreq >= lo - bw)
+			while(tonefreq - (float)(n * interval) >= lo - bw) n++;
+		*ntones = n > 0 ? n : 1;
+		return;
+	}
+	tonefreq = (double)((int)(lo / interval)) * interval;
+	if(tonefreq <= lo) tonefreq += interval;
+	if(tonefreq <= lo + bw)
+		while(tonefreq + (float)(n * interval) <= lo + bw) n++;
+	if(n == 0)
+	{
+		*ntones = 1;
+		*nbins = 0;
+		return;
+	}
+	*ntones = n;
+	off = (int)(long)(1e6 * tonefreq + 0 * 1e6 * interval + 1e6 * base - 1e6 * lo + 0.5);
+	{
+		const double fs = 2.0 * 1e6 * bw, sp = 1e6 * interval;
+		int No, Np, Nt;
+		No = (int)(fs / dgcd(fs, (double)off));
+		Np = (int)(fs / dgcd(fs, sp));
+		Nt = calc_num_tones(1e6 * bw, (double)off, sp);
+		while(fs / (2 * No) > 1e6) No *= 2;
+		if(Nt == 0) { *nbins = 0; return; }
+		if(off == 0 || (No % Np) != 0 || Nt != n) return;   /* not restated */
+		*nbins = No;
+		*step = (int)floor((double)No * (sp / fs));
+		*first = (int)floor((double)No * ((double)off / fs));
+	}
+}
 
 /* samplegranularity (format_vdif.c:3845-3849) */
 static int granularity(int nchan, int nbits)
@@ -306,6 +400,29 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 			j->zoom_choff[s][z] = off;
 		}
 	}
+	/* phase cal (configuration.cpp:1771-1846, pcal.cpp:139-191, 927-958) */
+	j->pcal_interval = (double *)calloc((size_t)(d->nstation > 0 ? d->nstation : 1), sizeof(double));
+	j->pcal_base = (double *)calloc((size_t)(d->nstation > 0 ? d->nstation : 1), sizeof(double));
+	j->pc_ntones = (int **)calloc(d->nstation, sizeof(int *));
+	j->pc_nbins = (int **)calloc(d->nstation, sizeof(int *));
+	j->pc_first = (int **)calloc(d->nstation, sizeof(int *));
+	j->pc_step = (int **)calloc(d->nstation, sizeof(int *));
+	for(s = 0; s < d->nstation; s++)
+	{
+		const fxb_station *st = &d->stations[s];
+		int k;
+		j->pcal_interval[s] = st->pcal_interval_mhz;
+		j->pcal_base[s] = st->pcal_base_mhz;
+		j->pc_ntones[s] = (int *)calloc(st->nband, sizeof(int));
+		j->pc_nbins[s] = (int *)calloc(st->nband, sizeof(int));
+		j->pc_first[s] = (int *)calloc(st->nband, sizeof(int));
+		j->pc_step[s] = (int *)calloc(st->nband, sizeof(int));
+		if(!(st->pcal_interval_mhz > 0))
+			continue;
+		for(k = 0; k < st->nband; k++)
+			pcal_plan(&d->freqs[st->band_freq[k]], st->pcal_interval_mhz, st->pcal_base_mhz, &j->pc_ntones[s][k],
+			          &j->pc_nbins[s][k], &j->pc_first[s][k], &j->pc_step[s][k]);
+	}
 	j->ds1 = (int *)calloc(d->nbaseline, sizeof(int));
 	j->ds2 = (int *)calloc(d->nbaseline, sizeof(int));
 	j->nprod = (int *)calloc(d->nbaseline, sizeof(int));
@@ -428,6 +545,17 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 			if(toadd == 0) toadd = 1;
 			idx += toadd;
 		}
+		/* then the phase-cal tones (configuration.cpp:2423-2431) */
+		j->pcoff = (int64_t *)malloc(sizeof(int64_t) * j->nstation);
+		for(s = 0; s < j->nstation; s++)
+		{
+			int k;
+			j->pcoff[s] = -1;
+			if(!(j->pcal_interval[s] > 0)) continue;
+			j->pcoff[s] = idx;
+			for(k = 0; k < j->nband[s]; k++)
+				idx += j->pc_ntones[s][k];
+		}
 		j->corelen = idx;
 	}
 
@@ -457,6 +585,10 @@ void fxo_destroy(fxo_job *j)
 		free(j->zoom_freq[i]);
 		free(j->zoom_parent[i]);
 		free(j->zoom_choff[i]);
+		free(j->pc_ntones[i]);
+		free(j->pc_nbins[i]);
+		free(j->pc_first[i]);
+		free(j->pc_step[i]);
 		free(j->poly[i].coeffs);
 	}
 	for(i = 0; i < j->nbaseline; i++)
@@ -468,6 +600,8 @@ void fxo_destroy(fxo_job *j)
 	free(j->freqs); free(j->nbits); free(j->payload); free(j->header); free(j->nband);
 	free(j->band_freq); free(j->band_pol); free(j->poly);
 	free(j->nzoom); free(j->zoom_freq); free(j->zoom_parent); free(j->zoom_choff);
+	free(j->pcal_interval); free(j->pcal_base); free(j->pc_ntones); free(j->pc_nbins); free(j->pc_first);
+	free(j->pc_step); free(j->pcoff);
 	free(j->ds1); free(j->ds2); free(j->nprod); free(j->prod_freq); free(j->prod_b1); free(j->prod_b2);
 	free(j->freqused); free(j->equivused); free(j->bloff); free(j->bwoff); free(j->acoff); free(j->acwoff);
 	free(j);
@@ -483,6 +617,7 @@ int fxo_layout(const fxo_job *j, int32_t *out)
 	for(i = 0; i < j->nfreq * j->nbaseline; i++) out[k++] = (int32_t)j->bwoff[i];
 	for(i = 0; i < j->nstation; i++) out[k++] = (int32_t)j->acoff[i];
 	for(i = 0; i < j->nstation; i++) out[k++] = (int32_t)j->acwoff[i];
+	for(i = 0; i < j->nstation; i++) out[k++] = (int32_t)j->pcoff[i];
 	return k;
 }
 
@@ -733,10 +868,17 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 	float *scratch;
 	dcx *work;
 	int32_t **allvalid = (int32_t **)calloc(S, sizeof(int32_t *));
+	double ***pbins = (double ***)calloc(S, sizeof(double **));   /* phase-cal bins [s][band][N] */
 
 	for(s = 0; s < S; s++)
 	{
 		int nchan = station_nchan(j, s);
+		if(j->pcal_interval[s] > 0)
+		{
+			pbins[s] = (double **)calloc(j->nband[s], sizeof(double *));
+			for(b = 0; b < j->nband[s]; b++)
+				pbins[s][b] = (double *)calloc(j->pc_nbins[s][b] > 0 ? j->pc_nbins[s][b] : 1, sizeof(double));
+		}
 		if(2 * nchan + 8 > maxn) maxn = 2 * nchan + 8;
 		if(j->nband[s] > maxnb) maxnb = j->nband[s];
 		spec[s] = (dcx *)calloc((size_t)T * j->nband[s] * nchan, sizeof(dcx));
@@ -769,6 +911,24 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 				w[(size_t)s * T + t] = fi.status == 1 ? fi.weight : 0.0f;
 				memset(sp, 0, sizeof(dcx) * nb * nchan);
 				continue;
+			}
+			/* phase cal: the window's unpacked samples, binned by their sample
+			 * number in the data second (datasamples + nearestsample + n)
+			 * modulo the bin count (mode.cpp:773-787, pcal.cpp:1000-1050) */
+			if(pbins[s])
+			{
+				int gran = granularity(nb, j->nbits[s]);
+				int stu = 2 * nchan + (gran > 1 ? gran : 0);
+				double sampletime = 1.0 / (2.0 * station_bw(j, s));
+				long long a0 = (long long)(int)(datans[s] / (sampletime * 1e3) + 0.5) + fi.nearestsample;
+				for(b = 0; b < nb; b++)
+				{
+					int N = j->pc_nbins[s][b];
+					const float *x = scratch + (size_t)b * stu + (fi.nearestsample - ups[s]);
+					if(N <= 0) continue;
+					for(c = 0; c < 2 * nchan; c++)
+						pbins[s][b][(a0 + c) % N] += x[c];
+				}
 			}
 			/* autocorrelations (mode.cpp:1293-1308) and cross-pol autos (:1356-1369) */
 			for(b = 0; b < nb; b++)
@@ -906,6 +1066,40 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 				}
 		}
 	}
+
+	/* phase-cal tones: a forward DFT of the bins at the tone bins, band by
+	 * band (pcal.cpp:1060-1086, core.cpp:1124-1150) */
+	for(s = 0; s < S; s++)
+	{
+		int64_t ridx;
+		if(!pbins[s]) continue;
+		ridx = j->pcoff[s];
+		for(b = 0; b < j->nband[s]; b++)
+		{
+			int N = j->pc_nbins[s][b], k;
+			for(k = 0; k < j->pc_ntones[s][b]; k++)
+			{
+				double re = 0.0, im = 0.0;
+				long long idx = (long long)j->pc_first[s][b] + (long long)k * j->pc_step[s][b];
+				if(N > 0 && idx < N)
+				{
+					int m;
+					for(m = 0; m < N; m++)
+					{
+						double ang = -TWO_PI_D * (double)((idx * m) % N) / (double)N;
+						re += pbins[s][b][m] * cos(ang);
+						im += pbins[s][b][m] * sin(ang);
+					}
+				}
+				coreresult[2 * (ridx + k)] += re;
+				coreresult[2 * (ridx + k) + 1] += im;
+			}
+			ridx += j->pc_ntones[s][b];
+			free(pbins[s][b]);
+		}
+		free(pbins[s]);
+	}
+	free(pbins);
 
 	if(fftweights)
 		memcpy(fftweights, w, sizeof(float) * (size_t)S * T);

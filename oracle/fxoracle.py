@@ -82,7 +82,7 @@ class OracleCorrelator:
 
     def layout(self) -> np.ndarray:
         nf, nb, ns = len(self.job.freqs), len(self.job.baselines), len(self.job.stations)
-        out = np.zeros(2 * nf * nb + 2 * ns, dtype=np.int32)
+        out = np.zeros(2 * nf * nb + 3 * ns, dtype=np.int32)
         lib().fxo_layout(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
         return out
 

@@ -106,6 +106,8 @@ void process_range(RefJob *j, int t, int startblock, int numblocks,
 		modes[d]->setData((u8 *)bufs[d], nbytes[d], dscan[d], dsec[d], dns[d]);
 		modes[d]->setOffsets(scan, sec, ns);
 		modes[d]->setDumpKurtosis(false);
+		if(config->getDPhaseCalIntervalMHz(0, d) > 0)
+			modes[d]->resetpcal();              /* core.cpp:716-728 */
 	}
 
 	int numfftloops = numblocks / nbuf + ((numblocks % nbuf) ? 1 : 0);
@@ -267,6 +269,25 @@ void process_range(RefJob *j, int t, int startblock, int numblocks,
 				widx++;
 			}
 	}
+
+	/* phase-cal tones of the thread's blocks, band by band (core.cpp:1124-1150) */
+	for(int d = 0; d < j->numds; d++)
+	{
+		if(config->getDPhaseCalIntervalMHz(0, d) <= 0)
+			continue;
+		modes[d]->finalisepcal();
+		int ridx = config->getCoreResultPCalOffset(0, d);
+		for(int b = 0; b < config->getDNumRecordedBands(0, d); b++)
+		{
+			int lf = config->getDLocalRecordedFreqIndex(0, d, b);
+			for(int k = 0; k < config->getDRecordedFreqNumPCalTones(0, d, lf); k++)
+			{
+				acc->results[ridx].re += modes[d]->getPcal(b, k).re;
+				acc->results[ridx].im += modes[d]->getPcal(b, k).im;
+				ridx++;
+			}
+		}
+	}
 }
 
 } // namespace
@@ -328,8 +349,9 @@ void dref_info(void *h, int *info)
 }
 
 /* Core-result offsets for layout parity: out[f*numbl + b] = baseline offset
- * (or -1), then bweight offsets likewise, then per-datastream autocorr and
- * acweight offsets.  out must hold 2*nfreq*numbl + 2*numds ints. */
+ * (or -1), then bweight offsets likewise, then per-datastream autocorr,
+ * acweight and phase-cal (-1 without phase cal) offsets.  out must hold
+ * 2*nfreq*numbl + 3*numds ints. */
 void dref_layout(void *h, int *out)
 {
 	RefJob *j = (RefJob *)h;
@@ -348,6 +370,8 @@ void dref_layout(void *h, int *out)
 		out[k++] = c->getCoreResultAutocorrOffset(0, d);
 	for(int d = 0; d < j->numds; d++)
 		out[k++] = c->getCoreResultACWeightOffset(0, d);
+	for(int d = 0; d < j->numds; d++)
+		out[k++] = c->getDPhaseCalIntervalMHz(0, d) > 0 ? c->getCoreResultPCalOffset(0, d) : -1;
 }
 
 /* Correlate one subintegration and ADD it into coreresult (2*corelen floats).

@@ -108,7 +108,7 @@ class RefCorrelator:
 
     def layout(self) -> np.ndarray:
         nf = len(self.job.freqs)
-        n = 2 * nf * self.numbl + 2 * self.numds
+        n = 2 * nf * self.numbl + 3 * self.numds
         out = np.zeros(n, dtype=np.int32)
         lib().dref_layout(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
         return out

@@ -20,16 +20,23 @@ def small_job(nstation=4, nchan=256, bw=16.0, nfreq=1, full_pol=False, nbits=2, 
 
 
 def regions(job: Job, layout: np.ndarray, corelen: int):
-    """(name, float slice) of the core result: cross, bweights, autos, acweights."""
+    """(name, float slice) of the core result: cross, bweights, autos,
+    acweights and (with phase cal) the phase-cal tones."""
     nf, nb, ns = len(job.freqs), len(job.baselines), len(job.stations)
     bl = layout[:nf * nb]
     bw = layout[nf * nb:2 * nf * nb]
     ac = layout[2 * nf * nb:2 * nf * nb + ns]
-    acw = layout[2 * nf * nb + ns:]
+    acw = layout[2 * nf * nb + ns:2 * nf * nb + 2 * ns]
+    pc = layout[2 * nf * nb + 2 * ns:2 * nf * nb + 3 * ns]
+    pc_valid = pc[pc >= 0]
+    acw_end = int(pc_valid.min()) if pc_valid.size else corelen
     bw_valid = bw[bw >= 0]
     xc_end = int(bw_valid.min()) if bw_valid.size else int(ac.min())
-    return [("cross", slice(0, 2 * xc_end)), ("bweight", slice(2 * xc_end, 2 * int(ac.min()))),
-            ("auto", slice(2 * int(ac.min()), 2 * int(acw.min()))), ("acweight", slice(2 * int(acw.min()), 2 * corelen))]
+    out = [("cross", slice(0, 2 * xc_end)), ("bweight", slice(2 * xc_end, 2 * int(ac.min()))),
+           ("auto", slice(2 * int(ac.min()), 2 * int(acw.min()))), ("acweight", slice(2 * int(acw.min()), 2 * acw_end))]
+    if pc_valid.size:
+        out.append(("pcal", slice(2 * acw_end, 2 * corelen)))
+    return out
 
 
 def rel_err(a: np.ndarray, b: np.ndarray) -> float:
@@ -93,3 +100,23 @@ def mixed_bw_zoom_job(seed=4) -> Job:
     synth.make_delay_polys(job, seed=seed)
     job.validate()
     return job
+
+
+def pcal_job(interval=1.0, base=0.0, **kw) -> Job:
+    """small_job with phase-cal extraction on every station."""
+    job = small_job(**kw)
+    for st in job.stations:
+        st.pcal_interval_mhz = interval
+        st.pcal_base_mhz = base
+    return job
+
+
+# integer LOs (32 bins), a fractional LO (3200 bins), 8-bit samples, a comb
+# whose spacing exceeds the band (one zero tone), and a 5 MHz comb
+PCAL_JOBS = {
+    "pcal_int_lo": lambda: pcal_job(nstation=3, nfreq=2, full_pol=True, subint_ns=2_048_000),
+    "pcal_frac_lo": lambda: pcal_job(nstation=3, nfreq=2, full_pol=True, freq0=8400.01, subint_ns=2_048_000),
+    "pcal_8bit": lambda: pcal_job(nstation=2, nbits=8, freq0=8400.25),
+    "pcal_no_tone": lambda: pcal_job(20.0, nstation=2, freq0=8401.0),
+    "pcal_5mhz": lambda: pcal_job(5.0, nstation=2, freq0=8402.0),
+}

@@ -76,6 +76,28 @@ def test_zoom_rejections():
         native.job_layout(job)
 
 
+@pytest.mark.parametrize("name", ["pcal_int_lo", "pcal_frac_lo", "pcal_8bit", "pcal_no_tone", "pcal_5mhz"])
+def test_pcal_layout_matches_oracle(name):
+    from helpers import PCAL_JOBS
+    job = PCAL_JOBS[name]()
+    lay, n = native.job_layout(job)
+    orc = fxoracle.OracleCorrelator(job)
+    assert n == orc.corelen
+    assert np.array_equal(lay, orc.layout())
+
+
+def test_pcal_rejections():
+    from helpers import pcal_job
+    # a 4 MHz first-tone offset with a 5 MHz comb in 32 Ms/s needs the
+    # shifting extractor (pcal.cpp:494-705), which is not built
+    job = pcal_job(5.0, nstation=2, freq0=8416.0)
+    with pytest.raises(native.FxbError, match="UNSUPPORTED"):
+        native.job_layout(job)
+    job = pcal_job(1.0, nstation=2, lsb=True)
+    with pytest.raises(native.FxbError, match="UNSUPPORTED"):
+        native.job_layout(job)
+
+
 def test_job_rejections():
     job = small_job()
     job.subint_ns = 4_000_100          # not a whole number of FFTs

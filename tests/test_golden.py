@@ -38,8 +38,10 @@ def load_corr():
 def test_oracle_correlation_matches_golden():
     job, z, inputs = load_corr()
     orc = fxoracle.OracleCorrelator(job)
-    assert np.array_equal(orc.layout(), z["layout"])
+    # the fixture predates the phase-cal offsets: a job without phase cal has -1 there
+    lay = orc.layout()
+    assert np.array_equal(lay[:len(z["layout"])], z["layout"]) and (lay[len(z["layout"]):] == -1).all()
     for s in range(len(job.stations)):
         assert np.array_equal(orc.interpolator(s, int(z["sec"]), int(z["ns"])), z["interp"][s])
     got = orc.process_subint(inputs, int(z["sec"]), int(z["ns"]))
-    compare_core(job, z["layout"], orc.corelen, z["core"].astype(np.float64), got, tol=2e-6)
+    compare_core(job, lay, orc.corelen, z["core"].astype(np.float64), got, tol=2e-6)

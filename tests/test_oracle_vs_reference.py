@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from fxb200 import synth
-from helpers import compare_core, mixed_bw_zoom_job, rel_err, small_job, zoom_job
+from helpers import PCAL_JOBS, compare_core, mixed_bw_zoom_job, rel_err, small_job, zoom_job
 
 import fxoracle
 import refcorr
@@ -67,6 +67,23 @@ def test_zoom_subint_matches_reference(name):
     r = ref.process_subint(inputs, vf, 0, sec, ns)
     o = orc.process_subint(inputs, sec, ns, validflags=vf)
     compare_core(job, orc.layout(), orc.corelen, r.astype(np.float64), o, tol=2e-6)
+
+
+@pytest.mark.parametrize("name", sorted(PCAL_JOBS))
+def test_pcal_subint_matches_reference(name):
+    # phase-cal tones of the implicit-shift extractor (pcal.cpp:927-1105) and
+    # of bands without a tone, copied band by band (core.cpp:1124-1150)
+    job = PCAL_JOBS[name]()
+    ref = refcorr.RefCorrelator(job)
+    orc = fxoracle.OracleCorrelator(job)
+    assert np.array_equal(ref.layout(), orc.layout())
+    sec, ns = 0, 1_024_000
+    inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=7)
+    vf = [synth.valid_flags(job) for _ in job.stations]
+    r = ref.process_subint(inputs, vf, 0, sec, ns)
+    o = orc.process_subint(inputs, sec, ns, validflags=vf)
+    errs = compare_core(job, orc.layout(), orc.corelen, r.astype(np.float64), o, tol=2e-6)
+    assert "pcal" in errs
 
 
 def test_mode_spectra_match_reference():
