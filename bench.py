@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (p50/p99 job latency)")
     ap.add_argument("--no-c3", action="store_true", help="skip the batched uneven-subband leg")
     ap.add_argument("--no-mux", action="store_true", help="skip the INTERLACEDVDIF muxing leg")
+    ap.add_argument("--no-features", action="store_true", help="skip the phase-cal and zoom-band legs")
     ap.add_argument("--serving-jobs", type=int, default=12)
     return ap.parse_args()
 
@@ -395,6 +396,65 @@ def mux_leg(args):
 
 
 # ---------------------------------------------------------------- GPU arm
+def features_leg(args, job, plain_value, step_device, max_over_ranks, data_s):
+    """The headline workload correlated with a 1 MHz phase-cal comb on every
+    station (integer LOs: 64 bins per band, register sums; LOs 10 kHz off the
+    comb: 6400 bins per band) and with two 8 MHz zoom windows per 32 MHz
+    subband correlated beside it; each on the headline's device-resident
+    subints, timed with CUDA events like the headline."""
+    import copy
+
+    import torch
+    from fxb200.job import add_zoom_bands
+    from fxb200.native import Correlator
+
+    def pcal(v, shift):
+        for st in v.stations:
+            st.pcal_interval_mhz = 1.0
+        for f in v.freqs:
+            f.freq_mhz += shift
+
+    variants = [
+        ("pcal_1mhz_comb_int_lo", lambda v: pcal(v, 0.0),
+         "1 MHz comb on every station, LOs on the comb: 32 tones and 64 bins per band"),
+        ("pcal_1mhz_comb_frac_lo", lambda v: pcal(v, 0.01),
+         "1 MHz comb on every station, LOs 10 kHz off the comb: 32 tones and 6400 bins per band"),
+        ("zoom_2x8mhz_per_subband", lambda v: add_zoom_bands(v, [(f, off, 8.0) for f in range(len(v.freqs))
+                                                                 for off in (4.0, 20.0)]),
+         "two 8 MHz zoom windows (256 channels) per 32 MHz subband, correlated beside the subbands"),
+    ]
+    out = {}
+    for name, mod, desc in variants:
+        v = copy.deepcopy(job)
+        mod(v)
+        v.validate()
+        c = Correlator(v, xmac=args.xmac, inflight=3)
+        c.autotune(2)
+        for _ in range(args.warmup):
+            step_device(c)
+        c.sync()
+        torch.cuda.synchronize()
+        c.timing_enable(True)
+        st = torch.cuda.ExternalStream(c.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            step_device(c)
+        e1.record(st)
+        e1.synchronize()
+        c.sync()
+        n, p, f, x = c.timing_read()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        val = v.station_mhz_per_sec() * data_s / (ms * 1e-3)
+        out[name] = {"desc": desc, "value": val, "unit": UNIT, "rtf": data_s / (ms * 1e-3),
+                     "vs_headline": val / plain_value,
+                     "kernel_ms_per_subint": {"prep": p / max(n, 1), "fstage_pcal_zoom": f / max(n, 1),
+                                              "xmac": x / max(n, 1)}}
+        c.close()
+    return out
+
+
 def gpu_arm(args, job):
     import torch
     import torch.distributed as dist
@@ -540,6 +600,12 @@ def gpu_arm(args, job):
     else:
         tc_vs_fp32 = None
 
+    # ---- the headline workload with phase-cal extraction or zoom bands, on
+    # the same device-resident inputs (rank 0, N=1)
+    feats = None
+    if rank == 0 and world == 1 and not args.no_features:
+        feats = features_leg(args, job, value, step_device, max_over_ranks, data_s)
+
     # ---- rooflines: F stage against HBM (its design bound), XMAC against the
     # tensor (bf16) or FP32 pipes
     hbm_peak, tf_peak, peak_src = load_peaks()
@@ -605,6 +671,7 @@ def gpu_arm(args, job):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps},
             "roofline": roofline, "xmac_roofline": xmac_roofline, "cpu_baseline": cpu, "clocks": clk,
             "other_form": other, "tc_vs_fp32": tc_vs_fp32, "tuning": tuning, "serving": serve, "batched_c3": c3, "vdif_mux": mux,
+            "features": feats,
             "gpu_launches": launches_per_subint * nsub * args.steps,
         }
         print(json.dumps(line), flush=True)

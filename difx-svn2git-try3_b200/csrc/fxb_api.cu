@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <tuple>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -97,6 +98,8 @@ struct fxb_ctx {
 	DevPcalBand *d_pbands = nullptr;
 	int npbands = 0;
 	int pchunks = 1;                     // chunks of FFTs, each with its own slice of the bins
+	struct PcalClass { int first, count, nbits, bpt, maxbins; size_t smem; };
+	std::vector<PcalClass> pclass;       // runs of groups of one sample layout: one launch each
 	size_t psmem = 0;
 	double *d_pbins = nullptr;           // [pchunks][job.pcal_bins]
 	float2 *d_core = nullptr;
@@ -258,13 +261,16 @@ static std::vector<DevPcalGroup> pcal_groups(const Job &job)
 	return out;
 }
 
-// Chunks of FFTs per subint for the phase-cal binning: about four CTAs per SM
-// over all groups, at most one FFT per chunk, and at most 64 MB of bins.
-static int pcal_chunks(const Job &job, size_t ngroups)
+// Chunks of FFTs per subint for the phase-cal binning: about four CTAs per
+// SM, at most one FFT per chunk, and at most 64 MB of bins.
+static int pcal_chunks(const Job &job, const std::vector<DevPcalGroup> &groups)
 {
-	if(ngroups == 0 || job.pcal_bins <= 0)
+	int64_t ctas = 0;                     // CTAs of one chunk: blocks of 256 bins per group
+	for(const DevPcalGroup &g : groups)
+		ctas += (g.nbins + 255) / 256;
+	if(ctas == 0 || job.pcal_bins <= 0)
 		return 1;
-	int n = (int)((600 + ngroups - 1) / ngroups);
+	int n = (int)((600 + ctas - 1) / ctas);
 	n = std::min(n, std::max(job.blockspersend, 1));
 	const int64_t cap = (int64_t)(64 << 20) / (8 * job.pcal_bins);
 	n = (int)std::min<int64_t>(n, std::max<int64_t>(cap, 1));
@@ -669,12 +675,29 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			for(const Job::PcalBand &p : job.pcal)
 				hb.push_back(DevPcalBand{p.ntones, p.nbins, p.first, p.step, p.bin_off, p.core});
 			ctx->h_pgroups = pcal_groups(job);
-			ctx->pchunks = pcal_chunks(job, ctx->h_pgroups.size());
+			auto class_of = [&](const DevPcalGroup &g) {
+				const Job::Station &js = job.stations[g.station];
+				return std::make_pair(js.nbits, js.nbits * js.nband);
+			};
+			std::stable_sort(ctx->h_pgroups.begin(), ctx->h_pgroups.end(),
+			                 [&](const DevPcalGroup &x, const DevPcalGroup &y) { return class_of(x) < class_of(y); });
+			ctx->pchunks = pcal_chunks(job, ctx->h_pgroups);
+			const int tpc = (ctx->T + ctx->pchunks - 1) / ctx->pchunks;
+			for(size_t i = 0; i < ctx->h_pgroups.size(); i++)
+			{
+				const DevPcalGroup &g = ctx->h_pgroups[i];
+				const auto c = class_of(g);
+				if(ctx->pclass.empty() || ctx->pclass.back().nbits != c.first || ctx->pclass.back().bpt != c.second)
+					ctx->pclass.push_back({(int)i, 0, c.first, c.second, 0, 0});
+				fxb_ctx::PcalClass &pc = ctx->pclass.back();
+				pc.count++;
+				pc.maxbins = std::max(pc.maxbins, g.nbins);
+				pc.smem = std::max(pc.smem, pcal_smem(pcal_group_smem(g), tpc));
+				ctx->psmem = std::max(ctx->psmem, pc.smem);
+			}
 			ctx->npbands = (int)hb.size();
 			if(ctx->npbands)
 			{
-				for(const DevPcalGroup &g : ctx->h_pgroups)
-					ctx->psmem = std::max(ctx->psmem, pcal_group_smem(g));
 				if(ctx->psmem)
 					CK(ctx, pcal_init(ctx->psmem));
 				CK(ctx, dalloc(ctx, &ctx->d_pbands, hb.size()));
@@ -999,8 +1022,10 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 		if(tuning)
 			cudaEventRecord(tn.ev[nk], st);
 	}
-	launch_pcal_bin(ctx->d_pgroups, (int)ctx->h_pgroups.size(), ctx->psmem, ctx->pchunks, ctx->d_st, sl.d_sub,
-	                ctx->d_params, ctx->d_valid, ctx->valid_stride, ctx->T, job.pcal_bins, ctx->d_pbins, st);
+	for(const auto &pc : ctx->pclass)
+		launch_pcal_bin(ctx->d_pgroups + pc.first, pc.count, pc.maxbins, ctx->pchunks, pc.nbits, pc.bpt, pc.smem,
+		                ctx->d_st, sl.d_sub, ctx->d_params, ctx->d_valid, ctx->valid_stride, ctx->T, job.pcal_bins,
+		                ctx->d_pbins, st);
 	launch_zoom_gather(ctx->d_zoom, ctx->nzoom, ctx->d_plans, ctx->T, ctx->tc,
 	                   ctx->tc ? ctx->d_specn : (void *)ctx->d_spec, st);
 	cudaEventRecordWithFlags(sl.tev[2], st, evf);
@@ -1363,7 +1388,7 @@ fxb_status fxb_job_footprint(const fxb_job_desc *desc, size_t *bytes)
 	                                     : job.xmac_kind == FXB_XMAC_BF16 ? 4.0 * 1.25 * pad32
 	                                                                      : (4.0 * pad64 + 2.0 * pad64 + 0.5) * 1.25);
 	b += (double)job.acc_total * 8.0 + (double)job.corelen * 16.0 + (double)S * T * 64.0 +
-	     (double)job.pcal_bins * 8.0 * pcal_chunks(job, pcal_groups(job).size());
+	     (double)job.pcal_bins * 8.0 * pcal_chunks(job, pcal_groups(job));
 	// raw VDIF staging of the in-flight subints (payload plus headers, 1/8 slack)
 	for(int s = 0; s < S; s++)
 	{

@@ -527,9 +527,11 @@ void launch_vdif_unpack(const uint8_t *data, int64_t nbytes, int payload, int he
 
 // ---------------------------------------------------------------- zoom bands
 // A zoom band's spectra are the channels [choff, choff + nchan) of its parent
-// band's (mode.cpp:169-208): one CTA per (FFT, zoom row) copies them into the
-// zoom frequency's own spectra rows, FP32 [t][row][chan] (float2) or the
+// band's (mode.cpp:169-208): one CTA per (8 FFTs, zoom row) copies them into
+// the zoom frequency's own spectra rows, FP32 [t][row][chan] (float2) or the
 // tensor-core form's blocked [t][block][row][tcb] (bf16x2 as uint32).
+constexpr int kZoomTimes = 8;
+
 __device__ __forceinline__ int64_t spec_index(const DevFreqPlan &p, int t, int row, int c)
 {
 	if(p.tcb == 0)
@@ -539,13 +541,20 @@ __device__ __forceinline__ int64_t spec_index(const DevFreqPlan &p, int t, int r
 
 template <typename V>
 __global__ void __launch_bounds__(256) k_zoom_gather(const DevZoomCopy *__restrict__ zc,
-                                                     const DevFreqPlan *__restrict__ plans, V *__restrict__ spec)
+                                                     const DevFreqPlan *__restrict__ plans, int T,
+                                                     V *__restrict__ spec)
 {
 	const DevZoomCopy z = zc[blockIdx.y];
-	const int t = blockIdx.x;
 	const DevFreqPlan src = plans[z.src_plan], dst = plans[z.dst_plan];
-	for(int c = threadIdx.x; c < z.nchan; c += blockDim.x)
+	const int t0 = blockIdx.x * kZoomTimes;
+	const int nt = min(kZoomTimes, T - t0);
+	// zoom channel counts are powers of two
+	const int lg = __ffs(z.nchan) - 1;
+	for(int i = threadIdx.x; i < (nt << lg); i += blockDim.x)
+	{
+		const int t = t0 + (i >> lg), c = i & (z.nchan - 1);
 		spec[spec_index(dst, t, z.dst_row, c)] = spec[spec_index(src, t, z.src_row, z.choff + c)];
+	}
 }
 
 void launch_zoom_gather(const DevZoomCopy *zc, int nzc, const DevFreqPlan *plans, int T, bool tc, void *spec,
@@ -553,11 +562,11 @@ void launch_zoom_gather(const DevZoomCopy *zc, int nzc, const DevFreqPlan *plans
 {
 	if(nzc <= 0 || T <= 0)
 		return;
-	const dim3 grid(T, nzc);
+	const dim3 grid((T + kZoomTimes - 1) / kZoomTimes, nzc);
 	if(tc)
-		k_zoom_gather<uint32_t><<<grid, 256, 0, stream>>>(zc, plans, (uint32_t *)spec);
+		k_zoom_gather<uint32_t><<<grid, 256, 0, stream>>>(zc, plans, T, (uint32_t *)spec);
 	else
-		k_zoom_gather<float2><<<grid, 256, 0, stream>>>(zc, plans, (float2 *)spec);
+		k_zoom_gather<float2><<<grid, 256, 0, stream>>>(zc, plans, T, (float2 *)spec);
 }
 
 void upload_lut8(cudaStream_t stream)

@@ -164,15 +164,21 @@ struct DevPcalBand {
 	int32_t ntones, nbins, first, step;
 	int64_t bin_off, core;
 };
+// shared memory of a group's lane sums (bin counts below the CTA width) and
+// of one launch with tpc FFTs per chunk
 size_t pcal_group_smem(const DevPcalGroup &g);
-constexpr size_t kPcalSmemMax = 192 * 1024;   // shared memory of one group at most
-// allows the binning kernel smem bytes of dynamic shared memory (once per context)
+size_t pcal_smem(size_t group_smem, int tpc);
+constexpr size_t kPcalSmemMax = 96 * 1024;    // lane sums of one group at most
+// allows the binning kernels smem bytes of dynamic shared memory (once per context)
 cudaError_t pcal_init(size_t smem);
 // folds the subint's samples into the FP64 bins: the FFTs are split into
-// nchunk chunks, chunk c adds to bins + c * chunk_stride
-void launch_pcal_bin(const DevPcalGroup *groups, int ngroups, size_t smem, int nchunk, const DevStation *st,
-                     const DevSubintStation *sub, const FftParam *params, const uint8_t *valid, int64_t valid_stride,
-                     int T, int64_t chunk_stride, double *bins, cudaStream_t stream);
+// nchunk chunks, chunk c adds to bins + c * chunk_stride.  Every group of one
+// launch belongs to stations of nbits-bit samples with bpt bits per time;
+// maxbins is the launch's largest bin count, smem its pcal_smem.
+void launch_pcal_bin(const DevPcalGroup *groups, int ngroups, int maxbins, int nchunk, int nbits, int bpt,
+                     size_t smem, const DevStation *st, const DevSubintStation *sub, const FftParam *params,
+                     const uint8_t *valid, int64_t valid_stride, int T, int64_t chunk_stride, double *bins,
+                     cudaStream_t stream);
 // writes the tones of every band into the core result
 void launch_pcal_final(const DevPcalBand *bands, int nbands, int nchunk, int64_t chunk_stride, const double *bins,
                        float2 *core, cudaStream_t stream);

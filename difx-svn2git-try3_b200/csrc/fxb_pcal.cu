@@ -7,13 +7,12 @@
 // summed over every subint of the integration (FP64, one slice per chunk of
 // FFTs) and takes the DFT once, when the core result is read.
 //
-// k_pcal_bin: one CTA per (chunk of FFTs, group of a station's bands with the
-// same bin count N).  Samples are decoded as the F stage decodes them (zero
-// outside valid frames and past the window's blanking point).  Each thread
-// owns bins and sums their samples in a fixed order -- with N below the CTA
-// width, Q = 256 / N lanes split a bin's samples and are added in lane
-// order -- and each CTA adds its bins, without atomics, into its chunk's own
-// slice of the FP64 bins, so that the result does not depend on scheduling.
+// k_pcal_bin: CTAs over (chunk of FFTs, block of bins, group of a station's
+// bands with the same bin count N).  Samples are decoded as the F stage
+// decodes them (zero outside valid frames and past the window's blanking
+// point).  Every bin is summed in a fixed order and each CTA adds its bins,
+// without atomics, into its chunk's own slice of the FP64 bins, so that the
+// result does not depend on scheduling.
 // k_pcal_final: one CTA per band, the chunks summed in order and the DFT at
 // the tone bins, in FP64.
 
@@ -27,58 +26,69 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ float level2(uint32_t code)
-{
-	// 2-bit code -> {-HiMag, -1, +1, +HiMag} (format_vdif.c:78)
-	const float mag = ((code ^ (code >> 1)) & 1u) ? 1.0f : 3.3359f;
-	return (code & 2u) ? mag : -mag;
-}
-
-// Decoder of one station's samples in one FFT window: sample n of the window
-// for every band of the group, 0 outside valid frames and past the blanking
-// point.  Samples are visited with a constant stride, so the frame and the
-// time within it advance without divisions.
-struct Window {
-	const uint8_t *buf, *vrow;
-	int64_t valid_stride;
-	uint32_t fa, fs, framebytes, header, bpt, nbits, mask;
-	int stuck;
-};
-
-// Adds samples n0, n0 + step, ... (< L) of the window, which starts so
-// samples into frame fa, to acc[band].
-template <int NB>
-__device__ __forceinline__ void sum_samples_from(const Window &w, const DevPcalGroup &g, const float *lut8,
-                                                 uint32_t so, int n0, int step, int L, float (&acc)[NB])
-{
-	if(n0 >= L)
-		return;
-	const uint32_t x0 = so + (uint32_t)n0;
-	uint32_t kf = x0 / w.fs, tin = x0 - kf * w.fs;
-	for(int n = n0; n < L; n += step)
+// Per-thread sums of one bin over samples: SWAR lane counters (2-bit, 16
+// bands to a word) or per-band float sums.
+template <int NBITS, bool ONEWORD, bool SWAR>
+struct BinSum {
+	uint32_t le = 0, lo = 0, he = 0, ho = 0;
+	int nv = 0;
+	float acc[kPcalGroupBands];
+	__device__ __forceinline__ BinSum()
 	{
-		const int64_t fr = (int64_t)w.fa + kf;
-		if(n < w.stuck && fr < w.valid_stride && w.vrow[fr] != 0)
-		{
-			const uint32_t *wp = (const uint32_t *)(w.buf + fr * w.framebytes + w.header);
 #pragma unroll
-			for(int j = 0; j < NB; j++)
-				if(j < g.nb)
+		for(int j = 0; j < kPcalGroupBands; j++)
+			acc[j] = 0.0f;
+	}
+	__device__ __forceinline__ void flush(const uint32_t (&boff)[kPcalGroupBands], int nb)
+	{
+#pragma unroll
+		for(int j = 0; j < kPcalGroupBands; j++)
+			if(j < nb)
+			{
+				const uint32_t f = boff[j] >> 1, sh = 4u * (f >> 1);
+				const int ca = (int)((((f & 1u) ? ho : he) >> sh) & 15u);
+				const int cb = (int)((((f & 1u) ? lo : le) >> sh) & 15u);
+				acc[j] += 3.3359f * (float)(ca + cb - nv) + (float)(ca - cb);
+			}
+		le = lo = he = ho = 0u;
+		nv = 0;
+	}
+	// one sample: its word (ONEWORD) or frame words, and the bit of its time
+	__device__ __forceinline__ void add(uint32_t word, const uint32_t *wp, uint32_t tbit,
+	                                    const uint32_t (&boff)[kPcalGroupBands], int nb, const float *lut)
+	{
+		if(SWAR)
+		{
+			le += word & 0x11111111u;
+			lo += (word >> 2) & 0x11111111u;
+			he += (word >> 1) & 0x11111111u;
+			ho += (word >> 3) & 0x11111111u;
+			if(++nv == 15)
+				flush(boff, nb);
+		}
+		else
+		{
+#pragma unroll
+			for(int j = 0; j < kPcalGroupBands; j++)
+				if(j < nb)
 				{
-					const uint32_t bit = tin * w.bpt + (uint32_t)g.band[j] * w.nbits;
-					const uint32_t code = (__ldg(wp + (bit >> 5)) >> (bit & 31u)) & w.mask;
-					acc[j] += w.nbits == 2 ? level2(code) : lut8[code];
+					const uint32_t bit = tbit + boff[j];
+					const uint32_t wd = ONEWORD ? word : __ldg(wp + (bit >> 5));
+					acc[j] += lut[(wd >> (bit & 31u)) & ((1u << NBITS) - 1u)];
 				}
 		}
-		tin += (uint32_t)step;
-		while(tin >= w.fs)
-		{
-			tin -= w.fs;
-			kf++;
-		}
 	}
-}
+};
 
+// One thread per (bin, lane) of a station's group: the thread walks its
+// lane's FFT windows of the CTA's chunk in order and sums every sample that
+// falls into its bin, all bands of a word at once.  Bin counts below the CTA
+// width give each bin Q = 256 / N lanes, which take every Q-th window of the
+// chunk and are added in lane order; larger counts give each bin one lane and
+// spread the bins over CTAs.  The CTA adds its sums, without atomics, into
+// its chunk's slice of the FP64 bins.  The samples of eight windows are loaded
+// before any is used.
+template <int NBITS, bool ONEWORD, bool SWAR>
 __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__restrict__ groups,
                                                       const DevStation *__restrict__ st,
                                                       const DevSubintStation *__restrict__ sub,
@@ -86,95 +96,144 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
                                                       const uint8_t *__restrict__ valid, int64_t valid_stride, int T,
                                                       int tpc, int64_t chunk_stride, double *__restrict__ bins)
 {
-	extern __shared__ float sm[];              // bins [nb][N], then (N < 256) lane partials [Q][nb][N]
-	__shared__ float lut8[256];
+	extern __shared__ int4 ftab[];             // per FFT of the chunk: residue of its first sample, first frame, offset, blanking
+	__shared__ float lut[1 << NBITS];
 	const DevPcalGroup &g = groups[blockIdx.y];
 	const int s = g.station, nb = g.nb, N = g.nbins;
 	const DevStation &S = st[s];
 	const int tid = threadIdx.x;
-	const int Q = N >= kThreads ? 1 : kThreads / N;
-	float *part = sm + nb * N;
-	for(int i = tid; i < nb * N; i += kThreads)
-		sm[i] = 0.0f;
-	if(S.nbits == 8)
-		for(int i = tid; i < 256; i += kThreads)
-			lut8[i] = (float)((i - 128) / 3.3);      // format_vdif.c:122
-	__syncthreads();
-	Window w;
-	w.buf = sub[s].buf;
-	w.vrow = valid + (int64_t)s * valid_stride;
-	w.valid_stride = valid_stride;
-	w.fs = (uint32_t)S.framesamples;
-	w.framebytes = (uint32_t)S.framebytes;
-	w.header = (uint32_t)S.header;
-	w.nbits = (uint32_t)S.nbits;
-	w.bpt = (uint32_t)(S.nbits * S.nband);
-	w.mask = (1u << S.nbits) - 1u;
-	const int64_t datasamples = (int)(sub[s].datans / (S.sampletime * 1e3) + 0.5);   // Mode::setData
 	const int L = S.fftchannels;
-	const int t1 = min(T, (int)(blockIdx.x + 1) * tpc);
-	for(int t = blockIdx.x * tpc; t < t1; t++)
+	const uint32_t fs = (uint32_t)S.framesamples;
+	// CTAs of bins per chunk: the launch's (gridDim.x / chunks) for its
+	// largest bin count; blocks past this group's bins have nothing to do
+	const int nbb = gridDim.x / ((T + tpc - 1) / tpc);
+	const int chunk = blockIdx.x / nbb, bb = blockIdx.x - chunk * nbb;
+	if(bb * kThreads >= N)
+		return;
+	const int t0 = chunk * tpc, t1 = min(T, t0 + tpc);
+	const int64_t datasamples = (int)(sub[s].datans / (S.sampletime * 1e3) + 0.5);   // Mode::setData
+	for(int t = t0 + tid; t < t1; t += kThreads)
 	{
 		const FftParam &p = params[(int64_t)s * T + t];
-		if(p.status != kFftOk)
-			continue;                               // the same for the whole CTA
-		const int r = (int)((datasamples + p.nearest) % N);
-		const uint32_t g0 = (uint32_t)p.nearest;
-		w.fa = g0 / w.fs;
-		w.stuck = p.stuck;
-		const uint32_t so = g0 - w.fa * w.fs;
-		if(N < kThreads)
+		int4 e = make_int4(-1, 0, 0, 0);
+		if(p.status == kFftOk)
 		{
-			const int q = tid / N, m = tid - q * N;
-			if(q < Q)
-			{
-				float acc[kPcalGroupBands];
-#pragma unroll
-				for(int j = 0; j < kPcalGroupBands; j++)
-					acc[j] = 0.0f;
-				int n0 = m - r;
-				if(n0 < 0)
-					n0 += N;
-				sum_samples_from(w, g, lut8, so, n0 + q * N, Q * N, L, acc);
-#pragma unroll
-				for(int j = 0; j < kPcalGroupBands; j++)
-					if(j < nb)
-						part[(q * nb + j) * N + m] = acc[j];
-			}
-			__syncthreads();
-			for(int i = tid; i < nb * N; i += kThreads)
-			{
-				const int j = i / N, m2 = i - j * N;
-				float v = 0.0f;
-				for(int q2 = 0; q2 < Q; q2++)
-					v += part[(q2 * nb + j) * N + m2];
-				sm[i] += v;
-			}
-			__syncthreads();
+			const uint32_t g0 = (uint32_t)p.nearest;
+			e.x = (int)((datasamples + p.nearest) % N);
+			e.y = (int)(g0 / fs);
+			e.z = (int)(g0 - (uint32_t)e.y * fs);
+			e.w = p.stuck;
 		}
-		else
-			for(int m = tid; m < N; m += kThreads)
-			{
-				float acc[kPcalGroupBands];
-#pragma unroll
-				for(int j = 0; j < kPcalGroupBands; j++)
-					acc[j] = 0.0f;
-				int n0 = m - r;
-				if(n0 < 0)
-					n0 += N;
-				sum_samples_from(w, g, lut8, so, n0, N, L, acc);
-#pragma unroll
-				for(int j = 0; j < kPcalGroupBands; j++)
-					if(j < nb)
-						sm[j * N + m] += acc[j];       // bin m belongs to this thread alone
-			}
+		ftab[t - t0] = e;
 	}
+	for(int i = tid; i < (1 << NBITS); i += kThreads)
+		lut[i] = NBITS == 2 ? ((i & 2) ? 1.0f : -1.0f) * (((i ^ (i >> 1)) & 1) ? 1.0f : 3.3359f)   // format_vdif.c:78
+		                    : (float)((i - 128) / 3.3);                                              // format_vdif.c:122
 	__syncthreads();
-	double *dst = bins + (int64_t)blockIdx.x * chunk_stride;
+	const int Q = N < kThreads ? kThreads / N : 1;
+	const int q = N < kThreads ? tid / N : 0;
+	const int m = N < kThreads ? tid - q * N : bb * kThreads + tid;
+	const bool active = q < Q && m < N;
+	uint32_t boff[kPcalGroupBands];
+#pragma unroll
+	for(int j = 0; j < kPcalGroupBands; j++)
+		boff[j] = j < nb ? (uint32_t)g.band[j] * NBITS : 0u;
+	BinSum<NBITS, ONEWORD, SWAR> sum;
+	if(active)
+	{
+		const uint8_t *buf = sub[s].buf;
+		const uint8_t *vrow = valid + (int64_t)s * valid_stride;
+		const uint32_t framebytes = (uint32_t)S.framebytes, header = (uint32_t)S.header,
+		               bpt = (uint32_t)(NBITS * S.nband);
+		const int nt = t1 - t0;
+		// the next sample of bin m: window t (relative to t0), sample n of it
+		// (n = L: not yet found in window t)
+		int t = q, n = L;
+		constexpr int K = 8;
+		while(true)
+		{
+			uint32_t word[K], tbit[K];
+			const uint32_t *wp[K];
+			bool ok[K];
+#pragma unroll
+			for(int k = 0; k < K; k++)
+			{
+				ok[k] = false;
+				word[k] = tbit[k] = 0u;
+				wp[k] = nullptr;
+				while(t < nt && n >= L)
+				{
+					const int4 e = ftab[t];
+					if(e.x >= 0)
+					{
+						n = m - e.x;
+						if(n < 0)
+							n += N;
+					}
+					if(e.x < 0 || n >= L)
+					{
+						t += Q;
+						n = L;
+					}
+				}
+				if(t < nt)
+				{
+					const int4 e = ftab[t];
+					uint32_t x = (uint32_t)e.z + (uint32_t)n, kf = 0;
+					while(x >= fs)
+					{
+						x -= fs;
+						kf++;
+					}
+					const int64_t fr = (int64_t)e.y + kf;
+					ok[k] = n < e.w && fr < valid_stride && vrow[fr] != 0;
+					tbit[k] = x * bpt;
+					wp[k] = (const uint32_t *)(buf + fr * framebytes + header);
+					if(ok[k] && ONEWORD)
+						word[k] = __ldg(wp[k] + (tbit[k] >> 5));
+					n += N;
+					if(n >= L)
+					{
+						t += Q;
+						n = L;
+					}
+				}
+			}
+#pragma unroll
+			for(int k = 0; k < K; k++)
+				if(ok[k])
+					sum.add(word[k], wp[k], tbit[k], boff, nb, lut);
+			if(t >= nt)
+				break;
+		}
+		if(SWAR && sum.nv)
+			sum.flush(boff, nb);
+	}
+	double *dst = bins + (int64_t)chunk * chunk_stride;
+	if(Q == 1)
+	{
+		if(active)
+#pragma unroll
+			for(int j = 0; j < kPcalGroupBands; j++)
+				if(j < nb)
+					dst[g.bin_off[j] + m] += (double)sum.acc[j];
+		return;
+	}
+	// lanes of a bin, added in lane order
+	float *part = reinterpret_cast<float *>(ftab + tpc);    // [Q][nb][N]
+	if(active)
+#pragma unroll
+		for(int j = 0; j < kPcalGroupBands; j++)
+			if(j < nb)
+				part[(q * nb + j) * N + m] = sum.acc[j];
+	__syncthreads();
 	for(int i = tid; i < nb * N; i += kThreads)
 	{
-		const int j = i / N;
-		dst[g.bin_off[j] + (i - j * N)] += (double)sm[i];
+		const int j = i / N, mm = i - j * N;
+		float v = 0.0f;
+		for(int q2 = 0; q2 < Q; q2++)
+			v += part[(q2 * nb + j) * N + mm];
+		dst[g.bin_off[j] + mm] += (double)v;
 	}
 }
 
@@ -230,25 +289,45 @@ __global__ void __launch_bounds__(kThreads) k_pcal_final(const DevPcalBand *__re
 
 size_t pcal_group_smem(const DevPcalGroup &g)
 {
-	const size_t lanes = g.nbins >= kThreads ? 0 : (size_t)(kThreads / g.nbins);
-	return (size_t)g.nb * g.nbins * (1 + lanes) * sizeof(float);
+	// the lanes' partial sums of a bin count below the CTA width
+	return g.nbins < kThreads ? (size_t)g.nb * g.nbins * (kThreads / g.nbins) * sizeof(float) : 0;
 }
 
-void launch_pcal_bin(const DevPcalGroup *groups, int ngroups, size_t smem, int nchunk, const DevStation *st,
-                     const DevSubintStation *sub, const FftParam *params, const uint8_t *valid, int64_t valid_stride,
-                     int T, int64_t chunk_stride, double *bins, cudaStream_t stream)
+size_t pcal_smem(size_t group_smem, int tpc) { return sizeof(int4) * (size_t)tpc + group_smem; }
+
+void launch_pcal_bin(const DevPcalGroup *groups, int ngroups, int maxbins, int nchunk, int nbits, int bpt,
+                     size_t smem, const DevStation *st, const DevSubintStation *sub, const FftParam *params,
+                     const uint8_t *valid, int64_t valid_stride, int T, int64_t chunk_stride, double *bins,
+                     cudaStream_t stream)
 {
 	if(ngroups <= 0)
 		return;
+	const bool swar = nbits == 2 && bpt == 32, one = bpt <= 32;
 	const int tpc = (T + nchunk - 1) / nchunk;
-	const dim3 grid((T + tpc - 1) / tpc, ngroups);
-	k_pcal_bin<<<grid, kThreads, smem, stream>>>(groups, st, sub, params, valid, valid_stride, T, tpc, chunk_stride,
-	                                            bins);
+	const int nbb = (maxbins + kThreads - 1) / kThreads;
+	const dim3 grid(nbb * ((T + tpc - 1) / tpc), ngroups);
+#define FXB_BIN(B, O, W) k_pcal_bin<B, O, W><<<grid, kThreads, smem, stream>>>(groups, st, sub, params, valid, \
+	                                                                      valid_stride, T, tpc, chunk_stride, bins)
+	if(swar) FXB_BIN(2, true, true);
+	else if(nbits == 2 && one) FXB_BIN(2, true, false);
+	else if(nbits == 2) FXB_BIN(2, false, false);
+	else if(one) FXB_BIN(8, true, false);
+	else FXB_BIN(8, false, false);
+#undef FXB_BIN
 }
 
 cudaError_t pcal_init(size_t smem)
 {
-	return cudaFuncSetAttribute(k_pcal_bin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	const void *k[] = {(const void *)k_pcal_bin<2, true, true>, (const void *)k_pcal_bin<2, true, false>,
+	                   (const void *)k_pcal_bin<2, false, false>, (const void *)k_pcal_bin<8, true, false>,
+	                   (const void *)k_pcal_bin<8, false, false>};
+	for(const void *f : k)
+	{
+		const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		if(e != cudaSuccess)
+			return e;
+	}
+	return cudaSuccess;
 }
 
 void launch_pcal_final(const DevPcalBand *bands, int nbands, int nchunk, int64_t chunk_stride, const double *bins,

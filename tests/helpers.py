@@ -112,11 +112,14 @@ def pcal_job(interval=1.0, base=0.0, **kw) -> Job:
 
 
 # integer LOs (32 bins), a fractional LO (3200 bins), 8-bit samples, a comb
-# whose spacing exceeds the band (one zero tone), and a 5 MHz comb
+# whose spacing exceeds the band (one zero tone), a 5 MHz comb, and 1024 bins
 PCAL_JOBS = {
     "pcal_int_lo": lambda: pcal_job(nstation=3, nfreq=2, full_pol=True, subint_ns=2_048_000),
     "pcal_frac_lo": lambda: pcal_job(nstation=3, nfreq=2, full_pol=True, freq0=8400.01, subint_ns=2_048_000),
     "pcal_8bit": lambda: pcal_job(nstation=2, nbits=8, freq0=8400.25),
     "pcal_no_tone": lambda: pcal_job(20.0, nstation=2, freq0=8401.0),
     "pcal_5mhz": lambda: pcal_job(5.0, nstation=2, freq0=8402.0),
+    # first tone 31.25 kHz above the LO: 1024 bins, fewer than the 4096
+    # samples of a window
+    "pcal_1024_bins": lambda: pcal_job(nstation=2, nchan=2048, freq0=8400.96875, subint_ns=4_096_000),
 }

@@ -76,7 +76,8 @@ def test_zoom_rejections():
         native.job_layout(job)
 
 
-@pytest.mark.parametrize("name", ["pcal_int_lo", "pcal_frac_lo", "pcal_8bit", "pcal_no_tone", "pcal_5mhz"])
+@pytest.mark.parametrize("name", ["pcal_int_lo", "pcal_frac_lo", "pcal_8bit", "pcal_no_tone", "pcal_5mhz",
+                                  "pcal_1024_bins"])
 def test_pcal_layout_matches_oracle(name):
     from helpers import PCAL_JOBS
     job = PCAL_JOBS[name]()
