@@ -1567,6 +1567,55 @@ fxb_status fxb_read_results_device(fxb_ctx *ctx, float *dev_out, size_t nfloats)
 	return FXB_OK;
 }
 
+fxb_status fxb_datastream_control(fxb_ctx *ctx, int32_t station, fxb_ring *ring, int32_t scan, int32_t sec,
+                                  int32_t ns, const double *delay_us, int64_t *offset, int32_t *nbytes,
+                                  int32_t *datasec, int32_t *datans, int32_t *validflags, size_t nflagint)
+{
+	if(!ctx || station < 0 || station >= ctx->S)
+		return FXB_ERR_ARG;
+	if(!delay_us && !ctx->delay_set[station])
+	{
+		ctx->err = "no delay model for the station";
+		return FXB_ERR_STATE;
+	}
+	return datastream_control(ctx->job, ctx->h_st[station], station, ring, scan, sec, ns, delay_us, offset, nbytes,
+	                          datasec, datans, validflags, nflagint, ctx->err);
+}
+
+fxb_status fxb_job_datastream_control(const fxb_job_desc *desc, int32_t station, int32_t npoly, int32_t order,
+                                      double poly0_sec, int32_t interval_s, const double *coeffs, fxb_ring *ring,
+                                      int32_t scan, int32_t sec, int32_t ns, const double *delay_us, int64_t *offset,
+                                      int32_t *nbytes, int32_t *datasec, int32_t *datans, int32_t *validflags,
+                                      size_t nflagint)
+{
+	Job job;
+	std::string err;
+	fxb_status st = FXB_OK;
+	auto fail = [&](fxb_status code) {
+		std::lock_guard<std::mutex> lk(g_err_mutex);
+		g_create_err = err;
+		return code;
+	};
+	if(!build_job(desc, job, err, st))
+		return fail(st);
+	if(station < 0 || station >= (int)job.stations.size() || npoly < 1 || npoly > kMaxPolys || order < 0 ||
+	   order > kMaxPolyOrder || interval_s <= 0 || !coeffs)
+	{
+		err = "bad station or delay polynomial";
+		return fail(FXB_ERR_ARG);
+	}
+	DevStation d;
+	memset(&d, 0, sizeof(d));
+	d.npoly = npoly;
+	d.order = order;
+	d.interval = interval_s;
+	d.poly0 = poly0_sec;
+	memcpy(d.coeffs, coeffs, sizeof(double) * npoly * (order + 1));
+	st = datastream_control(job, d, station, ring, scan, sec, ns, delay_us, offset, nbytes, datasec, datans,
+	                        validflags, nflagint, err);
+	return st == FXB_OK ? st : fail(st);
+}
+
 fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloats, int32_t *nfft, int32_t *nrow)
 {
 	if(!ctx || !out || freq < 0 || freq >= ctx->F) return FXB_ERR_ARG;

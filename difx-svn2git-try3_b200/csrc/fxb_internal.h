@@ -171,6 +171,11 @@ fxb_status vdif_mux(const uint8_t *dev_in, int64_t inbytes, int32_t nthreads, co
                     int32_t inframebytes, int32_t fps, int32_t nbits, uint8_t *dev_out, int64_t outcap,
                     int64_t *outbytes, void *stream, std::string &err);
 
+// DataStream control blocks (fxb_datastream.cpp): S is the station's delay model
+fxb_status datastream_control(const Job &job, const DevStation &S, int s, fxb_ring *ring, int scan, int sec, int ns,
+                              const double *delay_us, int64_t *offset, int32_t *nbytes, int32_t *datasec,
+                              int32_t *datans, int32_t *validflags, size_t nflagint, std::string &err);
+
 // integration output (fxb_vis.cpp)
 fxb_status vis_calibrate(const Job &job, const fxb_vis_params *p, float *coreresult);
 fxb_status vis_swin_write(const Job &job, const fxb_vis_params *p, const float *coreresult, const char *dir,

@@ -97,6 +97,48 @@ class DescHolder:
         return ctypes.byref(self.desc)
 
 
+class FxbSegment(ctypes.Structure):
+    _fields_ = [("scan", ctypes.c_int32), ("sec", ctypes.c_int32), ("ns", ctypes.c_int32), ("readto", ctypes.c_int32),
+                ("validbytes", ctypes.c_int64)]
+
+
+class FxbRing(ctypes.Structure):
+    _fields_ = [("nseg", ctypes.c_int32), ("readbytes", ctypes.c_int32), ("atsegment", ctypes.c_int32),
+                ("keepreading", ctypes.c_int32), ("lastvalid", ctypes.c_int32), ("guard_ns", ctypes.c_int32),
+                ("seg", ctypes.POINTER(FxbSegment))]
+
+
+INVALID_SUBINT = -99999999
+
+
+def _ring(segs, readbytes, at, keep, lastvalid, guard_ns):
+    arr = (FxbSegment * len(segs))(*[FxbSegment(int(a), int(b), int(c), int(d), int(e)) for a, b, c, d, e in segs])
+    return FxbRing(len(segs), readbytes, at, int(keep), lastvalid, guard_ns,
+                   ctypes.cast(arr, ctypes.POINTER(FxbSegment))), arr
+
+
+def job_datastream_control(job: Job, station: int, segs, readbytes: int, at: int, keep: bool, lastvalid: int,
+                           scan: int, sec: int, ns: int, guard_ns: int = 0, delays=None):
+    """DataStream control block of subint (scan, sec, ns) for a station, on
+    a ring of segments (scan, seconds, ns, readto, validbytes) of readbytes
+    each: (offset, nbytes, datasec, datans, validflags, atsegment), datasec
+    INVALID_SUBINT when the ring has no data for the subint."""
+    holder = DescHolder(job)
+    npoly, order, p0, interval, coeffs = poly_arrays(job, station)
+    ring, keep_alive = _ring(segs, readbytes, at, keep, lastvalid, guard_ns)
+    T = job.blocks_per_send()
+    flags = np.zeros(T // 30 + 1, dtype=np.int32)
+    off, nb = ctypes.c_int64(), ctypes.c_int32()
+    dsec, dns = ctypes.c_int32(), ctypes.c_int32()
+    d = None if delays is None else (ctypes.c_double * 2)(*delays)
+    check(lib().fxb_job_datastream_control(holder.ptr(), station, npoly, order, p0, interval,
+                                           coeffs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(ring),
+                                           scan, sec, ns, d, ctypes.byref(off), ctypes.byref(nb), ctypes.byref(dsec),
+                                           ctypes.byref(dns), flags.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                           flags.size), None, "job_datastream_control")
+    return off.value, nb.value, dsec.value, dns.value, flags, ring.atsegment
+
+
 def poly_arrays(job: Job, s: int) -> Tuple[int, int, float, int, np.ndarray]:
     """(npoly, order, poly0_sec, interval_s, coeffs) of station s, padded to
     a common order, in the form fxb_set_delay_poly takes."""
@@ -153,6 +195,11 @@ def lib():
     L.fxb_read_fft_weights.argtypes = [vp, fp, ctypes.c_size_t]
     L.fxb_vdif_unpack.argtypes = [ctypes.c_void_p, i64, i32, i32, i32, i32, i64, i32, fp, i32p]
     L.fxb_job_layout.argtypes = [ctypes.POINTER(FxbJobDesc), i32p, ctypes.c_size_t, i64p]
+    L.fxb_job_datastream_control.argtypes = [ctypes.POINTER(FxbJobDesc), i32, i32, i32, ctypes.c_double, i32, dp,
+                                             ctypes.POINTER(FxbRing), i32, i32, i32, dp, i64p, i32p, i32p, i32p, i32p,
+                                             ctypes.c_size_t]
+    L.fxb_datastream_control.argtypes = [vp, i32, ctypes.POINTER(FxbRing), i32, i32, i32, dp, i64p, i32p, i32p, i32p,
+                                         i32p, ctypes.c_size_t]
     L.fxb_timing_enable.argtypes = [vp, i32]
     L.fxb_timing_read.argtypes = [vp, i32p, dp, dp, dp]
     L.fxb_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]

@@ -296,6 +296,61 @@ FXB_API fxb_status fxb_vdif_mux(const uint8_t *dev_in, int64_t inbytes, int32_t 
                                 int32_t inframebytes, int32_t frames_per_second, int32_t nbits, uint8_t *dev_out,
                                 int64_t outcap, int64_t *outbytes, void *stream);
 
+/* ---- DataStream control blocks: which bytes of a datastream's receive ring
+ * hold a subint, their time, and which of its FFTs have data
+ * (DataStream::calculateControlParams, datastream.cpp:376-636, with the VDIF
+ * frame alignment of VDIFDataStream::calculateControlParams,
+ * vdiffile.cpp:358-485).  A ring is nseg segments of readbytes bytes (whole
+ * frames), filled in time order by the caller's reader; memory past the
+ * ring's end repeats its start for at least one subint, so that a subint's
+ * bytes are contiguous as the reference's overflow area makes them. */
+#define FXB_INVALID_SUBINT (-99999999)   /* Mode::INVALID_SUBINT (mode.h:232) */
+
+/* One read segment (DataStream::readinfo, datastream.h:95-120). */
+typedef struct {
+	int32_t scan;             /* scan of the segment's data */
+	int32_t sec, ns;          /* time of the segment's first frame (scanseconds, scanns) */
+	int32_t readto;           /* 1 once the reader has filled (or tried to fill) the segment */
+	int64_t validbytes;       /* bytes read into the segment; readbytes when full */
+} fxb_segment;
+
+typedef struct {
+	int32_t nseg;             /* segments in the ring (NUM DATA SEGMENTS) */
+	int32_t readbytes;        /* bytes of one segment, a whole number of frames */
+	int32_t atsegment;        /* in/out: the segment the previous subint started in (0 at the start) */
+	int32_t keepreading;      /* 1 while the reader may still fill segments */
+	int32_t lastvalid;        /* with keepreading 0: the last segment the reader filled */
+	int32_t guard_ns;         /* GUARD NANOSECONDS of the configuration (when the .input leaves it 0
+	                           * the reference derives it from the delay model's largest rate,
+	                           * configuration.cpp:2741-2795: pass that value) */
+	const fxb_segment *seg;   /* [nseg] */
+} fxb_ring;
+
+/* The control block of subint (scan, sec, ns) for station `station` of the
+ * context's job: *offset = the byte of the ring where the subint's frames
+ * start, *nbytes = how many bytes to hand to fxb_submit_subint,
+ * *datasec / *datans = the time of that byte, validflags[nflagint] = the
+ * valid-FFT bits (30 per int, FLAGS_PER_INT); *datasec = FXB_INVALID_SUBINT
+ * when the ring holds no data for the subint (it is then submitted with
+ * nbytes 0 or skipped).  delay_us = the station's delays (us, integer clock
+ * seconds removed) at the subint's start and end, or NULL to evaluate the
+ * context's delay model as Model::calculateDelayInterpolator does at order 0
+ * (model.cpp:229-269).  FXB_ERR_STATE: while keepreading, no segment reaches
+ * the subint yet (the reference's main thread waits for its reader there);
+ * read further and ask again.  Host arithmetic only: no device work. */
+FXB_API fxb_status fxb_datastream_control(fxb_ctx *ctx, int32_t station, fxb_ring *ring, int32_t scan, int32_t sec,
+                                          int32_t ns, const double *delay_us, int64_t *offset, int32_t *nbytes,
+                                          int32_t *datasec, int32_t *datans, int32_t *validflags, size_t nflagint);
+
+/* The same from a job description and the station's delay model (the
+ * arguments of fxb_set_delay_poly), without a GPU or a context. */
+FXB_API fxb_status fxb_job_datastream_control(const fxb_job_desc *desc, int32_t station, int32_t npoly, int32_t order,
+                                              double poly0_sec, int32_t interval_s, const double *coeffs,
+                                              fxb_ring *ring, int32_t scan, int32_t sec, int32_t ns,
+                                              const double *delay_us, int64_t *offset, int32_t *nbytes,
+                                              int32_t *datasec, int32_t *datans, int32_t *validflags,
+                                              size_t nflagint);
+
 /* Page-locked host memory for station buffers: fxb_submit_subint copies from
  * it asynchronously at full link speed, where a pageable buffer is staged by
  * the driver on the calling thread.  Free with fxb_host_free. */

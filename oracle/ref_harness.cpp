@@ -34,6 +34,8 @@
 #include "mk5mode.h"
 #include "model.h"
 #include "mark5access.h"
+#include "vdiffile.h"
+#include <pthread.h>
 
 namespace {
 
@@ -290,6 +292,76 @@ void process_range(RefJob *j, int t, int startblock, int numblocks,
 	}
 }
 
+/* DataStream control blocks: VDIFDataStream::calculateControlParams over
+ * DataStream::calculateControlParams (vdiffile.cpp:358-485,
+ * datastream.cpp:376-636), run by the stock code on a ring whose segments
+ * the caller describes the way the read thread fills them.  The VDIF muxer
+ * parameters are set as VDIFDataStream::initialiseFile sets them
+ * (vdiffile.cpp:520-545); the caller holds the locks of the current segment
+ * and the next, as the datastream's main thread does. */
+class RingVDIF : public VDIFDataStream
+{
+public:
+	RingVDIF(const Configuration *c, int ds, int factor, int nseg, int *cid)
+		: VDIFDataStream(c, ds, ds + 1, 1, cid, factor, nseg) {}
+	void setup()
+	{
+		initialise();
+		datastatuses = new MPI_Status[maxsendspersegment];
+		controlstatuses = new MPI_Status[maxsendspersegment];
+		const int ci = bufferinfo[0].configindex;
+		configurevdifmux(&vm, config->getFrameBytes(ci, streamnum),
+		                 (int)config->getFramesPerSecond(ci, streamnum) / config->getDNumMuxThreads(ci, streamnum),
+		                 config->getDNumBits(ci, streamnum), config->getDNumMuxThreads(ci, streamnum),
+		                 config->getDMuxThreadMap(ci, streamnum), nSort, nGap,
+		                 VDIF_MUX_FLAG_RESPECTGRANULARITY | VDIF_MUX_FLAG_PROPAGATEVALIDITY);
+		waitsegment = 0;
+	}
+	int sizes(int *out)
+	{
+		out[0] = readbytes;
+		out[1] = bufferbytes;
+		out[2] = bufferinfo[0].nsinc;
+		out[3] = bufferinfo[0].sendbytes;
+		out[4] = bufferinfo[0].controllength;
+		out[5] = config->getGuardNS(0);
+		return 0;
+	}
+	/* segs: per segment scan, seconds, ns, readto, validbytes */
+	int control(const long long *segs, int at, int keep, int lastvalid, int scan, int sec, int ns, int *out, int nout)
+	{
+		for(int i = 0; i < numdatasegments; i++)
+		{
+			bufferinfo[i].scan = (int)segs[5 * i];
+			bufferinfo[i].scanseconds = (int)segs[5 * i + 1];
+			bufferinfo[i].scanns = (int)segs[5 * i + 2];
+			bufferinfo[i].readto = segs[5 * i + 3] != 0;
+			bufferinfo[i].validbytes = segs[5 * i + 4];
+			bufferinfo[i].numsent = 0;
+			pthread_mutex_destroy(&bufferlock[i]);
+			pthread_mutex_init(&bufferlock[i], NULL);
+		}
+		atsegment = at;
+		waitsegment = at;
+		keepreading = keep != 0;
+		lastvalidsegment = lastvalid;
+		pthread_mutex_lock(&bufferlock[atsegment]);
+		pthread_mutex_lock(&bufferlock[(atsegment + 1) % numdatasegments]);
+		const int bufferindex = calculateControlParams(scan, sec, ns);
+		pthread_mutex_unlock(&bufferlock[atsegment]);
+		pthread_mutex_unlock(&bufferlock[(atsegment + 1) % numdatasegments]);
+		const s32 *cb = bufferinfo[atsegment].controlbuffer[0];
+		const int n = bufferinfo[atsegment].controllength;
+		if(nout < 2 + n)
+			return -1;
+		out[0] = bufferindex;
+		out[1] = atsegment;
+		for(int k = 0; k < n; k++)
+			out[2 + k] = cb[k];
+		return 2 + n;
+	}
+};
+
 } // namespace
 
 extern "C" {
@@ -517,3 +589,31 @@ int dref_vdif_mux(const unsigned char *in, int inbytes, int nthreads, const int 
 }
 
 } // extern "C"
+
+extern "C" {
+
+/* A datastream of the job with nseg segments of readbytes = factor / nseg *
+ * (the largest subint's bytes); out: readbytes, bufferbytes, nsinc,
+ * sendbytes, control words per subint, guard ns. */
+void *dref_ds_create(void *h, int ds, int factor, int nseg, int *out)
+{
+	RefJob *j = (RefJob *)h;
+	static int cid[1] = {1};
+	RingVDIF *d = new RingVDIF(j->config, ds, factor, nseg, cid);
+	d->setup();
+	d->sizes(out);
+	return d;
+}
+
+int dref_ds_control(void *d, const long long *segs, int at, int keep, int lastvalid, int scan, int sec, int ns,
+                    int *out, int nout)
+{
+	return ((RingVDIF *)d)->control(segs, at, keep, lastvalid, scan, sec, ns, out, nout);
+}
+
+void dref_ds_destroy(void *d)
+{
+	(void)d;   /* the stock destructor closes files and frees MPI state it never opened here: leak the test object */
+}
+
+}

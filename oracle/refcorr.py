@@ -106,6 +106,19 @@ class RefCorrelator:
         with open(files[0], "rb") as f:
             return f.read()
 
+    def datastream(self, ds: int, factor: int, nseg: int) -> "RefRing":
+        """The reference's VDIF datastream ds with nseg segments of
+        factor / nseg times the largest subint's bytes."""
+        L = lib()
+        L.dref_ds_create.restype = ctypes.c_void_p
+        L.dref_ds_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_int)]
+        out = (ctypes.c_int * 6)()
+        d = L.dref_ds_create(self.h, ds, factor, nseg, out)
+        ring = RefRing(d, *list(out))
+        ring.parent = self          # the datastream reads the job's configuration
+        return ring
+
     def layout(self) -> np.ndarray:
         nf = len(self.job.freqs)
         n = 2 * nf * self.numbl + 3 * self.numds
@@ -162,3 +175,28 @@ def vdif_mux(data: np.ndarray, nthreads: int, thread_ids: Sequence[int], frameby
     if n < 0:
         raise RuntimeError("reference VDIF muxer rejected the read")
     return out[:n].tobytes()
+
+
+class RefRing:
+    """DataStream control blocks from the stock VDIFDataStream code."""
+
+    def __init__(self, d, readbytes, bufferbytes, nsinc, sendbytes, controllength, guard_ns):
+        self.d = d
+        self.readbytes, self.bufferbytes, self.nsinc = readbytes, bufferbytes, nsinc
+        self.sendbytes, self.controllength, self.guard_ns = sendbytes, controllength, guard_ns
+
+    def control(self, segs, at: int, keep: bool, lastvalid: int, scan: int, sec: int, ns: int):
+        """segs: per segment (scan, seconds, ns, readto, validbytes).  Returns
+        (bufferindex, atsegment, control words [scan, sec, ns, flags...])."""
+        L = lib()
+        L.dref_ds_control.restype = ctypes.c_int
+        L.dref_ds_control.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        arr = np.ascontiguousarray(np.array(segs, dtype=np.int64).reshape(-1))
+        out = (ctypes.c_int * 256)()
+        n = L.dref_ds_control(self.d, arr.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), at, int(keep),
+                              lastvalid, scan, sec, ns, out, 256)
+        if n < 0:
+            raise RuntimeError("control buffer too small")
+        return out[0], out[1], list(out[2:n])

@@ -22,6 +22,9 @@ extern "C" {
 int difxMessageSendDifxAlert(const char *alertMessage, int severity);
 int difxMessageSendDifxStatus3(int state, const char *message, double visMJD, int numdatastreams, float *weight,
                                double mjdStart, double mjdStop);
+int difxMessageSendDifxDiagnosticBufferStatus(int threadid, int numelements, int startelement, int numactiveelements);
+int difxMessageSendDifxDiagnosticDataConsumed(long long bytes);
+int difxMessageSendDifxDiagnosticInputDatarate(double bytespersec);
 #ifdef __cplusplus
 }
 #endif

@@ -21,3 +21,21 @@ int difxMessageSendDifxStatus3(int state, const char *message, double visMJD, in
 	(void)state; (void)message; (void)visMJD; (void)numdatastreams; (void)weight; (void)mjdStart; (void)mjdStop;
 	return 0;
 }
+
+int difxMessageSendDifxDiagnosticBufferStatus(int threadid, int numelements, int startelement, int numactiveelements)
+{
+	(void)threadid; (void)numelements; (void)startelement; (void)numactiveelements;
+	return 0;
+}
+
+int difxMessageSendDifxDiagnosticDataConsumed(long long bytes)
+{
+	(void)bytes;
+	return 0;
+}
+
+int difxMessageSendDifxDiagnosticInputDatarate(double bytespersec)
+{
+	(void)bytespersec;
+	return 0;
+}
