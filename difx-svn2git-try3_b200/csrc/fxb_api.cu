@@ -682,7 +682,11 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			std::stable_sort(ctx->h_pgroups.begin(), ctx->h_pgroups.end(),
 			                 [&](const DevPcalGroup &x, const DevPcalGroup &y) { return class_of(x) < class_of(y); });
 			ctx->pchunks = pcal_chunks(job, ctx->h_pgroups);
-			const int tpc = (ctx->T + ctx->pchunks - 1) / ctx->pchunks;
+			// chunks of a multiple of four FFTs, so that the 2 or 4 lanes of a
+			// bin (bin counts of 128 or 64) share a chunk evenly
+			int tpc = (ctx->T + ctx->pchunks - 1) / ctx->pchunks;
+			tpc = std::min(ctx->T, (tpc + 3) / 4 * 4);
+			ctx->pchunks = (ctx->T + tpc - 1) / tpc;
 			for(size_t i = 0; i < ctx->h_pgroups.size(); i++)
 			{
 				const DevPcalGroup &g = ctx->h_pgroups[i];

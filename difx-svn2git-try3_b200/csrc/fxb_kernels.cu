@@ -529,15 +529,44 @@ void launch_vdif_unpack(const uint8_t *data, int64_t nbytes, int payload, int he
 // A zoom band's spectra are the channels [choff, choff + nchan) of its parent
 // band's (mode.cpp:169-208): one CTA per (8 FFTs, zoom row) copies them into
 // the zoom frequency's own spectra rows, FP32 [t][row][chan] (float2) or the
-// tensor-core form's blocked [t][block][row][tcb] (bf16x2 as uint32).
+// tensor-core form's blocked [t][block][row][tcb] (bf16x2 as uint32).  Each
+// thread finds its channel's block and offset once and steps them.
 constexpr int kZoomTimes = 8;
 
-__device__ __forceinline__ int64_t spec_index(const DevFreqPlan &p, int t, int row, int c)
+// Position of channel c in a spectra row: block and offset in it (blocks of
+// tcb channels; one block of nchan in the FP32 form), advanced by a constant
+// step without divisions.
+struct ChanPos {
+	int blk, off, dblk, doff, width;
+	__device__ __forceinline__ ChanPos(int c, int step, int tcb, int nchan)
+	{
+		width = tcb ? tcb : nchan;
+		blk = c / width;
+		off = c - blk * width;
+		dblk = step / width;
+		doff = step - dblk * width;
+	}
+	__device__ __forceinline__ void advance()
+	{
+		blk += dblk;
+		off += doff;
+		if(off >= width)
+		{
+			off -= width;
+			blk++;
+		}
+	}
+};
+
+// element (t, row, block 0, offset 0) and the distance between blocks
+__device__ __forceinline__ int64_t row_base(const DevFreqPlan &p, int t, int row)
 {
 	if(p.tcb == 0)
-		return p.spec_off + ((int64_t)t * p.nrow + row) * p.nchan + c;
-	return p.spec_off + (((int64_t)t * p.tnblk + c / p.tcb) * p.nrow + row) * p.tcb + c % p.tcb;
+		return p.spec_off + ((int64_t)t * p.nrow + row) * p.nchan;
+	return p.spec_off + ((int64_t)t * p.tnblk * p.nrow + row) * p.tcb;
 }
+
+__device__ __forceinline__ int64_t block_stride(const DevFreqPlan &p) { return p.tcb ? (int64_t)p.nrow * p.tcb : 0; }
 
 template <typename V>
 __global__ void __launch_bounds__(256) k_zoom_gather(const DevZoomCopy *__restrict__ zc,
@@ -546,14 +575,22 @@ __global__ void __launch_bounds__(256) k_zoom_gather(const DevZoomCopy *__restri
 {
 	const DevZoomCopy z = zc[blockIdx.y];
 	const DevFreqPlan src = plans[z.src_plan], dst = plans[z.dst_plan];
-	const int t0 = blockIdx.x * kZoomTimes;
-	const int nt = min(kZoomTimes, T - t0);
-	// zoom channel counts are powers of two
-	const int lg = __ffs(z.nchan) - 1;
-	for(int i = threadIdx.x; i < (nt << lg); i += blockDim.x)
+	const int t0 = blockIdx.x * kZoomTimes, t1 = min(T, t0 + kZoomTimes);
+	const int64_t sbs = block_stride(src), dbs = block_stride(dst);
+	const ChanPos sp0(z.choff + (int)threadIdx.x, blockDim.x, src.tcb, src.nchan);
+	const ChanPos dp0((int)threadIdx.x, blockDim.x, dst.tcb, dst.nchan);
+	const int64_t sts = row_base(src, 1, z.src_row) - row_base(src, 0, z.src_row);
+	const int64_t dts = row_base(dst, 1, z.dst_row) - row_base(dst, 0, z.dst_row);
+	int64_t sb = row_base(src, t0, z.src_row), db = row_base(dst, t0, z.dst_row);
+	for(int t = t0; t < t1; t++, sb += sts, db += dts)
 	{
-		const int t = t0 + (i >> lg), c = i & (z.nchan - 1);
-		spec[spec_index(dst, t, z.dst_row, c)] = spec[spec_index(src, t, z.src_row, z.choff + c)];
+		ChanPos sp = sp0, dp = dp0;
+		for(int c = threadIdx.x; c < z.nchan; c += blockDim.x)
+		{
+			spec[db + dp.blk * dbs + dp.off] = spec[sb + sp.blk * sbs + sp.off];
+			sp.advance();
+			dp.advance();
+		}
 	}
 }
 
