@@ -79,7 +79,7 @@ static int comb_tones(double bw, double offset, double step)
 constexpr int kMaxPcalBins = 32768;
 
 // One recorded band's tones and extractor: the comb tones of the band
-// (configuration.cpp:1813-1846) and, for the extractor PCal::getNew picks
+// (configuration.cpp:1776-1846) and, for the extractor PCal::getNew picks
 // (pcal.cpp:139-191, with Mode's 1 MHz minimum frequency resolution), the
 // bin count and tone bins of the implicit-shift extractor
 // (pcal.cpp:927-958, 1073-1086).  A band without a tone reads as one zero
@@ -88,24 +88,44 @@ static bool pcal_band(const fxb_freq &f, float interval, float base, Job::PcalBa
                       fxb_status &st)
 {
 	pb.nbins = pb.first = pb.step = 0;
-	if(f.lower_sideband)
-		return fail(err, st, FXB_ERR_UNSUPPORTED, "phase cal of lower-sideband bands");
 	const double lo = f.freq_mhz, bw = f.bw_mhz;
 	double tonefreq = (double)((int)(lo / interval)) * interval;
-	if(tonefreq <= lo)
-		tonefreq += interval;
 	int n = 0;
-	if(tonefreq <= lo + bw)
-		while(tonefreq + (float)(n * interval) <= lo + bw)
-			n++;
+	if(f.lower_sideband)
+	{
+		// tones below the LO, counted downwards; the extraction is the same, the
+		// tones lying at the same baseband offsets (configuration.cpp:1776-1811)
+		if(tonefreq == lo)
+			tonefreq -= interval;
+		if(tonefreq >= lo - bw)
+			while(tonefreq - (float)(n * interval) >= lo - bw)
+				n++;
+	}
+	else
+	{
+		if(tonefreq <= lo)
+			tonefreq += interval;
+		if(tonefreq <= lo + bw)
+			while(tonefreq + (float)(n * interval) <= lo + bw)
+				n++;
+	}
 	if(n == 0)
 	{
 		pb.ntones = 1;
 		return true;
 	}
 	pb.ntones = n;
-	const double tone0 = 1e6 * tonefreq + 0 * 1e6 * interval + 1e6 * base;
-	const int off = (int)(long)(tone0 - 1e6 * lo + 0.5);
+	int off;
+	if(f.lower_sideband)
+	{
+		const double tone0 = 1e6 * tonefreq - 0 * 1e6 * interval - 1e6 * base;
+		off = (int)(long)(1e6 * lo - tone0 + 0.5);
+	}
+	else
+	{
+		const double tone0 = 1e6 * tonefreq + 0 * 1e6 * interval + 1e6 * base;
+		off = (int)(long)(tone0 - 1e6 * lo + 0.5);
+	}
 	const double fs = 2.0 * 1e6 * bw, sp = 1e6 * interval;
 	int nbins = (int)(fs / gcd_rounded(fs, (double)off));
 	const int nspacing = (int)(fs / gcd_rounded(fs, sp));

@@ -170,8 +170,8 @@ static int calc_num_tones(double bw, double offset, double step)
 	return n;
 }
 
-/* Tones of one recorded band and its extractor (configuration.cpp:1813-1846
- * for the upper sideband, PCal::getNew pcal.cpp:139-191 with the minimum
+/* Tones of one recorded band and its extractor (configuration.cpp:1776-1846,
+ * lower and upper sideband, PCal::getNew pcal.cpp:139-191 with the minimum
  * frequency resolution of 1 MHz set by Mode, PCalExtractorImplicitShift
  * pcal.cpp:927-958, 1073-1086).  nbins 0: the band has no tone and reads as
  * one zero tone (the dummy extractor); nbins -1: an extractor this oracle
@@ -185,19 +185,20 @@ static void pcal_plan(const fxb_freq *f, double interval_d, double base_d, int *
 	int n = 0, off;
 	*nbins = -1;
 	*first = *step = 0;
+	tonefreq = (double)((int)(lo / interval)) * interval;
 	if(f->lower_sideband)
 	{
-		tonefreq = (double)((int)(lo / interval)) * interval;
+		/* tones below the LO, counted downwards (configuration.cpp:1776-1811) */
 		if(tonefreq == lo) tonefreq -= interval;
 		if(tonefreq >= lo - bw)
 			while(tonefreq - (float)(n * interval) >= lo - bw) n++;
-		*ntones = n > 0 ? n : 1;
-		return;
 	}
-	tonefreq = (double)((int)(lo / interval)) * interval;
-	if(tonefreq <= lo) tonefreq += interval;
-	if(tonefreq <= lo + bw)
-		while(tonefreq + (float)(n * interval) <= lo + bw) n++;
+	else
+	{
+		if(tonefreq <= lo) tonefreq += interval;
+		if(tonefreq <= lo + bw)
+			while(tonefreq + (float)(n * interval) <= lo + bw) n++;
+	}
 	if(n == 0)
 	{
 		*ntones = 1;
@@ -205,7 +206,10 @@ static void pcal_plan(const fxb_freq *f, double interval_d, double base_d, int *
 		return;
 	}
 	*ntones = n;
-	off = (int)(long)(1e6 * tonefreq + 0 * 1e6 * interval + 1e6 * base - 1e6 * lo + 0.5);
+	if(f->lower_sideband)
+		off = (int)(long)(1e6 * lo - (1e6 * tonefreq - 0 * 1e6 * interval - 1e6 * base) + 0.5);
+	else
+		off = (int)(long)(1e6 * tonefreq + 0 * 1e6 * interval + 1e6 * base - 1e6 * lo + 0.5);
 	{
 		const double fs = 2.0 * 1e6 * bw, sp = 1e6 * interval;
 		int No, Np, Nt;

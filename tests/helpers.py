@@ -122,4 +122,7 @@ PCAL_JOBS = {
     # first tone 31.25 kHz above the LO: 1024 bins, fewer than the 4096
     # samples of a window
     "pcal_1024_bins": lambda: pcal_job(nstation=2, nchan=2048, freq0=8400.96875, subint_ns=4_096_000),
+    # lower-sideband bands, LO on the comb and 10 kHz off it
+    "pcal_lsb": lambda: pcal_job(nstation=2, nfreq=2, full_pol=True, lsb=True, subint_ns=2_048_000),
+    "pcal_lsb_frac": lambda: pcal_job(nstation=2, lsb=True, freq0=8400.01),
 }

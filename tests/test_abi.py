@@ -77,7 +77,7 @@ def test_zoom_rejections():
 
 
 @pytest.mark.parametrize("name", ["pcal_int_lo", "pcal_frac_lo", "pcal_8bit", "pcal_no_tone", "pcal_5mhz",
-                                  "pcal_1024_bins"])
+                                  "pcal_1024_bins", "pcal_lsb", "pcal_lsb_frac"])
 def test_pcal_layout_matches_oracle(name):
     from helpers import PCAL_JOBS
     job = PCAL_JOBS[name]()
@@ -94,7 +94,9 @@ def test_pcal_rejections():
     job = pcal_job(5.0, nstation=2, freq0=8416.0)
     with pytest.raises(native.FxbError, match="UNSUPPORTED"):
         native.job_layout(job)
-    job = pcal_job(1.0, nstation=2, lsb=True)
+    # a phase-cal base that puts the first tone on the LO needs the trivial
+    # extractor, whose tone count then differs from the configuration's
+    job = pcal_job(1.0, base=-1.0, nstation=2)
     with pytest.raises(native.FxbError, match="UNSUPPORTED"):
         native.job_layout(job)
 
