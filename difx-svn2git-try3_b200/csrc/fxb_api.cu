@@ -98,7 +98,7 @@ struct fxb_ctx {
 	DevPcalBand *d_pbands = nullptr;
 	int npbands = 0;
 	int pchunks = 1;                     // chunks of FFTs, each with its own slice of the bins
-	struct PcalClass { int first, count, nbits, bpt, maxbins; size_t smem; };
+	struct PcalClass { int first, count, nbits, bpt, shift, maxbins; size_t smem; };
 	std::vector<PcalClass> pclass;       // runs of groups of one sample layout: one launch each
 	size_t psmem = 0;
 	double *d_pbins = nullptr;           // [pchunks][job.pcal_bins]
@@ -239,7 +239,7 @@ static std::vector<DevPcalGroup> pcal_groups(const Job &job)
 			continue;
 		DevPcalGroup *g = nullptr;
 		for(DevPcalGroup &c : out)
-			if(c.station == p.station && c.nbins == p.nbins && c.nb < kPcalGroupBands)
+			if(c.station == p.station && c.nbins == p.nbins && c.shift == p.shift && c.nb < kPcalGroupBands)
 			{
 				DevPcalGroup t = c;
 				t.nb++;
@@ -253,6 +253,8 @@ static std::vector<DevPcalGroup> pcal_groups(const Job &job)
 			memset(g, 0, sizeof(*g));
 			g->station = p.station;
 			g->nbins = p.nbins;
+			g->shift = p.shift;
+			g->fs = p.fs;
 		}
 		g->band[g->nb] = p.band;
 		g->bin_off[g->nb] = p.bin_off;
@@ -673,11 +675,11 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		{
 			std::vector<DevPcalBand> hb;
 			for(const Job::PcalBand &p : job.pcal)
-				hb.push_back(DevPcalBand{p.ntones, p.nbins, p.first, p.step, p.bin_off, p.core});
+				hb.push_back(DevPcalBand{p.ntones, p.nbins, p.first, p.step, p.shift, 0, p.bin_off, p.core});
 			ctx->h_pgroups = pcal_groups(job);
 			auto class_of = [&](const DevPcalGroup &g) {
 				const Job::Station &js = job.stations[g.station];
-				return std::make_pair(js.nbits, js.nbits * js.nband);
+				return std::make_tuple(js.nbits, js.nbits * js.nband, g.shift != 0);
 			};
 			std::stable_sort(ctx->h_pgroups.begin(), ctx->h_pgroups.end(),
 			                 [&](const DevPcalGroup &x, const DevPcalGroup &y) { return class_of(x) < class_of(y); });
@@ -691,8 +693,9 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			{
 				const DevPcalGroup &g = ctx->h_pgroups[i];
 				const auto c = class_of(g);
-				if(ctx->pclass.empty() || ctx->pclass.back().nbits != c.first || ctx->pclass.back().bpt != c.second)
-					ctx->pclass.push_back({(int)i, 0, c.first, c.second, 0, 0});
+				if(ctx->pclass.empty() || ctx->pclass.back().nbits != std::get<0>(c) ||
+				   ctx->pclass.back().bpt != std::get<1>(c) || ctx->pclass.back().shift != (int)std::get<2>(c))
+					ctx->pclass.push_back({(int)i, 0, std::get<0>(c), std::get<1>(c), (int)std::get<2>(c), 0, 0});
 				fxb_ctx::PcalClass &pc = ctx->pclass.back();
 				pc.count++;
 				pc.maxbins = std::max(pc.maxbins, g.nbins);
@@ -1027,9 +1030,9 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 			cudaEventRecord(tn.ev[nk], st);
 	}
 	for(const auto &pc : ctx->pclass)
-		launch_pcal_bin(ctx->d_pgroups + pc.first, pc.count, pc.maxbins, ctx->pchunks, pc.nbits, pc.bpt, pc.smem,
-		                ctx->d_st, sl.d_sub, ctx->d_params, ctx->d_valid, ctx->valid_stride, ctx->T, job.pcal_bins,
-		                ctx->d_pbins, st);
+		launch_pcal_bin(ctx->d_pgroups + pc.first, pc.count, pc.maxbins, ctx->pchunks, pc.nbits, pc.bpt, pc.shift != 0,
+		                pc.smem, ctx->d_st, sl.d_sub, ctx->d_params, ctx->d_valid, ctx->valid_stride, ctx->T,
+		                job.pcal_bins, ctx->d_pbins, st);
 	launch_zoom_gather(ctx->d_zoom, ctx->nzoom, ctx->d_plans, ctx->T, ctx->tc,
 	                   ctx->tc ? ctx->d_specn : (void *)ctx->d_spec, st);
 	cudaEventRecordWithFlags(sl.tev[2], st, evf);

@@ -151,8 +151,10 @@ struct Job {
 	// tone), the DFT bin of the first tone and the bin step between tones
 	struct PcalBand {
 		int station, band, ntones, nbins, first, step;
+		int shift;          // shifting extractor: samples rotated by this offset (Hz) into complex bins; else 0
+		int64_t fs;         // samples per second
 		int64_t core;       // core-result offset (complex) of the band's first tone
-		int64_t bin_off;    // offset of the band's bins in the bin accumulator
+		int64_t bin_off;    // offset (doubles) of the band's bins in the bin accumulator (complex bins: 2 per bin)
 	};
 	std::vector<PcalBand> pcal;
 	int64_t pcal_bins = 0;

@@ -82,12 +82,13 @@ constexpr int kMaxPcalBins = 32768;
 // (configuration.cpp:1776-1846) and, for the extractor PCal::getNew picks
 // (pcal.cpp:139-191, with Mode's 1 MHz minimum frequency resolution), the
 // bin count and tone bins of the implicit-shift extractor
-// (pcal.cpp:927-958, 1073-1086).  A band without a tone reads as one zero
+// (pcal.cpp:927-958, 1073-1086) or of the shifting one (pcal.cpp:494-705).  A band without a tone reads as one zero
 // tone (the dummy extractor).
 static bool pcal_band(const fxb_freq &f, float interval, float base, Job::PcalBand &pb, std::string &err,
                       fxb_status &st)
 {
-	pb.nbins = pb.first = pb.step = 0;
+	pb.nbins = pb.first = pb.step = pb.shift = 0;
+	pb.fs = (int64_t)(2e6 * f.bw_mhz + 0.5);
 	const double lo = f.freq_mhz, bw = f.bw_mhz;
 	double tonefreq = (double)((int)(lo / interval)) * interval;
 	int n = 0;
@@ -134,10 +135,27 @@ static bool pcal_band(const fxb_freq &f, float interval, float base, Job::PcalBa
 		nbins *= 2;
 	if(nt == 0)
 		return true;
-	if(off == 0 || nbins % nspacing != 0)
-		return fail(err, st, FXB_ERR_UNSUPPORTED, "phase-cal comb needs the trivial or the shifting extractor");
+	if(off == 0)
+		return fail(err, st, FXB_ERR_UNSUPPORTED, "phase-cal comb needs the trivial extractor");
 	if(nt != n)
 		return fail(err, st, FXB_ERR_UNSUPPORTED, "phase-cal tone count differs between extractor and configuration");
+	if(nbins % nspacing != 0)
+	{
+		// the shifting extractor (pcal.cpp:494-705): samples rotated by the
+		// offset, folded into fs / gcd(fs, spacing) bins, tones at multiples of
+		// the step from bin 0
+		const int N = (int)(fs / gcd_rounded(fs, sp));
+		const int stp = (int)std::floor(N * (sp / fs));
+		if((int64_t)(nt - 1) * stp >= N)
+			return fail(err, st, FXB_ERR_UNSUPPORTED, "phase-cal tones beyond the shifting extractor's bins");
+		if(N > kMaxPcalBins)
+			return fail(err, st, FXB_ERR_UNSUPPORTED, "phase-cal comb repeats after too many samples");
+		pb.nbins = N;
+		pb.step = stp;
+		pb.first = 0;
+		pb.shift = off;
+		return true;
+	}
 	if(nbins > kMaxPcalBins)
 		return fail(err, st, FXB_ERR_UNSUPPORTED, "phase-cal offset repeats after too many samples");
 	pb.nbins = nbins;
@@ -433,7 +451,7 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 				return false;
 			pb.core = idx;
 			pb.bin_off = job.pcal_bins;
-			job.pcal_bins += pb.nbins;
+			job.pcal_bins += (pb.shift ? 2 : 1) * (int64_t)pb.nbins;
 			idx += pb.ntones;
 			job.pcal.push_back(pb);
 		}

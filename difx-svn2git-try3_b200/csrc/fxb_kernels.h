@@ -156,12 +156,14 @@ void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, 
 // bands of one station with the same bin count; a band is one band's tones.
 constexpr int kPcalGroupBands = 16;
 struct DevPcalGroup {
-	int32_t station, nb, nbins, pad;
+	int32_t station, nb, nbins, shift;  // shift: the shifting extractor's offset (Hz), complex bins; else 0
+	int64_t fs;                         // samples per second
 	int32_t band[kPcalGroupBands];
-	int64_t bin_off[kPcalGroupBands];   // first bin of each band in the bin accumulator
+	int64_t bin_off[kPcalGroupBands];   // first bin (double) of each band in the bin accumulator
 };
 struct DevPcalBand {
 	int32_t ntones, nbins, first, step;
+	int32_t shift, pad;                 // complex bins when shift != 0
 	int64_t bin_off, core;
 };
 // shared memory of a group's lane sums (bin counts below the CTA width) and
@@ -173,9 +175,10 @@ constexpr size_t kPcalSmemMax = 96 * 1024;    // lane sums of one group at most
 cudaError_t pcal_init(size_t smem);
 // folds the subint's samples into the FP64 bins: the FFTs are split into
 // nchunk chunks, chunk c adds to bins + c * chunk_stride.  Every group of one
-// launch belongs to stations of nbits-bit samples with bpt bits per time;
-// maxbins is the launch's largest bin count, smem its pcal_smem.
-void launch_pcal_bin(const DevPcalGroup *groups, int ngroups, int maxbins, int nchunk, int nbits, int bpt,
+// launch belongs to stations of nbits-bit samples with bpt bits per time and
+// to one extractor (shift: the shifting extractor's complex bins); maxbins is
+// the launch's largest bin count, smem its pcal_smem.
+void launch_pcal_bin(const DevPcalGroup *groups, int ngroups, int maxbins, int nchunk, int nbits, int bpt, bool shift,
                      size_t smem, const DevStation *st, const DevSubintStation *sub, const FftParam *params,
                      const uint8_t *valid, int64_t valid_stride, int T, int64_t chunk_stride, double *bins,
                      cudaStream_t stream);

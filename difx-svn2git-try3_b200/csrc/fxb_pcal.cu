@@ -1,9 +1,11 @@
-// Phase-cal extraction (mode.cpp:773-787, pcal.cpp:927-1105, core.cpp:1124-1150).
+// Phase-cal extraction (mode.cpp:773-787, pcal.cpp:494-705, 927-1105,
+// core.cpp:1124-1150).
 //
 // The reference's implicit-shift extractor adds every unpacked sample of
 // every valid FFT window into bin (sample number in the data second) mod N
 // and, at the end of the subint, takes a length-N DFT whose bins at the tone
-// frequencies are the tones.  The DFT is linear, so the device keeps the bins
+// frequencies are the tones; the shifting extractor first rotates each sample
+// by exp(-2 pi i offset a / fs) and folds into complex bins.  The DFT is linear, so the device keeps the bins
 // summed over every subint of the integration (FP64, one slice per chunk of
 // FFTs) and takes the DFT once, when the core result is read.
 //
@@ -28,16 +30,20 @@ constexpr int kThreads = 256;
 
 // Per-thread sums of one bin over samples: SWAR lane counters (2-bit, 16
 // bands to a word) or per-band float sums.
-template <int NBITS, bool ONEWORD, bool SWAR>
+template <int NBITS, bool ONEWORD, bool SWAR, bool SHIFT>
 struct BinSum {
 	uint32_t le = 0, lo = 0, he = 0, ho = 0;
 	int nv = 0;
 	float acc[kPcalGroupBands];
+	float acci[SHIFT ? kPcalGroupBands : 1];   // imaginary parts (shifting extractor)
 	__device__ __forceinline__ BinSum()
 	{
 #pragma unroll
 		for(int j = 0; j < kPcalGroupBands; j++)
 			acc[j] = 0.0f;
+#pragma unroll
+		for(int j = 0; j < (SHIFT ? kPcalGroupBands : 1); j++)
+			acci[j] = 0.0f;
 	}
 	__device__ __forceinline__ void flush(const uint32_t (&boff)[kPcalGroupBands], int nb)
 	{
@@ -53,9 +59,11 @@ struct BinSum {
 		le = lo = he = ho = 0u;
 		nv = 0;
 	}
-	// one sample: its word (ONEWORD) or frame words, and the bit of its time
+	// one sample: its word (ONEWORD) or frame words, the bit of its time and
+	// (SHIFT) the rotator exp(-2 pi i offset a / fs) of its sample number a
 	__device__ __forceinline__ void add(uint32_t word, const uint32_t *wp, uint32_t tbit,
-	                                    const uint32_t (&boff)[kPcalGroupBands], int nb, const float *lut)
+	                                    const uint32_t (&boff)[kPcalGroupBands], int nb, const float *lut, float rc = 1.0f,
+	                                    float rs = 0.0f)
 	{
 		if(SWAR)
 		{
@@ -74,7 +82,14 @@ struct BinSum {
 				{
 					const uint32_t bit = tbit + boff[j];
 					const uint32_t wd = ONEWORD ? word : __ldg(wp + (bit >> 5));
-					acc[j] += lut[(wd >> (bit & 31u)) & ((1u << NBITS) - 1u)];
+					const float v = lut[(wd >> (bit & 31u)) & ((1u << NBITS) - 1u)];
+					if(SHIFT)
+					{
+						acc[j] += v * rc;
+						acci[SHIFT ? j : 0] += v * rs;
+					}
+					else
+						acc[j] += v;
 				}
 		}
 	}
@@ -88,7 +103,7 @@ struct BinSum {
 // spread the bins over CTAs.  The CTA adds its sums, without atomics, into
 // its chunk's slice of the FP64 bins.  The samples of eight windows are loaded
 // before any is used.
-template <int NBITS, bool ONEWORD, bool SWAR>
+template <int NBITS, bool ONEWORD, bool SWAR, bool SHIFT>
 __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__restrict__ groups,
                                                       const DevStation *__restrict__ st,
                                                       const DevSubintStation *__restrict__ sub,
@@ -96,7 +111,8 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
                                                       const uint8_t *__restrict__ valid, int64_t valid_stride, int T,
                                                       int tpc, int64_t chunk_stride, double *__restrict__ bins)
 {
-	extern __shared__ int4 ftab[];             // per FFT of the chunk: residue of its first sample, first frame, offset, blanking
+	extern __shared__ int4 ftab[];             // per FFT of the chunk: residue of its first sample, first frame, offset, blanking;
+	                                           // then the rotator phase of its first sample (SHIFT), then lane sums
 	__shared__ float lut[1 << NBITS];
 	const DevPcalGroup &g = groups[blockIdx.y];
 	const int s = g.station, nb = g.nb, N = g.nbins;
@@ -112,6 +128,8 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
 		return;
 	const int t0 = chunk * tpc, t1 = min(T, t0 + tpc);
 	const int64_t datasamples = (int)(sub[s].datans / (S.sampletime * 1e3) + 0.5);   // Mode::setData
+	int32_t *fph = reinterpret_cast<int32_t *>(ftab + tpc);   // (offset x first sample) mod fs
+	const int64_t fsi = g.fs, off = g.shift;
 	for(int t = t0 + tid; t < t1; t += kThreads)
 	{
 		const FftParam &p = params[(int64_t)s * T + t];
@@ -123,6 +141,8 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
 			e.y = (int)(g0 / fs);
 			e.z = (int)(g0 - (uint32_t)e.y * fs);
 			e.w = p.stuck;
+			if(SHIFT)
+				fph[t - t0] = (int32_t)((off * ((datasamples + p.nearest) % fsi)) % fsi);
 		}
 		ftab[t - t0] = e;
 	}
@@ -138,7 +158,9 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
 #pragma unroll
 	for(int j = 0; j < kPcalGroupBands; j++)
 		boff[j] = j < nb ? (uint32_t)g.band[j] * NBITS : 0u;
-	BinSum<NBITS, ONEWORD, SWAR> sum;
+	BinSum<NBITS, ONEWORD, SWAR, SHIFT> sum;
+	// rotator phase step between a bin's samples of one window (N apart)
+	const int64_t dph = SHIFT ? (off * N) % fsi : 0;
 	if(active)
 	{
 		const uint8_t *buf = sub[s].buf;
@@ -149,12 +171,14 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
 		// the next sample of bin m: window t (relative to t0), sample n of it
 		// (n = L: not yet found in window t)
 		int t = q, n = L;
+		int64_t ph = 0;                        // rotator phase (x fs) of sample n of window t
 		constexpr int K = 8;
 		while(true)
 		{
 			uint32_t word[K], tbit[K];
 			const uint32_t *wp[K];
 			bool ok[K];
+			int32_t phk[SHIFT ? K : 1];
 #pragma unroll
 			for(int k = 0; k < K; k++)
 			{
@@ -175,10 +199,14 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
 						t += Q;
 						n = L;
 					}
+					else if(SHIFT)
+						ph = (fph[t] + (off * n) % fsi) % fsi;
 				}
 				if(t < nt)
 				{
 					const int4 e = ftab[t];
+					if(SHIFT)
+						phk[SHIFT ? k : 0] = (int32_t)ph;
 					uint32_t x = (uint32_t)e.z + (uint32_t)n, kf = 0;
 					while(x >= fs)
 					{
@@ -192,6 +220,12 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
 					if(ok[k] && ONEWORD)
 						word[k] = __ldg(wp[k] + (tbit[k] >> 5));
 					n += N;
+					if(SHIFT)
+					{
+						ph += dph;
+						if(ph >= fsi)
+							ph -= fsi;
+					}
 					if(n >= L)
 					{
 						t += Q;
@@ -202,7 +236,12 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
 #pragma unroll
 			for(int k = 0; k < K; k++)
 				if(ok[k])
-					sum.add(word[k], wp[k], tbit[k], boff, nb, lut);
+				{
+					float rs = 0.0f, rc = 1.0f;
+					if(SHIFT)
+						sincospif(-2.0f * ((float)phk[SHIFT ? k : 0] / (float)fsi), &rs, &rc);
+					sum.add(word[k], wp[k], tbit[k], boff, nb, lut, rc, rs);
+				}
 			if(t >= nt)
 				break;
 		}
@@ -210,30 +249,45 @@ __global__ void __launch_bounds__(kThreads) k_pcal_bin(const DevPcalGroup *__res
 			sum.flush(boff, nb);
 	}
 	double *dst = bins + (int64_t)chunk * chunk_stride;
+	constexpr int C = SHIFT ? 2 : 1;          // doubles per bin
 	if(Q == 1)
 	{
 		if(active)
 #pragma unroll
 			for(int j = 0; j < kPcalGroupBands; j++)
 				if(j < nb)
-					dst[g.bin_off[j] + m] += (double)sum.acc[j];
+				{
+					dst[g.bin_off[j] + C * m] += (double)sum.acc[j];
+					if(SHIFT)
+						dst[g.bin_off[j] + C * m + 1] += (double)sum.acci[SHIFT ? j : 0];
+				}
 		return;
 	}
 	// lanes of a bin, added in lane order
-	float *part = reinterpret_cast<float *>(ftab + tpc);    // [Q][nb][N]
+	float *part = reinterpret_cast<float *>(fph + tpc);    // [Q][nb][N][C]
 	if(active)
 #pragma unroll
 		for(int j = 0; j < kPcalGroupBands; j++)
 			if(j < nb)
-				part[(q * nb + j) * N + m] = sum.acc[j];
+			{
+				part[((q * nb + j) * N + m) * C] = sum.acc[j];
+				if(SHIFT)
+					part[((q * nb + j) * N + m) * C + 1] = sum.acci[SHIFT ? j : 0];
+			}
 	__syncthreads();
 	for(int i = tid; i < nb * N; i += kThreads)
 	{
 		const int j = i / N, mm = i - j * N;
-		float v = 0.0f;
+		float v = 0.0f, vi = 0.0f;
 		for(int q2 = 0; q2 < Q; q2++)
-			v += part[(q2 * nb + j) * N + mm];
-		dst[g.bin_off[j] + mm] += (double)v;
+		{
+			v += part[((q2 * nb + j) * N + mm) * C];
+			if(SHIFT)
+				vi += part[((q2 * nb + j) * N + mm) * C + 1];
+		}
+		dst[g.bin_off[j] + C * mm] += (double)v;
+		if(SHIFT)
+			dst[g.bin_off[j] + C * mm + 1] += (double)vi;
 	}
 }
 
@@ -254,11 +308,19 @@ __global__ void __launch_bounds__(kThreads) k_pcal_final(const DevPcalBand *__re
 				// X[idx] = sum_m Z[m] exp(-2 pi i idx m / N), the angle reduced exactly
 				double sn, cs;
 				sincospi(-2.0 * (double)((idx * m) % N) / (double)N, &sn, &cs);
-				double z = 0.0;
+				double z = 0.0, zi = 0.0;
 				for(int c = 0; c < nchunk; c++)          // the chunks' bins, in chunk order
-					z += bins[c * chunk_stride + b.bin_off + m];
-				re += z * cs;
-				im += z * sn;
+				{
+					if(b.shift)
+					{
+						z += bins[c * chunk_stride + b.bin_off + 2 * m];
+						zi += bins[c * chunk_stride + b.bin_off + 2 * m + 1];
+					}
+					else
+						z += bins[c * chunk_stride + b.bin_off + m];
+				}
+				re += z * cs - zi * sn;
+				im += z * sn + zi * cs;
 			}
 		for(int o = 16; o > 0; o >>= 1)
 		{
@@ -289,38 +351,45 @@ __global__ void __launch_bounds__(kThreads) k_pcal_final(const DevPcalBand *__re
 
 size_t pcal_group_smem(const DevPcalGroup &g)
 {
-	// the lanes' partial sums of a bin count below the CTA width
-	return g.nbins < kThreads ? (size_t)g.nb * g.nbins * (kThreads / g.nbins) * sizeof(float) : 0;
+	// the lanes' partial sums of a bin count below the CTA width (complex for
+	// the shifting extractor)
+	return g.nbins < kThreads ? (size_t)g.nb * g.nbins * (kThreads / g.nbins) * sizeof(float) * (g.shift ? 2 : 1) : 0;
 }
 
-size_t pcal_smem(size_t group_smem, int tpc) { return sizeof(int4) * (size_t)tpc + group_smem; }
+size_t pcal_smem(size_t group_smem, int tpc) { return (sizeof(int4) + sizeof(int32_t)) * (size_t)tpc + group_smem; }
 
-void launch_pcal_bin(const DevPcalGroup *groups, int ngroups, int maxbins, int nchunk, int nbits, int bpt,
+void launch_pcal_bin(const DevPcalGroup *groups, int ngroups, int maxbins, int nchunk, int nbits, int bpt, bool shift,
                      size_t smem, const DevStation *st, const DevSubintStation *sub, const FftParam *params,
                      const uint8_t *valid, int64_t valid_stride, int T, int64_t chunk_stride, double *bins,
                      cudaStream_t stream)
 {
 	if(ngroups <= 0)
 		return;
-	const bool swar = nbits == 2 && bpt == 32, one = bpt <= 32;
+	const bool swar = nbits == 2 && bpt == 32 && !shift, one = bpt <= 32;
 	const int tpc = (T + nchunk - 1) / nchunk;
 	const int nbb = (maxbins + kThreads - 1) / kThreads;
 	const dim3 grid(nbb * ((T + tpc - 1) / tpc), ngroups);
-#define FXB_BIN(B, O, W) k_pcal_bin<B, O, W><<<grid, kThreads, smem, stream>>>(groups, st, sub, params, valid, \
-	                                                                      valid_stride, T, tpc, chunk_stride, bins)
-	if(swar) FXB_BIN(2, true, true);
-	else if(nbits == 2 && one) FXB_BIN(2, true, false);
-	else if(nbits == 2) FXB_BIN(2, false, false);
-	else if(one) FXB_BIN(8, true, false);
-	else FXB_BIN(8, false, false);
+#define FXB_BIN(B, O, W, S) k_pcal_bin<B, O, W, S><<<grid, kThreads, smem, stream>>>(groups, st, sub, params, valid, \
+	                                                                            valid_stride, T, tpc, chunk_stride, bins)
+	if(swar) FXB_BIN(2, true, true, false);
+	else if(!shift && nbits == 2 && one) FXB_BIN(2, true, false, false);
+	else if(!shift && nbits == 2) FXB_BIN(2, false, false, false);
+	else if(!shift && one) FXB_BIN(8, true, false, false);
+	else if(!shift) FXB_BIN(8, false, false, false);
+	else if(nbits == 2 && one) FXB_BIN(2, true, false, true);
+	else if(nbits == 2) FXB_BIN(2, false, false, true);
+	else if(one) FXB_BIN(8, true, false, true);
+	else FXB_BIN(8, false, false, true);
 #undef FXB_BIN
 }
 
 cudaError_t pcal_init(size_t smem)
 {
-	const void *k[] = {(const void *)k_pcal_bin<2, true, true>, (const void *)k_pcal_bin<2, true, false>,
-	                   (const void *)k_pcal_bin<2, false, false>, (const void *)k_pcal_bin<8, true, false>,
-	                   (const void *)k_pcal_bin<8, false, false>};
+	const void *k[] = {(const void *)k_pcal_bin<2, true, true, false>, (const void *)k_pcal_bin<2, true, false, false>,
+	                   (const void *)k_pcal_bin<2, false, false, false>, (const void *)k_pcal_bin<8, true, false, false>,
+	                   (const void *)k_pcal_bin<8, false, false, false>, (const void *)k_pcal_bin<2, true, false, true>,
+	                   (const void *)k_pcal_bin<2, false, false, true>, (const void *)k_pcal_bin<8, true, false, true>,
+	                   (const void *)k_pcal_bin<8, false, false, true>};
 	for(const void *f : k)
 	{
 		const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

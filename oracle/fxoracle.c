@@ -26,8 +26,9 @@
  *                              1068-1086, 1266-1363)
  *   - phase cal                tones per recorded band (configuration.cpp:
  *                              1771-1846), the extractor choice (pcal.cpp:
- *                              139-191) and the implicit-shift extractor
- *                              (pcal.cpp:927-1105), fed from Mode::process
+ *                              139-191), the implicit-shift and shifting
+ *                              extractors (pcal.cpp:927-1105, 494-705), fed
+ *                              from Mode::process
  *                              (mode.cpp:773-787), copied band by band
  *                              (core.cpp:1124-1150)
  *   - zoom bands               parent and channel offset
@@ -79,6 +80,7 @@ typedef struct fxo_job {
 	 * extractor's zeros), first tone bin and bin step */
 	double *pcal_interval, *pcal_base;
 	int **pc_ntones, **pc_nbins, **pc_first, **pc_step;
+	int **pc_shift;       /* shifting extractor: the rotation's offset (Hz), else 0 */
 	int64_t *pcoff;       /* core-result offset of each station's tones, or -1 */
 	oracle_poly *poly;
 	/* baselines: products grouped per freq in given order */
@@ -177,14 +179,14 @@ static int calc_num_tones(double bw, double offset, double step)
  * one zero tone (the dummy extractor); nbins -1: an extractor this oracle
  * does not restate (lower sideband, trivial or shifting extractor). */
 static void pcal_plan(const fxb_freq *f, double interval_d, double base_d, int *ntones, int *nbins, int *first,
-                      int *step)
+                      int *step, int *shift)
 {
 	const float interval = (float)interval_d, base = (float)base_d;
 	const double lo = f->freq_mhz, bw = f->bw_mhz;
 	double tonefreq;
 	int n = 0, off;
 	*nbins = -1;
-	*first = *step = 0;
+	*first = *step = *shift = 0;
 	tonefreq = (double)((int)(lo / interval)) * interval;
 	if(f->lower_sideband)
 	{
@@ -218,7 +220,21 @@ static void pcal_plan(const fxb_freq *f, double interval_d, double base_d, int *
 		Nt = calc_num_tones(1e6 * bw, (double)off, sp);
 		while(fs / (2 * No) > 1e6) No *= 2;
 		if(Nt == 0) { *nbins = 0; return; }
-		if(off == 0 || (No % Np) != 0 || Nt != n) return;   /* not restated */
+		if(off == 0 || Nt != n) return;   /* not restated */
+		if((No % Np) != 0)
+		{
+			/* PCalExtractorShifting (pcal.cpp:494-705): rotate by the offset,
+			 * fold into fs / gcd(fs, spacing) bins, tones at multiples of the
+			 * step from bin 0 (every tone inside the bins) */
+			int N = (int)(fs / dgcd(fs, sp));
+			int st = (int)floor(N * (sp / fs));
+			if((long long)(Nt - 1) * st >= N) return;
+			*nbins = N;
+			*step = st;
+			*first = 0;
+			*shift = off;
+			return;
+		}
 		*nbins = No;
 		*step = (int)floor((double)No * (sp / fs));
 		*first = (int)floor((double)No * ((double)off / fs));
@@ -411,6 +427,7 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 	j->pc_nbins = (int **)calloc(d->nstation, sizeof(int *));
 	j->pc_first = (int **)calloc(d->nstation, sizeof(int *));
 	j->pc_step = (int **)calloc(d->nstation, sizeof(int *));
+	j->pc_shift = (int **)calloc(d->nstation, sizeof(int *));
 	for(s = 0; s < d->nstation; s++)
 	{
 		const fxb_station *st = &d->stations[s];
@@ -421,11 +438,12 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 		j->pc_nbins[s] = (int *)calloc(st->nband, sizeof(int));
 		j->pc_first[s] = (int *)calloc(st->nband, sizeof(int));
 		j->pc_step[s] = (int *)calloc(st->nband, sizeof(int));
+		j->pc_shift[s] = (int *)calloc(st->nband, sizeof(int));
 		if(!(st->pcal_interval_mhz > 0))
 			continue;
 		for(k = 0; k < st->nband; k++)
 			pcal_plan(&d->freqs[st->band_freq[k]], st->pcal_interval_mhz, st->pcal_base_mhz, &j->pc_ntones[s][k],
-			          &j->pc_nbins[s][k], &j->pc_first[s][k], &j->pc_step[s][k]);
+			          &j->pc_nbins[s][k], &j->pc_first[s][k], &j->pc_step[s][k], &j->pc_shift[s][k]);
 	}
 	j->ds1 = (int *)calloc(d->nbaseline, sizeof(int));
 	j->ds2 = (int *)calloc(d->nbaseline, sizeof(int));
@@ -593,6 +611,7 @@ void fxo_destroy(fxo_job *j)
 		free(j->pc_nbins[i]);
 		free(j->pc_first[i]);
 		free(j->pc_step[i]);
+		free(j->pc_shift[i]);
 		free(j->poly[i].coeffs);
 	}
 	for(i = 0; i < j->nbaseline; i++)
@@ -605,7 +624,7 @@ void fxo_destroy(fxo_job *j)
 	free(j->band_freq); free(j->band_pol); free(j->poly);
 	free(j->nzoom); free(j->zoom_freq); free(j->zoom_parent); free(j->zoom_choff);
 	free(j->pcal_interval); free(j->pcal_base); free(j->pc_ntones); free(j->pc_nbins); free(j->pc_first);
-	free(j->pc_step); free(j->pcoff);
+	free(j->pc_step); free(j->pc_shift); free(j->pcoff);
 	free(j->ds1); free(j->ds2); free(j->nprod); free(j->prod_freq); free(j->prod_b1); free(j->prod_b2);
 	free(j->freqused); free(j->equivused); free(j->bloff); free(j->bwoff); free(j->acoff); free(j->acwoff);
 	free(j);
@@ -881,7 +900,7 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 		{
 			pbins[s] = (double **)calloc(j->nband[s], sizeof(double *));
 			for(b = 0; b < j->nband[s]; b++)
-				pbins[s][b] = (double *)calloc(j->pc_nbins[s][b] > 0 ? j->pc_nbins[s][b] : 1, sizeof(double));
+				pbins[s][b] = (double *)calloc(2 * (j->pc_nbins[s][b] > 0 ? j->pc_nbins[s][b] : 1), sizeof(double));
 		}
 		if(2 * nchan + 8 > maxn) maxn = 2 * nchan + 8;
 		if(j->nband[s] > maxnb) maxnb = j->nband[s];
@@ -927,11 +946,23 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 				long long a0 = (long long)(int)(datans[s] / (sampletime * 1e3) + 0.5) + fi.nearestsample;
 				for(b = 0; b < nb; b++)
 				{
-					int N = j->pc_nbins[s][b];
+					int N = j->pc_nbins[s][b], off = j->pc_shift[s][b];
 					const float *x = scratch + (size_t)b * stu + (fi.nearestsample - ups[s]);
+					long long fsi = (long long)(2e6 * station_bw(j, s) + 0.5);
 					if(N <= 0) continue;
 					for(c = 0; c < 2 * nchan; c++)
-						pbins[s][b][(a0 + c) % N] += x[c];
+					{
+						long long bin = (a0 + c) % N;
+						if(off == 0)
+							pbins[s][b][2 * bin] += x[c];
+						else
+						{
+							/* the shifting extractor's rotator, exp(-2 pi i off a / fs) */
+							double ang = -TWO_PI_D * (double)(((long long)off * ((a0 + c) % fsi)) % fsi) / (double)fsi;
+							pbins[s][b][2 * bin] += x[c] * cos(ang);
+							pbins[s][b][2 * bin + 1] += x[c] * sin(ang);
+						}
+					}
 				}
 			}
 			/* autocorrelations (mode.cpp:1293-1308) and cross-pol autos (:1356-1369) */
@@ -1091,8 +1122,9 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 					for(m = 0; m < N; m++)
 					{
 						double ang = -TWO_PI_D * (double)((idx * m) % N) / (double)N;
-						re += pbins[s][b][m] * cos(ang);
-						im += pbins[s][b][m] * sin(ang);
+						double zr = pbins[s][b][2 * m], zi = pbins[s][b][2 * m + 1];
+						re += zr * cos(ang) - zi * sin(ang);
+						im += zr * sin(ang) + zi * cos(ang);
 					}
 				}
 				coreresult[2 * (ridx + k)] += re;

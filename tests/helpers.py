@@ -122,6 +122,10 @@ PCAL_JOBS = {
     # first tone 31.25 kHz above the LO: 1024 bins, fewer than the 4096
     # samples of a window
     "pcal_1024_bins": lambda: pcal_job(nstation=2, nchan=2048, freq0=8400.96875, subint_ns=4_096_000),
+    # a 5 MHz comb over 8400-8432 MHz: the second subband's first tone is 4 MHz
+    # above its LO, whose period is not a multiple of the comb's (shifting
+    # extractor)
+    "pcal_shifting": lambda: pcal_job(5.0, nstation=2, nfreq=2, full_pol=True, subint_ns=2_048_000),
     # lower-sideband bands, LO on the comb and 10 kHz off it
     "pcal_lsb": lambda: pcal_job(nstation=2, nfreq=2, full_pol=True, lsb=True, subint_ns=2_048_000),
     "pcal_lsb_frac": lambda: pcal_job(nstation=2, lsb=True, freq0=8400.01),

@@ -77,7 +77,7 @@ def test_zoom_rejections():
 
 
 @pytest.mark.parametrize("name", ["pcal_int_lo", "pcal_frac_lo", "pcal_8bit", "pcal_no_tone", "pcal_5mhz",
-                                  "pcal_1024_bins", "pcal_lsb", "pcal_lsb_frac"])
+                                  "pcal_1024_bins", "pcal_lsb", "pcal_lsb_frac", "pcal_shifting"])
 def test_pcal_layout_matches_oracle(name):
     from helpers import PCAL_JOBS
     job = PCAL_JOBS[name]()
@@ -89,11 +89,6 @@ def test_pcal_layout_matches_oracle(name):
 
 def test_pcal_rejections():
     from helpers import pcal_job
-    # a 4 MHz first-tone offset with a 5 MHz comb in 32 Ms/s needs the
-    # shifting extractor (pcal.cpp:494-705), which is not built
-    job = pcal_job(5.0, nstation=2, freq0=8416.0)
-    with pytest.raises(native.FxbError, match="UNSUPPORTED"):
-        native.job_layout(job)
     # a phase-cal base that puts the first tone on the LO needs the trivial
     # extractor, whose tone count then differs from the configuration's
     job = pcal_job(1.0, base=-1.0, nstation=2)
