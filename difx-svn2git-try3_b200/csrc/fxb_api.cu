@@ -1527,6 +1527,23 @@ fxb_status fxb_vis_calibrate(const fxb_job_desc *desc, const fxb_vis_params *par
 	return st != FXB_OK ? st : vis_calibrate(job, params, coreresult);
 }
 
+fxb_status fxb_vis_write_pcal(const fxb_job_desc *desc, const fxb_vis_params *params, const float *coreresult,
+                              const char *dir)
+{
+	Job job;
+	fxb_status st = job_of(desc, job);
+	if(st != FXB_OK)
+		return st;
+	std::string err;
+	st = vis_pcal_write(job, params, coreresult, dir, err);
+	if(st != FXB_OK)
+	{
+		std::lock_guard<std::mutex> lk(g_err_mutex);
+		g_create_err = err;
+	}
+	return st;
+}
+
 fxb_status fxb_vis_write_swin(const fxb_job_desc *desc, const fxb_vis_params *params, const float *coreresult,
                               const char *dir)
 {

@@ -152,6 +152,8 @@ struct Job {
 	struct PcalBand {
 		int station, band, ntones, nbins, first, step;
 		int shift;          // shifting extractor: samples rotated by this offset (Hz) into complex bins; else 0
+		double tonefreq;    // comb tone nearest the LO inside the band, before the base (MHz); 0: no tone
+		int lsb;
 		int64_t fs;         // samples per second
 		int64_t core;       // core-result offset (complex) of the band's first tone
 		int64_t bin_off;    // offset (doubles) of the band's bins in the bin accumulator (complex bins: 2 per bin)
@@ -181,6 +183,8 @@ fxb_status datastream_control(const Job &job, const DevStation &S, int s, fxb_ri
 // integration output (fxb_vis.cpp)
 fxb_status vis_calibrate(const Job &job, const fxb_vis_params *p, float *coreresult);
 fxb_status vis_swin_write(const Job &job, const fxb_vis_params *p, const float *coreresult, const char *dir,
+                          std::string &err);
+fxb_status vis_pcal_write(const Job &job, const fxb_vis_params *p, const float *coreresult, const char *dir,
                           std::string &err);
 
 // fxb_create with the context's device memory taken from a cudaMemPool_t

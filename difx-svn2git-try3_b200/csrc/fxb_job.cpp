@@ -89,6 +89,8 @@ static bool pcal_band(const fxb_freq &f, float interval, float base, Job::PcalBa
 {
 	pb.nbins = pb.first = pb.step = pb.shift = 0;
 	pb.fs = (int64_t)(2e6 * f.bw_mhz + 0.5);
+	pb.tonefreq = 0.0;
+	pb.lsb = f.lower_sideband ? 1 : 0;
 	const double lo = f.freq_mhz, bw = f.bw_mhz;
 	double tonefreq = (double)((int)(lo / interval)) * interval;
 	int n = 0;
@@ -116,6 +118,7 @@ static bool pcal_band(const fxb_freq &f, float interval, float base, Job::PcalBa
 		return true;
 	}
 	pb.ntones = n;
+	pb.tonefreq = tonefreq;
 	int off;
 	if(f.lower_sideband)
 	{

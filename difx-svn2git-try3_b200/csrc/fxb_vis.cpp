@@ -14,6 +14,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -247,6 +248,25 @@ static fxb_status calibrate(const Job &job, const fxb_vis_params *p, float *fr)
 				}
 		}
 	}
+
+	// phase-cal tones, recorded band by recorded band (visibility.cpp:586-609):
+	// normalised by the band's autocorrelation weight, or by the data alone
+	// when zoom bands leave the recorded band without one
+	for(const Job::PcalBand &pb : job.pcal)
+	{
+		const int i = pb.station, j = pb.band;
+		const fxb_freq &f = job.freqs[job.stations[i].band_freq[j]];
+		const int fc = f.nchan / f.chans_to_avg;
+		double a = acw[i][0][j];
+		if(a == 0.0 && job.stations[i].total_bands() > job.stations[i].nband)
+			a = 1.0;
+		if(a > 0.0)
+		{
+			const float scale = (float)(1.0 / (a * in.meansubints * ((float)(job.blockspersend * 2 * fc * f.chans_to_avg))));
+			for(int c = 0; c < 2 * pb.ntones; c++)
+				fr[2 * pb.core + c] *= scale;
+		}
+	}
 	return FXB_OK;
 }
 
@@ -362,6 +382,102 @@ static fxb_status swin_write(const Job &job, const fxb_vis_params *p, const floa
 		return FXB_ERR_DATA;
 	}
 	return FXB_OK;
+}
+
+// One line per station and integration of its calibrated phase-cal tones,
+// appended to PCAL_<mjd>_<sec>_<station>, which starts with the reference's
+// comment header (Visibility::initialisePcalFiles, visibility.cpp:104-135;
+// the line: Visibility::writedifx, visibility.cpp:928-990).
+static fxb_status pcal_write(const Job &job, const fxb_vis_params *p, const float *fr, const char *dir,
+                             std::string &err)
+{
+	const int S = (int)job.stations.size();
+	const int isec = p->start_sec + p->scan_start_sec + p->int_start_sec;
+	const int dumpmjd = p->start_mjd + isec / 86400;
+	const double dumpseconds = double(isec % 86400) + ((double)p->int_start_ns) / 1000000000.0 + p->int_time_s / 2.0;
+	const double pcalmjd = dumpmjd + dumpseconds / 86400.0;
+	for(int i = 0; i < S; i++)
+	{
+		const Job::Station &st = job.stations[i];
+		if(!(st.pcal_interval > 0.0f))
+			continue;
+		char nm[32];
+		snprintf(nm, sizeof(nm), "DS%d", i);
+		const std::string name = p->names && p->names[i] ? p->names[i] : nm;
+		std::vector<const Job::PcalBand *> bands;
+		int maxtones = 0;
+		for(const Job::PcalBand &pb : job.pcal)
+			if(pb.station == i)
+			{
+				bands.push_back(&pb);
+				maxtones = std::max(maxtones, pb.ntones);
+			}
+		char buf[256];
+		snprintf(buf, sizeof(buf), "%s %13.7f %9.7f %d %d %d", name.c_str(), pcalmjd, p->int_time_s / 86400.0, i,
+		         st.nband, maxtones);
+		std::string line = buf;
+		bool nonzero = false;
+		for(const Job::PcalBand *pb : bands)
+		{
+			for(int t = 0; t < maxtones; t++)
+			{
+				if(t >= pb->ntones)
+				{
+					line += " -1 0 0 0";
+					continue;
+				}
+				// tone frequencies (configuration.cpp:1799-1801, 1830-1833); a band
+				// without a tone has one at 0
+				double hz = 0.0;
+				if(pb->nbins > 0 || pb->tonefreq != 0.0)
+					hz = pb->lsb ? 1e6 * pb->tonefreq - double(t) * 1e6 * st.pcal_interval - 1e6 * st.pcal_base
+					             : 1e6 * pb->tonefreq + t * 1e6 * st.pcal_interval + 1e6 * st.pcal_base;
+				const double tonefreq = 1e-6 * hz;
+				const float re = fr[2 * (pb->core + t)], im = fr[2 * (pb->core + t) + 1];
+				snprintf(buf, sizeof(buf), " %.12g %c %12.5e %12.5e", tonefreq, st.band_pol[pb->band], re,
+				         pb->lsb ? im : -im);
+				if(re != 0.0 && -im != 0.0)
+					nonzero = true;
+				line += buf;
+			}
+		}
+		if(!nonzero)
+			continue;
+		char fname[64];
+		snprintf(fname, sizeof(fname), "/PCAL_%05d_%06d_", p->start_mjd, p->start_sec);
+		const std::string path = std::string(dir) + fname + name;
+		FILE *fp = fopen(path.c_str(), "r");
+		const bool exists = fp != nullptr;
+		if(fp)
+			fclose(fp);
+		fp = fopen(path.c_str(), "a");
+		if(!fp)
+		{
+			err = "cannot open " + path;
+			return FXB_ERR_ARG;
+		}
+		bool ok = true;
+		if(!exists)
+			ok = fprintf(fp, "# DiFX-derived pulse cal data\n# File version = 1\n# Start MJD = %d\n"
+			                 "# Start seconds = %d\n# Telescope name = %s\n",
+			             p->start_mjd, p->start_sec, name.c_str()) > 0;
+		ok = ok && fprintf(fp, "%s\n", line.c_str()) > 0;
+		ok = (fclose(fp) == 0) && ok;
+		if(!ok)
+		{
+			err = "short write to " + path;
+			return FXB_ERR_DATA;
+		}
+	}
+	return FXB_OK;
+}
+
+fxb_status vis_pcal_write(const Job &job, const fxb_vis_params *p, const float *coreresult, const char *dir,
+                          std::string &err)
+{
+	if(!p || !coreresult || !dir || p->int_time_s <= 0.0)
+		return FXB_ERR_ARG;
+	return pcal_write(job, p, coreresult, dir, err);
 }
 
 fxb_status vis_calibrate(const Job &job, const fxb_vis_params *p, float *coreresult)

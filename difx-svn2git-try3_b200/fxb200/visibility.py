@@ -1,7 +1,8 @@
-"""Integration output: amplitude calibration of an integrated core result and
-SWIN ``.difx`` records (fxb_vis_calibrate / fxb_vis_write_swin of
-include/fxb200.h, the reference's Visibility::writedata and writedifx,
-mpifxcorr/src/visibility.cpp:348-900), plus a reader for those records.
+"""Integration output: amplitude calibration of an integrated core result,
+SWIN ``.difx`` records and phase-cal files (fxb_vis_calibrate /
+fxb_vis_write_swin / fxb_vis_write_pcal of include/fxb200.h, the reference's
+Visibility::writedata and writedifx, mpifxcorr/src/visibility.cpp:104-135,
+348-990), plus a reader for the records.
 
 An integration on the device is: ``Correlator.reset()``, submit its subints,
 ``Correlator.results()`` -- the sum the reference's Visibility::addData
@@ -32,7 +33,7 @@ class FxbVisParams(_c.Structure):
                 ("scan_start_sec", _c.c_int32), ("int_start_sec", _c.c_int32), ("int_start_ns", _c.c_int32),
                 ("config_index", _c.c_int32), ("source_index", _c.c_int32),
                 ("tsys", _c.POINTER(_c.c_double)), ("telescope", _c.POINTER(_c.c_int32)),
-                ("uvw", _c.POINTER(_c.c_double))]
+                ("uvw", _c.POINTER(_c.c_double)), ("names", _c.POINTER(_c.c_char_p))]
 
 
 @dataclasses.dataclass
@@ -48,16 +49,22 @@ class VisParams:
     tsys: Optional[Sequence[float]] = None
     telescope: Optional[Sequence[int]] = None
     uvw: Optional[np.ndarray] = None        # [nbaseline, 3]
+    names: Optional[Sequence[str]] = None   # station names (PCAL files)
 
     @staticmethod
     def for_job(job: Job, **kw) -> "VisParams":
-        """The job's own start and integration time."""
+        """The job's own start, integration time and station names."""
+        kw.setdefault("names", [st.name for st in job.stations])
         return VisParams(int_time_s=job.duration_s, start_mjd=job.start_mjd, start_sec=job.start_sec, **kw)
 
     def native(self):
         keep = []
         p = FxbVisParams(self.int_time_s, self.start_mjd, self.start_sec, self.scan_start_sec, self.int_start_sec,
-                         self.int_start_ns, self.config_index, self.source_index, None, None, None)
+                         self.int_start_ns, self.config_index, self.source_index, None, None, None, None)
+        if self.names is not None:
+            a = (_c.c_char_p * len(self.names))(*[n.encode() for n in self.names])
+            keep.append(a)
+            p.names = _c.cast(a, _c.POINTER(_c.c_char_p))
         if self.tsys is not None:
             a = np.ascontiguousarray(self.tsys, dtype=np.float64)
             keep.append(a)
@@ -81,6 +88,9 @@ def _bind():
         L.fxb_vis_write_swin.argtypes = [_c.POINTER(FxbJobDesc), _c.POINTER(FxbVisParams), _c.POINTER(_c.c_float),
                                          _c.c_char_p]
         L.fxb_vis_write_swin.restype = _c.c_int
+        L.fxb_vis_write_pcal.argtypes = [_c.POINTER(FxbJobDesc), _c.POINTER(FxbVisParams), _c.POINTER(_c.c_float),
+                                         _c.c_char_p]
+        L.fxb_vis_write_pcal.restype = _c.c_int
         L._vis_bound = True
     return L
 
@@ -108,6 +118,16 @@ def write_swin(job: Job, params: VisParams, calibrated: np.ndarray, outdir: str)
     p, keep = params.native()
     _check(_bind().fxb_vis_write_swin(d.ptr(), _c.byref(p), a.ctypes.data_as(_c.POINTER(_c.c_float)),
                                       outdir.encode()), "vis_write_swin")
+
+
+def write_pcal(job: Job, params: VisParams, calibrated: np.ndarray, outdir: str) -> None:
+    """Append the calibrated integration's phase-cal tones to
+    outdir/PCAL_<mjd>_<sec>_<station> of every station extracting them."""
+    a = np.ascontiguousarray(calibrated, dtype=np.float32)
+    d = DescHolder(job)
+    p, keep = params.native()
+    _check(_bind().fxb_vis_write_pcal(d.ptr(), _c.byref(p), a.ctypes.data_as(_c.POINTER(_c.c_float)),
+                                      outdir.encode()), "vis_write_pcal")
 
 
 @dataclasses.dataclass

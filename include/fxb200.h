@@ -269,18 +269,27 @@ typedef struct {
 	const double *tsys;           /* [ndatastream] a-priori Tsys (TSYS), NULL: none */
 	const int32_t *telescope;     /* [ndatastream] telescope index, NULL: the datastream index */
 	const double *uvw;            /* [nbaseline * 3] u, v, w (m) at the integration centre, NULL: 0 */
+	const char *const *names;     /* [ndatastream] station names (PCAL files), NULL: "DS<index>" */
 } fxb_vis_params;
 /* Amplitude-calibrate an integrated core result of the job in place:
  * baseline and autocorrelation weights normalised by the FFTs per
  * integration, products scaled to correlation coefficients, or with Tsys by
  * the band-averaged autocorrelations and the quantisation decorrelation
- * (weights stay raw).  Needs no GPU: the caller may be the process that
- * writes the output rather than the one correlating. */
+ * (weights stay raw); phase-cal tones scaled by their band's data weight.
+ * Needs no GPU: the caller may be the process that writes the output rather
+ * than the one correlating. */
 FXB_API fxb_status fxb_vis_calibrate(const fxb_job_desc *desc, const fxb_vis_params *params, float *coreresult);
 /* Append the calibrated integration to <dir>/DIFX_<mjd>_<sec>.s0000.b0000 as
  * SWIN records: every baseline product with weight > 0, then every
  * autocorrelation with weight > 0 (message via fxb_last_error(NULL)). */
 FXB_API fxb_status fxb_vis_write_swin(const fxb_job_desc *desc, const fxb_vis_params *params, const float *coreresult,
+                                      const char *dir);
+/* Append the calibrated integration's phase-cal tones to
+ * <dir>/PCAL_<mjd>_<sec>_<station> of every station extracting them, one line
+ * per integration with a non-zero tone, the file starting with the
+ * reference's comment header (Visibility::initialisePcalFiles and writedifx,
+ * visibility.cpp:104-135, 928-990). */
+FXB_API fxb_status fxb_vis_write_pcal(const fxb_job_desc *desc, const fxb_vis_params *params, const float *coreresult,
                                       const char *dir);
 
 /* ---- INTERLACEDVDIF: multi-thread VDIF to the single-thread, multi-channel

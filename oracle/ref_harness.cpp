@@ -562,6 +562,7 @@ int dref_visibility_write(void *h, const float *const *subints, int nsub)
 	if(!v.configuredOK())
 		return 1;
 	std::vector<float> tmp(nfl);
+	v.initialisePcalFiles();                 /* FxManager does this once (fxmanager.cpp:651) */
 	for(int k = 0; k < nsub; k++)
 	{
 		memcpy(tmp.data(), subints[k], sizeof(float) * 2 * j->corelen);

@@ -93,13 +93,17 @@ class RefCorrelator:
         import glob
         outdir = os.path.splitext(self.input_path)[0] + ".difx"
         os.makedirs(outdir, exist_ok=True)
-        for f in glob.glob(os.path.join(outdir, "DIFX_*")):
+        for f in glob.glob(os.path.join(outdir, "DIFX_*")) + glob.glob(os.path.join(outdir, "PCAL_*")):
             os.remove(f)
         arrs = [np.ascontiguousarray(r, dtype=np.float32) for r in subint_results]
         ptrs = (ctypes.POINTER(ctypes.c_float) * len(arrs))(*[_fptr(a) for a in arrs])
         rc = lib().dref_visibility_write(self.h, ptrs, len(arrs))
         if rc != 0:
             raise RuntimeError("reference Visibility not configured")
+        self.pcal_files = {}
+        for name in glob.glob(os.path.join(outdir, "PCAL_*")):
+            with open(name, "rb") as f:
+                self.pcal_files[os.path.basename(name)] = f.read()
         files = glob.glob(os.path.join(outdir, "DIFX_*"))
         if not files:
             return b""

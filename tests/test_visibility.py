@@ -108,3 +108,38 @@ def test_tsys_with_zoom_cross_hand_autos_is_refused():
 def _corelen(job):
     from fxb200.native import job_layout
     return job_layout(job)[1]
+
+
+@pytest.mark.parametrize("name", ["pcal_int_lo", "pcal_frac_lo", "pcal_lsb", "pcal_shifting", "pcal_no_tone"])
+def test_pcal_files_match_reference_visibility(name, tmp_path):
+    # phase-cal tones scaled by their band's data weight (visibility.cpp:586-609)
+    # and written as one line per station to PCAL_<mjd>_<sec>_<station> after
+    # the reference's header (visibility.cpp:104-135, 928-990)
+    from helpers import PCAL_JOBS
+    job = PCAL_JOBS[name]()
+    ref = refcorr.RefCorrelator(job)
+    subs = _subints(job, ref)
+    expect = ref.visibility_write(subs)
+    expect_pcal = dict(ref.pcal_files)
+    ref.close()
+    integ = np.zeros_like(subs[0])
+    for s in subs:
+        integ += s
+    params = visibility.VisParams.for_job(job)
+    cal = visibility.calibrate(job, params, integ)
+    visibility.write_swin(job, params, cal, str(tmp_path))
+    visibility.write_pcal(job, params, cal, str(tmp_path))
+    with open(os.path.join(str(tmp_path), "DIFX_%05d_%06d.s0000.b0000" % (job.start_mjd, job.start_sec)), "rb") as f:
+        assert f.read() == expect
+    got_pcal = {}
+    for fn in os.listdir(str(tmp_path)):
+        if fn.startswith("PCAL_"):
+            with open(os.path.join(str(tmp_path), fn), "rb") as f:
+                got_pcal[fn] = f.read()
+    # a station's file exists in the reference from its header alone
+    for fn, data in expect_pcal.items():
+        if data.count(b"\n") > 5:
+            assert got_pcal.get(fn) == data, fn
+        else:
+            assert fn not in got_pcal, fn
+    assert any(d.count(b"\n") > 5 for d in expect_pcal.values()) or name == "pcal_no_tone"
