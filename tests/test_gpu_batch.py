@@ -186,3 +186,34 @@ def test_batch_autotune_keeps_results():
     for g, r in zip(got, alone):
         assert np.array_equal(g, r)
     assert all(" ms" in rp for rp in reports)
+
+
+@pytest.mark.parametrize("xmac", ["fp32", "bf16"])
+def test_batch_of_zoom_and_pcal_jobs_matches_each_alone(xmac):
+    # zoom gather and phase-cal binning run inside the batch graph like the
+    # other kernels: every member's result is bit-identical to its own run
+    from helpers import PCAL_JOBS, zoom_job
+    jobs = [zoom_job(), PCAL_JOBS["pcal_frac_lo"](), PCAL_JOBS["pcal_int_lo"]()]
+    subs = [(0, 2_048_000 * (k + 1)) for k in range(3)]
+
+    def inputs(k, job, sec, ns):
+        return synth.subint_inputs(job, sec, ns, rho=0.05, seed=40 + k)
+
+    alone = []
+    for k, job in enumerate(jobs):
+        c = Correlator(job, xmac=xmac)
+        for sec, ns in subs:
+            c.submit(inputs(k, job, sec, ns), sec, ns)
+        alone.append(c.results())
+        c.close()
+    members = [Correlator(j, xmac=xmac) for j in jobs]
+    batch = Batch(members)
+    for sec, ns in subs:
+        batch.submit([inputs(k, j, sec, ns) for k, j in enumerate(jobs)], sec, ns)
+    batch.sync()
+    got = [m.results() for m in members]
+    batch.close()
+    for m in members:
+        m.close()
+    for g, a in zip(got, alone):
+        assert np.array_equal(g, a)
