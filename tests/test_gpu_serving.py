@@ -118,3 +118,17 @@ def test_a_failing_job_is_reported_and_the_others_complete():
         assert srv.poll(h)[0] == 2
     assert "bad station buffer" in serving._bind().fxb_server_last_error(srv.srv).decode()
     srv.close()
+
+
+def test_zoom_and_pcal_jobs_served_in_the_mix():
+    # a zoom job and a phase-cal job (fractional LO: 3200 bins) served beside
+    # a plain one give each job's own result bit for bit
+    from helpers import PCAL_JOBS, zoom_job
+    jobs = [zoom_job(), PCAL_JOBS["pcal_frac_lo"](), _jobs()[0][0]]
+    jobs = [(j, serving.job_subints(j, 3, seed=60 + k, rho=0.05)) for k, j in enumerate(jobs)]
+    alone = [_alone(j, s, "bf16") for j, s in jobs]
+    srv = serving.Server(budget_bytes=8 << 30, max_active=3)
+    handles = [srv.submit(j, s, xmac="bf16") for j, s in jobs]
+    for h, ref in zip(handles, alone):
+        assert np.array_equal(srv.wait(h, 120.0), ref)
+    srv.close()
