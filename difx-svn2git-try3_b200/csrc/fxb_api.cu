@@ -688,6 +688,13 @@ static fxb_status setup_device(fxb_ctx *ctx)
 			// bin (bin counts of 128 or 64) share a chunk evenly
 			int tpc = (ctx->T + ctx->pchunks - 1) / ctx->pchunks;
 			tpc = std::min(ctx->T, (tpc + 3) / 4 * 4);
+			// and short enough that the chunk's FFT table and the lane sums fit
+			// one CTA's shared memory
+			size_t lanes = 0;
+			for(const DevPcalGroup &g : ctx->h_pgroups)
+				lanes = std::max(lanes, pcal_group_smem(g));
+			while(tpc > 4 && pcal_smem(lanes, tpc) > kPcalSmemLaunchMax)
+				tpc = (tpc / 2 + 3) / 4 * 4;
 			ctx->pchunks = (ctx->T + tpc - 1) / tpc;
 			for(size_t i = 0; i < ctx->h_pgroups.size(); i++)
 			{

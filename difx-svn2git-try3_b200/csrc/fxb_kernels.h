@@ -171,6 +171,7 @@ struct DevPcalBand {
 size_t pcal_group_smem(const DevPcalGroup &g);
 size_t pcal_smem(size_t group_smem, int tpc);
 constexpr size_t kPcalSmemMax = 96 * 1024;    // lane sums of one group at most
+constexpr size_t kPcalSmemLaunchMax = 200 * 1024;   // a launch's FFT table and lane sums at most
 // allows the binning kernels smem bytes of dynamic shared memory (once per context)
 cudaError_t pcal_init(size_t smem);
 // folds the subint's samples into the FP64 bins: the FFTs are split into

@@ -13,7 +13,7 @@ import pytest
 
 from fxb200 import synth
 from fxb200.native import Correlator
-from helpers import PCAL_JOBS, compare_core, regions
+from helpers import PCAL_JOBS, compare_core, pcal_job, regions
 
 import fxoracle
 
@@ -72,3 +72,14 @@ def test_pcal_reset_starts_again():
 def _layout(job):
     from fxb200.native import job_layout
     return job_layout(job)[0]
+
+
+def test_pcal_long_subint_fine_bins():
+    """16000 FFT windows per subint and 32000 bins per band on 5 stations:
+    one chunk of FFTs per launch would need a 320 KB FFT table in shared
+    memory, so the windows are split into chunks that fit."""
+    job = pcal_job(nstation=5, nfreq=2, nchan=64, freq0=8400.001, subint_ns=64_000_000)
+    assert job.blocks_per_send() == 16000
+    got, ref, layout, n = _run(job, subints=[(0, 0)])
+    errs = compare_core(job, layout, n, got, ref)
+    assert "pcal" in errs
