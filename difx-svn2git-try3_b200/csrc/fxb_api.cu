@@ -83,6 +83,8 @@ struct fxb_ctx {
 	std::vector<void *> owned;          // misc device allocations
 	float2 *d_twiddle = nullptr;
 	FftParam *d_params = nullptr;
+	float *d_pbw = nullptr;              // per-band data weights of INTERLACEDVDIF stations [S][T][nbm]
+	int nbm = 0;
 	float2 *d_spec = nullptr;
 	float2 *d_acc = nullptr;
 	float *d_bwacc = nullptr, *d_acwacc = nullptr;
@@ -103,7 +105,8 @@ struct fxb_ctx {
 	size_t psmem = 0;
 	double *d_pbins = nullptr;           // [pchunks][job.pcal_bins]
 	float2 *d_core = nullptr;
-	uint8_t *d_valid = nullptr;
+	uint8_t *d_valid = nullptr;          // frame validity [S][valid_stride], then the band masks
+	uint32_t *d_bandok = nullptr;        // [S][valid_stride] in the same allocation
 	int64_t valid_stride = 0;
 	std::vector<Slot> slots;
 	int next_slot = 0;
@@ -314,6 +317,9 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		d.fftchannels = 2 * f.nchan;
 		d.asl = calcstridelength((unsigned)f.nchan);
 		d.sticky = (js.nbits == 8 && (js.nband == 2 || js.nband == 4)) ? 1 : 0;
+		d.mux = js.mux_threads > 0 ? 1 : 0;
+		if(d.mux)
+			ctx->nbm = std::max(ctx->nbm, js.nband);
 		d.bpbn = (js.nband * 1 * js.nbits) / 8;
 		d.bpbd = 1;
 		if(d.bpbn == 0)
@@ -593,7 +599,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				for(const FGroup &gg : kv.second)
 					any_lsb = any_lsb || gg.lsb;
 				const char *env = getenv("FXB_TC_FFT");
-				const bool allow = env && env[0] == '1';
+				const bool allow = env && env[0] == '1' && ctx->nbm == 0;   // no EDV4 band blanking there
 				if(allow && fstage_tc_eligible(k.N, job.fringe_rot_order, any_lsb))
 				{
 					if(!ctx->d_tctab)
@@ -636,6 +642,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 	}
 	// big buffers
 	CK(ctx, dalloc(ctx, &ctx->d_params, (size_t)ctx->S * ctx->T));
+	if(ctx->nbm)
+		CK(ctx, dalloc(ctx, &ctx->d_pbw, (size_t)ctx->S * ctx->T * ctx->nbm));
 	CK(ctx, dalloc(ctx, &ctx->d_spec, job.xmac_kind == FXB_XMAC_FP32 ? (size_t)job.spec_total : 1));
 	CK(ctx, dalloc(ctx, &ctx->d_acc, (size_t)job.acc_total));
 	CK(ctx, dalloc(ctx, &ctx->d_core, (size_t)job.corelen));
@@ -647,10 +655,11 @@ static fxb_status setup_device(fxb_ctx *ctx)
 	{
 		std::vector<DevBWeight> hbw(ctx->nbw);
 		for(int i = 0; i < ctx->nbw; i++)
-			hbw[i] = DevBWeight{job.bweights[i].s1, job.bweights[i].s2, job.bweights[i].dst_float};
+			hbw[i] = DevBWeight{job.bweights[i].s1, job.bweights[i].s2, job.bweights[i].b1, job.bweights[i].b2,
+			                    job.bweights[i].dst_float};
 		std::vector<DevACWeight> hacw(ctx->nacw);
 		for(int i = 0; i < ctx->nacw; i++)
-			hacw[i] = DevACWeight{job.acweights[i].s, 0, job.acweights[i].dst_float};
+			hacw[i] = DevACWeight{job.acweights[i].s, job.acweights[i].band, job.acweights[i].dst_float};
 		std::vector<DevOutMap> hom(ctx->nom);
 		for(int i = 0; i < ctx->nom; i++)
 		{
@@ -907,7 +916,9 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 			CK(ctx, cudaFreeAsync(ctx->d_valid, ctx->stream));
 			ctx->d_valid = nullptr;
 		}
-		CK(ctx, pool_alloc(ctx, (void **)&ctx->d_valid, (size_t)need * ctx->S, ctx->stream));
+		const size_t vbytes = ((size_t)need * ctx->S + 15) / 16 * 16;
+		CK(ctx, pool_alloc(ctx, (void **)&ctx->d_valid, vbytes + sizeof(uint32_t) * need * ctx->S, ctx->stream));
+		ctx->d_bandok = (uint32_t *)(ctx->d_valid + vbytes);
 		ctx->valid_stride = need;
 	}
 
@@ -995,9 +1006,9 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 	const unsigned evf = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
 	cudaEventRecordWithFlags(sl.tev[0], st, evf);
 	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, st);
-	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->valid_stride, ctx->S, st);
-	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->valid_stride, ctx->S, ctx->T,
-	                  job.fringe_rot_order, ctx->d_params, st);
+	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->d_bandok, ctx->valid_stride, ctx->S, st);
+	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->d_bandok, ctx->valid_stride,
+	                  ctx->S, ctx->T, job.fringe_rot_order, ctx->d_params, ctx->d_pbw, ctx->nbm, st);
 	cudaEventRecordWithFlags(sl.tev[1], st, evf);
 	{
 		FsArgs fa;
@@ -1007,6 +1018,7 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 		fa.groups = ctx->d_groups;
 		fa.plans = ctx->d_plans;
 		fa.valid = ctx->d_valid;
+		fa.bandok = ctx->nbm ? ctx->d_bandok : nullptr;
 		fa.valid_stride = ctx->valid_stride;
 		fa.params = ctx->d_params;
 		fa.maxN = ctx->maxN;
@@ -1071,7 +1083,8 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 	}
 	if(tuning)
 		cudaEventRecord(tn.ev[nk + 1 + ctx->xgroups.size()], st);
-	launch_weights(ctx->d_bw, ctx->nbw, ctx->d_acw, ctx->nacw, ctx->d_params, ctx->T, ctx->d_bwacc, ctx->d_acwacc, st);
+	launch_weights(ctx->d_bw, ctx->nbw, ctx->d_acw, ctx->nacw, ctx->d_params, ctx->d_pbw, ctx->nbm, ctx->d_st, ctx->T,
+	               ctx->d_bwacc, ctx->d_acwacc, st);
 	cudaEventRecordWithFlags(sl.tev[3], st, evf);
 }
 

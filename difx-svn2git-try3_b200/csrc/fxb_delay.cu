@@ -17,8 +17,45 @@ namespace fxb {
 // 4009-4056), no fill pattern in the first or last 64-bit payload word
 // (blanker_mark5.c:282-313).  Frames that do not fit in the buffer are
 // treated as invalid.
+//
+// bandok (may be null): the bands of each frame that keep their samples.  On
+// INTERLACEDVDIF stations a valid frame with an EDV4 validity mask blanks
+// band c when mask bit c / d is clear, d = channels / mask length, with the
+// geometry read from the buffer's first frame (blank_vdif_EDV4,
+// format_vdif.c:4699-4780; bit 31 of the C int shift tests mask bits 31-63,
+// and a 32-channel header's "good" mask is 0).  Headers whose geometry is not
+// the station's blank nothing.
+__device__ __forceinline__ uint32_t edv4_bands(const DevStation &S, const DevSubintStation &U, const uint8_t *f)
+{
+	if(U.nbytes < 32)
+		return 0xFFFFFFFFu;
+	const uint32_t w2 = *(const uint32_t *)(U.buf + 8), w3 = *(const uint32_t *)(U.buf + 12);
+	const uint32_t w4 = *(const uint32_t *)(U.buf + 16);
+	const int ml = (int)((w4 >> 16) & 0xFFu);
+	if((w4 >> 24) != 4u || ml < 1 || ml > 64)
+		return 0xFFFFFFFFu;
+	const int nch = 1 << ((w2 >> 24) & 31u);
+	const int flen = (int)(w2 & 0xFFFFFFu) * 8;
+	const int spf = (flen - 32) * 8 / (nch * (int)(((w3 >> 26) & 31u) + 1u));
+	const int d = nch / ml;
+	if(d < 1 || nch != S.nband || spf != S.framesamples || flen != S.framebytes)
+		return 0xFFFFFFFFu;
+	const uint64_t mask = *(const uint64_t *)(f + 24);
+	const uint64_t good = nch < 32 ? (uint64_t)((1u << nch) - 1u) : 0u;
+	if(mask == good)
+		return 0xFFFFFFFFu;
+	uint32_t ok = 0u;
+	for(int c = 0; c < nch; c++)
+	{
+		const int q = c / d;
+		const bool keep = q < 31 ? ((mask >> q) & 1u) != 0 : (mask & 0xFFFFFFFF80000000ULL) != 0;
+		ok |= (uint32_t)keep << c;
+	}
+	return ok | (nch < 32 ? ~((1u << nch) - 1u) : 0u);
+}
+
 __global__ void k_frame_valid(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
-                              uint8_t *__restrict__ valid, int64_t valid_stride)
+                              uint8_t *__restrict__ valid, uint32_t *__restrict__ bandok, int64_t valid_stride)
 {
 	const int s = blockIdx.y;
 	const DevStation &S = st[s];
@@ -38,6 +75,8 @@ __global__ void k_frame_valid(const DevStation *__restrict__ st, const DevSubint
 			v = (w2 != 0) && !((w0 >> 31) & 1) && first != FILL && last != FILL;
 		}
 		valid[s * valid_stride + fr] = v;
+		if(bandok)
+			bandok[s * valid_stride + fr] = (v && S.mux) ? edv4_bands(S, U, U.buf + fr * S.framebytes) : 0xFFFFFFFFu;
 	}
 }
 
@@ -122,13 +161,20 @@ __device__ inline bool flag_valid(const int32_t *vf, int i)
 // (mode.cpp:671-840) and the Mk5Mode::unpack weight (mk5mode.cpp:104-177).
 __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
                              const int32_t *__restrict__ validflags, int nflagint, const uint8_t *__restrict__ valid,
-                             int64_t valid_stride, int T, int order, FftParam *__restrict__ out)
+                             const uint32_t *__restrict__ bandok, int64_t valid_stride, int T, int order,
+                             FftParam *__restrict__ out, float *__restrict__ pbw, int nbm)
 {
 	const int s = blockIdx.y;
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if(i >= T)
 		return;
 	const DevStation &S = st[s];
+	// per-band weights of INTERLACEDVDIF stations (Mk5Mode::unpack,
+	// mk5mode.cpp:145-166): zero unless this FFT is unpacked (mode.cpp:663-668)
+	float *pb = (S.mux && pbw) ? pbw + ((int64_t)s * T + i) * nbm : nullptr;
+	if(pb)
+		for(int b = 0; b < S.nband; b++)
+			pb[b] = 0.0f;
 	const DevSubintStation &U = sub[s];
 	const int offsetsec = U.subsec, offsetns = U.subns;
 	const int32_t *vf = validflags + (int64_t)s * nflagint;
@@ -182,6 +228,11 @@ __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintS
 	const int stu = N + (S.gran > 1 ? S.gran : 0);
 	int count = 0;
 	int stuck = N;
+	int inv[32];                 // samples of EDV4-blanked bands in valid frames, per band
+	int totinv = 0;
+	if(pb)
+		for(int b = 0; b < S.nband; b++)
+			inv[b] = 0;
 	{
 		int64_t g0 = ups, g1 = (int64_t)ups + stu;            // [g0, g1)
 		int64_t f0 = g0 / S.framesamples, f1 = (g1 - 1) / S.framesamples;
@@ -203,11 +254,33 @@ __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintS
 				int64_t wa = a < nearest ? nearest : a;
 				int64_t wb = b > (int64_t)nearest + N ? (int64_t)nearest + N : b;
 				if(wb > wa)
+				{
 					count += (int)(wb - wa);
+					const uint32_t bo = (pb && bandok) ? bandok[(int64_t)s * valid_stride + fr] : 0xFFFFFFFFu;
+					if(bo != 0xFFFFFFFFu)
+						for(int b = 0; b < S.nband; b++)
+							if(!((bo >> b) & 1u))
+							{
+								inv[b] += (int)(wb - wa);
+								totinv += (int)(wb - wa);
+							}
+				}
 			}
 		}
 	}
 	float weight = __fdiv_rn((float)count, (float)N);
+	if(pb)
+	{
+		// float arithmetic of the reference: goodsamples - invalid[b] per band,
+		// goodsamples - totalinvalid / nchan for the FFT's own weight
+		const float gs = (float)count;
+		for(int b = 0; b < S.nband; b++)
+			pb[b] = __fdiv_rn(__fsub_rn(gs, (float)inv[b]), (float)N);
+		weight = __fdiv_rn(__fsub_rn(gs, __fdiv_rn((float)totinv, (float)S.nband)), (float)N);
+		if(!(weight > 0.0f))
+			for(int b = 0; b < S.nband; b++)
+				pb[b] = 0.0f;
+	}
 	if(!(weight > 0.0f))
 	{
 		out[(int64_t)s * T + i] = p;
@@ -264,11 +337,11 @@ __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintS
 	out[(int64_t)s * T + i] = p;
 }
 
-void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8_t *valid, int64_t valid_stride,
-                        int S, cudaStream_t stream)
+void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8_t *valid, uint32_t *bandok,
+                        int64_t valid_stride, int S, cudaStream_t stream)
 {
 	dim3 grid((unsigned)((valid_stride + 255) / 256 < 64 ? (valid_stride + 255) / 256 : 64), S);
-	k_frame_valid<<<grid, 256, 0, stream>>>(st, sub, valid, valid_stride);
+	k_frame_valid<<<grid, 256, 0, stream>>>(st, sub, valid, bandok, valid_stride);
 }
 
 void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, cudaStream_t stream)
@@ -277,11 +350,12 @@ void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, in
 }
 
 void launch_fft_params(const DevStation *st, const DevSubintStation *sub, const int32_t *validflags, int nflagint,
-                       const uint8_t *valid, int64_t valid_stride, int S, int T, int order, FftParam *out,
-                       cudaStream_t stream)
+                       const uint8_t *valid, const uint32_t *bandok, int64_t valid_stride, int S, int T, int order,
+                       FftParam *out, float *pbw, int nbm, cudaStream_t stream)
 {
 	dim3 grid((T + 127) / 128, S);
-	k_fft_params<<<grid, 128, 0, stream>>>(st, sub, validflags, nflagint, valid, valid_stride, T, order, out);
+	k_fft_params<<<grid, 128, 0, stream>>>(st, sub, validflags, nflagint, valid, bandok, valid_stride, T, order, out,
+	                                       pbw, nbm);
 }
 
 }  // namespace fxb

@@ -224,7 +224,8 @@ struct FftConst {
 	uint32_t fa, so;                     // first frame of the window, window start within it
 	uint32_t fmask;                      // validity of the window's frames (bit k: frame fa + k)
 	int32_t stuck;                       // samples [stuck, N) read as zero
-	int32_t flags;                       // 1: valid FFT, 2: fmask covers the window
+	int32_t flags;                       // 1: valid FFT, 2: fmask covers the window,
+	                                     // 4: a valid frame of the window blanks one of the item's bands
 };
 
 // One middle radix-8 pass (stride s = 2^LOGS, m = N / (8 s)) over the
@@ -444,6 +445,20 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 			c.fmask = __ballot_sync(0xffffffffu, v);
 			if(nwf <= 32)
 				c.flags |= 2;
+			if(a.bandok)
+			{
+				// EDV4-blanked bands (INTERLACEDVDIF): the slow decode path below
+				const uint32_t need = (1u << g.band[0]) | (g.band[1] >= 0 ? 1u << g.band[1] : 0u);
+				bool part = false;
+				for(uint32_t k = (uint32_t)lane; (c.flags & 1) && k < nwf; k += 32)
+				{
+					const int64_t fk = (int64_t)c.fa + k;
+					part = part || (fk < a.valid_stride && vrow[fk] != 0 &&
+					                (a.bandok[(int64_t)g.station * a.valid_stride + fk] & need) != need);
+				}
+				if(__any_sync(0xffffffffu, part))
+					c.flags |= 4;
+			}
 			if(lane == 0)
 				fcs[f] = c;
 		}
@@ -463,6 +478,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 		const float stc = fc.stc, sts = fc.sts;
 		const float dfs = fc.dfs, postf = fc.postf;
 		const bool narrow = (fc.flags & 2) != 0;
+		const bool blank = (fc.flags & 4) != 0;
 		// ---- 1-3. decode, fringe-rotate and run the first radix-8 pass (s = 1:
 		// butterfly b, twiddle w_N^(r b)), one butterfly at a time
 		{
@@ -540,6 +556,16 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 								const uint32_t w1 = (oneword ? raw0[r] : raw1[r]) >> ((pk[r] >> 8) & 31u);
 								v1 = nbits == 2 ? level2(w1 & 3u) : lut8[w1 & 255u];
 							}
+						}
+						if(blank)
+						{
+							// bands of this sample's frame blanked by its EDV4 validity mask
+							// (blank_vdif_EDV4, format_vdif.c:4699-4780)
+							const uint32_t bo = a.bandok[(int64_t)g.station * a.valid_stride + fa + (so + (uint32_t)n) / fs];
+							if(!((bo >> g.band[0]) & 1u))
+								v0 = 0.0f;
+							if(g.band[1] >= 0 && !((bo >> g.band[1]) & 1u))
+								v1 = 0.0f;
 						}
 					}
 					float sn = 0.0f, cs = 1.0f;

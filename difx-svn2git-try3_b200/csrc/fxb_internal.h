@@ -47,6 +47,7 @@ struct DevStation {
 	int32_t fftchannels;    // 2*nchan
 	int32_t asl;            // array stride length (calcstridelength(nchan))
 	int32_t sticky;         // 8-bit 2/4-channel blank semantics
+	int32_t mux;            // INTERLACEDVDIF: per-band weights, EDV4 band blanking
 	int32_t bpbn, bpbd;     // bytes-per-block numerator/denominator of Mode
 	double bw;              // MHz
 	double sampletime;      // us
@@ -88,6 +89,7 @@ struct Job {
 		std::vector<char> zoom_pol;
 		int nzoom() const { return (int)zoom_freq.size(); }
 		float pcal_interval = 0.0f, pcal_base = 0.0f;   // phase-cal comb (MHz), float as the reference
+		int mux_threads = 0;                           // INTERLACEDVDIF: per-band data weights
 		// frequency of band k: recorded bands, then zoom bands
 		int total_freq(int k) const { return k < nband ? band_freq[k] : zoom_freq[k - nband]; }
 		char total_pol(int k) const { return k < nband ? band_pol[k] : zoom_pol[k - nband]; }
@@ -162,8 +164,11 @@ struct Job {
 	int64_t pcal_bins = 0;
 	std::vector<int64_t> pcoff;   // core-result offset of each station's tones, -1 without phase cal
 	// weight plans
-	struct BWeight { int s1, s2; int64_t dst_float; };
+	// band indices pick the per-band data weights of INTERLACEDVDIF stations
+	struct BWeight { int s1, s2, b1, b2; int64_t dst_float; };
 	std::vector<BWeight> bweights;
+	// both autocorrelation passes carry the band's own weight (Core writes
+	// Mode::getWeight(false, band) for each, core.cpp:1324-1357)
 	struct ACWeight { int s; int band; int64_t dst_float; };
 	std::vector<ACWeight> acweights;
 };

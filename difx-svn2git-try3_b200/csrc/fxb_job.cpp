@@ -287,6 +287,13 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 			return fail(err, st, FXB_ERR_ARG, "bad phase-cal interval");
 		o.pcal_interval = (float)in.pcal_interval_mhz;
 		o.pcal_base = (float)in.pcal_base_mhz;
+		if(in.mux_threads < 0)
+			return fail(err, st, FXB_ERR_ARG, "bad mux thread count");
+		if(in.mux_threads > 0 && (in.mux_threads != in.nband || in.nbits != 2 || in.nband > 32 || in.nzoom > 0 ||
+		                          o.pcal_interval > 0.0f))
+			return fail(err, st, FXB_ERR_UNSUPPORTED,
+			            "INTERLACEDVDIF needs one 2-bit band per thread, at most 32, without zoom bands or phase cal");
+		o.mux_threads = in.mux_threads;
 		job.stations.push_back(o);
 	}
 	for(int b = 0; b < d->nbaseline; b++)
@@ -536,7 +543,9 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 	const int T = job.blockspersend;
 	std::vector<std::vector<int>> crossout(S);     // [s][band] -> cross-pol output index, -1
 	for(int s = 0; s < S; s++)
+	{
 		crossout[s].assign(job.stations[s].nband + job.stations[s].nzoom(), -1);
+	}
 	int64_t spec = 0, acc = 0;
 	for(int f = 0; f < F; f++)
 	{
@@ -590,7 +599,7 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 				job.outmap.push_back({acc + (int64_t)o * pl.nchan,
 				                      job.bloff[(size_t)f * B + b] + (int64_t)pf * pl.nchan / job.freqs[f].chans_to_avg,
 				                      pl.nchan, job.freqs[f].chans_to_avg, f, o});
-				job.bweights.push_back({bl.ds1, bl.ds2, 2 * job.bwoff[(size_t)f * B + b] + pf});
+				job.bweights.push_back({bl.ds1, bl.ds2, bl.prod_b1[p], bl.prod_b2[p], 2 * job.bwoff[(size_t)f * B + b] + pf});
 				pf++;
 			}
 		}

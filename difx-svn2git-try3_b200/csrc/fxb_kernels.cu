@@ -336,8 +336,12 @@ void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, 
 // in FFT order as Core does.  One warp per weight: the lanes load and multiply
 // 256 FFTs at a time in parallel, then lane 0 adds them in order (adding 0 for
 // an invalid FFT leaves a non-negative float sum unchanged).
+// INTERLACEDVDIF stations weigh each band by its own data weight
+// (Mode::getDataWeight, mode.h:168, mode.cpp:1300-1303).
 __global__ void k_weights(const DevBWeight *__restrict__ bw, int nbw, const DevACWeight *__restrict__ acw, int nacw,
-                          const FftParam *__restrict__ params, int T, float *__restrict__ bwacc, float *__restrict__ acwacc)
+                          const FftParam *__restrict__ params, const float *__restrict__ pbw, int nbm,
+                          const DevStation *__restrict__ st, int T, float *__restrict__ bwacc,
+                          float *__restrict__ acwacc)
 {
 	__shared__ float buf[4][256];
 	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -347,6 +351,10 @@ __global__ void k_weights(const DevBWeight *__restrict__ bw, int nbw, const DevA
 	const bool isb = k < nbw;
 	const FftParam *p1 = params + (int64_t)(isb ? bw[k].s1 : acw[k - nbw].s) * T;
 	const FftParam *p2 = params + (int64_t)(isb ? bw[k].s2 : 0) * T;
+	const int sa = isb ? bw[k].s1 : acw[k - nbw].s, sb = isb ? bw[k].s2 : sa;
+	const int ba = isb ? bw[k].b1 : acw[k - nbw].band, bb = isb ? bw[k].b2 : -1;
+	const float *wa = (pbw && st[sa].mux) ? pbw + (int64_t)sa * T * nbm + ba : nullptr;
+	const float *wb = (pbw && st[sb].mux && bb >= 0) ? pbw + (int64_t)sb * T * nbm + bb : nullptr;
 	float sum = 0.0f;
 	for(int t0 = 0; t0 < T; t0 += 256)
 	{
@@ -355,10 +363,13 @@ __global__ void k_weights(const DevBWeight *__restrict__ bw, int nbw, const DevA
 		{
 			const int t = t0 + j;
 			float v;
+			const float w1 = wa ? wa[(int64_t)t * nbm] : p1[t].weight;
 			if(isb)
-				v = __fmul_rn(p1[t].weight, p2[t].weight);
+				v = __fmul_rn(w1, wb ? wb[(int64_t)t * nbm] : p2[t].weight);
+			else if(p1[t].status != kFftOk)
+				v = 0.0f;
 			else
-				v = p1[t].status == kFftOk ? p1[t].weight : 0.0f;
+				v = w1;
 			buf[w][j] = v;
 		}
 		__syncwarp();
@@ -376,13 +387,14 @@ __global__ void k_weights(const DevBWeight *__restrict__ bw, int nbw, const DevA
 	}
 }
 
-void launch_weights(const DevBWeight *bw, int nbw, const DevACWeight *acw, int nacw, const FftParam *params, int T,
-                    float *bwacc, float *acwacc, cudaStream_t stream)
+void launch_weights(const DevBWeight *bw, int nbw, const DevACWeight *acw, int nacw, const FftParam *params,
+                    const float *pbw, int nbm, const DevStation *st, int T, float *bwacc, float *acwacc,
+                    cudaStream_t stream)
 {
 	int n = nbw + nacw;
 	if(n == 0)
 		return;
-	k_weights<<<(n + 3) / 4, 128, 0, stream>>>(bw, nbw, acw, nacw, params, T, bwacc, acwacc);
+	k_weights<<<(n + 3) / 4, 128, 0, stream>>>(bw, nbw, acw, nacw, params, pbw, nbm, st, T, bwacc, acwacc);
 }
 
 // Core-result assembly (core.cpp:1774-1802 channel averaging, 1266-1363):

@@ -32,12 +32,12 @@ struct DevOutMap {
 };
 
 struct DevBWeight {
-	int32_t s1, s2;
+	int32_t s1, s2, b1, b2;   // stations and recorded bands
 	int64_t dst;
 };
 
 struct DevACWeight {
-	int32_t s, pad;
+	int32_t s, band;          // station and band (per-band weights of INTERLACEDVDIF stations)
 	int64_t dst;
 };
 
@@ -47,13 +47,14 @@ struct DevZoomCopy {
 	int32_t src_plan, src_row, dst_plan, dst_row, choff, nchan;
 };
 
-void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8_t *valid, int64_t valid_stride,
-                        int S, cudaStream_t stream);
+// bandok (may be null): per frame, the bands that keep their samples
+void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8_t *valid, uint32_t *bandok,
+                        int64_t valid_stride, int S, cudaStream_t stream);
 // the subint time is read from sub[s].subsec / subns
 void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, cudaStream_t stream);
 void launch_fft_params(const DevStation *st, const DevSubintStation *sub, const int32_t *validflags, int nflagint,
-                       const uint8_t *valid, int64_t valid_stride, int S, int T, int order, FftParam *out,
-                       cudaStream_t stream);
+                       const uint8_t *valid, const uint32_t *bandok, int64_t valid_stride, int S, int T, int order,
+                       FftParam *out, float *pbw, int nbm, cudaStream_t stream);
 
 // Fused unpack -> fringe rotation -> FFT -> fractional-sample correction.
 // One CTA per (station, FFT); writes FP32 spectra into spec.
@@ -93,6 +94,7 @@ struct FsArgs {
 	const FGroup *groups;
 	const DevFreqPlan *plans;
 	const uint8_t *valid;
+	const uint32_t *bandok;       // per frame: bands that keep their samples (null: all)
 	int64_t valid_stride;
 	const FftParam *params;
 	const void *tw;          // set from FKind::tw by launch_fstage_kind
@@ -192,8 +194,10 @@ void launch_pcal_final(const DevPcalBand *bands, int nbands, int nchunk, int64_t
 void launch_zoom_gather(const DevZoomCopy *zc, int nzc, const DevFreqPlan *plans, int T, bool tc, void *spec,
                         cudaStream_t stream);
 
-void launch_weights(const DevBWeight *bw, int nbw, const DevACWeight *acw, int nacw, const FftParam *params, int T,
-                    float *bwacc, float *acwacc, cudaStream_t stream);
+// pbw: per-band data weights [station][FFT][nbm] of INTERLACEDVDIF stations (null: none)
+void launch_weights(const DevBWeight *bw, int nbw, const DevACWeight *acw, int nacw, const FftParam *params,
+                    const float *pbw, int nbm, const DevStation *st, int T, float *bwacc, float *acwacc,
+                    cudaStream_t stream);
 
 void launch_finalise(const DevOutMap *om, int nom, int maxout, const float2 *acc, const DevBWeight *bw, int nbw,
                      const float *bwacc, const DevACWeight *acw, int nacw, const float *acwacc, float2 *core,

@@ -234,9 +234,9 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
 		return FXB_ERR_CUDA;
 
 	launch_interpolators(d_st, d_sub, 1, T, cs);
-	launch_frame_valid(d_st, d_sub, d_valid, valid_stride, 1, cs);
-	launch_fft_params(d_st, d_sub, d_flags, nflagint, d_valid, valid_stride, 1, T, fringe_rot_order,
-	                  d_params, cs);
+	launch_frame_valid(d_st, d_sub, d_valid, nullptr, valid_stride, 1, cs);
+	launch_fft_params(d_st, d_sub, d_flags, nflagint, d_valid, nullptr, valid_stride, 1, T, fringe_rot_order,
+	                  d_params, nullptr, 0, cs);
 	launch_fstage(d_st, d_sub, d_bands, st.nband, d_plans, d_valid, valid_stride, d_params, d_tw, N, 1, T,
 	              fringe_rot_order, fraclo, N, (float2 *)dev_spectra, cs);
 	if(dev_weights)

@@ -59,6 +59,10 @@ class Station:
     # shifted by pcal_base_mhz
     pcal_interval_mhz: float = 0.0
     pcal_base_mhz: float = 0.0
+    # INTERLACEDVDIF: threads of one band each muxed into the frames (0: plain
+    # VDIF); data weights are then per band, and EDV4 validity masks in the
+    # frame headers blank absent bands
+    mux_threads: int = 0
 
     def recorded_freqs(self) -> List[int]:
         seen: List[int] = []

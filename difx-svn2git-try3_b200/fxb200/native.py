@@ -32,7 +32,7 @@ class FxbFreq(ctypes.Structure):
 class FxbStation(ctypes.Structure):
     _fields_ = [("nbits", ctypes.c_int32), ("payload_bytes", ctypes.c_int32), ("header_bytes", ctypes.c_int32),
                 ("nband", ctypes.c_int32), ("band_freq", ctypes.POINTER(ctypes.c_int32)),
-                ("band_pol", ctypes.c_char_p), ("nzoom", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("band_pol", ctypes.c_char_p), ("nzoom", ctypes.c_int32), ("mux_threads", ctypes.c_int32),
                 ("zoom_freq", ctypes.POINTER(ctypes.c_int32)), ("zoom_pol", ctypes.c_char_p),
                 ("pcal_interval_mhz", ctypes.c_double), ("pcal_base_mhz", ctypes.c_double)]
 
@@ -71,7 +71,7 @@ class DescHolder:
             self.keep += [bf, bp, zf, zp]
             st[i] = FxbStation(s.nbits, s.payload_bytes, s.header_bytes, s.nband,
                                ctypes.cast(bf, ctypes.POINTER(ctypes.c_int32)), ctypes.cast(bp, ctypes.c_char_p),
-                               nz, 0, ctypes.cast(zf, ctypes.POINTER(ctypes.c_int32)),
+                               nz, s.mux_threads, ctypes.cast(zf, ctypes.POINTER(ctypes.c_int32)),
                                ctypes.cast(zp, ctypes.c_char_p), s.pcal_interval_mhz, s.pcal_base_mhz)
         bl = (FxbBaseline * len(job.baselines))()
         for i, b in enumerate(job.baselines):

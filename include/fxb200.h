@@ -80,7 +80,12 @@ typedef struct {
 	const int32_t *band_freq; /* [nband] frequency-table index of each band */
 	const char *band_pol;     /* [nband] 'R'/'L'/'X'/'Y' */
 	int32_t nzoom;            /* zoom bands (0: none; the pointers may be null) */
-	int32_t reserved;
+	int32_t mux_threads;      /* INTERLACEDVDIF: threads of one band each, muxed into the frames
+	                           * passed (0: plain VDIF).  Data weights are then per band
+	                           * (Mk5Mode::unpack, mk5mode.cpp:145-166): a band of a valid frame whose
+	                           * header carries an EDV4 validity mask without the band's bit is
+	                           * blanked; baselines weigh w1(band1) * w2(band2) (core.cpp:1032).
+	                           * 2-bit only, no zoom bands, no phase cal. */
 	const int32_t *zoom_freq; /* [nzoom] frequency-table index of each zoom band */
 	const char *zoom_pol;     /* [nzoom] polarisation of each zoom band */
 	/* Phase-cal extraction (PHASE CAL INT (MHZ), PHASE CAL BASE(MHZ);

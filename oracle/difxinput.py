@@ -91,9 +91,16 @@ def write_job_files(job: Job, outdir: str, name: str = "job",
         s.append(_kv("TELESCOPE INDEX", i))
         ts = 0.0 if tsys is None else (tsys[i] if hasattr(tsys, "__len__") else tsys)
         s.append(_kv("TSYS", "%.6f" % ts))
-        s.append(_kv("DATA FORMAT", "VDIF"))
-        s.append(_kv("QUANTISATION BITS", st.nbits))
-        s.append(_kv("DATA FRAME SIZE", st.payload_bytes + st.header_bytes))
+        if st.mux_threads:
+            # the frames handed to the Mode are the muxer's; the .input names
+            # the threads and their own frame size (configuration.cpp:1517-1525, 1001-1009)
+            s.append(_kv("DATA FORMAT", "INTERLACEDVDIF/" + ":".join(str(k) for k in range(st.mux_threads))))
+            s.append(_kv("QUANTISATION BITS", st.nbits))
+            s.append(_kv("DATA FRAME SIZE", st.payload_bytes // st.mux_threads + st.header_bytes))
+        else:
+            s.append(_kv("DATA FORMAT", "VDIF"))
+            s.append(_kv("QUANTISATION BITS", st.nbits))
+            s.append(_kv("DATA FRAME SIZE", st.payload_bytes + st.header_bytes))
         s.append(_kv("DATA SAMPLING", "REAL"))
         s.append(_kv("DATA SOURCE", "FILE"))
         s.append(_kv("FILTERBANK USED", "FALSE"))

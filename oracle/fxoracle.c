@@ -72,6 +72,7 @@ typedef struct fxo_job {
 	fxb_freq *freqs;
 	/* stations */
 	int *nbits, *payload, *header, *nband;
+	int *mux;                                         /* INTERLACEDVDIF: per-band weights */
 	int **band_freq;
 	char **band_pol;
 	int *nzoom;
@@ -355,6 +356,7 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 	j->freqs = (fxb_freq *)malloc(sizeof(fxb_freq) * d->nfreq);
 	memcpy(j->freqs, d->freqs, sizeof(fxb_freq) * d->nfreq);
 	j->nbits = (int *)calloc(d->nstation, sizeof(int));
+	j->mux = (int *)calloc(d->nstation, sizeof(int));
 	j->payload = (int *)calloc(d->nstation, sizeof(int));
 	j->header = (int *)calloc(d->nstation, sizeof(int));
 	j->nband = (int *)calloc(d->nstation, sizeof(int));
@@ -365,6 +367,7 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 	{
 		const fxb_station *st = &d->stations[s];
 		j->nbits[s] = st->nbits;
+		j->mux[s] = st->mux_threads > 0;
 		j->payload[s] = st->payload_bytes;
 		j->header[s] = st->header_bytes;
 		j->nband[s] = st->nband;
@@ -620,7 +623,7 @@ void fxo_destroy(fxo_job *j)
 		free(j->prod_b1[i]);
 		free(j->prod_b2[i]);
 	}
-	free(j->freqs); free(j->nbits); free(j->payload); free(j->header); free(j->nband);
+	free(j->freqs); free(j->nbits); free(j->payload); free(j->header); free(j->nband); free(j->mux);
 	free(j->band_freq); free(j->band_pol); free(j->poly);
 	free(j->nzoom); free(j->zoom_freq); free(j->zoom_parent); free(j->zoom_choff);
 	free(j->pcal_interval); free(j->pcal_base); free(j->pc_ntones); free(j->pc_nbins); free(j->pc_first);
@@ -705,7 +708,71 @@ typedef struct {
 	int nearestsample;
 	float weight;
 	double fracsampleerror;
+	float pb[MAXBAND];   /* per-band data weights (INTERLACEDVDIF), Mk5Mode::perbandweights */
 } fft_info;
+
+/* blank_vdif_EDV4 (format_vdif.c:4699-4780) on decoded samples out[nchan][nsamp]
+ * from sample offsetsamples: in every frame whose invalid bit is clear and
+ * whose EDV4 validity mask lacks bit c / d (d = channels / mask length), the
+ * nonzero samples of band c are zeroed and counted in invalid[c].  The
+ * geometry (EDV version, mask length, channels, frame length, bits) is read
+ * from the buffer's first frame, as the reference does; the C int shift
+ * 1 << 31 tests mask bits 31-63, and a 32-channel "good" mask (1 << 32) - 1
+ * is 0 on x86.  Frames past nbytes hold no samples (the decoder zeroed
+ * them).  Headers whose geometry is not the station's blank nothing. */
+static void blank_edv4(const uint8_t *data, int64_t nbytes, int payload, int header, int nchan, int nbits,
+                       int64_t offsetsamples, int nsamp, float *out, int *invalid)
+{
+	uint32_t w2, w3, w4;
+	int ml, nch, flen, spf, d, c, v = 0;
+	const int64_t stride = nsamp;          /* row length of out; nsamp counts down below */
+	int64_t fr, start, end, s;
+	for(c = 0; c < nchan; c++) invalid[c] = 0;
+	if(nbytes < 32) return;
+	memcpy(&w2, data + 8, 4); memcpy(&w3, data + 12, 4); memcpy(&w4, data + 16, 4);
+	ml = (int)((w4 >> 16) & 0xFF);
+	if((w4 >> 24) != 4 || ml < 1 || ml > 64) return;
+	nch = 1 << ((w2 >> 24) & 31);
+	flen = (int)(w2 & 0xFFFFFF) * 8;
+	spf = (flen - 32) * 8 / (nch * (int)(((w3 >> 26) & 31) + 1));
+	d = nch / ml;
+	if(d < 1 || nch != nchan || flen != payload + header || (int64_t)spf != (int64_t)payload * 8 / (nchan * nbits))
+		return;
+	fr = offsetsamples / spf;
+	start = offsetsamples % spf;
+	end = start + nsamp < spf ? start + nsamp : spf;
+	for(;;)
+	{
+		int64_t n = end - start;
+		if((fr + 1) * flen <= nbytes)
+		{
+			const uint8_t *h = data + fr * flen;
+			uint32_t w0;
+			uint64_t mask, good = nch < 32 ? (uint64_t)((1u << nch) - 1u) : 0u;
+			memcpy(&w0, h, 4);
+			memcpy(&mask, h + 24, 8);
+			if(!((w0 >> 31) & 1) && mask != good)
+				for(c = 0; c < nchan; c++)
+				{
+					int q = c / d;
+					int keep = q < 31 ? (int)((mask >> q) & 1) : (mask & 0xFFFFFFFF80000000ULL) != 0;
+					if(keep) continue;
+					for(s = 0; s < n; s++)
+						if(out[(int64_t)c * stride + s + v] != 0.0f)
+						{
+							out[(int64_t)c * stride + s + v] = 0.0f;
+							invalid[c]++;
+						}
+				}
+		}
+		nsamp -= (int)n;
+		if(nsamp <= 0) break;
+		v += (int)n;
+		fr++;
+		start = 0;
+		end = nsamp < spf ? nsamp : spf;
+	}
+}
 
 /* Mode::process for station s, FFT index i (mode.cpp:649-1397, orders 0-2,
  * real-sampled USB/LSB).  spec receives [nband][nchan] complex.
@@ -772,6 +839,18 @@ static fft_info mode_process(const fxo_job *j, int s, const uint8_t *buf, int64_
 					for(c = 0; c < nb; c++)
 						if(scratch[(int64_t)c * samplestounpack + t] != 0.0f) { scratch[(int64_t)c * samplestounpack + t] = 0.0f; erased++; }
 				good -= erased / (float)nb;
+			}
+			if(j->mux[s])
+			{
+				/* per-band weights (mk5mode.cpp:145-166) */
+				int inv[MAXBAND], tot = 0;
+				blank_edv4(buf, nbytes, j->payload[s], j->header[s], nb, nbits, *ups, samplestounpack, scratch, inv);
+				for(c = 0; c < nb; c++)
+				{
+					info.pb[c] = (good - inv[c]) / (float)unpacksamples;
+					tot += inv[c];
+				}
+				good -= (float)tot / (float)nb;
 			}
 			if(good < 0) good = 0;
 			info.weight = good / (float)unpacksamples;
@@ -884,6 +963,10 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 	double **acc_ac = (double **)calloc(S, sizeof(double *));     /* [band][2][nchan][2] */
 	float **acw = (float **)calloc(S, sizeof(float *));           /* [band][2], float as Mode::weights */
 	float *w = (float *)calloc((size_t)S * T, sizeof(float));
+	float *pbw = NULL;                                            /* [s][t][band], INTERLACEDVDIF only */
+	for(s = 0; s < S; s++)
+		if(j->mux[s] && !pbw)
+			pbw = (float *)calloc((size_t)S * T * MAXBAND, sizeof(float));
 	int *ups = (int *)calloc(S, sizeof(int));
 	int *badsub = (int *)calloc(S, sizeof(int));
 	double (*interp)[3] = (double (*)[3])calloc(S, sizeof(double[3]));
@@ -929,6 +1012,8 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 			fft_info fi = mode_process(j, s, bufs[s], nbytes[s], datasec[s], datans[s], vf, sec, ns, badsub[s],
 			                           interp[s], t, &ups[s], sp, scratch, work);
 			w[(size_t)s * T + t] = fi.weight;
+			if(pbw)
+				memcpy(pbw + ((size_t)s * T + t) * MAXBAND, fi.pb, sizeof(fi.pb));
 			if(fi.status != 1)
 			{
 				w[(size_t)s * T + t] = fi.status == 1 ? fi.weight : 0.0f;
@@ -974,7 +1059,7 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 					dcx v = sp[(size_t)b * nchan + c];
 					ac[2 * c] += v.re * v.re + v.im * v.im;
 				}
-				acw[s][2 * b] += fi.weight;
+				acw[s][2 * b] += j->mux[s] ? fi.pb[b] : fi.weight;
 			}
 			if(j->write_autocorrs)
 			{
@@ -996,7 +1081,7 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 								ac[2 * c] += x0.re * x1.re + x0.im * x1.im;
 								ac[2 * c + 1] += x0.im * x1.re - x0.re * x1.im;
 							}
-							acw[s][2 * b0 + 1] += fi.weight;
+							acw[s][2 * b0 + 1] += j->mux[s] ? fi.pb[b0] * fi.pb[b1] : fi.weight;
 						}
 					}
 				}
@@ -1037,7 +1122,8 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 				coreresult[2 * (base + (int64_t)pf * nchan / avg + c / avg) + 1] += im / avg;
 			}
 			for(t = 0; t < T; t++)
-				wsum += w[(size_t)s1 * T + t] * w[(size_t)s2 * T + t];
+				wsum += (j->mux[s1] ? pbw[((size_t)s1 * T + t) * MAXBAND + k1] : w[(size_t)s1 * T + t]) *
+				        (j->mux[s2] ? pbw[((size_t)s2 * T + t) * MAXBAND + k2] : w[(size_t)s2 * T + t]);
 			coreresult[2 * j->bwoff[f * B + b] + pf] += wsum;
 			pf++;
 		}
@@ -1140,7 +1226,7 @@ int fxo_process_subint(const fxo_job *j, const uint8_t *const *bufs, const int64
 	if(fftweights)
 		memcpy(fftweights, w, sizeof(float) * (size_t)S * T);
 	for(s = 0; s < S; s++) { free(spec[s]); free(acc_ac[s]); free(acw[s]); free(allvalid[s]); }
-	free(spec); free(acc_ac); free(acw); free(w); free(ups); free(badsub); free(interp); free(allvalid);
+	free(spec); free(acc_ac); free(acw); free(w); free(pbw); free(ups); free(badsub); free(interp); free(allvalid);
 	free(scratch); free(work);
 	return 0;
 }

@@ -130,3 +130,43 @@ PCAL_JOBS = {
     "pcal_lsb": lambda: pcal_job(nstation=2, nfreq=2, full_pol=True, lsb=True, subint_ns=2_048_000),
     "pcal_lsb_frac": lambda: pcal_job(nstation=2, lsb=True, freq0=8400.01),
 }
+
+
+def mux_job(masklength=None, **kw) -> Job:
+    """small_job whose stations 0 and 2 are INTERLACEDVDIF (one band per
+    thread, muxed frames handed over); masklength: the EDV4 mask length that
+    edv4_inputs writes (default: one bit per band)."""
+    kw = dict(dict(nstation=3, nfreq=2, full_pol=True, subint_ns=2_048_000), **kw)
+    job = small_job(**kw)
+    for s in (0, 2):
+        job.stations[s].mux_threads = job.stations[s].nband
+    job.edv4_masklength = masklength or job.stations[0].nband
+    return job
+
+
+def edv4_inputs(job: Job, inputs, seed=5):
+    """Write EDV4 headers (version 4, the job's mask length, sync word, a
+    validity mask per frame: mostly complete, some frames missing one or two
+    bit groups) into the frames of the INTERLACEDVDIF stations."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s, (buf, dsec, dns) in enumerate(inputs):
+        st = job.stations[s]
+        if not st.mux_threads:
+            out.append((buf, dsec, dns))
+            continue
+        fb = st.payload_bytes + st.header_bytes
+        fr = buf.copy().reshape(-1, fb)
+        ml = job.edv4_masklength
+        full = (1 << ml) - 1
+        masks = np.full(len(fr), full, dtype=np.uint64)
+        for k in rng.choice(len(fr), size=max(1, len(fr) // 3), replace=False):
+            drop = rng.choice(ml, size=int(rng.integers(1, 3)), replace=False)
+            masks[k] = full & ~int(sum(1 << int(b) for b in drop))
+        words = fr[:, :32].copy().view(np.uint32)
+        words[:, 4] = (4 << 24) | (ml << 16)
+        words[:, 5] = 0xACABFEED
+        fr[:, :32] = words.view(np.uint8)
+        fr[:, 24:32] = masks.reshape(-1, 1).view(np.uint8)
+        out.append((fr.reshape(-1), dsec, dns))
+    return out

@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 
 from fxb200 import synth
-from helpers import PCAL_JOBS, compare_core, mixed_bw_zoom_job, rel_err, small_job, zoom_job
+from helpers import (PCAL_JOBS, compare_core, edv4_inputs, mixed_bw_zoom_job, mux_job, regions, rel_err, small_job,
+                     zoom_job)
 
 import fxoracle
 import refcorr
@@ -84,6 +85,52 @@ def test_pcal_subint_matches_reference(name):
     o = orc.process_subint(inputs, sec, ns, validflags=vf)
     errs = compare_core(job, orc.layout(), orc.corelen, r.astype(np.float64), o, tol=2e-6)
     assert "pcal" in errs
+
+
+@pytest.mark.parametrize("masklength", [4, 2])
+def test_interlaced_vdif_per_band_weights_match_reference(masklength):
+    # INTERLACEDVDIF stations: per-band data weights (mk5mode.cpp:145-166) from
+    # the frames' EDV4 validity masks (format_vdif.c:4699-4780), baseline and
+    # autocorrelation weights from them (core.cpp:1032, mode.cpp:1300-1303); one station also has invalid frames.
+    job = mux_job(masklength=masklength)
+    ref = refcorr.RefCorrelator(job)
+    orc = fxoracle.OracleCorrelator(job)
+    assert np.array_equal(ref.layout(), orc.layout())
+    sec, ns = 0, 1_024_000
+    f0 = synth.subint_window(job, 0, sec, ns)[0]
+    inputs = edv4_inputs(job, synth.subint_inputs(job, sec, ns, rho=0.05, seed=7, invalid={0: [f0 + 2, f0 + 9]}))
+    vf = [synth.valid_flags(job) for _ in job.stations]
+    r = ref.process_subint(inputs, vf, 0, sec, ns)
+    o = orc.process_subint(inputs, sec, ns, validflags=vf)
+    reg = dict(regions(job, orc.layout(), orc.corelen))
+    for name in ("bweight", "acweight"):
+        assert np.array_equal(o[reg[name]].astype(np.float32), r[reg[name]]), name
+    plain = fxoracle.OracleCorrelator(job_without_mux(job)).process_subint(inputs, sec, ns, validflags=vf)
+    assert not np.array_equal(o[reg["acweight"]], plain[reg["acweight"]])
+    compare_core(job, orc.layout(), orc.corelen, r.astype(np.float64), o, tol=2e-6)
+
+
+def test_interlaced_vdif_full_masks_match_reference():
+    # EDV4 headers whose masks keep every band: the whole subint as the reference's
+    job = mux_job()
+    ref = refcorr.RefCorrelator(job)
+    orc = fxoracle.OracleCorrelator(job)
+    sec, ns = 0, 1_024_000
+    inputs = edv4_inputs(job, synth.subint_inputs(job, sec, ns, rho=0.05, seed=7))
+    for s in (0, 2):
+        inputs[s][0].reshape(-1, job.frame_bytes(s))[:, 24:32] = np.frombuffer(np.uint64(15).tobytes(), np.uint8)
+    vf = [synth.valid_flags(job) for _ in job.stations]
+    r = ref.process_subint(inputs, vf, 0, sec, ns)
+    o = orc.process_subint(inputs, sec, ns, validflags=vf)
+    compare_core(job, orc.layout(), orc.corelen, r.astype(np.float64), o, tol=2e-6)
+
+
+def job_without_mux(job):
+    import copy
+    j = copy.deepcopy(job)
+    for st in j.stations:
+        st.mux_threads = 0
+    return j
 
 
 def test_mode_spectra_match_reference():
