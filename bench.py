@@ -55,13 +55,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fxb", choices=["fxb", "reference"])
-    ap.add_argument("--xmac", default="bf16", choices=["fp32", "bf16"],
-                    help="headline form: bf16 = tensor-core form (FP16 FFT, BF16 spectra, tcgen05 XMAC with FP32 "
-                         "accumulation), fp32 = the plain FP32 form; the other form is measured beside it")
+    ap.add_argument("--xmac", default="fp16", choices=["fp32", "fp16", "bf16"],
+                    help="headline form: fp16 = tensor-core form (FP16 spectra, tcgen05 XMAC with FP32 "
+                         "accumulation), bf16 = the same with BF16 spectra, fp32 = the plain FP32 form; the "
+                         "other form (FP32, or fp16 when the headline is FP32) is measured beside it")
     ap.add_argument("--no-other-form", "--no-tc-form", dest="no_other_form", action="store_true",
                     help="skip measuring the other form beside the headline")
     ap.add_argument("--subints-per-step", type=int, default=125)
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg (p50/p99 job latency)")
     ap.add_argument("--no-c3", action="store_true", help="skip the batched uneven-subband leg")
@@ -144,64 +144,101 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- reference CPU path
-def cpu_reference(job, pool, seconds_target, nthreads):
-    """Time the reference's own compiled CPU path (oracle/_ref) on a bounded
-    sample of the workload; returns (station.MHz/s, cores, sample text, kind)."""
-    import refcorr
-    vf = [synth.valid_flags(job) for _ in job.stations]
-    if refcorr.available():
-        ref = refcorr.RefCorrelator(job, nthreads=nthreads)
-        (sec, ns), inputs = pool[0]
-        out = np.zeros(2 * ref.corelen, dtype=np.float32)
+# One CPU sample definition for both arms: CPU_SAMPLE_SUBINTS consecutive
+# subints of the workload (cycling a pool of distinct subints) through one
+# reference correlator that has already processed one untimed subint.
+CPU_SAMPLE_SUBINTS = 24
+
+
+class CpuReference:
+    """The reference's own compiled CPU path (oracle/_ref) -- or, where it was
+    not built, the oracle's C restatement on one thread -- set up once for
+    the workload."""
+
+    def __init__(self, job, pool, nthreads):
+        import refcorr
+        self.job, self.pool = job, pool
+        self.vf = [synth.valid_flags(job) for _ in job.stations]
+        if refcorr.available():
+            self.ref = refcorr.RefCorrelator(job, nthreads=nthreads)
+            self.kind, self.cores, self.nthreads = "reference", nthreads, nthreads
+            self.out = np.zeros(2 * self.ref.corelen, dtype=np.float32)
+        else:
+            import fxoracle
+            self.ref = fxoracle.OracleCorrelator(job)
+            self.kind, self.cores, self.nthreads = "port", 1, 1
+        self.k = 0
+        self.one()                       # untimed: first-call set-up
+
+    def one(self):
+        (sec, ns), inputs = self.pool[self.k % len(self.pool)]
+        self.k += 1
+        if self.kind == "reference":
+            self.ref.process_subint(inputs, self.vf, 0, sec, ns, coreresult=self.out, nthreads=self.nthreads)
+        else:
+            self.ref.process_subint(inputs, sec, ns, validflags=self.vf)
+
+    def sample(self, nsub=CPU_SAMPLE_SUBINTS):
+        """Seconds of wall time for nsub subints, and the per-subint times."""
+        per = []
         t0 = time.perf_counter()
-        ref.process_subint(inputs, vf, 0, sec, ns, coreresult=out, nthreads=nthreads)
-        one = time.perf_counter() - t0
-        n = max(1, min(len(pool) * 4, int(seconds_target / max(one, 1e-3))))
-        t0 = time.perf_counter()
-        for k in range(n):
-            (sec, ns), inputs = pool[k % len(pool)]
-            ref.process_subint(inputs, vf, 0, sec, ns, coreresult=out, nthreads=nthreads)
-        dt = time.perf_counter() - t0
-        ref.close()
-        kind = "reference"
-        cores = nthreads
-    else:
-        import fxoracle
-        orc = fxoracle.OracleCorrelator(job)
-        n = 1
-        (sec, ns), inputs = pool[0]
-        t0 = time.perf_counter()
-        orc.process_subint(inputs, sec, ns, validflags=vf)
-        dt = time.perf_counter() - t0
-        kind = "port"
-        cores = 1
-    data_s = n * job.subint_ns * 1e-9
-    value = job.station_mhz_per_sec() * data_s / dt
-    sample = "%d subints x %.0f ms of the workload (%.3f s of data), %.1f s wall" % (n, job.subint_ns / 1e6, data_s, dt)
-    return value, cores, sample, kind
+        for _ in range(nsub):
+            t1 = time.perf_counter()
+            self.one()
+            per.append(time.perf_counter() - t1)
+        return time.perf_counter() - t0, per
+
+    def close(self):
+        if self.kind == "reference":
+            self.ref.close()
+
+    def describe(self, nsub, dt, per):
+        data_s = nsub * self.job.subint_ns * 1e-9
+        return ("%d consecutive subints x %.0f ms of the workload (%.3f s of data) through one reference "
+                "correlator after one untimed subint, %d host threads: %.2f s wall; per subint min/median/max "
+                "%.0f/%.0f/%.0f ms" % (nsub, self.job.subint_ns / 1e6, data_s, self.nthreads, dt,
+                                        1e3 * min(per), 1e3 * statistics.median(per), 1e3 * max(per)))
+
+
+def cpu_reference(job, pool, nthreads):
+    """One CPU sample; returns (station.MHz/s, cores, sample text, kind)."""
+    cr = CpuReference(job, pool, nthreads)
+    dt, per = cr.sample()
+    cr.close()
+    data_s = CPU_SAMPLE_SUBINTS * job.subint_ns * 1e-9
+    return job.station_mhz_per_sec() * data_s / dt, cr.cores, cr.describe(CPU_SAMPLE_SUBINTS, dt, per), cr.kind
 
 
 def reference_arm(args, job):
+    """The reference's CPU implementation of the path on all host threads:
+    each step is one CPU sample (CPU_SAMPLE_SUBINTS subints of the workload,
+    the same definition as the GPU arm's cpu_baseline); ms_per_step is the
+    measured wall time of a step."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    pool = make_pool(job, 4)
+    pool = make_pool(job, 8)
     nthreads = os.cpu_count() or 1
-    vals = []
-    t_all = []
-    for i in range(args.warmup + args.steps):
-        v, cores, sample, kind = cpu_reference(job, pool, max(2.0, args.cpu_seconds / max(1, args.steps)), nthreads)
-        if i >= args.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
+    cr = CpuReference(job, pool, nthreads)
+    for _ in range(args.warmup):
+        cr.sample()
+    dts, per_all = [], []
+    for _ in range(args.steps):
+        dt, per = cr.sample()
+        dts.append(dt)
+        per_all += per
+    cr.close()
+    data_step = CPU_SAMPLE_SUBINTS * job.subint_ns * 1e-9
+    value = job.station_mhz_per_sec() * data_step * len(dts) / sum(dts)
     rtf = value / job.station_mhz_per_sec()
+    sample = cr.describe(CPU_SAMPLE_SUBINTS * len(dts), sum(dts), per_all)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / rtf,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(dts) / len(dts),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "rtf": rtf,
+        "data": "synthetic", "rtf": rtf, "data_seconds_per_step": data_step,
         "config": workload_config(job),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cr.cores, "kind": cr.kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -209,7 +246,8 @@ def reference_arm(args, job):
 
 def workload_config(job):
     return {"workload": "c1: 10 stations x 8 x 32 MHz x 2 pol (full cross hands), 2-bit VDIF 16ch, "
-                        "1024 channels, 8 ms subints, 1 s of data per step",
+                        "1024 channels, 8 ms subints (GPU arm: 1 s of data per step; reference arm: "
+                        "%d subints per step)" % CPU_SAMPLE_SUBINTS,
             "stations": len(job.stations), "subbands": len(job.freqs), "bw_mhz": job.freqs[0].bw_mhz,
             "nchan": job.freqs[0].nchan, "fringe_rot_order": job.fringe_rot_order,
             "subint_ms": job.subint_ns / 1e6, "l2": "inputs larger than L2 (327 MB pool cycled)",
@@ -226,12 +264,14 @@ def load_traffic(kernel):
 
 
 def load_peaks():
+    """(HBM GB/s, burst dense bf16 TFLOP/s, sustained dense bf16 TFLOP/s, source)."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
             p = json.load(fh)
-        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+        return (float(p["hbm_gbs"]), float(p["bf16_tflops"]), float(p.get("bf16_tflops_sustained", 0.0)) or None,
+                "measured")
     except Exception:
-        return 6650.0, 1590.0, "fallback"
+        return 6650.0, 1590.0, 1400.0, "fallback"
 
 
 # ---------------------------------------------------------------- serving leg
@@ -293,9 +333,6 @@ def c3_leg(args):
     def run(form, batched):
         members = [Correlator(j, xmac=form, inflight=3) for j in jobs]
         batch = Batch(members) if batched else None
-        if not batched and form == "fp32":
-            for m in members:
-                m.set_graphs(False)
         # scheduling tuned online during the warm-up subints (results unchanged)
         for m in members:
             m.autotune(2)
@@ -351,10 +388,11 @@ def c3_leg(args):
                        "2/8-bit), dual pol with full cross hands, 8.192 ms subints, as %d jobs" % len(jobs),
            "station_mhz": smhz, "subints_timed": args.steps * nsub,
            "l2": "inputs larger than L2 (%d MB pool cycled)" % int(sum(sum(x[1]) for mm in meta for x in mm) / 1e6)}
-    out["tc_batched_graph"] = run(args.xmac if args.xmac != "fp32" else "bf16", True)
-    out["tc_per_job"] = run(args.xmac if args.xmac != "fp32" else "bf16", False)
-    out["fp32_per_job_eager"] = run("fp32", False)
-    out["tc_batched_vs_fp32"] = out["tc_batched_graph"]["rtf"] / out["fp32_per_job_eager"]["rtf"]
+    out["tc_batched_graph"] = run(args.xmac if args.xmac != "fp32" else "fp16", True)
+    out["tc_per_job"] = run(args.xmac if args.xmac != "fp32" else "fp16", False)
+    out["fp32_per_job"] = run("fp32", False)
+    out["tc_batched_vs_fp32"] = out["tc_batched_graph"]["rtf"] / out["fp32_per_job"]["rtf"]
+    out["note"] = "every form runs its subints as CUDA graphs (per job, or one per batch)"
     del dev
     torch.cuda.empty_cache()
     return out
@@ -386,7 +424,7 @@ def mux_leg(args):
     e1.record()
     e1.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    hbm_peak, _, src = load_peaks()
+    hbm_peak, _, _, src = load_peaks()
     gbs = (data.size + n) / (ms * 1e-3) / 1e9
     return {"workload": "16 threads x 1 channel, 2-bit, 64 Ms/s, 8000-byte payloads, one 0.5 s read (%d MB)"
                         % (data.size // 1000000),
@@ -568,7 +606,7 @@ def gpu_arm(args, job):
 
     # ---- the other form on the same workload (device-resident)
     other = None
-    other_name = "fp32" if args.xmac == "bf16" else "bf16"
+    other_name = "fp32" if args.xmac != "fp32" else "fp16"
     if not args.no_other_form:
         ctc = Correlator(job, xmac=other_name, inflight=3)
         ctc.autotune(2)
@@ -595,7 +633,7 @@ def gpu_arm(args, job):
         ctc.close()
         barrier()
     if other is not None:
-        tc_v, fp_v = (value, other["value"]) if args.xmac == "bf16" else (other["value"], value)
+        tc_v, fp_v = (value, other["value"]) if args.xmac != "fp32" else (other["value"], value)
         tc_vs_fp32 = tc_v / fp_v
     else:
         tc_vs_fp32 = None
@@ -612,7 +650,7 @@ def gpu_arm(args, job):
     T = job.blocks_per_send()
     rows = sum(st.nband for st in job.stations)
     in_bytes = sum(nbytes[k][s] for k in range(POOL) for s in range(S)) / POOL
-    s_out = 4 if args.xmac == "bf16" else 8
+    s_out = 4 if args.xmac != "fp32" else 8
     spec_bytes = T * rows * job.freqs[0].nchan * s_out
     f_avg = f_ms / max(nrec, 1)
     x_avg = x_ms / max(nrec, 1)
@@ -620,7 +658,7 @@ def gpu_arm(args, job):
     alg = in_bytes + spec_bytes
     achieved = alg / (f_avg * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": fname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": load_traffic(fname + ("_bf16" if args.xmac == "bf16" else "_fp32")),
+                "frac": achieved / hbm_peak, "traffic": load_traffic(fname + ("_bf16" if args.xmac != "fp32" else "_fp32")),
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": alg,
                 "note": "achieved = (packed VDIF bytes read + spectra bytes written) per subint / F-stage time",
                 "kernel_ms_per_subint": {"prep": prep_ms / max(nrec, 1), "fstage": f_avg, "xmac": x_avg}}
@@ -629,18 +667,19 @@ def gpu_arm(args, job):
     for f in range(len(job.freqs)):
         I = sum(1 for st in job.stations for fb, _ in st.bands if fb == f)
         useful += 8 * (I * (I + 1) // 2) * job.freqs[f].nchan * T
-    xname = "k_xmac_tc" if args.xmac == "bf16" else "k_xmac_fp32v2"
-    xmac_roofline = {"bound": "tensor" if args.xmac == "bf16" else "fp32 pipe", "kernel": xname,
+    tcx = args.xmac != "fp32"
+    xname = "k_xmac_tc" if tcx else "k_xmac_fp32v2"
+    xmac_roofline = {"bound": "tensor" if tcx else "fp32 pipe", "kernel": xname,
                      "achieved": useful / (x_avg * 1e-3) / 1e12, "unit": "TFLOP/s",
-                     "peak": tf_peak if args.xmac == "bf16" else None,
-                     "frac": (useful / (x_avg * 1e-3) / 1e12 / tf_peak) if args.xmac == "bf16" else None,
+                     "peak": tf_peak if tcx else None,
+                     "frac": (useful / (x_avg * 1e-3) / 1e12 / tf_peak) if tcx else None,
                      "useful_flops_per_subint": useful,
                      "note": "useful flops only (8 per Hermitian-unique pair); the time includes the weights kernel"}
 
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, sample, kind = cpu_reference(job, pool, args.cpu_seconds, os.cpu_count() or 1)
+        v, cores, sample, kind = cpu_reference(job, pool, os.cpu_count() or 1)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
     serve = None
@@ -664,7 +703,7 @@ def gpu_arm(args, job):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"fp32": "f32", "bf16": "bf16"}[args.xmac],
+            "vs_baseline": None, "dtype": {"fp32": "f32", "fp16": "f16", "bf16": "bf16"}[args.xmac],
             "data": "synthetic", "rtf": rtf, "xmac": args.xmac,
             "config": workload_config(job),
             "e2e": {"value": e2e_value, "unit": UNIT, "rtf": e2e_value / job.station_mhz_per_sec(),

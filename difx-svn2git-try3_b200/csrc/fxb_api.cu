@@ -2,6 +2,7 @@
 // the per-subint launch sequence and result readout.
 
 #include <cuda_runtime.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <tuple>
@@ -18,7 +19,7 @@
 #include "fxb_kernels.h"
 
 namespace fxb {
-void upload_lut8(cudaStream_t stream);
+cudaError_t upload_lut8(cudaStream_t stream);
 }
 
 using namespace fxb;
@@ -124,7 +125,7 @@ struct fxb_ctx {
 	// F-stage work items (by kind) and FP32 XMAC v2 launch groups
 	FGroup *d_groups = nullptr;
 	std::vector<FKind> fkinds;
-	void *d_specn = nullptr;             // bf16x2 spectra of the tensor-core form
+	void *d_specn = nullptr;             // half2 (or bf16x2) spectra of the tensor-core forms, X 2^-kTcSpecExp
 	void *d_tctab = nullptr;             // constant tables of the tensor-core FFT kernel
 	// XMAC launch groups (subbands of equal rows and channels); the
 	// tensor-core form also keeps each group's spectra in one block
@@ -140,7 +141,8 @@ struct fxb_ctx {
 	std::vector<XGroup> xgroups;
 	// tensor-core XMAC state
 	bool tc = false;
-	bool f8 = false;                     // FP8 form: quantise the bf16x2 spectra to e4m3 pairs for the XMAC
+	bool f8 = false;                     // FP8 form: quantise the half2 spectra to e4m3 pairs for the XMAC
+	bool h16 = false;                    // spectra (and XMAC operands unless FP8) as FP16; BF16 otherwise
 	uint16_t *d_spec8 = nullptr;
 	int64_t spec8_elems = 0, iscale_elems = 0;
 	int nsm = 0;
@@ -417,8 +419,9 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		}
 	}
 	// XMAC launch groups: frequencies with equal shape share a launch
-	ctx->tc = job.xmac_kind == FXB_XMAC_BF16 || job.xmac_kind == FXB_XMAC_FP8;
+	ctx->tc = job.xmac_kind == FXB_XMAC_BF16 || job.xmac_kind == FXB_XMAC_FP8 || job.xmac_kind == FXB_XMAC_FP16;
 	ctx->f8 = job.xmac_kind == FXB_XMAC_FP8;
+	ctx->h16 = job.xmac_kind == FXB_XMAC_FP16 || job.xmac_kind == FXB_XMAC_FP8;
 	std::vector<std::vector<int32_t>> gidx;
 	{
 		std::vector<int> used;
@@ -458,7 +461,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		{
 			fxb_ctx::XGroup &g = ctx->xgroups[gi];
 			const DevFreqPlan &p0 = ctx->h_plans[g.plan0];
-			if(!tc_shape(p0.nrow, p0.nchan, ctx->T, ctx->f8, &g.shape))
+			if(!tc_shape(p0.nrow, p0.nchan, ctx->T, ctx->f8, ctx->h16, &g.shape))
 			{
 				ctx->err = "tensor-core XMAC: at most 64 inputs per subband";
 				return FXB_ERR_UNSUPPORTED;
@@ -768,7 +771,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		for(cudaEvent_t &e : sl.tev)
 			CK(ctx, cudaEventCreate(&e));
 	}
-	upload_lut8(ctx->stream);
+	CK(ctx, upload_lut8(ctx->stream));
 	CK(ctx, cudaMemsetAsync(ctx->d_acc, 0, sizeof(float2) * std::max<int64_t>(job.acc_total, 1), ctx->stream));
 	CK(ctx, cudaMemsetAsync(ctx->d_bwacc, 0, sizeof(float) * std::max(ctx->nbw, 1), ctx->stream));
 	CK(ctx, cudaMemsetAsync(ctx->d_acwacc, 0, sizeof(float) * std::max(ctx->nacw, 1), ctx->stream));
@@ -1027,6 +1030,7 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 		fa.fraclo = job.fractionallofreq ? 1 : 0;
 		fa.spec = ctx->tc ? ctx->d_specn : (void *)ctx->d_spec;
 		fa.err = ctx->d_err;
+		fa.h16 = ctx->h16 ? 1 : 0;
 		for(size_t i = 0; i < nk; i++)
 		{
 			FKind k = ctx->fkinds[i];
@@ -1412,7 +1416,7 @@ fxb_status fxb_job_footprint(const fxb_job_desc *desc, size_t *bytes)
 	const double pad32 = (double)((T + 31) / 32 * 32) / (double)std::max<int64_t>(T, 1);
 	const double pad64 = (double)((T + 63) / 64 * 64) / (double)std::max<int64_t>(T, 1);
 	double b = (double)job.spec_total * (job.xmac_kind == FXB_XMAC_FP32 ? 8.0
-	                                     : job.xmac_kind == FXB_XMAC_BF16 ? 4.0 * 1.25 * pad32
+	                                     : job.xmac_kind != FXB_XMAC_FP8 ? 4.0 * 1.25 * pad32
 	                                                                      : (4.0 * pad64 + 2.0 * pad64 + 0.5) * 1.25);
 	b += (double)job.acc_total * 8.0 + (double)job.corelen * 16.0 + (double)S * T * 64.0 +
 	     (double)job.pcal_bins * 8.0 * pcal_chunks(job, pcal_groups(job));
@@ -1669,11 +1673,27 @@ fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloa
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
 	if(n && ctx->tc)
 	{
-		// bf16x2 [t][block][row][tcb] -> FP32 [t][row][chan]
+		// half2 or bf16x2 [t][block][row][tcb], scaled by 2^-kTcSpecExp -> FP32 [t][row][chan]
 		const size_t nb = (size_t)ctx->T * p.tnblk * p.nrow * p.tcb;
 		std::vector<uint32_t> h(nb);
 		CK(ctx, cudaMemcpy(h.data(), (const uint32_t *)ctx->d_specn + p.spec_off, nb * 4, cudaMemcpyDeviceToHost));
-		auto bf = [](uint32_t v) { uint32_t u = v << 16; float f; memcpy(&f, &u, 4); return f; };
+		const float unscale = (float)(1 << kTcSpecExp);
+		const bool h16 = ctx->h16;
+		auto bf = [h16, unscale](uint32_t v) {
+			float f;
+			if(h16)
+			{
+				__half_raw r;
+				r.x = (unsigned short)v;
+				f = __half2float(__half(r));
+			}
+			else
+			{
+				const uint32_t u = v << 16;
+				memcpy(&f, &u, 4);
+			}
+			return f * unscale;
+		};
 		for(int t = 0; t < ctx->T; t++)
 			for(int r = 0; r < p.nrow; r++)
 				for(int c = 0; c < p.nchan; c++)
@@ -1721,12 +1741,9 @@ fxb_status fxb_vdif_unpack(const uint8_t *data, int64_t nbytes, int32_t payload,
 	int *d_good = nullptr;
 	cudaStream_t st = 0;
 	fxb_status rc = FXB_OK;
-	static bool lut_ready = false;
-	if(!lut_ready)
-	{
-		upload_lut8(0);
-		lut_ready = true;
-	}
+	// the 8-bit table is per device: uploaded for the current one on every call
+	if(upload_lut8(st) != cudaSuccess)
+		return FXB_ERR_CUDA;
 	if(cudaMalloc(&d_data, nbytes) != cudaSuccess || cudaMalloc(&d_out, sizeof(float) * nchan * (size_t)nsamp) != cudaSuccess ||
 	   cudaMalloc(&d_good, sizeof(int)) != cudaSuccess)
 		rc = FXB_ERR_NOMEM;

@@ -25,9 +25,10 @@
 // Two arithmetic forms:
 //   out 0: FP32 FFT, spectra as float2 (the plain FP32 form);
 //   out 1: FP16 FFT with the two bands packed in half2 lanes (one instruction
-//          advances both polarisations), spectra as bf16x2 (re, im) for the
-//          tensor-core XMAC.  Samples are scaled by 2^-e so that no FFT value
-//          can leave the FP16 range; the outputs are scaled back exactly.
+//          advances both polarisations), spectra as half2 or bf16x2 (re, im)
+//          for the tensor-core XMAC.  Samples are scaled by 2^-e so that no
+//          FFT value can leave the FP16 range; the outputs are rescaled
+//          exactly to X 2^-kTcSpecExp.
 //
 // Twiddles come from a per-length table laid out [pass][r - 1][p] (entry
 // w_N^(r p s) for pass stride s), so that the twiddle loads of a warp are
@@ -204,6 +205,18 @@ __host__ __device__ inline float level2(uint32_t code)
 
 __device__ __forceinline__ float frac_centered(double x) { return (float)(x - rint(x)); }
 
+// one spectral value of the tensor-core forms: (re, im) as half2 or bf16x2
+__device__ __forceinline__ uint32_t pack_spec(bool h16, float re, float im)
+{
+	if(h16)
+	{
+		const __half2 h = __floats2half2_rn(re, im);
+		return *(const uint32_t *)&h;
+	}
+	const __nv_bfloat162 b = __floats2bfloat162_rn(re, im);
+	return *(const uint32_t *)&b;
+}
+
 // CTAs per SM the register budget is sized for: four for the FP16 form at
 // the lengths where 64 registers hold the kernel without spills (2048 points:
 // 6 % faster than three on the B200), else the shape's default
@@ -366,7 +379,8 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 		while(lvl * (float)N > 32768.0f * (float)(1 << hexp))
 			hexp++;
 	}
-	const float hin = H ? ldexpf(1.0f, -hexp) : 1.0f, hout = H ? ldexpf(1.0f, hexp) : 1.0f;
+	const float hin = H ? ldexpf(1.0f, -hexp) : 1.0f, hout = H ? ldexpf(1.0f, hexp - kTcSpecExp) : 1.0f;
+	const bool h16 = a.h16 != 0;
 	if(nbits == 8)
 	{
 		// (b - 128) / 3.3 in double, rounded to float (format_vdif.c:122)
@@ -682,23 +696,23 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 						const hc v = y[0][r];
 						const float xr0 = __low2float(v.x) * hout, xi0 = cj * __low2float(v.y) * hout;
 						const float xr1 = __high2float(v.x) * hout, xi1 = cj * __high2float(v.y) * hout;
-						__nv_bfloat162 *o;
+						uint32_t *o;
 						int64_t rstride;
 						if(tcb)
 						{
 							const uint32_t blk = __umulhi((uint32_t)c, tcb_magic), cl = (uint32_t)c - blk * tcb;
-							o = (__nv_bfloat162 *)a.spec + spec_off + (((int64_t)t * tnblk + blk) * prow) * tcb + cl;
+							o = (uint32_t *)a.spec + spec_off + (((int64_t)t * tnblk + blk) * prow) * tcb + cl;
 							rstride = tcb;
 						}
 						else
 						{
-							o = (__nv_bfloat162 *)a.spec + obase + c;
+							o = (uint32_t *)a.spec + obase + c;
 							rstride = nchan;
 						}
 						if(row0 >= 0)
-							o[(int64_t)row0 * rstride] = __floats2bfloat162_rn(xr0 * cs - xi0 * sn, xr0 * sn + xi0 * cs);
+							o[(int64_t)row0 * rstride] = pack_spec(h16, xr0 * cs - xi0 * sn, xr0 * sn + xi0 * cs);
 						if(row1 >= 0)
-							o[(int64_t)row1 * rstride] = __floats2bfloat162_rn(xr1 * cs - xi1 * sn, xr1 * sn + xi1 * cs);
+							o[(int64_t)row1 * rstride] = pack_spec(h16, xr1 * cs - xi1 * sn, xr1 * sn + xi1 * cs);
 					}
 					else
 					{

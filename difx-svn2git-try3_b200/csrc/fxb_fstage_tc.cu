@@ -158,7 +158,7 @@ struct TcFftConst {
 // DFT-32 columns (upper, lower sideband), twiddles [n2][k1] (float2), the
 // operand tile of MMA 1 (reused for the operand tiles of MMA 2), and the
 // staging of the next unit's VDIF words ([sample][thread]).
-constexpr int kOffB3 = kA1, kOffTw = kA1 + 2 * kB3, kOffB = kOffTw + (kN2 / 2) * kN1 * 8;
+constexpr int kOffB3 = kA1, kOffTw = kA1 + 2 * kB3, kOffB = kOffTw + kN2 * kN1 * 8;
 constexpr int kOffStage = kOffB + kTileB;
 constexpr int kTablesBytes = kOffB;                 // copied from the table in global memory
 constexpr size_t kSmemTc = 1024 + (size_t)kOffStage + 16 * kThreadsF * 4;
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(kThreadsF, 2) k_fstage_tc(const FsArgs a, cons
 	__shared__ uint32_t tmem_s;
 	unsigned char *base = (unsigned char *)(((uintptr_t)fsm_tc + 1023) & ~(uintptr_t)1023);
 	unsigned char *sB = base + kOffB;
-	const uint2 *stw = (const uint2 *)(base + kOffTw);
+	const float2 *stw = (const float2 *)(base + kOffTw);
 	const uint32_t *stage = (const uint32_t *)(base + kOffStage);
 	const uint32_t stage_addr = su32(base + kOffStage);
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -498,12 +498,12 @@ __global__ void __launch_bounds__(kThreadsF, 2) k_fstage_tc(const FsArgs a, cons
 		}
 		asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
-		// ---- (d) twiddle w_N^(n2 k1) in half2 over neighbouring n2; rows
-		// (FFT, k1) of the MMA 2 operands
+		// ---- (d) twiddle w_N^(n2 k1) in FP32 (one rounding to FP16 per value);
+		// rows (FFT, k1) of the MMA 2 operands
 		{
 			const int q = warp & 3, hcol = warp >> 2;
 			const int r = 32 * q + lane, k1 = r >> 1, part = r & 1;
-			const uint32_t sgnmask = part ? 0u : 0x80008000u;      // re lane subtracts o wi
+			const float sg = part ? 1.0f : -1.0f;                  // re lane subtracts o wi
 #pragma unroll
 			for(int cc = 0; cc < 2; cc++)
 			{
@@ -516,11 +516,8 @@ __global__ void __launch_bounds__(kThreadsF, 2) k_fstage_tc(const FsArgs a, cons
 				{
 					const float o0 = __shfl_xor_sync(0xffffffffu, v[n2], 1);
 					const float o1 = __shfl_xor_sync(0xffffffffu, v[n2 + 1], 1);
-					const uint2 w = stw[(n2 >> 1) * kN1 + k1];
-					const __half2 V = __floats2half2_rn(v[n2], v[n2 + 1]), O = __floats2half2_rn(o0, o1);
-					uint32_t wi = w.y ^ sgnmask;
-					const __half2 r2 = __hfma2(O, *(const __half2 *)&wi, __hmul2(V, *(const __half2 *)&w.x));
-					pkv[n2 >> 1] = *(const uint32_t *)&r2;
+					const float2 w0 = stw[n2 * kN1 + k1], w1 = stw[(n2 + 1) * kN1 + k1];
+					pkv[n2 >> 1] = pack_h2(fmaf(sg * o0, w0.y, v[n2] * w0.x), fmaf(sg * o1, w1.y, v[n2 + 1] * w1.x));
 				}
 				const int R3 = fftl * 64 + k1;
 				unsigned char *tile = sB + (R3 >> 7) * 16384;
@@ -557,7 +554,8 @@ __global__ void __launch_bounds__(kThreadsF, 2) k_fstage_tc(const FsArgs a, cons
 		}
 		asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
-		// ---- (f) channels c = k1 + 64 j: fractional-sample rotation, bf16x2 out
+		// ---- (f) channels c = k1 + 64 j: fractional-sample rotation, half2 or
+		// bf16x2 out, scaled by 2^-kTcSpecExp
 		{
 			const int q = warp & 3, m = warp >> 2;
 			const int r = 32 * q + lane;
@@ -577,17 +575,28 @@ __global__ void __launch_bounds__(kThreadsF, 2) k_fstage_tc(const FsArgs a, cons
 				turns -= rintf(turns);
 				float qr, qi;
 				__sincosf(6.283185307179586f * turns, &qi, &qr);
+				constexpr float osc = 1.0f / (float)(1 << kTcSpecExp);
+				qr *= osc;
+				qi *= osc;
 				// channel k1 + 64 j -> (block, position): start, then step by 64 channels
 				const uint32_t PT = (uint32_t)prow * tcb;
 				uint32_t blk = (uint32_t)k1 / tcb, cl = (uint32_t)k1 - blk * tcb;
 				const uint32_t dblk = 64u / tcb, dcl = 64u - dblk * tcb;
 				uint32_t off = blk * PT + cl;
-				__nv_bfloat162 *o = (__nv_bfloat162 *)a.spec + spec_off + ((int64_t)c.t * tnblk * prow + rw) * tcb;
+				uint32_t *o = (uint32_t *)a.spec + spec_off + ((int64_t)c.t * tnblk * prow + rw) * tcb;
+				const bool h16 = a.h16 != 0;
 #pragma unroll
 				for(int j = 0; j < 16; j++)
 				{
 					const float xr = v[j], xi = v[16 + j];
-					o[off] = __floats2bfloat162_rn(xr * qr - xi * qi, xr * qi + xi * qr);
+					const float yr = xr * qr - xi * qi, yi = xr * qi + xi * qr;
+					if(h16)
+						o[off] = pack_h2(yr, yi);
+					else
+					{
+						const __nv_bfloat162 b = __floats2bfloat162_rn(yr, yi);
+						o[off] = *(const uint32_t *)&b;
+					}
 					const float nr = qr * c.Rr - qi * c.Ri;
 					qi = qr * c.Ri + qi * c.Rr;
 					qr = nr;
@@ -663,19 +672,13 @@ void make_fstage_tc_tables(void *out)
 			}
 		}
 	}
-	// twiddles w_2048^(n2 k1) for neighbouring n2 as half2 pairs:
-	// entry [n2 / 2][k1] = ((wr(n2), wr(n2 + 1)), (wi(n2), wi(n2 + 1)))
-	__half *tw = (__half *)(o + kOffTw);
-	for(int n2 = 0; n2 < kN2; n2 += 2)
+	// twiddles w_2048^(n2 k1) as float2 [n2][k1]
+	float2 *tw = (float2 *)(o + kOffTw);
+	for(int n2 = 0; n2 < kN2; n2++)
 		for(int k1 = 0; k1 < kN1; k1++)
 		{
-			__half *e = tw + 4 * ((n2 / 2) * kN1 + k1);
-			for(int d = 0; d < 2; d++)
-			{
-				const double ang = -2.0 * M_PI * (double)((n2 + d) * k1) / kN;
-				e[d] = __double2half(cos(ang));
-				e[2 + d] = __double2half(sin(ang));
-			}
+			const double ang = -2.0 * M_PI * (double)(n2 * k1) / kN;
+			tw[n2 * kN1 + k1] = make_float2((float)cos(ang), (float)sin(ang));
 		}
 }
 

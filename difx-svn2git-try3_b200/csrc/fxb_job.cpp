@@ -176,7 +176,7 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 		return fail(err, st, FXB_ERR_UNSUPPORTED, "too many stations");
 	if(d->fringe_rot_order < 0 || d->fringe_rot_order > 2)
 		return fail(err, st, FXB_ERR_ARG, "fringe rotation order must be 0, 1 or 2");
-	if(d->xmac_kind < FXB_XMAC_FP32 || d->xmac_kind > FXB_XMAC_FP8)
+	if(d->xmac_kind < FXB_XMAC_FP32 || d->xmac_kind > FXB_XMAC_FP16)
 		return fail(err, st, FXB_ERR_ARG, "unknown xmac kind");
 	job.freqs.assign(d->freqs, d->freqs + d->nfreq);
 	for(auto &f : job.freqs)

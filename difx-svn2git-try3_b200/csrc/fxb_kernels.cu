@@ -15,7 +15,7 @@ __constant__ float c_lut2[4] = {-3.3359f, -1.0f, 1.0f, 3.3359f};
 // 8-bit offset binary -> (b - 128) / 3.3 (format_vdif.c:122), filled from the host.
 __constant__ float c_lut8[256];
 
-void upload_lut8(cudaStream_t stream);
+cudaError_t upload_lut8(cudaStream_t stream);
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
@@ -190,21 +190,21 @@ __global__ void __launch_bounds__(256) k_fstage(const DevStation *__restrict__ s
 	}
 }
 
-void launch_fstage(const DevStation *st, const DevSubintStation *sub, const DevBand *bands, int maxband,
+cudaError_t launch_fstage(const DevStation *st, const DevSubintStation *sub, const DevBand *bands, int maxband,
                    const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride, const FftParam *params,
                    const float2 *twiddle, int maxN, int S, int T, int order, bool fractionallofreq, int maxfft,
                    float2 *spec, cudaStream_t stream)
 {
 	size_t smem = (size_t)maxfft * sizeof(float2);
-	static bool attr_set = false;
-	if(!attr_set)
-	{
-		cudaFuncSetAttribute(k_fstage, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-		attr_set = true;
-	}
+	// the shared-memory limit is a per-device attribute: raised on every call
+	// (cheap), so that a launch on any device of the process gets it
+	const cudaError_t e = cudaFuncSetAttribute(k_fstage, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+	if(e != cudaSuccess)
+		return e;
 	dim3 grid(T, S);
 	k_fstage<<<grid, 256, smem, stream>>>(st, sub, bands, maxband, plans, valid, valid_stride, params, twiddle, maxN, T,
 	                                      order, fractionallofreq ? 1 : 0, spec);
+	return cudaGetLastError();
 }
 
 // FP32 cross-multiply-accumulate (core.cpp:877-972 with the autocorrelations
@@ -318,12 +318,9 @@ void launch_xmac_fp32(const DevFreqPlan &plan, const DevFreqPlan *dplan, int T, 
 	if(TC > 32) TC = 32;
 	if(TC < 1) TC = 1;
 	size_t smem = (size_t)TC * nrowpad * CB * sizeof(float2);
-	static bool attr_set = false;
-	if(!attr_set)
-	{
-		cudaFuncSetAttribute(k_xmac_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
-		attr_set = true;
-	}
+	// per-device attribute: raised on every call
+	if(cudaFuncSetAttribute(k_xmac_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024) != cudaSuccess)
+		return;
 	dim3 grid((plan.npair + 7) / 8, (plan.nchan + CB - 1) / CB);
 	k_xmac_fp32<<<grid, 256, smem, stream>>>(dplan, T, TC, spec, acc);
 }
@@ -618,12 +615,15 @@ void launch_zoom_gather(const DevZoomCopy *zc, int nzc, const DevFreqPlan *plans
 		k_zoom_gather<float2><<<grid, 256, 0, stream>>>(zc, plans, T, (float2 *)spec);
 }
 
-void upload_lut8(cudaStream_t stream)
+// 8-bit levels (b - 128) / 3.3 (format_vdif.c:122) into the current
+// device's constant table; pageable source, so the copy has been taken when
+// this returns
+cudaError_t upload_lut8(cudaStream_t stream)
 {
 	float lut[256];
 	for(int b = 0; b < 256; b++)
 		lut[b] = (float)((b - 128) / 3.3);
-	cudaMemcpyToSymbolAsync(c_lut8, lut, sizeof(lut), 0, cudaMemcpyHostToDevice, stream);
+	return cudaMemcpyToSymbolAsync(c_lut8, lut, sizeof(lut), 0, cudaMemcpyHostToDevice, stream);
 }
 
 }  // namespace fxb

@@ -57,8 +57,9 @@ void launch_fft_params(const DevStation *st, const DevSubintStation *sub, const 
                        FftParam *out, float *pbw, int nbm, cudaStream_t stream);
 
 // Fused unpack -> fringe rotation -> FFT -> fractional-sample correction.
-// One CTA per (station, FFT); writes FP32 spectra into spec.
-void launch_fstage(const DevStation *st, const DevSubintStation *sub, const DevBand *bands, int maxband,
+// One CTA per (station, FFT); writes FP32 spectra into spec.  Returns the
+// launch's error (including that of raising the shared-memory limit).
+cudaError_t launch_fstage(const DevStation *st, const DevSubintStation *sub, const DevBand *bands, int maxband,
                    const DevFreqPlan *plans, const uint8_t *valid, int64_t valid_stride, const FftParam *params,
                    const float2 *twiddle, int maxN, int S, int T, int order, bool fractionallofreq, int maxfft,
                    float2 *spec, cudaStream_t stream);
@@ -88,6 +89,12 @@ struct FKind {
 	const void *tctab;       // constant tables of the tensor-core FFT kernel
 };
 
+// Spectra of the tensor-core forms hold X 2^-kTcSpecExp (FP16 or BF16), so
+// that the largest value of any supported FFT (16384 points of 8-bit levels,
+// |X| <= 16384 x 38.8) stays inside the FP16 range; the XMAC epilogue scales
+// the products back by 2^(2 kTcSpecExp), exactly.
+constexpr int kTcSpecExp = 5;
+
 struct FsArgs {
 	const DevStation *st;
 	const DevSubintStation *sub;
@@ -100,8 +107,10 @@ struct FsArgs {
 	const void *tw;          // set from FKind::tw by launch_fstage_kind
 	int32_t maxN, T, tq, order;
 	int32_t fraclo, pp, first, items_fast;
-	void *spec;              // [t][row][chan]: float2 (out 0) or bf16x2 (out 1)
+	void *spec;              // [t][row][chan]: float2 (out 0), or half2 / bf16x2 (out 1) scaled by 2^-kTcSpecExp
 	int32_t *err;            // device error flag (bounded waits of the tensor-core FFT kernel)
+	int32_t h16;             // out 1: spectra as FP16 (else BF16)
+	int32_t pad_;
 };
 
 bool fstage_plan(int N, int nb, int out, FKind *k);
@@ -126,6 +135,7 @@ void launch_xmac_fp32v2(const DevFreqPlan &plan0, const DevFreqPlan *dplans, con
 // subbands whose bf16x2 spectra lie in one block [subband][Tpad][nrow][nchan].
 struct TcShape {
 	int32_t f8;                       // FP8 form: e4m3 pairs, K tiles of 64 times
+	int32_t h16;                      // operands (or the FP8 form's source spectra) FP16, else BF16
 	int32_t w8;                       // FP8 form: values per time of a block, nrow * CB padded to 8
 	int32_t nrow, nchan, r2p, G, CB, Tpad;
 	int32_t raw_bytes, raw_stride;    // bytes of one TMA box, stride of the raw stages
@@ -134,7 +144,7 @@ struct TcShape {
 	int32_t dstride, dump_off;        // accumulator copy: floats per row, byte offset
 	size_t smem;
 };
-bool tc_shape(int nrow, int nchan, int T, bool f8, TcShape *s);
+bool tc_shape(int nrow, int nchan, int T, bool f8, bool h16, TcShape *s);
 // set the raw / operand ring depths and accumulator buffers of a shape (and
 // its shared-memory plan); false if they do not fit (227 KB for one CTA per
 // SM, 112 KB each for two)

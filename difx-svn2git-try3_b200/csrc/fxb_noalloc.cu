@@ -31,7 +31,7 @@
 #include "fxb_kernels.h"
 
 namespace fxb {
-void upload_lut8(cudaStream_t stream);
+cudaError_t upload_lut8(cudaStream_t stream);
 }
 
 using namespace fxb;
@@ -84,7 +84,8 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
                                                          double poly0_sec, int32_t interval_s, const double *coeffs,
                                                          const uint8_t *dev_vdif, int64_t nbytes, int32_t datasec,
                                                          int32_t datans, const int32_t *validflags, int32_t sec,
-                                                         int32_t ns, float *dev_spectra, float *dev_weights,
+                                                         int32_t ns, float *dev_spectra, size_t spectra_floats,
+                                                         float *dev_weights, size_t weight_floats, int32_t *nfft,
                                                          void *stream)
 {
 	if(!freqs || nfreq < 1 || nfreq > kNoallocMaxFreq || !station || !coeffs || !dev_vdif || nbytes <= 0 ||
@@ -92,6 +93,10 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
 	   order < 0 || order > kMaxPolyOrder || interval_s <= 0)
 		return FXB_ERR_ARG;
 	const fxb_station &st = *station;
+	// INTERLACEDVDIF stations need per-band weights and EDV4 band blanking,
+	// whose per-frame band masks do not fit the fixed scratch array
+	if(st.mux_threads != 0)
+		return FXB_ERR_UNSUPPORTED;
 	if(st.nband < 1 || st.nband > kMaxBandsPerStation || !st.band_freq || (st.nband & (st.nband - 1)) ||
 	   (st.nbits != 2 && st.nbits != 8) || (st.nbits == 8 && st.nband > 4) || st.payload_bytes <= 0 ||
 	   st.payload_bytes % 8 || ((int64_t)st.payload_bytes * 8) % (st.nbits * st.nband) ||
@@ -117,6 +122,11 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
 	if(T > kNoallocMaxFft || valid_stride > kNoallocMaxFrames)
 		return FXB_ERR_UNSUPPORTED;
 	(void)framebytes;
+	if(nfft)
+		*nfft = T;
+	// the caller's buffers must hold the whole result: spectra [T][nband][nchan] complex, weights [T]
+	if(spectra_floats < (size_t)T * st.nband * f0.nchan * 2 || (dev_weights && weight_floats < (size_t)T))
+		return FXB_ERR_ARG;
 
 	cudaStream_t cs = (cudaStream_t)stream;
 	int dev = 0;
@@ -135,7 +145,8 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
 		scratch = (unsigned char *)g_noalloc_ptr[dev];
 		if(!g_noalloc_lut[dev])
 		{
-			upload_lut8(cs);
+			if(upload_lut8(cs) != cudaSuccess)
+				return FXB_ERR_CUDA;
 			g_noalloc_lut[dev] = true;
 		}
 	}
@@ -237,8 +248,9 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
 	launch_frame_valid(d_st, d_sub, d_valid, nullptr, valid_stride, 1, cs);
 	launch_fft_params(d_st, d_sub, d_flags, nflagint, d_valid, nullptr, valid_stride, 1, T, fringe_rot_order,
 	                  d_params, nullptr, 0, cs);
-	launch_fstage(d_st, d_sub, d_bands, st.nband, d_plans, d_valid, valid_stride, d_params, d_tw, N, 1, T,
-	              fringe_rot_order, fraclo, N, (float2 *)dev_spectra, cs);
+	if(launch_fstage(d_st, d_sub, d_bands, st.nband, d_plans, d_valid, valid_stride, d_params, d_tw, N, 1, T,
+	                 fringe_rot_order, fraclo, N, (float2 *)dev_spectra, cs) != cudaSuccess)
+		return FXB_ERR_CUDA;
 	if(dev_weights)
 		launch_param_weights(d_params, T, dev_weights, cs);
 	if(cudaGetLastError() != cudaSuccess)

@@ -12,14 +12,17 @@
 // K tiles of 64 times (still 64-byte operand rows), kind::f8f6f4 MMAs of
 // K = 32, and the epilogue dividing each product by the two inputs' scales.
 //
-// Input: the F stage's bf16x2 spectra, per group of equally shaped subbands
+// Input: the F stage's half2 (or bf16x2) spectra X 2^-kTcSpecExp, per group of
+// equally shaped subbands
 // one block [subband][Tpad][block][nrow][CB] (times T..Tpad-1 zero), with CB
 // the channels of one work unit.  A unit is two M = 128 operand tiles of
 // G = floor(128 / R2p) channels each, R2p the real rows per channel rounded up
 // to 8 (rows past G R2p stay zero).  One tcgen05.mma (kind::f16, M = N = 128,
 // K = 16) uses the same shared-memory tile as A and B, so the G diagonal
 // R2p x R2p blocks of each 128 x 128 FP32 accumulator are the G channels'
-// A A^T.  A unit's two accumulators take 256 tensor-memory columns; two units
+// A A^T.  FP16 operands (11-bit significands) are the default; BF16 (8 bits)
+// is kept as a measured alternative.  The epilogue multiplies every product
+// by 2^(2 kTcSpecExp), which undoes the spectra's scale exactly.  A unit's two accumulators take 256 tensor-memory columns; two units
 // alternate, so the epilogue of one overlaps the MMAs of the next.
 //
 // One persistent CTA per SM, warp-specialised:
@@ -40,6 +43,7 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
+#include <cuda_fp16.h>
 #include <cstdint>
 
 #include "fxb_internal.h"
@@ -199,6 +203,7 @@ struct TcParams {
 	int32_t nrs, nas;               // raw and operand stages in use
 	int32_t dstride, dump_off;      // floats per row of the accumulator copy, its byte offset in shared memory
 	int32_t rpitch;                 // values per time of one raw box (FP8 form: padded to 8)
+	int32_t h16;                    // FP16 operands (else BF16)
 	int32_t *err;
 };
 
@@ -294,10 +299,13 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 	{
 		if(lane == 0)
 		{
-			// ---- MMA issuer: M = N = 128, BF16 x BF16 (FP8 form: e4m3 x e4m3)
-			// -> FP32, A and B K-major; unit ku accumulates into columns 256 (ku & 1)
-			const uint32_t idesc = (1u << 4) | (F8 ? 0u : (1u << 7) | (1u << 10)) | ((128u >> 3) << 17) |
-			                       ((128u >> 4) << 24);
+			// ---- MMA issuer: M = N = 128, FP16 x FP16 or BF16 x BF16 (FP8 form:
+			// e4m3 x e4m3) -> FP32, A and B K-major; unit ku accumulates into
+			// columns 256 (ku & 1).  Instruction descriptor: D format F32 (bit 4),
+			// A / B formats (bits 7-9 / 10-12: 0 F16 or E4M3, 1 BF16), N >> 3
+			// (bits 17-22), M >> 4 (bits 24-28).
+			const uint32_t ab = (F8 || tp.h16) ? 0u : (1u << 7) | (1u << 10);
+			const uint32_t idesc = (1u << 4) | ab | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 			int kk = 0, ku = 0;
 			bool ok = true;
 			for(int u = blockIdx.x; u < tp.nunits && ok; u += gridDim.x, ku++)
@@ -559,6 +567,7 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 			// and subint, so the sum is that of a load-add-store)
 			const int32_t *outsrc = P.outsrc;
 			const float *isc = F8 ? P.iscale + (int64_t)c_first * nin : nullptr;   // FP8 form: [channel][input] 1 / scale
+			constexpr float unscale = (float)(1 << (2 * kTcSpecExp));
 			float2 *dst = acc + P.acc_off + (int64_t)c_first * nout;
 			for(int o = et; o < nout; o += 128)
 			{
@@ -583,6 +592,11 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 						const float f = isc[cl * nin + a] * isc[cl * nin + b];
 						vre *= f;
 						vim *= f;
+					}
+					else
+					{
+						vre *= unscale;
+						vim *= unscale;
 					}
 					atomicAdd(dst + (int64_t)cl * nout + o, make_float2(vre, cj ? -vim : vim));
 					if(++cln == nin)
@@ -614,9 +628,10 @@ typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32
                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-bool tc_shape(int nrow, int nchan, int T, bool f8, TcShape *s)
+bool tc_shape(int nrow, int nchan, int T, bool f8, bool h16, TcShape *s)
 {
 	s->f8 = f8 ? 1 : 0;
+	s->h16 = h16 ? 1 : 0;
 	s->nrow = nrow;
 	s->nchan = nchan;
 	s->r2p = (2 * nrow + 7) & ~7;
@@ -713,6 +728,7 @@ void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplan
 	tp.nas = s.nas;
 	tp.dstride = s.dstride;
 	tp.dump_off = s.dump_off;
+	tp.h16 = s.h16;
 	tp.err = err;
 	const int ctas = nsm * (s.nb == 1 ? 2 : 1);
 	const int grid = tp.nunits < ctas ? tp.nunits : ctas;
@@ -743,9 +759,19 @@ void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplan
 // One CTA per (channel block, subband); thread = one (input, channel) column
 // of the block.  Two passes over the subint's T times: the column's largest
 // |re| or |im|, then the scaled e4m3 pairs (saturating, round to nearest).
-// Columns of channels past nchan hold zeros and keep scale 1.
+// Columns of channels past nchan hold zeros and keep scale 1.  The source
+// spectra (half2, or bf16x2) hold X 2^-kTcSpecExp; the inverse scale written
+// per (channel, input) includes 2^kTcSpecExp, so that the epilogue's product
+// of two inverse scales restores X X^H.
+__device__ __forceinline__ float2 spec_value(uint32_t w, bool h16)
+{
+	if(h16)
+		return __half22float2(*(const __half2 *)&w);
+	return __bfloat1622float2(*(const __nv_bfloat162 *)&w);
+}
+
 __global__ void k_quant_fp8(const DevFreqPlan *__restrict__ plans, const int32_t *__restrict__ plan_idx, int T,
-                            int w8, const uint32_t *__restrict__ spec16, uint16_t *__restrict__ spec8)
+                            int w8, int h16, const uint32_t *__restrict__ spec16, uint16_t *__restrict__ spec8)
 {
 	const DevFreqPlan &P = plans[plan_idx[blockIdx.y]];
 	const int blk = blockIdx.x;
@@ -759,21 +785,19 @@ __global__ void k_quant_fp8(const DevFreqPlan *__restrict__ plans, const int32_t
 	float amax = 0.0f;
 	for(int t = 0; t < T; t++)
 	{
-		const uint32_t w = __ldg(src + t * ts16);
-		const float2 v = __bfloat1622float2(*(const __nv_bfloat162 *)&w);
+		const float2 v = spec_value(__ldg(src + t * ts16), h16 != 0);
 		amax = fmaxf(amax, fmaxf(fabsf(v.x), fabsf(v.y)));
 	}
 	const float sc = amax > 0.0f ? 240.0f / amax : 1.0f;
 	uint16_t *dst = spec8 + P.spec8_off + (int64_t)blk * w8 + col;
 	for(int t = 0; t < T; t++)
 	{
-		const uint32_t w = __ldg(src + t * ts16);
-		const float2 v = __bfloat1622float2(*(const __nv_bfloat162 *)&w);
+		const float2 v = spec_value(__ldg(src + t * ts16), h16 != 0);
 		dst[t * ts8] = (uint16_t)__nv_cvt_float2_to_fp8x2(make_float2(v.x * sc, v.y * sc), __NV_SATFINITE, __NV_E4M3);
 	}
 	const int c = blk * P.tcb + cl;
 	if(c < P.nchan)
-		P.iscale[(int64_t)c * P.nrow + row] = 1.0f / sc;
+		P.iscale[(int64_t)c * P.nrow + row] = (float)(1 << kTcSpecExp) / sc;
 }
 
 void launch_quant_fp8(const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf, int T,
@@ -783,7 +807,7 @@ void launch_quant_fp8(const TcShape &s, const DevFreqPlan *dplans, const int32_t
 		return;
 	const int W = s.nrow * s.CB;
 	const int nblk = (s.nchan + s.CB - 1) / s.CB;
-	k_quant_fp8<<<dim3(nblk, nf), (W + 31) / 32 * 32, 0, stream>>>(dplans, plan_idx, T, s.w8, spec16, spec8);
+	k_quant_fp8<<<dim3(nblk, nf), (W + 31) / 32 * 32, 0, stream>>>(dplans, plan_idx, T, s.w8, s.h16, spec16, spec8);
 }
 
 }  // namespace fxb

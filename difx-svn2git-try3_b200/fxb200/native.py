@@ -21,7 +21,7 @@ FXB_STATUS = {
     0: "FXB_OK", 1: "FXB_ERR_ARG", 2: "FXB_ERR_UNSUPPORTED", 3: "FXB_ERR_CUDA", 4: "FXB_ERR_NOMEM",
     5: "FXB_ERR_STATE", 6: "FXB_ERR_TIMEOUT", 7: "FXB_ERR_BUSY", 8: "FXB_ERR_DATA",
 }
-XMAC_KIND = {"fp32": 0, "bf16": 1, "fp8": 2}
+XMAC_KIND = {"fp32": 0, "bf16": 1, "fp8": 2, "fp16": 3}
 
 
 class FxbFreq(ctypes.Structure):

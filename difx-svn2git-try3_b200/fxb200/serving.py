@@ -60,7 +60,7 @@ def _bind():
     return L
 
 
-def job_footprint(job: Job, xmac: str = "bf16", inflight: int = 2) -> int:
+def job_footprint(job: Job, xmac: str = "fp16", inflight: int = 2) -> int:
     d = DescHolder(job, xmac, inflight)
     out = _c.c_size_t(0)
     rc = _bind().fxb_job_footprint(_c.byref(d.desc), _c.byref(out))
@@ -125,7 +125,7 @@ class Server:
             msg = _bind().fxb_server_last_error(self.srv)
             raise FxbError("%s failed: %s %s" % (what, FXB_STATUS.get(rc, rc), msg.decode() if msg else ""))
 
-    def submit(self, job: Job, subints: Sequence[Tuple[list, int, int]], xmac: str = "bf16",
+    def submit(self, job: Job, subints: Sequence[Tuple[list, int, int]], xmac: str = "fp16",
                inflight: int = 2) -> ServedJob:
         sj = ServedJob(job, subints, xmac, inflight)
         jid = _c.c_uint64(0)
@@ -232,7 +232,7 @@ def poisson_arrivals(rng: np.random.Generator, n: int, rate_hz: float) -> np.nda
     return np.cumsum(rng.exponential(1.0 / rate_hz, size=n))
 
 
-def run_stream(server: Server, jobs: Sequence[Tuple[Job, list]], arrivals: Sequence[float], xmac: str = "bf16",
+def run_stream(server: Server, jobs: Sequence[Tuple[Job, list]], arrivals: Sequence[float], xmac: str = "fp16",
                timeout_s: float = 600.0) -> dict:
     """Submit each job at its arrival time (seconds from now), wait for all,
     return the server's statistics."""

@@ -46,7 +46,8 @@ typedef enum {
 typedef enum {
 	FXB_XMAC_FP32 = 0,        /* CUDA-core complex FP32 MAC (the plain FP32 form) */
 	FXB_XMAC_BF16 = 1,        /* BF16 spectra, tensor-core MAC, FP32 accumulate */
-	FXB_XMAC_FP8 = 2          /* FP8 e4m3 spectra with per-(channel, station) scale */
+	FXB_XMAC_FP8 = 2,         /* FP8 e4m3 spectra with per-(channel, station) scale */
+	FXB_XMAC_FP16 = 3         /* FP16 spectra (fixed 2^-5 scale), tensor-core MAC, FP32 accumulate */
 } fxb_xmac_kind;
 
 /* One frequency-table entry (FREQ TABLE of the .input file,
@@ -416,13 +417,20 @@ FXB_API fxb_status fxb_vdif_unpack(const uint8_t *data, int64_t nbytes, int32_t 
  * Its device address is looked up on the first call on each device, which
  * should therefore come before any stream capture.  Arguments otherwise mean
  * what they mean for fxb_job_desc, fxb_set_delay_poly and fxb_submit_subint
- * (one station).  Returns when the work on `stream` has completed. */
+ * (one station).  The subint holds T = subint_ns / (2 nchan x 1000 / (2 bw_mhz))
+ * FFTs (returned in *nfft when nfft is not NULL): spectra_floats must be at
+ * least T x nband x nchan x 2 and, with dev_weights, weight_floats at least
+ * T, else FXB_ERR_ARG.  INTERLACEDVDIF stations (mux_threads != 0) are
+ * refused with FXB_ERR_UNSUPPORTED; zoom bands and phase-cal tones of the
+ * station are not produced.  Returns when the work on `stream` has
+ * completed. */
 FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, int32_t nfreq, const fxb_station *station,
                                               int32_t fringe_rot_order, int64_t subint_ns, int32_t npoly,
                                               int32_t order, double poly0_sec, int32_t interval_s,
                                               const double *coeffs, const uint8_t *dev_vdif, int64_t nbytes,
                                               int32_t datasec, int32_t datans, const int32_t *validflags,
-                                              int32_t sec, int32_t ns, float *dev_spectra, float *dev_weights,
+                                              int32_t sec, int32_t ns, float *dev_spectra, size_t spectra_floats,
+                                              float *dev_weights, size_t weight_floats, int32_t *nfft,
                                               void *stream);
 
 /* ------------------------------------------------------------------ serving

@@ -8,6 +8,11 @@ from fxb200.job import Freq, Job, full_job
 
 # FP32 form vs the FP64 oracle: relative visibility tolerance (north star)
 FP32_TOL = 1e-5
+# tensor-core form (FP16 spectra, FP32 accumulation) vs the FP64 oracle:
+# relative visibility tolerance (north star), applied norm-wise to the cross
+# and autocorrelations and as the rms of the per-visibility relative
+# amplitude and phase (radians) errors
+TC_REL_TOL = 1e-3
 
 
 def small_job(nstation=4, nchan=256, bw=16.0, nfreq=1, full_pol=False, nbits=2, subint_ns=4_000_000,
@@ -44,6 +49,42 @@ def rel_err(a: np.ndarray, b: np.ndarray) -> float:
     if nb == 0:
         return float(np.linalg.norm(a))
     return float(np.linalg.norm(a - b) / nb)
+
+
+def _cplx(a):
+    return a[0::2].astype(np.float64) + 1j * a[1::2].astype(np.float64)
+
+
+def vis_errors(job, layout, corelen, got, ref):
+    """Errors of a core result against the FP64 oracle's, over the cross
+    visibilities (and norm-wise over the autocorrelations):
+      cross_rel / auto_rel   ||V - V64|| / ||V64||;
+      amp_rms / amp_p99      per-visibility (|V| - |V64|) / |V64|;
+      phase_rms / phase_p99  per-visibility arg(V conj V64), radians;
+      ccu                    rms cross error over the autocorrelation scale
+                             (correlation-coefficient units).
+    The per-visibility figures leave out visibilities with |V64| under a
+    tenth of the median (noise-dominated visibilities near zero, whose
+    relative error is unbounded; `left_out` counts them)."""
+    reg = dict(regions(job, layout, corelen))
+    xc, ac = reg["cross"], reg["auto"]
+    v, r = _cplx(got[xc]), _cplx(ref[xc])
+    auto_rms = np.sqrt(np.mean(ref[ac][0::2].astype(np.float64) ** 2))
+    keep = np.abs(r) >= 0.1 * np.median(np.abs(r))
+    amp = (np.abs(v[keep]) - np.abs(r[keep])) / np.abs(r[keep])
+    ph = np.angle(v[keep] * np.conj(r[keep]))
+    return {"cross_rel": float(np.linalg.norm(v - r) / np.linalg.norm(r)),
+            "auto_rel": rel_err(got[ac], ref[ac]),
+            "amp_rms": float(np.sqrt(np.mean(amp ** 2))), "amp_p99": float(np.quantile(np.abs(amp), 0.99)),
+            "phase_rms": float(np.sqrt(np.mean(ph ** 2))), "phase_p99": float(np.quantile(np.abs(ph), 0.99)),
+            "ccu": float(np.sqrt(np.mean((got[xc].astype(np.float64) - ref[xc]) ** 2)) / auto_rms),
+            "left_out": int((~keep).sum()), "visibilities": int(keep.size)}
+
+
+def assert_tc_gate(e, tol=TC_REL_TOL):
+    """The tensor-core form's relative gate on vis_errors' figures."""
+    for k in ("cross_rel", "auto_rel", "amp_rms", "phase_rms"):
+        assert e[k] <= tol, (k, e)
 
 
 def compare_core(job, layout, corelen, got, ref, tol=FP32_TOL, weights_exact=True):

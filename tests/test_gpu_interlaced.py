@@ -16,7 +16,7 @@ import fxoracle
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("masklength,xmac", [(4, "fp32"), (2, "fp32"), (4, "bf16")])
+@pytest.mark.parametrize("masklength,xmac", [(4, "fp32"), (2, "fp32"), (4, "fp16")])
 def test_interlaced_vdif_matches_oracle(masklength, xmac):
     job = mux_job(masklength=masklength)
     corr = Correlator(job, xmac=xmac)
@@ -34,4 +34,4 @@ def test_interlaced_vdif_matches_oracle(masklength, xmac):
     if xmac == "fp32":
         compare_core(job, layout, n, got, ref)
     else:
-        compare_core(job, layout, n, got, ref, tol=1e-2)
+        compare_core(job, layout, n, got, ref, tol=1e-3)

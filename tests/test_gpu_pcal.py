@@ -47,7 +47,7 @@ def test_pcal_matches_oracle(name):
 def test_pcal_with_invalid_frames_and_tensor_core_form():
     job = PCAL_JOBS["pcal_frac_lo"]()
     f0 = synth.subint_window(job, 0, *SUBINTS[0])[0]
-    got, ref, layout, n = _run(job, xmac="bf16", invalid={0: [f0 + 1, f0 + 5], 2: [f0 + 2]})
+    got, ref, layout, n = _run(job, xmac="fp16", invalid={0: [f0 + 1, f0 + 5], 2: [f0 + 2]})
     pc = dict(regions(job, layout, n))["pcal"]
     e = np.linalg.norm(got[pc] - ref[pc]) / np.linalg.norm(ref[pc])
     assert e < 1e-5, e

@@ -8,7 +8,8 @@ import pytest
 from fxb200 import serving
 from fxb200.native import Correlator
 from helpers import small_job
-from test_gpu_tc import TC_TOL, tc_errors
+from test_gpu_tc import tc_errors
+from helpers import assert_tc_gate
 
 import fxoracle
 
@@ -36,7 +37,7 @@ def _alone(job, subints, xmac):
     return r
 
 
-@pytest.mark.parametrize("xmac", ["bf16", "fp32"])
+@pytest.mark.parametrize("xmac", ["fp16", "fp32"])
 def test_results_same_alone_and_in_the_mix(xmac):
     jobs = _jobs()
     alone = [_alone(j, s, xmac) for j, s in jobs]
@@ -72,11 +73,10 @@ def test_served_job_matches_oracle():
     ref = None
     for inputs, sec, ns in subints:
         ref = orc.process_subint(inputs, sec, ns, coreresult=ref)
-    c = Correlator(job, xmac="bf16")
+    c = Correlator(job, xmac="fp16")
     layout, n = c.layout(), c.corelen
     c.close()
-    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
-    assert cross_err <= TC_TOL and auto_err <= TC_TOL
+    assert_tc_gate(tc_errors(job, layout, n, got, ref))
 
 
 def test_pinned_buffers_give_the_same_result_and_phases_add_up():
@@ -84,7 +84,7 @@ def test_pinned_buffers_give_the_same_result_and_phases_add_up():
     pinned = []
     for k, (job, _) in enumerate(jobs):
         pinned.append((job, serving.job_subints(job, 3, seed=20 + k, rho=0.05, pinned=True)))
-    alone = [_alone(j, s, "bf16") for j, s in jobs]
+    alone = [_alone(j, s, "fp16") for j, s in jobs]
     srv = serving.Server(budget_bytes=8 << 30, max_active=3)
     handles = [srv.submit(j, s) for j, s in pinned]
     for h, ref in zip(handles, alone):
@@ -103,7 +103,7 @@ def test_a_failing_job_is_reported_and_the_others_complete():
     srv = serving.Server(budget_bytes=8 << 30, max_active=3)
     good = srv.submit(*jobs[0])
     job, subints = jobs[1]
-    bad = serving.ServedJob(job, subints, "bf16", 2)
+    bad = serving.ServedJob(job, subints, "fp16", 2)
     bad.nbytes[len(job.stations)] = -1            # second subint, first station: rejected by the host check
     jid = ctypes.c_uint64(0)
     assert serving._bind().fxb_server_submit(srv.srv, ctypes.byref(bad.req), ctypes.byref(jid)) == 0
@@ -126,9 +126,9 @@ def test_zoom_and_pcal_jobs_served_in_the_mix():
     from helpers import PCAL_JOBS, zoom_job
     jobs = [zoom_job(), PCAL_JOBS["pcal_frac_lo"](), _jobs()[0][0]]
     jobs = [(j, serving.job_subints(j, 3, seed=60 + k, rho=0.05)) for k, j in enumerate(jobs)]
-    alone = [_alone(j, s, "bf16") for j, s in jobs]
+    alone = [_alone(j, s, "fp16") for j, s in jobs]
     srv = serving.Server(budget_bytes=8 << 30, max_active=3)
-    handles = [srv.submit(j, s, xmac="bf16") for j, s in jobs]
+    handles = [srv.submit(j, s, xmac="fp16") for j, s in jobs]
     for h, ref in zip(handles, alone):
         assert np.array_equal(srv.wait(h, 120.0), ref)
     srv.close()

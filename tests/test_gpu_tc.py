@@ -1,26 +1,29 @@
-"""Tensor-core (BF16 tcgen05) form against the FP64 oracle.
+"""Tensor-core forms against the FP64 oracle.
 
-BF16 spectra carry ~2^-9 relative rounding per value, so a noise-dominated
-cross-correlation differs from the FP64 result by ~1e-3 of its own (noise)
-amplitude.  The meaningful error of a correlator output is in correlation-
-coefficient units: the error of V_ab relative to sqrt(A_aa A_bb), the
-autocorrelation scale.  Gates: cross-correlation error <= 1e-3 in those units,
-autocorrelations within 1e-3 relative, weights and layout exact."""
+The headline tensor-core form keeps the F stage's spectra in FP16 (11-bit
+significands, ~2^-12 relative rounding per value) and accumulates in FP32.
+Its gate is the north star's relative visibility tolerance, 1e-3
+(``helpers.TC_REL_TOL``): norm-wise over the cross and autocorrelations and
+as the rms of the per-visibility relative amplitude and phase errors.  BF16
+spectra (8-bit significands) are kept as a measured alternative: a value's
+rounding is ~8 times coarser, so they are held to correlation-coefficient
+units (the error of V_ab over sqrt(A_aa A_bb)), not to the relative gate.
+Weights and layout are exact in every form."""
 import numpy as np
 import pytest
 
-from fxb200 import synth
+from fxb200 import configs, synth
 from fxb200.native import Correlator
-from helpers import regions, rel_err, small_job
+from helpers import assert_tc_gate, regions, rel_err, small_job, vis_errors
 
 import fxoracle
 
 pytestmark = pytest.mark.gpu
 
-TC_TOL = 1e-3
+BF16_CCU_TOL = 1e-3
 
 
-def run_tc(job, subints, rho=0.05, seed=5, xmac="bf16"):
+def run_tc(job, subints, rho=0.05, seed=5, xmac="fp16"):
     corr = Correlator(job, xmac=xmac)
     orc = fxoracle.OracleCorrelator(job)
     ref = None
@@ -37,32 +40,61 @@ def run_tc(job, subints, rho=0.05, seed=5, xmac="bf16"):
 
 def tc_errors(job, layout, n, got, ref):
     reg = dict(regions(job, layout, n))
-    xc, ac = reg["cross"], reg["auto"]
-    # correlation-coefficient units: cross error over the autocorrelation scale
-    auto_rms = np.sqrt(np.mean(ref[ac][0::2] ** 2))
-    cross_err = np.sqrt(np.mean((got[xc] - ref[xc]) ** 2)) / auto_rms
-    auto_err = rel_err(got[ac], ref[ac])
     for name in ("bweight", "acweight"):
         assert np.array_equal(got[reg[name]].astype(np.float32), ref[reg[name]].astype(np.float32)), name
-    return cross_err, auto_err
+    return vis_errors(job, layout, n, got, ref)
 
 
 @pytest.mark.parametrize("kw", [dict(nstation=4, full_pol=True),
                                 dict(nstation=10, full_pol=True, nchan=256),
+                                dict(nstation=3, nchan=1024, bw=32.0, nfreq=8, full_pol=True, subint_ns=2_048_000),
+                                dict(nstation=4, nchan=512, bw=16.0, nfreq=2, full_pol=True, nbits=8,
+                                     subint_ns=2_048_000)])
+def test_fp16_tensor_core_vs_fp64(kw):
+    job = small_job(**kw)
+    got, ref, layout, n = run_tc(job, [(0, 1_024_000), (0, 3_072_000)])
+    e = tc_errors(job, layout, n, got, ref)
+    print(kw, e)
+    assert_tc_gate(e)
+
+
+def test_fp16_c1_ten_stations_vs_fp64():
+    """The c1 shape (10 stations, eight 32 MHz subbands, 1024 channels, full
+    cross hands), two 2.048 ms subints."""
+    job = configs.c1(subint_ns=2_048_000)
+    got, ref, layout, n = run_tc(job, [(0, 0), (0, 2_048_000)], rho=0.01, seed=21)
+    e = tc_errors(job, layout, n, got, ref)
+    print(e)
+    assert_tc_gate(e)
+
+
+@pytest.mark.parametrize("bw,nchan,nbits", [(16.0, 1024, 8), (64.0, 4096, 2), (4.0, 128, 8)])
+def test_fp16_c3_shapes_twenty_stations_vs_fp64(bw, nchan, nbits):
+    """Subband shapes of the c3 batch (widths 4..64 MHz, 128..4096 channels,
+    2- and 8-bit samples) at its 20 stations, one 8.192 ms subint."""
+    job = small_job(nstation=20, nchan=nchan, bw=bw, nfreq=1, full_pol=True, nbits=nbits, subint_ns=8_192_000)
+    got, ref, layout, n = run_tc(job, [(0, 0)], rho=0.01, seed=23)
+    e = tc_errors(job, layout, n, got, ref)
+    print(bw, nchan, nbits, e)
+    assert_tc_gate(e)
+
+
+@pytest.mark.parametrize("kw", [dict(nstation=4, full_pol=True),
                                 dict(nstation=3, nchan=1024, bw=32.0, nfreq=8, full_pol=True, subint_ns=2_048_000)])
 def test_bf16_tensor_core_vs_fp64(kw):
     job = small_job(**kw)
-    got, ref, layout, n = run_tc(job, [(0, 1_024_000), (0, 3_072_000)])
-    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
-    assert cross_err <= TC_TOL, cross_err
-    assert auto_err <= TC_TOL, auto_err
+    got, ref, layout, n = run_tc(job, [(0, 1_024_000), (0, 3_072_000)], xmac="bf16")
+    e = tc_errors(job, layout, n, got, ref)
+    assert e["ccu"] <= BF16_CCU_TOL, e
+    assert e["auto_rel"] <= 1e-3, e
 
 
-def test_bf16_spectra_readback_matches_oracle():
+@pytest.mark.parametrize("xmac,tol", [("fp16", 2e-3), ("bf16", 8e-3)])
+def test_tc_spectra_readback_matches_oracle(xmac, tol):
     job = small_job(nstation=2, full_pol=True)
     sec, ns = 0, 1_000_000
     inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=9)
-    corr = Correlator(job, xmac="bf16")
+    corr = Correlator(job, xmac=xmac)
     corr.submit(inputs, sec, ns)
     spec = corr.spectra(0)
     corr.close()
@@ -71,7 +103,7 @@ def test_bf16_spectra_readback_matches_oracle():
     for t in (0, 5, 100):
         ref, _, _ = orc.mode_fft(0, buf, dsec, dns, sec, ns, t)
         for b in range(2):
-            assert rel_err(spec[t, b], ref[b]) < 8e-3
+            assert rel_err(spec[t, b], ref[b]) < tol
 
 
 def _tc_fft_job(lsb=False, order=1):
@@ -82,13 +114,13 @@ def _tc_fft_job(lsb=False, order=1):
 @pytest.mark.parametrize("lsb,order", [(False, 1), (True, 1), (False, 0)])
 def test_tensor_core_fft_spectra_match_oracle(lsb, order, monkeypatch):
     """Spectra of the tensor-core FFT (FXB_TC_FFT=1: FP16 operands, FP32
-    accumulation, BF16 out) against the FP64 oracle's Mode FFT output, both
+    accumulation, FP16 out) against the FP64 oracle's Mode FFT output, both
     sidebands."""
     monkeypatch.setenv("FXB_TC_FFT", "1")
     job = _tc_fft_job(lsb=lsb, order=order)
     sec, ns = 0, 1_024_000
     inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=11)
-    corr = Correlator(job, xmac="bf16")
+    corr = Correlator(job, xmac="fp16")
     corr.submit(inputs, sec, ns)
     spec = corr.spectra(0)
     corr.close()
@@ -97,22 +129,20 @@ def test_tensor_core_fft_spectra_match_oracle(lsb, order, monkeypatch):
     for t in (0, 7, 31):
         ref, _, _ = orc.mode_fft(0, buf, dsec, dns, sec, ns, t)
         for b in range(2):
-            assert rel_err(spec[t, b], ref[b]) < 8e-3, (t, b)
+            assert rel_err(spec[t, b], ref[b]) < 2e-3, (t, b)
 
 
 def test_tensor_core_fft_matches_cuda_core_fstage(monkeypatch):
     """The same subints through the tensor-core FFT (FXB_TC_FFT=1) and through
-    the default CUDA-core FP16 F stage: both within the tensor-core tolerance
-    of the FP64 oracle and of each other."""
+    the default CUDA-core FP16 F stage: both within the tensor-core relative
+    tolerance of the FP64 oracle and of each other."""
     job = _tc_fft_job()
     subints = [(0, 1_024_000), (0, 3_072_000)]
     got_cc, ref, layout, n = run_tc(job, subints)
     monkeypatch.setenv("FXB_TC_FFT", "1")
     got_tc, _, _, _ = run_tc(job, subints)
     for got in (got_tc, got_cc):
-        cross_err, auto_err = tc_errors(job, layout, n, got, ref)
-        assert cross_err <= TC_TOL, cross_err
-        assert auto_err <= TC_TOL, auto_err
+        assert_tc_gate(tc_errors(job, layout, n, got, ref))
     reg = dict(regions(job, layout, n))
     assert rel_err(got_tc[reg["auto"]], got_cc[reg["auto"]]) < 2e-3
 
@@ -130,18 +160,16 @@ FP8_TOL = 2e-2
 def test_fp8_tensor_core_vs_fp64(kw):
     job = small_job(**kw)
     got, ref, layout, n = run_tc(job, [(0, 1_024_000), (0, 3_072_000)], xmac="fp8")
-    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
-    assert cross_err <= FP8_TOL, cross_err
-    assert auto_err <= FP8_TOL, auto_err
+    e = tc_errors(job, layout, n, got, ref)
+    assert e["ccu"] <= FP8_TOL, e
+    assert e["auto_rel"] <= FP8_TOL, e
 
 
 @pytest.mark.parametrize("nchan", [2048, 4096, 8192])
-def test_bf16_long_ffts_vs_fp64(nchan):
-    # the FP16 FFT's rounding over 12..14 radix stages averages down with the
-    # number of FFTs integrated: 8.192 ms subints give 8..32 per subint (a 1 s
-    # integration has 60..250 times more)
+def test_fp16_long_ffts_vs_fp64(nchan):
+    # 4096..16384-point FFTs: the longest transforms of the serving workload
     job = small_job(nstation=3, nchan=nchan, bw=16.0, nfreq=2, full_pol=True, subint_ns=8_192_000)
     got, ref, layout, n = run_tc(job, [(0, 8_192_000), (0, 16_384_000)])
-    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
-    assert cross_err <= TC_TOL, cross_err
-    assert auto_err <= TC_TOL, auto_err
+    e = tc_errors(job, layout, n, got, ref)
+    print(nchan, e)
+    assert_tc_gate(e)

@@ -19,7 +19,7 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not refcorr.available(), reason="reference build oracle/_ref absent")]
 
 
-@pytest.mark.parametrize("xmac,tol", [("fp32", 1e-5), ("bf16", 1e-3)])
+@pytest.mark.parametrize("xmac,tol", [("fp32", 1e-5), ("fp16", 1e-3)])
 def test_device_integration_to_swin_matches_reference(xmac, tol, tmp_path):
     job = small_job(nstation=3, full_pol=True, nfreq=2)
     ref = refcorr.RefCorrelator(job)
@@ -50,7 +50,7 @@ def test_device_integration_to_swin_matches_reference(xmac, tol, tmp_path):
         parallel_auto = a.baseline % 257 == 0 and a.polpair[0] == a.polpair[1]
         if xmac == "fp32" or parallel_auto:
             assert err <= tol, (a.baseline, a.polpair, err)
-    if xmac == "bf16":
+    if xmac == "fp16":
         # cross products and cross-hand autocorrelations (noise-sized): error
         # in correlation-coefficient units (the calibrated autocorrelation scale is 1)
         cross = [(a, b) for a, b in zip(g, e) if a.baseline % 257 or a.polpair[0] != a.polpair[1]]

@@ -14,7 +14,8 @@ import pytest
 from fxb200 import synth
 from fxb200.native import Correlator, job_layout
 from helpers import compare_core, mixed_bw_zoom_job, zoom_job
-from test_gpu_tc import FP8_TOL, TC_TOL, tc_errors
+from test_gpu_tc import FP8_TOL, tc_errors
+from helpers import assert_tc_gate
 
 import fxoracle
 
@@ -53,21 +54,20 @@ def test_zoom_fp32_matches_oracle(name):
 
 
 @pytest.mark.parametrize("name", sorted(JOBS))
-def test_zoom_bf16_matches_oracle(name):
+def test_zoom_fp16_matches_oracle(name):
     job = JOBS[name]()
-    got, ref, layout, n = _run(job, "bf16")
-    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
-    assert cross_err <= TC_TOL and auto_err <= TC_TOL, (cross_err, auto_err)
+    got, ref, layout, n = _run(job, "fp16")
+    assert_tc_gate(tc_errors(job, layout, n, got, ref))
 
 
 def test_zoom_fp8_matches_oracle():
     job = zoom_job()
     got, ref, layout, n = _run(job, "fp8")
-    cross_err, auto_err = tc_errors(job, layout, n, got, ref)
-    assert cross_err <= FP8_TOL and auto_err <= FP8_TOL, (cross_err, auto_err)
+    e = tc_errors(job, layout, n, got, ref)
+    assert e["ccu"] <= FP8_TOL and e["auto_rel"] <= FP8_TOL, e
 
 
-@pytest.mark.parametrize("xmac", ["fp32", "bf16"])
+@pytest.mark.parametrize("xmac", ["fp32", "fp16"])
 def test_zoom_spectra_are_parent_channels(xmac):
     # zoom frequency 2 is channels 64..127 of frequency 0 (4 MHz in, 62.5 kHz
     # channels); every station zooms both polarisations, so zoom row r is
@@ -91,7 +91,7 @@ def _zoom_region(job, layout, f):
     return np.concatenate([np.arange(2 * o, 2 * (o + k * chans)) for o, k in zip(bl, nprod) if o >= 0])
 
 
-@pytest.mark.parametrize("xmac", ["fp32", "bf16"])
+@pytest.mark.parametrize("xmac", ["fp32", "fp16"])
 def test_zoom_results_independent_of_parents(xmac):
     # the same zoom windows correlated with and without their parents'
     # products give bit-identical zoom visibilities
