@@ -263,6 +263,24 @@ def load_traffic(kernel):
         return None
 
 
+def h2d_link_gbs():
+    """Host-to-device copy bandwidth from page-locked memory (256 MB, best of 5),
+    the ceiling of the end-to-end figure."""
+    import torch
+    src = torch.empty(256 << 20, dtype=torch.uint8).pin_memory()
+    dst = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        best = max(best, src.numel() / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del src, dst
+    return best
+
+
 def load_peaks():
     """(HBM GB/s, burst dense bf16 TFLOP/s, sustained dense bf16 TFLOP/s, source)."""
     try:
@@ -644,9 +662,9 @@ def gpu_arm(args, job):
     if rank == 0 and world == 1 and not args.no_features:
         feats = features_leg(args, job, value, step_device, max_over_ranks, data_s)
 
-    # ---- rooflines: F stage against HBM (its design bound), XMAC against the
-    # tensor (bf16) or FP32 pipes
-    hbm_peak, tf_peak, peak_src = load_peaks()
+    # ---- rooflines: F stage against HBM (its design bound); XMAC against the
+    # tensor pipe (burst and sustained peaks) and against HBM (its spectra read)
+    hbm_peak, tf_peak, tf_sus, peak_src = load_peaks()
     T = job.blocks_per_send()
     rows = sum(st.nband for st in job.stations)
     in_bytes = sum(nbytes[k][s] for k in range(POOL) for s in range(S)) / POOL
@@ -654,13 +672,15 @@ def gpu_arm(args, job):
     spec_bytes = T * rows * job.freqs[0].nchan * s_out
     f_avg = f_ms / max(nrec, 1)
     x_avg = x_ms / max(nrec, 1)
-    fname = "k_fstage"
+    tcfft = args.xmac != "fp32" and any("tensor-core FFT" in t for t in tuning)
+    fname = "k_fstage_tc" if tcfft else "k_fstage"
     alg = in_bytes + spec_bytes
     achieved = alg / (f_avg * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": fname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": load_traffic(fname + ("_bf16" if args.xmac != "fp32" else "_fp32")),
+                "frac": achieved / hbm_peak, "traffic": load_traffic(fname + "_c1_" + args.xmac),
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": alg,
-                "note": "achieved = (packed VDIF bytes read + spectra bytes written) per subint / F-stage time",
+                "note": "achieved = (packed VDIF bytes read + spectra bytes written) per 8 ms subint / F-stage "
+                        "event time per subint (F-stage launches only)",
                 "kernel_ms_per_subint": {"prep": prep_ms / max(nrec, 1), "fstage": f_avg, "xmac": x_avg}}
     # useful XMAC flops: 8 per Hermitian-unique input pair, channel and FFT
     useful = 0
@@ -669,12 +689,16 @@ def gpu_arm(args, job):
         useful += 8 * (I * (I + 1) // 2) * job.freqs[f].nchan * T
     tcx = args.xmac != "fp32"
     xname = "k_xmac_tc" if tcx else "k_xmac_fp32v2"
-    xmac_roofline = {"bound": "tensor" if tcx else "fp32 pipe", "kernel": xname,
-                     "achieved": useful / (x_avg * 1e-3) / 1e12, "unit": "TFLOP/s",
-                     "peak": tf_peak if tcx else None,
-                     "frac": (useful / (x_avg * 1e-3) / 1e12 / tf_peak) if tcx else None,
+    xach = useful / (x_avg * 1e-3) / 1e12
+    xmac_roofline = {"bound": "tensor" if tcx else "fp32 pipe", "kernel": xname, "achieved": xach, "unit": "TFLOP/s",
+                     "peak_burst": tf_peak if tcx else None, "frac_burst": xach / tf_peak if tcx else None,
+                     "peak_sustained": tf_sus if tcx else None,
+                     "frac_sustained": xach / tf_sus if (tcx and tf_sus) else None,
+                     "hbm_bound": {"spectra_bytes_read": spec_bytes, "achieved_gbs": spec_bytes / (x_avg * 1e-3) / 1e9,
+                                   "frac": spec_bytes / (x_avg * 1e-3) / 1e9 / hbm_peak},
                      "useful_flops_per_subint": useful,
-                     "note": "useful flops only (8 per Hermitian-unique pair); the time includes the weights kernel"}
+                     "note": "useful flops only (8 per Hermitian-unique pair); the time includes the weights kernel; "
+                             "at 20 inputs the contraction carries ~21 useful flops per spectra byte, so HBM bounds it"}
 
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
@@ -700,6 +724,14 @@ def gpu_arm(args, job):
     flens = {2 * job.freqs[st.bands[0][0]].nchan for st in job.stations}
     launches_per_subint = 3 + len(flens) + len(shapes) + 1
     if rank == 0:
+        link = h2d_link_gbs() if world == 1 else None
+        e2e_gbs = h2d / (e2e_ms / args.steps * 1e-3) / 1e9
+        # the full record first, then the headline line (last, compact) carrying
+        # the secondary figures
+        detail = {"bench_detail": True, "tuning": tuning, "serving": serve, "batched_c3": c3, "vdif_mux": mux,
+                  "features": feats, "other_form": other, "roofline": roofline, "xmac_roofline": xmac_roofline,
+                  "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(detail), flush=True)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -707,10 +739,23 @@ def gpu_arm(args, job):
             "data": "synthetic", "rtf": rtf, "xmac": args.xmac,
             "config": workload_config(job),
             "e2e": {"value": e2e_value, "unit": UNIT, "rtf": e2e_value / job.station_mhz_per_sec(),
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps},
-            "roofline": roofline, "xmac_roofline": xmac_roofline, "cpu_baseline": cpu, "clocks": clk,
-            "other_form": other, "tc_vs_fp32": tc_vs_fp32, "tuning": tuning, "serving": serve, "batched_c3": c3, "vdif_mux": mux,
-            "features": feats,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps,
+                    "h2d_gbs": e2e_gbs, "h2d_link_gbs": link, "link_frac": (e2e_gbs / link) if link else None},
+            "roofline": {k: roofline[k] for k in ("bound", "kernel", "achieved", "peak", "unit", "frac", "traffic",
+                                                  "peak_source", "kernel_ms_per_subint")},
+            "xmac_roofline": {k: xmac_roofline[k] for k in ("kernel", "achieved", "unit", "frac_burst",
+                                                            "frac_sustained", "hbm_bound")},
+            "cpu_baseline": cpu, "clocks": clk,
+            "other_form": None if other is None else {k: other[k] for k in ("xmac", "value", "rtf",
+                                                                            "kernel_ms_per_subint")},
+            "tc_vs_fp32": tc_vs_fp32,
+            "serving": None if serve is None else {k: serve[k] for k in ("jobs", "p50_ms", "p99_ms", "rtf",
+                                                                          "station_mhz_per_s") if k in serve},
+            "batched_c3": None if c3 is None else {"tc_batched_vs_fp32": c3["tc_batched_vs_fp32"],
+                                                   "tc_batched_rtf": c3["tc_batched_graph"]["rtf"],
+                                                   "tc_per_job_rtf": c3["tc_per_job"]["rtf"],
+                                                   "fp32_per_job_rtf": c3["fp32_per_job"]["rtf"]},
+            "vdif_mux_frac": None if mux is None else mux["frac"],
             "gpu_launches": launches_per_subint * nsub * args.steps,
         }
         print(json.dumps(line), flush=True)

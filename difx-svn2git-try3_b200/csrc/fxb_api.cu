@@ -193,6 +193,71 @@ static cudaError_t dalloc(fxb_ctx *ctx, T **p, size_t n)
 	return e;
 }
 
+// Work units of the tensor-core FFT F stage for one kind's items (FGroups at
+// absolute indices first ..): pairs of subbands of one station with equal
+// sideband, as [n][2] absolute FGroup indices (-1: no second subband),
+// ordered (pair position, station) so that the stations of one subband
+// pair are neighbours.  False if a station's sample layout does not suit the
+// kernel (2-bit, 2..32 bands alike in every station of the kind, each
+// subband's bands in one 4-bit field, 16-byte aligned frames of at least 128
+// samples); *bpt = bits per time.
+static bool tc_fft_pairs(const Job &job, const std::vector<FGroup> &items, int first, std::vector<int32_t> &pairs,
+                         int *bpt)
+{
+	std::map<int, std::vector<int>> bystation;
+	*bpt = 0;
+	for(size_t i = 0; i < items.size(); i++)
+	{
+		const FGroup &g = items[i];
+		const Job::Station &js = job.stations[g.station];
+		const int fb = js.payload + js.header;
+		const int b = js.nbits * js.nband;
+		const int fs = js.payload * 8 / b;
+		if(js.nbits != 2 || (b != 4 && b != 8 && b != 16 && b != 32 && b != 64) || (*bpt && b != *bpt) ||
+		   js.payload % 16 || js.header % 16 || fb % 16 || fs < 128)
+			return false;
+		*bpt = b;
+		if((g.band[0] & 1) || (g.nb == 2 && g.band[1] != g.band[0] + 1))
+			return false;
+		bystation[g.station].push_back(first + (int)i);
+	}
+	std::vector<std::vector<std::pair<int, int>>> per;     // [station] pairs
+	for(auto &kv : bystation)
+	{
+		std::vector<int> &v = kv.second;
+		std::stable_sort(v.begin(), v.end(), [&](int x, int y) {
+			const FGroup &a = items[x - first], &b = items[y - first];
+			return a.lsb != b.lsb ? a.lsb < b.lsb : a.freq < b.freq;
+		});
+		std::vector<std::pair<int, int>> ps;
+		for(size_t i = 0; i < v.size();)
+		{
+			if(i + 1 < v.size() && items[v[i] - first].lsb == items[v[i + 1] - first].lsb)
+			{
+				ps.push_back({v[i], v[i + 1]});
+				i += 2;
+			}
+			else
+			{
+				ps.push_back({v[i], -1});
+				i += 1;
+			}
+		}
+		per.push_back(ps);
+	}
+	size_t most = 0;
+	for(const auto &ps : per)
+		most = std::max(most, ps.size());
+	for(size_t k = 0; k < most; k++)
+		for(const auto &ps : per)
+			if(k < ps.size())
+			{
+				pairs.push_back(ps[k].first);
+				pairs.push_back(ps[k].second);
+			}
+	return !pairs.empty();
+}
+
 static void free_ctx(fxb_ctx *ctx)
 {
 	if(!ctx)
@@ -534,7 +599,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		{
 			const Job::Station &js = job.stations[s];
 			const int N = ctx->h_st[s].fftchannels;
-			const bool pairs = out == 1 || N <= 2048;
+			const bool pairs = N <= 2048;
 			std::vector<int> done(js.nband, 0);
 			for(int b = 0; b < js.nband; b++)
 			{
@@ -562,7 +627,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				g.nb = b1 >= 0 ? 2 : 1;
 				g.lsb = job.freqs[f].lower_sideband;
 				g.lofreq = job.freqs[f].freq_mhz;
-				bykind[{N, out == 1 ? 2 : g.nb}].push_back(g);
+				bykind[{N, g.nb}].push_back(g);
 			}
 		}
 		std::vector<FGroup> hg;
@@ -593,17 +658,20 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				if((int64_t)((ctx->T + per - 1) / per) * k.count >= 2 * (int64_t)ctx->nsm)
 					break;
 			}
-			// tensor-core form at N = 2048: FXB_TC_FFT=1 runs the FFT on the
-			// tensor cores (fxb_fstage_tc.cu); the default is the CUDA-core FP16
-			// F stage, which is faster on the B200 today
+			// tensor-core form at N = 2048: the FFT runs on the tensor cores
+			// (fxb_fstage_tc.cu) wherever the stations' sample layout allows it
+			// (FXB_TC_FFT=0 selects the CUDA-core FP16 F stage instead)
 			if(out == 1)
 			{
 				bool any_lsb = false;
 				for(const FGroup &gg : kv.second)
 					any_lsb = any_lsb || gg.lsb;
 				const char *env = getenv("FXB_TC_FFT");
-				const bool allow = env && env[0] == '1' && ctx->nbm == 0;   // no EDV4 band blanking there
-				if(allow && fstage_tc_eligible(k.N, job.fringe_rot_order, any_lsb))
+				const bool allow = !(env && env[0] == '0') && ctx->nbm == 0;   // no EDV4 band blanking there
+				std::vector<int32_t> pairs;
+				int bpt = 0;
+				if(allow && fstage_tc_eligible(k.N, job.fringe_rot_order, any_lsb) &&
+				   tc_fft_pairs(job, kv.second, (int)hg.size(), pairs, &bpt))
 				{
 					if(!ctx->d_tctab)
 					{
@@ -614,23 +682,20 @@ static fxb_status setup_device(fxb_ctx *ctx)
 						CK(ctx, cudaMemcpyAsync(d, h.data(), h.size(), cudaMemcpyHostToDevice, ctx->stream));
 						ctx->d_tctab = d;
 					}
+					int32_t *dp = nullptr;
+					CK(ctx, dalloc(ctx, &dp, pairs.size()));
+					CK(ctx, cudaMemcpyAsync(dp, pairs.data(), sizeof(int32_t) * pairs.size(), cudaMemcpyHostToDevice,
+					                        ctx->stream));
 					k.tcfft = 1;
 					k.tctab = ctx->d_tctab;
+					k.tcpairs = dp;
+					k.tcnpairs = (int32_t)(pairs.size() / 2);
+					k.tcbpt = bpt;
 				}
 			}
-			if(out == 1)
-			{
-				std::vector<uint2> h((size_t)k.twn);
-				make_fstage_twiddles(k.N, nullptr, h.data());
-				uint2 *d = nullptr;
-				CK(ctx, dalloc(ctx, &d, h.size()));
-				CK(ctx, cudaMemcpyAsync(d, h.data(), sizeof(uint2) * h.size(), cudaMemcpyHostToDevice, ctx->stream));
-				k.tw = d;
-			}
-			else
 			{
 				std::vector<float2> h((size_t)k.twn);
-				make_fstage_twiddles(k.N, h.data(), nullptr);
+				make_fstage_twiddles(k.N, h.data());
 				float2 *d = nullptr;
 				CK(ctx, dalloc(ctx, &d, h.size()));
 				CK(ctx, cudaMemcpyAsync(d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice, ctx->stream));

@@ -22,13 +22,12 @@
 //      1279-1286) and the post-F fringe phase of order 0 (mode.cpp:1061-1070),
 //      and stores its channels to the spectra [t][row][chan].
 //
-// Two arithmetic forms:
-//   out 0: FP32 FFT, spectra as float2 (the plain FP32 form);
-//   out 1: FP16 FFT with the two bands packed in half2 lanes (one instruction
-//          advances both polarisations), spectra as half2 or bf16x2 (re, im)
-//          for the tensor-core XMAC.  Samples are scaled by 2^-e so that no
-//          FFT value can leave the FP16 range; the outputs are rescaled
-//          exactly to X 2^-kTcSpecExp.
+// The FFT is FP32.  Two output forms:
+//   out 0: spectra as float2 [t][row][chan] (the plain FP32 form);
+//   out 1: spectra of the tensor-core forms, half2 or bf16x2 (re, im) of
+//          X 2^-kTcSpecExp in the blocked layout the tensor-core XMAC reads
+//          (one rounding per value, for the kinds the tensor-core FFT of
+//          fxb_fstage_tc.cu does not cover).
 //
 // Twiddles come from a per-length table laid out [pass][r - 1][p] (entry
 // w_N^(r p s) for pass stride s), so that the twiddle loads of a warp are
@@ -80,10 +79,8 @@ __host__ __device__ constexpr int tw_offset(int N, int pass)
 	return o;
 }
 
-// ---- lane values: FP32 complex (one band), packed FP16 complex (two bands)
+// ---- lane values: FP32 complex
 struct cf { float x, y; };
-struct hc { __half2 x, y; };      // x = (re band0, re band1), y = (im band0, im band1)
-struct hw { __half2 r, i; };      // twiddle as (wr, wr), (wi, wi)
 
 __device__ __forceinline__ cf add(cf a, cf b) { return {a.x + b.x, a.y + b.y}; }
 __device__ __forceinline__ cf sub(cf a, cf b) { return {a.x - b.x, a.y - b.y}; }
@@ -96,30 +93,7 @@ __device__ __forceinline__ cf rot45(cf a)                                       
 }
 __device__ __forceinline__ cf twid(cf a, float2 w) { return {a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x}; }
 
-__device__ __forceinline__ hc add(hc a, hc b) { return {__hadd2(a.x, b.x), __hadd2(a.y, b.y)}; }
-__device__ __forceinline__ hc sub(hc a, hc b) { return {__hsub2(a.x, b.x), __hsub2(a.y, b.y)}; }
-__device__ __forceinline__ hc add_mi(hc a, hc b) { return {__hadd2(a.x, b.y), __hsub2(a.y, b.x)}; }
-__device__ __forceinline__ hc add_pi(hc a, hc b) { return {__hsub2(a.x, b.y), __hadd2(a.y, b.x)}; }
-__device__ __forceinline__ hc rot45(hc a)
-{
-	const __half2 r = __float2half2_rn(0.70710678118654752440f);
-	return {__hmul2(__hadd2(a.x, a.y), r), __hmul2(__hsub2(a.y, a.x), r)};
-}
-__device__ __forceinline__ hc twid(hc a, hw w)
-{
-	return {__hfma2(a.x, w.r, __hneg2(__hmul2(a.y, w.i))), __hfma2(a.x, w.i, __hmul2(a.y, w.r))};
-}
-
 __device__ __forceinline__ float2 ldtw(const float2 *t, int i) { return __ldg(t + i); }
-__device__ __forceinline__ hw ldtw(const hw *t, int i)
-{
-	const uint2 u = __ldg((const uint2 *)t + i);
-	hw w;
-	w.r = *(const __half2 *)&u.x;
-	w.i = *(const __half2 *)&u.y;
-	return w;
-}
-
 // 8-byte shared-memory element <-> lane value
 template <typename C> __device__ __forceinline__ C lds(const uint2 *p);
 template <> __device__ __forceinline__ cf lds<cf>(const uint2 *p)
@@ -127,16 +101,7 @@ template <> __device__ __forceinline__ cf lds<cf>(const uint2 *p)
 	const float2 v = *(const float2 *)p;
 	return {v.x, v.y};
 }
-template <> __device__ __forceinline__ hc lds<hc>(const uint2 *p)
-{
-	const uint2 u = *p;
-	hc v;
-	v.x = *(const __half2 *)&u.x;
-	v.y = *(const __half2 *)&u.y;
-	return v;
-}
 __device__ __forceinline__ uint2 bits(cf v) { return make_uint2(__float_as_uint(v.x), __float_as_uint(v.y)); }
-__device__ __forceinline__ uint2 bits(hc v) { return make_uint2(*(const uint32_t *)&v.x, *(const uint32_t *)&v.y); }
 template <typename C> __device__ __forceinline__ void sts(uint2 *p, C v) { *p = bits(v); }
 template <typename C> __device__ __forceinline__ void sts2(uint2 *p, C a, C b)
 {
@@ -217,14 +182,11 @@ __device__ __forceinline__ uint32_t pack_spec(bool h16, float re, float im)
 	return *(const uint32_t *)&b;
 }
 
-// CTAs per SM the register budget is sized for: four for the FP16 form at
-// the lengths where 64 registers hold the kernel without spills (2048 points:
-// 6 % faster than three on the B200), else the shape's default
-template <typename C, int LOGN>
+// CTAs per SM the register budget is sized for
+template <int LOGN>
 constexpr int fstage_minb()
 {
-	return (std::is_same<C, hc>::value && (LOGN == 7 || LOGN == 8 || LOGN == 9 || LOGN == 11)) ? 4
-	                                                                                           : FShape<LOGN>::MINB;
+	return FShape<LOGN>::MINB;
 }
 
 constexpr int kMaxTQ = 4;         // FFT iterations per CTA at most
@@ -328,15 +290,14 @@ struct MidPasses {
 
 }  // namespace
 
-// C: lane type (cf: FP32, one band per value; hc: FP16, both bands per value);
-// NV: values per point (cf: bands of the item; hc: 1).
-template <typename C, int NV, int LOGN>
-__global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fstage(const FsArgs a)
+// NV: bands of the item (values per point); TCO: tensor-core spectra out.
+template <int NV, int LOGN, bool TCO>
+__global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstage(const FsArgs a)
 {
 	using SH = FShape<LOGN>;
+	using C = cf;
+	using TW = float2;
 	constexpr int N = SH::N, KB = SH::KB, TPF = SH::TPF, FPC = SH::FPC, PADN = SH::PADN, RL = SH::RL;
-	constexpr bool H = std::is_same<C, hc>::value;
-	using TW = typename std::conditional<H, hw, float2>::type;
 	extern __shared__ __align__(16) uint2 fsm[];
 	__shared__ float lut8[256];
 	__shared__ float2 lut4[16];            // two adjacent 2-bit bands -> (band0, band1) levels
@@ -369,17 +330,9 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 	const int row0 = g.row[0], row1 = g.row[1];
 	const uint32_t boff0 = (uint32_t)(g.band[0] * nbits), boff1 = (uint32_t)(g.band[1] * nbits);
 	const bool oneword = bpt <= 32;       // all bands of a sample time in one 32-bit word
-	const bool pair4 = (H || NV == 2) && nbits == 2 && oneword && boff1 == boff0 + 2;
+	const bool pair4 = NV == 2 && nbits == 2 && oneword && boff1 == boff0 + 2;
 	const int order = a.order;
-	int hexp = 0;
-	if(H)
-	{
-		// largest |X| is N times the largest level; keep it below 2^15
-		const float lvl = nbits == 2 ? 3.3359f : 38.8f;
-		while(lvl * (float)N > 32768.0f * (float)(1 << hexp))
-			hexp++;
-	}
-	const float hin = H ? ldexpf(1.0f, -hexp) : 1.0f, hout = H ? ldexpf(1.0f, hexp - kTcSpecExp) : 1.0f;
+	constexpr float osc = 1.0f / (float)(1 << kTcSpecExp);
 	const bool h16 = a.h16 != 0;
 	if(nbits == 8)
 	{
@@ -525,7 +478,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 					const uint32_t bit0 = tin * bpt + boff0, bit1 = tin * bpt + boff1;
 					const uint32_t *wp = (const uint32_t *)fp;
 					raw0[r] = ok ? __ldg(wp + (bit0 >> 5)) : 0u;
-					raw1[r] = (ok && !oneword && (H || NV == 2)) ? __ldg(wp + (bit1 >> 5)) : 0u;
+					raw1[r] = (ok && !oneword && NV == 2) ? __ldg(wp + (bit1 >> 5)) : 0u;
 					pk[r] = (bit0 & 31u) | ((bit1 & 31u) << 8) | ((uint32_t)ok << 16);
 					if(r < 7)
 					{
@@ -565,7 +518,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 						else
 						{
 							v0 = nbits == 2 ? level2(w0 & 3u) : lut8[w0 & 255u];
-							if(H || NV == 2)
+							if(NV == 2)
 							{
 								const uint32_t w1 = (oneword ? raw0[r] : raw1[r]) >> ((pk[r] >> 8) & 31u);
 								v1 = nbits == 2 ? level2(w1 & 3u) : lut8[w1 & 255u];
@@ -599,17 +552,9 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 						ph -= rintf(ph);
 						__sincosf(-6.283185307179586f * ph, &sn, &cs);
 					}
-					if constexpr(H)
-					{
-						x[0][r].x = __floats2half2_rn(v0 * cs * hin, v1 * cs * hin);
-						x[0][r].y = __floats2half2_rn(v0 * sn * hin, v1 * sn * hin);
-					}
-					else
-					{
-						x[0][r] = cf{v0 * cs, v0 * sn};
-						if constexpr(NV == 2)
-							x[1][r] = cf{v1 * cs, v1 * sn};
-					}
+					x[0][r] = cf{v0 * cs, v0 * sn};
+					if constexpr(NV == 2)
+						x[1][r] = cf{v1 * cs, v1 * sn};
 				}
 #pragma unroll
 				for(int j = 0; j < NV; j++)
@@ -691,11 +636,8 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 					turns -= rintf(turns);
 					float sn, cs;
 					__sincosf(6.283185307179586f * turns, &sn, &cs);
-					if constexpr(H)
+					if constexpr(TCO)
 					{
-						const hc v = y[0][r];
-						const float xr0 = __low2float(v.x) * hout, xi0 = cj * __low2float(v.y) * hout;
-						const float xr1 = __high2float(v.x) * hout, xi1 = cj * __high2float(v.y) * hout;
 						uint32_t *o;
 						int64_t rstride;
 						if(tcb)
@@ -709,10 +651,17 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<C, LOGN>()) k_fs
 							o = (uint32_t *)a.spec + obase + c;
 							rstride = nchan;
 						}
-						if(row0 >= 0)
-							o[(int64_t)row0 * rstride] = pack_spec(h16, xr0 * cs - xi0 * sn, xr0 * sn + xi0 * cs);
-						if(row1 >= 0)
-							o[(int64_t)row1 * rstride] = pack_spec(h16, xr1 * cs - xi1 * sn, xr1 * sn + xi1 * cs);
+						const float ocs = cs * osc, osn = sn * osc;
+#pragma unroll
+						for(int j = 0; j < NV; j++)
+						{
+							const int rw = j == 0 ? row0 : row1;
+							if(rw >= 0)
+							{
+								const float xr = y[j][r].x, xi = cj * y[j][r].y;
+								o[(int64_t)rw * rstride] = pack_spec(h16, xr * ocs - xi * osn, xr * osn + xi * ocs);
+							}
+						}
 					}
 					else
 					{
@@ -749,25 +698,25 @@ bool fstage_plan(int N, int nb, int out, FKind *k)
 	k->N = N;
 	k->nb = nb;
 	k->kb = N <= 2048 ? 1 : (N <= 8192 ? 2 : 4);
-	if(out == 0 && nb == 2 && k->kb != 1)
-		return false;                               // FP32 items of long FFTs hold one band
+	if(nb == 2 && k->kb != 1)
+		return false;                               // items of long FFTs hold one band
 	const int tpf = N / (8 * k->kb);
 	k->threads = tpf >= 256 ? tpf : 256;
 	k->fpc = k->threads / tpf;
-	const int nv = out == 1 ? 1 : nb;
+	const int nv = nb;
 	const size_t side = (size_t)k->fpc * nv * xpad(N) * 8;
 	k->pp = 2 * side <= 80 * 1024 ? 1 : 0;
 	k->smem = side * (k->pp ? 2 : 1);
 	k->tq = 4;
 	k->out = out;
-	k->items_fast = out == 1 ? 1 : 0;
+	k->items_fast = out == 1 ? 1 : 0;          // tensor-core spectra: a subband's stations side by side
 	k->twn = tw_offset(N, ilog2(N) / 3);
 	return k->smem <= 200 * 1024 && k->threads <= 512;
 }
 
 // Twiddle table of FFT length N in the kernel's [pass][r - 1][p] layout
 // (values computed in double): n = tw_offset(N, npass) entries.
-void make_fstage_twiddles(int N, float2 *out32, void *out16)
+void make_fstage_twiddles(int N, float2 *out32)
 {
 	int n8 = N / 8, s = 1, o = 0;
 	while(n8 >= 1)
@@ -776,18 +725,7 @@ void make_fstage_twiddles(int N, float2 *out32, void *out16)
 			for(int p = 0; p < n8; p++)
 			{
 				const double ang = -2.0 * M_PI * (double)((int64_t)r * p * s % N) / (double)N;
-				const double c = cos(ang), sn = sin(ang);
-				const int i = o + (r - 1) * n8 + p;
-				if(out32)
-					out32[i] = make_float2((float)c, (float)sn);
-				if(out16)
-				{
-					const __half hr = __double2half(c), hi = __double2half(sn);
-					const __half2 rr = __halves2half2(hr, hr), ii = __halves2half2(hi, hi);
-					uint2 *u = (uint2 *)out16 + i;
-					u->x = *(const uint32_t *)&rr;
-					u->y = *(const uint32_t *)&ii;
-				}
+				out32[o + (r - 1) * n8 + p] = make_float2((float)cos(ang), (float)sin(ang));
 			}
 		o += 7 * n8;
 		n8 /= 8;
@@ -795,38 +733,38 @@ void make_fstage_twiddles(int N, float2 *out32, void *out16)
 	}
 }
 
-template <typename C, int NV, int LOGN>
+template <int NV, int LOGN, bool TCO>
 static void launch_t(const FKind &k, const FsArgs &a, cudaStream_t stream)
 {
-	cudaFuncSetAttribute(k_fstage<C, NV, LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
-	cudaFuncSetAttribute(k_fstage<C, NV, LOGN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 	const int per = k.tq * k.fpc;
 	const int nt = (a.T + per - 1) / per;
 	const dim3 grid = a.items_fast ? dim3(k.count, nt) : dim3(nt, k.count);
-	k_fstage<C, NV, LOGN><<<grid, k.threads, k.smem, stream>>>(a);
+	k_fstage<NV, LOGN, TCO><<<grid, k.threads, k.smem, stream>>>(a);
 }
 
-template <typename C, int NV>
+template <int NV, bool TCO>
 static void launch_n(const FKind &k, const FsArgs &a, cudaStream_t stream)
 {
 	switch(k.N)
 	{
-	case 32: launch_t<C, NV, 5>(k, a, stream); break;
-	case 64: launch_t<C, NV, 6>(k, a, stream); break;
-	case 128: launch_t<C, NV, 7>(k, a, stream); break;
-	case 256: launch_t<C, NV, 8>(k, a, stream); break;
-	case 512: launch_t<C, NV, 9>(k, a, stream); break;
-	case 1024: launch_t<C, NV, 10>(k, a, stream); break;
-	case 2048: launch_t<C, NV, 11>(k, a, stream); break;
+	case 32: launch_t<NV, 5, TCO>(k, a, stream); break;
+	case 64: launch_t<NV, 6, TCO>(k, a, stream); break;
+	case 128: launch_t<NV, 7, TCO>(k, a, stream); break;
+	case 256: launch_t<NV, 8, TCO>(k, a, stream); break;
+	case 512: launch_t<NV, 9, TCO>(k, a, stream); break;
+	case 1024: launch_t<NV, 10, TCO>(k, a, stream); break;
+	case 2048: launch_t<NV, 11, TCO>(k, a, stream); break;
 	default:
 		if constexpr(NV == 1)
 		{
 			if(k.N == 4096)
-				launch_t<C, NV, 12>(k, a, stream);
+				launch_t<NV, 12, TCO>(k, a, stream);
 			else if(k.N == 8192)
-				launch_t<C, NV, 13>(k, a, stream);
+				launch_t<NV, 13, TCO>(k, a, stream);
 			else if(k.N == 16384)
-				launch_t<C, NV, 14>(k, a, stream);
+				launch_t<NV, 14, TCO>(k, a, stream);
 		}
 		break;
 	}
@@ -842,11 +780,16 @@ void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream)
 	a.tw = k.tw;
 	a.items_fast = k.items_fast;
 	if(k.out == 1)
-		launch_n<hc, 1>(k, a, stream);
+	{
+		if(k.nb == 2)
+			launch_n<2, true>(k, a, stream);
+		else
+			launch_n<1, true>(k, a, stream);
+	}
 	else if(k.nb == 2)
-		launch_n<cf, 2>(k, a, stream);
+		launch_n<2, false>(k, a, stream);
 	else
-		launch_n<cf, 1>(k, a, stream);
+		launch_n<1, false>(k, a, stream);
 }
 
 }  // namespace fxb

@@ -1,37 +1,46 @@
 // F stage of the tensor-core form with the FFT on the tensor cores (sm_100a).
 //
 // Mode::process (mpifxcorr/src/mode.cpp:845-1308) per FFT of N = 2048 points:
-// decode, fringe rotation, complex FFT, sideband selection, fractional-sample
-// rotation.  The FFT runs as the four-step factorisation N = 64 x 32
-// (n = 32 n1 + n2, k = k1 + 64 k2):
-//   Y[k1][n2] = sum_n1 F64[k1][n1] x[32 n1 + n2]         (MMA 1)
-//   Y[k1][n2] *= w_N^(n2 k1)                              (CUDA cores)
-//   X[k1 + 64 k2] = sum_n2 Y[k1][n2] F32[n2][k2]          (MMA 2, 16 values of k2)
-// with complex products written as real ones:
-//   MMA 1: rows (k1, re|im) of [[Fr, -Fi], [Fi, Fr]] (M = 128, K = 128 = (re|im, n1))
-//          times columns (FFT, n2) holding (x_re[n1], x_im[n1]) (N = 128: 4 FFTs);
-//   MMA 2: rows (FFT, k1) holding (Y_re[n2], Y_im[n2]) (M = 128: 2 FFTs, K = 64)
-//          times columns (re|im, k2) of [[Fr, Fi], [-Fi, Fr]] (N = 32).
-// Operands are FP16 (11-bit significands) with FP32 accumulation in tensor
-// memory: |x| <= 38.8 (8-bit levels), so every FP16 value stays in range.
+// VDIF decode, fringe rotation, complex FFT, sideband selection and
+// fractional-sample rotation.  The FFT runs as the four-step factorisation
+// N = 32 x 64 (n = 64 n1 + n2, k = k1 + 32 k2):
+//   Y[k1][n2] = sum_n1 x[64 n1 + n2] w_32^(n1 k1)        (MMA 1)
+//   Z[k1][n2] = Y[k1][n2] w_2048^(n2 k1)                 (CUDA cores, FP32)
+//   X[k1 + 32 k2] = sum_n2 Z[k1][n2] w_64^(n2 k2)         (MMA 2, the 32 k2 of the sideband)
+// with complex products written as real ones.  Operands are FP16 (11-bit
+// significands), accumulation FP32 in tensor memory; the samples, the
+// twiddled intermediate and the output are each rounded to FP16 once.
 //
-// A work unit is one subband of one station (its one or two polarisation
-// bands) at two consecutive FFT times: 4 FFTs.  CTAs are persistent (two per
-// SM); per unit the 256 threads
-//   1. decode: thread (time, n1 quarter, n2) issues the loads of its 16 VDIF
-//      words x[32 n1 + n2] (both bands share a word), then forms the fringe-
-//      rotated samples (rotator advanced by the per-FFT step exp(-2 pi i 32 a))
-//      and stores them as FP16 into the K-major operand tile,
-//   2. one thread issues MMA 1 (8 x K = 16), all wait on its mbarrier,
-//   3. twiddle: each thread reads its accumulator row (k1, re|im), combines it
-//      with the neighbouring lane's (the other part), multiplies by the
-//      twiddle and stores FP16 rows (FFT, k1) over the spent operand tile,
-//   4. one thread issues MMA 2 (2 tiles x 4 x K = 16), all wait,
-//   5. output: each thread reads row (FFT, k1) = 16 channels c = k1 + 64 j,
-//      applies exp(+2 pi i f_c fse) (advanced by exp(2 pi i 64 dfs)) and stores
-//      bf16x2 into the blocked spectra [t][block][row][tcb].
-// Every wait is bounded; a timeout sets the error flag, the CTA waits
-// (bounded) for its MMAs and still frees its tensor memory.
+// A work unit is one station at one FFT time with two subbands of equal
+// sideband (four FFTs: subband sb, polarisation p, channel ch = 2 sb + p).
+//   MMA 1: A = samples, MN-major (M = 128 rows (p, n2) per subband, K = 64 =
+//          (re|im, n1)); B = the real-ified DFT-32 (N = 64 = (k1, re|im)),
+//          K-major.  One thread (tensor-memory lane (p, n2)) then holds
+//          Y[.][n2] of both parts for all k1.
+//   MMA 2: A = Z, MN-major (M = 128 rows (ch, k1), K = 128 = (re|im, n2));
+//          B = the real-ified DFT-64 columns of the sideband (N = 64 =
+//          (k2, re|im)), K-major.  Lane (ch, k1) holds channels k1 + 32 k2.
+// MN-major operands let each thread store 16-byte runs: the decode writes 8
+// consecutive times n2 of one n1, the twiddle 8 consecutive k1 of one n2.
+//
+// Persistent CTAs (one per SM), warp-specialised:
+//   warp 13     producer: builds the records of 32 units at a time (one lane
+//               per unit: pair, FFT parameters, fringe and fractional-sample
+//               constants, output offsets) into a shared-memory ring and
+//               stages each unit's VDIF window into shared memory (bulk
+//               copies of the valid frames),
+//   warps 0-3   decode: 8 consecutive times -> the fringe-rotated FP16
+//               samples of the unit's four channels (two-time lookup of
+//               both polarisations, FP32 rotation),
+//   warps 4-7   twiddle: D1 (tensor memory) -> Z (FP16 operand, in the
+//               operand buffer MMA 1 has finished with),
+//   warps 8-11  output: D2 -> fractional-sample rotation -> FP16 (or BF16) spectra,
+//   warp 12     MMA issuer (one thread).
+// Three operand buffers and two tensor-memory slots (D1 + D2 per slot)
+// keep decode, MMAs, twiddle and output of different units overlapped.
+// Every wait is bounded; a timeout sets the error flag, the CTA stops,
+// waits (bounded) for its copies and MMAs in flight and frees its tensor
+// memory.
 
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -49,16 +58,42 @@ namespace fxb {
 
 namespace {
 
-constexpr int kN = 2048, kN1 = 64, kN2 = 32;
-constexpr int kThreadsF = 256;
-constexpr int kTileB = 2 * 128 * 128;          // MMA 1 operand: 2 K blocks x 128 columns x 128 bytes
-constexpr int kA1 = 2 * 128 * 128;             // DFT-64 matrix: 2 K blocks x 128 rows x 128 bytes
-constexpr int kB3 = 32 * 128;                  // DFT-32 columns of one sideband
+constexpr int kN = 2048, kN1 = 32, kN2 = 64;
+constexpr int kNS = 3;                          // operand buffers
+constexpr int kOpBytes = 32768;                 // A1 (two 16 KB tiles) or A2 (32 KB)
+constexpr int kB1Bytes = 64 * 128;              // DFT-32: 64 rows x 128 bytes (K = 64)
+constexpr int kB2Bytes = 2 * 64 * 128;          // DFT-64 of one sideband: 2 K halves x 64 rows x 128 bytes
+constexpr int kOffB1 = 0, kOffB2 = kB1Bytes;
+constexpr int kTablesBytes = kOffB2 + 2 * kB2Bytes;
+constexpr int kOffOp = kTablesBytes;            // 1024-aligned
+// 14 warps: the SM sub-partitions that hold four of them give each thread at
+// most 128 registers
+constexpr int kThreadsTc = 448;
 constexpr uint32_t kWaitLimitF = 1u << 22;
+constexpr int kTmemCols = 512;
+
+static_assert(kOffOp % 1024 == 0, "operand buffers must be 1024-aligned");
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ bool mbar_wait_f(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(su32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(su32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(su32(bar)), "r"(bytes) : "memory");
+}
+
+// bounded wait for the phase with parity `parity`; gives up early once
+// another role has recorded a failure
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *fail)
 {
 	const uint32_t a = su32(bar);
 	for(uint32_t it = 0; it < kWaitLimitF; it++)
@@ -73,12 +108,25 @@ __device__ __forceinline__ bool mbar_wait_f(uint64_t *bar, uint32_t parity)
 		    : "memory");
 		if(done)
 			return true;
+		if((it & 255u) == 255u && *fail)
+			return false;
 	}
 	return false;
 }
 
-// K-major, 128-byte swizzle (8-row groups 1024 bytes apart), tcgen05 version
-__device__ __forceinline__ uint64_t sdesc128(uint32_t saddr)
+// global -> shared bulk copy (both addresses and the size multiples of 16),
+// completion counted in bytes on the mbarrier
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+	asm volatile(
+	    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(su32(dst)),
+	    "l"(src), "r"(bytes), "r"(su32(bar))
+	    : "memory");
+}
+
+// shared-memory matrix descriptors (tcgen05 version 1, 128-byte swizzle)
+// K-major: rows of 128 bytes, 8-row groups 1024 bytes apart
+__device__ __forceinline__ uint64_t desc_k128(uint32_t saddr)
 {
 	uint64_t d = 0;
 	d |= (uint64_t)((saddr >> 4) & 0x3FFF);
@@ -87,6 +135,27 @@ __device__ __forceinline__ uint64_t sdesc128(uint32_t saddr)
 	d |= (uint64_t)1 << 46;
 	d |= (uint64_t)2 << 61;
 	return d;
+}
+// MN-major: 1024-byte atoms of 8 K rows x 64 MN values; the two MN atoms of
+// a 128-row tile 1024 bytes apart (leading byte offset), K atoms 2048 bytes
+// apart (stride byte offset)
+__device__ __forceinline__ uint64_t desc_mn128(uint32_t saddr)
+{
+	uint64_t d = 0;
+	d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+	d |= (uint64_t)(1024 >> 4) << 16;
+	d |= (uint64_t)(2048 >> 4) << 32;
+	d |= (uint64_t)1 << 46;
+	d |= (uint64_t)2 << 61;
+	return d;
+}
+
+// byte offset of element (m, k) in a 128-row MN-major tile laid out
+// [k / 8][m / 64][k % 8][128 bytes] with the 128-byte swizzle
+__device__ __forceinline__ uint32_t mn_off(int m, int k)
+{
+	const int r = k & 7;
+	return (uint32_t)((k >> 3) * 2048 + (m >> 6) * 1024 + r * 128 + ((((m & 63) >> 3) ^ r) << 4) + (m & 7) * 2);
 }
 
 __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -116,11 +185,12 @@ __device__ __forceinline__ void tld32(uint32_t taddr, float *v)
 	      "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
 	      "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
 	    : "r"(taddr));
-	asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
 	for(int i = 0; i < 32; i++)
 		v[i] = __uint_as_float(r[i]);
 }
+
+__device__ __forceinline__ void tld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t pack_h2(float a, float b)
 {
@@ -128,8 +198,14 @@ __device__ __forceinline__ uint32_t pack_h2(float a, float b)
 	return *(const uint32_t *)&h;
 }
 
-// byte offset of 16-byte chunk `chunk` of row `row` in a K-major SW128 tile
-__device__ __forceinline__ int swz(int row, int chunk) { return row * 128 + ((chunk ^ (row & 7)) << 4); }
+// one spectral value of the tensor-core forms: (re, im) as half2 or bf16x2
+__device__ __forceinline__ uint32_t pack_spec(bool h16, float re, float im)
+{
+	if(h16)
+		return pack_h2(re, im);
+	const __nv_bfloat162 b = __floats2bfloat162_rn(re, im);
+	return *(const uint32_t *)&b;
+}
 
 __device__ __forceinline__ float level2f(uint32_t code)
 {
@@ -139,203 +215,194 @@ __device__ __forceinline__ float level2f(uint32_t code)
 
 __device__ __forceinline__ float fracc(double x) { return (float)(x - rint(x)); }
 
-// constants of one FFT time of the unit
-struct TcFftConst {
-	float c0r, c0i;          // unused padding for alignment
-	float P0, alpha;         // fringe phase (turns): start, per sample
-	float Ur, Ui;            // rotator step over 32 samples: exp(-2 pi i 32 alpha)
-	float dfs, postf;        // fractional-sample turns per channel, order-0 post-F turns
-	float Rr, Ri;            // fractional-sample step over 64 channels: exp(2 pi i 64 dfs)
-	uint32_t fa, so, fmask;
-	int32_t stuck, flags;    // flags: 1 valid FFT, 2 fmask covers the window
-	int32_t t;
+// Everything the roles need of one work unit, built by the producer warp
+// (one lane per unit, 32 units at a time) into a shared-memory ring.
+struct UnitRec {
+	float P0[2], alpha[2];        // fringe phase (turns) at n = 0 and per sample, per subband
+	float Sr[2], Si[2];           // rotator step per sample exp(-2 pi i alpha)
+	uint32_t fmask;               // validity of the window's frames (bit j: frame fa + j)
+	int32_t so, fs;               // window start within frame fa, samples per frame
+	int32_t swbits;               // staged bit of sample 0
+	int32_t nib[2];               // 4-bit field of each subband's two bands in a time
+	int32_t flags;                // kOk, kAllValid, kManual, kHas0, kHas1, kLsb0, kLsb1
+	uint32_t fa;                  // first frame of the window
+	int64_t a0;                   // first staged byte of the payloads from frame fa on
+	int32_t nstage, station;      // staged bytes; station
+	int32_t t;                    // FFT time
+	float dfs;                    // fractional-sample turns per channel
+	float postf[2];               // order-0 post-F turns per subband
+	int32_t row[2][2];            // spectra row of [subband][polarisation] (-1: not written)
+	int64_t spec[2];              // first spectra value of the subband's [t][block][row][tcb] block
+	int32_t tnblk[2], nrow[2], tcb[2];
+};
+enum : int32_t { kOk = 1, kAllValid = 2, kManual = 4, kHas0 = 8, kHas1 = 16, kLsb0 = 32, kLsb1 = 64 };
+constexpr int kRing = 16;         // unit records in flight (>= staging + operand buffers + 2, with margin)
+constexpr int kNStg = 3;          // VDIF staging buffers
+
+template <int BPT>
+struct TcLayout {
+	static constexpr int kStgBytes = kN * BPT / 8 + 64;   // one window, 16-byte slack either side
+	static constexpr int kOffStg = kOffOp + kNS * kOpBytes;
+	static constexpr int kOffLut = kOffStg + kNStg * kStgBytes;
+	static constexpr int kOffTw = kOffLut + 256 * 16;     // twiddles w_2048^(n2 k1), float2 [k1][n2]
+	static constexpr int kOffRing = kOffTw + kN1 * kN2 * 8;
+	static constexpr int kUsed = kOffRing + kRing * (int)sizeof(UnitRec);
+	static constexpr size_t kSmem = 1024 + (size_t)kUsed;
+	static_assert(kOffStg % 16 == 0 && kStgBytes % 16 == 0, "staging must be 16-aligned");
+	static_assert(kSmem <= 227 * 1024, "shared memory");
 };
 
-}  // namespace
-
-
-// Shared-memory layout (bytes from a 1024-aligned base): DFT-64 matrix,
-// DFT-32 columns (upper, lower sideband), twiddles [n2][k1] (float2), the
-// operand tile of MMA 1 (reused for the operand tiles of MMA 2), and the
-// staging of the next unit's VDIF words ([sample][thread]).
-constexpr int kOffB3 = kA1, kOffTw = kA1 + 2 * kB3, kOffB = kOffTw + kN2 * kN1 * 8;
-constexpr int kOffStage = kOffB + kTileB;
-constexpr int kTablesBytes = kOffB;                 // copied from the table in global memory
-constexpr size_t kSmemTc = 1024 + (size_t)kOffStage + 16 * kThreadsF * 4;
-
-namespace {
-
-// fields of one work unit (subband of one station, two FFT times)
-struct TcUnit {
-	const uint8_t *buf;
-	uint32_t fs, bpt, boff0, boff1;
-	int nbits, header, framebytes, station, freq, row0, row1, t0;
-	bool lsb, oneword, pair4;
-	double lo, bw;
-};
-
-__device__ __forceinline__ TcUnit tc_unit(const FsArgs &a, int u, int count)
-{
-	TcUnit U;
-	const FGroup &g = a.groups[a.first + u % count];     // work items fastest: a subband's stations together
-	const DevStation *Sp = a.st + g.station;
-	U.station = g.station;
-	U.freq = g.freq;
-	U.row0 = g.row[0];
-	U.row1 = g.row[1];
-	U.lsb = g.lsb != 0;
-	U.lo = g.lofreq;
-	U.fs = (uint32_t)Sp->framesamples;
-	U.nbits = Sp->nbits;
-	U.bpt = (uint32_t)(Sp->nband * U.nbits);
-	U.header = Sp->header;
-	U.framebytes = Sp->framebytes;
-	U.bw = Sp->bw;
-	U.buf = a.sub[g.station].buf;
-	U.boff0 = (uint32_t)(g.band[0] * U.nbits);
-	U.boff1 = (uint32_t)(g.band[1] * U.nbits);
-	U.oneword = U.bpt <= 32;
-	U.pair4 = U.nbits == 2 && U.oneword && U.boff1 == U.boff0 + 2;
-	U.t0 = (u / count) * 2;
-	return U;
-}
-
-// constants of FFT time t of a unit from its FFT parameters (mode.cpp:906-1097)
-__device__ __forceinline__ TcFftConst tc_consts(const TcUnit &U, const FftParam &p, int t, int T, int order,
-                                               int fraclo)
+// the producer lane's record of unit k (u = blockIdx.x + k gridDim.x)
+template <int BPT>
+__device__ __forceinline__ UnitRec build_unit(const FsArgs &a, const int32_t *pairs, int npairs, int u)
 {
 	constexpr int nchan = kN / 2;
-	TcFftConst c;
-	memset(&c, 0, sizeof(c));
-	c.Ur = 1.0f;
-	c.Rr = 1.0f;
-	c.t = t;
-	if(t >= T || p.status != kFftOk)
-		return c;
-	c.flags = 1 | (p.mflags ? 2 : 0);
-	c.fmask = p.fmask;
-	const uint32_t g0 = (uint32_t)p.nearest;
-	c.fa = g0 / U.fs;
-	c.so = g0 - c.fa * U.fs;
-	c.stuck = p.stuck;
-	const int idl = p.integerdelay;
-	const double fl = fraclo ? (U.lo - (int)U.lo) * (double)idl : 0.0;
-	if(order == 1)
+	UnitRec r;
+	memset(&r, 0, sizeof(r));
+	r.Sr[0] = r.Sr[1] = 1.0f;
+	const int pi = u % npairs;
+	r.t = u / npairs;
+	const int gi[2] = {pairs[2 * pi], pairs[2 * pi + 1]};
+	const FGroup g0 = a.groups[gi[0]];
+	const int s = g0.station;
+	r.station = s;
+	const DevStation *Sp = a.st + s;
+	const FftParam p = a.params[(int64_t)s * a.T + r.t];
+	r.fs = Sp->framesamples;
+	const double bw = Sp->bw;
+	for(int sb = 0; sb < 2; sb++)
 	{
-		c.P0 = fracc(U.lo * p.b + fl);
-		c.alpha = (float)(U.lo * p.a * (1.0 / kN));
-		const double step = U.lo * p.a * (32.0 / kN);
-		float sn, cs;
-		sincospif((float)(-2.0 * (step - rint(step))), &sn, &cs);
-		c.Ur = cs;
-		c.Ui = sn;
-	}
-	c.dfs = (float)(U.bw * (1.0 / nchan) * (double)p.fse);
-	if(order == 0)
-	{
-		double pr = (p.averagedelay - idl) * U.lo;
-		if(fraclo)
-			pr += idl * (U.lo - (int)U.lo);
-		c.postf = -(float)(pr - (int)pr);
-	}
-	const double r64 = U.bw * (64.0 / nchan) * (double)p.fse;
-	float sn, cs;
-	sincospif((float)(2.0 * (r64 - rint(r64))), &sn, &cs);
-	c.Rr = cs;
-	c.Ri = sn;
-	return c;
-}
-
-__device__ __forceinline__ void cp_async4(uint32_t dst, const void *src, uint32_t bytes)
-{
-	asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
-}
-
-// Issue the loads of this thread's 16 VDIF words x[32 n1 + n2] of a unit
-// (n1 in the warp's quarter, times by warp half) into the staging; invalid
-// samples are zero-filled without a load.  Returns the valid-sample bits.
-__device__ __forceinline__ uint32_t tc_prefetch(const FsArgs &a, const TcUnit &U, const TcFftConst &c, uint32_t stage_addr,
-                                                int warp, int lane, int tid)
-{
-	const int q4 = warp & 3, n2 = lane;
-	const bool active = (c.flags & 1) != 0, narrow = (c.flags & 2) != 0;
-	const uint8_t *vrow = a.valid + (int64_t)U.station * a.valid_stride;
-	const int nfirst = n2 + 32 * 16 * q4;
-	const uint32_t xs = c.so + (uint32_t)nfirst;
-	uint32_t kf = xs / U.fs, tin = xs - kf * U.fs;
-	const uint8_t *fp = U.buf + ((int64_t)c.fa + kf) * U.framebytes + U.header;
-	uint32_t okm = 0;
-#pragma unroll
-	for(int i = 0; i < 16; i++)
-	{
-		const int n = nfirst + 32 * i;
-		bool ok;
-		if(narrow)
-			ok = (c.fmask >> kf) & 1u;
-		else
+		r.row[sb][0] = r.row[sb][1] = -1;
+		if(gi[sb] < 0)
+			continue;
+		const FGroup g = sb == 0 ? g0 : a.groups[gi[sb]];
+		const DevFreqPlan &P = a.plans[g.freq];
+		r.flags |= (sb == 0 ? kHas0 : kHas1) | (g.lsb ? (sb == 0 ? kLsb0 : kLsb1) : 0);
+		r.nib[sb] = g.band[0] >> 1;
+		r.row[sb][0] = g.row[0];
+		r.row[sb][1] = g.row[1];
+		r.spec[sb] = P.spec_off + (int64_t)r.t * P.tnblk * P.nrow * P.tcb;
+		r.tnblk[sb] = P.tnblk;
+		r.nrow[sb] = P.nrow;
+		r.tcb[sb] = P.tcb;
+		if(p.status != kFftOk)
+			continue;
+		const double lo = g.lofreq;
+		const int idl = p.integerdelay;
+		if(a.order == 1)
 		{
-			const int64_t fr = (int64_t)c.fa + kf;
-			ok = active && fr < a.valid_stride && vrow[fr] != 0;
+			const double fl = a.fraclo ? (lo - (int)lo) * (double)idl : 0.0;
+			r.P0[sb] = fracc(lo * p.b + fl);
+			r.alpha[sb] = (float)(lo * p.a * (1.0 / kN));
+			float sn, cs;
+			sincospif(-2.0f * r.alpha[sb], &sn, &cs);
+			r.Sr[sb] = cs;
+			r.Si[sb] = sn;
 		}
-		ok = ok && n < c.stuck;
-		const uint32_t bit0 = tin * U.bpt + U.boff0;
-		const void *src = ok ? (const void *)((const uint32_t *)fp + (bit0 >> 5)) : (const void *)U.buf;
-		cp_async4(stage_addr + (uint32_t)(i * kThreadsF + tid) * 4u, src, ok ? 4u : 0u);
-		okm |= (uint32_t)ok << i;
-		if(i < 15)
+		else if(a.order == 0)
 		{
-			tin += 32u;
-			while(tin >= U.fs)
-			{
-				tin -= U.fs;
-				kf++;
-				fp += U.framebytes;
-			}
+			double pr0 = (p.averagedelay - idl) * lo;
+			if(a.fraclo)
+				pr0 += idl * (lo - (int)lo);
+			r.postf[sb] = -(float)(pr0 - (int)pr0);
 		}
 	}
-	asm volatile("cp.async.commit_group;\n" ::: "memory");
-	return okm;
+	if(p.status == kFftOk)
+	{
+		r.flags |= kOk;
+		const uint32_t g = (uint32_t)p.nearest;
+		r.fa = g / (uint32_t)r.fs;
+		r.so = (int32_t)(g - r.fa * (uint32_t)r.fs);
+		r.fmask = p.fmask;
+		const int nwf = (r.so + kN - 1) / r.fs + 1;
+		if(nwf < 32 ? (r.fmask == (1u << nwf) - 1u) : r.fmask == 0xFFFFFFFFu)
+			r.flags |= kAllValid;
+		r.dfs = (float)(bw * (1.0 / nchan) * (double)p.fse);
+		// the window's times [so, so + N) of the payloads from frame fa on, 16-byte aligned
+		const int64_t b0 = (int64_t)r.so * BPT, b1 = (int64_t)(r.so + kN) * BPT;
+		r.a0 = (b0 >> 3) & ~(int64_t)15;
+		const int64_t a1 = (((b1 + 7) >> 3) + 15) & ~(int64_t)15;
+		r.swbits = (int32_t)(b0 - 8 * r.a0);
+		r.nstage = (int32_t)(a1 - r.a0);
+		if(((uintptr_t)a.sub[s].buf & 15u) != 0)
+			r.flags |= kManual;
+	}
+	return r;
 }
 
 }  // namespace
 
-__global__ void __launch_bounds__(kThreadsF, 2) k_fstage_tc(const FsArgs a, const uint4 *__restrict__ tables,
-                                                         int count, int nunits, int32_t *err)
+// tables: DFT-32 (B of MMA 1), DFT-64 upper and lower sideband (B of MMA 2),
+// in their shared-memory byte layouts.  pairs: [npairs][2] FGroup indices of
+// the two subbands of a work unit (-1: none); unit u = pair u % npairs at
+// FFT time u / npairs.  BPT: bits per time of the stations' VDIF words
+// (2-bit bands: 2 x bands).
+template <int BPT>
+__global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, const uint4 *__restrict__ tables,
+                                                          const int32_t *__restrict__ pairs, int npairs, int nunits,
+                                                          int32_t *err)
 {
+	using LY = TcLayout<BPT>;
 	extern __shared__ __align__(1024) unsigned char fsm_tc[];
-	__shared__ float lut8[256];
-	__shared__ float2 lut4[16];
-	__shared__ TcFftConst fc[2][2];                 // [unit parity][time of the unit]
-	__shared__ uint32_t okms[kThreadsF];            // valid-sample bits of each thread's staged words
-	__shared__ TcUnit tus[2];                       // [unit parity] fields of the unit
-	__shared__ uint64_t mb1, mb2, mbd;
+	__shared__ uint64_t stg_full[kNStg], stg_empty[kNStg], op_full[kNS], op_empty[kNS], d1_full[2], d1_empty[2],
+	    a2_full[2], d2_full[2], d2_empty[2], mma_done;
 	__shared__ uint32_t tmem_s;
+	__shared__ volatile int fail_s;
+	__shared__ int stg_issued_s, stg_used_s;
 	unsigned char *base = (unsigned char *)(((uintptr_t)fsm_tc + 1023) & ~(uintptr_t)1023);
-	unsigned char *sB = base + kOffB;
-	const float2 *stw = (const float2 *)(base + kOffTw);
-	const uint32_t *stage = (const uint32_t *)(base + kOffStage);
-	const uint32_t stage_addr = su32(base + kOffStage);
+	unsigned char *ops = base + kOffOp;
+	unsigned char *stg = base + LY::kOffStg;
+	float4 *lut = (float4 *)(base + LY::kOffLut);
+	float2 *twt = (float2 *)(base + LY::kOffTw);
+	UnitRec *ring = (UnitRec *)(base + LY::kOffRing);
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 	const int order = a.order;
 	constexpr int nchan = kN / 2;
+	const int nk = ((int)blockIdx.x < nunits) ? (nunits - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
 
-	for(int i = tid; i < kTablesBytes / 16; i += kThreadsF)
+	for(int i = tid; i < kTablesBytes / 16; i += blockDim.x)
 		((uint4 *)base)[i] = __ldg(tables + i);
-	for(int i = tid; i < 256; i += kThreadsF)
-		lut8[i] = (float)((i - 128) / 3.3);               // format_vdif.c:122
-	if(tid < 16)
-		lut4[tid] = make_float2(level2f(tid & 3u), level2f(tid >> 2));
+	// two times of both polarisations of one subband: index = nibble(t) |
+	// nibble(t + 1) << 4, nibble = code(p0) | code(p1) << 2 (format_vdif.c:78)
+	for(int i = tid; i < 256; i += blockDim.x)
+		lut[i] = make_float4(level2f(i & 3u), level2f((i >> 4) & 3u), level2f((i >> 2) & 3u), level2f((i >> 6) & 3u));
+	for(int i = tid; i < kN1 * kN2; i += blockDim.x)
+	{
+		const int k1 = i / kN2, n2 = i - k1 * kN2;
+		float sn, cs;
+		sincospif(-(float)(n2 * k1) / (float)(kN / 2), &sn, &cs);
+		twt[i] = make_float2(cs, sn);
+	}
 	if(tid == 0)
 	{
-		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(su32(&mb1)));
-		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(su32(&mb2)));
-		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(su32(&mbd)));
+		for(int i = 0; i < kNStg; i++)
+		{
+			mbar_init(&stg_full[i], 1);
+			mbar_init(&stg_empty[i], 4);
+		}
+		for(int i = 0; i < 2; i++)
+		{
+			mbar_init(&d1_full[i], 1);
+			mbar_init(&d1_empty[i], 4);
+			mbar_init(&a2_full[i], 4);
+			mbar_init(&d2_full[i], 1);
+			mbar_init(&d2_empty[i], 4);
+		}
+		for(int i = 0; i < kNS; i++)
+		{
+			mbar_init(&op_full[i], 4);
+			mbar_init(&op_empty[i], 1);
+		}
+		mbar_init(&mma_done, 1);
+		fail_s = 0;
+		stg_issued_s = 0;
+		stg_used_s = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 	}
-	if(warp == 0)
+	if(warp == 12)
 	{
 		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(su32(&tmem_s)),
-		             "r"(256u));
+		             "r"((uint32_t)kTmemCols));
 		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
 	}
 	asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");      // tables -> tensor-core reads
@@ -344,295 +411,458 @@ __global__ void __launch_bounds__(kThreadsF, 2) k_fstage_tc(const FsArgs a, cons
 	asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 	const uint32_t tmem = tmem_s;
 
-	// prologue: constants and word loads of the first unit
-	const int u0 = blockIdx.x;
-	if(u0 < nunits)
+	if(warp == 13)
 	{
-		if(tid == 0)
-			tus[0] = tc_unit(a, u0, count);
-		__syncthreads();
-		const TcUnit &U = tus[0];
-		if(warp < 2 && lane == 0)
+		// ================================================================ producer
+		bool ok = true;
+		for(int kb = 0; kb < nk && ok; kb += 32)
 		{
-			const int t = U.t0 + warp;
-			FftParam p;
-			p.status = kFftZero;
-			if(t < a.T)
-				p = a.params[(int64_t)U.station * a.T + t];
-			fc[0][warp] = tc_consts(U, p, t, a.T, order, a.fraclo);
-		}
-		__syncthreads();
-		okms[tid] = tc_prefetch(a, U, fc[0][warp >> 2], stage_addr, warp, lane, tid);
-	}
-
-	int ku = 0;
-	for(int u = u0; u < nunits; u += gridDim.x, ku++)
-	{
-		const int slot = ku & 1;
-		const TcUnit &U = tus[slot];
-		const int un = u + gridDim.x;
-		const bool has_next = un < nunits;
-		// the next unit's fields and FFT parameters (lanes 0 of warps 0, 1):
-		// loads in flight during this decode
-		TcUnit Un;
-		FftParam pn;
-		pn.status = kFftZero;
-		if(has_next && warp < 2 && lane == 0)
-		{
-			Un = tc_unit(a, un, count);
-			if(Un.t0 + warp < a.T)
-				pn = a.params[(int64_t)Un.station * a.T + Un.t0 + warp];
-		}
-		asm volatile("cp.async.wait_all;\n" ::: "memory");
-		__syncthreads();
-
-		// ---- (b) decode x[32 n1 + n2] (n1 in this warp's quarter) from the
-		// staged words into the operand of MMA 1: column (FFT = 2 time + band,
-		// n2), K = (re|im, n1)
-		{
-			const int tl = warp >> 2, q4 = warp & 3, n2 = lane;
-			const TcFftConst &c = fc[slot][tl];
-			const uint32_t okm = okms[tid];
-			const int nfirst = n2 + 32 * 16 * q4;
-			const uint32_t xs = c.so + (uint32_t)nfirst;
-			uint32_t kf = xs / U.fs, tin = xs - kf * U.fs;
-			const uint8_t *fp = U.buf + ((int64_t)c.fa + kf) * U.framebytes + U.header;
-			float ph = c.P0 + (float)nfirst * c.alpha;
-			ph -= rintf(ph);
-			float rr, ri;
-			__sincosf(-6.283185307179586f * ph, &ri, &rr);
-#pragma unroll
-			for(int h = 0; h < 2; h++)
+			UnitRec r;
+			if(kb + lane < nk)
+				r = build_unit<BPT>(a, pairs, npairs, (int)blockIdx.x + (kb + lane) * (int)gridDim.x);
+			for(int i = 0; i < 32 && kb + i < nk; i++)
 			{
-				uint32_t re0[4], im0[4], re1[4], im1[4];
-#pragma unroll
-				for(int i2 = 0; i2 < 4; i2++)
+				const int k = kb + i, slot = k % kNStg;
+				// every lane takes the same decision (the warp meets at __syncwarp below)
+				const bool okw = k < kNStg || mbar_wait(&stg_empty[slot], (uint32_t)((k / kNStg) - 1) & 1u, &fail_s);
+				if(!__all_sync(0xffffffffu, okw))
 				{
-					float x0r[2], x0i[2], x1r[2], x1i[2];
-#pragma unroll
-					for(int e = 0; e < 2; e++)
+					fail_s = 10;
+					ok = false;
+					break;
+				}
+				if(lane == i)
+				{
+					ring[k % kRing] = r;
+					uint32_t want = 0;
+					const bool copy = (r.flags & kOk) && !(r.flags & kManual);
+					const int nwf = (r.so + kN - 1) / r.fs + 1;
+					const DevStation *Sp = a.st + r.station;
+					const int P = Sp->payload;
+					const int64_t a1 = r.a0 + r.nstage;
+					for(int j = 0; copy && j < nwf && j < 32; j++)
 					{
-						const int i = 8 * h + 2 * i2 + e;
-						float v0 = 0.0f, v1 = 0.0f;
-						if((okm >> i) & 1u)
+						const int64_t f0 = (int64_t)j * P, lo_ = r.a0 > f0 ? r.a0 : f0, hi_ = a1 < f0 + P ? a1 : f0 + P;
+						if(hi_ > lo_ && ((r.fmask >> j) & 1u))
+							want += (uint32_t)(hi_ - lo_);
+					}
+					if(want)
+					{
+						// the byte count is armed before the copies that complete it
+						mbar_expect_tx(&stg_full[slot], want);
+						unsigned char *dst = stg + slot * LY::kStgBytes;
+						const uint8_t *buf = a.sub[r.station].buf;
+						for(int j = 0; j < nwf && j < 32; j++)
 						{
-							const uint32_t bit0 = tin * U.bpt + U.boff0;
-							const uint32_t raw = stage[i * kThreadsF + tid];
-							const uint32_t w0 = raw >> (bit0 & 31u);
-							if(U.pair4)
-							{
-								const float2 l = lut4[w0 & 15u];
-								v0 = l.x;
-								v1 = l.y;
-							}
-							else
-							{
-								const uint32_t bit1 = tin * U.bpt + U.boff1;
-								const uint32_t w1 = (U.oneword ? raw : __ldg((const uint32_t *)fp + (bit1 >> 5))) >> (bit1 & 31u);
-								v0 = U.nbits == 2 ? level2f(w0 & 3u) : lut8[w0 & 255u];
-								v1 = U.nbits == 2 ? level2f(w1 & 3u) : lut8[w1 & 255u];
-							}
-						}
-						x0r[e] = v0 * rr;
-						x0i[e] = v0 * ri;
-						x1r[e] = v1 * rr;
-						x1i[e] = v1 * ri;
-						const float nr = rr * c.Ur - ri * c.Ui;
-						ri = rr * c.Ui + ri * c.Ur;
-						rr = nr;
-						if(i < 15)
-						{
-							tin += 32u;
-							while(tin >= U.fs)
-							{
-								tin -= U.fs;
-								kf++;
-								fp += U.framebytes;
-							}
+							const int64_t f0 = (int64_t)j * P, lo_ = r.a0 > f0 ? r.a0 : f0, hi_ = a1 < f0 + P ? a1 : f0 + P;
+							if(hi_ <= lo_ || !((r.fmask >> j) & 1u))
+								continue;
+							const uint8_t *src = buf + ((int64_t)r.fa + j) * Sp->framebytes + Sp->header + (lo_ - f0);
+							bulk_g2s(dst + (lo_ - r.a0), src, (uint32_t)(hi_ - lo_), &stg_full[slot]);
 						}
 					}
-					re0[i2] = pack_h2(x0r[0], x0r[1]);
-					im0[i2] = pack_h2(x0i[0], x0i[1]);
-					re1[i2] = pack_h2(x1r[0], x1r[1]);
-					im1[i2] = pack_h2(x1i[0], x1i[1]);
-				}
-				const int chunk = 2 * q4 + h;
-				const int col0 = (tl * 2) * 32 + n2, col1 = col0 + 32;
-				*(uint4 *)(sB + swz(col0, chunk)) = make_uint4(re0[0], re0[1], re0[2], re0[3]);
-				*(uint4 *)(sB + 16384 + swz(col0, chunk)) = make_uint4(im0[0], im0[1], im0[2], im0[3]);
-				*(uint4 *)(sB + swz(col1, chunk)) = make_uint4(re1[0], re1[1], re1[2], re1[3]);
-				*(uint4 *)(sB + 16384 + swz(col1, chunk)) = make_uint4(im1[0], im1[1], im1[2], im1[3]);
-			}
-		}
-		if(has_next && warp < 2 && lane == 0)
-		{
-			fc[slot ^ 1][warp] = tc_consts(Un, pn, Un.t0 + warp, a.T, order, a.fraclo);
-			if(warp == 0)
-				tus[slot ^ 1] = Un;
-		}
-		asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-		__syncthreads();
-		// the next unit's word loads: in flight during the MMAs, twiddle and output
-		if(has_next)
-			okms[tid] = tc_prefetch(a, tus[slot ^ 1], fc[slot ^ 1][warp >> 2], stage_addr, warp, lane, tid);
-
-		// ---- (c) MMA 1: D1[(k1, re|im)][(FFT, n2)], FP16 x FP16 -> FP32, M = N = 128
-		if(tid == 0)
-		{
-			asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-			const uint32_t idesc = (1u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
-			const uint32_t aA = su32(base), aB = su32(sB);
-#pragma unroll
-			for(int kk = 0; kk < 8; kk++)
-			{
-				const uint32_t off = (uint32_t)((kk >> 2) * 16384 + (kk & 3) * 32);
-				mma_f16(tmem, sdesc128(aA + off), sdesc128(aB + off), idesc, kk > 0 ? 1u : 0u);
-			}
-			commit_to(&mb1);
-		}
-		if(!__syncthreads_and(mbar_wait_f(&mb1, ku & 1)))
-		{
-			if(tid == 0)
-				atomicExch(err, 7);
-			break;
-		}
-		asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-
-		// ---- (d) twiddle w_N^(n2 k1) in FP32 (one rounding to FP16 per value);
-		// rows (FFT, k1) of the MMA 2 operands
-		{
-			const int q = warp & 3, hcol = warp >> 2;
-			const int r = 32 * q + lane, k1 = r >> 1, part = r & 1;
-			const float sg = part ? 1.0f : -1.0f;                  // re lane subtracts o wi
-#pragma unroll
-			for(int cc = 0; cc < 2; cc++)
-			{
-				const int fftl = 2 * hcol + cc;
-				float v[32];
-				tld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * fftl), v);
-				uint32_t pkv[16];
-#pragma unroll
-				for(int n2 = 0; n2 < 32; n2 += 2)
-				{
-					const float o0 = __shfl_xor_sync(0xffffffffu, v[n2], 1);
-					const float o1 = __shfl_xor_sync(0xffffffffu, v[n2 + 1], 1);
-					const float2 w0 = stw[n2 * kN1 + k1], w1 = stw[(n2 + 1) * kN1 + k1];
-					pkv[n2 >> 1] = pack_h2(fmaf(sg * o0, w0.y, v[n2] * w0.x), fmaf(sg * o1, w1.y, v[n2 + 1] * w1.x));
-				}
-				const int R3 = fftl * 64 + k1;
-				unsigned char *tile = sB + (R3 >> 7) * 16384;
-				const int rr3 = R3 & 127;
-#pragma unroll
-				for(int cq = 0; cq < 4; cq++)
-					*(uint4 *)(tile + swz(rr3, part * 4 + cq)) =
-					    make_uint4(pkv[4 * cq], pkv[4 * cq + 1], pkv[4 * cq + 2], pkv[4 * cq + 3]);
-			}
-		}
-		asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-		asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-		__syncthreads();
-
-		// ---- (e) MMA 2: D3[(FFT, k1)][(re|im, k2)] for the sideband's 16 k2, M = 128, N = 32
-		if(tid == 0)
-		{
-			asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-			const uint32_t idesc = (1u << 4) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
-			const uint32_t aB3 = su32(base + kOffB3 + (U.lsb ? kB3 : 0)), aA = su32(sB);
-#pragma unroll
-			for(int m = 0; m < 2; m++)
-#pragma unroll
-				for(int kk = 0; kk < 4; kk++)
-					mma_f16(tmem + 128u + 32u * m, sdesc128(aA + m * 16384 + kk * 32), sdesc128(aB3 + kk * 32), idesc,
-					        kk > 0 ? 1u : 0u);
-			commit_to(&mb2);
-		}
-		if(!__syncthreads_and(mbar_wait_f(&mb2, ku & 1)))
-		{
-			if(tid == 0)
-				atomicExch(err, 8);
-			break;
-		}
-		asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-
-		// ---- (f) channels c = k1 + 64 j: fractional-sample rotation, half2 or
-		// bf16x2 out, scaled by 2^-kTcSpecExp
-		{
-			const int q = warp & 3, m = warp >> 2;
-			const int r = 32 * q + lane;
-			const int fftl = 2 * m + (r >> 6), k1 = r & 63;
-			const int tl = fftl >> 1, b = fftl & 1;
-			float v[32];
-			tld32(tmem + ((uint32_t)(32 * q) << 16) + 128u + 32u * m, v);
-			const TcFftConst &c = fc[slot][tl];
-			const int rw = b ? U.row1 : U.row0;
-			if(c.t < a.T && rw >= 0)
-			{
-				const DevFreqPlan &P = a.plans[U.freq];
-				const int64_t spec_off = P.spec_off;
-				const int prow = P.nrow;
-				const uint32_t tcb = (uint32_t)P.tcb, tnblk = (uint32_t)P.tnblk;
-				float turns = (float)(U.lsb ? k1 - nchan : k1) * c.dfs + c.postf;
-				turns -= rintf(turns);
-				float qr, qi;
-				__sincosf(6.283185307179586f * turns, &qi, &qr);
-				constexpr float osc = 1.0f / (float)(1 << kTcSpecExp);
-				qr *= osc;
-				qi *= osc;
-				// channel k1 + 64 j -> (block, position): start, then step by 64 channels
-				const uint32_t PT = (uint32_t)prow * tcb;
-				uint32_t blk = (uint32_t)k1 / tcb, cl = (uint32_t)k1 - blk * tcb;
-				const uint32_t dblk = 64u / tcb, dcl = 64u - dblk * tcb;
-				uint32_t off = blk * PT + cl;
-				uint32_t *o = (uint32_t *)a.spec + spec_off + ((int64_t)c.t * tnblk * prow + rw) * tcb;
-				const bool h16 = a.h16 != 0;
-#pragma unroll
-				for(int j = 0; j < 16; j++)
-				{
-					const float xr = v[j], xi = v[16 + j];
-					const float yr = xr * qr - xi * qi, yi = xr * qi + xi * qr;
-					if(h16)
-						o[off] = pack_h2(yr, yi);
 					else
+						mbar_arrive(&stg_full[slot]);
+					stg_issued_s = k + 1;
+				}
+				__syncwarp();
+			}
+		}
+	}
+	else if(warp < 4)
+	{
+		// ================================================================ decode
+		const int dt = tid;
+		for(int k = 0; k < nk; k++)
+		{
+			const int slot = k % kNStg, s = k % kNS;
+			bool okw = mbar_wait(&stg_full[slot], (uint32_t)(k / kNStg) & 1u, &fail_s);
+			if(okw && k >= kNS)
+				okw = mbar_wait(&op_empty[s], (uint32_t)((k / kNS) - 1) & 1u, &fail_s);
+			if(!__all_sync(0xffffffffu, okw))      // the warp leaves together
+			{
+				fail_s = 11;
+				break;
+			}
+			if(dt == 0)
+				stg_used_s = k + 1;
+			const UnitRec &R = ring[k % kRing];
+			const int flags = R.flags;
+			unsigned char *A1 = ops + s * kOpBytes;
+			const uint32_t *words = (const uint32_t *)(stg + slot * LY::kStgBytes);
+			if((flags & kOk) && (flags & kManual))
+			{
+				// station buffer without 16-byte alignment: every decode warp copies the
+				// window's valid frames with byte loads (the same values, so the warps
+				// may overlap) before reading it
+				const DevStation *Sp = a.st + R.station;
+				const uint8_t *buf = a.sub[R.station].buf;
+				uint32_t *sw_ = (uint32_t *)(stg + slot * LY::kStgBytes);
+				for(int i = lane; i < R.nstage / 4; i += 32)
+				{
+					const int64_t c = R.a0 + 4 * (int64_t)i;
+					const int j = (int)(c / Sp->payload);
+					uint32_t v = 0u;
+					if(j < 32 && ((R.fmask >> j) & 1u))
 					{
-						const __nv_bfloat162 b = __floats2bfloat162_rn(yr, yi);
-						o[off] = *(const uint32_t *)&b;
+						const uint8_t *b = buf + ((int64_t)R.fa + j) * Sp->framebytes + Sp->header + (c - (int64_t)j * Sp->payload);
+						v = (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
 					}
-					const float nr = qr * c.Rr - qi * c.Ri;
-					qi = qr * c.Ri + qi * c.Rr;
-					qr = nr;
-					cl += dcl;
-					off += dblk * PT + dcl;
-					if(cl >= tcb)
+					sw_[i] = v;
+				}
+				__syncwarp();
+			}
+			const int so = R.so, fs = R.fs, swbits = R.swbits;
+			const uint32_t fmask = R.fmask;
+#pragma unroll 1
+			for(int it = 0; it < 2; it++)
+			{
+				const int item = dt + 128 * it;
+				const int n1 = item >> 3, g = item & 7;
+				const int n0 = 64 * n1 + 8 * g;             // first time of the item
+				// the item's 8 times (bits swbits + n0 BPT ..) as NW aligned 32-bit
+				// words, from the covering 16-byte quads of the staged window
+				constexpr int NW = BPT / 4 > 1 ? BPT / 4 : 1;      // words of 8 times
+				constexpr int NQ = (3 + NW + 1 + 3) / 4;            // quads that cover them from any start
+				const int bitpos = swbits + n0 * BPT;
+				const int wq = (bitpos >> 5) & ~3;
+				const int ws = (bitpos >> 5) - wq, bs = bitpos & 31;
+				uint32_t all[4 * NQ];
+#pragma unroll
+				for(int q = 0; q < NQ; q++)
+				{
+					const uint4 v4 = *(const uint4 *)(words + wq + 4 * q);
+					all[4 * q] = v4.x;
+					all[4 * q + 1] = v4.y;
+					all[4 * q + 2] = v4.z;
+					all[4 * q + 3] = v4.w;
+				}
+				uint32_t w[NW];
+				switch(ws)
+				{
+				case 0:
+#pragma unroll
+					for(int i = 0; i < NW; i++) w[i] = __funnelshift_r(all[i], all[i + 1], bs);
+					break;
+				case 1:
+#pragma unroll
+					for(int i = 0; i < NW; i++) w[i] = __funnelshift_r(all[i + 1], all[i + 2], bs);
+					break;
+				case 2:
+#pragma unroll
+					for(int i = 0; i < NW; i++) w[i] = __funnelshift_r(all[i + 2], all[i + 3], bs);
+					break;
+				default:
+#pragma unroll
+					for(int i = 0; i < NW; i++) w[i] = __funnelshift_r(all[i + 3], all[i + 4], bs);
+					break;
+				}
+				// per-time validity (frames of the window that were not copied read as zero)
+				uint32_t vm = (flags & kOk) ? 0xFFu : 0u;
+				if((flags & kOk) && !(flags & kAllValid))
+				{
+					vm = 0u;
+					const int x0 = so + n0;
+					int kf = x0 / fs;
+					int nb = (kf + 1) * fs - so;                // first time of the next frame
+#pragma unroll
+					for(int j = 0; j < 8; j++)
 					{
-						cl -= tcb;
-						off += PT - tcb;
+						if(n0 + j >= nb)
+						{
+							kf++;
+							nb += fs;
+						}
+						vm |= (kf < 32 ? ((fmask >> kf) & 1u) : 0u) << j;
 					}
+				}
+#pragma unroll
+				for(int sb = 0; sb < 2; sb++)
+				{
+					const int nsh = 4 * R.nib[sb];
+					const uint32_t vms = (flags & (sb == 0 ? kHas0 : kHas1)) ? vm : 0u;
+					float dv0[8], dv1[8];
+#pragma unroll
+					for(int j = 0; j < 8; j += 2)
+					{
+						// nibble of time j: bits j BPT + nsh of the item's words (for 64
+						// bits per time the subband's word of the time pair is picked by nsh)
+						uint32_t wa, wb;
+						int sa, sb2;
+						if constexpr(BPT <= 32)
+						{
+							wa = w[(j * BPT) >> 5];
+							wb = w[((j + 1) * BPT) >> 5];
+							sa = ((j * BPT) & 31) + nsh;
+							sb2 = (((j + 1) * BPT) & 31) + nsh;
+						}
+						else
+						{
+							const bool hi = nsh >= 32;
+							wa = hi ? w[2 * j + 1] : w[2 * j];
+							wb = hi ? w[2 * j + 3] : w[2 * j + 2];
+							sa = sb2 = nsh & 31;
+						}
+						const uint32_t idx = ((wa >> sa) & 15u) | (((wb >> sb2) & 15u) << 4);
+						const float4 l = lut[idx];
+						const bool v0 = (vms >> j) & 1u, v1 = (vms >> (j + 1)) & 1u;
+						dv0[j] = v0 ? l.x : 0.0f;
+						dv0[j + 1] = v1 ? l.y : 0.0f;
+						dv1[j] = v0 ? l.z : 0.0f;
+						dv1[j + 1] = v1 ? l.w : 0.0f;
+					}
+					// fringe rotator exp(-2 pi i (P0 + alpha n)) at n = n0 .. n0 + 7
+					const float Sr = R.Sr[sb], Si = R.Si[sb];
+					float rr = 1.0f, ri = 0.0f;
+					if(order == 1)
+					{
+						float ph = R.P0[sb] + R.alpha[sb] * (float)n0;
+						ph -= rintf(ph);
+						__sincosf(-6.283185307179586f * ph, &ri, &rr);
+					}
+					uint32_t re0[4], im0[4], re1[4], im1[4];
+#pragma unroll
+					for(int j = 0; j < 8; j += 2)
+					{
+						const float rr1 = rr * Sr - ri * Si;
+						const float ri1 = rr * Si + ri * Sr;
+						re0[j >> 1] = pack_h2(dv0[j] * rr, dv0[j + 1] * rr1);
+						im0[j >> 1] = pack_h2(dv0[j] * ri, dv0[j + 1] * ri1);
+						re1[j >> 1] = pack_h2(dv1[j] * rr, dv1[j + 1] * rr1);
+						im1[j >> 1] = pack_h2(dv1[j] * ri, dv1[j + 1] * ri1);
+						rr = rr1 * Sr - ri1 * Si;
+						ri = rr1 * Si + ri1 * Sr;
+					}
+					// A1 tile sb: rows m = p 64 + n2 (the 8 times 8g..8g+7 are one 16-byte
+					// run), K = part 32 + n1
+					unsigned char *T1 = A1 + sb * 16384;
+					const uint32_t ore = mn_off(8 * g, n1), oim = mn_off(8 * g, 32 + n1);
+					*(uint4 *)(T1 + ore) = make_uint4(re0[0], re0[1], re0[2], re0[3]);
+					*(uint4 *)(T1 + oim) = make_uint4(im0[0], im0[1], im0[2], im0[3]);
+					*(uint4 *)(T1 + ore + 1024) = make_uint4(re1[0], re1[1], re1[2], re1[3]);
+					*(uint4 *)(T1 + oim + 1024) = make_uint4(im1[0], im1[1], im1[2], im1[3]);
+				}
+			}
+			asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+			__syncwarp();
+			if(lane == 0)
+			{
+				mbar_arrive(&op_full[s]);
+				mbar_arrive(&stg_empty[slot]);
+			}
+		}
+	}
+	else if(warp < 8)
+	{
+		// ================================================================ twiddle
+		const int L = tid - 128;                // tensor-memory lane (p, n2)
+		const int p = L >> 6, n2 = L & 63;
+		const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+		const float2 *tw = twt + n2;             // w_2048^(n2 k1) at tw[k1 kN2]
+		for(int k = 0; k < nk; k++)
+		{
+			const int b = k & 1, s = k % kNS;
+			if(!__all_sync(0xffffffffu, mbar_wait(&d1_full[b], (uint32_t)(k >> 1) & 1u, &fail_s)))
+			{
+				fail_s = 12;
+				break;
+			}
+			asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+			unsigned char *A2 = ops + s * kOpBytes;
+#pragma unroll 1
+			for(int sb = 0; sb < 2; sb++)
+			{
+				float v[64];
+				const uint32_t tcol = tmem + lane_base + (uint32_t)(256 * b + 64 * sb);
+				tld32(tcol, v);
+				tld32(tcol + 32, v + 32);
+				tld_wait();
+				// Z[k1][n2] = Y[k1][n2] w^(n2 k1); A2 row m = ch 32 + k1 with ch = 2 sb + p,
+				// K = part 64 + n2
+				const int m0 = (2 * sb + p) * 32;
+				uint32_t zr[16], zi[16];
+#pragma unroll
+				for(int k1 = 0; k1 < kN1; k1 += 2)
+				{
+					const float y0r = v[2 * k1], y0i = v[2 * k1 + 1], y1r = v[2 * k1 + 2], y1i = v[2 * k1 + 3];
+					const float2 w0 = tw[k1 * kN2], w1 = tw[(k1 + 1) * kN2];
+					zr[k1 >> 1] = pack_h2(y0r * w0.x - y0i * w0.y, y1r * w1.x - y1i * w1.y);
+					zi[k1 >> 1] = pack_h2(y0r * w0.y + y0i * w0.x, y1r * w1.y + y1i * w1.x);
+				}
+#pragma unroll
+				for(int c = 0; c < 4; c++)
+				{
+					*(uint4 *)(A2 + mn_off(m0 + 8 * c, n2)) = make_uint4(zr[4 * c], zr[4 * c + 1], zr[4 * c + 2], zr[4 * c + 3]);
+					*(uint4 *)(A2 + mn_off(m0 + 8 * c, 64 + n2)) =
+					    make_uint4(zi[4 * c], zi[4 * c + 1], zi[4 * c + 2], zi[4 * c + 3]);
+				}
+			}
+			asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+			asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+			__syncwarp();
+			if(lane == 0)
+			{
+				mbar_arrive(&d1_empty[b]);
+				mbar_arrive(&a2_full[b]);
+			}
+		}
+	}
+	else if(warp < 12)
+	{
+		// ================================================================ output
+		const int ch = warp - 8, k1 = lane;
+		const int sb = ch >> 1, p = ch & 1;
+		const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+		constexpr float osc = 1.0f / (float)(1 << kTcSpecExp);
+		const bool h16 = a.h16 != 0;
+		for(int k = 0; k < nk; k++)
+		{
+			const int b = k & 1;
+			if(!__all_sync(0xffffffffu, mbar_wait(&d2_full[b], (uint32_t)(k >> 1) & 1u, &fail_s)))
+			{
+				fail_s = 13;
+				break;
+			}
+			asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+			float v[64];
+			const uint32_t tcol = tmem + lane_base + (uint32_t)(256 * b + 128);
+			tld32(tcol, v);
+			tld32(tcol + 32, v + 32);
+			tld_wait();
+			asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+			__syncwarp();
+			if(lane == 0)
+				mbar_arrive(&d2_empty[b]);
+			const UnitRec &R = ring[k % kRing];
+			const int row = R.row[sb][p];
+			if(row < 0)
+				continue;
+			// channel c = k1 + 32 j: exp(2 pi i (ce dfs + postf)), ce = c (upper
+			// sideband) or c - nchan (lower), stepped by exp(2 pi i 32 dfs)
+			const float dfs = R.dfs;
+			const bool lsb = (R.flags & (sb == 0 ? kLsb0 : kLsb1)) != 0;
+			float turns = (float)(lsb ? k1 - nchan : k1) * dfs + R.postf[sb];
+			turns -= rintf(turns);
+			float qr, qi;
+			__sincosf(6.283185307179586f * turns, &qi, &qr);
+			qr *= osc;
+			qi *= osc;
+			float st32 = 32.0f * dfs;
+			st32 -= rintf(st32);
+			float sr, si;
+			__sincosf(6.283185307179586f * st32, &si, &sr);
+			const uint32_t tcb = (uint32_t)R.tcb[sb];
+			uint32_t *o = (uint32_t *)a.spec + R.spec[sb] + (int64_t)row * tcb;
+			const uint32_t PT = (uint32_t)R.nrow[sb] * tcb;
+			uint32_t blk = (uint32_t)k1 / tcb, cl = (uint32_t)k1 - blk * tcb;
+			const uint32_t dblk = 32u / tcb, dcl = 32u - dblk * tcb;
+			uint32_t off = blk * PT + cl;
+#pragma unroll
+			for(int j = 0; j < 32; j++)
+			{
+				const float xr = v[2 * j], xi = v[2 * j + 1];
+				o[off] = pack_spec(h16, xr * qr - xi * qi, xr * qi + xi * qr);
+				const float nr = qr * sr - qi * si;
+				qi = qr * si + qi * sr;
+				qr = nr;
+				cl += dcl;
+				off += dblk * PT + dcl;
+				if(cl >= tcb)
+				{
+					cl -= tcb;
+					off += PT - tcb;
 				}
 			}
 		}
-		asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-		__syncthreads();
 	}
-	// copies still in flight (error path) land before the CTA exits
-	asm volatile("cp.async.wait_all;\n" ::: "memory");
-	// every MMA issued by thread 0 has completed once mbd arrives
+	else if(warp == 12 && lane == 0)
+	{
+		// ================================================================ MMA issuer
+		// instruction descriptor: D F32 (bit 4), A and B F16, A MN-major (bit 15),
+		// B K-major, N = 64 (bits 17-22: N >> 3), M = 128 (bits 24-28: M >> 4)
+		const uint32_t idesc = (1u << 4) | (1u << 15) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+		const uint32_t aB1 = su32(base + kOffB1), aB2 = su32(base + kOffB2);
+		auto mma2 = [&](int j) -> bool {
+			const int b = j & 1, s = j % kNS;
+			if(!mbar_wait(&a2_full[b], (uint32_t)(j >> 1) & 1u, &fail_s))
+				return false;
+			if(j >= 2 && !mbar_wait(&d2_empty[b], (uint32_t)((j >> 1) - 1) & 1u, &fail_s))
+				return false;
+			asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+			const uint32_t bside = aB2 + ((ring[j % kRing].flags & kLsb0) ? kB2Bytes : 0);
+			const uint32_t aA = su32(ops + s * kOpBytes);
+			const uint32_t dcol = tmem + (uint32_t)(256 * b + 128);
+#pragma unroll
+			for(int ks = 0; ks < 8; ks++)
+				mma_f16(dcol, desc_mn128(aA + ks * 4096), desc_k128(bside + (ks >> 2) * 8192 + (ks & 3) * 32), idesc,
+				        ks > 0 ? 1u : 0u);
+			commit_to(&d2_full[b]);
+			commit_to(&op_empty[s]);
+			return true;
+		};
+		bool ok = true;
+		int k = 0;
+		for(; k < nk && ok; k++)
+		{
+			const int b = k & 1, s = k % kNS;
+			if(!mbar_wait(&op_full[s], (uint32_t)(k / kNS) & 1u, &fail_s) ||
+			   (k >= 2 && !mbar_wait(&d1_empty[b], (uint32_t)((k >> 1) - 1) & 1u, &fail_s)))
+			{
+				fail_s = 14;
+				ok = false;
+				break;
+			}
+			asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+			const uint32_t aA = su32(ops + s * kOpBytes);
+#pragma unroll
+			for(int sb = 0; sb < 2; sb++)
+			{
+				const uint32_t dcol = tmem + (uint32_t)(256 * b + 64 * sb);
+#pragma unroll
+				for(int ks = 0; ks < 4; ks++)
+					mma_f16(dcol, desc_mn128(aA + sb * 16384 + ks * 4096), desc_k128(aB1 + ks * 32), idesc,
+					        ks > 0 ? 1u : 0u);
+			}
+			commit_to(&d1_full[b]);
+			if(k >= 1 && !mma2(k - 1))
+			{
+				fail_s = 15;
+				ok = false;
+			}
+		}
+		if(ok && k >= 1 && !mma2(k - 1))
+			fail_s = 15;
+		// every MMA issued by this thread has completed once this arrives
+		commit_to(&mma_done);
+		if(!mbar_wait(&mma_done, 0, &fail_s))
+			fail_s = 16;
+	}
+
+	asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+	__syncthreads();
 	if(tid == 0)
 	{
-		commit_to(&mbd);
-		if(!mbar_wait_f(&mbd, 0))
-			atomicExch(err, 9);
+		// staged windows that no decode consumed (error path): wait (bounded) for
+		// their copies before the shared memory goes away
+		for(int k = stg_used_s; k < stg_issued_s; k++)
+			mbar_wait(&stg_full[k % kNStg], (uint32_t)(k / kNStg) & 1u, &fail_s);
+		if(fail_s && err)
+			atomicExch(err, fail_s);
 	}
 	__syncthreads();
 	asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-	if(warp == 0)
-		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(256u));
+	if(warp == 12)
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"((uint32_t)kTmemCols));
 }
 
 // ---------------------------------------------------------------- host side
-// Constant tables in the kernel's shared-memory byte layout (values in double,
-// rounded once): DFT-64 rows (k1, re|im) over K = (re|im, n1); DFT-32
-// columns (re|im, k2) over K = (re|im, n2) for k2 in [0, 16) (upper sideband)
-// and [16, 32) (lower); twiddles w_2048^(n2 k1) as float2 [n2][k1].
+// Constant tables in the kernel's shared-memory byte layout (values in
+// double, rounded once to FP16), K-major with the 128-byte swizzle:
+//   DFT-32: rows j = 2 k1 + part (out), K = part_in 32 + n1;
+//   DFT-64 of the upper (k2 in [0, 32)) and lower (k2 in [32, 64)) sideband:
+//          rows j = 2 k2' + part, K = part_in 64 + n2, two K halves of 64.
+// A complex product (x_r + i x_i)(cos t - i sin t) is
+//   re: x_r cos t + x_i sin t,  im: -x_r sin t + x_i cos t.
 size_t fstage_tc_tables_bytes() { return kTablesBytes; }
 
 void make_fstage_tc_tables(void *out)
@@ -650,36 +880,29 @@ void make_fstage_tc_tables(void *out)
 		{
 			const double th = 2.0 * M_PI * (double)(k1 * n1 % kN1) / kN1;
 			const double c = cos(th), sn = sin(th);
-			put(o, 2 * k1, n1, c);                  // re out: [cos | sin]
-			put(o + 16384, 2 * k1, n1, sn);
-			put(o, 2 * k1 + 1, n1, -sn);            // im out: [-sin | cos]
-			put(o + 16384, 2 * k1 + 1, n1, c);
+			put(o + kOffB1, 2 * k1, n1, c);
+			put(o + kOffB1, 2 * k1, 32 + n1, sn);
+			put(o + kOffB1, 2 * k1 + 1, n1, -sn);
+			put(o + kOffB1, 2 * k1 + 1, 32 + n1, c);
 		}
 	for(int side = 0; side < 2; side++)
 	{
-		unsigned char *t = o + kOffB3 + side * kB3;
-		for(int j = 0; j < 16; j++)
+		unsigned char *t = o + kOffB2 + side * kB2Bytes;
+		for(int j = 0; j < 32; j++)
 		{
-			const int k2 = 16 * side + j;
+			const int k2 = j + 32 * side;
 			for(int n2 = 0; n2 < kN2; n2++)
 			{
 				const double ph = 2.0 * M_PI * (double)(n2 * k2 % kN2) / kN2;
 				const double c = cos(ph), sn = sin(ph);
-				put(t, j, n2, c);                   // re out: [cos | sin]
-				put(t, j, 32 + n2, sn);
-				put(t, 16 + j, n2, -sn);            // im out: [-sin | cos]
-				put(t, 16 + j, 32 + n2, c);
+				// K = part_in 64 + n2: the real part's K half, then the imaginary part's
+				put(t, 2 * j, n2, c);
+				put(t + 8192, 2 * j, n2, sn);
+				put(t, 2 * j + 1, n2, -sn);
+				put(t + 8192, 2 * j + 1, n2, c);
 			}
 		}
 	}
-	// twiddles w_2048^(n2 k1) as float2 [n2][k1]
-	float2 *tw = (float2 *)(o + kOffTw);
-	for(int n2 = 0; n2 < kN2; n2++)
-		for(int k1 = 0; k1 < kN1; k1++)
-		{
-			const double ang = -2.0 * M_PI * (double)(n2 * k1) / kN;
-			tw[n2 * kN1 + k1] = make_float2((float)cos(ang), (float)sin(ang));
-		}
 }
 
 bool fstage_tc_eligible(int N, int order, bool any_lsb)
@@ -689,16 +912,26 @@ bool fstage_tc_eligible(int N, int order, bool any_lsb)
 
 void launch_fstage_tc(const FKind &k, FsArgs a, int nsm, cudaStream_t stream)
 {
-	if(k.count <= 0 || a.T <= 0 || !k.tctab)
+	if(k.count <= 0 || a.T <= 0 || !k.tctab || !k.tcpairs || k.tcnpairs <= 0)
 		return;
 	a.first = k.first;
-	const int nunits = k.count * ((a.T + 1) / 2);
-	cudaFuncSetAttribute(k_fstage_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTc);
-	cudaFuncSetAttribute(k_fstage_tc, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-	int grid = 2 * nsm;
+	const int nunits = k.tcnpairs * a.T;
+	int grid = nsm;
 	if(grid > nunits)
 		grid = nunits;
-	k_fstage_tc<<<grid, kThreadsF, kSmemTc, stream>>>(a, (const uint4 *)k.tctab, k.count, nunits, a.err);
+	auto go = [&](auto kern, size_t smem) {
+		cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		kern<<<grid, kThreadsTc, smem, stream>>>(a, (const uint4 *)k.tctab, k.tcpairs, k.tcnpairs, nunits, a.err);
+	};
+	switch(k.tcbpt)
+	{
+	case 4: go(k_fstage_tc<4>, TcLayout<4>::kSmem); break;
+	case 8: go(k_fstage_tc<8>, TcLayout<8>::kSmem); break;
+	case 16: go(k_fstage_tc<16>, TcLayout<16>::kSmem); break;
+	case 32: go(k_fstage_tc<32>, TcLayout<32>::kSmem); break;
+	case 64: go(k_fstage_tc<64>, TcLayout<64>::kSmem); break;
+	default: break;
+	}
 }
 
 }  // namespace fxb

@@ -81,12 +81,15 @@ struct FKind {
 	int32_t N, nb;           // FFT length, bands per item
 	int32_t kb, fpc;         // radix-8 butterflies per thread and pass, FFTs side by side per CTA
 	int32_t threads, tq;     // CTA size, FFT iterations per CTA
-	int32_t pp, out;         // two exchange buffers (else one), output form (0 FP32, 1 FP16 FFT -> bf16x2)
+	int32_t pp, out;         // two exchange buffers (else one), output form (0 FP32 spectra, 1 tensor-core spectra)
 	int32_t items_fast;      // grid order: work items fastest (else time chunks); scheduling only
 	int32_t twn, tcfft;      // twiddle entries of length N; 1: tensor-core FFT kernel (fxb_fstage_tc.cu)
 	size_t smem;
 	const void *tw;          // twiddle table of length N (make_fstage_twiddles layout)
 	const void *tctab;       // constant tables of the tensor-core FFT kernel
+	const int32_t *tcpairs;  // tensor-core FFT: [tcnpairs][2] FGroup indices of each work unit's two subbands
+	int32_t tcnpairs;
+	int32_t tcbpt;           // tensor-core FFT: bits per time of the stations' VDIF words
 };
 
 // Spectra of the tensor-core forms hold X 2^-kTcSpecExp (FP16 or BF16), so
@@ -116,15 +119,18 @@ struct FsArgs {
 bool fstage_plan(int N, int nb, int out, FKind *k);
 void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream);
 // F stage of the tensor-core form with the FFT on the tensor cores (N = 2048;
-// csrc/fxb_fstage_tc.cu)
+// csrc/fxb_fstage_tc.cu).  Eligible: 2048-point FFTs, fringe rotation order
+// 1 (or 0 with upper sidebands only), 2-bit stations of 2..32 bands (all
+// stations of the kind alike), each subband's two bands in one 4-bit field,
+// 16-byte aligned frames of at least 128 samples; a work unit is two
+// subbands of one station with equal sideband at one FFT time.
 size_t fstage_tc_tables_bytes();
 void make_fstage_tc_tables(void *out);
 bool fstage_tc_eligible(int N, int order, bool any_lsb);
 void launch_fstage_tc(const FKind &k, FsArgs a, int nsm, cudaStream_t stream);
 
-// twiddles of FFT length N: float2 (out 0) or half2 pairs (wr, wr), (wi, wi)
-// (out 1), FKind::twn entries
-void make_fstage_twiddles(int N, float2 *out32, void *out16);
+// twiddles of FFT length N, FKind::twn entries
+void make_fstage_twiddles(int N, float2 *out32);
 
 // FP32 XMAC v2 over a set of frequencies with equal (rows, channels):
 // plan_idx[0..nf) index dplans.
