@@ -627,6 +627,30 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				g.nb = b1 >= 0 ? 2 : 1;
 				g.lsb = job.freqs[f].lower_sideband;
 				g.lofreq = job.freqs[f].freq_mhz;
+				if(js.has_corr)
+				{
+					// the phase offset rotates the non-R band of the frequency's
+					// first two bands, or the first when neither is R
+					// (mode.cpp:1336-1347)
+					int q0 = -1, q1 = -1;
+					for(int c = 0; c < js.nband && q1 < 0; c++)
+						if(js.band_freq[c] == f)
+						{
+							if(q0 < 0)
+								q0 = c;
+							else
+								q1 = c;
+						}
+					const int lcp = q1 < 0 ? -1 : (js.band_pol[q0] == 'R' ? q1 : q0);
+					for(int j = 0; j < 2; j++)
+					{
+						const int bj = g.band[j];
+						g.clk[j] = js.clk[bj] - (js.band_pol[bj] == 'R' ? 0.5 : -0.5) * js.dclk[bj];
+						g.phase[j] = bj == lcp ? (float)(js.phase[bj] / 720.0) : 0.0f;
+					}
+					g.looff = js.looff[b];
+					g.corr = 1;
+				}
 				bykind[{N, g.nb}].push_back(g);
 			}
 		}

@@ -195,12 +195,14 @@ constexpr int kMaxTQ = 4;         // FFT iterations per CTA at most
 struct FftConst {
 	float P0, alpha, beta, gamma, eps;   // fringe phase (turns): start and per-sample terms
 	float stc, sts;                      // order 1: rotator step over N/8 samples, exp(-2 pi i alpha N/8)
-	float dfs, postf;                    // fractional-sample turns per channel, order-0 post-F turns
+	float dhi[2], dlo[2];                // fractional-sample turns per channel of each band (split_turns)
+	float postf;                         // order-0 post-F turns
 	uint32_t fa, so;                     // first frame of the window, window start within it
 	uint32_t fmask;                      // validity of the window's frames (bit k: frame fa + k)
 	int32_t stuck;                       // samples [stuck, N) read as zero
 	int32_t flags;                       // 1: valid FFT, 2: fmask covers the window,
-	                                     // 4: a valid frame of the window blanks one of the item's bands
+	                                     // 4: a valid frame of the window blanks one of the item's bands,
+	                                     // 8: the two bands take the same output rotation
 };
 
 // One middle radix-8 pass (stride s = 2^LOGS, m = N / (8 s)) over the
@@ -327,6 +329,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 	const uint32_t tcb_magic = tcb ? 0xFFFFFFFFu / tcb + 1u : 0u;    // c / tcb = umulhi(c, magic) for c < 2^16
 	const bool lsb = g.lsb != 0;
 	const double lo = g.lofreq;
+	const float ph0 = g.phase[0], ph1 = g.phase[1];     // phase-offset rotation of each band (turns)
 	const int row0 = g.row[0], row1 = g.row[1];
 	const uint32_t boff0 = (uint32_t)(g.band[0] * nbits), boff1 = (uint32_t)(g.band[1] * nbits);
 	const bool oneword = bpt <= 32;       // all bands of a sample time in one 32-bit word
@@ -355,7 +358,8 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 		{
 			const int t = t0 + f;
 			FftConst c;
-			c.P0 = c.alpha = c.beta = c.gamma = c.eps = c.dfs = c.postf = 0.0f;
+			c.P0 = c.alpha = c.beta = c.gamma = c.eps = c.postf = 0.0f;
+			c.dhi[0] = c.dhi[1] = c.dlo[0] = c.dlo[1] = 0.0f;
 			c.stc = 1.0f;
 			c.sts = 0.0f;
 			c.fa = c.so = c.fmask = 0u;
@@ -374,10 +378,17 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 					const double invN = 1.0 / N;
 					const int idl = pq->integerdelay;
 					const double fraclo = a.fraclo ? (lo - (int)lo) * (double)idl : 0.0;
+					// LO offset: seconds since the job start of the FFT's first
+					// sample (mode.cpp:686-694; the scan starts with the job) and
+					// the offset's turns per sample
+					const double walls = (double)a.sub[g.station].subsec + a.sub[g.station].subns / 1.0e9 +
+					                     (double)t * N * Sp->sampletime / 1.0e6;
+					const double low = g.corr ? looff_wall_turns(g.looff, walls) : 0.0;
+					const double los = -g.looff * Sp->sampletime / 1.0e6;
 					if(order == 1)
 					{
-						c.P0 = frac_centered(lo * pq->b + fraclo);
-						c.alpha = (float)(lo * pq->a * invN);
+						c.P0 = frac_centered(lo * pq->b + fraclo + low);
+						c.alpha = (float)(lo * pq->a * invN + los);
 						// each thread's samples are N/8 apart: one step phasor per FFT
 						const double st = (double)c.alpha * (double)(N / 8);
 						double ss, sc;
@@ -389,18 +400,21 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 					{
 						const double pa = pq->a, pb = pq->b;
 						const double X1 = (double)asl * invN;
-						c.P0 = frac_centered(lo * pq->c + fraclo);
-						c.alpha = (float)(lo * (pb + pa * X1) * invN);
+						c.P0 = frac_centered(lo * pq->c + fraclo + low);
+						c.alpha = (float)(lo * (pb + pa * X1) * invN + los);
 						c.beta = (float)(lo * 2.0 * pa * X1 * invN);
-						c.gamma = (float)(lo * pb * asl * invN);
+						c.gamma = (float)(lo * pb * asl * invN + los * asl);
 						c.eps = (float)(lo * pa * X1 * X1);
 					}
-					c.dfs = (float)(bw * (1.0 / nchan) * (double)pq->fse);
+					// per band: fse - clock offset (mode.cpp:1053-1059, 1099-1106)
+					split_turns(bw * (1.0 / nchan) * ((double)pq->fse - g.clk[0]), c.dhi[0], c.dlo[0]);
+					split_turns(bw * (1.0 / nchan) * ((double)pq->fse - g.clk[1]), c.dhi[1], c.dlo[1]);
 					if(order == 0)
 					{
 						double pr = (pq->averagedelay - idl) * lo;
 						if(a.fraclo)
 							pr += idl * (lo - (int)lo);
+						pr -= walls * g.looff;
 						c.postf = -(float)(pr - (int)pr);
 					}
 				}
@@ -412,6 +426,8 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 			c.fmask = __ballot_sync(0xffffffffu, v);
 			if(nwf <= 32)
 				c.flags |= 2;
+			if(c.dhi[0] == c.dhi[1] && c.dlo[0] == c.dlo[1] && g.phase[0] == g.phase[1])
+				c.flags |= 8;
 			if(a.bandok)
 			{
 				// EDV4-blanked bands (INTERLACEDVDIF): the slow decode path below
@@ -443,8 +459,9 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 		const int stuck = fc.stuck;
 		const float P0 = fc.P0, alpha = fc.alpha, beta = fc.beta, gamma = fc.gamma, eps = fc.eps;
 		const float stc = fc.stc, sts = fc.sts;
-		const float dfs = fc.dfs, postf = fc.postf;
+		const float dhi0 = fc.dhi[0], dlo0 = fc.dlo[0], dhi1 = fc.dhi[1], dlo1 = fc.dlo[1], postf = fc.postf;
 		const bool narrow = (fc.flags & 2) != 0;
+		const bool same = (fc.flags & 8) != 0;
 		const bool blank = (fc.flags & 4) != 0;
 		// ---- 1-3. decode, fringe-rotate and run the first radix-8 pass (s = 1:
 		// butterfly b, twiddle w_N^(r b)), one butterfly at a time
@@ -632,10 +649,24 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 						ce = c - nchan;
 						cj = -1.0f;
 					}
-					float turns = (float)ce * dfs + postf;
+					// fractional-sample (and order-0 fringe) rotation of band 0 and,
+					// where its clock or phase offset differs, of band 1
+					const float fce = (float)ce;
+					float t0h = fce * dhi0;             // exact (split_turns)
+					t0h -= rintf(t0h);
+					float turns = t0h + fmaf(fce, dlo0, postf + ph0);
 					turns -= rintf(turns);
 					float sn, cs;
 					__sincosf(6.283185307179586f * turns, &sn, &cs);
+					float sn1 = sn, cs1 = cs;
+					if(NV == 2 && !same)
+					{
+						float t1h = fce * dhi1;
+						t1h -= rintf(t1h);
+						float turns1 = t1h + fmaf(fce, dlo1, postf + ph1);
+						turns1 -= rintf(turns1);
+						__sincosf(6.283185307179586f * turns1, &sn1, &cs1);
+					}
 					if constexpr(TCO)
 					{
 						uint32_t *o;
@@ -651,11 +682,11 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 							o = (uint32_t *)a.spec + obase + c;
 							rstride = nchan;
 						}
-						const float ocs = cs * osc, osn = sn * osc;
 #pragma unroll
 						for(int j = 0; j < NV; j++)
 						{
 							const int rw = j == 0 ? row0 : row1;
+							const float ocs = (j == 0 ? cs : cs1) * osc, osn = (j == 0 ? sn : sn1) * osc;
 							if(rw >= 0)
 							{
 								const float xr = y[j][r].x, xi = cj * y[j][r].y;
@@ -670,10 +701,11 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 						for(int j = 0; j < NV; j++)
 						{
 							const int rw = j == 0 ? row0 : row1;
+							const float ocs = j == 0 ? cs : cs1, osn = j == 0 ? sn : sn1;
 							if(rw >= 0)
 							{
 								const float xr = y[j][r].x, xi = cj * y[j][r].y;
-								o[(int64_t)rw * nchan] = make_float2(xr * cs - xi * sn, xr * sn + xi * cs);
+								o[(int64_t)rw * nchan] = make_float2(xr * ocs - xi * osn, xr * osn + xi * ocs);
 							}
 						}
 					}

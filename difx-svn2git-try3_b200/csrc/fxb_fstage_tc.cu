@@ -229,8 +229,9 @@ struct UnitRec {
 	int64_t a0;                   // first staged byte of the payloads from frame fa on
 	int32_t nstage, station;      // staged bytes; station
 	int32_t t;                    // FFT time
-	float dfs;                    // fractional-sample turns per channel
-	float postf[2];               // order-0 post-F turns per subband
+	float dhi[2][2], dlo[2][2];   // fractional-sample turns per channel of [subband][polarisation] (split_turns)
+	float st32[2][2];             // the same over 32 channels, reduced to [-1/2, 1/2)
+	float post[2][2];             // order-0 post-F turns plus the phase-offset rotation, per [subband][polarisation]
 	int32_t row[2][2];            // spectra row of [subband][polarisation] (-1: not written)
 	int64_t spec[2];              // first spectra value of the subband's [t][block][row][tcb] block
 	int32_t tnblk[2], nrow[2], tcb[2];
@@ -289,11 +290,17 @@ __device__ __forceinline__ UnitRec build_unit(const FsArgs &a, const int32_t *pa
 			continue;
 		const double lo = g.lofreq;
 		const int idl = p.integerdelay;
+		// LO offset (mode.cpp:873-882, 932-951, 1061-1070): seconds since the
+		// job start of the FFT's first sample (the scan starts with the job)
+		const double walls = (double)a.sub[s].subsec + a.sub[s].subns / 1.0e9 +
+		                     (double)r.t * kN * Sp->sampletime / 1.0e6;
+		double postf = 0.0;
 		if(a.order == 1)
 		{
 			const double fl = a.fraclo ? (lo - (int)lo) * (double)idl : 0.0;
-			r.P0[sb] = fracc(lo * p.b + fl);
-			r.alpha[sb] = (float)(lo * p.a * (1.0 / kN));
+			const double low = g.corr ? looff_wall_turns(g.looff, walls) : 0.0;
+			r.P0[sb] = fracc(lo * p.b + fl + low);
+			r.alpha[sb] = (float)(lo * p.a * (1.0 / kN) - g.looff * Sp->sampletime / 1.0e6);
 			float sn, cs;
 			sincospif(-2.0f * r.alpha[sb], &sn, &cs);
 			r.Sr[sb] = cs;
@@ -304,7 +311,17 @@ __device__ __forceinline__ UnitRec build_unit(const FsArgs &a, const int32_t *pa
 			double pr0 = (p.averagedelay - idl) * lo;
 			if(a.fraclo)
 				pr0 += idl * (lo - (int)lo);
-			r.postf[sb] = -(float)(pr0 - (int)pr0);
+			pr0 -= walls * g.looff;
+			postf = -(double)(float)(pr0 - (int)pr0);
+		}
+		// per polarisation: fse - clock offset (mode.cpp:1053-1059, 1099-1106)
+		// and the phase-offset rotation (mode.cpp:1336-1347)
+		for(int q = 0; q < 2; q++)
+		{
+			const double D = bw * (1.0 / nchan) * ((double)p.fse - g.clk[q]);
+			split_turns(D, r.dhi[sb][q], r.dlo[sb][q]);
+			r.st32[sb][q] = fracc(32.0 * D);
+			r.post[sb][q] = (float)(postf + (double)g.phase[q]);
 		}
 	}
 	if(p.status == kFftOk)
@@ -317,7 +334,6 @@ __device__ __forceinline__ UnitRec build_unit(const FsArgs &a, const int32_t *pa
 		const int nwf = (r.so + kN - 1) / r.fs + 1;
 		if(nwf < 32 ? (r.fmask == (1u << nwf) - 1u) : r.fmask == 0xFFFFFFFFu)
 			r.flags |= kAllValid;
-		r.dfs = (float)(bw * (1.0 / nchan) * (double)p.fse);
 		// the window's times [so, so + N) of the payloads from frame fa on, 16-byte aligned
 		const int64_t b0 = (int64_t)r.so * BPT, b1 = (int64_t)(r.so + kN) * BPT;
 		r.a0 = (b0 >> 3) & ~(int64_t)15;
@@ -737,20 +753,21 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 			const int row = R.row[sb][p];
 			if(row < 0)
 				continue;
-			// channel c = k1 + 32 j: exp(2 pi i (ce dfs + postf)), ce = c (upper
-			// sideband) or c - nchan (lower), stepped by exp(2 pi i 32 dfs)
-			const float dfs = R.dfs;
+			// channel c = k1 + 32 j: exp(2 pi i (ce D + post)), ce = c (upper
+			// sideband) or c - nchan (lower), D = hi + lo (ce hi exact), stepped
+			// by exp(2 pi i 32 D)
 			const bool lsb = (R.flags & (sb == 0 ? kLsb0 : kLsb1)) != 0;
-			float turns = (float)(lsb ? k1 - nchan : k1) * dfs + R.postf[sb];
+			const float fce = (float)(lsb ? k1 - nchan : k1);
+			float th = fce * R.dhi[sb][p];
+			th -= rintf(th);
+			float turns = th + fmaf(fce, R.dlo[sb][p], R.post[sb][p]);
 			turns -= rintf(turns);
 			float qr, qi;
 			__sincosf(6.283185307179586f * turns, &qi, &qr);
 			qr *= osc;
 			qi *= osc;
-			float st32 = 32.0f * dfs;
-			st32 -= rintf(st32);
 			float sr, si;
-			__sincosf(6.283185307179586f * st32, &si, &sr);
+			__sincosf(6.283185307179586f * R.st32[sb][p], &si, &sr);
 			const uint32_t tcb = (uint32_t)R.tcb[sb];
 			uint32_t *o = (uint32_t *)a.spec + R.spec[sb] + (int64_t)row * tcb;
 			const uint32_t PT = (uint32_t)R.nrow[sb] * tcb;

@@ -90,6 +90,10 @@ struct Job {
 		int nzoom() const { return (int)zoom_freq.size(); }
 		float pcal_interval = 0.0f, pcal_base = 0.0f;   // phase-cal comb (MHz), float as the reference
 		int mux_threads = 0;                           // INTERLACEDVDIF: per-band data weights
+		// per band, of its recorded frequency: clock offset and R/L delta (us),
+		// phase offset (degrees), LO offset (Hz); has_corr: any of them nonzero
+		std::vector<double> clk, dclk, phase, looff;
+		bool has_corr = false;
 		// frequency of band k: recorded bands, then zoom bands
 		int total_freq(int k) const { return k < nband ? band_freq[k] : zoom_freq[k - nband]; }
 		char total_pol(int k) const { return k < nband ? band_pol[k] : zoom_pol[k - nband]; }

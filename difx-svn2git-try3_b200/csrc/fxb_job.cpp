@@ -219,6 +219,29 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 		for(int b = 0; b < in.nband; b++)
 			if(o.band_freq[b] < 0 || o.band_freq[b] >= d->nfreq)
 				return fail(err, st, FXB_ERR_ARG, "band frequency index out of range");
+		// corrections of each band's recorded frequency (configuration.cpp:1641-1672)
+		{
+			const double *src[4] = {in.band_clock_us, in.band_clock_delta_us, in.band_phase_deg, in.band_lo_offset_hz};
+			std::vector<double> *dst[4] = {&o.clk, &o.dclk, &o.phase, &o.looff};
+			for(int q = 0; q < 4; q++)
+			{
+				dst[q]->assign(in.nband, 0.0);
+				if(!src[q])
+					continue;
+				for(int b = 0; b < in.nband; b++)
+				{
+					const double v = src[q][b];
+					if(!std::isfinite(v))
+						return fail(err, st, FXB_ERR_ARG, "band corrections must be finite");
+					(*dst[q])[b] = v;
+					if(v != 0.0)
+						o.has_corr = true;
+					for(int c = 0; c < b; c++)
+						if(o.band_freq[c] == o.band_freq[b] && (*dst[q])[c] != v)
+							return fail(err, st, FXB_ERR_ARG, "bands of one frequency carry different corrections");
+				}
+			}
+		}
 		const fxb_freq &f0 = job.freqs[o.band_freq[0]];
 		for(int b = 1; b < in.nband; b++)
 		{

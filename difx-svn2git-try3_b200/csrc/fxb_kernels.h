@@ -74,7 +74,46 @@ struct FGroup {
 	int32_t nb;
 	int32_t lsb;
 	double lofreq;
+	// corrections of the subband's recorded frequency (mode.cpp:870-1145,
+	// 1296-1347): per band the clock term of the fractional-sample rotation,
+	// fse - clk[j] (us; offset -/+ delta/2 by polarisation), and the
+	// phase-offset rotation (turns); the LO offset (Hz) of the fringe rotation
+	double clk[2];
+	double looff;
+	float phase[2];
+	int32_t corr;            // any correction nonzero
+	int32_t pad_;
 };
+
+#if defined(__CUDACC__)
+// D (turns per channel) as hi + lo with hi holding 10 significant bits, so
+// that c * hi is exact in FP32 for |c| <= 8192 and the channel phase
+// c * D = (c * hi mod 1) + c * lo keeps FP32 accuracy however many turns
+// c * D spans (large clock offsets)
+__device__ __forceinline__ void split_turns(double D, float &hi, float &lo)
+{
+	int e;
+	frexp(D, &e);
+	const double h = D == 0.0 ? 0.0 : ldexp(rint(ldexp(D, 9 - e)), e - 9);
+	hi = (float)h;
+	lo = (float)(D - h);
+}
+
+// LO-offset fringe phase (turns) at wall-clock time w (seconds since the job
+// start) except the per-sample term: -looff (w - int w) - frac(looff) int w,
+// the integer seconds entering only through the offset's fractional part
+// (mode.cpp:873-882, 932-951)
+__device__ __forceinline__ double looff_wall_turns(double looff, double w)
+{
+	if(looff == 0.0)
+		return 0.0;
+	const int iw = (int)w;
+	double fl = fabs(looff) - (int)fabs(looff);
+	if(looff < 0)
+		fl = -fl;
+	return -looff * (w - iw) - (fabs(fl) > (double)1e-9f ? fl * iw : 0.0);
+}
+#endif
 
 struct FKind {
 	int32_t first, count;    // range of work items in the item table

@@ -97,6 +97,15 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
 	// whose per-frame band masks do not fit the fixed scratch array
 	if(st.mux_threads != 0)
 		return FXB_ERR_UNSUPPORTED;
+	// per-band clock, phase and LO offsets are applied by the context path's
+	// F stages only
+	{
+		const double *corr[4] = {st.band_clock_us, st.band_clock_delta_us, st.band_phase_deg, st.band_lo_offset_hz};
+		for(int q = 0; q < 4; q++)
+			for(int b = 0; corr[q] && b < st.nband && b < kMaxBandsPerStation; b++)
+				if(corr[q][b] != 0.0)
+					return FXB_ERR_UNSUPPORTED;
+	}
 	if(st.nband < 1 || st.nband > kMaxBandsPerStation || !st.band_freq || (st.nband & (st.nband - 1)) ||
 	   (st.nbits != 2 && st.nbits != 8) || (st.nbits == 8 && st.nband > 4) || st.payload_bytes <= 0 ||
 	   st.payload_bytes % 8 || ((int64_t)st.payload_bytes * 8) % (st.nbits * st.nband) ||

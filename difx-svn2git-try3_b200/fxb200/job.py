@@ -63,6 +63,14 @@ class Station:
     # VDIF); data weights are then per band, and EDV4 validity masks in the
     # frame headers blank absent bands
     mux_threads: int = 0
+    # per recorded frequency (freq index -> (clock offset us, R/L clock delta
+    # us, phase offset degrees, LO offset Hz)): the datastream table's
+    # "CLK OFFSET n (us)" = offset[:delta[:phase]] and "FREQ OFFSET n (Hz)"
+    freq_corr: dict = dataclasses.field(default_factory=dict)
+
+    def band_corr(self, b: int) -> Tuple[float, float, float, float]:
+        """(clock us, clock delta us, phase deg, LO offset Hz) of band b's frequency."""
+        return tuple(self.freq_corr.get(self.bands[b][0], (0.0, 0.0, 0.0, 0.0)))
 
     def recorded_freqs(self) -> List[int]:
         seen: List[int] = []

@@ -34,7 +34,11 @@ class FxbStation(ctypes.Structure):
                 ("nband", ctypes.c_int32), ("band_freq", ctypes.POINTER(ctypes.c_int32)),
                 ("band_pol", ctypes.c_char_p), ("nzoom", ctypes.c_int32), ("mux_threads", ctypes.c_int32),
                 ("zoom_freq", ctypes.POINTER(ctypes.c_int32)), ("zoom_pol", ctypes.c_char_p),
-                ("pcal_interval_mhz", ctypes.c_double), ("pcal_base_mhz", ctypes.c_double)]
+                ("pcal_interval_mhz", ctypes.c_double), ("pcal_base_mhz", ctypes.c_double),
+                ("band_clock_us", ctypes.POINTER(ctypes.c_double)),
+                ("band_clock_delta_us", ctypes.POINTER(ctypes.c_double)),
+                ("band_phase_deg", ctypes.POINTER(ctypes.c_double)),
+                ("band_lo_offset_hz", ctypes.POINTER(ctypes.c_double))]
 
 
 class FxbBaseline(ctypes.Structure):
@@ -69,10 +73,16 @@ class DescHolder:
             zf = (ctypes.c_int32 * max(nz, 1))(*[b[0] for b in s.zoom_bands])
             zp = ctypes.create_string_buffer("".join(b[1] for b in s.zoom_bands).encode(), nz + 1)
             self.keep += [bf, bp, zf, zp]
+            corr = [None] * 4
+            if s.freq_corr:
+                for q in range(4):
+                    arr = (ctypes.c_double * s.nband)(*[s.band_corr(k)[q] for k in range(s.nband)])
+                    self.keep.append(arr)
+                    corr[q] = ctypes.cast(arr, ctypes.POINTER(ctypes.c_double))
             st[i] = FxbStation(s.nbits, s.payload_bytes, s.header_bytes, s.nband,
                                ctypes.cast(bf, ctypes.POINTER(ctypes.c_int32)), ctypes.cast(bp, ctypes.c_char_p),
                                nz, s.mux_threads, ctypes.cast(zf, ctypes.POINTER(ctypes.c_int32)),
-                               ctypes.cast(zp, ctypes.c_char_p), s.pcal_interval_mhz, s.pcal_base_mhz)
+                               ctypes.cast(zp, ctypes.c_char_p), s.pcal_interval_mhz, s.pcal_base_mhz, *corr)
         bl = (FxbBaseline * len(job.baselines))()
         for i, b in enumerate(job.baselines):
             pf, p1, p2 = [], [], []

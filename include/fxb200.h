@@ -98,6 +98,25 @@ typedef struct {
 	 * weights, band by band (core.cpp:1124-1150). */
 	double pcal_interval_mhz;
 	double pcal_base_mhz;
+	/* Corrections per recorded frequency, given per band (bands of one
+	 * frequency carry equal values; each pointer may be null for all zero):
+	 * the DATASTREAM TABLE's "CLK OFFSET n (us)", read as offset[:delta[:phase]],
+	 * and "FREQ OFFSET n (Hz)" (configuration.cpp:1641-1672).  As Mode::process
+	 * applies them (mode.cpp:870-1145, 1296-1347, 435-460):
+	 *  - the fractional-sample rotation of a band uses fse - offset + delta/2
+	 *    when the band's polarisation is R, fse - offset - delta/2 otherwise;
+	 *  - the fringe rotation subtracts LO offset x wall-clock time (seconds
+	 *    since the job start) from the fringe phase in turns;
+	 *  - where a frequency has two or more bands, the first two in band order
+	 *    carry the phase offset: the one that is not R (the first, if neither
+	 *    is) is rotated by exp(+i pi phase / 360).
+	 * (The reference's VDIF Mode receives its FILTERBANK flag in the place of
+	 * linear2circular, configuration.cpp:1009, so no linear-to-circular
+	 * conversion happens on this path.) */
+	const double *band_clock_us;       /* [nband] clock offset, us */
+	const double *band_clock_delta_us; /* [nband] R/L clock delta, us */
+	const double *band_phase_deg;      /* [nband] phase offset, degrees */
+	const double *band_lo_offset_hz;   /* [nband] LO offset, Hz */
 } fxb_station;
 
 /* One baseline (BASELINE TABLE, configuration.cpp:1059-1120): products are
@@ -420,8 +439,9 @@ FXB_API fxb_status fxb_vdif_unpack(const uint8_t *data, int64_t nbytes, int32_t 
  * (one station).  The subint holds T = subint_ns / (2 nchan x 1000 / (2 bw_mhz))
  * FFTs (returned in *nfft when nfft is not NULL): spectra_floats must be at
  * least T x nband x nchan x 2 and, with dev_weights, weight_floats at least
- * T, else FXB_ERR_ARG.  INTERLACEDVDIF stations (mux_threads != 0) are
- * refused with FXB_ERR_UNSUPPORTED; zoom bands and phase-cal tones of the
+ * T, else FXB_ERR_ARG.  INTERLACEDVDIF stations (mux_threads != 0) and
+ * stations with nonzero per-band clock, phase or LO offsets are refused with
+ * FXB_ERR_UNSUPPORTED; zoom bands and phase-cal tones of the
  * station are not produced.  Returns when the work on `stream` has
  * completed. */
 FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, int32_t nfreq, const fxb_station *station,

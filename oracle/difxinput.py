@@ -112,8 +112,12 @@ def write_job_files(job: Job, outdir: str, name: str = "job",
         for j, f in enumerate(rf):
             npol = sum(1 for ff, _ in st.bands if ff == f)
             s.append(_kv("REC FREQ INDEX %d" % j, f))
-            s.append(_kv("CLK OFFSET %d (us)" % j, "0.000000"))
-            s.append(_kv("FREQ OFFSET %d (Hz)" % j, "0.000000"))
+            clk, dclk, ph, looff = st.freq_corr.get(f, (0.0, 0.0, 0.0, 0.0))
+            if dclk or ph:
+                s.append(_kv("CLK OFFSET %d (us)" % j, "%.9f:%.9f:%.9f" % (clk, dclk, ph)))
+            else:
+                s.append(_kv("CLK OFFSET %d (us)" % j, "%.9f" % clk))
+            s.append(_kv("FREQ OFFSET %d (Hz)" % j, "%.9f" % looff))
             s.append(_kv("NUM REC POLS %d" % j, npol))
         for k, (f, pol) in enumerate(st.bands):
             s.append(_kv("REC BAND %d POL" % k, pol))

@@ -75,6 +75,9 @@ typedef struct fxo_job {
 	int *mux;                                         /* INTERLACEDVDIF: per-band weights */
 	int **band_freq;
 	char **band_pol;
+	/* per band: clock offset and R/L delta (us), phase offset (degrees), LO
+	 * offset (Hz) of the band's recorded frequency (configuration.cpp:1641-1672) */
+	double **bclk, **bdclk, **bphase, **blooff;
 	int *nzoom;
 	int **zoom_freq, **zoom_parent, **zoom_choff;   /* parent: recorded band index */
 	/* phase cal per station and recorded band: tones, bins (0: the dummy
@@ -363,9 +366,25 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 	j->band_freq = (int **)calloc(d->nstation, sizeof(int *));
 	j->band_pol = (char **)calloc(d->nstation, sizeof(char *));
 	j->poly = (oracle_poly *)calloc(d->nstation, sizeof(oracle_poly));
+	j->bclk = (double **)calloc(d->nstation, sizeof(double *));
+	j->bdclk = (double **)calloc(d->nstation, sizeof(double *));
+	j->bphase = (double **)calloc(d->nstation, sizeof(double *));
+	j->blooff = (double **)calloc(d->nstation, sizeof(double *));
 	for(s = 0; s < d->nstation; s++)
 	{
 		const fxb_station *st = &d->stations[s];
+		int k;
+		j->bclk[s] = (double *)calloc(st->nband + 1, sizeof(double));
+		j->bdclk[s] = (double *)calloc(st->nband + 1, sizeof(double));
+		j->bphase[s] = (double *)calloc(st->nband + 1, sizeof(double));
+		j->blooff[s] = (double *)calloc(st->nband + 1, sizeof(double));
+		for(k = 0; k < st->nband; k++)
+		{
+			if(st->band_clock_us) j->bclk[s][k] = st->band_clock_us[k];
+			if(st->band_clock_delta_us) j->bdclk[s][k] = st->band_clock_delta_us[k];
+			if(st->band_phase_deg) j->bphase[s][k] = st->band_phase_deg[k];
+			if(st->band_lo_offset_hz) j->blooff[s][k] = st->band_lo_offset_hz[k];
+		}
 		j->nbits[s] = st->nbits;
 		j->mux[s] = st->mux_threads > 0;
 		j->payload[s] = st->payload_bytes;
@@ -810,8 +829,9 @@ static fft_info mode_process(const fxo_job *j, int s, const uint8_t *buf, int64_
 	fftstartmicrosec = i * fftchannels * sampletime;
 	starttime = (offsetsec - datasec) * 1000000.0 + ((double)((long long)offsetns - (long long)datans)) / 1000.0 + fftstartmicrosec - averagedelay;
 	nearestsample = (int)(starttime / sampletime + 0.5);
+	/* seconds since the job start: the scan starts with the job here
+	 * (Model::getScanStartSec is 0 for it) */
 	walltimesecs = offsetsec + offsetns / 1.0e9 + fftstartmicrosec / 1.0e6;
-	(void)walltimesecs;
 	info.nearestsample = nearestsample;
 	if(nearestsample < -1 || (((int64_t)(nearestsample + fftchannels) / 1) * bpbn) / bpbd > nbytes)
 		return info;
@@ -890,20 +910,39 @@ static fft_info mode_process(const fxo_job *j, int s, const uint8_t *buf, int64_
 		}
 
 		/* one pass per recorded frequency; bands are matched to it */
+		const int intwalltime = (int)walltimesecs;
+		const double fracwalltime = walltimesecs - intwalltime;
 		for(b = 0; b < nb; b++)
 		{
 			int fi = j->band_freq[s][b];
 			int lsb = j->freqs[fi].lower_sideband;
 			double lofreq = j->freqs[fi].freq_mhz;
 			double fraclo = (lofreq - (int)lofreq) * (double)integerdelay;
+			/* LO offset (mode.cpp:873-882, 932-951): the fringe phase loses
+			 * looff x (sample time + wall-clock time) in turns, the integer
+			 * seconds only through the offset's fractional part */
+			const double looff = j->blooff[s][b];
+			double fraclooff = 0.0, lowall = 0.0;
+			/* fractional-sample error of this band: per-frequency clock offset,
+			 * R/L delta split by polarisation (mode.cpp:1053-1059, 1099-1106,
+			 * 1264-1268) */
+			const double fseb = info.fracsampleerror - j->bclk[s][b] +
+			                    (j->band_pol[s][b] == 'R' ? 0.5 : -0.5) * j->bdclk[s][b];
 			const float *x = scratch + (int64_t)b * samplestounpack + off;
 			int n, c;
+			if(looff != 0.0)
+			{
+				fraclooff = fabs(looff) - (int)fabs(looff);
+				if(looff < 0) fraclooff = -fraclooff;
+				lowall = -looff * fracwalltime - (fabs(fraclooff) > (double)1e-9f ? fraclooff * intwalltime : 0.0);
+			}
 			if(order == 0)
 			{
 				/* post-F: real FFT, fringe phase at the FFT centre (mode.cpp:1061-1070, 1157-1180) */
 				double pr = (averagedelay - integerdelay) * lofreq;
 				double prf;
 				if(j->fractionallofreq) pr += integerdelay * (lofreq - (int)lofreq);
+				pr -= walltimesecs * looff;
 				prf = -TWO_PI_D * (pr - (int)pr);
 				for(n = 0; n < fftchannels; n++) { work[n].re = x[n]; work[n].im = 0.0; }
 				dfft(work, fftchannels);
@@ -911,7 +950,7 @@ static fft_info mode_process(const fxo_job *j, int s, const uint8_t *buf, int64_
 				{
 					dcx v = lsb ? (dcx){ work[nchan - c].re, -work[nchan - c].im } : work[c];
 					double fc = lsb ? (double)(c - nchan) * bw / nchan : (double)c * bw / nchan;
-					double arg = TWO_PI_D * fc * info.fracsampleerror + prf;
+					double arg = TWO_PI_D * fc * fseb + prf;
 					double cr = cos(arg), ci = sin(arg);
 					spec[(int64_t)b * nchan + c].re = v.re * cr - v.im * ci;
 					spec[(int64_t)b * nchan + c].im = v.re * ci + v.im * cr;
@@ -930,6 +969,8 @@ static fft_info mode_process(const fxo_job *j, int s, const uint8_t *buf, int64_
 					ph = (xj * (bb + a * X1) + cc) * lofreq + kk * (xj * (2.0 * a * X1)) * lofreq
 					     + (Xk * bb + Xk * Xk * a) * lofreq;
 				if(j->fractionallofreq) ph += fraclo;
+				if(looff != 0.0)
+					ph += -looff * ((double)n * sampletime / 1e6) + lowall;
 				ph = -TWO_PI_D * (ph - floor(ph));
 				work[n].re = x[n] * cos(ph);
 				work[n].im = x[n] * sin(ph);
@@ -939,10 +980,33 @@ static fft_info mode_process(const fxo_job *j, int s, const uint8_t *buf, int64_
 			{
 				dcx v = lsb ? work[nchan + c] : work[c];
 				double fc = lsb ? (double)(c - nchan) * bw / nchan : (double)c * bw / nchan;
-				double arg = TWO_PI_D * fc * info.fracsampleerror;
+				double arg = TWO_PI_D * fc * fseb;
 				double cr = cos(arg), ci = sin(arg);
 				spec[(int64_t)b * nchan + c].re = v.re * cr - v.im * ci;
 				spec[(int64_t)b * nchan + c].im = v.re * ci + v.im * cr;
+			}
+		}
+		/* phase offset (mode.cpp:435-460, 1336-1347): of a frequency with two
+		 * or more bands, the first two in band order, the one that is not R
+		 * (the first if it is not R) is rotated by exp(+i pi phase / 360) */
+		for(b = 0; b < nb; b++)
+		{
+			int fi = j->band_freq[s][b], q, b1 = -1, lcp, c;
+			int first = 1;
+			double ang, cr, ci;
+			for(q = 0; q < b; q++) if(j->band_freq[s][q] == fi) first = 0;
+			if(!first || j->bphase[s][b] == 0.0) continue;
+			for(q = b + 1; q < nb; q++) if(j->band_freq[s][q] == fi) { b1 = q; break; }
+			if(b1 < 0) continue;
+			lcp = j->band_pol[s][b] == 'R' ? b1 : b;
+			ang = TWO_PI_D * j->bphase[s][b] / 720.0;
+			cr = cos(ang);
+			ci = sin(ang);
+			for(c = 0; c < nchan; c++)
+			{
+				dcx v = spec[(int64_t)lcp * nchan + c];
+				spec[(int64_t)lcp * nchan + c].re = v.re * cr - v.im * ci;
+				spec[(int64_t)lcp * nchan + c].im = v.re * ci + v.im * cr;
 			}
 		}
 	}

@@ -211,3 +211,24 @@ def edv4_inputs(job: Job, inputs, seed=5):
         fr[:, 24:32] = masks.reshape(-1, 1).view(np.uint8)
         out.append((fr.reshape(-1), dsec, dns))
     return out
+
+
+def corr_job(order=1, clock=True, delta=True, phase=True, looff=True, seed=9, **kw) -> Job:
+    """A full-polarisation job whose stations carry per-frequency clock
+    offsets, R/L clock deltas, phase offsets and LO offsets (the datastream
+    table's CLK OFFSET offset:delta:phase and FREQ OFFSET), seeded; the first
+    station's first frequency keeps a zero clock offset, as the reference asks
+    of a telescope's first band."""
+    kw.setdefault("nstation", 3)
+    kw.setdefault("full_pol", True)
+    kw.setdefault("nfreq", 2)
+    job = small_job(order=order, **kw)
+    rng = np.random.default_rng(seed)
+    for s, st in enumerate(job.stations):
+        for f in st.recorded_freqs():
+            clk = 0.0 if (s == 0 and f == st.bands[0][0]) or not clock else float(rng.uniform(-0.2, 0.2))
+            dclk = float(rng.uniform(-0.02, 0.02)) if delta else 0.0
+            ph = float(rng.uniform(-60.0, 60.0)) if phase else 0.0
+            lo = float(rng.uniform(-2500.0, 2500.0)) if looff else 0.0
+            st.freq_corr[f] = (clk, dclk, ph, lo)
+    return job

@@ -105,3 +105,21 @@ def test_job_rejections():
     job.stations[0].nbits = 4
     with pytest.raises(Exception):
         native.job_layout(job)
+
+
+def test_band_corrections_accepted_and_checked():
+    # per-frequency clock / phase / LO offsets leave the layout as it is; bands
+    # of one frequency must agree on them
+    from helpers import corr_job
+    job = corr_job()
+    lay, n = native.job_layout(job)
+    plain = small_job(nstation=3, full_pol=True, nfreq=2, order=1)
+    lay0, n0 = native.job_layout(plain)
+    assert n == n0 and np.array_equal(lay, lay0)
+    holder = native.DescHolder(job)
+    st = holder.desc.stations[1]
+    st.band_clock_us[1] = st.band_clock_us[0] + 0.001      # bands 0 and 1 record the same frequency
+    out = np.zeros(64, dtype=np.int32)
+    rc = native.lib().fxb_job_layout(holder.ptr(), out.ctypes.data_as(native.ctypes.POINTER(native.ctypes.c_int32)),
+                                     out.size, native.ctypes.byref(native.ctypes.c_int64(0)))
+    assert rc == 1                      # FXB_ERR_ARG

@@ -166,3 +166,26 @@ def test_adjacent_station_buffers_give_the_same_result(xmac):
         res.append(corr.results())
         corr.close()
     assert np.array_equal(res[0], res[1])
+
+
+@pytest.mark.parametrize("name,kw", [("order1", dict(order=1)), ("order0", dict(order=0)),
+                                     ("order2", dict(order=2, seed=3)),
+                                     ("lsb_fraclo", dict(order=1, lsb=True, freq0=8400.25)),
+                                     ("clock_large", dict(order=1, looff=False, phase=False)),
+                                     ("2048pt_8bands", dict(order=1, nchan=1024, bw=32.0, nfreq=4,
+                                                            subint_ns=2_048_000))])
+def test_band_corrections(name, kw):
+    """Per-frequency clock offsets with R/L deltas, phase offsets and LO offsets
+    (mode.cpp:870-1145, 1296-1347) on a subint 1.5 s into the job, against the
+    oracle (itself pinned to the compiled reference on the same corrections)."""
+    from helpers import corr_job
+    job = corr_job(**kw)
+    if name == "clock_large":
+        # offsets of several microseconds: tens of turns across the band
+        for st in job.stations:
+            for f in st.freq_corr:
+                clk, dclk, ph, lo = st.freq_corr[f]
+                st.freq_corr[f] = (clk * 25.0, dclk, ph, lo)
+    got, ref, layout, n, w, wref = run_both(job, [(1, 500_000_000)])
+    compare_core(job, layout, n, got, ref)
+    assert np.array_equal(w, wref)

@@ -176,3 +176,19 @@ def test_fp16_long_ffts_vs_fp64(nchan):
     e = tc_errors(job, layout, n, got, ref)
     print(nchan, e)
     assert_tc_gate(e)
+
+
+@pytest.mark.parametrize("kw", [dict(order=1, nchan=1024, bw=32.0, nfreq=4, subint_ns=2_048_000),
+                                dict(order=0, nchan=1024, bw=32.0, nfreq=2, subint_ns=2_048_000),
+                                dict(order=1, nchan=256),
+                                dict(order=2, nchan=512, seed=3)])
+def test_fp16_band_corrections_vs_fp64(kw):
+    """Clock, phase and LO offsets in the tensor-core form: the 2048-point
+    kinds run the tensor-core FFT (k_fstage_tc), the others the CUDA-core F
+    stage with FP16 output; both within the relative gate."""
+    from helpers import corr_job
+    job = corr_job(**kw)
+    got, ref, layout, n = run_tc(job, [(1, 500_000_000), (1, 502_048_000 if kw.get("subint_ns") else 504_000_000)])
+    e = tc_errors(job, layout, n, got, ref)
+    print(kw, e)
+    assert_tc_gate(e)

@@ -167,3 +167,31 @@ def test_vdif_decode_matches_mark5access(nchan, nbits):
         o, ogood = fxoracle.vdif_unpack(data, 1024, 32, nchan, nbits, off, n)
         assert rgood == ogood, (off, n, rgood, ogood)
         assert np.array_equal(r, o), (off, n)
+
+
+CORR_JOBS = {
+    "corr_order1": dict(order=1),
+    "corr_order0": dict(order=0),
+    "corr_order2": dict(order=2, seed=3),
+    "corr_lsb_fraclo": dict(order=1, lsb=True, freq0=8400.25),
+    "corr_looff_only": dict(order=1, clock=False, delta=False, phase=False),
+    "corr_clock_only_8bit": dict(order=1, looff=False, phase=False, delta=False, nbits=8),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CORR_JOBS))
+def test_corrections_subint_matches_reference(name):
+    # per-frequency clock offsets and R/L deltas in the fractional-sample
+    # rotation, LO offsets in the fringe rotation and phase offsets of the
+    # non-R band (mode.cpp:870-1145, 1296-1347, 435-460), on a subint that
+    # starts 1.5 s into the job so that the wall-clock terms matter
+    from helpers import corr_job
+    job = corr_job(**CORR_JOBS[name])
+    ref = refcorr.RefCorrelator(job)
+    orc = fxoracle.OracleCorrelator(job)
+    sec, ns = 1, 500_000_000
+    inputs = synth.subint_inputs(job, sec, ns, rho=0.05, seed=17)
+    vf = [synth.valid_flags(job) for _ in job.stations]
+    r = ref.process_subint(inputs, vf, 0, sec, ns)
+    o = orc.process_subint(inputs, sec, ns, validflags=vf)
+    compare_core(job, orc.layout(), orc.corelen, r.astype(np.float64), o, tol=2e-6)
