@@ -971,11 +971,11 @@ static void slot_account(fxb_ctx *ctx, Slot &sl)
 // `copied` event marks their end.
 static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes,
                                const int32_t *datasec, const int32_t *datans, const int32_t *const *validflags,
-                               int32_t sec, int32_t ns, bool device, Slot **slot)
+                               int32_t sec, int32_t ns, bool device, Slot **slot, const double *interp = nullptr)
 {
 	if(!ctx || !bufs || !nbytes || !datasec || !datans)
 		return FXB_ERR_ARG;
-	for(int s = 0; s < ctx->S; s++)
+	for(int s = 0; s < ctx->S && !interp; s++)
 		if(!ctx->delay_set[s])
 		{
 			ctx->err = "delay model not set for every station";
@@ -1046,6 +1046,16 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 		u.datans = datans[s];
 		u.subsec = sec;
 		u.subns = ns;
+		if(interp)
+		{
+			// the caller's interpolator (Mode::setOffsets' own, mode.cpp:1541-1554);
+			// NaN: no model for this time, the subint is torched
+			u.interp_given = 1;
+			u.interp[0] = interp[3 * s];
+			u.interp[1] = interp[3 * s + 1];
+			u.interp[2] = interp[3 * s + 2];
+			u.invalid_subint = std::isnan(interp[3 * s]) ? 1 : 0;
+		}
 		if(device)
 			u.buf = bufs[s];
 		else if(merged)
@@ -1259,7 +1269,8 @@ static fxb_status slot_graph(fxb_ctx *ctx, Slot &sl)
 }
 
 static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes, const int32_t *datasec,
-                         const int32_t *datans, const int32_t *const *validflags, int32_t sec, int32_t ns, bool device)
+                         const int32_t *datans, const int32_t *const *validflags, int32_t sec, int32_t ns, bool device,
+                         const double *interp = nullptr)
 {
 	if(ctx && ctx->batched)
 	{
@@ -1267,7 +1278,7 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 		return FXB_ERR_STATE;
 	}
 	Slot *slp = nullptr;
-	const fxb_status rc = stage_subint(ctx, bufs, nbytes, datasec, datans, validflags, sec, ns, device, &slp);
+	const fxb_status rc = stage_subint(ctx, bufs, nbytes, datasec, datans, validflags, sec, ns, device, &slp, interp);
 	if(rc != FXB_OK)
 		return rc;
 	Slot &sl = *slp;
@@ -1405,6 +1416,15 @@ fxb_status fxb_submit_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const int
                              const int32_t *datans, const int32_t *const *validflags, int32_t sec, int32_t ns)
 {
 	return submit(ctx, bufs, nbytes, datasec, datans, validflags, sec, ns, false);
+}
+
+fxb_status fxb_submit_subint_interp(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes,
+                                    const int32_t *datasec, const int32_t *datans, const int32_t *const *validflags,
+                                    int32_t sec, int32_t ns, const double *interp)
+{
+	if(!interp)
+		return FXB_ERR_ARG;
+	return submit(ctx, bufs, nbytes, datasec, datans, validflags, sec, ns, false, interp);
 }
 
 fxb_status fxb_submit_subint_device(fxb_ctx *ctx, const uint8_t *const *dev_bufs, const int64_t *nbytes,

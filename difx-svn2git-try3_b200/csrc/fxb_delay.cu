@@ -120,7 +120,7 @@ __global__ void k_interpolators(const DevStation *__restrict__ st, DevSubintStat
                                 int blockspersend)
 {
 	int s = blockIdx.x * blockDim.x + threadIdx.x;
-	if(s >= S)
+	if(s >= S || sub[s].interp_given)
 		return;
 	double c[3] = {0.0, 0.0, 0.0};
 	bool ok = delay_interpolator(st[s], blockspersend, sub[s].subsec, sub[s].subns, c);

@@ -72,7 +72,7 @@ struct DevSubintStation {
 	int32_t datasec, datans;
 	int32_t invalid_subint; // no delay model for this time (subint torched)
 	int32_t subsec, subns;  // subint start (the setOffsets time), the same for every station
-	int32_t pad;
+	int32_t interp_given;   // interp was given by the caller (no device evaluation of the polynomials)
 	double interp[3];       // quadratic delay interpolator (Mode::setOffsets)
 };
 

@@ -178,6 +178,21 @@ FXB_API fxb_status fxb_submit_subint(fxb_ctx *ctx, const uint8_t *const *bufs, c
                              const int32_t *datasec, const int32_t *datans,
                              const int32_t *const *validflags, int32_t sec, int32_t ns);
 
+/* As fxb_submit_subint, with each station's quadratic delay interpolator for
+ * this subint given by the caller instead of derived on the device from the
+ * polynomials of fxb_set_delay_poly (which then need not be set): interp[3 s
+ * .. 3 s + 2] are the coefficients Mode::setOffsets obtains from
+ * Model::calculateDelayInterpolator(scan, sec + ns / 1e9, subint seconds,
+ * blockspersend, ..., 2, c) with 1e6 x the integer clock seconds taken from
+ * c[2] (mode.cpp:1541-1549): delay(us) = c[0] i^2 + c[1] i + c[2] at FFT
+ * index i.  NaN in interp[3 s] marks a station without a model for this time
+ * (its subint is torched, mode.cpp:1551-1554).  This is the call an
+ * integration into mpifxcorr makes, with the reference's own Model. */
+FXB_API fxb_status fxb_submit_subint_interp(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t *nbytes,
+                                    const int32_t *datasec, const int32_t *datans,
+                                    const int32_t *const *validflags, int32_t sec, int32_t ns,
+                                    const double *interp);
+
 /* As fxb_submit_subint but with the station buffers already in device
  * memory (pointers from cudaMalloc); they must stay valid until the next
  * fxb_sync.  validflags stay in host memory. */

@@ -35,6 +35,8 @@
 #include "model.h"
 #include "mark5access.h"
 #include "vdiffile.h"
+#include "fxb_config_adapter.h"
+#include <dlfcn.h>
 #include <pthread.h>
 
 namespace {
@@ -618,3 +620,104 @@ void dref_ds_destroy(void *d)
 }
 
 }
+
+/* ---- the integration flow: Configuration -> fxb200 C ABI ---------------- */
+
+extern "C" {
+
+/* The fxb_job_desc of configuration 0, built by fxb_desc_from_configuration
+ * from the stock Configuration; it stays valid until the process exits.
+ * Returns null with err filled for a configuration outside the ABI. */
+const void *dref_fxb_desc(void *h, int xmac_kind, char *err, int errlen)
+{
+	RefJob *j = (RefJob *)h;
+	static std::vector<FxbConfigDesc *> keep;    // one per call, kept until the process exits
+	FxbConfigDesc *d = new FxbConfigDesc;
+	std::string e;
+	if(!fxb_desc_from_configuration(j->config, 0, xmac_kind, *d, e))
+	{
+		snprintf(err, errlen, "%s", e.c_str());
+		delete d;
+		return 0;
+	}
+	keep.push_back(d);
+	return &d->desc;
+}
+
+/* Each datastream's delay interpolator for (scan, sec, ns), from the stock
+ * Model as Mode::setOffsets obtains it; returns the datastreams without one. */
+int dref_fxb_interpolators(void *h, int scan, int sec, int ns, double *interp)
+{
+	RefJob *j = (RefJob *)h;
+	return fxb_interpolators_from_model(j->config, 0, scan, sec, ns, interp);
+}
+
+/* What an integration into mpifxcorr does per configuration, written against
+ * the product library's C ABI (loaded from libpath): the descriptor from the
+ * Configuration, a context, then per subint k the interpolators from the
+ * Model and fxb_submit_subint_interp with the datastreams' buffers
+ * bufs[k * nds + ds]; finally fxb_read_results into coreresult (2 corelen
+ * floats).  Returns 0, or -1 with err filled. */
+int dref_fxb_correlate(void *h, const char *libpath, int xmac_kind, int nsub, const unsigned char *const *bufs,
+                       const long long *nbytes, const int *datasec, const int *datans, const int *sec, const int *ns,
+                       float *coreresult, long long nfloats, char *err, int errlen)
+{
+	RefJob *j = (RefJob *)h;
+	typedef fxb_ctx *(*create_t)(const fxb_job_desc *, fxb_status *);
+	typedef fxb_status (*submit_t)(fxb_ctx *, const uint8_t *const *, const int64_t *, const int32_t *,
+	                               const int32_t *, const int32_t *const *, int32_t, int32_t, const double *);
+	typedef fxb_status (*read_t)(fxb_ctx *, float *, size_t);
+	typedef void (*destroy_t)(fxb_ctx *);
+	typedef const char *(*lasterr_t)(const fxb_ctx *);
+	void *lib = dlopen(libpath, RTLD_NOW | RTLD_LOCAL);
+	if(!lib)
+	{
+		snprintf(err, errlen, "dlopen: %s", dlerror());
+		return -1;
+	}
+	create_t fxb_create_p = (create_t)dlsym(lib, "fxb_create");
+	submit_t fxb_submit_subint_interp_p = (submit_t)dlsym(lib, "fxb_submit_subint_interp");
+	read_t fxb_read_results_p = (read_t)dlsym(lib, "fxb_read_results");
+	destroy_t fxb_destroy_p = (destroy_t)dlsym(lib, "fxb_destroy");
+	lasterr_t fxb_last_error_p = (lasterr_t)dlsym(lib, "fxb_last_error");
+	if(!fxb_create_p || !fxb_submit_subint_interp_p || !fxb_read_results_p || !fxb_destroy_p || !fxb_last_error_p)
+	{
+		snprintf(err, errlen, "missing fxb200 entry points");
+		return -1;
+	}
+
+	FxbConfigDesc d;
+	std::string e;
+	if(!fxb_desc_from_configuration(j->config, 0, xmac_kind, d, e))
+	{
+		snprintf(err, errlen, "%s", e.c_str());
+		return -1;
+	}
+	fxb_status st = FXB_OK;
+	fxb_ctx *ctx = fxb_create_p(&d.desc, &st);
+	if(!ctx)
+	{
+		snprintf(err, errlen, "fxb_create: %d %s", (int)st, fxb_last_error_p(0));
+		return -1;
+	}
+	const int nds = j->numds;
+	std::vector<double> interp(3 * nds);
+	std::vector<int64_t> nb(nds);
+	for(int k = 0; k < nsub && st == FXB_OK; k++)
+	{
+		fxb_interpolators_from_model(j->config, 0, 0, sec[k], ns[k], interp.data());
+		for(int ds = 0; ds < nds; ds++)
+			nb[ds] = nbytes[k * nds + ds];
+		st = fxb_submit_subint_interp_p(ctx, bufs + (size_t)k * nds, nb.data(), datasec + (size_t)k * nds,
+		                                datans + (size_t)k * nds, 0, sec[k], ns[k], interp.data());
+	}
+	if(st == FXB_OK)
+		st = fxb_read_results_p(ctx, coreresult, (size_t)nfloats);
+	if(st != FXB_OK)
+		snprintf(err, errlen, "fxb200: %d %s", (int)st, fxb_last_error_p(ctx));
+	fxb_destroy_p(ctx);
+	return st == FXB_OK ? 0 : -1;
+}
+
+}
+

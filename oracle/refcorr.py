@@ -110,6 +110,54 @@ class RefCorrelator:
         with open(files[0], "rb") as f:
             return f.read()
 
+    # ---- the integration flow (oracle/fxb_config_adapter.cpp)
+    def fxb_desc_address(self, xmac_kind: int = 0) -> int:
+        """Address of the fxb_job_desc that fxb_desc_from_configuration builds
+        from this job's stock Configuration (kept alive by the library)."""
+        L = lib()
+        L.dref_fxb_desc.restype = ctypes.c_void_p
+        L.dref_fxb_desc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        err = ctypes.create_string_buffer(256)
+        p = L.dref_fxb_desc(self.h, xmac_kind, err, 256)
+        if not p:
+            raise RuntimeError("adapter: " + err.value.decode())
+        return p
+
+    def fxb_interpolators(self, scan: int, sec: int, ns: int) -> Tuple[np.ndarray, int]:
+        L = lib()
+        L.dref_fxb_interpolators.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_double)]
+        out = np.zeros(3 * self.numds, dtype=np.float64)
+        missing = L.dref_fxb_interpolators(self.h, scan, sec, ns, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out.reshape(self.numds, 3), missing
+
+    def fxb_correlate(self, libpath: str, subints, xmac_kind: int = 0) -> np.ndarray:
+        """The adapter's integration flow against the product library at
+        libpath: subints = [(inputs, sec, ns)] with inputs per datastream
+        (bytes, datasec, datans); returns the product's core result."""
+        L = lib()
+        L.dref_fxb_correlate.restype = ctypes.c_int
+        L.dref_fxb_correlate.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_float), ctypes.c_longlong, ctypes.c_char_p,
+                                         ctypes.c_int]
+        keep = [np.ascontiguousarray(b) for inputs, _, _ in subints for b, _, _ in inputs]
+        bufs = (ctypes.c_void_p * len(keep))(*[k.ctypes.data for k in keep])
+        nb = (ctypes.c_longlong * len(keep))(*[k.size for k in keep])
+        dsec = _iarr([x for inputs, _, _ in subints for _, x, _ in inputs])
+        dns = _iarr([x for inputs, _, _ in subints for _, _, x in inputs])
+        sec = _iarr([s for _, s, _ in subints])
+        ns = _iarr([n for _, _, n in subints])
+        out = np.zeros(2 * self.corelen, dtype=np.float32)
+        err = ctypes.create_string_buffer(512)
+        rc = L.dref_fxb_correlate(self.h, libpath.encode(), xmac_kind, len(subints), bufs, nb, dsec, dns, sec, ns,
+                                  _fptr(out), out.size, err, 512)
+        if rc != 0:
+            raise RuntimeError("integration flow: " + err.value.decode())
+        return out
+
     def datastream(self, ds: int, factor: int, nseg: int) -> "RefRing":
         """The reference's VDIF datastream ds with nseg segments of
         factor / nseg times the largest subint's bytes."""
