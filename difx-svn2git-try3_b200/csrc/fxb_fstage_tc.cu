@@ -247,7 +247,10 @@ struct TcLayout {
 	static constexpr int kOffLut = kOffStg + kNStg * kStgBytes;
 	static constexpr int kOffTw = kOffLut + 256 * 16;     // twiddles w_2048^(n2 k1), float2 [k1][n2]
 	static constexpr int kOffRing = kOffTw + kN1 * kN2 * 8;
-	static constexpr int kUsed = kOffRing + kRing * (int)sizeof(UnitRec);
+	// per output warp and lane: the spectra offset of channel k1 + 32 j (j = 0..31)
+	// in the blocked layout of the last (tcb, nrow) seen
+	static constexpr int kOffOutTab = (kOffRing + kRing * (int)sizeof(UnitRec) + 15) & ~15;
+	static constexpr int kUsed = kOffOutTab + 4 * 32 * 32 * 4;
 	static constexpr size_t kSmem = 1024 + (size_t)kUsed;
 	static_assert(kOffStg % 16 == 0 && kStgBytes % 16 == 0, "staging must be 16-aligned");
 	static_assert(kSmem <= 227 * 1024, "shared memory");
@@ -353,7 +356,7 @@ __device__ __forceinline__ UnitRec build_unit(const FsArgs &a, const int32_t *pa
 // the two subbands of a work unit (-1: none); unit u = pair u % npairs at
 // FFT time u / npairs.  BPT: bits per time of the stations' VDIF words
 // (2-bit bands: 2 x bands).
-template <int BPT>
+template <int BPT, bool H16>
 __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, const uint4 *__restrict__ tables,
                                                           const int32_t *__restrict__ pairs, int npairs, int nunits,
                                                           int32_t *err)
@@ -730,7 +733,9 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 		const int sb = ch >> 1, p = ch & 1;
 		const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
 		constexpr float osc = 1.0f / (float)(1 << kTcSpecExp);
-		const bool h16 = a.h16 != 0;
+		// this lane's offsets, read back only by itself
+		uint32_t *otab = (uint32_t *)(base + LY::kOffOutTab) + ch * 1024 + lane;
+		int tab_tcb = -1, tab_nrow = -1;
 		for(int k = 0; k < nk; k++)
 		{
 			const int b = k & 1;
@@ -768,27 +773,28 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 			qi *= osc;
 			float sr, si;
 			__sincosf(6.283185307179586f * R.st32[sb][p], &si, &sr);
-			const uint32_t tcb = (uint32_t)R.tcb[sb];
+			const int tcb = R.tcb[sb];
 			uint32_t *o = (uint32_t *)a.spec + R.spec[sb] + (int64_t)row * tcb;
-			const uint32_t PT = (uint32_t)R.nrow[sb] * tcb;
-			uint32_t blk = (uint32_t)k1 / tcb, cl = (uint32_t)k1 - blk * tcb;
-			const uint32_t dblk = 32u / tcb, dcl = 32u - dblk * tcb;
-			uint32_t off = blk * PT + cl;
+			if(tcb != tab_tcb || R.nrow[sb] != tab_nrow)
+			{
+				// channel c = k1 + 32 j sits at (c / tcb) nrow tcb + c % tcb
+				tab_tcb = tcb;
+				tab_nrow = R.nrow[sb];
+				const uint32_t PT = (uint32_t)tab_nrow * (uint32_t)tcb;
+				for(int j = 0; j < 32; j++)
+				{
+					const uint32_t c = (uint32_t)(k1 + 32 * j), blk = c / (uint32_t)tcb;
+					otab[32 * j] = blk * PT + (c - blk * (uint32_t)tcb);
+				}
+			}
 #pragma unroll
 			for(int j = 0; j < 32; j++)
 			{
 				const float xr = v[2 * j], xi = v[2 * j + 1];
-				o[off] = pack_spec(h16, xr * qr - xi * qi, xr * qi + xi * qr);
+				o[otab[32 * j]] = pack_spec(H16, xr * qr - xi * qi, xr * qi + xi * qr);
 				const float nr = qr * sr - qi * si;
 				qi = qr * si + qi * sr;
 				qr = nr;
-				cl += dcl;
-				off += dblk * PT + dcl;
-				if(cl >= tcb)
-				{
-					cl -= tcb;
-					off += PT - tcb;
-				}
 			}
 		}
 	}
@@ -940,13 +946,14 @@ void launch_fstage_tc(const FKind &k, FsArgs a, int nsm, cudaStream_t stream)
 		cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 		kern<<<grid, kThreadsTc, smem, stream>>>(a, (const uint4 *)k.tctab, k.tcpairs, k.tcnpairs, nunits, a.err);
 	};
+	const bool h = a.h16 != 0;
 	switch(k.tcbpt)
 	{
-	case 4: go(k_fstage_tc<4>, TcLayout<4>::kSmem); break;
-	case 8: go(k_fstage_tc<8>, TcLayout<8>::kSmem); break;
-	case 16: go(k_fstage_tc<16>, TcLayout<16>::kSmem); break;
-	case 32: go(k_fstage_tc<32>, TcLayout<32>::kSmem); break;
-	case 64: go(k_fstage_tc<64>, TcLayout<64>::kSmem); break;
+	case 4: h ? go(k_fstage_tc<4, true>, TcLayout<4>::kSmem) : go(k_fstage_tc<4, false>, TcLayout<4>::kSmem); break;
+	case 8: h ? go(k_fstage_tc<8, true>, TcLayout<8>::kSmem) : go(k_fstage_tc<8, false>, TcLayout<8>::kSmem); break;
+	case 16: h ? go(k_fstage_tc<16, true>, TcLayout<16>::kSmem) : go(k_fstage_tc<16, false>, TcLayout<16>::kSmem); break;
+	case 32: h ? go(k_fstage_tc<32, true>, TcLayout<32>::kSmem) : go(k_fstage_tc<32, false>, TcLayout<32>::kSmem); break;
+	case 64: h ? go(k_fstage_tc<64, true>, TcLayout<64>::kSmem) : go(k_fstage_tc<64, false>, TcLayout<64>::kSmem); break;
 	default: break;
 	}
 }
