@@ -148,6 +148,7 @@ struct fxb_ctx {
 	int nsm = 0;
 	int64_t specn_elems = 0;
 	int32_t *d_err = nullptr;
+	cudaError_t launch_err = cudaSuccess;   // first failed kernel launch of the last launch_compute
 };
 
 static std::mutex g_err_mutex;
@@ -1144,7 +1145,11 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 				}
 			}
 			if(k.tcfft)
-				launch_fstage_tc(k, fa, ctx->nsm, st);
+			{
+				const cudaError_t le = launch_fstage_tc(k, fa, ctx->nsm, st);
+				if(le != cudaSuccess && ctx->launch_err == cudaSuccess)
+					ctx->launch_err = le;
+			}
 			else
 				launch_fstage_kind(k, fa, st);
 		}
@@ -1189,6 +1194,24 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 	launch_weights(ctx->d_bw, ctx->nbw, ctx->d_acw, ctx->nacw, ctx->d_params, ctx->d_pbw, ctx->nbm, ctx->d_st, ctx->T,
 	               ctx->d_bwacc, ctx->d_acwacc, st);
 	cudaEventRecordWithFlags(sl.tev[3], st, evf);
+	// a launch that could not start (resources, configuration) leaves its
+	// error behind; keep it for the submit to report
+	const cudaError_t le = cudaPeekAtLastError();
+	if(le != cudaSuccess && ctx->launch_err == cudaSuccess)
+		ctx->launch_err = le;
+}
+
+// The first kernel-launch failure recorded by launch_compute since the last
+// call, as a status (cleared).
+static fxb_status take_launch_err(fxb_ctx *ctx)
+{
+	const cudaError_t e = ctx->launch_err;
+	if(e == cudaSuccess)
+		return FXB_OK;
+	ctx->launch_err = cudaSuccess;
+	cudaGetLastError();
+	ctx->err = std::string("kernel launch failed: ") + cudaGetErrorString(e);
+	return FXB_ERR_CUDA;
 }
 
 // Reads one tuning subint's launch times (waits for it), and after the last
@@ -1295,6 +1318,11 @@ static fxb_status submit(fxb_ctx *ctx, const uint8_t *const *bufs, const int64_t
 		CK(ctx, cudaGraphLaunch(sl.gexec, st));
 	else
 		launch_compute(ctx, sl, st, false);
+	{
+		const fxb_status le = take_launch_err(ctx);
+		if(le != FXB_OK)
+			return le;
+	}
 	if(tuning)
 		tune_collect(ctx);
 	CK(ctx, cudaGetLastError());
@@ -2070,6 +2098,12 @@ static fxb_status batch_submit(fxb_batch *b, const fxb_member_subint *data, int3
 	else
 		for(size_t i = 0; i < n; i++)
 			launch_compute(b->m[i], *slots[i], b->stream, false);
+	for(fxb_ctx *c : b->m)
+		if(take_launch_err(c) != FXB_OK)
+		{
+			b->err = c->err;
+			return FXB_ERR_CUDA;
+		}
 	for(fxb_ctx *c : b->m)
 		if(c->tune.iter < c->tune.total)
 			tune_collect(c);

@@ -23,19 +23,21 @@
 // MN-major operands let each thread store 16-byte runs: the decode writes 8
 // consecutive times n2 of one n1, the twiddle 8 consecutive k1 of one n2.
 //
-// Persistent CTAs (one per SM), warp-specialised:
-//   warp 13     producer: builds the records of 32 units at a time (one lane
+// Persistent CTAs (one per SM, 18 warps at 96 registers: an SM sub-partition
+// holds at most five of them in its 16384 registers), warp-specialised:
+//   warp 17     producer: builds the records of 32 units at a time (one lane
 //               per unit: pair, FFT parameters, fringe and fractional-sample
 //               constants, output offsets) into a shared-memory ring and
 //               stages each unit's VDIF window into shared memory (bulk
 //               copies of the valid frames),
-//   warps 0-3   decode: 8 consecutive times -> the fringe-rotated FP16
+//   warps 0-7   decode: 8 consecutive times -> the fringe-rotated FP16
 //               samples of the unit's four channels (two-time lookup of
 //               both polarisations, FP32 rotation),
-//   warps 4-7   twiddle: D1 (tensor memory) -> Z (FP16 operand, in the
-//               operand buffer MMA 1 has finished with),
-//   warps 8-11  output: D2 -> fractional-sample rotation -> FP16 (or BF16) spectra,
-//   warp 12     MMA issuer (one thread).
+//   warps 8-11  twiddle: D1 (tensor memory, 32 columns at a time) -> Z (FP16
+//               operand, in the operand buffer MMA 1 has finished with),
+//   warps 12-15 output: D2 (32 columns at a time) -> fractional-sample
+//               rotation -> FP16 (or BF16) spectra,
+//   warp 16     MMA issuer (one thread).
 // Three operand buffers and two tensor-memory slots (D1 + D2 per slot)
 // keep decode, MMAs, twiddle and output of different units overlapped.
 // Every wait is bounded; a timeout sets the error flag, the CTA stops,
@@ -66,9 +68,13 @@ constexpr int kB2Bytes = 2 * 64 * 128;          // DFT-64 of one sideband: 2 K h
 constexpr int kOffB1 = 0, kOffB2 = kB1Bytes;
 constexpr int kTablesBytes = kOffB2 + 2 * kB2Bytes;
 constexpr int kOffOp = kTablesBytes;            // 1024-aligned
-// 14 warps: the SM sub-partitions that hold four of them give each thread at
-// most 128 registers
-constexpr int kThreadsTc = 448;
+// warp roles: kDecW decode warps, then 4 twiddle and 4 output warps (each
+// set covers the four tensor-memory lane quadrants, warp % 4), the MMA warp
+// and the producer warp
+constexpr int kDecW = 8;
+constexpr int kTwW0 = kDecW, kOutW0 = kDecW + 4, kMmaW = kDecW + 8, kProdW = kDecW + 9;
+constexpr int kThreadsTc = 32 * (kDecW + 10);
+static_assert(kTwW0 % 4 == 0 && kOutW0 % 4 == 0 && 8 % kDecW == 0, "warp roles");
 constexpr uint32_t kWaitLimitF = 1u << 22;
 constexpr int kTmemCols = 512;
 
@@ -397,7 +403,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 		for(int i = 0; i < kNStg; i++)
 		{
 			mbar_init(&stg_full[i], 1);
-			mbar_init(&stg_empty[i], 4);
+			mbar_init(&stg_empty[i], kDecW);
 		}
 		for(int i = 0; i < 2; i++)
 		{
@@ -409,7 +415,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 		}
 		for(int i = 0; i < kNS; i++)
 		{
-			mbar_init(&op_full[i], 4);
+			mbar_init(&op_full[i], kDecW);
 			mbar_init(&op_empty[i], 1);
 		}
 		mbar_init(&mma_done, 1);
@@ -418,7 +424,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 		stg_used_s = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 	}
-	if(warp == 12)
+	if(warp == kMmaW)
 	{
 		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(su32(&tmem_s)),
 		             "r"((uint32_t)kTmemCols));
@@ -430,7 +436,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 	asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 	const uint32_t tmem = tmem_s;
 
-	if(warp == 13)
+	if(warp == kProdW)
 	{
 		// ================================================================ producer
 		bool ok = true;
@@ -488,7 +494,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 			}
 		}
 	}
-	else if(warp < 4)
+	else if(warp < kDecW)
 	{
 		// ================================================================ decode
 		const int dt = tid;
@@ -534,9 +540,9 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 			const int so = R.so, fs = R.fs, swbits = R.swbits;
 			const uint32_t fmask = R.fmask;
 #pragma unroll 1
-			for(int it = 0; it < 2; it++)
+			for(int it = 0; it < 8 / kDecW; it++)
 			{
-				const int item = dt + 128 * it;
+				const int item = dt + 32 * kDecW * it;
 				const int n1 = item >> 3, g = item & 7;
 				const int n0 = 64 * n1 + 8 * g;             // first time of the item
 				// the item's 8 times (bits swbits + n0 BPT ..) as NW aligned 32-bit
@@ -671,10 +677,10 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 			}
 		}
 	}
-	else if(warp < 8)
+	else if(warp < kOutW0)
 	{
 		// ================================================================ twiddle
-		const int L = tid - 128;                // tensor-memory lane (p, n2)
+		const int L = tid - 32 * kTwW0;         // tensor-memory lane (p, n2)
 		const int p = L >> 6, n2 = L & 63;
 		const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
 		const float2 *tw = twt + n2;             // w_2048^(n2 k1) at tw[k1 kN2]
@@ -689,27 +695,28 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 			asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 			unsigned char *A2 = ops + s * kOpBytes;
 #pragma unroll 1
-			for(int sb = 0; sb < 2; sb++)
+			for(int h = 0; h < 4; h++)
 			{
-				float v[64];
-				const uint32_t tcol = tmem + lane_base + (uint32_t)(256 * b + 64 * sb);
-				tld32(tcol, v);
-				tld32(tcol + 32, v + 32);
+				// subband sb, channels k1 in [16 hh, 16 hh + 16): 32 columns
+				const int sb = h >> 1, hh = h & 1;
+				float v[32];
+				tld32(tmem + lane_base + (uint32_t)(256 * b + 64 * sb + 32 * hh), v);
 				tld_wait();
 				// Z[k1][n2] = Y[k1][n2] w^(n2 k1); A2 row m = ch 32 + k1 with ch = 2 sb + p,
 				// K = part 64 + n2
-				const int m0 = (2 * sb + p) * 32;
-				uint32_t zr[16], zi[16];
+				const int m0 = (2 * sb + p) * 32 + 16 * hh;
+				uint32_t zr[8], zi[8];
 #pragma unroll
-				for(int k1 = 0; k1 < kN1; k1 += 2)
+				for(int q = 0; q < 16; q += 2)
 				{
-					const float y0r = v[2 * k1], y0i = v[2 * k1 + 1], y1r = v[2 * k1 + 2], y1i = v[2 * k1 + 3];
+					const int k1 = 16 * hh + q;
+					const float y0r = v[2 * q], y0i = v[2 * q + 1], y1r = v[2 * q + 2], y1i = v[2 * q + 3];
 					const float2 w0 = tw[k1 * kN2], w1 = tw[(k1 + 1) * kN2];
-					zr[k1 >> 1] = pack_h2(y0r * w0.x - y0i * w0.y, y1r * w1.x - y1i * w1.y);
-					zi[k1 >> 1] = pack_h2(y0r * w0.y + y0i * w0.x, y1r * w1.y + y1i * w1.x);
+					zr[q >> 1] = pack_h2(y0r * w0.x - y0i * w0.y, y1r * w1.x - y1i * w1.y);
+					zi[q >> 1] = pack_h2(y0r * w0.y + y0i * w0.x, y1r * w1.y + y1i * w1.x);
 				}
 #pragma unroll
-				for(int c = 0; c < 4; c++)
+				for(int c = 0; c < 2; c++)
 				{
 					*(uint4 *)(A2 + mn_off(m0 + 8 * c, n2)) = make_uint4(zr[4 * c], zr[4 * c + 1], zr[4 * c + 2], zr[4 * c + 3]);
 					*(uint4 *)(A2 + mn_off(m0 + 8 * c, 64 + n2)) =
@@ -726,10 +733,10 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 			}
 		}
 	}
-	else if(warp < 12)
+	else if(warp < kMmaW)
 	{
 		// ================================================================ output
-		const int ch = warp - 8, k1 = lane;
+		const int ch = warp - kOutW0, k1 = lane;
 		const int sb = ch >> 1, p = ch & 1;
 		const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
 		constexpr float osc = 1.0f / (float)(1 << kTcSpecExp);
@@ -745,19 +752,13 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 				break;
 			}
 			asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-			float v[64];
+			// channels k1 + 32 j, j in [0, 16) then [16, 32): 32 columns each
+			float v[32];
 			const uint32_t tcol = tmem + lane_base + (uint32_t)(256 * b + 128);
 			tld32(tcol, v);
-			tld32(tcol + 32, v + 32);
 			tld_wait();
-			asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-			__syncwarp();
-			if(lane == 0)
-				mbar_arrive(&d2_empty[b]);
 			const UnitRec &R = ring[k % kRing];
 			const int row = R.row[sb][p];
-			if(row < 0)
-				continue;
 			// channel c = k1 + 32 j: exp(2 pi i (ce D + post)), ce = c (upper
 			// sideband) or c - nchan (lower), D = hi + lo (ce hi exact), stepped
 			// by exp(2 pi i 32 D)
@@ -774,8 +775,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 			float sr, si;
 			__sincosf(6.283185307179586f * R.st32[sb][p], &si, &sr);
 			const int tcb = R.tcb[sb];
-			uint32_t *o = (uint32_t *)a.spec + R.spec[sb] + (int64_t)row * tcb;
-			if(tcb != tab_tcb || R.nrow[sb] != tab_nrow)
+			uint32_t *o = (uint32_t *)a.spec + R.spec[sb] + (int64_t)(row < 0 ? 0 : row) * tcb;
+			if(row >= 0 && (tcb != tab_tcb || R.nrow[sb] != tab_nrow))
 			{
 				// channel c = k1 + 32 j sits at (c / tcb) nrow tcb + c % tcb
 				tab_tcb = tcb;
@@ -788,17 +789,33 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 				}
 			}
 #pragma unroll
-			for(int j = 0; j < 32; j++)
+			for(int hh = 0; hh < 2; hh++)
 			{
-				const float xr = v[2 * j], xi = v[2 * j + 1];
-				o[otab[32 * j]] = pack_spec(H16, xr * qr - xi * qi, xr * qi + xi * qr);
-				const float nr = qr * sr - qi * si;
-				qi = qr * si + qi * sr;
-				qr = nr;
+				if(hh == 1)
+				{
+					tld32(tcol + 32, v);
+					tld_wait();
+					asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+					__syncwarp();
+					if(lane == 0)
+						mbar_arrive(&d2_empty[b]);
+				}
+				if(row < 0)
+					continue;
+#pragma unroll
+				for(int q = 0; q < 16; q++)
+				{
+					const int j = 16 * hh + q;
+					const float xr = v[2 * q], xi = v[2 * q + 1];
+					o[otab[32 * j]] = pack_spec(H16, xr * qr - xi * qi, xr * qi + xi * qr);
+					const float nr = qr * sr - qi * si;
+					qi = qr * si + qi * sr;
+					qr = nr;
+				}
 			}
 		}
 	}
-	else if(warp == 12 && lane == 0)
+	else if(warp == kMmaW && lane == 0)
 	{
 		// ================================================================ MMA issuer
 		// instruction descriptor: D F32 (bit 4), A and B F16, A MN-major (bit 15),
@@ -874,7 +891,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 	}
 	__syncthreads();
 	asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-	if(warp == 12)
+	if(warp == kMmaW)
 		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"((uint32_t)kTmemCols));
 }
 
@@ -933,10 +950,10 @@ bool fstage_tc_eligible(int N, int order, bool any_lsb)
 	return N == kN && (order == 1 || (order == 0 && !any_lsb));
 }
 
-void launch_fstage_tc(const FKind &k, FsArgs a, int nsm, cudaStream_t stream)
+cudaError_t launch_fstage_tc(const FKind &k, FsArgs a, int nsm, cudaStream_t stream)
 {
 	if(k.count <= 0 || a.T <= 0 || !k.tctab || !k.tcpairs || k.tcnpairs <= 0)
-		return;
+		return cudaSuccess;
 	a.first = k.first;
 	const int nunits = k.tcnpairs * a.T;
 	int grid = nsm;
@@ -956,6 +973,7 @@ void launch_fstage_tc(const FKind &k, FsArgs a, int nsm, cudaStream_t stream)
 	case 64: h ? go(k_fstage_tc<64, true>, TcLayout<64>::kSmem) : go(k_fstage_tc<64, false>, TcLayout<64>::kSmem); break;
 	default: break;
 	}
+	return cudaGetLastError();
 }
 
 }  // namespace fxb

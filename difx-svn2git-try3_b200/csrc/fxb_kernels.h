@@ -166,7 +166,8 @@ void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream);
 size_t fstage_tc_tables_bytes();
 void make_fstage_tc_tables(void *out);
 bool fstage_tc_eligible(int N, int order, bool any_lsb);
-void launch_fstage_tc(const FKind &k, FsArgs a, int nsm, cudaStream_t stream);
+// returns the launch's error
+cudaError_t launch_fstage_tc(const FKind &k, FsArgs a, int nsm, cudaStream_t stream);
 
 // twiddles of FFT length N, FKind::twn entries
 void make_fstage_twiddles(int N, float2 *out32);
