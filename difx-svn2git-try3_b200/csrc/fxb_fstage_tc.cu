@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1) k_fstage_tc(const FsArgs a, con
 						vm |= (kf < 32 ? ((fmask >> kf) & 1u) : 0u) << j;
 					}
 				}
-#pragma unroll
+#pragma unroll 1
 				for(int sb = 0; sb < 2; sb++)
 				{
 					const int nsh = 4 * R.nib[sb];
