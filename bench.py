@@ -295,20 +295,21 @@ def load_peaks():
 # ---------------------------------------------------------------- serving leg
 def serving_leg(args):
     """p50/p99 job latency and sustained throughput of the serving loop on a
-    seeded Poisson stream of jobs drawn from the serving workload's shape
-    ranges (4-32 stations, 1-16 subbands of 8-64 MHz, 256-8192 channels,
-    dual polarisation with cross hands); integrations of 0.1 s, the short end
-    of its 0.1-2 s range, so that the stream's VDIF (14 GB for 12 jobs) fits
-    in page-locked host memory (a 32-station, 16 x 64 MHz job holds 33 GB
-    per second of data)."""
+    seeded Poisson stream of jobs drawn from the serving workload's ranges
+    (4-32 stations, 1-16 subbands of 8-64 MHz, 256-8192 channels, 0.1-2 s
+    integrations, dual polarisation with cross hands).  Each job's subints
+    cycle three distinct subints of page-locked VDIF with their own times
+    (serving.job_subints pool=3), so that a 2 s job of the largest shape
+    (66 GB of VDIF) needs under 1 GB of host memory; every byte is still
+    copied to the device per subint."""
     from fxb200 import serving
     rng = np.random.default_rng(11)
     jobs = []
     for k in range(args.serving_jobs):
         job, nsub = serving.serving_job(rng, seed=100 + k, stations=(4, 32), subbands=(1, 16),
                                         bws=(8.0, 16.0, 32.0, 64.0), nchans=(256, 512, 1024, 2048, 4096, 8192),
-                                        seconds=(0.1, 0.1))
-        jobs.append((job, serving.job_subints(job, nsub, seed=100 + k, pinned=True)))
+                                        seconds=(0.1, 2.0))
+        jobs.append((job, serving.job_subints(job, nsub, seed=100 + k, pinned=True, pool=3)))
     rate = 20.0
     arrivals = serving.poisson_arrivals(rng, len(jobs), rate)
     srv = serving.Server(budget_bytes=96 << 30, max_active=4)
@@ -317,15 +318,21 @@ def serving_leg(args):
     srv.close()
     phase_p50 = {k: float(np.median([p[k] for p in phases])) for k in phases[0]} if phases else {}
     smhz = sum(job.station_mhz_per_sec() * len(subs) * job.subint_ns * 1e-9 for job, subs in jobs)
-    host_gb = sum(b.nbytes for _, subs in jobs for inputs, _, _ in subs for b, _, _ in inputs) / 1e9
-    shapes = [(len(j.stations), len(j.freqs), j.freqs[0].bw_mhz, j.freqs[0].nchan) for j, _ in jobs]
+    h2d = sum(b.nbytes for _, subs in jobs for inputs, _, _ in subs for b, _, _ in inputs)
+    shapes = [(len(j.stations), len(j.freqs), j.freqs[0].bw_mhz, j.freqs[0].nchan,
+               round(len(subs) * j.subint_ns * 1e-9, 3)) for j, subs in jobs]
+    link = h2d_link_gbs()
+    h2d_gbs = h2d / 1e9 / st["wall_seconds"] if st["wall_seconds"] > 0 else None
     return {"jobs": st["completed"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "rtf": st["rtf"], "station_mhz_per_s": smhz / st["wall_seconds"] if st["wall_seconds"] > 0 else None,
             "arrival_rate_hz": rate, "max_active": 4, "hbm_budget_gb": 96, "xmac": args.xmac,
-            "phase_ms_p50": phase_p50, "vdif_gb": host_gb, "shapes": shapes,
+            "phase_ms_p50": phase_p50, "h2d_gb": h2d / 1e9, "h2d_gbs": h2d_gbs, "h2d_link_gbs": link,
+            "h2d_link_frac": (h2d_gbs / link) if (h2d_gbs and link) else None,
+            "data_seconds": st["data_seconds"], "shapes": shapes,
             "sample": "%d seeded jobs, Poisson arrivals at %.0f/s; 4-32 stations, 1-16 subbands of 8-64 MHz, "
-                      "256-8192 channels, 0.1 s each, dual pol with cross hands; station buffers in "
-                      "page-locked host memory; latency = submit to core result in host memory" % (len(jobs), rate)}
+                      "256-8192 channels, 0.1-2 s each, dual pol with cross hands; station buffers in "
+                      "page-locked host memory (three distinct subints per job, cycled with their own times); "
+                      "latency = submit to core result in host memory" % (len(jobs), rate)}
 
 
 # ---------------------------------------------------------------- batched uneven subbands
@@ -750,7 +757,8 @@ def gpu_arm(args, job):
                                                                             "kernel_ms_per_subint")},
             "tc_vs_fp32": tc_vs_fp32,
             "serving": None if serve is None else {k: serve[k] for k in ("jobs", "p50_ms", "p99_ms", "rtf",
-                                                                          "station_mhz_per_s") if k in serve},
+                                                                          "station_mhz_per_s", "h2d_link_frac")
+                                                   if k in serve},
             "batched_c3": None if c3 is None else {"tc_batched_vs_fp32": c3["tc_batched_vs_fp32"],
                                                    "tc_batched_rtf": c3["tc_batched_graph"]["rtf"],
                                                    "tc_per_job_rtf": c3["tc_per_job"]["rtf"],

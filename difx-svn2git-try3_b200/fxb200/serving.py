@@ -198,33 +198,58 @@ def serving_job(rng: np.random.Generator, seed: int, stations=(4, 32), subbands=
     return job, nsub
 
 
-def job_subints(job: Job, nsub: int, seed: int, rho: float = 0.0, pinned: bool = False) -> List[Tuple[list, int, int]]:
+def job_subints(job: Job, nsub: int, seed: int, rho: float = 0.0, pinned: bool = False,
+                pool: int = 0) -> List[Tuple[list, int, int]]:
     """Host VDIF of nsub consecutive subints (starting one subint in): the bulk
     code-statistics generator for rho = 0, the correlated sky + noise model
     otherwise.  pinned=True places every buffer in one page-locked block, as
-    a datastream's receive ring would be."""
-    out = []
+    a datastream's receive ring would be.
+
+    pool > 0 generates only `pool` distinct subints of bytes (each as long as
+    the longest window of the job) and lets subint k reuse those of subint
+    k % pool, with its own data time and window length: a job of 2 s of a
+    32-station, 16 x 64 MHz array (66 GB of VDIF) then holds a few subints of
+    host memory, as a receive ring of a few segments does.  Every subint
+    still has its own time, delay interpolator and FFT windows; only the
+    sample values repeat."""
+    times = []
     for k in range(nsub):
         t = (k + 1) * job.subint_ns
-        sec, ns = t // 1_000_000_000, t % 1_000_000_000
+        times.append((t // 1_000_000_000, t % 1_000_000_000))
+    S = len(job.stations)
+    windows = [[synth.subint_window(job, s, sec, ns) for s in range(S)] for sec, ns in times]
+    ndistinct = nsub if pool <= 0 else min(pool, nsub)
+    longest = [max(w[s][1] for w in windows) for s in range(S)]
+    distinct = []
+    for k in range(ndistinct):
+        sec, ns = times[k]
         if rho == 0.0:
-            inputs = []
-            for s in range(len(job.stations)):
-                f0, nf, dsec, dns = synth.subint_window(job, s, sec, ns)
-                inputs.append((synth.bulk_station_frames(job, s, f0, nf, seed), dsec, dns))
+            bufs = []
+            for s in range(S):
+                f0, nf, _, _ = windows[k][s]
+                bufs.append(synth.bulk_station_frames(job, s, f0, longest[s] if pool > 0 else nf, seed))
         else:
-            inputs = synth.subint_inputs(job, sec, ns, rho=rho, seed=seed)
-        out.append((inputs, sec, ns))
+            bufs = [synth.gen_station_frames(job, s, windows[k][s][0], longest[s] if pool > 0 else windows[k][s][1],
+                                             rho, seed) for s in range(S)]
+        distinct.append(bufs)
     if pinned:
-        total = sum(b.nbytes for inputs, _, _ in out for b, _, _ in inputs)
+        total = sum(b.nbytes for bufs in distinct for b in bufs)
         block = pinned_empty(total)
         off = 0
-        for inputs, _, _ in out:
-            for k, (b, dsec, dns) in enumerate(inputs):
+        for bufs in distinct:
+            for s, b in enumerate(bufs):
                 v = block[off:off + b.nbytes]
                 v[:] = np.frombuffer(np.ascontiguousarray(b).data, dtype=np.uint8)
-                inputs[k] = (v, dsec, dns)
+                bufs[s] = v
                 off += b.nbytes
+    out = []
+    for k, (sec, ns) in enumerate(times):
+        bufs = distinct[k % ndistinct]
+        inputs = []
+        for s in range(S):
+            _, nf, dsec, dns = windows[k][s]
+            inputs.append((bufs[s][:nf * job.frame_bytes(s)] if pool > 0 else bufs[s], dsec, dns))
+        out.append((inputs, sec, ns))
     return out
 
 

@@ -132,3 +132,24 @@ def test_zoom_and_pcal_jobs_served_in_the_mix():
     for h, ref in zip(handles, alone):
         assert np.array_equal(srv.wait(h, 120.0), ref)
     srv.close()
+
+
+def test_long_jobs_served_beside_short_ones():
+    """The serving workload's 0.1-2 s range: a 2 s job (500 subints of 4 ms,
+    three distinct subints of VDIF cycled with their own times) and a 1 s job
+    served beside a 0.1 s one give each job's own result bit for bit."""
+    short = small_job(nstation=3, nchan=256, bw=16.0, nfreq=2, full_pol=True, seed=2)
+    long_ = small_job(nstation=4, nchan=256, bw=16.0, nfreq=1, full_pol=True, seed=5)
+    mid = small_job(nstation=2, nchan=512, bw=32.0, nfreq=2, full_pol=True, nbits=8, subint_ns=2_048_000, seed=6)
+    jobs = [(long_, serving.job_subints(long_, 500, seed=71, pinned=True, pool=3)),
+            (short, serving.job_subints(short, 25, seed=72, pool=3)),
+            (mid, serving.job_subints(mid, 488, seed=73, pool=3))]
+    assert abs(len(jobs[0][1]) * long_.subint_ns * 1e-9 - 2.0) < 1e-9
+    alone = [_alone(j, s, "fp16") for j, s in jobs]
+    srv = serving.Server(budget_bytes=8 << 30, max_active=3)
+    handles = [srv.submit(j, s, xmac="fp16") for j, s in jobs]
+    for h, ref in zip(handles, alone):
+        assert np.array_equal(srv.wait(h, 300.0), ref)
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == 3 and st["data_seconds"] > 3.0
