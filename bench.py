@@ -458,6 +458,90 @@ def mux_leg(args):
             "note": "three launches per read (placement, headers, corner turn) plus one 8-byte status read"}
 
 
+def mux_fused_leg(args):
+    """c1 with every station recorded as INTERLACEDVDIF (16 single-channel
+    threads of 8000-byte payloads, 2-bit, 64 Ms/s each; 128000-byte muxed
+    frames), device-resident raw reads of 3 distinct subints cycled: (a) the
+    reads muxed by fxb_vdif_mux and the muxed frames correlated, (b) the raw
+    reads correlated directly (fxb_station.mux_raw: placement inside the
+    context, each band read from its thread's frame in the F stage, no muxed
+    copy).  Both on the headline form; CUDA events on the context stream."""
+    import copy
+
+    import torch
+    from fxb200.native import Correlator, vdif_mux_device
+    job = configs.c1()
+    for st in job.stations:
+        st.payload_bytes = 8000 * 16
+        st.mux_threads = 16
+    job.validate()
+    raw_job = copy.deepcopy(job)
+    for st in raw_job.stations:
+        st.mux_raw = True
+    npool, nsub = 3, 16
+    rng = np.random.default_rng(5)
+    tp = 8000
+    fps = int(round(2 * job.station_bw(0) * 1e6 / (tp * 8 // 2)))
+    raw_dev, raw_meta, mux_out = [], [], []
+    for k in range(npool):
+        sec, ns = subint_time(job, k + 1)
+        bufs, nb, ds, dn, outs = [], [], [], [], []
+        for s in range(len(job.stations)):
+            f0, nf, dsec, dns = synth.subint_window(job, s, sec, ns)
+            muxed = synth.bulk_station_frames(job, s, f0, nf, seed=3 + k)
+            rb, _ = synth.raw_read(job, s, muxed, rng)
+            t = torch.from_numpy(rb).cuda()
+            bufs.append(t)
+            nb.append(rb.size)
+            ds.append(dsec)
+            dn.append(dns)
+            outs.append(torch.empty(muxed.size, dtype=torch.uint8, device="cuda"))
+        raw_dev.append(bufs)
+        raw_meta.append((nb, ds, dn, (sec, ns)))
+        mux_out.append(outs)
+
+    def run(fused):
+        c = Correlator(raw_job if fused else job, xmac=args.xmac, inflight=3)
+        st = torch.cuda.ExternalStream(c.stream())
+
+        def step():
+            for j in range(nsub):
+                k = j % npool
+                nb, ds, dn, (sec, ns) = raw_meta[k]
+                if fused:
+                    c.submit_device([t.data_ptr() for t in raw_dev[k]], nb, ds, dn, sec, ns)
+                else:
+                    nout = [vdif_mux_device(raw_dev[k][s].data_ptr(), nb[s], list(range(16)), tp + 32, fps, 2,
+                                            mux_out[k][s].data_ptr(), mux_out[k][s].numel())
+                            for s in range(len(job.stations))]
+                    c.submit_device([t.data_ptr() for t in mux_out[k]], nout, ds, dn, sec, ns)
+        for _ in range(args.warmup):
+            step()
+        c.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            step()
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / (args.steps * nsub)
+        r = c.results()
+        c.close()
+        return ms, r
+
+    ms_mux, r_mux = run(False)
+    ms_raw, r_raw = run(True)
+    data_ms = job.subint_ns * 1e-6
+    return {"workload": "c1 as INTERLACEDVDIF: 10 stations x 16 threads x 1 channel, 2-bit, 8000-byte thread "
+                        "payloads; raw reads of 3 distinct subints cycled (%d MB per subint)"
+                        % (sum(raw_meta[0][0]) // 1000000),
+            "mux_then_correlate_ms_per_subint": ms_mux, "fused_ms_per_subint": ms_raw,
+            "fused_speedup": ms_mux / ms_raw, "fused_rtf": data_ms / ms_raw,
+            "identical_results": bool(np.array_equal(r_mux, r_raw)),
+            "note": "(a) fxb_vdif_mux per station read (placement, headers, corner turn, status read) then the "
+                    "muxed frames correlated; (b) the raw reads correlated with no muxed copy"}
+
+
 # ---------------------------------------------------------------- GPU arm
 def features_leg(args, job, plain_value, step_device, max_over_ranks, data_s):
     """The headline workload correlated with a 1 MHz phase-cal comb on every
@@ -720,8 +804,10 @@ def gpu_arm(args, job):
     if rank == 0 and world == 1 and not args.no_c3:
         c3 = c3_leg(args)
     mux = None
+    muxf = None
     if rank == 0 and world == 1 and not args.no_mux:
         mux = mux_leg(args)
+        muxf = mux_fused_leg(args)
 
     # per subint: interpolators, frame validity, FFT parameters, one F-stage
     # launch per FFT length, one XMAC launch per group of equally shaped
@@ -736,6 +822,7 @@ def gpu_arm(args, job):
         # the full record first, then the headline line (last, compact) carrying
         # the secondary figures
         detail = {"bench_detail": True, "tuning": tuning, "serving": serve, "batched_c3": c3, "vdif_mux": mux,
+                  "vdif_mux_fused": muxf,
                   "features": feats, "other_form": other, "roofline": roofline, "xmac_roofline": xmac_roofline,
                   "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(detail), flush=True)
@@ -764,6 +851,9 @@ def gpu_arm(args, job):
                                                    "tc_per_job_rtf": c3["tc_per_job"]["rtf"],
                                                    "fp32_per_job_rtf": c3["fp32_per_job"]["rtf"]},
             "vdif_mux_frac": None if mux is None else mux["frac"],
+            "vdif_mux_fused": None if muxf is None else {k: muxf[k] for k in ("fused_ms_per_subint",
+                                                                              "mux_then_correlate_ms_per_subint",
+                                                                              "fused_speedup", "identical_results")},
             "gpu_launches": launches_per_subint * nsub * args.steps,
         }
         print(json.dumps(line), flush=True)

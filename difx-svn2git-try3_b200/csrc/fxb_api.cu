@@ -108,6 +108,11 @@ struct fxb_ctx {
 	float2 *d_core = nullptr;
 	uint8_t *d_valid = nullptr;          // frame validity [S][valid_stride], then the band masks
 	uint32_t *d_bandok = nullptr;        // [S][valid_stride] in the same allocation
+	// raw INTERLACEDVDIF reads: frame-slot tables, muxed headers and status
+	// words of those stations, carved per subint from one scratch block
+	int nraw = 0;
+	int32_t *d_mux = nullptr;
+	size_t mux_cap = 0;                  // int32 words
 	int64_t valid_stride = 0;
 	std::vector<Slot> slots;
 	int next_slot = 0;
@@ -273,6 +278,8 @@ static void free_ctx(fxb_ctx *ctx)
 		cudaFreeAsync(p, ctx->stream);
 	if(ctx->d_valid)
 		cudaFreeAsync(ctx->d_valid, ctx->stream);
+	if(ctx->d_mux)
+		cudaFreeAsync(ctx->d_mux, ctx->stream);
 	for(auto &s : ctx->slots)
 	{
 		for(auto *p : s.raw)
@@ -388,6 +395,22 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		d.mux = js.mux_threads > 0 ? 1 : 0;
 		if(d.mux)
 			ctx->nbm = std::max(ctx->nbm, js.nband);
+		if(js.mux_raw)
+		{
+			d.muxraw = 1;
+			d.nthr = js.mux_threads;
+			d.inframebytes = js.payload / js.mux_threads + 32;
+			const double fps = 2.0 * f.bw_mhz * 1e6 / d.framesamples;
+			d.fps = (int)(fps + 0.5);
+			if(std::fabs(fps - d.fps) > 1e-9 || d.fps < 1)
+			{
+				ctx->err = "raw INTERLACEDVDIF reads need a whole number of frames per second";
+				return FXB_ERR_UNSUPPORTED;
+			}
+			for(int t = 0; t < js.mux_threads; t++)
+				d.tmap[t] = js.mux_tids[t];
+			ctx->nraw++;
+		}
 		d.bpbn = (js.nband * 1 * js.nbits) / 8;
 		d.bpbd = 1;
 		if(d.bpbn == 0)
@@ -1015,6 +1038,32 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 		ctx->valid_stride = need;
 	}
 
+	// raw INTERLACEDVDIF reads: slot tables, muxed headers and status words
+	// (shared by the staging slots: their kernels run in stream order)
+	std::vector<size_t> mux_off(ctx->S, 0);
+	if(ctx->nraw)
+	{
+		size_t words = 0;
+		for(int s = 0; s < ctx->S; s++)
+		{
+			const DevStation &d = ctx->h_st[s];
+			if(!d.muxraw)
+				continue;
+			const int64_t nin = nbytes[s] / d.inframebytes;
+			mux_off[s] = words;
+			words += (size_t)(4 * nin / d.nthr) * d.nthr + (size_t)(nin / d.nthr + 1) * 16 + 4;
+			words = (words + 3) & ~(size_t)3;
+		}
+		if(words > ctx->mux_cap)
+		{
+			if(ctx->d_mux)
+				CK(ctx, cudaFreeAsync(ctx->d_mux, ctx->stream));
+			ctx->d_mux = nullptr;
+			CK(ctx, pool_alloc(ctx, (void **)&ctx->d_mux, sizeof(int32_t) * words, ctx->stream));
+			ctx->mux_cap = words;
+		}
+	}
+
 	// host buffers one after the other (as a datastream's receive ring holds
 	// them) with 16-byte aligned starts: one copy for the whole subint
 	bool merged = !device && ctx->S > 1;
@@ -1047,6 +1096,16 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 		u.datans = datans[s];
 		u.subsec = sec;
 		u.subns = ns;
+		if(ctx->h_st[s].muxraw)
+		{
+			const DevStation &d = ctx->h_st[s];
+			u.mux_nin = (int32_t)(nbytes[s] / d.inframebytes);
+			u.mux_nproc = u.mux_nin / d.nthr;
+			u.mux_nslot = 4 * u.mux_nin / d.nthr;
+			u.mux_slot = ctx->d_mux + mux_off[s];
+			u.mux_hdr = (uint32_t *)(u.mux_slot + (size_t)u.mux_nslot * d.nthr);
+			u.mux_status = (int32_t *)(u.mux_hdr + (size_t)(u.mux_nproc + 1) * 16);
+		}
 		if(interp)
 		{
 			// the caller's interpolator (Mode::setOffsets' own, mode.cpp:1541-1554);
@@ -1109,6 +1168,8 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 	const unsigned evf = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
 	cudaEventRecordWithFlags(sl.tev[0], st, evf);
 	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, st);
+	if(ctx->nraw)
+		launch_mux_raw(ctx->d_st, sl.d_sub, ctx->S, 0, 0, st);
 	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->d_bandok, ctx->valid_stride, ctx->S, st);
 	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->d_bandok, ctx->valid_stride,
 	                  ctx->S, ctx->T, job.fringe_rot_order, ctx->d_params, ctx->d_pbw, ctx->nbm, st);

@@ -29,8 +29,10 @@ __device__ __forceinline__ uint32_t edv4_bands(const DevStation &S, const DevSub
 {
 	if(U.nbytes < 32)
 		return 0xFFFFFFFFu;
-	const uint32_t w2 = *(const uint32_t *)(U.buf + 8), w3 = *(const uint32_t *)(U.buf + 12);
-	const uint32_t w4 = *(const uint32_t *)(U.buf + 16);
+	// the first frame of the (muxed) stream
+	const uint8_t *f0 = S.muxraw ? (const uint8_t *)U.mux_hdr : U.buf;
+	const uint32_t w2 = *(const uint32_t *)(f0 + 8), w3 = *(const uint32_t *)(f0 + 12);
+	const uint32_t w4 = *(const uint32_t *)(f0 + 16);
 	const int ml = (int)((w4 >> 16) & 0xFFu);
 	if((w4 >> 24) != 4u || ml < 1 || ml > 64)
 		return 0xFFFFFFFFu;
@@ -65,18 +67,29 @@ __global__ void k_frame_valid(const DevStation *__restrict__ st, const DevSubint
 	for(int64_t fr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; fr < valid_stride; fr += (int64_t)gridDim.x * blockDim.x)
 	{
 		uint8_t v = 0;
+		// raw INTERLACEDVDIF reads: the muxed frame's header and first and last
+		// payload words as the placement kernels wrote them
+		const uint8_t *f = S.muxraw ? (const uint8_t *)(U.mux_hdr + fr * 16) : U.buf + fr * S.framebytes;
 		if(fr < nframes)
 		{
-			const uint8_t *f = U.buf + fr * S.framebytes;
 			uint32_t w0 = *(const uint32_t *)(f);
 			uint32_t w2 = *(const uint32_t *)(f + 8);
-			uint64_t first = *(const uint64_t *)(f + S.header);
-			uint64_t last = *(const uint64_t *)(f + S.header + (S.payload / 8 - 1) * 8);
+			uint64_t first, last;
+			if(S.muxraw)
+			{
+				first = *(const uint64_t *)(f + 32);
+				last = *(const uint64_t *)(f + 40);
+			}
+			else
+			{
+				first = *(const uint64_t *)(f + S.header);
+				last = *(const uint64_t *)(f + S.header + (S.payload / 8 - 1) * 8);
+			}
 			v = (w2 != 0) && !((w0 >> 31) & 1) && first != FILL && last != FILL;
 		}
 		valid[s * valid_stride + fr] = v;
 		if(bandok)
-			bandok[s * valid_stride + fr] = (v && S.mux) ? edv4_bands(S, U, U.buf + fr * S.framebytes) : 0xFFFFFFFFu;
+			bandok[s * valid_stride + fr] = (v && S.mux) ? edv4_bands(S, U, f) : 0xFFFFFFFFu;
 	}
 }
 

@@ -313,7 +313,13 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 	constexpr int nchan = N / 2;
 	const uint32_t fs = (uint32_t)Sp->framesamples;
 	const int nbits = Sp->nbits;
-	const uint32_t bpt = (uint32_t)(Sp->nband * nbits);
+	// raw INTERLACEDVDIF reads: band b's samples are those of its thread's
+	// frame, found through the frame-slot table (one band per frame)
+	const bool muxraw = Sp->muxraw != 0;
+	const int32_t *mslot = muxraw ? a.sub[g.station].mux_slot : nullptr;
+	const int64_t mk0 = muxraw ? a.sub[g.station].mux_k0 : 0;
+	const int mnthr = Sp->nthr, minfb = Sp->inframebytes;
+	const uint32_t bpt = muxraw ? (uint32_t)nbits : (uint32_t)(Sp->nband * nbits);
 	const int header = Sp->header, framebytes = Sp->framebytes, asl = Sp->asl;
 	const double bw = Sp->bw;
 	const uint8_t *buf = a.sub[g.station].buf;
@@ -331,8 +337,8 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 	const double lo = g.lofreq;
 	const float ph0 = g.phase[0], ph1 = g.phase[1];     // phase-offset rotation of each band (turns)
 	const int row0 = g.row[0], row1 = g.row[1];
-	const uint32_t boff0 = (uint32_t)(g.band[0] * nbits), boff1 = (uint32_t)(g.band[1] * nbits);
-	const bool oneword = bpt <= 32;       // all bands of a sample time in one 32-bit word
+	const uint32_t boff0 = muxraw ? 0u : (uint32_t)(g.band[0] * nbits), boff1 = muxraw ? 0u : (uint32_t)(g.band[1] * nbits);
+	const bool oneword = !muxraw && bpt <= 32;       // all bands of a sample time in one 32-bit word
 	const bool pair4 = NV == 2 && nbits == 2 && oneword && boff1 == boff0 + 2;
 	const int order = a.order;
 	constexpr float osc = 1.0f / (float)(1 << kTcSpecExp);
@@ -493,9 +499,21 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 					}
 					ok = ok && n < stuck;
 					const uint32_t bit0 = tin * bpt + boff0, bit1 = tin * bpt + boff1;
-					const uint32_t *wp = (const uint32_t *)fp;
-					raw0[r] = ok ? __ldg(wp + (bit0 >> 5)) : 0u;
-					raw1[r] = (ok && !oneword && NV == 2) ? __ldg(wp + (bit1 >> 5)) : 0u;
+					if(muxraw)
+					{
+						// valid frames of raw reads are complete slots: every thread is there
+						const int32_t *slr = mslot + (mk0 + (int64_t)fa + kf) * mnthr;
+						const int i0 = ok ? __ldg(slr + g.band[0]) : -1;
+						const int i1 = (ok && NV == 2) ? __ldg(slr + g.band[1]) : -1;
+						raw0[r] = i0 >= 0 ? __ldg((const uint32_t *)(buf + (int64_t)i0 * minfb + 32) + (bit0 >> 5)) : 0u;
+						raw1[r] = i1 >= 0 ? __ldg((const uint32_t *)(buf + (int64_t)i1 * minfb + 32) + (bit1 >> 5)) : 0u;
+					}
+					else
+					{
+						const uint32_t *wp = (const uint32_t *)fp;
+						raw0[r] = ok ? __ldg(wp + (bit0 >> 5)) : 0u;
+						raw1[r] = (ok && !oneword && NV == 2) ? __ldg(wp + (bit1 >> 5)) : 0u;
+					}
 					pk[r] = (bit0 & 31u) | ((bit1 & 31u) << 8) | ((uint32_t)ok << 16);
 					if(r < 7)
 					{

@@ -49,6 +49,10 @@ struct DevStation {
 	int32_t sticky;         // 8-bit 2/4-channel blank semantics
 	int32_t mux;            // INTERLACEDVDIF: per-band weights, EDV4 band blanking
 	int32_t bpbn, bpbd;     // bytes-per-block numerator/denominator of Mode
+	// raw INTERLACEDVDIF reads (muxraw): the threads' frames, one band each;
+	// the geometry above is the muxed stream's
+	int32_t muxraw, nthr, inframebytes, fps;
+	int32_t tmap[32];       // VDIF thread id of each band's thread
 	double bw;              // MHz
 	double sampletime;      // us
 	int32_t npoly, order, interval;
@@ -74,6 +78,15 @@ struct DevSubintStation {
 	int32_t subsec, subns;  // subint start (the setOffsets time), the same for every station
 	int32_t interp_given;   // interp was given by the caller (no device evaluation of the polynomials)
 	double interp[3];       // quadratic delay interpolator (Mode::setOffsets)
+	// raw INTERLACEDVDIF reads: buf holds nin thread frames; the device
+	// places them into frame slots ([nslot][nthr] input frame or -1), writes
+	// the muxed stream's headers (16 words per output frame: header, first
+	// and last 64-bit payload words) and then sets nbytes / datasec / datans
+	// to the muxed stream's and k0 to its first slot
+	int32_t *mux_slot;
+	uint32_t *mux_hdr;
+	int32_t *mux_status;    // [0] error, [2] first filled slot
+	int32_t mux_nin, mux_nproc, mux_nslot, mux_k0;
 };
 
 // Host-side job after validation.
@@ -90,6 +103,8 @@ struct Job {
 		int nzoom() const { return (int)zoom_freq.size(); }
 		float pcal_interval = 0.0f, pcal_base = 0.0f;   // phase-cal comb (MHz), float as the reference
 		int mux_threads = 0;                           // INTERLACEDVDIF: per-band data weights
+		bool mux_raw = false;                          // buffers are raw reads, de-interleaved in the F stage
+		std::vector<int> mux_tids;                     // raw reads: VDIF thread id of each band's thread
 		// per band, of its recorded frequency: clock offset and R/L delta (us),
 		// phase offset (degrees), LO offset (Hz); has_corr: any of them nonzero
 		std::vector<double> clk, dclk, phase, looff;

@@ -317,6 +317,26 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 			return fail(err, st, FXB_ERR_UNSUPPORTED,
 			            "INTERLACEDVDIF needs one 2-bit band per thread, at most 32, without zoom bands or phase cal");
 		o.mux_threads = in.mux_threads;
+		if(in.mux_raw)
+		{
+			// raw reads: thread frames of payload / threads bytes (whole 8-byte
+			// VDIF units, so that every frame's payload words are aligned)
+			if(in.mux_threads < 1 || in.header_bytes != 32 || in.payload_bytes % in.mux_threads ||
+			   (in.payload_bytes / in.mux_threads) % 8)
+				return fail(err, st, FXB_ERR_UNSUPPORTED,
+				            "raw INTERLACEDVDIF reads need 32-byte headers and thread payloads of a multiple of 8 bytes");
+			o.mux_raw = true;
+			for(int t = 0; t < in.mux_threads; t++)
+			{
+				const int id = in.mux_thread_ids ? in.mux_thread_ids[t] : t;
+				if(id < 0 || id > 1023)
+					return fail(err, st, FXB_ERR_ARG, "bad VDIF thread id");
+				for(int q : o.mux_tids)
+					if(q == id)
+						return fail(err, st, FXB_ERR_ARG, "duplicate VDIF thread id");
+				o.mux_tids.push_back(id);
+			}
+		}
 		job.stations.push_back(o);
 	}
 	for(int b = 0; b < d->nbaseline; b++)

@@ -47,6 +47,11 @@ struct DevZoomCopy {
 	int32_t src_plan, src_row, dst_plan, dst_row, choff, nchan;
 };
 
+// raw INTERLACEDVDIF reads (DevStation::muxraw): frame slots, muxed headers
+// and the muxed stream's length and start, before the frame validity
+// (fxb_mux.cu); maxslots / maxproc bound every raw station's slots / frames
+void launch_mux_raw(const DevStation *st, DevSubintStation *sub, int S, int maxslots, int maxproc,
+                    cudaStream_t stream);
 // bandok (may be null): per frame, the bands that keep their samples
 void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8_t *valid, uint32_t *bandok,
                         int64_t valid_stride, int S, cudaStream_t stream);

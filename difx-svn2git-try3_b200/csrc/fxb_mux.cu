@@ -24,10 +24,12 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 
 #include "fxb_internal.h"
+#include "fxb_kernels.h"
 
 namespace fxb {
 
@@ -275,7 +277,240 @@ __global__ void k_mux_turn(const MuxArgs a, const int32_t *outidx)
 	}
 }
 
+// ---------------------------------------------------------------- raw reads inside a context
+// The same placement and headers for the stations of a context whose buffers
+// are raw reads (DevStation::muxraw), without the corner turn: the F stage
+// reads each band's samples from its thread's frame through the slot table.
+// Grids are (work, station); stations without raw reads return at once.
+
+__global__ void k_mr_init(const DevStation *__restrict__ st, DevSubintStation *__restrict__ sub)
+{
+	const int s = blockIdx.y;
+	if(!st[s].muxraw)
+		return;
+	DevSubintStation &U = sub[s];
+	const int64_t n = (int64_t)U.mux_nslot * st[s].nthr;
+	for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+		U.mux_slot[i] = -1;
+	if(blockIdx.x == 0 && threadIdx.x == 0)
+	{
+		U.mux_status[0] = 0;
+		U.mux_status[1] = 0;
+		U.mux_status[2] = U.mux_nproc;
+	}
+}
+
+// VDIFMuxer::deinterlace (datamuxer.cpp:765-846): every input frame finds its
+// slot (frames since the read's first frame) and thread; the later input
+// frame wins a slot filled twice
+__global__ void k_mr_index(const DevStation *__restrict__ st, DevSubintStation *__restrict__ sub)
+{
+	const int s = blockIdx.y;
+	const DevStation &S = st[s];
+	if(!S.muxraw)
+		return;
+	DevSubintStation &U = sub[s];
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < U.mux_nin; i += gridDim.x * blockDim.x)
+	{
+		const uint8_t *h = U.buf + (int64_t)i * S.inframebytes;
+		const int tid = (int)((hw(h, 3) >> 16) & 0x3FFu);
+		const int fbytes = (int)(hw(h, 2) & 0xFFFFFFu) * 8;
+		if(fbytes != S.inframebytes)
+		{
+			atomicCAS(U.mux_status, 0, 1);     // frame size changed
+			continue;
+		}
+		int ti = -1;
+		for(int j = 0; j < S.nthr; j++)
+			if(S.tmap[j] == tid)
+			{
+				ti = j;
+				break;
+			}
+		if(ti < 0)
+			continue;
+		int m0, s0, f0, m, sc, f;
+		frame_time(U.buf, &m0, &s0, &f0);
+		frame_time(h, &m, &sc, &f);
+		const int64_t cur = ((int64_t)(m - m0) * 86400 + sc - s0) * S.fps + f - f0;
+		if(cur < 0)
+			continue;
+		if(cur >= U.mux_nslot)
+		{
+			atomicCAS(U.mux_status, 0, 2);     // beyond the muxer's buffer
+			continue;
+		}
+		atomicMax(U.mux_slot + cur * S.nthr + ti, i);
+	}
+}
+
+__global__ void k_mr_first(const DevStation *__restrict__ st, DevSubintStation *__restrict__ sub)
+{
+	const int s = blockIdx.y;
+	const DevStation &S = st[s];
+	if(!S.muxraw)
+		return;
+	DevSubintStation &U = sub[s];
+	if(U.mux_status[0] != 0)
+		return;
+	for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < U.mux_nproc; k += gridDim.x * blockDim.x)
+	{
+		const int32_t *sl = U.mux_slot + (int64_t)k * S.nthr;
+		for(int j = 0; j < S.nthr; j++)
+			if(sl[j] >= 0)
+			{
+				atomicMin(U.mux_status + 2, k);
+				break;
+			}
+	}
+}
+
+// muxed payload word q of a complete slot (the corner turn of
+// VDIFMuxer::cornerturn_generic, datamuxer.cpp:253-274: output word
+// i nthreads + j packs, for k < spow and thread l, sample j spow + k of
+// thread l at bit (k nthreads + l) nbits)
+__device__ uint32_t mr_word(const DevStation &S, const DevSubintStation &U, const int32_t *sl, int q)
+{
+	const int nt = S.nthr, i = q / nt, j = q - i * nt;
+	const int wordsin = (S.inframebytes - 32) / 4;
+	const int spow = (32 / S.nbits) / nt;
+	const uint32_t mask = (1u << S.nbits) - 1u;
+	uint32_t word = 0u;
+	for(int l = 0; l < nt; l++)
+	{
+		const uint32_t w = (i < wordsin) ? ((const uint32_t *)(U.buf + (int64_t)sl[l] * S.inframebytes + 32))[i] : 0u;
+		for(int kk = 0; kk < spow; kk++)
+			word |= ((w >> ((j * spow + kk) * S.nbits)) & mask) << ((kk * nt + l) * S.nbits);
+	}
+	return word;
+}
+
+// header of slot k before the empty-slot step (as slot_header above)
+__device__ void mr_slot_header(const DevStation &S, const DevSubintStation &U, int k, uint32_t *o, bool *all_out,
+                               bool *any_out)
+{
+	const int32_t *sl = U.mux_slot + (int64_t)k * S.nthr;
+	bool all = true;
+	int first = -1;
+	for(int j = 0; j < S.nthr; j++)
+	{
+		if(sl[j] < 0)
+			all = false;
+		else if(first < 0)
+			first = j;
+	}
+	*all_out = all;
+	*any_out = first >= 0;
+	if(first < 0)
+		return;
+	put_header(o, (const uint32_t *)(U.buf + (int64_t)sl[all ? 0 : first] * S.inframebytes));
+	int logch = 0;
+	for(int n = S.nthr; n > 1; n /= 2)
+		logch++;
+	o[0] = (o[0] & 0x7FFFFFFFu) | (all ? 0u : 0x80000000u);
+	if(all)
+		o[2] = (o[2] & ~(0x1Fu << 24)) | ((uint32_t)logch << 24);
+	o[2] = (o[2] & ~0xFFFFFFu) | ((uint32_t)(S.framebytes / 8) & 0xFFFFFFu);
+	o[3] &= ~(0x3FFu << 16);
+}
+
+// header and first / last payload words of output frame k - k0 (slot k)
+__device__ void mr_header(const DevStation &S, const DevSubintStation &U, int k, int k0)
+{
+	uint32_t h[8];
+	bool all, any;
+	mr_slot_header(S, U, k, h, &all, &any);
+	if(!any)
+	{
+		int g = k - 1;
+		bool ga = false, gy = false;
+		while(true)
+		{
+			mr_slot_header(S, U, g, h, &ga, &gy);
+			if(gy)
+				break;
+			g--;
+		}
+		h[0] |= 0x80000000u;
+		uint32_t fr = h[1] & 0xFFFFFFu;
+		uint32_t secs = h[0] & 0x3FFFFFFFu;
+		for(int step = 0; step < k - g; step++)
+		{
+			fr = (fr + 1u) & 0xFFFFFFu;
+			if((int)fr == S.fps)
+			{
+				fr = 0u;
+				secs = (secs + 1u) & 0x3FFFFFFFu;
+			}
+		}
+		h[0] = (h[0] & 0xC0000000u) | secs;
+		h[1] = (h[1] & ~0xFFFFFFu) | fr;
+	}
+	uint32_t *o = U.mux_hdr + (int64_t)(k - k0) * 16;
+	put_header(o, h);
+	const int words = S.payload / 4;
+	const int32_t *sl = U.mux_slot + (int64_t)k * S.nthr;
+	o[8] = all ? mr_word(S, U, sl, 0) : 0u;
+	o[9] = all ? mr_word(S, U, sl, 1) : 0u;
+	o[10] = all ? mr_word(S, U, sl, words - 2) : 0u;
+	o[11] = all ? mr_word(S, U, sl, words - 1) : 0u;
+}
+
+// VDIFMuxer::multiplex headers (datamuxer.cpp:680-763) of output frame
+// k - k0 for slot k, with the muxed payload's first and last 64-bit words of
+// complete slots (what the frame-validity check reads)
+__global__ void k_mr_headers(const DevStation *__restrict__ st, DevSubintStation *__restrict__ sub)
+{
+	const int s = blockIdx.y;
+	const DevStation &S = st[s];
+	if(!S.muxraw)
+		return;
+	const DevSubintStation &U = sub[s];
+	if(U.mux_status[0] != 0)
+		return;
+	const int k0 = U.mux_status[2];
+	for(int k = k0 + blockIdx.x * blockDim.x + threadIdx.x; k < U.mux_nproc; k += gridDim.x * blockDim.x)
+		mr_header(S, U, k, k0);
+}
+
+
+// the muxed stream's length and start: leading empty slots are dropped, so
+// the stream starts k0 frames after the read's first frame
+__global__ void k_mr_fix(const DevStation *__restrict__ st, DevSubintStation *__restrict__ sub, int S)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if(s >= S || !st[s].muxraw)
+		return;
+	DevSubintStation &U = sub[s];
+	if(U.mux_status[0] != 0)
+	{
+		U.nbytes = 0;                            // the reference aborts on such a read
+		U.mux_k0 = 0;
+		return;
+	}
+	const int k0 = U.mux_status[2];
+	U.mux_k0 = k0;
+	U.nbytes = (int64_t)(U.mux_nproc - k0) * st[s].framebytes;
+	const int64_t ns = (int64_t)U.datans + ((int64_t)k0 * 1000000000LL) / st[s].fps;
+	U.datasec += (int32_t)(ns / 1000000000LL);
+	U.datans = (int32_t)(ns % 1000000000LL);
+}
+
 }  // namespace
+
+void launch_mux_raw(const DevStation *st, DevSubintStation *sub, int S, int maxslots, int maxproc,
+                    cudaStream_t stream)
+{
+	// fixed grids (grid-stride loops), so that a captured graph fits any read
+	(void)maxslots;
+	(void)maxproc;
+	const dim3 g(32, S);
+	k_mr_init<<<g, 256, 0, stream>>>(st, sub);
+	k_mr_index<<<g, 256, 0, stream>>>(st, sub);
+	k_mr_first<<<g, 256, 0, stream>>>(st, sub);
+	k_mr_headers<<<g, 128, 0, stream>>>(st, sub);
+	k_mr_fix<<<(S + 63) / 64, 64, 0, stream>>>(st, sub, S);
+}
 
 fxb_status vdif_mux(const uint8_t *dev_in, int64_t inbytes, int32_t nthreads, const int32_t *thread_ids,
                     int32_t inframebytes, int32_t fps, int32_t nbits, uint8_t *dev_out, int64_t outcap,

@@ -67,6 +67,11 @@ class Station:
     # us, phase offset degrees, LO offset Hz)): the datastream table's
     # "CLK OFFSET n (us)" = offset[:delta[:phase]] and "FREQ OFFSET n (Hz)"
     freq_corr: dict = dataclasses.field(default_factory=dict)
+    # INTERLACEDVDIF: the buffers are the raw reads (the threads' own frames,
+    # placed and read inside the F stage) rather than the muxer's output;
+    # thread id of each band's thread (empty: 0, 1, ..)
+    mux_raw: bool = False
+    mux_thread_ids: List[int] = dataclasses.field(default_factory=list)
 
     def band_corr(self, b: int) -> Tuple[float, float, float, float]:
         """(clock us, clock delta us, phase deg, LO offset Hz) of band b's frequency."""

@@ -38,7 +38,8 @@ class FxbStation(ctypes.Structure):
                 ("band_clock_us", ctypes.POINTER(ctypes.c_double)),
                 ("band_clock_delta_us", ctypes.POINTER(ctypes.c_double)),
                 ("band_phase_deg", ctypes.POINTER(ctypes.c_double)),
-                ("band_lo_offset_hz", ctypes.POINTER(ctypes.c_double))]
+                ("band_lo_offset_hz", ctypes.POINTER(ctypes.c_double)),
+                ("mux_raw", ctypes.c_int32), ("mux_thread_ids", ctypes.POINTER(ctypes.c_int32))]
 
 
 class FxbBaseline(ctypes.Structure):
@@ -79,10 +80,16 @@ class DescHolder:
                     arr = (ctypes.c_double * s.nband)(*[s.band_corr(k)[q] for k in range(s.nband)])
                     self.keep.append(arr)
                     corr[q] = ctypes.cast(arr, ctypes.POINTER(ctypes.c_double))
+            tids = None
+            if s.mux_threads and s.mux_thread_ids:
+                arr = (ctypes.c_int32 * s.mux_threads)(*s.mux_thread_ids)
+                self.keep.append(arr)
+                tids = ctypes.cast(arr, ctypes.POINTER(ctypes.c_int32))
             st[i] = FxbStation(s.nbits, s.payload_bytes, s.header_bytes, s.nband,
                                ctypes.cast(bf, ctypes.POINTER(ctypes.c_int32)), ctypes.cast(bp, ctypes.c_char_p),
                                nz, s.mux_threads, ctypes.cast(zf, ctypes.POINTER(ctypes.c_int32)),
-                               ctypes.cast(zp, ctypes.c_char_p), s.pcal_interval_mhz, s.pcal_base_mhz, *corr)
+                               ctypes.cast(zp, ctypes.c_char_p), s.pcal_interval_mhz, s.pcal_base_mhz, *corr,
+                               1 if s.mux_raw else 0, tids)
         bl = (FxbBaseline * len(job.baselines))()
         for i, b in enumerate(job.baselines):
             pf, p1, p2 = [], [], []

@@ -308,3 +308,55 @@ def interlaced_vdif(nthreads: int, nframes: int, payload: int = 8000, nbits: int
                 body = rng.integers(0, 256, size=payload, dtype=np.uint8)
                 frames.append(np.concatenate([h.view(np.uint8), body]))
     return np.concatenate(frames) if frames else np.zeros(0, dtype=np.uint8)
+
+
+def raw_read(job: Job, s: int, buf: np.ndarray, rng, drop_frac: float = 0.0, lead_extra: bool = False):
+    """The raw multi-thread read a DataStream would hold for station s's
+    muxed frames `buf` (one band per thread): every muxed frame split into its
+    threads' frames (thread t: band t's samples in time order, the muxed
+    header with one channel, the thread's frame size and id t), each time's
+    thread frames in a seeded random order, a fraction of thread frames left
+    out (incomplete slots), and -- with lead_extra -- a frame of a thread
+    nobody asks for one frame time earlier at the front, so that the read's
+    first slot is empty and the muxed stream starts one frame in.  Returns the
+    bytes and the number of leading frame times (0 or 1)."""
+    st = job.stations[s]
+    nt, nbits = st.mux_threads, st.nbits
+    fb = st.payload_bytes + st.header_bytes
+    tp = st.payload_bytes // nt                      # thread payload bytes
+    frames = buf.reshape(-1, fb)
+    out = []
+    lead = 0
+    if lead_extra:
+        h = frames[0, :32].copy().view(np.uint32)
+        secs, fr = int(h[0] & 0x3FFFFFFF), int(h[1] & 0xFFFFFF)
+        fps = int(round(2 * job.station_bw(s) * 1e6 / (tp * 8 // nbits)))
+        fr -= 1
+        if fr < 0:
+            fr += fps
+            secs -= 1
+        e = h.copy()
+        e[0] = (e[0] & 0xC0000000) | (secs & 0x3FFFFFFF)
+        e[1] = (e[1] & ~np.uint32(0xFFFFFF)) | np.uint32(fr)
+        e[2] = (e[2] & ~np.uint32(0x1F << 24) & ~np.uint32(0xFFFFFF)) | np.uint32((tp + 32) // 8)
+        e[3] = (e[3] & ~np.uint32(0x3FF << 16)) | np.uint32(nt << 16)      # thread id nt: not wanted
+        out.append(np.concatenate([e.view(np.uint8), rng.integers(0, 256, size=tp, dtype=np.uint8)]))
+        lead = 1
+    per_word = 32 // nbits
+    for f in frames:
+        h = f[:32].copy().view(np.uint32)
+        words = f[32:].view(np.uint32)
+        # codes[n, c]: sample n of channel c (LSB-first fields, channels fastest)
+        shifts = (np.arange(per_word, dtype=np.uint32) * nbits)
+        codes = ((words[:, None] >> shifts[None, :]) & ((1 << nbits) - 1)).reshape(-1, nt)
+        order = rng.permutation(nt)
+        for t in order:
+            if rng.random() < drop_frac:
+                continue
+            c = codes[:, t].reshape(-1, per_word).astype(np.uint32)
+            tw = np.bitwise_or.reduce(c << shifts[None, :], axis=1).astype(np.uint32)
+            th = h.copy()
+            th[2] = (th[2] & ~np.uint32(0x1F << 24) & ~np.uint32(0xFFFFFF)) | np.uint32((tp + 32) // 8)
+            th[3] = (th[3] & ~np.uint32(0x3FF << 16)) | np.uint32(t << 16)
+            out.append(np.concatenate([th.view(np.uint8), tw.view(np.uint8)]))
+    return np.concatenate(out), lead

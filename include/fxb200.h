@@ -117,6 +117,17 @@ typedef struct {
 	const double *band_clock_delta_us; /* [nband] R/L clock delta, us */
 	const double *band_phase_deg;      /* [nband] phase offset, degrees */
 	const double *band_lo_offset_hz;   /* [nband] LO offset, Hz */
+	/* INTERLACEDVDIF stations (mux_threads > 0) only.  mux_raw = 1: the buffers
+	 * passed for this station are the DataStream's raw reads -- the threads'
+	 * own frames (payload_bytes / mux_threads + header_bytes bytes each, one
+	 * band per thread) interleaved in any order -- and the context places them
+	 * and reads each band's samples from its thread's frame inside the F
+	 * stage, with no muxed copy (frame slots, output headers, validity and
+	 * dropped leading slots as VDIFMuxer, datamuxer.cpp:106-848);
+	 * datasec/datans then give the time of the buffer's first frame.
+	 * mux_raw = 0: the buffers hold the muxer's output (fxb_vdif_mux). */
+	int32_t mux_raw;
+	const int32_t *mux_thread_ids;   /* [mux_threads] VDIF thread id of band b's thread (null: 0, 1, ..) */
 } fxb_station;
 
 /* One baseline (BASELINE TABLE, configuration.cpp:1059-1120): products are

@@ -20,8 +20,14 @@ LIB = os.path.join(HERE, "_build", "libfxoracle.so")
 _lib = None
 
 
+HDR = os.path.join(os.path.dirname(HERE), "include", "fxb200.h")
+
+
 def build(force: bool = False) -> str:
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+    # the restatement reads the job description through the C ABI's structs:
+    # rebuilt when either the source or the header is newer
+    newest = max(os.path.getmtime(SRC), os.path.getmtime(HDR) if os.path.exists(HDR) else 0.0)
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         os.makedirs(os.path.dirname(LIB), exist_ok=True)
         subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", LIB, SRC, "-lm"])
     return LIB

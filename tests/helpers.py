@@ -232,3 +232,9 @@ def corr_job(order=1, clock=True, delta=True, phase=True, looff=True, seed=9, **
             lo = float(rng.uniform(-2500.0, 2500.0)) if looff else 0.0
             st.freq_corr[f] = (clk, dclk, ph, lo)
     return job
+
+
+def raw_read(job: Job, s: int, buf: np.ndarray, rng, drop_frac: float = 0.05, lead_extra: bool = True):
+    """synth.raw_read with a fraction of thread frames left out and an
+    unwanted thread's frame leading the read (see there)."""
+    return synth.raw_read(job, s, buf, rng, drop_frac=drop_frac, lead_extra=lead_extra)
