@@ -675,7 +675,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 					g.looff = js.looff[b];
 					g.corr = 1;
 				}
-				bykind[{N, g.nb}].push_back(g);
+				// raw INTERLACEDVDIF reads take their own kernel instantiation
+				bykind[{N, g.nb + (ctx->h_st[s].muxraw ? 16 : 0)}].push_back(g);
 			}
 		}
 		std::vector<FGroup> hg;
@@ -691,11 +692,12 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		{
 			FKind k;
 			memset(&k, 0, sizeof(k));
-			if(!fstage_plan(kv.first.first, kv.first.second, out, &k))
+			if(!fstage_plan(kv.first.first, kv.first.second & 15, out, &k))
 			{
 				ctx->err = "F stage: no kernel shape for FFT length " + std::to_string(kv.first.first);
 				return FXB_ERR_UNSUPPORTED;
 			}
+			k.muxraw = kv.first.second >> 4;
 			k.first = (int)hg.size();
 			k.count = (int)kv.second.size();
 			// FFT iterations per CTA: as many as still leave two CTAs per SM

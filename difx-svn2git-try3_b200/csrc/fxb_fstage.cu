@@ -292,8 +292,9 @@ struct MidPasses {
 
 }  // namespace
 
-// NV: bands of the item (values per point); TCO: tensor-core spectra out.
-template <int NV, int LOGN, bool TCO>
+// NV: bands of the item (values per point); TCO: tensor-core spectra out;
+// MUX: raw INTERLACEDVDIF reads (each band read from its thread's frame).
+template <int NV, int LOGN, bool TCO, bool MUX>
 __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstage(const FsArgs a)
 {
 	using SH = FShape<LOGN>;
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 	const int nbits = Sp->nbits;
 	// raw INTERLACEDVDIF reads: band b's samples are those of its thread's
 	// frame, found through the frame-slot table (one band per frame)
-	const bool muxraw = Sp->muxraw != 0;
+	constexpr bool muxraw = MUX;
 	const int32_t *mslot = muxraw ? a.sub[g.station].mux_slot : nullptr;
 	const int64_t mk0 = muxraw ? a.sub[g.station].mux_k0 : 0;
 	const int mnthr = Sp->nthr, minfb = Sp->inframebytes;
@@ -783,38 +784,38 @@ void make_fstage_twiddles(int N, float2 *out32)
 	}
 }
 
-template <int NV, int LOGN, bool TCO>
+template <int NV, int LOGN, bool TCO, bool MUX>
 static void launch_t(const FKind &k, const FsArgs &a, cudaStream_t stream)
 {
-	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
-	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO, MUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO, MUX>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 	const int per = k.tq * k.fpc;
 	const int nt = (a.T + per - 1) / per;
 	const dim3 grid = a.items_fast ? dim3(k.count, nt) : dim3(nt, k.count);
-	k_fstage<NV, LOGN, TCO><<<grid, k.threads, k.smem, stream>>>(a);
+	k_fstage<NV, LOGN, TCO, MUX><<<grid, k.threads, k.smem, stream>>>(a);
 }
 
-template <int NV, bool TCO>
+template <int NV, bool TCO, bool MUX>
 static void launch_n(const FKind &k, const FsArgs &a, cudaStream_t stream)
 {
 	switch(k.N)
 	{
-	case 32: launch_t<NV, 5, TCO>(k, a, stream); break;
-	case 64: launch_t<NV, 6, TCO>(k, a, stream); break;
-	case 128: launch_t<NV, 7, TCO>(k, a, stream); break;
-	case 256: launch_t<NV, 8, TCO>(k, a, stream); break;
-	case 512: launch_t<NV, 9, TCO>(k, a, stream); break;
-	case 1024: launch_t<NV, 10, TCO>(k, a, stream); break;
-	case 2048: launch_t<NV, 11, TCO>(k, a, stream); break;
+	case 32: launch_t<NV, 5, TCO, MUX>(k, a, stream); break;
+	case 64: launch_t<NV, 6, TCO, MUX>(k, a, stream); break;
+	case 128: launch_t<NV, 7, TCO, MUX>(k, a, stream); break;
+	case 256: launch_t<NV, 8, TCO, MUX>(k, a, stream); break;
+	case 512: launch_t<NV, 9, TCO, MUX>(k, a, stream); break;
+	case 1024: launch_t<NV, 10, TCO, MUX>(k, a, stream); break;
+	case 2048: launch_t<NV, 11, TCO, MUX>(k, a, stream); break;
 	default:
 		if constexpr(NV == 1)
 		{
 			if(k.N == 4096)
-				launch_t<NV, 12, TCO>(k, a, stream);
+				launch_t<NV, 12, TCO, MUX>(k, a, stream);
 			else if(k.N == 8192)
-				launch_t<NV, 13, TCO>(k, a, stream);
+				launch_t<NV, 13, TCO, MUX>(k, a, stream);
 			else if(k.N == 16384)
-				launch_t<NV, 14, TCO>(k, a, stream);
+				launch_t<NV, 14, TCO, MUX>(k, a, stream);
 		}
 		break;
 	}
@@ -829,17 +830,31 @@ void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream)
 	a.pp = k.pp;
 	a.tw = k.tw;
 	a.items_fast = k.items_fast;
-	if(k.out == 1)
+	if(k.muxraw)
+	{
+		if(k.out == 1)
+		{
+			if(k.nb == 2)
+				launch_n<2, true, true>(k, a, stream);
+			else
+				launch_n<1, true, true>(k, a, stream);
+		}
+		else if(k.nb == 2)
+			launch_n<2, false, true>(k, a, stream);
+		else
+			launch_n<1, false, true>(k, a, stream);
+	}
+	else if(k.out == 1)
 	{
 		if(k.nb == 2)
-			launch_n<2, true>(k, a, stream);
+			launch_n<2, true, false>(k, a, stream);
 		else
-			launch_n<1, true>(k, a, stream);
+			launch_n<1, true, false>(k, a, stream);
 	}
 	else if(k.nb == 2)
-		launch_n<2, false>(k, a, stream);
+		launch_n<2, false, false>(k, a, stream);
 	else
-		launch_n<1, false>(k, a, stream);
+		launch_n<1, false, false>(k, a, stream);
 }
 
 }  // namespace fxb

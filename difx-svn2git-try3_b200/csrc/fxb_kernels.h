@@ -134,6 +134,7 @@ struct FKind {
 	const int32_t *tcpairs;  // tensor-core FFT: [tcnpairs][2] FGroup indices of each work unit's two subbands
 	int32_t tcnpairs;
 	int32_t tcbpt;           // tensor-core FFT: bits per time of the stations' VDIF words
+	int32_t muxraw;          // 1: the items' stations hand over raw INTERLACEDVDIF reads
 };
 
 // Spectra of the tensor-core forms hold X 2^-kTcSpecExp (FP16 or BF16), so
