@@ -108,6 +108,7 @@ struct fxb_ctx {
 	float2 *d_core = nullptr;
 	uint8_t *d_valid = nullptr;          // frame validity [S][valid_stride], then the band masks
 	uint32_t *d_bandok = nullptr;        // [S][valid_stride] in the same allocation
+	uint8_t *d_fillok = nullptr;         // [S][valid_stride] frames without fill pattern, same allocation
 	// raw INTERLACEDVDIF reads: frame-slot tables, muxed headers and status
 	// words of those stations, carved per subint from one scratch block
 	int nraw = 0;
@@ -384,14 +385,20 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		d.payload = js.payload;
 		d.header = js.header;
 		d.nband = js.nband;
+		// a complex sample holds a real and an imaginary field (mode.cpp:51-59,
+		// 77-82, 140-143; format_vdif.c:3828-3849)
+		const int cpl = js.cplx ? 2 : 1;
+		d.cplx = js.cplx ? 1 : 0;
 		d.framebytes = js.payload + js.header;
-		d.framesamples = js.payload * 8 / (js.nbits * js.nband);
-		d.gran = 8 / (js.nband * js.nbits);
+		d.framesamples = js.payload * 8 / (js.nbits * js.nband * cpl);
+		d.gran = 8 / (js.nband * js.nbits * cpl);
 		if(d.gran <= 0) d.gran = 1;
 		d.nchan = f.nchan;
-		d.fftchannels = 2 * f.nchan;
+		d.fftchannels = js.cplx ? f.nchan : 2 * f.nchan;
 		d.asl = calcstridelength((unsigned)f.nchan);
-		d.sticky = (js.nbits == 8 && (js.nband == 2 || js.nband == 4)) ? 1 : 0;
+		// 8-bit decoders that stop advancing in a blanked frame: real 2 and 4
+		// channels (format_vdif.c:1879-1922), complex 1, 2 and 4 (:2829-2955)
+		d.sticky = (js.nbits == 8 && (js.cplx ? js.nband <= 4 : (js.nband == 2 || js.nband == 4))) ? 1 : 0;
 		d.mux = js.mux_threads > 0 ? 1 : 0;
 		if(d.mux)
 			ctx->nbm = std::max(ctx->nbm, js.nband);
@@ -411,15 +418,15 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				d.tmap[t] = js.mux_tids[t];
 			ctx->nraw++;
 		}
-		d.bpbn = (js.nband * 1 * js.nbits) / 8;
+		d.bpbn = (js.nband * 1 * js.nbits * cpl) / 8;
 		d.bpbd = 1;
 		if(d.bpbn == 0)
 		{
 			d.bpbn = 1;
-			d.bpbd = 8 / (js.nband * js.nbits);
+			d.bpbd = 8 / (js.nband * js.nbits * cpl);
 		}
 		d.bw = f.bw_mhz;
-		d.sampletime = 1.0 / (2.0 * f.bw_mhz);
+		d.sampletime = js.cplx ? 1.0 / f.bw_mhz : 1.0 / (2.0 * f.bw_mhz);
 		ctx->maxband = std::max(ctx->maxband, js.nband);
 		ctx->maxN = std::max(ctx->maxN, d.fftchannels);
 	}
@@ -651,6 +658,10 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				g.nb = b1 >= 0 ? 2 : 1;
 				g.lsb = job.freqs[f].lower_sideband;
 				g.lofreq = job.freqs[f].freq_mhz;
+				// complex lower sideband: the effective LO is at negative
+				// frequency (mode.cpp:899-903)
+				if(js.cplx && g.lsb)
+					g.lofreq = -g.lofreq;
 				if(js.has_corr)
 				{
 					// the phase offset rotates the non-R band of the frequency's
@@ -675,8 +686,9 @@ static fxb_status setup_device(fxb_ctx *ctx)
 					g.looff = js.looff[b];
 					g.corr = 1;
 				}
-				// raw INTERLACEDVDIF reads take their own kernel instantiation
-				bykind[{N, g.nb + (ctx->h_st[s].muxraw ? 16 : 0)}].push_back(g);
+				// raw INTERLACEDVDIF reads and complex sampling take their own
+				// kernel instantiations
+				bykind[{N, g.nb + (ctx->h_st[s].muxraw ? 16 : 0) + (ctx->h_st[s].cplx ? 32 : 0)}].push_back(g);
 			}
 		}
 		std::vector<FGroup> hg;
@@ -697,7 +709,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				ctx->err = "F stage: no kernel shape for FFT length " + std::to_string(kv.first.first);
 				return FXB_ERR_UNSUPPORTED;
 			}
-			k.muxraw = kv.first.second >> 4;
+			k.muxraw = (kv.first.second >> 4) & 1;
+			k.cplx = (kv.first.second >> 5) & 1;
 			k.first = (int)hg.size();
 			k.count = (int)kv.second.size();
 			// FFT iterations per CTA: as many as still leave two CTAs per SM
@@ -717,7 +730,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				for(const FGroup &gg : kv.second)
 					any_lsb = any_lsb || gg.lsb;
 				const char *env = getenv("FXB_TC_FFT");
-				const bool allow = !(env && env[0] == '0') && ctx->nbm == 0;   // no EDV4 band blanking there
+				// no EDV4 band blanking and no complex sampling there
+				const bool allow = !(env && env[0] == '0') && ctx->nbm == 0 && !k.cplx;
 				std::vector<int32_t> pairs;
 				int bpt = 0;
 				if(allow && fstage_tc_eligible(k.N, job.fringe_rot_order, any_lsb) &&
@@ -1035,8 +1049,9 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 			ctx->d_valid = nullptr;
 		}
 		const size_t vbytes = ((size_t)need * ctx->S + 15) / 16 * 16;
-		CK(ctx, pool_alloc(ctx, (void **)&ctx->d_valid, vbytes + sizeof(uint32_t) * need * ctx->S, ctx->stream));
+		CK(ctx, pool_alloc(ctx, (void **)&ctx->d_valid, 2 * vbytes + sizeof(uint32_t) * need * ctx->S, ctx->stream));
 		ctx->d_bandok = (uint32_t *)(ctx->d_valid + vbytes);
+		ctx->d_fillok = ctx->d_valid + vbytes + sizeof(uint32_t) * need * ctx->S;
 		ctx->valid_stride = need;
 	}
 
@@ -1172,9 +1187,9 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, st);
 	if(ctx->nraw)
 		launch_mux_raw(ctx->d_st, sl.d_sub, ctx->S, 0, 0, st);
-	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->d_bandok, ctx->valid_stride, ctx->S, st);
+	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->d_bandok, ctx->valid_stride, ctx->S, st, ctx->d_fillok);
 	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->d_bandok, ctx->valid_stride,
-	                  ctx->S, ctx->T, job.fringe_rot_order, ctx->d_params, ctx->d_pbw, ctx->nbm, st);
+	                  ctx->S, ctx->T, job.fringe_rot_order, ctx->d_params, ctx->d_pbw, ctx->nbm, st, ctx->d_fillok);
 	cudaEventRecordWithFlags(sl.tev[1], st, evf);
 	{
 		FsArgs fa;
@@ -1185,6 +1200,7 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 		fa.plans = ctx->d_plans;
 		fa.valid = ctx->d_valid;
 		fa.bandok = ctx->nbm ? ctx->d_bandok : nullptr;
+		fa.fillok = ctx->d_fillok;
 		fa.valid_stride = ctx->valid_stride;
 		fa.params = ctx->d_params;
 		fa.maxN = ctx->maxN;

@@ -57,7 +57,8 @@ __device__ __forceinline__ uint32_t edv4_bands(const DevStation &S, const DevSub
 }
 
 __global__ void k_frame_valid(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
-                              uint8_t *__restrict__ valid, uint32_t *__restrict__ bandok, int64_t valid_stride)
+                              uint8_t *__restrict__ valid, uint32_t *__restrict__ bandok, int64_t valid_stride,
+                              uint8_t *__restrict__ fillok)
 {
 	const int s = blockIdx.y;
 	const DevStation &S = st[s];
@@ -66,7 +67,7 @@ __global__ void k_frame_valid(const DevStation *__restrict__ st, const DevSubint
 	const uint64_t FILL = 0x1122334411223344ULL;
 	for(int64_t fr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; fr < valid_stride; fr += (int64_t)gridDim.x * blockDim.x)
 	{
-		uint8_t v = 0;
+		uint8_t v = 0, nofill = 0;
 		// raw INTERLACEDVDIF reads: the muxed frame's header and first and last
 		// payload words as the placement kernels wrote them
 		const uint8_t *f = S.muxraw ? (const uint8_t *)(U.mux_hdr + fr * 16) : U.buf + fr * S.framebytes;
@@ -86,8 +87,11 @@ __global__ void k_frame_valid(const DevStation *__restrict__ st, const DevSubint
 				last = *(const uint64_t *)(f + S.header + (S.payload / 8 - 1) * 8);
 			}
 			v = (w2 != 0) && !((w0 >> 31) & 1) && first != FILL && last != FILL;
+			nofill = first != FILL && last != FILL;
 		}
 		valid[s * valid_stride + fr] = v;
+		if(fillok)
+			fillok[s * valid_stride + fr] = nofill;
 		if(bandok)
 			bandok[s * valid_stride + fr] = (v && S.mux) ? edv4_bands(S, U, f) : 0xFFFFFFFFu;
 	}
@@ -100,6 +104,8 @@ __device__ bool delay_interpolator(const DevStation &S, int blockspersend, int s
 	double offsettime = (double)sec + ((double)ns) / 1000000000.0;
 	double polyoffset = -S.poly0;
 	double timespan = blockspersend * 2 * S.nchan * S.sampletime / 1e6;
+	if(S.cplx)
+		timespan /= 2;        // mode.cpp:1546-1547
 	if(S.npoly <= 0)
 		return false;
 	int scansample = (int)((offsettime + polyoffset) / (double)S.interval);
@@ -175,7 +181,8 @@ __device__ inline bool flag_valid(const int32_t *vf, int i)
 __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
                              const int32_t *__restrict__ validflags, int nflagint, const uint8_t *__restrict__ valid,
                              const uint32_t *__restrict__ bandok, int64_t valid_stride, int T, int order,
-                             FftParam *__restrict__ out, float *__restrict__ pbw, int nbm)
+                             FftParam *__restrict__ out, float *__restrict__ pbw, int nbm,
+                             const uint8_t *__restrict__ fillok)
 {
 	const int s = blockIdx.y;
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -255,7 +262,10 @@ __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintS
 			int64_t a = fr * S.framesamples, b = a + S.framesamples;
 			if(a < g0) a = g0;
 			if(b > g1) b = g1;
-			bool v = fr < valid_stride && valid[(int64_t)s * valid_stride + fr];
+			// complex data: the unpack's first frame is checked for fill
+			// pattern only (mark5_stream_unpacker.c:189, a second blanker call)
+			bool v = fr < valid_stride && ((S.cplx && fillok && fr == f0) ? fillok[(int64_t)s * valid_stride + fr] != 0
+			                                                                : valid[(int64_t)s * valid_stride + fr] != 0);
 			if(S.sticky && !v && !blanked)
 			{
 				blanked = true;
@@ -310,7 +320,10 @@ __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintS
 		for(int k = 0; k < 32 && k < nwf; k++)
 		{
 			const int64_t fr = fa + k;
-			if(fr < valid_stride && valid[(int64_t)s * valid_stride + fr])
+			const bool vk = fr < valid_stride &&
+			                ((S.cplx && fillok && k == 0) ? fillok[(int64_t)s * valid_stride + fr] != 0
+			                                              : valid[(int64_t)s * valid_stride + fr] != 0);
+			if(vk)
 				m |= 1u << k;
 		}
 		p.fmask = m;
@@ -351,10 +364,10 @@ __global__ void k_fft_params(const DevStation *__restrict__ st, const DevSubintS
 }
 
 void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8_t *valid, uint32_t *bandok,
-                        int64_t valid_stride, int S, cudaStream_t stream)
+                        int64_t valid_stride, int S, cudaStream_t stream, uint8_t *fillok)
 {
 	dim3 grid((unsigned)((valid_stride + 255) / 256 < 64 ? (valid_stride + 255) / 256 : 64), S);
-	k_frame_valid<<<grid, 256, 0, stream>>>(st, sub, valid, bandok, valid_stride);
+	k_frame_valid<<<grid, 256, 0, stream>>>(st, sub, valid, bandok, valid_stride, fillok);
 }
 
 void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, cudaStream_t stream)
@@ -364,11 +377,11 @@ void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, in
 
 void launch_fft_params(const DevStation *st, const DevSubintStation *sub, const int32_t *validflags, int nflagint,
                        const uint8_t *valid, const uint32_t *bandok, int64_t valid_stride, int S, int T, int order,
-                       FftParam *out, float *pbw, int nbm, cudaStream_t stream)
+                       FftParam *out, float *pbw, int nbm, cudaStream_t stream, const uint8_t *fillok)
 {
 	dim3 grid((T + 127) / 128, S);
 	k_fft_params<<<grid, 128, 0, stream>>>(st, sub, validflags, nflagint, valid, bandok, valid_stride, T, order, out,
-	                                       pbw, nbm);
+	                                       pbw, nbm, fillok);
 }
 
 }  // namespace fxb

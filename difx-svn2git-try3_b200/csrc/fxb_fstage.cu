@@ -293,8 +293,11 @@ struct MidPasses {
 }  // namespace
 
 // NV: bands of the item (values per point); TCO: tensor-core spectra out;
-// MUX: raw INTERLACEDVDIF reads (each band read from its thread's frame).
-template <int NV, int LOGN, bool TCO, bool MUX>
+// VAR 1: raw INTERLACEDVDIF reads (each band read from its thread's frame);
+// VAR 2: complex sampling (nchan-point complex FFT: every bin a channel of
+// the upper sideband, or bin 0 and the conjugated mirror of the rest for the
+// lower sideband, mode.cpp:1182-1234).
+template <int NV, int LOGN, bool TCO, int VAR>
 __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstage(const FsArgs a)
 {
 	using SH = FShape<LOGN>;
@@ -311,7 +314,8 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 	const int tchunk = a.items_fast ? blockIdx.y : blockIdx.x;
 	const FGroup g = a.groups[a.first + item];
 	const DevStation *Sp = a.st + g.station;
-	constexpr int nchan = N / 2;
+	constexpr bool MUX = VAR == 1, CPLX = VAR == 2;
+	constexpr int nchan = CPLX ? N : N / 2;
 	const uint32_t fs = (uint32_t)Sp->framesamples;
 	const int nbits = Sp->nbits;
 	// raw INTERLACEDVDIF reads: band b's samples are those of its thread's
@@ -320,7 +324,9 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 	const int32_t *mslot = muxraw ? a.sub[g.station].mux_slot : nullptr;
 	const int64_t mk0 = muxraw ? a.sub[g.station].mux_k0 : 0;
 	const int mnthr = Sp->nthr, minfb = Sp->inframebytes;
-	const uint32_t bpt = muxraw ? (uint32_t)nbits : (uint32_t)(Sp->nband * nbits);
+	// complex samples: real then imaginary field of nbits per band and time
+	constexpr uint32_t cpl = CPLX ? 2u : 1u;
+	const uint32_t bpt = muxraw ? (uint32_t)nbits : (uint32_t)(Sp->nband * nbits) * cpl;
 	const int header = Sp->header, framebytes = Sp->framebytes, asl = Sp->asl;
 	const double bw = Sp->bw;
 	const uint8_t *buf = a.sub[g.station].buf;
@@ -338,9 +344,10 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 	const double lo = g.lofreq;
 	const float ph0 = g.phase[0], ph1 = g.phase[1];     // phase-offset rotation of each band (turns)
 	const int row0 = g.row[0], row1 = g.row[1];
-	const uint32_t boff0 = muxraw ? 0u : (uint32_t)(g.band[0] * nbits), boff1 = muxraw ? 0u : (uint32_t)(g.band[1] * nbits);
+	const uint32_t boff0 = muxraw ? 0u : (uint32_t)(g.band[0] * nbits) * cpl,
+	               boff1 = muxraw ? 0u : (uint32_t)(g.band[1] * nbits) * cpl;
 	const bool oneword = !muxraw && bpt <= 32;       // all bands of a sample time in one 32-bit word
-	const bool pair4 = NV == 2 && nbits == 2 && oneword && boff1 == boff0 + 2;
+	const bool pair4 = !CPLX && NV == 2 && nbits == 2 && oneword && boff1 == boff0 + 2;
 	const int order = a.order;
 	constexpr float osc = 1.0f / (float)(1 << kTcSpecExp);
 	const bool h16 = a.h16 != 0;
@@ -429,7 +436,10 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 			// validity of the window's frames, one bit per frame relative to fa
 			const uint32_t nwf = (c.so + (uint32_t)N - 1) / fs + 1;
 			const int64_t fr = (int64_t)c.fa + lane;
-			const bool v = (c.flags & 1) && (uint32_t)lane < nwf && fr < a.valid_stride && vrow[fr] != 0;
+			// complex data: the unpack's first frame is checked for fill pattern
+			// only (mark5_stream_unpacker.c:189)
+			const uint8_t *vsrc = (CPLX && lane == 0 && a.fillok) ? a.fillok + (int64_t)g.station * a.valid_stride : vrow;
+			const bool v = (c.flags & 1) && (uint32_t)lane < nwf && fr < a.valid_stride && vsrc[fr] != 0;
 			c.fmask = __ballot_sync(0xffffffffu, v);
 			if(nwf <= 32)
 				c.flags |= 2;
@@ -541,7 +551,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 				for(int r = 0; r < 8; r++)
 				{
 					const int n = b + r * (N / 8);
-					float v0 = 0.0f, v1 = 0.0f;
+					float v0 = 0.0f, v1 = 0.0f, u0 = 0.0f, u1 = 0.0f;     // u: imaginary parts (complex sampling)
 					if((pk[r] >> 16) & 1u)
 					{
 						const uint32_t w0 = raw0[r] >> (pk[r] & 31u);
@@ -554,10 +564,14 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 						else
 						{
 							v0 = nbits == 2 ? level2(w0 & 3u) : lut8[w0 & 255u];
+							if constexpr(CPLX)
+								u0 = nbits == 2 ? level2((w0 >> 2) & 3u) : lut8[(w0 >> 8) & 255u];
 							if(NV == 2)
 							{
 								const uint32_t w1 = (oneword ? raw0[r] : raw1[r]) >> ((pk[r] >> 8) & 31u);
 								v1 = nbits == 2 ? level2(w1 & 3u) : lut8[w1 & 255u];
+								if constexpr(CPLX)
+									u1 = nbits == 2 ? level2((w1 >> 2) & 3u) : lut8[(w1 >> 8) & 255u];
 							}
 						}
 						if(blank)
@@ -566,9 +580,9 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 							// (blank_vdif_EDV4, format_vdif.c:4699-4780)
 							const uint32_t bo = a.bandok[(int64_t)g.station * a.valid_stride + fa + (so + (uint32_t)n) / fs];
 							if(!((bo >> g.band[0]) & 1u))
-								v0 = 0.0f;
+								v0 = u0 = 0.0f;
 							if(g.band[1] >= 0 && !((bo >> g.band[1]) & 1u))
-								v1 = 0.0f;
+								v1 = u1 = 0.0f;
 						}
 					}
 					float sn = 0.0f, cs = 1.0f;
@@ -588,9 +602,18 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 						ph -= rintf(ph);
 						__sincosf(-6.283185307179586f * ph, &sn, &cs);
 					}
-					x[0][r] = cf{v0 * cs, v0 * sn};
-					if constexpr(NV == 2)
-						x[1][r] = cf{v1 * cs, v1 * sn};
+					if constexpr(CPLX)
+					{
+						x[0][r] = cf{v0 * cs - u0 * sn, v0 * sn + u0 * cs};
+						if constexpr(NV == 2)
+							x[1][r] = cf{v1 * cs - u1 * sn, v1 * sn + u1 * cs};
+					}
+					else
+					{
+						x[0][r] = cf{v0 * cs, v0 * sn};
+						if constexpr(NV == 2)
+							x[1][r] = cf{v1 * cs, v1 * sn};
+					}
 				}
 #pragma unroll
 				for(int j = 0; j < NV; j++)
@@ -646,7 +669,23 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 					const int k = q + sL * r;
 					int c, ce;
 					float cj = 1.0f;
-					if(!lsb)
+					if constexpr(CPLX)
+					{
+						// every bin is a channel; the lower sideband keeps bin 0 and
+						// mirrors and conjugates the rest (mode.cpp:1217-1226)
+						if(!lsb)
+						{
+							c = k;
+							ce = k;
+						}
+						else
+						{
+							c = k == 0 ? 0 : N - k;
+							ce = c - nchan;
+							cj = k == 0 ? 1.0f : -1.0f;
+						}
+					}
+					else if(!lsb)
 					{
 						if(r >= RL / 2)
 							continue;                  // bins >= nchan
@@ -784,41 +823,57 @@ void make_fstage_twiddles(int N, float2 *out32)
 	}
 }
 
-template <int NV, int LOGN, bool TCO, bool MUX>
+template <int NV, int LOGN, bool TCO, int VAR>
 static void launch_t(const FKind &k, const FsArgs &a, cudaStream_t stream)
 {
-	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO, MUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
-	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO, MUX>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+	cudaFuncSetAttribute(k_fstage<NV, LOGN, TCO, VAR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 	const int per = k.tq * k.fpc;
 	const int nt = (a.T + per - 1) / per;
 	const dim3 grid = a.items_fast ? dim3(k.count, nt) : dim3(nt, k.count);
-	k_fstage<NV, LOGN, TCO, MUX><<<grid, k.threads, k.smem, stream>>>(a);
+	k_fstage<NV, LOGN, TCO, VAR><<<grid, k.threads, k.smem, stream>>>(a);
 }
 
-template <int NV, bool TCO, bool MUX>
+template <int NV, bool TCO, int VAR>
 static void launch_n(const FKind &k, const FsArgs &a, cudaStream_t stream)
 {
 	switch(k.N)
 	{
-	case 32: launch_t<NV, 5, TCO, MUX>(k, a, stream); break;
-	case 64: launch_t<NV, 6, TCO, MUX>(k, a, stream); break;
-	case 128: launch_t<NV, 7, TCO, MUX>(k, a, stream); break;
-	case 256: launch_t<NV, 8, TCO, MUX>(k, a, stream); break;
-	case 512: launch_t<NV, 9, TCO, MUX>(k, a, stream); break;
-	case 1024: launch_t<NV, 10, TCO, MUX>(k, a, stream); break;
-	case 2048: launch_t<NV, 11, TCO, MUX>(k, a, stream); break;
+	case 32: launch_t<NV, 5, TCO, VAR>(k, a, stream); break;
+	case 64: launch_t<NV, 6, TCO, VAR>(k, a, stream); break;
+	case 128: launch_t<NV, 7, TCO, VAR>(k, a, stream); break;
+	case 256: launch_t<NV, 8, TCO, VAR>(k, a, stream); break;
+	case 512: launch_t<NV, 9, TCO, VAR>(k, a, stream); break;
+	case 1024: launch_t<NV, 10, TCO, VAR>(k, a, stream); break;
+	case 2048: launch_t<NV, 11, TCO, VAR>(k, a, stream); break;
 	default:
 		if constexpr(NV == 1)
 		{
 			if(k.N == 4096)
-				launch_t<NV, 12, TCO, MUX>(k, a, stream);
+				launch_t<NV, 12, TCO, VAR>(k, a, stream);
 			else if(k.N == 8192)
-				launch_t<NV, 13, TCO, MUX>(k, a, stream);
+				launch_t<NV, 13, TCO, VAR>(k, a, stream);
 			else if(k.N == 16384)
-				launch_t<NV, 14, TCO, MUX>(k, a, stream);
+				launch_t<NV, 14, TCO, VAR>(k, a, stream);
 		}
 		break;
 	}
+}
+
+template <int VAR>
+static void launch_var(const FKind &k, const FsArgs &a, cudaStream_t stream)
+{
+	if(k.out == 1)
+	{
+		if(k.nb == 2)
+			launch_n<2, true, VAR>(k, a, stream);
+		else
+			launch_n<1, true, VAR>(k, a, stream);
+	}
+	else if(k.nb == 2)
+		launch_n<2, false, VAR>(k, a, stream);
+	else
+		launch_n<1, false, VAR>(k, a, stream);
 }
 
 void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream)
@@ -831,30 +886,11 @@ void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream)
 	a.tw = k.tw;
 	a.items_fast = k.items_fast;
 	if(k.muxraw)
-	{
-		if(k.out == 1)
-		{
-			if(k.nb == 2)
-				launch_n<2, true, true>(k, a, stream);
-			else
-				launch_n<1, true, true>(k, a, stream);
-		}
-		else if(k.nb == 2)
-			launch_n<2, false, true>(k, a, stream);
-		else
-			launch_n<1, false, true>(k, a, stream);
-	}
-	else if(k.out == 1)
-	{
-		if(k.nb == 2)
-			launch_n<2, true, false>(k, a, stream);
-		else
-			launch_n<1, true, false>(k, a, stream);
-	}
-	else if(k.nb == 2)
-		launch_n<2, false, false>(k, a, stream);
+		launch_var<1>(k, a, stream);
+	else if(k.cplx)
+		launch_var<2>(k, a, stream);
 	else
-		launch_n<1, false, false>(k, a, stream);
+		launch_var<0>(k, a, stream);
 }
 
 }  // namespace fxb

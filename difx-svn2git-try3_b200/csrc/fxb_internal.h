@@ -52,6 +52,8 @@ struct DevStation {
 	// raw INTERLACEDVDIF reads (muxraw): the threads' frames, one band each;
 	// the geometry above is the muxed stream's
 	int32_t muxraw, nthr, inframebytes, fps;
+	int32_t cplx;           // complex sampling: nchan-point complex FFT, real and imaginary fields per sample
+	int32_t pad_;
 	int32_t tmap[32];       // VDIF thread id of each band's thread
 	double bw;              // MHz
 	double sampletime;      // us
@@ -104,6 +106,7 @@ struct Job {
 		float pcal_interval = 0.0f, pcal_base = 0.0f;   // phase-cal comb (MHz), float as the reference
 		int mux_threads = 0;                           // INTERLACEDVDIF: per-band data weights
 		bool mux_raw = false;                          // buffers are raw reads, de-interleaved in the F stage
+		bool cplx = false;                             // complex (single-sideband) sampling
 		std::vector<int> mux_tids;                     // raw reads: VDIF thread id of each band's thread
 		// per band, of its recorded frequency: clock offset and R/L delta (us),
 		// phase offset (degrees), LO offset (Hz); has_corr: any of them nonzero

@@ -317,6 +317,28 @@ bool build_job(const fxb_job_desc *d, Job &job, std::string &err, fxb_status &st
 			return fail(err, st, FXB_ERR_UNSUPPORTED,
 			            "INTERLACEDVDIF needs one 2-bit band per thread, at most 32, without zoom bands or phase cal");
 		o.mux_threads = in.mux_threads;
+		if(in.complex_sampling)
+		{
+			// single-sideband complex sampling (mode.cpp:51-59, 889-905, 1155-1234);
+			// 1-channel 2-bit complex data unpack in pairs of samples, whose edge
+			// erasure Mk5Mode applies to the real arrays (mk5mode.cpp:129-147)
+			if(in.complex_sampling != 1)
+				return fail(err, st, FXB_ERR_ARG, "bad complex sampling kind");
+			if(d->fringe_rot_order == 0)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "post-F fringe rotation of complex data (mode.cpp:1159-1162)");
+			if((in.nbits == 2 && in.nband < 2) || (in.nbits == 8 && in.nband > 4) || in.mux_threads > 0 ||
+			   in.nzoom > 0 || o.pcal_interval > 0.0f || f0.nchan < 32)
+				return fail(err, st, FXB_ERR_UNSUPPORTED,
+				            "complex sampling: 2-bit with 2..64 or 8-bit with 1..4 channels of at least 32 channels each, "
+				            "without zoom bands, phase cal or INTERLACEDVDIF");
+			if(((int64_t)in.payload_bytes * 8) % (2 * in.nbits * in.nband))
+				return fail(err, st, FXB_ERR_ARG, "payload must hold whole complex samples");
+			// an FFT window within 32 frames (the F stage's per-window frame mask)
+			const int64_t fsamp = (int64_t)in.payload_bytes * 8 / (2 * in.nbits * in.nband);
+			if((f0.nchan + fsamp - 1) / fsamp + 1 > 32)
+				return fail(err, st, FXB_ERR_UNSUPPORTED, "complex sampling: an FFT window spans more than 32 frames");
+			o.cplx = true;
+		}
 		if(in.mux_raw)
 		{
 			// raw reads: thread frames of payload / threads bytes (whole 8-byte

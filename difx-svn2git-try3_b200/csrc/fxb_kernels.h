@@ -53,13 +53,15 @@ struct DevZoomCopy {
 void launch_mux_raw(const DevStation *st, DevSubintStation *sub, int S, int maxslots, int maxproc,
                     cudaStream_t stream);
 // bandok (may be null): per frame, the bands that keep their samples
+// fillok (may be null): per frame, no fill pattern (the only check that the
+// first frame of a complex unpack window gets)
 void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8_t *valid, uint32_t *bandok,
-                        int64_t valid_stride, int S, cudaStream_t stream);
+                        int64_t valid_stride, int S, cudaStream_t stream, uint8_t *fillok = nullptr);
 // the subint time is read from sub[s].subsec / subns
 void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, cudaStream_t stream);
 void launch_fft_params(const DevStation *st, const DevSubintStation *sub, const int32_t *validflags, int nflagint,
                        const uint8_t *valid, const uint32_t *bandok, int64_t valid_stride, int S, int T, int order,
-                       FftParam *out, float *pbw, int nbm, cudaStream_t stream);
+                       FftParam *out, float *pbw, int nbm, cudaStream_t stream, const uint8_t *fillok = nullptr);
 
 // Fused unpack -> fringe rotation -> FFT -> fractional-sample correction.
 // One CTA per (station, FFT); writes FP32 spectra into spec.  Returns the
@@ -135,6 +137,7 @@ struct FKind {
 	int32_t tcnpairs;
 	int32_t tcbpt;           // tensor-core FFT: bits per time of the stations' VDIF words
 	int32_t muxraw;          // 1: the items' stations hand over raw INTERLACEDVDIF reads
+	int32_t cplx;            // 1: the items' stations sample complex (N = nchan points)
 };
 
 // Spectra of the tensor-core forms hold X 2^-kTcSpecExp (FP16 or BF16), so
@@ -150,6 +153,7 @@ struct FsArgs {
 	const DevFreqPlan *plans;
 	const uint8_t *valid;
 	const uint32_t *bandok;       // per frame: bands that keep their samples (null: all)
+	const uint8_t *fillok;        // per frame: no fill pattern (complex data: the window's first frame)
 	int64_t valid_stride;
 	const FftParam *params;
 	const void *tw;          // set from FKind::tw by launch_fstage_kind

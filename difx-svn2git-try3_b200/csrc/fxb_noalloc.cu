@@ -95,7 +95,7 @@ extern "C" FXB_API fxb_status fxb_station_fstage_noalloc(const fxb_freq *freqs, 
 	const fxb_station &st = *station;
 	// INTERLACEDVDIF stations need per-band weights and EDV4 band blanking,
 	// whose per-frame band masks do not fit the fixed scratch array
-	if(st.mux_threads != 0)
+	if(st.mux_threads != 0 || st.complex_sampling != 0)
 		return FXB_ERR_UNSUPPORTED;
 	// per-band clock, phase and LO offsets are applied by the context path's
 	// F stages only

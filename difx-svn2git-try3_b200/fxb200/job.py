@@ -72,6 +72,9 @@ class Station:
     # thread id of each band's thread (empty: 0, 1, ..)
     mux_raw: bool = False
     mux_thread_ids: List[int] = dataclasses.field(default_factory=list)
+    # complex (single-sideband) sampling: bw complex samples per second per
+    # band, real and imaginary fields side by side (DATA SAMPLING COMPLEX)
+    complex_sampling: bool = False
 
     def band_corr(self, b: int) -> Tuple[float, float, float, float]:
         """(clock us, clock delta us, phase deg, LO offset Hz) of band b's frequency."""
@@ -132,11 +135,13 @@ class Job:
         return int(round(n))
 
     def samples_per_sec(self, s: int) -> int:
-        return int(round(2e6 * self.station_bw(s)))
+        k = 1 if self.stations[s].complex_sampling else 2
+        return int(round(k * 1e6 * self.station_bw(s)))
 
     def frame_samples(self, s: int) -> int:
         st = self.stations[s]
-        return st.payload_bytes * 8 // (st.nbits * st.nband)
+        k = 2 if st.complex_sampling else 1
+        return st.payload_bytes * 8 // (st.nbits * st.nband * k)
 
     def frame_bytes(self, s: int) -> int:
         st = self.stations[s]
@@ -147,11 +152,13 @@ class Job:
 
     def mbps(self, s: int) -> int:
         st = self.stations[s]
-        return int(round(self.samples_per_sec(s) * st.nbits * st.nband / 1e6))
+        k = 2 if st.complex_sampling else 1
+        return int(round(self.samples_per_sec(s) * st.nbits * st.nband * k / 1e6))
 
     def vdif_format(self, s: int) -> str:
         st = self.stations[s]
-        return "VDIF_%d-%d-%d-%d" % (st.payload_bytes, self.mbps(s), st.nband, st.nbits)
+        return "VDIF%s_%d-%d-%d-%d" % ("C" if st.complex_sampling else "", st.payload_bytes, self.mbps(s), st.nband,
+                                        st.nbits)
 
     def max_products(self) -> int:
         return max(len(pp) for b in self.baselines for _, pp in b.products)

@@ -39,7 +39,8 @@ class FxbStation(ctypes.Structure):
                 ("band_clock_delta_us", ctypes.POINTER(ctypes.c_double)),
                 ("band_phase_deg", ctypes.POINTER(ctypes.c_double)),
                 ("band_lo_offset_hz", ctypes.POINTER(ctypes.c_double)),
-                ("mux_raw", ctypes.c_int32), ("mux_thread_ids", ctypes.POINTER(ctypes.c_int32))]
+                ("mux_raw", ctypes.c_int32), ("mux_thread_ids", ctypes.POINTER(ctypes.c_int32)),
+                ("complex_sampling", ctypes.c_int32)]
 
 
 class FxbBaseline(ctypes.Structure):
@@ -89,7 +90,7 @@ class DescHolder:
                                ctypes.cast(bf, ctypes.POINTER(ctypes.c_int32)), ctypes.cast(bp, ctypes.c_char_p),
                                nz, s.mux_threads, ctypes.cast(zf, ctypes.POINTER(ctypes.c_int32)),
                                ctypes.cast(zp, ctypes.c_char_p), s.pcal_interval_mhz, s.pcal_base_mhz, *corr,
-                               1 if s.mux_raw else 0, tids)
+                               1 if s.mux_raw else 0, tids, 1 if s.complex_sampling else 0)
         bl = (FxbBaseline * len(job.baselines))()
         for i, b in enumerate(job.baselines):
             pf, p1, p2 = [], [], []

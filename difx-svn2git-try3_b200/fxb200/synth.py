@@ -86,10 +86,32 @@ def _band_block(job: Job, s: int, band: int, blk: int, rho: float, seed: int) ->
     return np.sqrt(rho) * skyd + np.sqrt(1.0 - rho) * noise
 
 
+def _band_block_complex(job: Job, s: int, band: int, blk: int, rho: float, seed: int) -> np.ndarray:
+    """Complex voltage samples of one band for one BLOCK (complex sampling at
+    bw samples per second): a complex sky signal per (frequency, polarisation)
+    whose baseband frequency f in [0, bw) is sky frequency LO + f, delayed per
+    station (phase exp(-2 pi i (LO + f) tau)), plus complex station noise."""
+    st = job.stations[s]
+    f, pol = st.bands[band]
+    fr = job.freqs[f]
+    fs = fr.bw_mhz                             # M complex samples / s
+    r = _rng("csky", seed, f, pol, blk)
+    sky = (r.standard_normal(BLOCK) + 1j * r.standard_normal(BLOCK)) / np.sqrt(2.0)
+    spec = np.fft.fft(sky)
+    fb = np.arange(BLOCK) * (fs / BLOCK)       # baseband frequency in [0, bw), MHz
+    tmid = (blk + 0.5) * BLOCK / (fs * 1e6)
+    tau = float(station_delay_us(job, s, tmid))
+    skyd = np.fft.ifft(spec * np.exp(-2j * np.pi * (fr.freq_mhz + fb) * tau))
+    q = _rng("cnoise", seed, s, band, blk)
+    noise = (q.standard_normal(BLOCK) + 1j * q.standard_normal(BLOCK)) / np.sqrt(2.0)
+    return np.sqrt(rho) * skyd + np.sqrt(1.0 - rho) * noise
+
+
 def band_samples(job: Job, s: int, band: int, n0: int, n: int, rho: float, seed: int) -> np.ndarray:
     """Voltage samples [n0, n0+n) (job-relative sample index) of one band."""
     b0, b1 = n0 // BLOCK, (n0 + n - 1) // BLOCK
-    parts = [_band_block(job, s, band, b, rho, seed) for b in range(b0, b1 + 1)]
+    blockfn = _band_block_complex if job.stations[s].complex_sampling else _band_block
+    parts = [blockfn(job, s, band, b, rho, seed) for b in range(b0, b1 + 1)]
     x = np.concatenate(parts)
     off = n0 - b0 * BLOCK
     return x[off:off + n]
@@ -129,7 +151,7 @@ def vdif_header(job: Job, s: int, frame_global: int, invalid: bool = False, stat
     w[1] = (fnum & 0xFFFFFF)
     log2ch = int(np.log2(st.nband)) if st.nband & (st.nband - 1) == 0 else 0
     w[2] = (1 << 29) | (log2ch << 24) | ((job.frame_bytes(s) // 8) & 0xFFFFFF)
-    w[3] = ((st.nbits - 1) << 26) | (station_id & 0xFFFF)
+    w[3] = ((st.nbits - 1) << 26) | (station_id & 0xFFFF) | ((1 << 31) if st.complex_sampling else 0)
     return w.view(np.uint8)
 
 
@@ -148,7 +170,14 @@ def gen_station_frames(job: Job, s: int, frame0: int, nframes: int, rho: float, 
     fil = set(fill)
     n0 = frame0 * fsamp
     n = nframes * fsamp
-    codes = np.stack([quantise(band_samples(job, s, b, n0, n, rho, seed), st.nbits) for b in range(st.nband)])
+    if st.complex_sampling:
+        # real and imaginary fields side by side, per (time, channel)
+        # (the complex VDIF decoders' order, format_vdif.c:2369-2410, 2868-2907)
+        # (rows 2 c + part: the payload's field order is (time, channel, part))
+        x = [band_samples(job, s, b, n0, n, rho, seed) for b in range(st.nband)]
+        codes = np.stack([q for v in x for q in (quantise(v.real, st.nbits), quantise(v.imag, st.nbits))])
+    else:
+        codes = np.stack([quantise(band_samples(job, s, b, n0, n, rho, seed), st.nbits) for b in range(st.nband)])
     out = np.empty(nframes * fb, dtype=np.uint8)
     for k in range(nframes):
         g = frame0 + k

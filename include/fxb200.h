@@ -128,6 +128,16 @@ typedef struct {
 	 * mux_raw = 0: the buffers hold the muxer's output (fxb_vdif_mux). */
 	int32_t mux_raw;
 	const int32_t *mux_thread_ids;   /* [mux_threads] VDIF thread id of band b's thread (null: 0, 1, ..) */
+	/* DATA SAMPLING: 0 = REAL; 1 = COMPLEX (single sideband, "COMPLEX",
+	 * "COMPLEX_IQ" or "COMPLEX_SSB", configuration.cpp:1545-1556): bw complex
+	 * samples per second per band, each the real then the imaginary field of
+	 * nbits (VDIFC decoders, format_vdif.c:2369-2410, 2868-2907); the FFT is a
+	 * complex one of nchan points whose bins are the channels (upper sideband),
+	 * or bin 0 then the conjugates of bins nchan - 1 .. 1 (lower sideband; the
+	 * fringe rotation then uses -LO), mode.cpp:889-905, 1182-1234.  Fringe
+	 * rotation order 1 or 2; 2-bit with at least 2 VDIF channels or 8-bit with
+	 * at most 4; no zoom bands, phase cal or INTERLACEDVDIF. */
+	int32_t complex_sampling;
 } fxb_station;
 
 /* One baseline (BASELINE TABLE, configuration.cpp:1059-1120): products are

@@ -101,7 +101,7 @@ def write_job_files(job: Job, outdir: str, name: str = "job",
             s.append(_kv("DATA FORMAT", "VDIF"))
             s.append(_kv("QUANTISATION BITS", st.nbits))
             s.append(_kv("DATA FRAME SIZE", st.payload_bytes + st.header_bytes))
-        s.append(_kv("DATA SAMPLING", "REAL"))
+        s.append(_kv("DATA SAMPLING", "COMPLEX" if st.complex_sampling else "REAL"))
         s.append(_kv("DATA SOURCE", "FILE"))
         s.append(_kv("FILTERBANK USED", "FALSE"))
         s.append(_kv("PHASE CAL INT (MHZ)", ("%.6f" % st.pcal_interval_mhz) if st.pcal_interval_mhz else 0))

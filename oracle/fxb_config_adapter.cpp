@@ -21,7 +21,27 @@ struct ModeFields : Mode
 	static const double *phase(const Mode *m) { return m->*(&ModeFields::recordedfreqphaseoffset); }
 	static const double *looff(const Mode *m) { return m->*(&ModeFields::recordedfreqlooffsets); }
 	static int order(const Mode *m) { return m->*(&ModeFields::fringerotationorder); }
+	static int dsb(const Mode *m) { return m->*(&ModeFields::usedouble); }
+	static u8 *&workbuf(Mode *m) { return m->*(&ModeFields::fftbuffer); }
 };
+
+}  // namespace
+
+void fxb_delete_mode(Mode *m)
+{
+#if defined(ARCH) && defined(GENERIC) && (ARCH == GENERIC)
+	if(m && ModeFields::order(m) == 0)
+		ModeFields::workbuf(m) = 0;
+#endif
+	delete m;
+}
+
+namespace {
+
+void delete_mode(Mode *m, int)
+{
+	fxb_delete_mode(m);
+}
 
 }  // namespace
 
@@ -55,11 +75,7 @@ bool fxb_desc_from_configuration(Configuration *c, int ci, int32_t xmac_kind, Fx
 			err = "datastream " + std::to_string(ds) + " is not VDIF";
 			return false;
 		}
-		if(c->getDSampling(ci, ds) != Configuration::REAL)
-		{
-			err = "datastream " + std::to_string(ds) + " is complex sampled";
-			return false;
-		}
+		s.complex_sampling = c->getDSampling(ci, ds) == Configuration::COMPLEX ? 1 : 0;
 		const int header = fmt == Configuration::VDIFL ? 16 : 32;
 		s.nbits = c->getDNumBits(ci, ds);
 		s.header_bytes = header;
@@ -99,11 +115,17 @@ bool fxb_desc_from_configuration(Configuration *c, int ci, int32_t xmac_kind, Fx
 		Mode *m = c->getMode(ci, ds);
 		if(!m || !m->initialisedOK())
 		{
-			delete m;
+			delete_mode(m, m ? ModeFields::order(m) : 1);
 			err = "no Mode for datastream " + std::to_string(ds);
 			return false;
 		}
 		order = ModeFields::order(m);
+		if(s.complex_sampling && ModeFields::dsb(m))
+		{
+			delete_mode(m, order);
+			err = "datastream " + std::to_string(ds) + " is complex double-sideband sampled";
+			return false;
+		}
 		const double *src[4] = {ModeFields::clock(m), ModeFields::delta(m), ModeFields::phase(m), ModeFields::looff(m)};
 		const double **dst[4] = {&s.band_clock_us, &s.band_clock_delta_us, &s.band_phase_deg, &s.band_lo_offset_hz};
 		for(int q = 0; q < 4; q++)
@@ -114,7 +136,7 @@ bool fxb_desc_from_configuration(Configuration *c, int ci, int32_t xmac_kind, Fx
 			d.corr.push_back(v);
 			*dst[q] = d.corr.back().data();
 		}
-		delete m;
+		delete_mode(m, order);
 		d.stations.push_back(s);
 	}
 	const int nbl = c->getNumBaselines();

@@ -41,7 +41,7 @@ struct FxbConfigDesc
  * datastream's Mode, configuration.cpp:954-1016), the baseline products
  * (configuration.cpp:1059-1120), the subint, fringe-rotation order and
  * autocorrelation flag.  Returns false, with err set, for a configuration
- * outside the ABI (a non-VDIF datastream, complex sampling, a filterbank). */
+ * outside the ABI (a non-VDIF datastream, complex double-sideband sampling). */
 bool fxb_desc_from_configuration(Configuration *config, int configindex, int32_t xmac_kind, FxbConfigDesc &d,
                                  std::string &err);
 
@@ -50,5 +50,14 @@ bool fxb_desc_from_configuration(Configuration *config, int configindex, int32_t
  * NaN in interp[3 ds] where the model has none.  Returns the number of
  * datastreams without one. */
 int fxb_interpolators_from_model(Configuration *config, int configindex, int scan, int sec, int ns, double *interp);
+
+/* Deletes a Mode that Configuration::getMode made.  With the FFTW build of
+ * the vector library, the real-to-complex set-up that a fringe-rotation
+ * order 0 Mode uses (architecture.h.in genericInitDFTR_f32) never assigns the
+ * work-buffer pointer it is handed, and ~Mode frees that pointer
+ * (mode.cpp:551): it is cleared first, so that ~Mode frees nothing it did
+ * not allocate. */
+class Mode;
+void fxb_delete_mode(Mode *m);
 
 #endif

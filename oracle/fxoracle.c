@@ -73,6 +73,7 @@ typedef struct fxo_job {
 	/* stations */
 	int *nbits, *payload, *header, *nband;
 	int *mux;                                         /* INTERLACEDVDIF: per-band weights */
+	int *cplx;                                        /* complex (single-sideband) sampling */
 	int **band_freq;
 	char **band_pol;
 	/* per band: clock offset and R/L delta (us), phase offset (degrees), LO
@@ -345,6 +346,74 @@ static int vdif_unpack(const uint8_t *data, int64_t nbytes, int payload, int hea
 	return nsamp - nblanksamp;
 }
 
+/* mark5_unpack_complex_with_offset for a single-thread complex VDIF stream
+ * (VDIFC decoders, format_vdif.c:2369-2690 2-bit, 2829-2955 8-bit): sample t
+ * of channel c is the real then the imaginary field q = 2 (t nchan + c), q + 1
+ * of nbits each.  out[c][o] = (re, im).  The complex 8-bit decoders of 1, 2
+ * and 4 channels do not advance inside a blanked frame: every later sample of
+ * the call is blank.  mark5_unpack_complex_with_offset runs the blanker once
+ * more after positioning on the first frame (mark5_stream_unpacker.c:189),
+ * which only looks for fill pattern: that frame's header validity (invalid
+ * bit, word 2) is not applied. */
+static int vdif_unpack_complex(const uint8_t *data, int64_t nbytes, int payload, int header, int nchan, int nbits,
+                               int64_t offsetsamples, int nsamp, float *out /* [nchan][nsamp][2] */)
+{
+	int64_t framebytes = payload + header;
+	int64_t framesamples = (int64_t)payload * 8 / (nchan * nbits * 2);
+	int sticky = (nbits == 8 && nchan <= 4);
+	int stuck = 0, nblanksamp = 0, o, c;
+	int64_t cur_frame = -1;
+	int cur_valid = 0;
+	for(o = 0; o < nsamp; o++)
+	{
+		int64_t g = offsetsamples + o;
+		int64_t fr = g / framesamples;
+		int64_t t = g % framesamples;
+		if(fr != cur_frame)
+		{
+			cur_frame = fr;
+			if((fr + 1) * framebytes > nbytes)
+				cur_valid = 0;
+			else if(o == 0)
+			{
+				uint64_t first, last;
+				const uint64_t FILL = 0x1122334411223344ULL;
+				memcpy(&first, data + fr * framebytes + header, 8);
+				memcpy(&last, data + fr * framebytes + header + (payload / 8 - 1) * 8, 8);
+				cur_valid = first != FILL && last != FILL;
+			}
+			else
+				cur_valid = frame_valid(data + fr * framebytes, header, payload);
+		}
+		if(!cur_valid)
+			stuck = sticky;
+		if(!cur_valid || stuck)
+		{
+			for(c = 0; c < nchan; c++)
+			{
+				out[2 * ((int64_t)c * nsamp + o)] = 0.0f;
+				out[2 * ((int64_t)c * nsamp + o) + 1] = 0.0f;
+			}
+			nblanksamp++;
+			continue;
+		}
+		{
+			const uint8_t *pl = data + fr * framebytes + header;
+			for(c = 0; c < nchan; c++)
+			{
+				int64_t q = 2 * (t * nchan + c), k;
+				for(k = 0; k < 2; k++)
+				{
+					int64_t bit = (q + k) * nbits;
+					int b = pl[bit >> 3];
+					out[2 * ((int64_t)c * nsamp + o) + k] = (nbits == 2) ? lut2(b >> (bit & 7)) : lut8(b);
+				}
+			}
+		}
+	}
+	return nsamp - nblanksamp;
+}
+
 /* ------------------------------------------------------------ job set-up */
 
 void fxo_destroy(fxo_job *j);
@@ -360,6 +429,7 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 	memcpy(j->freqs, d->freqs, sizeof(fxb_freq) * d->nfreq);
 	j->nbits = (int *)calloc(d->nstation, sizeof(int));
 	j->mux = (int *)calloc(d->nstation, sizeof(int));
+	j->cplx = (int *)calloc(d->nstation, sizeof(int));
 	j->payload = (int *)calloc(d->nstation, sizeof(int));
 	j->header = (int *)calloc(d->nstation, sizeof(int));
 	j->nband = (int *)calloc(d->nstation, sizeof(int));
@@ -387,6 +457,7 @@ fxo_job *fxo_create(const fxb_job_desc *d)
 		}
 		j->nbits[s] = st->nbits;
 		j->mux[s] = st->mux_threads > 0;
+		j->cplx[s] = st->complex_sampling != 0;
 		j->payload[s] = st->payload_bytes;
 		j->header[s] = st->header_bytes;
 		j->nband[s] = st->nband;
@@ -680,7 +751,9 @@ int fxo_set_delay_poly(fxo_job *j, int s, int npoly, int order, double poly0_sec
 }
 
 /* Model::calculateDelayInterpolator, order 2 (model.cpp:229-299), with the
- * timespan of Mode::setOffsets (mode.cpp:1546-1547).  Returns 0 on success,
+ * timespan of Mode::setOffsets (mode.cpp:1546-1547; complex data doubles the
+ * sample time and halves the span, so the real-data span serves both).
+ * Returns 0 on success,
  * -1 when the time lies outside the polynomials (subint torched). */
 int fxo_interpolator(const fxo_job *j, int s, int sec, int ns, double *c)
 {
@@ -802,23 +875,26 @@ static fft_info mode_process(const fxo_job *j, int s, const uint8_t *buf, int64_
 {
 	fft_info info = { 0, 0, 0.0f, 0.0 };
 	int nchan = station_nchan(j, s);
-	int fftchannels = 2 * nchan;
+	/* complex sampling (mode.cpp:51-59, 77-82, 140-143): nchan complex samples
+	 * per FFT at bw per second; a sample holds two fields */
+	const int cpl = j->cplx[s] ? 2 : 1;
+	int fftchannels = j->cplx[s] ? nchan : 2 * nchan;
 	int nb = j->nband[s];
 	double bw = station_bw(j, s);
-	double sampletime = 1.0 / (2.0 * bw);          /* microseconds */
+	double sampletime = j->cplx[s] ? 1.0 / bw : 1.0 / (2.0 * bw);    /* microseconds */
 	int nbits = j->nbits[s];
-	int gran = granularity(nb, nbits);
+	int gran = granularity(nb, nbits * cpl);
 	int samplestounpack = fftchannels + (gran > 1 ? gran : 0);
 	int unpacksamples = fftchannels;
 	/* Mode's block bookkeeping for the range check (mode.cpp:124-139):
 	 * samplesperblock = 1 for Mk5Mode */
-	int bpbn = (nb * 1 * nbits) / 8, bpbd = 1;
+	int bpbn = (nb * 1 * nbits * cpl) / 8, bpbd = 1;
 	int asl = calcstridelength(nchan);
 	double fftcentre, averagedelay, starttime, walltimesecs;
 	int nearestsample, k, b;
 	double fftstartmicrosec;
 
-	if(bpbn == 0) { bpbn = 1; bpbd = 8 / (nb * nbits); }
+	if(bpbn == 0) { bpbn = 1; bpbd = 8 / (nb * nbits * cpl); }
 	memset(spec, 0, sizeof(dcx) * nb * nchan);
 
 	if(nbytes <= 1 || invalid_subint || (((validflags[i / FLAGS_PER_INT] >> (i % FLAGS_PER_INT)) & 0x01) == 0))
@@ -848,7 +924,12 @@ static fft_info mode_process(const fxo_job *j, int s, const uint8_t *buf, int64_
 			int munged, c, t, erased = 0;
 			float good;
 			*ups = sampleoffset - (sampleoffset % gran);
-			good = (float)vdif_unpack(buf, nbytes, j->payload[s], j->header[s], nb, nbits, *ups, samplestounpack, scratch);
+			if(j->cplx[s])
+				good = (float)vdif_unpack_complex(buf, nbytes, j->payload[s], j->header[s], nb, nbits, *ups,
+				                                  samplestounpack, scratch);
+			else
+				good = (float)vdif_unpack(buf, nbytes, j->payload[s], j->header[s], nb, nbits, *ups, samplestounpack,
+				                          scratch);
 			if(gran > 1)
 			{
 				munged = sampleoffset % gran;
@@ -935,6 +1016,59 @@ static fft_info mode_process(const fxo_job *j, int s, const uint8_t *buf, int64_
 				fraclooff = fabs(looff) - (int)fabs(looff);
 				if(looff < 0) fraclooff = -fraclooff;
 				lowall = -looff * fracwalltime - (fabs(fraclooff) > (double)1e-9f ? fraclooff * intwalltime : 0.0);
+			}
+			if(j->cplx[s])
+			{
+				/* complex samples (mode.cpp:1182-1234): the rotator of the order in
+				 * use (LO negated for the lower sideband, mode.cpp:899-903), an
+				 * nchan-point complex FFT whose bins are the channels (upper
+				 * sideband) or bin 0 then the conjugates of bins nchan-1 .. 1 */
+				const double lo = lsb ? -lofreq : lofreq;
+				const double flo = (lo - (int)lo) * (double)integerdelay;
+				const float *xf = scratch + 2 * ((int64_t)b * samplestounpack + off);
+				for(n = 0; n < fftchannels; n++)
+				{
+					int kk = n / asl, jj = n % asl;
+					double xj = (double)jj / (double)fftchannels;
+					double Xk = (double)(kk * asl) / (double)fftchannels;
+					double ph;
+					if(order == 1)
+						ph = (xj * a + bb) * lo + Xk * a * lo;
+					else
+						ph = (xj * (bb + a * X1) + cc) * lo + kk * (xj * (2.0 * a * X1)) * lo
+						     + (Xk * bb + Xk * Xk * a) * lo;
+					if(j->fractionallofreq) ph += flo;
+					if(looff != 0.0)
+						ph += -looff * ((double)n * sampletime / 1e6) + lowall;
+					ph = -TWO_PI_D * (ph - floor(ph));
+					{
+						const double xr = xf[2 * n], xi = xf[2 * n + 1], cr = cos(ph), ci = sin(ph);
+						work[n].re = xr * cr - xi * ci;
+						work[n].im = xr * ci + xi * cr;
+					}
+				}
+				dfft(work, fftchannels);
+				for(c = 0; c < nchan; c++)
+				{
+					dcx v;
+					double fc, arg, cr, ci;
+					if(!lsb)
+						v = work[c];
+					else if(c == 0)
+						v = work[0];
+					else
+					{
+						v.re = work[nchan - c].re;
+						v.im = -work[nchan - c].im;
+					}
+					fc = lsb ? (double)(c - nchan) * bw / nchan : (double)c * bw / nchan;
+					arg = TWO_PI_D * fc * fseb;
+					cr = cos(arg);
+					ci = sin(arg);
+					spec[(int64_t)b * nchan + c].re = v.re * cr - v.im * ci;
+					spec[(int64_t)b * nchan + c].im = v.re * ci + v.im * cr;
+				}
+				continue;
 			}
 			if(order == 0)
 			{

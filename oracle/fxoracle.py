@@ -29,7 +29,11 @@ def build(force: bool = False) -> str:
     newest = max(os.path.getmtime(SRC), os.path.getmtime(HDR) if os.path.exists(HDR) else 0.0)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         os.makedirs(os.path.dirname(LIB), exist_ok=True)
-        subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", LIB, SRC, "-lm"])
+        # built under a private name and renamed into place, so that a
+        # concurrent test process never loads a half-written library
+        tmp = "%s.%d.tmp" % (LIB, os.getpid())
+        subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", tmp, SRC, "-lm"])
+        os.replace(tmp, LIB)
     return LIB
 
 

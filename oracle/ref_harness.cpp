@@ -404,7 +404,7 @@ void dref_close(void *h)
 	if(!j) return;
 	for(size_t t = 0; t < j->modes.size(); t++)
 		for(size_t d = 0; d < j->modes[t].size(); d++)
-			delete j->modes[t][d];
+			fxb_delete_mode(j->modes[t][d]);
 	delete j->config;
 	delete j;
 }

@@ -238,3 +238,15 @@ def raw_read(job: Job, s: int, buf: np.ndarray, rng, drop_frac: float = 0.05, le
     """synth.raw_read with a fraction of thread frames left out and an
     unwanted thread's frame leading the read (see there)."""
     return synth.raw_read(job, s, buf, rng, drop_frac=drop_frac, lead_extra=lead_extra)
+
+
+def cplx_job(lsb=False, nbits=2, nstation=3, nfreq=2, nchan=256, bw=16.0, order=1, **kw) -> Job:
+    """A full-polarisation job of complex-sampled (single-sideband) stations:
+    bw complex samples per second per band, nchan-point complex FFTs."""
+    job = full_job(nstation, [Freq(8400.0 + k * bw, bw, nchan, "L" if lsb else "U") for k in range(nfreq)],
+                   full_pol=True, subint_ns=kw.pop("subint_ns", 4_000_000), nbits=nbits, fringe_rot_order=order)
+    for st in job.stations:
+        st.complex_sampling = True
+    synth.make_delay_polys(job, seed=kw.pop("seed", 4))
+    job.validate()
+    return job

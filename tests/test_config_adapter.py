@@ -20,7 +20,7 @@ import numpy as np
 import pytest
 
 from fxb200 import native, synth
-from helpers import FP32_TOL, compare_core, corr_job, pcal_job, small_job, zoom_job
+from helpers import FP32_TOL, compare_core, corr_job, cplx_job, pcal_job, small_job, zoom_job
 
 import refcorr
 
@@ -33,6 +33,7 @@ JOBS = {
     "zoom": lambda: zoom_job(),
     "pcal": lambda: pcal_job(),
     "8bit_order2": lambda: small_job(nstation=3, nbits=8, order=2, seed=3),
+    "complex_lsb": lambda: cplx_job(lsb=True),
 }
 
 
@@ -58,7 +59,7 @@ def test_adapter_descriptor_matches_job(name):
                (b.freq_mhz, b.bw_mhz, b.nchan, b.lower_sideband, b.chans_to_avg), f
     for s in range(want.nstation):
         a, b = got.stations[s], want.stations[s]
-        for k in ("nbits", "payload_bytes", "header_bytes", "nband", "nzoom", "mux_threads"):
+        for k in ("nbits", "payload_bytes", "header_bytes", "nband", "nzoom", "mux_threads", "complex_sampling"):
             assert getattr(a, k) == getattr(b, k), (s, k)
         assert (np.float32(a.pcal_interval_mhz), np.float32(a.pcal_base_mhz)) == \
                (np.float32(b.pcal_interval_mhz), np.float32(b.pcal_base_mhz))
@@ -98,7 +99,7 @@ def test_adapter_layout_and_interpolators_match_reference(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["c0", "corrections_order1", "zoom", "pcal"])
+@pytest.mark.parametrize("name", ["c0", "corrections_order1", "zoom", "pcal", "complex_lsb"])
 def test_adapter_flow_through_product_matches_reference(name):
     job = JOBS[name]()
     ref = refcorr.RefCorrelator(job)

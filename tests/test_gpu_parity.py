@@ -189,3 +189,19 @@ def test_band_corrections(name, kw):
     got, ref, layout, n, w, wref = run_both(job, [(1, 500_000_000)])
     compare_core(job, layout, n, got, ref)
     assert np.array_equal(w, wref)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(lsb=True), dict(nbits=8, nfreq=1), dict(order=2),
+                                dict(nchan=1024, bw=32.0, subint_ns=2_048_000)])
+def test_complex_sampling(kw):
+    """Single-sideband complex sampling (nchan-point complex FFTs, VDIFC
+    decoding), with an invalid frame (the complex 8-bit decoders stop
+    advancing in it; the first frame of a complex unpack is checked for fill
+    pattern only), against the oracle pinned to the compiled reference."""
+    from helpers import cplx_job
+    job = cplx_job(**kw)
+    sec, ns = 1, 500_000_000
+    f0 = synth.subint_window(job, 0, sec, ns)[0]
+    got, ref, layout, n, w, wref = run_both(job, [(sec, ns)], invalid={0: [f0 + 2]})
+    compare_core(job, layout, n, got, ref)
+    assert np.array_equal(w, wref)

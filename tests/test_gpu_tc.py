@@ -192,3 +192,15 @@ def test_fp16_band_corrections_vs_fp64(kw):
     e = tc_errors(job, layout, n, got, ref)
     print(kw, e)
     assert_tc_gate(e)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(lsb=True, nbits=8, nfreq=1)])
+def test_fp16_complex_sampling_vs_fp64(kw):
+    """Complex-sampled stations in the tensor-core form (CUDA-core complex FFT,
+    FP16 spectra) within the relative gate."""
+    from helpers import cplx_job
+    job = cplx_job(**kw)
+    got, ref, layout, n = run_tc(job, [(0, 1_000_000), (0, 5_000_000)])
+    e = tc_errors(job, layout, n, got, ref)
+    print(kw, e)
+    assert_tc_gate(e)
