@@ -355,9 +355,10 @@ def c3_leg(args):
     smhz = sum(j.station_mhz_per_sec() for j in jobs)
     data_s = args.steps * nsub * jobs[0].subint_ns * 1e-9
 
-    def run(form, batched):
+    def run(form, batched, fused=True):
         members = [Correlator(j, xmac=form, inflight=3) for j in jobs]
         batch = Batch(members) if batched else None
+        is_fused = batch.set_fused(fused) if batched else False
         # scheduling tuned online during the warm-up subints (results unchanged)
         for m in members:
             m.autotune(2)
@@ -405,6 +406,8 @@ def c3_leg(args):
         out = {"value": smhz * data_s / (ms * 1e-3), "unit": UNIT, "rtf": data_s / (ms * 1e-3),
                "ms_per_subint": ms / nrun,
                "kernel_ms_per_subint_summed": {"prep": kern[0] / nrun, "fstage": kern[1] / nrun, "xmac": kern[2] / nrun}}
+        if batched:
+            out["fused"] = is_fused
         if tuning:
             out["tuning"] = [line for rp in tuning for line in rp.strip().split("\n") if "|" in line]
         return out
@@ -413,8 +416,10 @@ def c3_leg(args):
                        "2/8-bit), dual pol with full cross hands, 8.192 ms subints, as %d jobs" % len(jobs),
            "station_mhz": smhz, "subints_timed": args.steps * nsub,
            "l2": "inputs larger than L2 (%d MB pool cycled)" % int(sum(sum(x[1]) for mm in meta for x in mm) / 1e6)}
-    out["tc_batched_graph"] = run(args.xmac if args.xmac != "fp32" else "fp16", True)
-    out["tc_per_job"] = run(args.xmac if args.xmac != "fp32" else "fp16", False)
+    tcf = args.xmac if args.xmac != "fp32" else "fp16"
+    out["tc_batched_graph"] = run(tcf, True)
+    out["tc_batched_branches"] = run(tcf, True, fused=False)
+    out["tc_per_job"] = run(tcf, False)
     out["fp32_per_job"] = run("fp32", False)
     out["tc_batched_vs_fp32"] = out["tc_batched_graph"]["rtf"] / out["fp32_per_job"]["rtf"]
     out["note"] = "every form runs its subints as CUDA graphs (per job, or one per batch)"
@@ -848,6 +853,8 @@ def gpu_arm(args, job):
                                                    if k in serve},
             "batched_c3": None if c3 is None else {"tc_batched_vs_fp32": c3["tc_batched_vs_fp32"],
                                                    "tc_batched_rtf": c3["tc_batched_graph"]["rtf"],
+                                                   "tc_batched_fused": c3["tc_batched_graph"].get("fused"),
+                                                   "tc_batched_branches_rtf": c3["tc_batched_branches"]["rtf"],
                                                    "tc_per_job_rtf": c3["tc_per_job"]["rtf"],
                                                    "fp32_per_job_rtf": c3["fp32_per_job"]["rtf"]},
             "vdif_mux_frac": None if mux is None else mux["frac"],

@@ -131,6 +131,14 @@ struct fxb_ctx {
 	// F-stage work items (by kind) and FP32 XMAC v2 launch groups
 	FGroup *d_groups = nullptr;
 	std::vector<FKind> fkinds;
+	// the kinds of the persistent F launches and their work list (wide units
+	// first), on the host and on the device, and the launches' unit counters
+	std::vector<FsMultiKind> pkinds;
+	std::vector<FsMultiUnit> punits;
+	int32_t pnwide = 0, pnnarrow = 0;
+	FsMultiKind *d_pkinds = nullptr;
+	FsMultiUnit *d_punits = nullptr;
+	int32_t *d_pctr = nullptr;
 	void *d_specn = nullptr;             // half2 (or bf16x2) spectra of the tensor-core forms, X 2^-kTcSpecExp
 	void *d_tctab = nullptr;             // constant tables of the tensor-core FFT kernel
 	// XMAC launch groups (subbands of equal rows and channels); the
@@ -765,8 +773,53 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				CK(ctx, cudaMemcpyAsync(d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice, ctx->stream));
 				k.tw = d;
 			}
+			bool wide = false;
+			if(out == 1 && !k.tcfft && !k.muxraw && !k.cplx && fstage_multi_shape(k.N, k.nb, &wide))
+				k.persist = 1;
 			hg.insert(hg.end(), kv.second.begin(), kv.second.end());
 			ctx->fkinds.push_back(k);
+		}
+		// the persistent launches' work list: per kind tq x fpc FFT times of
+		// one item per unit, times outer and items inner
+		{
+			std::vector<FsMultiUnit> wide, narrow;
+			for(const FKind &k : ctx->fkinds)
+			{
+				if(!k.persist)
+					continue;
+				bool w = false;
+				fstage_multi_shape(k.N, k.nb, &w);
+				FsMultiKind mk;
+				memset(&mk, 0, sizeof(mk));
+				mk.tw = k.tw;
+				int logn = 0;
+				while((1 << logn) < k.N)
+					logn++;
+				mk.code = 32 * k.nb + logn;
+				mk.first = k.first;
+				mk.tq = fstage_multi_tq(k.N, k.nb, k.tq);
+				const int ki = (int)ctx->pkinds.size();
+				ctx->pkinds.push_back(mk);
+				const int per = mk.tq * k.fpc, nt = (ctx->T + per - 1) / per;
+				std::vector<FsMultiUnit> &dst = w ? wide : narrow;
+				for(int t = 0; t < nt; t++)
+					for(int it = 0; it < k.count; it++)
+						dst.push_back(FsMultiUnit{ki, it, t});
+			}
+			ctx->pnwide = (int32_t)wide.size();
+			ctx->pnnarrow = (int32_t)narrow.size();
+			ctx->punits = wide;
+			ctx->punits.insert(ctx->punits.end(), narrow.begin(), narrow.end());
+			if(!ctx->pkinds.empty())
+			{
+				CK(ctx, dalloc(ctx, &ctx->d_pkinds, ctx->pkinds.size()));
+				CK(ctx, dalloc(ctx, &ctx->d_punits, ctx->punits.size()));
+				CK(ctx, dalloc(ctx, &ctx->d_pctr, 2));
+				CK(ctx, cudaMemcpyAsync(ctx->d_pkinds, ctx->pkinds.data(), sizeof(FsMultiKind) * ctx->pkinds.size(),
+				                        cudaMemcpyHostToDevice, ctx->stream));
+				CK(ctx, cudaMemcpyAsync(ctx->d_punits, ctx->punits.data(), sizeof(FsMultiUnit) * ctx->punits.size(),
+				                        cudaMemcpyHostToDevice, ctx->stream));
+			}
 		}
 		CK(ctx, dalloc(ctx, &ctx->d_groups, std::max<size_t>(hg.size(), 1)));
 		if(!hg.empty())
@@ -1176,13 +1229,11 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 // subint time travels in the slot's records), so that the sequence can be
 // captured once per slot and replayed.  capture: the slot's four timing
 // events become event-record nodes of the graph.
-static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool capture)
+// Delay interpolators, raw-read placement, frame validity and per-FFT
+// parameters of one subint (Mode::setOffsets, Mk5Mode::unpack's checks).
+static void launch_prep(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, unsigned evf)
 {
 	const Job &job = ctx->job;
-	Tuner &tn = ctx->tune;
-	const bool tuning = !capture && tn.iter < tn.total;
-	const size_t nk = ctx->fkinds.size();
-	const unsigned evf = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
 	cudaEventRecordWithFlags(sl.tev[0], st, evf);
 	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, st);
 	if(ctx->nraw)
@@ -1191,31 +1242,55 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->d_bandok, ctx->valid_stride,
 	                  ctx->S, ctx->T, job.fringe_rot_order, ctx->d_params, ctx->d_pbw, ctx->nbm, st, ctx->d_fillok);
 	cudaEventRecordWithFlags(sl.tev[1], st, evf);
+}
+
+// The F-stage arguments of one subint (every kind but the twiddles and the
+// scheduling fields).
+static FsArgs fs_args(const fxb_ctx *ctx, const Slot &sl)
+{
+	const Job &job = ctx->job;
+	FsArgs fa;
+	memset(&fa, 0, sizeof(fa));
+	fa.st = ctx->d_st;
+	fa.sub = sl.d_sub;
+	fa.groups = ctx->d_groups;
+	fa.plans = ctx->d_plans;
+	fa.valid = ctx->d_valid;
+	fa.bandok = ctx->nbm ? ctx->d_bandok : nullptr;
+	fa.fillok = ctx->d_fillok;
+	fa.valid_stride = ctx->valid_stride;
+	fa.params = ctx->d_params;
+	fa.maxN = ctx->maxN;
+	fa.T = ctx->T;
+	fa.order = job.fringe_rot_order;
+	fa.fraclo = job.fractionallofreq ? 1 : 0;
+	fa.spec = ctx->tc ? ctx->d_specn : (void *)ctx->d_spec;
+	fa.err = ctx->d_err;
+	fa.h16 = ctx->h16 ? 1 : 0;
+	return fa;
+}
+
+static void launch_xmac_weights(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, unsigned evf, bool tuning,
+                                bool xmac = true);
+
+static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool capture)
+{
+	Tuner &tn = ctx->tune;
+	const bool tuning = !capture && tn.iter < tn.total;
+	const size_t nk = ctx->fkinds.size();
+	const unsigned evf = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
+	launch_prep(ctx, sl, st, evf);
 	{
-		FsArgs fa;
-		memset(&fa, 0, sizeof(fa));
-		fa.st = ctx->d_st;
-		fa.sub = sl.d_sub;
-		fa.groups = ctx->d_groups;
-		fa.plans = ctx->d_plans;
-		fa.valid = ctx->d_valid;
-		fa.bandok = ctx->nbm ? ctx->d_bandok : nullptr;
-		fa.fillok = ctx->d_fillok;
-		fa.valid_stride = ctx->valid_stride;
-		fa.params = ctx->d_params;
-		fa.maxN = ctx->maxN;
-		fa.T = ctx->T;
-		fa.order = job.fringe_rot_order;
-		fa.fraclo = job.fractionallofreq ? 1 : 0;
-		fa.spec = ctx->tc ? ctx->d_specn : (void *)ctx->d_spec;
-		fa.err = ctx->d_err;
-		fa.h16 = ctx->h16 ? 1 : 0;
+		const FsArgs fa = fs_args(ctx, sl);
 		for(size_t i = 0; i < nk; i++)
 		{
 			FKind k = ctx->fkinds[i];
 			if(tuning)
-			{
 				cudaEventRecord(tn.ev[i], st);
+			if(k.persist)
+				continue;
+			if(tuning)
+			{
 				if(!k.tcfft)
 				{
 					const auto &c = tn.fc[tn.iter % tn.fc.size()];
@@ -1232,9 +1307,35 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 			else
 				launch_fstage_kind(k, fa, st);
 		}
+		if(!ctx->pkinds.empty())
+		{
+			FsMultiArgs ma;
+			memset(&ma, 0, sizeof(ma));
+			ma.m[0] = fa;
+			ma.kinds = ctx->d_pkinds;
+			ma.units = ctx->d_punits;
+			ma.nwide = ctx->pnwide;
+			ma.nnarrow = ctx->pnnarrow;
+			ma.ctr = ctx->d_pctr;
+			cudaMemsetAsync(ctx->d_pctr, 0, 2 * sizeof(int32_t), st);
+			const cudaError_t le = launch_fstage_multi(ma, ctx->nsm, st);
+			if(le != cudaSuccess && ctx->launch_err == cudaSuccess)
+				ctx->launch_err = le;
+		}
 		if(tuning)
 			cudaEventRecord(tn.ev[nk], st);
 	}
+	launch_xmac_weights(ctx, sl, st, evf, tuning);
+}
+
+// Phase-cal bins and zoom gathers (after the F stage), the FP8 quantisation,
+// every XMAC group (unless xmac is false: the caller runs them) and the
+// weights of one subint.
+static void launch_xmac_weights(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, unsigned evf, bool tuning, bool xmac)
+{
+	const Job &job = ctx->job;
+	Tuner &tn = ctx->tune;
+	const size_t nk = ctx->fkinds.size();
 	for(const auto &pc : ctx->pclass)
 		launch_pcal_bin(ctx->d_pgroups + pc.first, pc.count, pc.maxbins, ctx->pchunks, pc.nbits, pc.bpt, pc.shift != 0,
 		                pc.smem, ctx->d_st, sl.d_sub, ctx->d_params, ctx->d_valid, ctx->valid_stride, ctx->T,
@@ -1253,7 +1354,7 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 		TcShape sh = g.shape;
 		if(tuning)
 			cudaEventRecord(tn.ev[nk + 1 + gi], st);
-		if(!g.xmac)
+		if(!g.xmac || !xmac)
 			continue;
 		if(tuning)
 		{
@@ -1320,7 +1421,7 @@ static void tune_collect(fxb_ctx *ctx)
 		return;
 	for(size_t i = 0; i < nk; i++)
 	{
-		if(ctx->fkinds[i].tcfft)
+		if(ctx->fkinds[i].tcfft || ctx->fkinds[i].persist)
 			continue;
 		const size_t c = std::min_element(t.fms[i].begin(), t.fms[i].end()) - t.fms[i].begin();
 		ctx->fkinds[i].tq = t.fc[c].first;
@@ -1468,10 +1569,14 @@ fxb_status fxb_tuning_report(const fxb_ctx *ctx, char *buf, size_t len, size_t *
 	for(size_t i = 0; i < ctx->fkinds.size(); i++)
 	{
 		const FKind &k = ctx->fkinds[i];
-		snprintf(line, sizeof(line), "fstage N=%d items=%d%s: %d FFT iterations per CTA, %s fastest", k.N, k.count,
-		         k.tcfft ? " tensor-core FFT" : "", k.tq, k.items_fast ? "items" : "times");
+		if(k.persist)
+			snprintf(line, sizeof(line), "fstage N=%d items=%d: persistent launch, %d FFT iterations per unit", k.N,
+			         k.count, fstage_multi_tq(k.N, k.nb, k.tq));
+		else
+			snprintf(line, sizeof(line), "fstage N=%d items=%d%s: %d FFT iterations per CTA, %s fastest", k.N, k.count,
+			         k.tcfft ? " tensor-core FFT" : "", k.tq, k.items_fast ? "items" : "times");
 		r += line;
-		if(t.done && !k.tcfft)
+		if(t.done && !k.tcfft && !k.persist)
 			for(size_t c = 0; c < t.fc.size(); c++)
 			{
 				snprintf(line, sizeof(line), "%s(%d,%s) %.4f ms", c ? ", " : " | ", t.fc[c].first,
@@ -1995,7 +2100,15 @@ struct fxb_batch {
 	std::vector<std::vector<const uint8_t *>> g_valid; // [slot][member] validity arrays captured with
 	std::vector<std::vector<int64_t>> g_stride;
 	std::vector<std::vector<int>> g_gen;
+	std::vector<int> g_fused;                         // [slot] the graph runs the fused launches
 	bool graphs = true;
+	// fused mode: the persistent F launches' work list over all members and
+	// their two unit counters
+	bool fused = true;
+	FsMultiKind *d_kinds = nullptr;
+	FsMultiUnit *d_units = nullptr;
+	int32_t nwide = 0, nnarrow = 0;
+	int32_t *d_ctr = nullptr;
 	std::string err;
 };
 
@@ -2010,6 +2123,9 @@ static void free_batch(fxb_batch *b)
 	if(b->fork) cudaEventDestroy(b->fork);
 	if(b->done) cudaEventDestroy(b->done);
 	if(b->stream) cudaStreamDestroy(b->stream);
+	if(b->d_kinds) cudaFree(b->d_kinds);
+	if(b->d_units) cudaFree(b->d_units);
+	if(b->d_ctr) cudaFree(b->d_ctr);
 	for(fxb_ctx *c : b->m)
 		c->batched = false;
 	delete b;
@@ -2025,11 +2141,144 @@ static void free_batch(fxb_batch *b)
 		}                                                                    \
 	} while(0)
 
-// capture every member's kernels for slot k as parallel branches
-static fxb_status batch_graph(fxb_batch *b, int k, const std::vector<Slot *> &slots)
+// Whether the members allow the fused launches (see fxb_batch_set_fused):
+// every F kind a tensor-core FFT kind or a persistent one.
+static bool batch_fusable(const fxb_batch *b)
+{
+	if(!b->fused || b->m.size() > (size_t)kFsMultiMembers)
+		return false;
+	for(const fxb_ctx *c : b->m)
+	{
+		if(!c->tc || c->f8 || !c->pclass.empty() || c->nzoom || c->nraw)
+			return false;
+		for(const FKind &k : c->fkinds)
+			if(!k.tcfft && !k.persist)
+				return false;
+	}
+	return true;
+}
+
+// The fused F launch's work list: the members' own lists, wide units of all
+// members first, each member's kinds renumbered.
+static fxb_status batch_fused_plan(fxb_batch *b)
+{
+	if(b->d_units)
+		return FXB_OK;
+	std::vector<FsMultiKind> kinds;
+	std::vector<FsMultiUnit> wide, narrow;
+	for(size_t i = 0; i < b->m.size(); i++)
+	{
+		const fxb_ctx *c = b->m[i];
+		const int k0 = (int)kinds.size();
+		for(FsMultiKind mk : c->pkinds)
+		{
+			mk.member = (int32_t)i;
+			kinds.push_back(mk);
+		}
+		for(int u = 0; u < (int)c->punits.size(); u++)
+		{
+			FsMultiUnit w = c->punits[u];
+			w.kind += k0;
+			(u < c->pnwide ? wide : narrow).push_back(w);
+		}
+	}
+	std::vector<FsMultiUnit> units(wide);
+	units.insert(units.end(), narrow.begin(), narrow.end());
+	BK(b, cudaMalloc(&b->d_kinds, sizeof(FsMultiKind) * std::max<size_t>(kinds.size(), 1)));
+	BK(b, cudaMalloc(&b->d_units, sizeof(FsMultiUnit) * std::max<size_t>(units.size(), 1)));
+	BK(b, cudaMalloc(&b->d_ctr, 2 * sizeof(int32_t)));
+	if(!kinds.empty())
+		BK(b, cudaMemcpy(b->d_kinds, kinds.data(), sizeof(FsMultiKind) * kinds.size(), cudaMemcpyHostToDevice));
+	if(!units.empty())
+		BK(b, cudaMemcpy(b->d_units, units.data(), sizeof(FsMultiUnit) * units.size(), cudaMemcpyHostToDevice));
+	b->nwide = (int32_t)wide.size();
+	b->nnarrow = (int32_t)narrow.size();
+	return FXB_OK;
+}
+
+// The fused launches of one subint on the batch stream: every member's
+// preparation as a branch, then one persistent F launch (and the members'
+// tensor-core FFT kinds), then every member's XMAC groups and weights as
+// branches.
+static void batch_fused_launch(fxb_batch *b, const std::vector<Slot *> &slots, bool capture)
+{
+	const unsigned evf = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
+	const size_t n = b->m.size();
+	cudaEventRecord(b->fork, b->stream);
+	for(size_t i = 0; i < n; i++)
+	{
+		fxb_ctx *c = b->m[i];
+		cudaStreamWaitEvent(c->stream, b->fork, 0);
+		launch_prep(c, *slots[i], c->stream, evf);
+	}
+	for(size_t i = 0; i < n; i++)
+	{
+		cudaEventRecord(b->join[i], b->m[i]->stream);
+		cudaStreamWaitEvent(b->stream, b->join[i], 0);
+	}
+	FsMultiArgs ma;
+	memset(&ma, 0, sizeof(ma));
+	for(size_t i = 0; i < n; i++)
+	{
+		fxb_ctx *c = b->m[i];
+		ma.m[i] = fs_args(c, *slots[i]);
+		for(const FKind &k : c->fkinds)
+			if(k.tcfft)
+			{
+				const cudaError_t le = launch_fstage_tc(k, ma.m[i], c->nsm, b->stream);
+				if(le != cudaSuccess && c->launch_err == cudaSuccess)
+					c->launch_err = le;
+			}
+	}
+	ma.kinds = b->d_kinds;
+	ma.units = b->d_units;
+	ma.nwide = b->nwide;
+	ma.nnarrow = b->nnarrow;
+	ma.ctr = b->d_ctr;
+	cudaMemsetAsync(b->d_ctr, 0, 2 * sizeof(int32_t), b->stream);
+	const cudaError_t le = launch_fstage_multi(ma, b->m[0]->nsm, b->stream);
+	if(le != cudaSuccess && b->m[0]->launch_err == cudaSuccess)
+		b->m[0]->launch_err = le;
+	cudaEventRecord(b->fork, b->stream);
+	// the members' weights beside one XMAC launch over every member's groups
+	// of the first group's rows (groups of other rows: a launch each)
+	for(size_t i = 0; i < n; i++)
+	{
+		fxb_ctx *c = b->m[i];
+		cudaStreamWaitEvent(c->stream, b->fork, 0);
+		launch_xmac_weights(c, *slots[i], c->stream, evf, false, false);
+	}
+	XMultiArgs xm;
+	memset(&xm, 0, sizeof(xm));
+	const TcShape *common = nullptr;
+	for(size_t i = 0; i < n; i++)
+	{
+		fxb_ctx *c = b->m[i];
+		for(const auto &g : c->xgroups)
+		{
+			if(!g.xmac)
+				continue;
+			if(!common)
+				common = &g.shape;
+			if(g.shape.nrow != common->nrow || g.shape.h16 != common->h16 ||
+			   !xmac_multi_add(&xm, g.tmap, g.shape, c->d_plans, g.d_idx, g.nf, c->d_acc))
+				launch_xmac_tc(g.tmap, g.shape, c->d_plans, g.d_idx, g.nf, c->nsm, c->d_err, c->d_acc, b->stream);
+		}
+	}
+	if(common)
+		launch_xmac_tc_multi(xm, *common, b->m[0]->nsm, b->m[0]->d_err, b->stream);
+	for(size_t i = 0; i < n; i++)
+	{
+		cudaEventRecord(b->join[i], b->m[i]->stream);
+		cudaStreamWaitEvent(b->stream, b->join[i], 0);
+	}
+}
+
+// capture every member's kernels for slot k (fused, or as parallel branches)
+static fxb_status batch_graph(fxb_batch *b, int k, const std::vector<Slot *> &slots, bool fused)
 {
 	const size_t n = b->m.size();
-	bool ok = b->gexec[k] != nullptr;
+	bool ok = b->gexec[k] != nullptr && b->g_fused[k] == (int)fused;
 	for(size_t i = 0; ok && i < n; i++)
 		ok = b->g_valid[k][i] == b->m[i]->d_valid && b->g_stride[k][i] == b->m[i]->valid_stride &&
 		     b->g_gen[k][i] == b->m[i]->gen;
@@ -2042,17 +2291,22 @@ static fxb_status batch_graph(fxb_batch *b, int k, const std::vector<Slot *> &sl
 	}
 	// one fork for all members, then every join: the branches are independent
 	BK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-	cudaEventRecord(b->fork, b->stream);
-	for(size_t i = 0; i < n; i++)
+	if(fused)
+		batch_fused_launch(b, slots, true);
+	else
 	{
-		fxb_ctx *c = b->m[i];
-		cudaStreamWaitEvent(c->stream, b->fork, 0);
-		launch_compute(c, *slots[i], c->stream, true);
-	}
-	for(size_t i = 0; i < n; i++)
-	{
-		cudaEventRecord(b->join[i], b->m[i]->stream);
-		cudaStreamWaitEvent(b->stream, b->join[i], 0);
+		cudaEventRecord(b->fork, b->stream);
+		for(size_t i = 0; i < n; i++)
+		{
+			fxb_ctx *c = b->m[i];
+			cudaStreamWaitEvent(c->stream, b->fork, 0);
+			launch_compute(c, *slots[i], c->stream, true);
+		}
+		for(size_t i = 0; i < n; i++)
+		{
+			cudaEventRecord(b->join[i], b->m[i]->stream);
+			cudaStreamWaitEvent(b->stream, b->join[i], 0);
+		}
 	}
 	cudaGraph_t g = nullptr;
 	cudaError_t e = cudaStreamEndCapture(b->stream, &g);
@@ -2073,6 +2327,7 @@ static fxb_status batch_graph(fxb_batch *b, int k, const std::vector<Slot *> &sl
 		b->g_stride[k][i] = b->m[i]->valid_stride;
 		b->g_gen[k][i] = b->m[i]->gen;
 	}
+	b->g_fused[k] = (int)fused;
 	return FXB_OK;
 }
 
@@ -2100,6 +2355,7 @@ fxb_batch *fxb_batch_create(fxb_ctx *const *members, int32_t n, fxb_status *stat
 	b->g_valid.assign(nslot, std::vector<const uint8_t *>(n, nullptr));
 	b->g_stride.assign(nslot, std::vector<int64_t>(n, 0));
 	b->g_gen.assign(nslot, std::vector<int>(n, -1));
+	b->g_fused.assign(nslot, -1);
 	b->join.assign(n, nullptr);
 	bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
 	          cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
@@ -2166,14 +2422,23 @@ static fxb_status batch_submit(fxb_batch *b, const fxb_member_subint *data, int3
 	bool tuning = false;
 	for(fxb_ctx *c : b->m)
 		tuning = tuning || c->tune.iter < c->tune.total;
+	const bool fused = !tuning && batch_fusable(b);
+	if(fused)
+	{
+		const fxb_status rc = batch_fused_plan(b);
+		if(rc != FXB_OK)
+			return rc;
+	}
 	if(b->graphs && !tuning)
 	{
-		const fxb_status rc = batch_graph(b, k, slots);
+		const fxb_status rc = batch_graph(b, k, slots, fused);
 		if(rc != FXB_OK)
 			return rc;
 	}
 	if(b->graphs && !tuning)
 		BK(b, cudaGraphLaunch(b->gexec[k], b->stream));
+	else if(fused)
+		batch_fused_launch(b, slots, false);
 	else
 		for(size_t i = 0; i < n; i++)
 			launch_compute(b->m[i], *slots[i], b->stream, false);
@@ -2246,6 +2511,15 @@ fxb_status fxb_batch_set_graphs(fxb_batch *b, int32_t on)
 {
 	if(!b) return FXB_ERR_ARG;
 	b->graphs = on != 0;
+	return FXB_OK;
+}
+
+fxb_status fxb_batch_set_fused(fxb_batch *b, int32_t on, int32_t *fused)
+{
+	if(!b) return FXB_ERR_ARG;
+	b->fused = on != 0;
+	if(fused)
+		*fused = batch_fusable(b) ? 1 : 0;
 	return FXB_OK;
 }
 

@@ -210,8 +210,9 @@ struct FftConst {
 // Y[q + s (8 p + r)] = y_r w_N^(r p s).  With two buffers each butterfly
 // reads, transforms and writes on its own; with one buffer all reads of the
 // pass come before any write.
-template <typename C, int NV, int LOGN, int LOGS, typename TW>
-__device__ __forceinline__ void mid_pass(int &wb, uint2 *side0, uint2 *side1, int pp, int bt, const TW *twp)
+template <typename C, int NV, int LOGN, int LOGS, typename TW, class Team>
+__device__ __forceinline__ void mid_pass(int &wb, uint2 *side0, uint2 *side1, int pp, int bt, const TW *twp,
+                                         const Team &tm)
 {
 	using SH = FShape<LOGN>;
 	constexpr int N = SH::N, KB = SH::KB, TPF = SH::TPF, PADN = SH::PADN;
@@ -261,7 +262,7 @@ __device__ __forceinline__ void mid_pass(int &wb, uint2 *side0, uint2 *side1, in
 	}
 	if(!pp)
 	{
-		__syncthreads();
+		tm.sync();
 #pragma unroll
 		for(int k = 0; k < KB; k++)
 		{
@@ -274,45 +275,71 @@ __device__ __forceinline__ void mid_pass(int &wb, uint2 *side0, uint2 *side1, in
 					sts(dst + j * PADN + xpad(q + s * (8 * p8 + r)), x[k][j][r]);
 		}
 	}
-	__syncthreads();
+	tm.sync();
 }
 
 template <typename C, int NV, int LOGN, int PS>
 struct MidPasses {
-	template <typename TW>
-	__device__ static __forceinline__ void run(int &wb, uint2 *side0, uint2 *side1, int pp, int bt, const TW *tw)
+	template <typename TW, class Team>
+	__device__ static __forceinline__ void run(int &wb, uint2 *side0, uint2 *side1, int pp, int bt, const TW *tw,
+	                                           const Team &tm)
 	{
 		if constexpr(PS < FShape<LOGN>::NMID)
 		{
-			mid_pass<C, NV, LOGN, 3 * (PS + 1)>(wb, side0, side1, pp, bt, tw + tw_offset(1 << LOGN, PS + 1));
-			MidPasses<C, NV, LOGN, PS + 1>::run(wb, side0, side1, pp, bt, tw);
+			mid_pass<C, NV, LOGN, 3 * (PS + 1)>(wb, side0, side1, pp, bt, tw + tw_offset(1 << LOGN, PS + 1), tm);
+			MidPasses<C, NV, LOGN, PS + 1>::run(wb, side0, side1, pp, bt, tw, tm);
 		}
 	}
 };
 
 }  // namespace
 
+// The threads that run one work unit: the whole CTA (barrier 0), or one
+// half of a persistent CTA (named barrier 1 + half, 256 threads).
+struct CtaTeam {
+	__device__ __forceinline__ int tid() const { return threadIdx.x; }
+	__device__ __forceinline__ int nt() const { return blockDim.x; }
+	__device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct HalfTeam {
+	int h;
+	__device__ __forceinline__ int tid() const { return threadIdx.x & 255; }
+	__device__ __forceinline__ int nt() const { return 256; }
+	__device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, 256;\n" ::"r"(1 + h) : "memory"); }
+};
+
+// Level tables of the decode: 8-bit levels (b - 128) / 3.3 computed in double
+// and rounded to float (format_vdif.c:122), and two adjacent 2-bit bands ->
+// (band0, band1) levels.
+template <class Team>
+__device__ __forceinline__ void fstage_luts(const Team &tm, bool eight, float *lut8, float2 *lut4)
+{
+	if(eight)
+		for(int i = tm.tid(); i < 256; i += tm.nt())
+			lut8[i] = (float)((i - 128) / 3.3);
+	if(tm.tid() < 16)
+		lut4[tm.tid()] = make_float2(level2(tm.tid() & 3u), level2(tm.tid() >> 2u));
+}
+
+// One work unit of the F stage: FFT times [tchunk tq FPC, +tq FPC) of work
+// item gidx (an FGroup), run by the team's FShape<LOGN>::NT threads with the
+// level tables already in shared memory, fsm the unit's exchange buffers
+// (two when pp) and fcs room for tq FPC FFT constants.
 // NV: bands of the item (values per point); TCO: tensor-core spectra out;
 // VAR 1: raw INTERLACEDVDIF reads (each band read from its thread's frame);
 // VAR 2: complex sampling (nchan-point complex FFT: every bin a channel of
 // the upper sideband, or bin 0 and the conjugated mirror of the rest for the
 // lower sideband, mode.cpp:1182-1234).
-template <int NV, int LOGN, bool TCO, int VAR>
-__global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstage(const FsArgs a)
+template <int NV, int LOGN, bool TCO, int VAR, class Team>
+__device__ __forceinline__ void fstage_unit(const FsArgs &a, const int gidx, const int tchunk, const int tq, const int pp,
+                                            const float2 *tw, uint2 *fsm, const float *lut8, const float2 *lut4,
+                                            FftConst *fcs, const Team &tm)
 {
 	using SH = FShape<LOGN>;
 	using C = cf;
 	using TW = float2;
 	constexpr int N = SH::N, KB = SH::KB, TPF = SH::TPF, FPC = SH::FPC, PADN = SH::PADN, RL = SH::RL;
-	extern __shared__ __align__(16) uint2 fsm[];
-	__shared__ float lut8[256];
-	__shared__ float2 lut4[16];            // two adjacent 2-bit bands -> (band0, band1) levels
-
-	// grid: (time chunks, items), or (items, time chunks) when the stations of a
-	// subband should run side by side (blocked tensor-core spectra)
-	const int item = a.items_fast ? blockIdx.x : blockIdx.y;
-	const int tchunk = a.items_fast ? blockIdx.y : blockIdx.x;
-	const FGroup g = a.groups[a.first + item];
+	const FGroup g = a.groups[gidx];
 	const DevStation *Sp = a.st + g.station;
 	constexpr bool MUX = VAR == 1, CPLX = VAR == 2;
 	constexpr int nchan = CPLX ? N : N / 2;
@@ -330,11 +357,10 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 	const int header = Sp->header, framebytes = Sp->framebytes, asl = Sp->asl;
 	const double bw = Sp->bw;
 	const uint8_t *buf = a.sub[g.station].buf;
-	const int slot = threadIdx.x / TPF, bt = threadIdx.x - slot * TPF;
+	const int slot = tm.tid() / TPF, bt = tm.tid() - slot * TPF;
 	uint2 *const side0 = fsm + (size_t)slot * NV * PADN;
-	uint2 *const side1 = a.pp ? side0 + (size_t)FPC * NV * PADN : side0;
+	uint2 *const side1 = pp ? side0 + (size_t)FPC * NV * PADN : side0;
 	const uint8_t *vrow = a.valid + (int64_t)g.station * a.valid_stride;
-	const TW *tw = (const TW *)a.tw;
 	const int64_t spec_off = a.plans[g.freq].spec_off;
 	const int prow = a.plans[g.freq].nrow;
 	// tensor-core form: spectra blocked [t][block][row][tcb] (tcb channels per block)
@@ -351,24 +377,14 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 	const int order = a.order;
 	constexpr float osc = 1.0f / (float)(1 << kTcSpecExp);
 	const bool h16 = a.h16 != 0;
-	if(nbits == 8)
-	{
-		// (b - 128) / 3.3 in double, rounded to float (format_vdif.c:122)
-		for(int i = threadIdx.x; i < 256; i += blockDim.x)
-			lut8[i] = (float)((i - 128) / 3.3);
-	}
-	if(threadIdx.x < 16)
-		lut4[threadIdx.x] = make_float2(level2(threadIdx.x & 3u), level2(threadIdx.x >> 2));
-	__syncthreads();
 
-	const int t0 = tchunk * a.tq * FPC;
-	const int nit = min(a.tq, (a.T - t0 + FPC - 1) / FPC);
-	// ---- constants of the CTA's FFTs (FFT f is time t0 + f), one warp per FFT
-	__shared__ FftConst fcs[kMaxTQ * FPC];
+	const int t0 = tchunk * tq * FPC;
+	const int nit = min(tq, (a.T - t0 + FPC - 1) / FPC);
+	// ---- constants of the unit's FFTs (FFT f is time t0 + f), one warp per FFT
 	{
-		const int lane = threadIdx.x & 31;
+		const int lane = tm.tid() & 31;
 		const int nfc = nit * FPC;
-		for(int f = threadIdx.x >> 5; f < nfc; f += blockDim.x >> 5)
+		for(int f = tm.tid() >> 5; f < nfc; f += tm.nt() >> 5)
 		{
 			const int t = t0 + f;
 			FftConst c;
@@ -462,7 +478,7 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 			if(lane == 0)
 				fcs[f] = c;
 		}
-		__syncthreads();
+		tm.sync();
 	}
 	int wb = 0;
 	for(int it = 0; it < nit; it++)
@@ -484,8 +500,8 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 		// butterfly b, twiddle w_N^(r b)), one butterfly at a time
 		{
 			uint2 *dst = wb ? side1 : side0;
-			if(!a.pp)
-				__syncthreads();              // the single buffer has been read by the last FFT
+			if(!pp)
+				tm.sync();                    // the single buffer has been read by the last FFT
 #pragma unroll
 			for(int k = 0; k < KB; k++)
 			{
@@ -637,10 +653,10 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 					sts2(q + 6, x[j][6], x[j][7]);
 				}
 			}
-			__syncthreads();
+			tm.sync();
 		}
 		// ---- middle radix-8 passes through shared memory
-		MidPasses<C, NV, LOGN, 0>::run(wb, side0, side1, a.pp, bt, tw);
+		MidPasses<C, NV, LOGN, 0>::run(wb, side0, side1, pp, bt, tw, tm);
 		// ---- 4. last pass, sideband selection, fractional-sample rotation, output
 		{
 			constexpr int sL = N / RL;
@@ -771,6 +787,161 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 			}
 		}
 	}
+}
+
+// One CTA per work unit.  grid: (time chunks, items), or (items, time chunks)
+// when the stations of a subband should run side by side (blocked
+// tensor-core spectra).
+template <int NV, int LOGN, bool TCO, int VAR>
+__global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstage(const FsArgs a)
+{
+	extern __shared__ __align__(16) uint2 fsm[];
+	__shared__ float lut8[256];
+	__shared__ float2 lut4[16];
+	__shared__ FftConst fcs[kMaxTQ * FShape<LOGN>::FPC];
+	const CtaTeam tm;
+	const int item = a.items_fast ? blockIdx.x : blockIdx.y;
+	const int tchunk = a.items_fast ? blockIdx.y : blockIdx.x;
+	fstage_luts(tm, a.st[a.groups[a.first + item].station].nbits == 8, lut8, lut4);
+	tm.sync();
+	fstage_unit<NV, LOGN, TCO, VAR>(a, a.first + item, tchunk, a.tq, a.pp, (const float2 *)a.tw, fsm, lut8, lut4, fcs,
+	                                tm);
+}
+
+// ---------------------------------------------------------------- persistent launches
+// Two persistent kernels take the tensor-core-form kinds of plain VDIF
+// stations (of one context or of a batch of them) from a work list: the
+// narrow one every length up to 4096 points in CTAs of 256 threads (the
+// shape of k_fstage for those lengths), the wide one 8192-point FFTs of one
+// band in CTAs of 512.  Each CTA takes a unit at a time from a counter and
+// runs it as one CTA of k_fstage would.
+constexpr size_t kNarrowSide = 36864;            // exchange buffer: 2048 points x 2 bands (or 4096 x 1), padded
+constexpr size_t kWideSmem = 73728;              // 8192 points of one band, padded
+
+template <class Team>
+__device__ __forceinline__ void narrow_unit(const FsArgs &a, const FsMultiKind &k, const FsMultiUnit &w, int pp,
+                                            uint2 *fsm, const float *lut8, const float2 *lut4, FftConst *fcs,
+                                            const Team &tm)
+{
+	const float2 *tw = (const float2 *)k.tw;
+	const int gi = k.first + w.item;
+	switch(k.code)
+	{
+#define FXB_MULTI_CASE(NV, LOGN)                                                                               \
+	case 32 * NV + LOGN:                                                                                       \
+		fstage_unit<NV, LOGN, true, 0>(a, gi, w.tchunk, k.tq, pp, tw, fsm, lut8, lut4, fcs, tm);              \
+		break;
+		FXB_MULTI_CASE(2, 5)
+		FXB_MULTI_CASE(2, 6)
+		FXB_MULTI_CASE(2, 7)
+		FXB_MULTI_CASE(2, 8)
+		FXB_MULTI_CASE(2, 9)
+		FXB_MULTI_CASE(2, 10)
+		FXB_MULTI_CASE(2, 11)
+		FXB_MULTI_CASE(1, 5)
+		FXB_MULTI_CASE(1, 6)
+		FXB_MULTI_CASE(1, 7)
+		FXB_MULTI_CASE(1, 8)
+		FXB_MULTI_CASE(1, 9)
+		FXB_MULTI_CASE(1, 10)
+		FXB_MULTI_CASE(1, 11)
+		FXB_MULTI_CASE(1, 12)
+#undef FXB_MULTI_CASE
+	default:
+		break;
+	}
+}
+
+// the next unit of this CTA (counter ctr), shared through slot
+__device__ __forceinline__ int next_unit(int32_t *ctr, int *slot)
+{
+	if(threadIdx.x == 0)
+		*slot = atomicAdd(ctr, 1);
+	__syncthreads();
+	const int u = *slot;
+	__syncthreads();
+	return u;
+}
+
+// one exchange buffer per unit (three CTAs per SM): faster than two buffers
+// at two CTAs per SM on every length measured
+__global__ void __launch_bounds__(256, 3) k_fstage_pn(const __grid_constant__ FsMultiArgs m)
+{
+	extern __shared__ __align__(16) uint2 fsm[];
+	__shared__ float lut8[256];
+	__shared__ float2 lut4[16];
+	__shared__ FftConst fcs[kFsMultiFc];
+	__shared__ int unit_s;
+	const CtaTeam cta;
+	fstage_luts(cta, true, lut8, lut4);
+	for(;;)
+	{
+		const int u = next_unit(m.ctr + 1, &unit_s);
+		if(u >= m.nnarrow)
+			break;
+		const FsMultiUnit w = m.units[m.nwide + u];
+		const FsMultiKind k = m.kinds[w.kind];
+		narrow_unit(m.m[k.member], k, w, 0, fsm, lut8, lut4, fcs, cta);
+	}
+}
+
+__global__ void __launch_bounds__(512, 2) k_fstage_pw(const __grid_constant__ FsMultiArgs m)
+{
+	extern __shared__ __align__(16) uint2 fsm[];
+	__shared__ float lut8[256];
+	__shared__ float2 lut4[16];
+	__shared__ FftConst fcs[kMaxTQ];
+	__shared__ int unit_s;
+	const CtaTeam cta;
+	fstage_luts(cta, true, lut8, lut4);
+	for(;;)
+	{
+		const int u = next_unit(m.ctr, &unit_s);
+		if(u >= m.nwide)
+			break;
+		const FsMultiUnit w = m.units[u];
+		const FsMultiKind k = m.kinds[w.kind];
+		fstage_unit<1, 13, true, 0>(m.m[k.member], k.first + w.item, w.tchunk, k.tq, 0, (const float2 *)k.tw, fsm,
+		                            lut8, lut4, fcs, cta);
+	}
+}
+
+bool fstage_multi_shape(int N, int nb, bool *wide)
+{
+	*wide = N == 8192 && nb == 1;
+	return (nb == 2 && N >= 32 && N <= 2048) || (nb == 1 && N >= 32 && N <= 8192);
+}
+
+int fstage_multi_tq(int N, int nb, int tq)
+{
+	FKind k;
+	memset(&k, 0, sizeof(k));
+	if(!fstage_plan(N, nb, 1, &k))
+		return 1;
+	const int cap = N == 8192 ? kMaxTQ : kFsMultiFc / k.fpc;
+	return tq < 1 ? 1 : (tq > cap ? cap : tq);
+}
+
+cudaError_t launch_fstage_multi(const FsMultiArgs &m, int nsm, cudaStream_t stream)
+{
+	if(m.nwide + m.nnarrow <= 0)
+		return cudaSuccess;
+	// the wide units first: they are the longest
+	if(m.nwide > 0)
+	{
+		cudaFuncSetAttribute(k_fstage_pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWideSmem);
+		cudaFuncSetAttribute(k_fstage_pw, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+		const int grid = m.nwide < 2 * nsm ? m.nwide : 2 * nsm;
+		k_fstage_pw<<<grid, 512, kWideSmem, stream>>>(m);
+	}
+	if(m.nnarrow > 0)
+	{
+		cudaFuncSetAttribute(k_fstage_pn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNarrowSide);
+		cudaFuncSetAttribute(k_fstage_pn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+		const int grid = m.nnarrow < 3 * nsm ? m.nnarrow : 3 * nsm;
+		k_fstage_pn<<<grid, 256, kNarrowSide, stream>>>(m);
+	}
+	return cudaGetLastError();
 }
 
 static int ilog2(int n)

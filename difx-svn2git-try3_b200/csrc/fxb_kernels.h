@@ -138,6 +138,7 @@ struct FKind {
 	int32_t tcbpt;           // tensor-core FFT: bits per time of the stations' VDIF words
 	int32_t muxraw;          // 1: the items' stations hand over raw INTERLACEDVDIF reads
 	int32_t cplx;            // 1: the items' stations sample complex (N = nchan points)
+	int32_t persist;         // 1: run by the persistent launches (launch_fstage_multi), not launch_fstage_kind
 };
 
 // Spectra of the tensor-core forms hold X 2^-kTcSpecExp (FP16 or BF16), so
@@ -167,6 +168,36 @@ struct FsArgs {
 
 bool fstage_plan(int N, int nb, int out, FKind *k);
 void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream);
+
+// The persistent F-stage launches over the CUDA-core kinds of tensor-core-
+// form contexts (plain VDIF stations) of one context or several: CTAs take
+// work units from a list in order, each run as one CTA of launch_fstage_kind
+// runs it (tq x fpc FFT times of one work item).  Narrow units (FFTs of up to
+// 4096 points) run in CTAs of 256 threads, wide units (8192-point FFTs of one
+// band) in CTAs of 512, one launch each.  Every tensor-core-form context runs
+// these kinds this way, alone or in a batch, so results do not depend on it.
+constexpr int kFsMultiMembers = 16;
+constexpr int kFsMultiFc = 128;          // FFT constants of one narrow unit at most (tq x fpc)
+struct FsMultiKind {
+	const void *tw;                      // twiddles of length N
+	int32_t member, code;                // context; 32 x bands per item + log2 N
+	int32_t first, tq;                   // first FGroup of the kind, FFT iterations per unit
+};
+struct FsMultiUnit {
+	int32_t kind, item, tchunk;
+};
+struct FsMultiArgs {
+	FsArgs m[kFsMultiMembers];           // per context, with its subint's staging
+	const FsMultiKind *kinds;
+	const FsMultiUnit *units;            // wide units [0, nwide), then narrow ones
+	int32_t nwide, nnarrow;
+	int32_t *ctr;                        // two counters (wide, narrow), zero before the launch
+};
+// whether a kind (FFT length N, bands per item nb) runs in the persistent
+// launches, and as a wide unit; the FFT iterations per unit for a kind's tq
+bool fstage_multi_shape(int N, int nb, bool *wide);
+int fstage_multi_tq(int N, int nb, int tq);
+cudaError_t launch_fstage_multi(const FsMultiArgs &m, int nsm, cudaStream_t stream);
 // F stage of the tensor-core form with the FFT on the tensor cores (N = 2048;
 // csrc/fxb_fstage_tc.cu).  Eligible: 2048-point FFTs, fringe rotation order
 // 1 (or 0 with upper sidebands only), 2-bit stations of 2..32 bands (all
@@ -209,6 +240,29 @@ bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf
 size_t tc_tensormap_size();
 void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf,
                     int nsm, int32_t *err, float2 *acc, cudaStream_t stream);
+// One launch over several groups (of one context or several) whose shapes
+// share rows, form and ring depths: the CTAs stride over the groups' work
+// units in turn.  Each product is added to its accumulator once per subint
+// whatever the schedule, so results equal those of a launch per group.
+constexpr int kXMultiGroups = 16;
+struct alignas(64) TmapBytes {
+	unsigned char b[128];
+};
+struct XGroupRec {
+	const DevFreqPlan *plans;
+	const int32_t *plan_idx;             // [subbands of the group] plan of each
+	float2 *acc;                         // the context's accumulators
+	int32_t nchan, nkt, nblk, unit0;     // channels, K tiles, channel blocks per subband, first unit
+};
+struct XMultiArgs {
+	TmapBytes map[kXMultiGroups];        // CUtensorMap of each group's spectra block
+	XGroupRec g[kXMultiGroups];
+	int32_t ngroups, nunits;
+};
+// appends a group (false when the launch is full)
+bool xmac_multi_add(XMultiArgs *xm, const void *tmap, const TcShape &s, const DevFreqPlan *dplans,
+                    const int32_t *plan_idx, int nf, float2 *acc);
+void launch_xmac_tc_multi(const XMultiArgs &xm, const TcShape &s, int nsm, int32_t *err, cudaStream_t stream);
 // FP8 form: per subband of the group (plan_idx[nf]), the bf16x2 spectra
 // [Tpad][nblk][nrow][CB] at spec_off -> e4m3x2 [Tpad][nblk][w8] at spec8_off,
 // scaled per (channel, input) so that the input's largest component over the

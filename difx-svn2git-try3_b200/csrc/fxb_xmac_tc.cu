@@ -45,6 +45,7 @@
 #include <cuda_fp8.h>
 #include <cuda_fp16.h>
 #include <cstdint>
+#include <cstring>
 
 #include "fxb_internal.h"
 #include "fxb_kernels.h"
@@ -195,10 +196,10 @@ __device__ __forceinline__ bool epi_sync_or(bool v)
 
 }  // namespace
 
+// the launch's common shape (every group has the same rows); the groups'
+// own extents are in XMultiArgs
 struct TcParams {
 	int32_t nrow, r2p, G, CB;       // inputs, real rows per channel (padded to 8), channels per tile, per unit
-	int32_t nchan, Tpad, nkt, nf;   // channels, padded times, K tiles, subbands in the group
-	int32_t nblk, nunits;           // channel blocks per subband, work units
 	int32_t raw_bytes, raw_stride;  // bytes per raw box, stage stride
 	int32_t nrs, nas;               // raw and operand stages in use
 	int32_t dstride, dump_off;      // floats per row of the accumulator copy, its byte offset in shared memory
@@ -210,11 +211,24 @@ struct TcParams {
 // NB: accumulator buffers per CTA.  2: 512 tensor-memory columns, the
 // epilogue of one unit overlaps the MMAs of the next, one CTA per SM; 1: 256
 // columns, two CTAs per SM overlap each other instead
+// unit u of a launch: its group, subband of the group and channel block
+struct UnitLoc {
+	int gi, fi, blk;
+};
+__device__ __forceinline__ UnitLoc locate(const XMultiArgs &xm, int u)
+{
+	int gi = 0;
+	while(gi + 1 < xm.ngroups && u >= xm.g[gi + 1].unit0)
+		gi++;
+	const int lu = u - xm.g[gi].unit0, nblk = xm.g[gi].nblk;
+	const int fi = lu / nblk;
+	return UnitLoc{gi, fi, lu - fi * nblk};
+}
+
+// Work units of every group of the launch in turn (a group's units are its
+// subbands' channel blocks), CTAs striding over them.
 template <bool F8, int NB>
-__global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_constant__ CUtensorMap tmap,
-                                                         const DevFreqPlan *__restrict__ plans,
-                                                         const int32_t *__restrict__ plan_idx, TcParams tp,
-                                                         float2 *__restrict__ acc)
+__global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_constant__ XMultiArgs xm, TcParams tp)
 {
 	extern __shared__ __align__(1024) unsigned char smem_tc[];
 	__shared__ uint64_t full_raw[kRS], empty_raw[kRS], full_a[kAS], empty_a[kAS], acc_full[NB], acc_empty[NB], mma_done;
@@ -266,7 +280,6 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 	__syncthreads();
 	asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 	const uint32_t tmem = tmem_base_s;
-	const int nkt = tp.nkt;
 	constexpr int KT = F8 ? kKT8 : kKT;
 
 	if(warp == 0)
@@ -276,9 +289,11 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 			// ---- TMA producer
 			int kk = 0;
 			bool ok = true;
-			for(int u = blockIdx.x; u < tp.nunits && ok; u += gridDim.x)
+			for(int u = blockIdx.x; u < xm.nunits && ok; u += gridDim.x)
 			{
-				const int fi = u / tp.nblk, blk = u - fi * tp.nblk;
+				const UnitLoc L = locate(xm, u);
+				const int nkt = xm.g[L.gi].nkt;
+				const CUtensorMap *map = (const CUtensorMap *)&xm.map[L.gi];
 				for(int kt = 0; kt < nkt; kt++, kk++)
 				{
 					const int s = kk % nrs;
@@ -289,7 +304,7 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 						break;
 					}
 					mbar_expect_tx(&full_raw[s], (uint32_t)tp.raw_bytes);
-					tma_load_3d(raw0 + (size_t)s * tp.raw_stride, &tmap, 0, blk, fi * tp.Tpad + kt * KT, &full_raw[s]);
+					tma_load_3d(raw0 + (size_t)s * tp.raw_stride, map, 0, L.blk, (L.fi * nkt + kt) * KT, &full_raw[s]);
 					issued_s = kk + 1;
 				}
 			}
@@ -308,8 +323,9 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 			const uint32_t idesc = (1u << 4) | ab | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 			int kk = 0, ku = 0;
 			bool ok = true;
-			for(int u = blockIdx.x; u < tp.nunits && ok; u += gridDim.x, ku++)
+			for(int u = blockIdx.x; u < xm.nunits && ok; u += gridDim.x, ku++)
 			{
+				const int nkt = xm.g[locate(xm, u).gi].nkt;
 				const int buf = ku % NB;
 				if(ku >= NB)
 				{
@@ -404,8 +420,9 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 		}
 		int kk = 0;
 		bool ok = true;
-		for(int u = blockIdx.x; u < tp.nunits && ok; u += gridDim.x)
+		for(int u = blockIdx.x; u < xm.nunits && ok; u += gridDim.x)
 		{
+			const int nkt = xm.g[locate(xm, u).gi].nkt;
 			for(int kt = 0; kt < nkt; kt++, kk++)
 			{
 				const int rs = kk % nrs, as = kk % nas;
@@ -504,15 +521,21 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 		const int et = threadIdx.x - 192;
 		const int row = 32 * lq + lane;          // accumulator row of this thread
 		const int nin = tp.nrow, ds = tp.dstride;
+		constexpr int kOB = 8;                   // outputs per thread with sources in registers
+		int srcv[kOB];
+		const int32_t *src_plan = nullptr;
+		int src_nout = -1;
 		int ku = 0;
-		for(int u = blockIdx.x; u < tp.nunits; u += gridDim.x, ku++)
+		for(int u = blockIdx.x; u < xm.nunits; u += gridDim.x, ku++)
 		{
 			const int buf = ku % NB;
-			const int fi = u / tp.nblk, blk = u - fi * tp.nblk;
-			const DevFreqPlan &P = plans[plan_idx[fi]];
+			const UnitLoc L = locate(xm, u);
+			const XGroupRec &GR = xm.g[L.gi];
+			const DevFreqPlan &P = GR.plans[GR.plan_idx[L.fi]];
+			float2 *const acc = GR.acc;
 			const int nout = P.acc_cstride;
-			const int c_first = blk * tp.CB;
-			const int ncv = min(tp.CB, tp.nchan - c_first);
+			const int c_first = L.blk * tp.CB;
+			const int ncv = min(tp.CB, GR.nchan - c_first);
 			bool bad = !mbar_wait(&acc_full[buf], (ku / NB) & 1, &fail_s);
 			if(bad)
 				fail_s = 6;
@@ -569,7 +592,58 @@ __global__ void __launch_bounds__(kThreads, 3 - NB) k_xmac_tc(const __grid_const
 			const float *isc = F8 ? P.iscale + (int64_t)c_first * nin : nullptr;   // FP8 form: [channel][input] 1 / scale
 			constexpr float unscale = (float)(1 << (2 * kTcSpecExp));
 			float2 *dst = acc + P.acc_off + (int64_t)c_first * nout;
-			for(int o = et; o < nout; o += 128)
+			// the thread's first kOB outputs: sources held in registers (read
+			// again only when the plan changes), every channel's reductions of
+			// them issued back to back
+			if(outsrc != src_plan || nout != src_nout)
+			{
+				src_plan = outsrc;
+				src_nout = nout;
+#pragma unroll
+				for(int j = 0; j < kOB; j++)
+				{
+					const int o = et + 128 * j;
+					srcv[j] = o < nout ? __ldg(outsrc + o) : -1;
+				}
+			}
+			{
+				int cln = 0;                      // cl mod nin
+				for(int cl = 0; cl < ncv; cl++)
+				{
+#pragma unroll
+					for(int j = 0; j < kOB; j++)
+					{
+						const int src = srcv[j];
+						if(src < 0)
+							continue;
+						const int a = src & 0xFF, b = (src >> 8) & 0xFF;
+						int pa = a + cln, pb = b + cln;
+						if(pa >= nin)
+							pa -= nin;
+						if(pb >= nin)
+							pb -= nin;
+						const float *r0 = dump + ((size_t)cl * 2 * nin + 2 * pa) * ds + 2 * pb, *r1 = r0 + ds;
+						const float2 x0 = *(const float2 *)r0, x1 = *(const float2 *)r1;
+						float vre = x0.x + x1.y;
+						float vim = x1.x - x0.y;
+						if constexpr(F8)
+						{
+							const float f = isc[cl * nin + a] * isc[cl * nin + b];
+							vre *= f;
+							vim *= f;
+						}
+						else
+						{
+							vre *= unscale;
+							vim *= unscale;
+						}
+						atomicAdd(dst + (int64_t)cl * nout + et + 128 * j, make_float2(vre, (src >> 16) ? -vim : vim));
+					}
+					if(++cln == nin)
+						cln = 0;
+				}
+			}
+			for(int o = et + 128 * kOB; o < nout; o += 128)
 			{
 				const int src = __ldg(outsrc + o);
 				if(src < 0)
@@ -705,23 +779,35 @@ bool tc_make_tensormap(void *map_out, const void *spec, const TcShape &s, int nf
 
 size_t tc_tensormap_size() { return sizeof(CUtensorMap); }
 
-void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf,
-                    int nsm, int32_t *err, float2 *acc, cudaStream_t stream)
+bool xmac_multi_add(XMultiArgs *xm, const void *tmap, const TcShape &s, const DevFreqPlan *dplans,
+                    const int32_t *plan_idx, int nf, float2 *acc)
 {
-	if(((uintptr_t)tmap & 63) != 0 || nf <= 0)
-		return;                      // refused by tc_make_tensormap at set-up already
+	if(xm->ngroups >= kXMultiGroups || ((uintptr_t)tmap & 63) != 0 || nf <= 0)
+		return false;
+	XGroupRec &g = xm->g[xm->ngroups];
+	memcpy(&xm->map[xm->ngroups], tmap, sizeof(CUtensorMap));
+	g.plans = dplans;
+	g.plan_idx = plan_idx;
+	g.acc = acc;
+	g.nchan = s.nchan;
+	g.nkt = s.Tpad / (s.f8 ? kKT8 : kKT);
+	g.nblk = (s.nchan + s.CB - 1) / s.CB;
+	g.unit0 = xm->nunits;
+	xm->nunits += g.nblk * nf;
+	xm->ngroups++;
+	return true;
+}
+
+void launch_xmac_tc_multi(const XMultiArgs &xm, const TcShape &s, int nsm, int32_t *err, cudaStream_t stream)
+{
+	if(xm.ngroups <= 0 || xm.nunits <= 0)
+		return;
 	TcParams tp;
 	tp.nrow = s.nrow;
 	tp.r2p = s.r2p;
 	tp.G = s.G;
 	tp.CB = s.CB;
-	tp.nchan = s.nchan;
-	tp.Tpad = s.Tpad;
-	tp.nkt = s.Tpad / (s.f8 ? kKT8 : kKT);
 	tp.rpitch = s.f8 ? s.w8 : s.nrow * s.CB;
-	tp.nf = nf;
-	tp.nblk = (s.nchan + s.CB - 1) / s.CB;
-	tp.nunits = tp.nblk * nf;
 	tp.raw_bytes = s.raw_bytes;
 	tp.raw_stride = s.raw_stride;
 	tp.nrs = s.nrs;
@@ -731,28 +817,37 @@ void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplan
 	tp.h16 = s.h16;
 	tp.err = err;
 	const int ctas = nsm * (s.nb == 1 ? 2 : 1);
-	const int grid = tp.nunits < ctas ? tp.nunits : ctas;
-	const CUtensorMap &map = *(const CUtensorMap *)tmap;
+	const int grid = xm.nunits < ctas ? xm.nunits : ctas;
 	if(s.f8 && s.nb == 1)
 	{
 		cudaFuncSetAttribute(k_xmac_tc<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-		k_xmac_tc<true, 1><<<grid, kThreads, s.smem, stream>>>(map, dplans, plan_idx, tp, acc);
+		k_xmac_tc<true, 1><<<grid, kThreads, s.smem, stream>>>(xm, tp);
 	}
 	else if(s.f8)
 	{
 		cudaFuncSetAttribute(k_xmac_tc<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-		k_xmac_tc<true, 2><<<grid, kThreads, s.smem, stream>>>(map, dplans, plan_idx, tp, acc);
+		k_xmac_tc<true, 2><<<grid, kThreads, s.smem, stream>>>(xm, tp);
 	}
 	else if(s.nb == 1)
 	{
 		cudaFuncSetAttribute(k_xmac_tc<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-		k_xmac_tc<false, 1><<<grid, kThreads, s.smem, stream>>>(map, dplans, plan_idx, tp, acc);
+		k_xmac_tc<false, 1><<<grid, kThreads, s.smem, stream>>>(xm, tp);
 	}
 	else
 	{
 		cudaFuncSetAttribute(k_xmac_tc<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-		k_xmac_tc<false, 2><<<grid, kThreads, s.smem, stream>>>(map, dplans, plan_idx, tp, acc);
+		k_xmac_tc<false, 2><<<grid, kThreads, s.smem, stream>>>(xm, tp);
 	}
+}
+
+void launch_xmac_tc(const void *tmap, const TcShape &s, const DevFreqPlan *dplans, const int32_t *plan_idx, int nf,
+                    int nsm, int32_t *err, float2 *acc, cudaStream_t stream)
+{
+	XMultiArgs xm;
+	memset(&xm, 0, sizeof(xm));
+	if(!xmac_multi_add(&xm, tmap, s, dplans, plan_idx, nf, acc))
+		return;                      // refused by tc_make_tensormap at set-up already
+	launch_xmac_tc_multi(xm, s, nsm, err, stream);
 }
 
 // ---------------------------------------------------------------- FP8 quantisation

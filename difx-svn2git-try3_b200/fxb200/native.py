@@ -237,6 +237,8 @@ def lib():
     L.fxb_batch_submit_device.restype = ctypes.c_int
     L.fxb_batch_sync.argtypes = [vp]
     L.fxb_batch_set_graphs.argtypes = [vp, i32]
+    L.fxb_batch_set_fused.argtypes = [vp, i32, ctypes.POINTER(i32)]
+    L.fxb_batch_set_fused.restype = i32
     for name in ("fxb_batch_submit", "fxb_batch_sync", "fxb_batch_set_graphs"):
         getattr(L, name).restype = ctypes.c_int
     L.fxb_batch_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
@@ -507,6 +509,14 @@ class Batch:
 
     def set_graphs(self, on: bool = True):
         self._check(lib().fxb_batch_set_graphs(self.b, 1 if on else 0), "batch_set_graphs")
+
+    def set_fused(self, on: bool = True) -> bool:
+        """Fused launches (one persistent F launch and one XMAC launch for
+        all members) where the members allow them; returns whether the next
+        subints run fused."""
+        f = ctypes.c_int32(0)
+        self._check(lib().fxb_batch_set_fused(self.b, 1 if on else 0, ctypes.byref(f)), "batch_set_fused")
+        return bool(f.value)
 
     def autotune(self, rounds: int = 2):
         self._check(lib().fxb_batch_autotune(self.b, rounds), "batch_autotune")

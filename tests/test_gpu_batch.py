@@ -4,7 +4,8 @@ A context's subints replayed as per-slot CUDA graphs give exactly the result
 of launching the kernels one by one.  A batch of contexts with uneven
 subband shapes (width, channels, bits), run as one graph launch per subint,
 gives every member exactly the result it has alone, matches the FP64 oracle,
-and keeps doing so after a reset."""
+and keeps doing so after a reset; so does the fused form (one persistent F
+launch and one XMAC launch over all members)."""
 import numpy as np
 import pytest
 
@@ -80,6 +81,51 @@ def test_batch_members_match_each_job_alone(xmac):
     for g, a, r in zip(got, again, alone):
         assert np.array_equal(g, r)
         assert np.array_equal(a, r)
+
+
+# beside SHAPES: 8192-point FFTs (whole-CTA units of the persistent F launch)
+# and 2-bit 2048-point FFTs (the tensor-core FFT kernel)
+FUSED_SHAPES = SHAPES + [(4.0, 4096, 8), (16.0, 1024, 2)]
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_fused_batch_matches_each_job_alone(fused):
+    # one persistent F launch and one XMAC launch for all members, or every
+    # member as its own graph branch: either way each member's result is the
+    # one it has alone, bit for bit
+    jobs = []
+    for k, (bw, nchan, bits) in enumerate(FUSED_SHAPES):
+        job = full_job(3, [Freq(8400.0 + 100.0 * k, bw, nchan)], full_pol=True, subint_ns=SUBINT_NS, nbits=bits)
+        synth.make_delay_polys(job, seed=30 + k)
+        job.validate()
+        jobs.append(job)
+    alone = [_alone(j, k, "fp16") for k, j in enumerate(jobs)]
+    members = [Correlator(j, xmac="fp16") for j in jobs]
+    batch = Batch(members)
+    assert batch.set_fused(fused) == fused
+    for graphs in (True, False):
+        batch.set_graphs(graphs)
+        for m in members:
+            m.reset()
+        for sec, ns in SUBINTS:
+            batch.submit([_inputs(j, k, sec, ns) for k, j in enumerate(jobs)], sec, ns)
+        batch.sync()
+        got = [m.results() for m in members]
+        for k, (g, a) in enumerate(zip(got, alone)):
+            assert np.array_equal(g, a), (graphs, FUSED_SHAPES[k])
+    batch.close()
+    for m in members:
+        m.close()
+
+
+def test_fused_batch_refused_for_fp32_members():
+    jobs = _uneven_jobs()
+    members = [Correlator(j, xmac="fp32") for j in jobs]
+    batch = Batch(members)
+    assert not batch.set_fused(True)
+    batch.close()
+    for m in members:
+        m.close()
 
 
 @pytest.mark.parametrize("xmac", ["fp32", "fp16"])
