@@ -125,6 +125,9 @@ struct fxb_ctx {
 	bool batched = false;     // a member of an fxb_batch: subints arrive through the batch
 	Tuner tune;
 	int gen = 0;              // bumped whenever launch parameters change: graphs are captured again
+	// work enqueued on the context's stream since a pipelined batch last
+	// ordered itself after it (a read, a reset, a reallocation)
+	bool dirty = false;
 	double t_prep = 0, t_f = 0, t_x = 0; // per-stage sums over timed subints (ms)
 	int32_t t_n = 0;
 	std::vector<bool> delay_set;
@@ -1019,6 +1022,8 @@ const char *fxb_last_error(const fxb_ctx *ctx)
 fxb_status fxb_set_delay_poly(fxb_ctx *ctx, int32_t station, int32_t npoly, int32_t order, double poly0_sec,
                               int32_t interval_s, const double *coeffs)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx) return FXB_ERR_ARG;
 	if(station < 0 || station >= ctx->S || npoly < 1 || npoly > kMaxPolys || order < 0 || order > kMaxPolyOrder ||
 	   interval_s <= 0 || !coeffs)
@@ -1099,6 +1104,7 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 		if(ctx->d_valid)
 		{
 			CK(ctx, cudaFreeAsync(ctx->d_valid, ctx->stream));
+		ctx->dirty = true;
 			ctx->d_valid = nullptr;
 		}
 		const size_t vbytes = ((size_t)need * ctx->S + 15) / 16 * 16;
@@ -1128,6 +1134,7 @@ static fxb_status stage_subint(fxb_ctx *ctx, const uint8_t *const *bufs, const i
 		{
 			if(ctx->d_mux)
 				CK(ctx, cudaFreeAsync(ctx->d_mux, ctx->stream));
+			ctx->dirty = true;
 			ctx->d_mux = nullptr;
 			CK(ctx, pool_alloc(ctx, (void **)&ctx->d_mux, sizeof(int32_t) * words, ctx->stream));
 			ctx->mux_cap = words;
@@ -1522,6 +1529,8 @@ fxb_status fxb_set_graphs(fxb_ctx *ctx, int32_t on)
 
 fxb_status fxb_autotune(fxb_ctx *ctx, int32_t rounds)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx || rounds < 0)
 		return FXB_ERR_ARG;
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1662,6 +1671,8 @@ static fxb_status check_device_error(fxb_ctx *ctx)
 
 fxb_status fxb_sync(fxb_ctx *ctx)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx) return FXB_ERR_ARG;
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
 	CK(ctx, cudaStreamSynchronize(ctx->copy_stream));
@@ -1758,6 +1769,8 @@ fxb_status fxb_job_footprint(const fxb_job_desc *desc, size_t *bytes)
 
 fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx || !coreresult) return FXB_ERR_ARG;
 	if(nfloats < (size_t)(2 * ctx->job.corelen))
 	{
@@ -1775,6 +1788,8 @@ fxb_status fxb_read_results(fxb_ctx *ctx, float *coreresult, size_t nfloats)
 
 fxb_status fxb_reset(fxb_ctx *ctx)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx) return FXB_ERR_ARG;
 	CK(ctx, cudaMemsetAsync(ctx->d_acc, 0, sizeof(float2) * std::max<int64_t>(ctx->job.acc_total, 1), ctx->stream));
 	CK(ctx, cudaMemsetAsync(ctx->d_bwacc, 0, sizeof(float) * std::max(ctx->nbw, 1), ctx->stream));
@@ -1804,6 +1819,8 @@ fxb_status fxb_last_timing(const fxb_ctx *ctx, float *fstage_ms, float *xmac_ms,
 
 fxb_status fxb_timing_enable(fxb_ctx *ctx, int32_t on)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx) return FXB_ERR_ARG;
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
 	for(Slot &sl : ctx->slots)
@@ -1816,6 +1833,8 @@ fxb_status fxb_timing_enable(fxb_ctx *ctx, int32_t on)
 
 fxb_status fxb_timing_read(fxb_ctx *ctx, int32_t *nsubint, double *prep_ms, double *fstage_ms, double *xmac_ms)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx) return FXB_ERR_ARG;
 	CK(ctx, cudaStreamSynchronize(ctx->stream));
 	for(Slot &sl : ctx->slots)
@@ -1922,6 +1941,8 @@ void fxb_host_free(void *p)
 
 fxb_status fxb_read_results_device(fxb_ctx *ctx, float *dev_out, size_t nfloats)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx || !dev_out) return FXB_ERR_ARG;
 	if(nfloats < (size_t)(2 * ctx->job.corelen))
 	{
@@ -1940,6 +1961,8 @@ fxb_status fxb_datastream_control(fxb_ctx *ctx, int32_t station, fxb_ring *ring,
                                   int32_t ns, const double *delay_us, int64_t *offset, int32_t *nbytes,
                                   int32_t *datasec, int32_t *datans, int32_t *validflags, size_t nflagint)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx || station < 0 || station >= ctx->S)
 		return FXB_ERR_ARG;
 	if(!delay_us && !ctx->delay_set[station])
@@ -1987,6 +2010,8 @@ fxb_status fxb_job_datastream_control(const fxb_job_desc *desc, int32_t station,
 
 fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloats, int32_t *nfft, int32_t *nrow)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx || !out || freq < 0 || freq >= ctx->F) return FXB_ERR_ARG;
 	const DevFreqPlan &p = ctx->h_plans[freq];
 	size_t n = (size_t)ctx->T * p.nrow * p.nchan;
@@ -2034,6 +2059,8 @@ fxb_status fxb_read_spectra(fxb_ctx *ctx, int32_t freq, float *out, size_t nfloa
 
 fxb_status fxb_read_fft_weights(fxb_ctx *ctx, float *out, size_t nfloats)
 {
+	if(ctx)
+		ctx->dirty = true;
 	if(!ctx || !out) return FXB_ERR_ARG;
 	size_t n = (size_t)ctx->S * ctx->T;
 	if(nfloats < n) return FXB_ERR_ARG;
@@ -2104,7 +2131,14 @@ struct fxb_batch {
 	bool graphs = true;
 	// fused mode: the persistent F launches' work list over all members and
 	// their two unit counters
-	bool fused = true;
+	bool fused = false;
+	// fused mode pipelines subints: the XMAC of a subint runs on xstream
+	// beside the next subint's F stage, so every slot has its own spectra of
+	// every member (slot 0: the member's own buffer) and tensor maps over them
+	std::vector<std::vector<void *>> fspec;                    // [slot][member]
+	std::vector<std::vector<std::vector<TmapBytes>>> ftmap;    // [slot][member][XMAC group]
+	cudaStream_t xstream = nullptr;
+	std::vector<cudaEvent_t> fdone, xdone;                     // [slot]
 	FsMultiKind *d_kinds = nullptr;
 	FsMultiUnit *d_units = nullptr;
 	int32_t nwide = 0, nnarrow = 0;
@@ -2123,9 +2157,19 @@ static void free_batch(fxb_batch *b)
 	if(b->fork) cudaEventDestroy(b->fork);
 	if(b->done) cudaEventDestroy(b->done);
 	if(b->stream) cudaStreamDestroy(b->stream);
+	if(b->xstream)
+		cudaStreamSynchronize(b->xstream);
 	if(b->d_kinds) cudaFree(b->d_kinds);
 	if(b->d_units) cudaFree(b->d_units);
 	if(b->d_ctr) cudaFree(b->d_ctr);
+	for(size_t k = 1; k < b->fspec.size(); k++)
+		for(void *p : b->fspec[k])
+			if(p) cudaFree(p);
+	for(cudaEvent_t e : b->fdone)
+		if(e) cudaEventDestroy(e);
+	for(cudaEvent_t e : b->xdone)
+		if(e) cudaEventDestroy(e);
+	if(b->xstream) cudaStreamDestroy(b->xstream);
 	for(fxb_ctx *c : b->m)
 		c->batched = false;
 	delete b;
@@ -2193,14 +2237,52 @@ static fxb_status batch_fused_plan(fxb_batch *b)
 		BK(b, cudaMemcpy(b->d_units, units.data(), sizeof(FsMultiUnit) * units.size(), cudaMemcpyHostToDevice));
 	b->nwide = (int32_t)wide.size();
 	b->nnarrow = (int32_t)narrow.size();
+	const size_t nslot = b->gexec.size();
+	b->fspec.assign(nslot, std::vector<void *>(b->m.size(), nullptr));
+	b->ftmap.assign(nslot, std::vector<std::vector<TmapBytes>>(b->m.size()));
+	BK(b, cudaStreamCreateWithFlags(&b->xstream, cudaStreamNonBlocking));
+	b->fdone.assign(nslot, nullptr);
+	b->xdone.assign(nslot, nullptr);
+	for(size_t k = 0; k < nslot; k++)
+	{
+		BK(b, cudaEventCreateWithFlags(&b->fdone[k], cudaEventDisableTiming));
+		BK(b, cudaEventCreateWithFlags(&b->xdone[k], cudaEventDisableTiming));
+		for(size_t i = 0; i < b->m.size(); i++)
+		{
+			fxb_ctx *c = b->m[i];
+			void *sp = c->d_specn;
+			if(k > 0)
+			{
+				// times past T of every block stay zero
+				BK(b, cudaMalloc(&sp, sizeof(uint32_t) * (size_t)c->specn_elems));
+				b->fspec[k][i] = sp;
+				BK(b, cudaMemset(sp, 0, sizeof(uint32_t) * (size_t)c->specn_elems));
+			}
+			else
+				b->fspec[k][i] = sp;
+			for(const auto &g : c->xgroups)
+			{
+				TmapBytes tm;
+				memset(&tm, 0, sizeof(tm));
+				if(k == 0)
+					memcpy(&tm, g.tmap, sizeof(tm));
+				else if(g.xmac && !tc_make_tensormap(&tm, (const uint32_t *)sp + g.spec_base, g.shape, g.nf))
+				{
+					b->err = "cuTensorMapEncodeTiled failed for a batch spectra buffer";
+					return FXB_ERR_CUDA;
+				}
+				b->ftmap[k][i].push_back(tm);
+			}
+		}
+	}
 	return FXB_OK;
 }
 
-// The fused launches of one subint on the batch stream: every member's
-// preparation as a branch, then one persistent F launch (and the members'
-// tensor-core FFT kinds), then every member's XMAC groups and weights as
-// branches.
-static void batch_fused_launch(fxb_batch *b, const std::vector<Slot *> &slots, bool capture)
+// The fused F part of one subint (slot k) on the batch stream: every
+// member's preparation as a branch, then the members' tensor-core FFT kinds
+// and the persistent F launches into slot k's spectra, then the members'
+// weights as branches.
+static void batch_fused_launch(fxb_batch *b, int k, const std::vector<Slot *> &slots, bool capture)
 {
 	const unsigned evf = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
 	const size_t n = b->m.size();
@@ -2222,10 +2304,11 @@ static void batch_fused_launch(fxb_batch *b, const std::vector<Slot *> &slots, b
 	{
 		fxb_ctx *c = b->m[i];
 		ma.m[i] = fs_args(c, *slots[i]);
-		for(const FKind &k : c->fkinds)
-			if(k.tcfft)
+		ma.m[i].spec = b->fspec[k][i];
+		for(const FKind &fk : c->fkinds)
+			if(fk.tcfft)
 			{
-				const cudaError_t le = launch_fstage_tc(k, ma.m[i], c->nsm, b->stream);
+				const cudaError_t le = launch_fstage_tc(fk, ma.m[i], c->nsm, b->stream);
 				if(le != cudaSuccess && c->launch_err == cudaSuccess)
 					c->launch_err = le;
 			}
@@ -2240,38 +2323,44 @@ static void batch_fused_launch(fxb_batch *b, const std::vector<Slot *> &slots, b
 	if(le != cudaSuccess && b->m[0]->launch_err == cudaSuccess)
 		b->m[0]->launch_err = le;
 	cudaEventRecord(b->fork, b->stream);
-	// the members' weights beside one XMAC launch over every member's groups
-	// of the first group's rows (groups of other rows: a launch each)
 	for(size_t i = 0; i < n; i++)
 	{
 		fxb_ctx *c = b->m[i];
 		cudaStreamWaitEvent(c->stream, b->fork, 0);
 		launch_xmac_weights(c, *slots[i], c->stream, evf, false, false);
 	}
-	XMultiArgs xm;
-	memset(&xm, 0, sizeof(xm));
-	const TcShape *common = nullptr;
-	for(size_t i = 0; i < n; i++)
-	{
-		fxb_ctx *c = b->m[i];
-		for(const auto &g : c->xgroups)
-		{
-			if(!g.xmac)
-				continue;
-			if(!common)
-				common = &g.shape;
-			if(g.shape.nrow != common->nrow || g.shape.h16 != common->h16 ||
-			   !xmac_multi_add(&xm, g.tmap, g.shape, c->d_plans, g.d_idx, g.nf, c->d_acc))
-				launch_xmac_tc(g.tmap, g.shape, c->d_plans, g.d_idx, g.nf, c->nsm, c->d_err, c->d_acc, b->stream);
-		}
-	}
-	if(common)
-		launch_xmac_tc_multi(xm, *common, b->m[0]->nsm, b->m[0]->d_err, b->stream);
 	for(size_t i = 0; i < n; i++)
 	{
 		cudaEventRecord(b->join[i], b->m[i]->stream);
 		cudaStreamWaitEvent(b->stream, b->join[i], 0);
 	}
+}
+
+// The fused XMAC of slot k's spectra: one launch over every member's groups
+// of the first group's rows (groups of other rows: a launch each).
+static void batch_fused_xmac(fxb_batch *b, int k, cudaStream_t st)
+{
+	XMultiArgs xm;
+	memset(&xm, 0, sizeof(xm));
+	const TcShape *common = nullptr;
+	for(size_t i = 0; i < b->m.size(); i++)
+	{
+		fxb_ctx *c = b->m[i];
+		for(size_t gi = 0; gi < c->xgroups.size(); gi++)
+		{
+			const auto &g = c->xgroups[gi];
+			if(!g.xmac)
+				continue;
+			const void *tm = &b->ftmap[k][i][gi];
+			if(!common)
+				common = &g.shape;
+			if(g.shape.nrow != common->nrow || g.shape.h16 != common->h16 ||
+			   !xmac_multi_add(&xm, tm, g.shape, c->d_plans, g.d_idx, g.nf, c->d_acc))
+				launch_xmac_tc(tm, g.shape, c->d_plans, g.d_idx, g.nf, c->nsm, c->d_err, c->d_acc, st);
+		}
+	}
+	if(common)
+		launch_xmac_tc_multi(xm, *common, b->m[0]->nsm, b->m[0]->d_err, st);
 }
 
 // capture every member's kernels for slot k (fused, or as parallel branches)
@@ -2292,7 +2381,7 @@ static fxb_status batch_graph(fxb_batch *b, int k, const std::vector<Slot *> &sl
 	// one fork for all members, then every join: the branches are independent
 	BK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
 	if(fused)
-		batch_fused_launch(b, slots, true);
+		batch_fused_launch(b, k, slots, true);
 	else
 	{
 		cudaEventRecord(b->fork, b->stream);
@@ -2400,6 +2489,10 @@ static fxb_status batch_submit(fxb_batch *b, const fxb_member_subint *data, int3
 		}
 	}
 	const int k = b->m[0]->next_slot;
+	bool tuning = false;
+	for(fxb_ctx *c : b->m)
+		tuning = tuning || c->tune.iter < c->tune.total;
+	const bool pipelined = !tuning && batch_fusable(b) && !b->fspec.empty();
 	std::vector<Slot *> slots(n, nullptr);
 	for(size_t i = 0; i < n; i++)
 	{
@@ -2413,15 +2506,18 @@ static fxb_status batch_submit(fxb_batch *b, const fxb_member_subint *data, int3
 			return rc;
 		}
 		BK(b, cudaStreamWaitEvent(b->stream, slots[i]->copied, 0));
-		// and after whatever the member's own stream still holds (a reset, a read)
-		BK(b, cudaEventRecord(b->join[i], c->stream));
-		BK(b, cudaStreamWaitEvent(b->stream, b->join[i], 0));
+		// and after whatever the member's own stream still holds (a reset, a
+		// read); a pipelined batch only when the member has enqueued any,
+		// since that stream also waits for the last subint's XMAC
+		if(!pipelined || c->dirty)
+		{
+			BK(b, cudaEventRecord(b->join[i], c->stream));
+			BK(b, cudaStreamWaitEvent(b->stream, b->join[i], 0));
+			c->dirty = false;
+		}
 	}
 	// a member still tuning runs eagerly (one member after the other, so
 	// that its launch times are its own)
-	bool tuning = false;
-	for(fxb_ctx *c : b->m)
-		tuning = tuning || c->tune.iter < c->tune.total;
 	const bool fused = !tuning && batch_fusable(b);
 	if(fused)
 	{
@@ -2435,13 +2531,26 @@ static fxb_status batch_submit(fxb_batch *b, const fxb_member_subint *data, int3
 		if(rc != FXB_OK)
 			return rc;
 	}
+	// fused: slot k's spectra are free once the XMAC of its last subint is done
+	if(fused)
+		BK(b, cudaStreamWaitEvent(b->stream, b->xdone[k], 0));
 	if(b->graphs && !tuning)
 		BK(b, cudaGraphLaunch(b->gexec[k], b->stream));
 	else if(fused)
-		batch_fused_launch(b, slots, false);
+		batch_fused_launch(b, k, slots, false);
 	else
 		for(size_t i = 0; i < n; i++)
 			launch_compute(b->m[i], *slots[i], b->stream, false);
+	cudaStream_t endst = b->stream;
+	if(fused)
+	{
+		// the XMAC beside the next subint's F stage
+		BK(b, cudaEventRecord(b->fdone[k], b->stream));
+		BK(b, cudaStreamWaitEvent(b->xstream, b->fdone[k], 0));
+		batch_fused_xmac(b, k, b->xstream);
+		BK(b, cudaEventRecord(b->xdone[k], b->xstream));
+		endst = b->xstream;
+	}
 	for(fxb_ctx *c : b->m)
 		if(take_launch_err(c) != FXB_OK)
 		{
@@ -2452,10 +2561,10 @@ static fxb_status batch_submit(fxb_batch *b, const fxb_member_subint *data, int3
 		if(c->tune.iter < c->tune.total)
 			tune_collect(c);
 	BK(b, cudaGetLastError());
-	BK(b, cudaEventRecord(b->done, b->stream));
+	BK(b, cudaEventRecord(b->done, endst));
 	for(size_t i = 0; i < n; i++)
 	{
-		BK(b, cudaEventRecord(slots[i]->done, b->stream));
+		BK(b, cudaEventRecord(slots[i]->done, endst));
 		BK(b, cudaStreamWaitEvent(b->m[i]->stream, b->done, 0));
 		slots[i]->tpending = b->m[i]->timing_on;
 		b->m[i]->last_slot = (int)(slots[i] - b->m[i]->slots.data());
@@ -2479,6 +2588,8 @@ fxb_status fxb_batch_sync(fxb_batch *b)
 	if(!b)
 		return FXB_ERR_ARG;
 	BK(b, cudaStreamSynchronize(b->stream));
+	if(b->xstream)
+		BK(b, cudaStreamSynchronize(b->xstream));
 	for(fxb_ctx *c : b->m)
 	{
 		const fxb_status st = check_device_error(c);

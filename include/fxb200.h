@@ -246,13 +246,14 @@ FXB_API fxb_status fxb_tuning_report(const fxb_ctx *ctx, char *buf, size_t len, 
  * per subband shape (bandwidth, channels, bits) of an observation whose
  * subbands are uneven.  Per subint every member copies its station buffers
  * on its own copy stream, then one CUDA graph launch runs the members'
- * kernels.  Fused (the default where every member allows it: tensor-core
- * forms without FP8, phase cal, zoom bands, raw INTERLACEDVDIF reads or
- * complex sampling, and FFTs of at most 8192 points): the F stages of all
- * members run as one persistent launch over a work list that spans the
- * members (the N = 2048 tensor-core FFT kinds as their own launches), and
- * every XMAC group of every member as one persistent launch; the rest are
- * parallel branches, one per member.  Results do not depend on the mode.  A
+ * kernels as parallel branches, one per member.  Fused (fxb_batch_set_fused;
+ * where every member allows it: tensor-core forms without FP8, phase cal,
+ * zoom bands, raw INTERLACEDVDIF reads or complex sampling, and FFTs of at
+ * most 8192 points): the F stages of all members run as the persistent
+ * launches over one work list that spans the members (the N = 2048
+ * tensor-core FFT kinds as their own launches), and every XMAC group of
+ * every member as one persistent launch on a second stream, beside the next
+ * subint's F stage.  Results do not depend on the mode.  A
  * member takes no fxb_submit_subint of its own while it belongs to a batch;
  * its results are read and reset through the usual calls (ordered after the
  * batch's launches).  All members need the same max_subints_in_flight. */
@@ -272,9 +273,9 @@ FXB_API fxb_status fxb_batch_submit(fxb_batch *batch, const fxb_member_subint *d
 FXB_API fxb_status fxb_batch_submit_device(fxb_batch *batch, const fxb_member_subint *data, int32_t sec, int32_t ns);
 FXB_API fxb_status fxb_batch_sync(fxb_batch *batch);
 FXB_API fxb_status fxb_batch_set_graphs(fxb_batch *batch, int32_t on);
-/* on = 0: every member's kernels as its own graph branch even where the
- * fused launches are possible; *fused (may be NULL) = whether the next
- * subints run fused. */
+/* on = 1: the fused launches where the members allow them (off by
+ * default); *fused (may be NULL) = whether the next subints run fused.
+ * fxb_read_spectra of a fused member reads the first slot's spectra. */
 FXB_API fxb_status fxb_batch_set_fused(fxb_batch *batch, int32_t on, int32_t *fused);
 /* fxb_autotune on every member (members still tuning run eagerly). */
 FXB_API fxb_status fxb_batch_autotune(fxb_batch *batch, int32_t rounds);
