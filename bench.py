@@ -68,7 +68,38 @@ def parse():
     ap.add_argument("--no-mux", action="store_true", help="skip the INTERLACEDVDIF muxing leg")
     ap.add_argument("--no-features", action="store_true", help="skip the phase-cal and zoom-band legs")
     ap.add_argument("--serving-jobs", type=int, default=12)
+    ap.add_argument("--c3-only", choices=["branches", "fused", "per-job"], default=None,
+                    help="profiling aid: run only the c3 batch in one form for --warmup + --steps subints "
+                         "(no timing) and print one record")
     return ap.parse_args()
+
+
+def c3_only(args):
+    """The c3 leg in one form, for launch lists and captures of its kernels."""
+    import torch
+    from fxb200.native import Batch, Correlator
+    jobs = configs.c3()
+    pools = [make_pool(j, 1, seed=7 + m) for m, j in enumerate(jobs)]
+    dev = [[torch.from_numpy(b).to("cuda") for b, _, _ in pool[0][1]] for pool in pools]
+    meta = [([t.data_ptr() for t in dev[m]], [b.size for b, _, _ in pools[m][0][1]],
+             [x for _, x, _ in pools[m][0][1]], [x for _, _, x in pools[m][0][1]]) for m in range(len(jobs))]
+    when = pools[0][0][0]
+    members = [Correlator(j, xmac="fp16", inflight=3) for j in jobs]
+    batch = None if args.c3_only == "per-job" else Batch(members)
+    fused = batch.set_fused(args.c3_only == "fused") if batch is not None else False
+    for _ in range(args.warmup + args.steps):
+        if batch is not None:
+            batch.submit_device(meta, *when)
+        else:
+            for m, c in enumerate(members):
+                c.submit_device(*meta[m], *when)
+    if batch is not None:
+        batch.sync()
+        batch.close()
+    for m in members:
+        m.sync()
+        m.close()
+    print(json.dumps({"c3_only": args.c3_only, "fused": fused, "subints": args.warmup + args.steps}))
 
 
 def subint_time(job, k):
@@ -873,7 +904,9 @@ def gpu_arm(args, job):
 def main():
     args = parse()
     job = configs.c1()
-    if args.impl == "reference":
+    if args.c3_only:
+        c3_only(args)
+    elif args.impl == "reference":
         reference_arm(args, job)
     else:
         gpu_arm(args, job)

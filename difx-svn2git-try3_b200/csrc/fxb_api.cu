@@ -138,7 +138,7 @@ struct fxb_ctx {
 	// first), on the host and on the device, and the launches' unit counters
 	std::vector<FsMultiKind> pkinds;
 	std::vector<FsMultiUnit> punits;
-	int32_t pnwide = 0, pnnarrow = 0;
+	int32_t punit0[kFsMultiClasses] = {}, pnunit[kFsMultiClasses] = {};
 	FsMultiKind *d_pkinds = nullptr;
 	FsMultiUnit *d_punits = nullptr;
 	int32_t *d_pctr = nullptr;
@@ -777,7 +777,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				k.tw = d;
 			}
 			bool wide = false;
-			if(out == 1 && !k.tcfft && !k.muxraw && !k.cplx && fstage_multi_shape(k.N, k.nb, &wide))
+			if(out == 1 && !k.tcfft && !k.cplx && fstage_multi_shape(k.N, k.nb, &wide))
 				k.persist = 1;
 			hg.insert(hg.end(), kv.second.begin(), kv.second.end());
 			ctx->fkinds.push_back(k);
@@ -785,7 +785,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		// the persistent launches' work list: per kind tq x fpc FFT times of
 		// one item per unit, times outer and items inner
 		{
-			std::vector<FsMultiUnit> wide, narrow;
+			// classes: wide, narrow units of plain VDIF; wide, narrow of raw reads
+			std::vector<FsMultiUnit> cls[kFsMultiClasses];
 			for(const FKind &k : ctx->fkinds)
 			{
 				if(!k.persist)
@@ -798,26 +799,28 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				int logn = 0;
 				while((1 << logn) < k.N)
 					logn++;
-				mk.code = 32 * k.nb + logn;
+				mk.code = 64 * k.muxraw + 32 * k.nb + logn;
 				mk.first = k.first;
 				mk.tq = fstage_multi_tq(k.N, k.nb, k.tq);
 				const int ki = (int)ctx->pkinds.size();
 				ctx->pkinds.push_back(mk);
 				const int per = mk.tq * k.fpc, nt = (ctx->T + per - 1) / per;
-				std::vector<FsMultiUnit> &dst = w ? wide : narrow;
+				std::vector<FsMultiUnit> &dst = cls[2 * k.muxraw + (w ? 0 : 1)];
 				for(int t = 0; t < nt; t++)
 					for(int it = 0; it < k.count; it++)
 						dst.push_back(FsMultiUnit{ki, it, t});
 			}
-			ctx->pnwide = (int32_t)wide.size();
-			ctx->pnnarrow = (int32_t)narrow.size();
-			ctx->punits = wide;
-			ctx->punits.insert(ctx->punits.end(), narrow.begin(), narrow.end());
+			for(int c = 0; c < kFsMultiClasses; c++)
+			{
+				ctx->punit0[c] = (int32_t)ctx->punits.size();
+				ctx->pnunit[c] = (int32_t)cls[c].size();
+				ctx->punits.insert(ctx->punits.end(), cls[c].begin(), cls[c].end());
+			}
 			if(!ctx->pkinds.empty())
 			{
 				CK(ctx, dalloc(ctx, &ctx->d_pkinds, ctx->pkinds.size()));
 				CK(ctx, dalloc(ctx, &ctx->d_punits, ctx->punits.size()));
-				CK(ctx, dalloc(ctx, &ctx->d_pctr, 2));
+				CK(ctx, dalloc(ctx, &ctx->d_pctr, kFsMultiClasses));
 				CK(ctx, cudaMemcpyAsync(ctx->d_pkinds, ctx->pkinds.data(), sizeof(FsMultiKind) * ctx->pkinds.size(),
 				                        cudaMemcpyHostToDevice, ctx->stream));
 				CK(ctx, cudaMemcpyAsync(ctx->d_punits, ctx->punits.data(), sizeof(FsMultiUnit) * ctx->punits.size(),
@@ -1321,10 +1324,13 @@ static void launch_compute(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, bool c
 			ma.m[0] = fa;
 			ma.kinds = ctx->d_pkinds;
 			ma.units = ctx->d_punits;
-			ma.nwide = ctx->pnwide;
-			ma.nnarrow = ctx->pnnarrow;
+			for(int c = 0; c < kFsMultiClasses; c++)
+			{
+				ma.unit0[c] = ctx->punit0[c];
+				ma.nunit[c] = ctx->pnunit[c];
+			}
 			ma.ctr = ctx->d_pctr;
-			cudaMemsetAsync(ctx->d_pctr, 0, 2 * sizeof(int32_t), st);
+			cudaMemsetAsync(ctx->d_pctr, 0, kFsMultiClasses * sizeof(int32_t), st);
 			const cudaError_t le = launch_fstage_multi(ma, ctx->nsm, st);
 			if(le != cudaSuccess && ctx->launch_err == cudaSuccess)
 				ctx->launch_err = le;
@@ -2141,7 +2147,7 @@ struct fxb_batch {
 	std::vector<cudaEvent_t> fdone, xdone;                     // [slot]
 	FsMultiKind *d_kinds = nullptr;
 	FsMultiUnit *d_units = nullptr;
-	int32_t nwide = 0, nnarrow = 0;
+	int32_t unit0[kFsMultiClasses] = {}, nunit[kFsMultiClasses] = {};
 	int32_t *d_ctr = nullptr;
 	std::string err;
 };
@@ -2202,41 +2208,46 @@ static bool batch_fusable(const fxb_batch *b)
 	return true;
 }
 
-// The fused F launch's work list: the members' own lists, wide units of all
-// members first, each member's kinds renumbered.
+// The fused F launch's work list: the members' own lists, class by class
+// (wide units of all members first), each member's kinds renumbered.
 static fxb_status batch_fused_plan(fxb_batch *b)
 {
 	if(b->d_units)
 		return FXB_OK;
 	std::vector<FsMultiKind> kinds;
-	std::vector<FsMultiUnit> wide, narrow;
+	std::vector<int> k0(b->m.size());
 	for(size_t i = 0; i < b->m.size(); i++)
 	{
-		const fxb_ctx *c = b->m[i];
-		const int k0 = (int)kinds.size();
-		for(FsMultiKind mk : c->pkinds)
+		k0[i] = (int)kinds.size();
+		for(FsMultiKind mk : b->m[i]->pkinds)
 		{
 			mk.member = (int32_t)i;
 			kinds.push_back(mk);
 		}
-		for(int u = 0; u < (int)c->punits.size(); u++)
-		{
-			FsMultiUnit w = c->punits[u];
-			w.kind += k0;
-			(u < c->pnwide ? wide : narrow).push_back(w);
-		}
 	}
-	std::vector<FsMultiUnit> units(wide);
-	units.insert(units.end(), narrow.begin(), narrow.end());
+	std::vector<FsMultiUnit> units;
+	for(int cl = 0; cl < kFsMultiClasses; cl++)
+	{
+		b->unit0[cl] = (int32_t)units.size();
+		for(size_t i = 0; i < b->m.size(); i++)
+		{
+			const fxb_ctx *c = b->m[i];
+			for(int u = c->punit0[cl]; u < c->punit0[cl] + c->pnunit[cl]; u++)
+			{
+				FsMultiUnit w = c->punits[u];
+				w.kind += k0[i];
+				units.push_back(w);
+			}
+		}
+		b->nunit[cl] = (int32_t)units.size() - b->unit0[cl];
+	}
 	BK(b, cudaMalloc(&b->d_kinds, sizeof(FsMultiKind) * std::max<size_t>(kinds.size(), 1)));
 	BK(b, cudaMalloc(&b->d_units, sizeof(FsMultiUnit) * std::max<size_t>(units.size(), 1)));
-	BK(b, cudaMalloc(&b->d_ctr, 2 * sizeof(int32_t)));
+	BK(b, cudaMalloc(&b->d_ctr, kFsMultiClasses * sizeof(int32_t)));
 	if(!kinds.empty())
 		BK(b, cudaMemcpy(b->d_kinds, kinds.data(), sizeof(FsMultiKind) * kinds.size(), cudaMemcpyHostToDevice));
 	if(!units.empty())
 		BK(b, cudaMemcpy(b->d_units, units.data(), sizeof(FsMultiUnit) * units.size(), cudaMemcpyHostToDevice));
-	b->nwide = (int32_t)wide.size();
-	b->nnarrow = (int32_t)narrow.size();
 	const size_t nslot = b->gexec.size();
 	b->fspec.assign(nslot, std::vector<void *>(b->m.size(), nullptr));
 	b->ftmap.assign(nslot, std::vector<std::vector<TmapBytes>>(b->m.size()));
@@ -2315,10 +2326,13 @@ static void batch_fused_launch(fxb_batch *b, int k, const std::vector<Slot *> &s
 	}
 	ma.kinds = b->d_kinds;
 	ma.units = b->d_units;
-	ma.nwide = b->nwide;
-	ma.nnarrow = b->nnarrow;
+	for(int cl = 0; cl < kFsMultiClasses; cl++)
+	{
+		ma.unit0[cl] = b->unit0[cl];
+		ma.nunit[cl] = b->nunit[cl];
+	}
 	ma.ctr = b->d_ctr;
-	cudaMemsetAsync(b->d_ctr, 0, 2 * sizeof(int32_t), b->stream);
+	cudaMemsetAsync(b->d_ctr, 0, kFsMultiClasses * sizeof(int32_t), b->stream);
 	const cudaError_t le = launch_fstage_multi(ma, b->m[0]->nsm, b->stream);
 	if(le != cudaSuccess && b->m[0]->launch_err == cudaSuccess)
 		b->m[0]->launch_err = le;

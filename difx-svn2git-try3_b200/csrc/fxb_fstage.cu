@@ -380,11 +380,10 @@ __device__ __forceinline__ void fstage_unit(const FsArgs &a, const int gidx, con
 
 	const int t0 = tchunk * tq * FPC;
 	const int nit = min(tq, (a.T - t0 + FPC - 1) / FPC);
-	// ---- constants of the unit's FFTs (FFT f is time t0 + f), one warp per FFT
+	// ---- constants of the unit's FFTs (FFT f is time t0 + f), one thread per FFT
 	{
-		const int lane = tm.tid() & 31;
 		const int nfc = nit * FPC;
-		for(int f = tm.tid() >> 5; f < nfc; f += tm.nt() >> 5)
+		for(int f = tm.tid(); f < nfc; f += tm.nt())
 		{
 			const int t = t0 + f;
 			FftConst c;
@@ -451,12 +450,20 @@ __device__ __forceinline__ void fstage_unit(const FsArgs &a, const int gidx, con
 			}
 			// validity of the window's frames, one bit per frame relative to fa
 			const uint32_t nwf = (c.so + (uint32_t)N - 1) / fs + 1;
-			const int64_t fr = (int64_t)c.fa + lane;
-			// complex data: the unpack's first frame is checked for fill pattern
-			// only (mark5_stream_unpacker.c:189)
-			const uint8_t *vsrc = (CPLX && lane == 0 && a.fillok) ? a.fillok + (int64_t)g.station * a.valid_stride : vrow;
-			const bool v = (c.flags & 1) && (uint32_t)lane < nwf && fr < a.valid_stride && vsrc[fr] != 0;
-			c.fmask = __ballot_sync(0xffffffffu, v);
+			if(c.flags & 1)
+			{
+				const uint32_t nm = nwf < 32u ? nwf : 32u;
+				for(uint32_t k = 0; k < nm; k++)
+				{
+					const int64_t fr = (int64_t)c.fa + k;
+					// complex data: the unpack's first frame is checked for fill
+					// pattern only (mark5_stream_unpacker.c:189)
+					const uint8_t *vsrc =
+					    (CPLX && k == 0 && a.fillok) ? a.fillok + (int64_t)g.station * a.valid_stride : vrow;
+					if(fr < a.valid_stride && vsrc[fr] != 0)
+						c.fmask |= 1u << k;
+				}
+			}
 			if(nwf <= 32)
 				c.flags |= 2;
 			if(c.dhi[0] == c.dhi[1] && c.dlo[0] == c.dlo[1] && g.phase[0] == g.phase[1])
@@ -466,17 +473,16 @@ __device__ __forceinline__ void fstage_unit(const FsArgs &a, const int gidx, con
 				// EDV4-blanked bands (INTERLACEDVDIF): the slow decode path below
 				const uint32_t need = (1u << g.band[0]) | (g.band[1] >= 0 ? 1u << g.band[1] : 0u);
 				bool part = false;
-				for(uint32_t k = (uint32_t)lane; (c.flags & 1) && k < nwf; k += 32)
+				for(uint32_t k = 0; (c.flags & 1) && k < nwf && !part; k++)
 				{
 					const int64_t fk = (int64_t)c.fa + k;
-					part = part || (fk < a.valid_stride && vrow[fk] != 0 &&
-					                (a.bandok[(int64_t)g.station * a.valid_stride + fk] & need) != need);
+					part = fk < a.valid_stride && vrow[fk] != 0 &&
+					       (a.bandok[(int64_t)g.station * a.valid_stride + fk] & need) != need;
 				}
-				if(__any_sync(0xffffffffu, part))
+				if(part)
 					c.flags |= 4;
 			}
-			if(lane == 0)
-				fcs[f] = c;
+			fcs[f] = c;
 		}
 		tm.sync();
 	}
@@ -809,8 +815,9 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 }
 
 // ---------------------------------------------------------------- persistent launches
-// Two persistent kernels take the tensor-core-form kinds of plain VDIF
-// stations (of one context or of a batch of them) from a work list: the
+// Two persistent kernels take the tensor-core-form kinds of VDIF stations
+// (plain, or raw INTERLACEDVDIF reads; of one context or of a batch of them)
+// from a work list: the
 // narrow one every length up to 4096 points in CTAs of 256 threads (the
 // shape of k_fstage for those lengths), the wide one 8192-point FFTs of one
 // band in CTAs of 512.  Each CTA takes a unit at a time from a counter and
@@ -818,18 +825,17 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 constexpr size_t kNarrowSide = 36864;            // exchange buffer: 2048 points x 2 bands (or 4096 x 1), padded
 constexpr size_t kWideSmem = 73728;              // 8192 points of one band, padded
 
-template <class Team>
-__device__ __forceinline__ void narrow_unit(const FsArgs &a, const FsMultiKind &k, const FsMultiUnit &w, int pp,
-                                            uint2 *fsm, const float *lut8, const float2 *lut4, FftConst *fcs,
-                                            const Team &tm)
+template <int VAR, class Team>
+__device__ __forceinline__ void narrow_unit(const FsArgs &a, const FsMultiKind &k, const FsMultiUnit &w, uint2 *fsm,
+                                            const float *lut8, const float2 *lut4, FftConst *fcs, const Team &tm)
 {
 	const float2 *tw = (const float2 *)k.tw;
 	const int gi = k.first + w.item;
-	switch(k.code)
+	switch(k.code & 63)
 	{
 #define FXB_MULTI_CASE(NV, LOGN)                                                                               \
 	case 32 * NV + LOGN:                                                                                       \
-		fstage_unit<NV, LOGN, true, 0>(a, gi, w.tchunk, k.tq, pp, tw, fsm, lut8, lut4, fcs, tm);              \
+		fstage_unit<NV, LOGN, true, VAR>(a, gi, w.tchunk, k.tq, 0, tw, fsm, lut8, lut4, fcs, tm);             \
 		break;
 		FXB_MULTI_CASE(2, 5)
 		FXB_MULTI_CASE(2, 6)
@@ -863,8 +869,10 @@ __device__ __forceinline__ int next_unit(int32_t *ctr, int *slot)
 	return u;
 }
 
-// one exchange buffer per unit (three CTAs per SM): faster than two buffers
-// at two CTAs per SM on every length measured
+// One exchange buffer per unit (three CTAs per SM): faster than two buffers
+// at two CTAs per SM on every c3 length measured.  VAR 0: plain VDIF, 1: raw
+// INTERLACEDVDIF reads; work-list class 2 VAR + 1.
+template <int VAR>
 __global__ void __launch_bounds__(256, 3) k_fstage_pn(const __grid_constant__ FsMultiArgs m)
 {
 	extern __shared__ __align__(16) uint2 fsm[];
@@ -873,18 +881,21 @@ __global__ void __launch_bounds__(256, 3) k_fstage_pn(const __grid_constant__ Fs
 	__shared__ FftConst fcs[kFsMultiFc];
 	__shared__ int unit_s;
 	const CtaTeam cta;
+	constexpr int cls = 2 * VAR + 1;
 	fstage_luts(cta, true, lut8, lut4);
 	for(;;)
 	{
-		const int u = next_unit(m.ctr + 1, &unit_s);
-		if(u >= m.nnarrow)
+		const int u = next_unit(m.ctr + cls, &unit_s);
+		if(u >= m.nunit[cls])
 			break;
-		const FsMultiUnit w = m.units[m.nwide + u];
+		const FsMultiUnit w = m.units[m.unit0[cls] + u];
 		const FsMultiKind k = m.kinds[w.kind];
-		narrow_unit(m.m[k.member], k, w, 0, fsm, lut8, lut4, fcs, cta);
+		narrow_unit<VAR>(m.m[k.member], k, w, fsm, lut8, lut4, fcs, cta);
 	}
 }
 
+// work-list class 2 VAR
+template <int VAR>
 __global__ void __launch_bounds__(512, 2) k_fstage_pw(const __grid_constant__ FsMultiArgs m)
 {
 	extern __shared__ __align__(16) uint2 fsm[];
@@ -893,16 +904,17 @@ __global__ void __launch_bounds__(512, 2) k_fstage_pw(const __grid_constant__ Fs
 	__shared__ FftConst fcs[kMaxTQ];
 	__shared__ int unit_s;
 	const CtaTeam cta;
+	constexpr int cls = 2 * VAR;
 	fstage_luts(cta, true, lut8, lut4);
 	for(;;)
 	{
-		const int u = next_unit(m.ctr, &unit_s);
-		if(u >= m.nwide)
+		const int u = next_unit(m.ctr + cls, &unit_s);
+		if(u >= m.nunit[cls])
 			break;
-		const FsMultiUnit w = m.units[u];
+		const FsMultiUnit w = m.units[m.unit0[cls] + u];
 		const FsMultiKind k = m.kinds[w.kind];
-		fstage_unit<1, 13, true, 0>(m.m[k.member], k.first + w.item, w.tchunk, k.tq, 0, (const float2 *)k.tw, fsm,
-		                            lut8, lut4, fcs, cta);
+		fstage_unit<1, 13, true, VAR>(m.m[k.member], k.first + w.item, w.tchunk, k.tq, 0, (const float2 *)k.tw, fsm,
+		                              lut8, lut4, fcs, cta);
 	}
 }
 
@@ -922,25 +934,30 @@ int fstage_multi_tq(int N, int nb, int tq)
 	return tq < 1 ? 1 : (tq > cap ? cap : tq);
 }
 
+template <int VAR>
+static void launch_multi_var(const FsMultiArgs &m, int nsm, cudaStream_t stream)
+{
+	// the wide units first: they are the longest
+	if(m.nunit[2 * VAR] > 0)
+	{
+		cudaFuncSetAttribute(k_fstage_pw<VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWideSmem);
+		cudaFuncSetAttribute(k_fstage_pw<VAR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+		const int n = m.nunit[2 * VAR], grid = n < 2 * nsm ? n : 2 * nsm;
+		k_fstage_pw<VAR><<<grid, 512, kWideSmem, stream>>>(m);
+	}
+	if(m.nunit[2 * VAR + 1] > 0)
+	{
+		cudaFuncSetAttribute(k_fstage_pn<VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNarrowSide);
+		cudaFuncSetAttribute(k_fstage_pn<VAR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+		const int n = m.nunit[2 * VAR + 1], grid = n < 3 * nsm ? n : 3 * nsm;
+		k_fstage_pn<VAR><<<grid, 256, kNarrowSide, stream>>>(m);
+	}
+}
+
 cudaError_t launch_fstage_multi(const FsMultiArgs &m, int nsm, cudaStream_t stream)
 {
-	if(m.nwide + m.nnarrow <= 0)
-		return cudaSuccess;
-	// the wide units first: they are the longest
-	if(m.nwide > 0)
-	{
-		cudaFuncSetAttribute(k_fstage_pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWideSmem);
-		cudaFuncSetAttribute(k_fstage_pw, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-		const int grid = m.nwide < 2 * nsm ? m.nwide : 2 * nsm;
-		k_fstage_pw<<<grid, 512, kWideSmem, stream>>>(m);
-	}
-	if(m.nnarrow > 0)
-	{
-		cudaFuncSetAttribute(k_fstage_pn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNarrowSide);
-		cudaFuncSetAttribute(k_fstage_pn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-		const int grid = m.nnarrow < 3 * nsm ? m.nnarrow : 3 * nsm;
-		k_fstage_pn<<<grid, 256, kNarrowSide, stream>>>(m);
-	}
+	launch_multi_var<0>(m, nsm, stream);
+	launch_multi_var<1>(m, nsm, stream);
 	return cudaGetLastError();
 }
 

@@ -170,7 +170,8 @@ bool fstage_plan(int N, int nb, int out, FKind *k);
 void launch_fstage_kind(const FKind &k, FsArgs a, cudaStream_t stream);
 
 // The persistent F-stage launches over the CUDA-core kinds of tensor-core-
-// form contexts (plain VDIF stations) of one context or several: CTAs take
+// form contexts (VDIF stations, plain or raw INTERLACEDVDIF reads) of one
+// context or several: CTAs take
 // work units from a list in order, each run as one CTA of launch_fstage_kind
 // runs it (tq x fpc FFT times of one work item).  Narrow units (FFTs of up to
 // 4096 points) run in CTAs of 256 threads, wide units (8192-point FFTs of one
@@ -180,7 +181,7 @@ constexpr int kFsMultiMembers = 16;
 constexpr int kFsMultiFc = 128;          // FFT constants of one narrow unit at most (tq x fpc)
 struct FsMultiKind {
 	const void *tw;                      // twiddles of length N
-	int32_t member, code;                // context; 32 x bands per item + log2 N
+	int32_t member, code;                // context; 64 x raw INTERLACEDVDIF reads + 32 x bands per item + log2 N
 	int32_t first, tq;                   // first FGroup of the kind, FFT iterations per unit
 };
 struct FsMultiUnit {
@@ -189,10 +190,11 @@ struct FsMultiUnit {
 struct FsMultiArgs {
 	FsArgs m[kFsMultiMembers];           // per context, with its subint's staging
 	const FsMultiKind *kinds;
-	const FsMultiUnit *units;            // wide units [0, nwide), then narrow ones
-	int32_t nwide, nnarrow;
-	int32_t *ctr;                        // two counters (wide, narrow), zero before the launch
+	const FsMultiUnit *units;            // four classes: wide and narrow units of plain VDIF, of raw reads
+	int32_t unit0[4], nunit[4];          // each class's first unit and units
+	int32_t *ctr;                        // one counter per class, zero before the launch
 };
+constexpr int kFsMultiClasses = 4;
 // whether a kind (FFT length N, bands per item nb) runs in the persistent
 // launches, and as a wide unit; the FFT iterations per unit for a kind's tq
 bool fstage_multi_shape(int N, int nb, bool *wide);
