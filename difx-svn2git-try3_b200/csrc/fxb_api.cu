@@ -799,7 +799,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				int logn = 0;
 				while((1 << logn) < k.N)
 					logn++;
-				mk.code = 64 * k.muxraw + 32 * k.nb + logn;
+				mk.code = 128 * k.muxraw + 32 * k.nb + logn;
 				mk.first = k.first;
 				mk.tq = fstage_multi_tq(k.N, k.nb, k.tq);
 				const int ki = (int)ctx->pkinds.size();

@@ -831,7 +831,7 @@ __device__ __forceinline__ void narrow_unit(const FsArgs &a, const FsMultiKind &
 {
 	const float2 *tw = (const float2 *)k.tw;
 	const int gi = k.first + w.item;
-	switch(k.code & 63)
+	switch(k.code & 127)
 	{
 #define FXB_MULTI_CASE(NV, LOGN)                                                                               \
 	case 32 * NV + LOGN:                                                                                       \

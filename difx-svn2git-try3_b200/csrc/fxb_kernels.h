@@ -181,7 +181,7 @@ constexpr int kFsMultiMembers = 16;
 constexpr int kFsMultiFc = 128;          // FFT constants of one narrow unit at most (tq x fpc)
 struct FsMultiKind {
 	const void *tw;                      // twiddles of length N
-	int32_t member, code;                // context; 64 x raw INTERLACEDVDIF reads + 32 x bands per item + log2 N
+	int32_t member, code;                // context; 128 x raw INTERLACEDVDIF reads + 32 x bands per item + log2 N
 	int32_t first, tq;                   // first FGroup of the kind, FFT iterations per unit
 };
 struct FsMultiUnit {
