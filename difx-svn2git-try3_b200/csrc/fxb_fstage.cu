@@ -79,6 +79,19 @@ __host__ __device__ constexpr int tw_offset(int N, int pass)
 	return o;
 }
 
+// padded index of element i + S r (i >= 0): for S a multiple of 16 the
+// padding of i + S r is that of i plus r S / 8, a constant offset per r.
+// Used for FFTs of 8192 points and more (FAST); shorter lengths keep the
+// plain form, whose register allocation measured better.
+template <int S, bool FAST>
+__device__ __forceinline__ int st_index(int i, int r)
+{
+	if constexpr(FAST && S % 16 == 0)
+		return xpad(i) + r * xpad(S);
+	else
+		return xpad(i + S * r);
+}
+
 // ---- lane values: FP32 complex
 struct cf { float x, y; };
 
@@ -257,7 +270,7 @@ __device__ __forceinline__ void mid_pass(int &wb, uint2 *side0, uint2 *side1, in
 			for(int j = 0; j < NV; j++)
 #pragma unroll
 				for(int r = 0; r < 8; r++)
-					sts(dst + j * PADN + xpad(q + s * (8 * p8 + r)), x[k][j][r]);
+					sts(dst + j * PADN + st_index<s, (N >= 8192)>(q + s * 8 * p8, r), x[k][j][r]);
 		}
 	}
 	if(!pp)
@@ -272,7 +285,7 @@ __device__ __forceinline__ void mid_pass(int &wb, uint2 *side0, uint2 *side1, in
 			for(int j = 0; j < NV; j++)
 #pragma unroll
 				for(int r = 0; r < 8; r++)
-					sts(dst + j * PADN + xpad(q + s * (8 * p8 + r)), x[k][j][r]);
+					sts(dst + j * PADN + st_index<s, (N >= 8192)>(q + s * 8 * p8, r), x[k][j][r]);
 		}
 	}
 	tm.sync();
@@ -680,7 +693,7 @@ __device__ __forceinline__ void fstage_unit(const FsArgs &a, const int gidx, con
 				{
 #pragma unroll
 					for(int r = 0; r < RL; r++)
-						y[j][r] = lds<C>(src + j * PADN + xpad(q + sL * r));
+						y[j][r] = lds<C>(src + j * PADN + st_index<sL, (N >= 8192)>(q, r));
 					dftR<RL>(y[j]);
 				}
 				if(!tok)
