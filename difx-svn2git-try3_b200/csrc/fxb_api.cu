@@ -785,7 +785,8 @@ static fxb_status setup_device(fxb_ctx *ctx)
 		// the persistent launches' work list: per kind tq x fpc FFT times of
 		// one item per unit, times outer and items inner
 		{
-			// classes: wide, narrow units of plain VDIF; wide, narrow of raw reads
+			// classes: wide, two-band narrow, one-band narrow units of plain
+			// VDIF, then of raw reads
 			std::vector<FsMultiUnit> cls[kFsMultiClasses];
 			for(const FKind &k : ctx->fkinds)
 			{
@@ -805,7 +806,7 @@ static fxb_status setup_device(fxb_ctx *ctx)
 				const int ki = (int)ctx->pkinds.size();
 				ctx->pkinds.push_back(mk);
 				const int per = mk.tq * k.fpc, nt = (ctx->T + per - 1) / per;
-				std::vector<FsMultiUnit> &dst = cls[2 * k.muxraw + (w ? 0 : 1)];
+				std::vector<FsMultiUnit> &dst = cls[3 * k.muxraw + (w ? 0 : 3 - k.nb)];
 				for(int t = 0; t < nt; t++)
 					for(int it = 0; it < k.count; it++)
 						dst.push_back(FsMultiUnit{ki, it, t});

@@ -838,34 +838,30 @@ __global__ void __launch_bounds__(FShape<LOGN>::NT, fstage_minb<LOGN>()) k_fstag
 constexpr size_t kNarrowSide = 36864;            // exchange buffer: 2048 points x 2 bands (or 4096 x 1), padded
 constexpr size_t kWideSmem = 73728;              // 8192 points of one band, padded
 
-template <int VAR, class Team>
+template <int VAR, int NV, class Team>
 __device__ __forceinline__ void narrow_unit(const FsArgs &a, const FsMultiKind &k, const FsMultiUnit &w, uint2 *fsm,
                                             const float *lut8, const float2 *lut4, FftConst *fcs, const Team &tm)
 {
 	const float2 *tw = (const float2 *)k.tw;
 	const int gi = k.first + w.item;
-	switch(k.code & 127)
+	switch(k.code & 31)
 	{
-#define FXB_MULTI_CASE(NV, LOGN)                                                                               \
-	case 32 * NV + LOGN:                                                                                       \
+#define FXB_MULTI_CASE(LOGN)                                                                                   \
+	case LOGN:                                                                                                 \
 		fstage_unit<NV, LOGN, true, VAR>(a, gi, w.tchunk, k.tq, 0, tw, fsm, lut8, lut4, fcs, tm);             \
 		break;
-		FXB_MULTI_CASE(2, 5)
-		FXB_MULTI_CASE(2, 6)
-		FXB_MULTI_CASE(2, 7)
-		FXB_MULTI_CASE(2, 8)
-		FXB_MULTI_CASE(2, 9)
-		FXB_MULTI_CASE(2, 10)
-		FXB_MULTI_CASE(2, 11)
-		FXB_MULTI_CASE(1, 5)
-		FXB_MULTI_CASE(1, 6)
-		FXB_MULTI_CASE(1, 7)
-		FXB_MULTI_CASE(1, 8)
-		FXB_MULTI_CASE(1, 9)
-		FXB_MULTI_CASE(1, 10)
-		FXB_MULTI_CASE(1, 11)
-		FXB_MULTI_CASE(1, 12)
+		FXB_MULTI_CASE(5)
+		FXB_MULTI_CASE(6)
+		FXB_MULTI_CASE(7)
+		FXB_MULTI_CASE(8)
+		FXB_MULTI_CASE(9)
+		FXB_MULTI_CASE(10)
+		FXB_MULTI_CASE(11)
 #undef FXB_MULTI_CASE
+	case 12:
+		if constexpr(NV == 1)
+			fstage_unit<1, 12, true, VAR>(a, gi, w.tchunk, k.tq, 0, tw, fsm, lut8, lut4, fcs, tm);
+		break;
 	default:
 		break;
 	}
@@ -884,8 +880,10 @@ __device__ __forceinline__ int next_unit(int32_t *ctr, int *slot)
 
 // One exchange buffer per unit (three CTAs per SM): faster than two buffers
 // at two CTAs per SM on every c3 length measured.  VAR 0: plain VDIF, 1: raw
-// INTERLACEDVDIF reads; work-list class 2 VAR + 1.
-template <int VAR>
+// INTERLACEDVDIF reads; NV: bands per item (an instance each keeps the
+// register allocation of every length close to its own kernel's); work-list
+// class 3 VAR + 3 - NV.
+template <int VAR, int NV>
 __global__ void __launch_bounds__(256, 3) k_fstage_pn(const __grid_constant__ FsMultiArgs m)
 {
 	extern __shared__ __align__(16) uint2 fsm[];
@@ -894,7 +892,7 @@ __global__ void __launch_bounds__(256, 3) k_fstage_pn(const __grid_constant__ Fs
 	__shared__ FftConst fcs[kFsMultiFc];
 	__shared__ int unit_s;
 	const CtaTeam cta;
-	constexpr int cls = 2 * VAR + 1;
+	constexpr int cls = 3 * VAR + 3 - NV;
 	fstage_luts(cta, true, lut8, lut4);
 	for(;;)
 	{
@@ -903,11 +901,11 @@ __global__ void __launch_bounds__(256, 3) k_fstage_pn(const __grid_constant__ Fs
 			break;
 		const FsMultiUnit w = m.units[m.unit0[cls] + u];
 		const FsMultiKind k = m.kinds[w.kind];
-		narrow_unit<VAR>(m.m[k.member], k, w, fsm, lut8, lut4, fcs, cta);
+		narrow_unit<VAR, NV>(m.m[k.member], k, w, fsm, lut8, lut4, fcs, cta);
 	}
 }
 
-// work-list class 2 VAR
+// work-list class 3 VAR
 template <int VAR>
 __global__ void __launch_bounds__(512, 2) k_fstage_pw(const __grid_constant__ FsMultiArgs m)
 {
@@ -917,7 +915,7 @@ __global__ void __launch_bounds__(512, 2) k_fstage_pw(const __grid_constant__ Fs
 	__shared__ FftConst fcs[kMaxTQ];
 	__shared__ int unit_s;
 	const CtaTeam cta;
-	constexpr int cls = 2 * VAR;
+	constexpr int cls = 3 * VAR;
 	fstage_luts(cta, true, lut8, lut4);
 	for(;;)
 	{
@@ -951,20 +949,23 @@ template <int VAR>
 static void launch_multi_var(const FsMultiArgs &m, int nsm, cudaStream_t stream)
 {
 	// the wide units first: they are the longest
-	if(m.nunit[2 * VAR] > 0)
+	if(m.nunit[3 * VAR] > 0)
 	{
 		cudaFuncSetAttribute(k_fstage_pw<VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWideSmem);
 		cudaFuncSetAttribute(k_fstage_pw<VAR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-		const int n = m.nunit[2 * VAR], grid = n < 2 * nsm ? n : 2 * nsm;
+		const int n = m.nunit[3 * VAR], grid = n < 2 * nsm ? n : 2 * nsm;
 		k_fstage_pw<VAR><<<grid, 512, kWideSmem, stream>>>(m);
 	}
-	if(m.nunit[2 * VAR + 1] > 0)
-	{
-		cudaFuncSetAttribute(k_fstage_pn<VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNarrowSide);
-		cudaFuncSetAttribute(k_fstage_pn<VAR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-		const int n = m.nunit[2 * VAR + 1], grid = n < 3 * nsm ? n : 3 * nsm;
-		k_fstage_pn<VAR><<<grid, 256, kNarrowSide, stream>>>(m);
-	}
+	auto narrow = [&](auto kern, int cls) {
+		if(m.nunit[cls] <= 0)
+			return;
+		cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNarrowSide);
+		cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+		const int n = m.nunit[cls], grid = n < 3 * nsm ? n : 3 * nsm;
+		kern<<<grid, 256, kNarrowSide, stream>>>(m);
+	};
+	narrow(k_fstage_pn<VAR, 2>, 3 * VAR + 1);
+	narrow(k_fstage_pn<VAR, 1>, 3 * VAR + 2);
 }
 
 cudaError_t launch_fstage_multi(const FsMultiArgs &m, int nsm, cudaStream_t stream)

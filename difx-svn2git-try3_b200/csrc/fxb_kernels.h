@@ -190,11 +190,12 @@ struct FsMultiUnit {
 struct FsMultiArgs {
 	FsArgs m[kFsMultiMembers];           // per context, with its subint's staging
 	const FsMultiKind *kinds;
-	const FsMultiUnit *units;            // four classes: wide and narrow units of plain VDIF, of raw reads
-	int32_t unit0[4], nunit[4];          // each class's first unit and units
+	const FsMultiUnit *units;            // six classes: wide, two-band narrow and one-band narrow units
+	                                     // of plain VDIF, then of raw reads
+	int32_t unit0[6], nunit[6];          // each class's first unit and units
 	int32_t *ctr;                        // one counter per class, zero before the launch
 };
-constexpr int kFsMultiClasses = 4;
+constexpr int kFsMultiClasses = 6;
 // whether a kind (FFT length N, bands per item nb) runs in the persistent
 // launches, and as a wide unit; the FFT iterations per unit for a kind's tq
 bool fstage_multi_shape(int N, int nb, bool *wide);
