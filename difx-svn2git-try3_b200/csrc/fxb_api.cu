@@ -2446,7 +2446,7 @@ fxb_batch *fxb_batch_create(fxb_ctx *const *members, int32_t n, fxb_status *stat
 	for(int i = 0; i < n; i++)
 	{
 		if(!members[i] || members[i]->batched || members[i]->slots.size() != members[0]->slots.size() ||
-		   members[i]->next_slot != members[0]->next_slot)
+		   members[i]->next_slot != members[0]->next_slot || members[i]->device != members[0]->device)
 			return fail(FXB_ERR_ARG);
 		for(int j = 0; j < i; j++)
 			if(members[j] == members[i])

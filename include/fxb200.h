@@ -256,7 +256,8 @@ FXB_API fxb_status fxb_tuning_report(const fxb_ctx *ctx, char *buf, size_t len, 
  * subint's F stage.  Results do not depend on the mode.  A
  * member takes no fxb_submit_subint of its own while it belongs to a batch;
  * its results are read and reset through the usual calls (ordered after the
- * batch's launches).  All members need the same max_subints_in_flight. */
+ * batch's launches).  All members need the same max_subints_in_flight and
+ * device; call the batch functions with that device current. */
 typedef struct fxb_batch fxb_batch;
 typedef struct {
 	const uint8_t *const *bufs;       /* [nstation] host station buffers */
