@@ -42,7 +42,7 @@
  * double-precision expressions term by term.  The floating-point signal path
  * (rotators, FFT, products, sums) is evaluated in double with exact
  * sin/cos, so the result is the reference's algorithm without its FP32
- * rounding: the FP64 oracle the FP32 and tensor-core forms are judged by.
+ * rounding: the FP64 oracle the FP32 and tensor-core forms are checked against.
  *
  * Compile with -ffp-contract=off so that the double expressions that decide
  * integers are evaluated exactly as written.

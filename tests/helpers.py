@@ -6,10 +6,10 @@ import numpy as np
 from fxb200 import synth
 from fxb200.job import Freq, Job, full_job
 
-# FP32 form vs the FP64 oracle: relative visibility tolerance (north star)
+# FP32 form vs the FP64 oracle: relative visibility tolerance of the FP32 form
 FP32_TOL = 1e-5
 # tensor-core form (FP16 spectra, FP32 accumulation) vs the FP64 oracle:
-# relative visibility tolerance (north star), applied norm-wise to the cross
+# relative visibility tolerance of the tensor-core forms, applied norm-wise to the cross
 # and autocorrelations and as the rms of the per-visibility relative
 # amplitude and phase (radians) errors
 TC_REL_TOL = 1e-3

@@ -9,7 +9,7 @@ norm-wise relative cross and autocorrelation errors, per-visibility relative
 amplitude and phase (radians) errors (rms and 99th percentile), the error in
 correlation-coefficient units, and the band-averaged amplitude and phase
 errors of each (baseline, product, band), where the common sky signal
-dominates.  Gates (north star): the FP32 form within 1e-5 norm-wise, the
+dominates.  Gates (the stated tolerances): the FP32 form within 1e-5 norm-wise, the
 FP16 tensor-core form within 1e-3 (``helpers.assert_tc_gate``).  With
 FXB_REPORT_DIR set the table is written there as precision_c2.json."""
 import json

@@ -2,7 +2,7 @@
 
 The headline tensor-core form keeps the F stage's spectra in FP16 (11-bit
 significands, ~2^-12 relative rounding per value) and accumulates in FP32.
-Its gate is the north star's relative visibility tolerance, 1e-3
+Its gate is the stated relative visibility tolerance of the tensor-core form, 1e-3
 (``helpers.TC_REL_TOL``): norm-wise over the cross and autocorrelations and
 as the rms of the per-visibility relative amplitude and phase errors.  BF16
 spectra (8-bit significands) are kept as a measured alternative: a value's
