@@ -2310,21 +2310,12 @@ static void batch_fused_launch(fxb_batch *b, int k, const std::vector<Slot *> &s
 		cudaEventRecord(b->join[i], b->m[i]->stream);
 		cudaStreamWaitEvent(b->stream, b->join[i], 0);
 	}
+	// the F launches as parallel branches: each member's tensor-core FFT kinds
+	// on its own stream, the persistent class kernels on the streams of
+	// members without such kinds (or on the batch stream), so that each fills
+	// the others' tails
 	FsMultiArgs ma;
 	memset(&ma, 0, sizeof(ma));
-	for(size_t i = 0; i < n; i++)
-	{
-		fxb_ctx *c = b->m[i];
-		ma.m[i] = fs_args(c, *slots[i]);
-		ma.m[i].spec = b->fspec[k][i];
-		for(const FKind &fk : c->fkinds)
-			if(fk.tcfft)
-			{
-				const cudaError_t le = launch_fstage_tc(fk, ma.m[i], c->nsm, b->stream);
-				if(le != cudaSuccess && c->launch_err == cudaSuccess)
-					c->launch_err = le;
-			}
-	}
 	ma.kinds = b->d_kinds;
 	ma.units = b->d_units;
 	for(int cl = 0; cl < kFsMultiClasses; cl++)
@@ -2334,9 +2325,51 @@ static void batch_fused_launch(fxb_batch *b, int k, const std::vector<Slot *> &s
 	}
 	ma.ctr = b->d_ctr;
 	cudaMemsetAsync(b->d_ctr, 0, kFsMultiClasses * sizeof(int32_t), b->stream);
-	const cudaError_t le = launch_fstage_multi(ma, b->m[0]->nsm, b->stream);
+	cudaEventRecord(b->fork, b->stream);
+	std::vector<cudaStream_t> free_st;
+	std::vector<char> used(n, 0);
+	for(size_t i = 0; i < n; i++)
+	{
+		fxb_ctx *c = b->m[i];
+		ma.m[i] = fs_args(c, *slots[i]);
+		ma.m[i].spec = b->fspec[k][i];
+		bool tc = false;
+		for(const FKind &fk : c->fkinds)
+			tc = tc || fk.tcfft;
+		if(!tc)
+		{
+			free_st.push_back(c->stream);
+			continue;
+		}
+		cudaStreamWaitEvent(c->stream, b->fork, 0);
+		used[i] = 1;
+		for(const FKind &fk : c->fkinds)
+			if(fk.tcfft)
+			{
+				const cudaError_t le = launch_fstage_tc(fk, ma.m[i], c->nsm, c->stream);
+				if(le != cudaSuccess && c->launch_err == cudaSuccess)
+					c->launch_err = le;
+			}
+	}
+	const size_t nps = std::min<size_t>(free_st.size(), 2 * kFsMultiClasses);
+	free_st.resize(nps);
+	for(size_t j = 0; j < n && nps; j++)
+		if(!used[j] && std::find(free_st.begin(), free_st.end(), b->m[j]->stream) != free_st.end())
+		{
+			cudaStreamWaitEvent(b->m[j]->stream, b->fork, 0);
+			used[j] = 1;
+		}
+	if(nps == 0)
+		free_st.assign(1, b->stream);
+	const cudaError_t le = launch_fstage_multi_on(ma, b->m[0]->nsm, free_st.data(), (int)free_st.size());
 	if(le != cudaSuccess && b->m[0]->launch_err == cudaSuccess)
 		b->m[0]->launch_err = le;
+	for(size_t i = 0; i < n; i++)
+		if(used[i])
+		{
+			cudaEventRecord(b->join[i], b->m[i]->stream);
+			cudaStreamWaitEvent(b->stream, b->join[i], 0);
+		}
 	cudaEventRecord(b->fork, b->stream);
 	for(size_t i = 0; i < n; i++)
 	{

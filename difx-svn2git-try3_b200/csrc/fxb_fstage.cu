@@ -945,16 +945,18 @@ int fstage_multi_tq(int N, int nb, int tq)
 	return tq < 1 ? 1 : (tq > cap ? cap : tq);
 }
 
+// class kernels of one read form, each on the next stream of the set
 template <int VAR>
-static void launch_multi_var(const FsMultiArgs &m, int nsm, cudaStream_t stream)
+static void launch_multi_var(const FsMultiArgs &m, int nsm, const cudaStream_t *streams, int nstream, int &next)
 {
+	auto pick = [&]() { return streams[(next++) % nstream]; };
 	// the wide units first: they are the longest
 	if(m.nunit[3 * VAR] > 0)
 	{
 		cudaFuncSetAttribute(k_fstage_pw<VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWideSmem);
 		cudaFuncSetAttribute(k_fstage_pw<VAR>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 		const int n = m.nunit[3 * VAR], grid = n < 2 * nsm ? n : 2 * nsm;
-		k_fstage_pw<VAR><<<grid, 512, kWideSmem, stream>>>(m);
+		k_fstage_pw<VAR><<<grid, 512, kWideSmem, pick()>>>(m);
 	}
 	auto narrow = [&](auto kern, int cls) {
 		if(m.nunit[cls] <= 0)
@@ -962,7 +964,7 @@ static void launch_multi_var(const FsMultiArgs &m, int nsm, cudaStream_t stream)
 		cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNarrowSide);
 		cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 		const int n = m.nunit[cls], grid = n < 3 * nsm ? n : 3 * nsm;
-		kern<<<grid, 256, kNarrowSide, stream>>>(m);
+		kern<<<grid, 256, kNarrowSide, pick()>>>(m);
 	};
 	narrow(k_fstage_pn<VAR, 2>, 3 * VAR + 1);
 	narrow(k_fstage_pn<VAR, 1>, 3 * VAR + 2);
@@ -970,8 +972,14 @@ static void launch_multi_var(const FsMultiArgs &m, int nsm, cudaStream_t stream)
 
 cudaError_t launch_fstage_multi(const FsMultiArgs &m, int nsm, cudaStream_t stream)
 {
-	launch_multi_var<0>(m, nsm, stream);
-	launch_multi_var<1>(m, nsm, stream);
+	return launch_fstage_multi_on(m, nsm, &stream, 1);
+}
+
+cudaError_t launch_fstage_multi_on(const FsMultiArgs &m, int nsm, const cudaStream_t *streams, int nstream)
+{
+	int next = 0;
+	launch_multi_var<0>(m, nsm, streams, nstream, next);
+	launch_multi_var<1>(m, nsm, streams, nstream, next);
 	return cudaGetLastError();
 }
 

@@ -201,6 +201,9 @@ constexpr int kFsMultiClasses = 6;
 bool fstage_multi_shape(int N, int nb, bool *wide);
 int fstage_multi_tq(int N, int nb, int tq);
 cudaError_t launch_fstage_multi(const FsMultiArgs &m, int nsm, cudaStream_t stream);
+// the same with the class kernels spread over streams (each kernel on the
+// next stream of the set), for callers that run them as parallel branches
+cudaError_t launch_fstage_multi_on(const FsMultiArgs &m, int nsm, const cudaStream_t *streams, int nstream);
 // F stage of the tensor-core form with the FFT on the tensor cores (N = 2048;
 // csrc/fxb_fstage_tc.cu).  Eligible: 2048-point FFTs, fringe rotation order
 // 1 (or 0 with upper sidebands only), 2-bit stations of 2..32 bands (all
