@@ -49,7 +49,9 @@ def tc_errors(job, layout, n, got, ref):
                                 dict(nstation=10, full_pol=True, nchan=256),
                                 dict(nstation=3, nchan=1024, bw=32.0, nfreq=8, full_pol=True, subint_ns=2_048_000),
                                 dict(nstation=4, nchan=512, bw=16.0, nfreq=2, full_pol=True, nbits=8,
-                                     subint_ns=2_048_000)])
+                                     subint_ns=2_048_000),
+                                # one band per work item (the one-band persistent F kernel)
+                                dict(nstation=4, nchan=256, bw=16.0, nfreq=2, full_pol=False)])
 def test_fp16_tensor_core_vs_fp64(kw):
     job = small_job(**kw)
     got, ref, layout, n = run_tc(job, [(0, 1_024_000), (0, 3_072_000)])
