@@ -49,9 +49,13 @@ def _muxed_and_raw(job, sec, ns, k, rng):
     return muxed, raw
 
 
-@pytest.mark.parametrize("masklength,xmac", [(4, "fp32"), (2, "fp16")])
-def test_fused_raw_reads_equal_muxed_frames(masklength, xmac):
-    job = mux_job(masklength=masklength)
+@pytest.mark.parametrize("masklength,xmac,kw", [(4, "fp32", {}), (2, "fp16", {}),
+                                                # one band per work item; 8192-point FFTs (the
+                                                # persistent F kernels' other raw-read classes)
+                                                (2, "fp16", dict(full_pol=False)),
+                                                (2, "fp16", dict(nchan=4096, bw=16.0))])
+def test_fused_raw_reads_equal_muxed_frames(masklength, xmac, kw):
+    job = mux_job(masklength=masklength, **kw)
     fused = copy.deepcopy(job)
     for st in fused.stations:
         if st.mux_threads:
