@@ -2292,8 +2292,8 @@ static fxb_status batch_fused_plan(fxb_batch *b)
 
 // The fused F part of one subint (slot k) on the batch stream: every
 // member's preparation as a branch, then the members' tensor-core FFT kinds
-// and the persistent F launches into slot k's spectra, then the members'
-// weights as branches.
+// and the persistent F launches into slot k's spectra (each its own branch),
+// then the members' weights as branches.
 static void batch_fused_launch(fxb_batch *b, int k, const std::vector<Slot *> &slots, bool capture)
 {
 	const unsigned evf = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
