@@ -1246,10 +1246,16 @@ static void launch_prep(fxb_ctx *ctx, const Slot &sl, cudaStream_t st, unsigned 
 {
 	const Job &job = ctx->job;
 	cudaEventRecordWithFlags(sl.tev[0], st, evf);
-	launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, st);
 	if(ctx->nraw)
+	{
+		launch_interpolators(ctx->d_st, sl.d_sub, ctx->S, ctx->T, st);
 		launch_mux_raw(ctx->d_st, sl.d_sub, ctx->S, 0, 0, st);
-	launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->d_bandok, ctx->valid_stride, ctx->S, st, ctx->d_fillok);
+		launch_frame_valid(ctx->d_st, sl.d_sub, ctx->d_valid, ctx->d_bandok, ctx->valid_stride, ctx->S, st,
+		                   ctx->d_fillok);
+	}
+	else
+		fxb::launch_prep(ctx->d_st, sl.d_sub, ctx->S, ctx->T, ctx->d_valid, ctx->d_bandok, ctx->valid_stride, st,
+		                 ctx->d_fillok);
 	launch_fft_params(ctx->d_st, sl.d_sub, sl.d_vflags, ctx->nflagint, ctx->d_valid, ctx->d_bandok, ctx->valid_stride,
 	                  ctx->S, ctx->T, job.fringe_rot_order, ctx->d_params, ctx->d_pbw, ctx->nbm, st, ctx->d_fillok);
 	cudaEventRecordWithFlags(sl.tev[1], st, evf);

@@ -56,16 +56,17 @@ __device__ __forceinline__ uint32_t edv4_bands(const DevStation &S, const DevSub
 	return ok | (nch < 32 ? ~((1u << nch) - 1u) : 0u);
 }
 
-__global__ void k_frame_valid(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
-                              uint8_t *__restrict__ valid, uint32_t *__restrict__ bandok, int64_t valid_stride,
-                              uint8_t *__restrict__ fillok)
+// block bx of gx blocks of station s's frame-validity pass
+__device__ __forceinline__ void frame_valid_blk(const DevStation *__restrict__ st, const DevSubintStation *sub,
+                                                uint8_t *__restrict__ valid, uint32_t *__restrict__ bandok,
+                                                int64_t valid_stride, uint8_t *__restrict__ fillok, int s, int bx,
+                                                int gx)
 {
-	const int s = blockIdx.y;
 	const DevStation &S = st[s];
 	const DevSubintStation &U = sub[s];
 	const int64_t nframes = U.nbytes / S.framebytes;
 	const uint64_t FILL = 0x1122334411223344ULL;
-	for(int64_t fr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; fr < valid_stride; fr += (int64_t)gridDim.x * blockDim.x)
+	for(int64_t fr = bx * (int64_t)blockDim.x + threadIdx.x; fr < valid_stride; fr += (int64_t)gx * blockDim.x)
 	{
 		uint8_t v = 0, nofill = 0;
 		// raw INTERLACEDVDIF reads: the muxed frame's header and first and last
@@ -95,6 +96,13 @@ __global__ void k_frame_valid(const DevStation *__restrict__ st, const DevSubint
 		if(bandok)
 			bandok[s * valid_stride + fr] = (v && S.mux) ? edv4_bands(S, U, f) : 0xFFFFFFFFu;
 	}
+}
+
+__global__ void k_frame_valid(const DevStation *__restrict__ st, const DevSubintStation *__restrict__ sub,
+                              uint8_t *__restrict__ valid, uint32_t *__restrict__ bandok, int64_t valid_stride,
+                              uint8_t *__restrict__ fillok)
+{
+	frame_valid_blk(st, sub, valid, bandok, valid_stride, fillok, blockIdx.y, blockIdx.x, gridDim.x);
 }
 
 // Model::calculateDelayInterpolator, order 2 (model.cpp:229-299), with the
@@ -133,6 +141,29 @@ __device__ bool delay_interpolator(const DevStation &S, int blockspersend, int s
 	c[1] = (-3.0 * d[0] + 4.0 * d[1] - d[2]) / blockspersend;
 	c[2] = d[0];
 	return true;
+}
+
+// The interpolators and the frame-validity pass of a subint as one launch
+// (neither reads what the other writes): blocks x < gx check station y's
+// frames, block gx computes station y's interpolator.
+__global__ void k_prep(const DevStation *__restrict__ st, DevSubintStation *sub, int blockspersend,
+                       uint8_t *__restrict__ valid, uint32_t *__restrict__ bandok, int64_t valid_stride,
+                       uint8_t *__restrict__ fillok, int gx)
+{
+	const int s = blockIdx.y;
+	if((int)blockIdx.x < gx)
+	{
+		frame_valid_blk(st, sub, valid, bandok, valid_stride, fillok, s, blockIdx.x, gx);
+		return;
+	}
+	if(threadIdx.x != 0 || sub[s].interp_given)
+		return;
+	double c[3] = {0.0, 0.0, 0.0};
+	const bool ok = delay_interpolator(st[s], blockspersend, sub[s].subsec, sub[s].subns, c);
+	sub[s].interp[0] = c[0];
+	sub[s].interp[1] = c[1];
+	sub[s].interp[2] = c[2];
+	sub[s].invalid_subint = ok ? 0 : 1;
 }
 
 __global__ void k_interpolators(const DevStation *__restrict__ st, DevSubintStation *__restrict__ sub, int S,
@@ -368,6 +399,13 @@ void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8
 {
 	dim3 grid((unsigned)((valid_stride + 255) / 256 < 64 ? (valid_stride + 255) / 256 : 64), S);
 	k_frame_valid<<<grid, 256, 0, stream>>>(st, sub, valid, bandok, valid_stride, fillok);
+}
+
+void launch_prep(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, uint8_t *valid,
+                 uint32_t *bandok, int64_t valid_stride, cudaStream_t stream, uint8_t *fillok)
+{
+	const int gx = (int)((valid_stride + 255) / 256 < 64 ? (valid_stride + 255) / 256 : 64);
+	k_prep<<<dim3(gx + 1, S), 256, 0, stream>>>(st, sub, blockspersend, valid, bandok, valid_stride, fillok, gx);
 }
 
 void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, cudaStream_t stream)

@@ -59,6 +59,10 @@ void launch_frame_valid(const DevStation *st, const DevSubintStation *sub, uint8
                         int64_t valid_stride, int S, cudaStream_t stream, uint8_t *fillok = nullptr);
 // the subint time is read from sub[s].subsec / subns
 void launch_interpolators(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, cudaStream_t stream);
+// launch_interpolators and launch_frame_valid as one launch (stations without
+// raw INTERLACEDVDIF reads, whose frame check needs the placement first)
+void launch_prep(const DevStation *st, DevSubintStation *sub, int S, int blockspersend, uint8_t *valid,
+                 uint32_t *bandok, int64_t valid_stride, cudaStream_t stream, uint8_t *fillok);
 void launch_fft_params(const DevStation *st, const DevSubintStation *sub, const int32_t *validflags, int nflagint,
                        const uint8_t *valid, const uint32_t *bandok, int64_t valid_stride, int S, int T, int order,
                        FftParam *out, float *pbw, int nbm, cudaStream_t stream, const uint8_t *fillok = nullptr);
