@@ -294,19 +294,23 @@ def load_traffic(kernel):
         return None
 
 
-def h2d_link_gbs():
-    """Host-to-device copy bandwidth from page-locked memory: 256 MB copied as
-    16 MB pieces back to back on one stream (the end-to-end path copies a
-    subint of ~21 MB at a time), best of 10 after an untimed round that maps
-    the buffers; the ceiling of the end-to-end figure."""
+def h2d_link_gbs(blocks=None):
+    """Host-to-device copy bandwidth from page-locked memory, the ceiling of
+    the end-to-end figure: the given page-locked blocks (the end-to-end path's
+    own subint blocks, one copy each) or 256 MB copied as 16 MB pieces, back
+    to back on one stream; best of 10 after an untimed round that maps the
+    buffers."""
     import torch
-    n, piece = 256 << 20, 16 << 20
-    src = torch.empty(n, dtype=torch.uint8).pin_memory()
-    dst = torch.empty(n, dtype=torch.uint8, device="cuda")
+    if blocks is None:
+        n, piece = 256 << 20, 16 << 20
+        src = torch.empty(n, dtype=torch.uint8).pin_memory()
+        blocks = [src[o:o + piece] for o in range(0, n, piece)]
+    dst = torch.empty(max(b.numel() for b in blocks), dtype=torch.uint8, device="cuda")
+    total = sum(b.numel() for b in blocks)
 
     def once():
-        for o in range(0, n, piece):
-            dst[o:o + piece].copy_(src[o:o + piece], non_blocking=True)
+        for b in blocks:
+            dst[:b.numel()].copy_(b, non_blocking=True)
 
     once()
     torch.cuda.synchronize()
@@ -317,8 +321,8 @@ def h2d_link_gbs():
         once()
         e1.record()
         e1.synchronize()
-        best = max(best, n / (e0.elapsed_time(e1) * 1e-3) / 1e9)
-    del src, dst
+        best = max(best, total / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del dst
     return best
 
 
@@ -667,11 +671,13 @@ def gpu_arm(args, job):
     S = len(job.stations)
     dev = []        # [k][s] device tensors
     host = []       # [k][s] pinned host tensors
+    blocks = []                       # the page-locked subint blocks (the link probe copies them too)
     for (_, inputs) in pool:
         dev.append([torch.from_numpy(b).to("cuda") for b, _, _ in inputs])
         # the subint's station buffers one after the other in one page-locked
         # block, as a datastream's receive ring holds them: one copy per subint
         blk = torch.from_numpy(np.concatenate([b for b, _, _ in inputs])).pin_memory()
+        blocks.append(blk)
         offs = np.cumsum([0] + [b.size for b, _, _ in inputs])
         host.append([blk[int(offs[i]):int(offs[i + 1])] for i in range(len(inputs))])
     nbytes = [[b.size for b, _, _ in inputs] for (_, inputs) in pool]
@@ -857,15 +863,16 @@ def gpu_arm(args, job):
         mux = mux_leg(args)
         muxf = mux_fused_leg(args)
 
-    # per subint: interpolators, frame validity, FFT parameters, one F-stage
-    # launch per FFT length, one XMAC launch per group of equally shaped
+    # per subint: interpolators and frame validity (one launch), FFT
+    # parameters, one F-stage launch per FFT length (the workload's are
+    # tensor-core FFT kinds), one XMAC launch per group of equally shaped
     # subbands, weights
     shapes = {(sum(1 for st in job.stations for fb, _ in st.bands if fb == f), job.freqs[f].nchan)
               for f in range(len(job.freqs)) if any(fb == f for st in job.stations for fb, _ in st.bands)}
     flens = {2 * job.freqs[st.bands[0][0]].nchan for st in job.stations}
-    launches_per_subint = 3 + len(flens) + len(shapes) + 1
+    launches_per_subint = 2 + len(flens) + len(shapes) + 1
     if rank == 0:
-        link = h2d_link_gbs() if world == 1 else None
+        link = h2d_link_gbs(blocks) if world == 1 else None
         e2e_gbs = h2d / (e2e_ms / args.steps * 1e-3) / 1e9
         # the full record first, then the headline line (last, compact) carrying
         # the secondary figures
